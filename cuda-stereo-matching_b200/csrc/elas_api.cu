@@ -1,0 +1,538 @@
+// C ABI and host orchestration of the B200 ELAS pipeline.
+//
+// Replaces Elas::process and its helpers (src/Elas.cu:19-565).  Differences
+// in how the work is organised, not in what is computed:
+//  * one device workspace arena per handle, grown on demand; the reference
+//    allocates (and partly leaks, src/Elas.cu:349-371) every buffer per call;
+//  * no host round trips inside the pipeline: the support-point count and the
+//    triangle counts stay on the device (the reference reads num_sp back,
+//    src/Elas.cu:374, and triangulates on the CPU, :282-328);
+//  * errors are returned as status codes instead of exit() (src/Utils.h:11-38).
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/elas_b200.h"
+#include "common.cuh"
+#include "kernels.h"
+
+using namespace elas;
+
+struct elas_handle {
+    elas_params params;
+    int device = 0;
+    int num_sms = 0;
+    int flip_blocks = 0;
+    std::string last_error;
+    int64_t launches = 0;
+
+    // workspace arena
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    Geom g{};          // geometry of the last call
+    bool have_last = false;
+
+    uint8_t *img0 = nullptr, *img1 = nullptr;
+    uint4 *desc0 = nullptr, *desc1 = nullptr;
+    int32_t *can_lr = nullptr, *can = nullptr, *row_cnt = nullptr, *row_off = nullptr;
+    int32_t *uvd = nullptr, *x0 = nullptr, *x1 = nullptr, *y = nullptr;
+    uint32_t *gtmp0 = nullptr, *gtmp1 = nullptr, *grid0 = nullptr, *grid1 = nullptr;
+    DelDev del[2]{};
+    unsigned long long *prior0 = nullptr, *prior1 = nullptr;
+    float *raw0 = nullptr, *raw1 = nullptr, *lr0 = nullptr, *lr1 = nullptr, *tmp = nullptr;
+    float *out0 = nullptr, *out1 = nullptr;
+    int32_t *lab = nullptr, *usize = nullptr;
+    unsigned* err = nullptr;
+};
+
+namespace {
+
+int fail(elas_handle* h, int code, const std::string& msg) {
+    if (h) h->last_error = msg;
+    return code;
+}
+
+int cuda_fail(elas_handle* h, cudaError_t e, const char* where) {
+    return fail(h, ELAS_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                      \
+    do {                                                              \
+        cudaError_t e_ = (call);                                      \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #call);        \
+    } while (0)
+
+size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+uint32_t next_pow2(size_t x) {
+    uint32_t c = 64;
+    while (c < x) c <<= 1;
+    return c;
+}
+
+int check_params(const elas_params& p, std::string& why) {
+    if (p.subsampling) { why = "subsampling is not supported"; return ELAS_ERR_UNSUPPORTED; }
+    if (p.candidate_stepsize < 1) { why = "candidate_stepsize must be >= 1"; return ELAS_ERR_INVALID_ARG; }
+    if (p.grid_size < 1) { why = "grid_size must be >= 1"; return ELAS_ERR_INVALID_ARG; }
+    if (p.disp_max < 1 || p.disp_max > 4095) { why = "disp_max must be in [1, 4095]"; return ELAS_ERR_INVALID_ARG; }
+    if (p.disp_min > p.disp_max) { why = "disp_min > disp_max"; return ELAS_ERR_INVALID_ARG; }
+    if (!(p.beta > 0.0f) || !(p.gamma > 0.0f) || !(p.sigma > 0.0f) || !(p.sradius >= 0.0f)) {
+        why = "beta, gamma, sigma must be > 0 and sradius >= 0";
+        return ELAS_ERR_INVALID_ARG;
+    }
+    float r = std::max(std::ceil(p.sigma * p.sradius), 2.0f);
+    if (r > 15.0f) { why = "sigma*sradius must be <= 15"; return ELAS_ERR_UNSUPPORTED; }
+    if (p.incon_window_size < 0) { why = "incon_window_size must be >= 0"; return ELAS_ERR_INVALID_ARG; }
+    return ELAS_OK;
+}
+
+// P(|d - d_plane|) of kerComputeDisparity (src/Kernels/KerComputeDisparity.cu:
+// 270-271) evaluated once on the host: float exp/log, double division by beta.
+int penalty(int dd, const elas_params& p) {
+    float two_sigma_squared = 2 * p.sigma * p.sigma;
+    float e = std::exp(float(-dd * dd) / two_sigma_squared);
+    float num = -std::log(p.gamma + e) + std::log(p.gamma);
+    return int32_t(double(num) / double(p.beta));
+}
+
+DevParams dev_params(const elas_params& p) {
+    DevParams d{};
+    d.support_threshold = p.support_threshold;
+    d.support_texture = p.support_texture;
+    d.lr_threshold = p.lr_threshold;
+    d.incon_window = p.incon_window_size;
+    d.incon_threshold = p.incon_threshold;
+    d.incon_min_support = p.incon_min_support;
+    d.match_texture = p.match_texture;
+    d.plane_radius = int32_t(std::max(float(std::ceil(p.sigma * p.sradius)), 2.0f));
+    for (int i = 0; i < 16; ++i) d.penalty[i] = i <= d.plane_radius ? penalty(i, p) : 0;
+    d.speckle_sim_threshold = p.speckle_sim_threshold;
+    d.speckle_size = p.speckle_size;
+    d.ipol_gap_width = p.ipol_gap_width;
+    return d;
+}
+
+Geom geom_of(int W, int H, const elas_params& p) {
+    Geom g;
+    g.W = W; g.H = H;
+    g.step = p.candidate_stepsize;
+    g.gs = p.grid_size;
+    g.cw = W / g.step;
+    g.ch = H / g.step;
+    g.gw = int(std::ceil(float(W) / float(g.gs)));
+    g.gh = int(std::ceil(float(H) / float(g.gs)));
+    g.D = p.disp_max;
+    g.dmin = std::max(p.disp_min, 0);
+    g.words = (g.D + 1 + 31) / 32;
+    return g;
+}
+
+// Lay out (and, if `base` is non-null, assign) every workspace buffer.
+size_t layout(elas_handle* h, const Geom& g, char* base) {
+    size_t off = 0;
+    auto take = [&](size_t bytes) -> char* {
+        char* p = base ? base + off : nullptr;
+        off += align_up(bytes);
+        return p;
+    };
+    const size_t px = size_t(g.W) * g.H;
+    const size_t nmax = size_t(std::max(g.cw, 1)) * std::max(g.ch, 1);
+    const size_t rows = size_t(std::max(g.ch, 1));
+    const size_t tmax = 2 * nmax + 16;
+    const size_t hmax = next_pow2(6 * tmax);
+    const size_t cells = size_t(g.gw) * g.gh * g.words;
+    h->img0 = (uint8_t*)take(px);
+    h->img1 = (uint8_t*)take(px);
+    h->desc0 = (uint4*)take(px * 16);
+    h->desc1 = (uint4*)take(px * 16);
+    h->can_lr = (int32_t*)take(nmax * 4);
+    h->can = (int32_t*)take(nmax * 4);
+    h->row_cnt = (int32_t*)take(rows * 4);
+    h->row_off = (int32_t*)take((rows + 1) * 4);
+    h->uvd = (int32_t*)take(3 * nmax * 4);
+    h->x0 = (int32_t*)take(nmax * 4);
+    h->x1 = (int32_t*)take(nmax * 4);
+    h->y = (int32_t*)take(nmax * 4);
+    h->gtmp0 = (uint32_t*)take(cells * 4);
+    h->gtmp1 = (uint32_t*)take(cells * 4);
+    h->grid0 = (uint32_t*)take(cells * 4);
+    h->grid1 = (uint32_t*)take(cells * 4);
+    for (int k = 0; k < 2; ++k) {
+        DelDev& D = h->del[k];
+        D.srt = (int32_t*)take(nmax * 4);
+        D.rcnt = (int32_t*)take(rows * 4);
+        D.ne = (int32_t*)take(rows * 4);
+        D.soff = (int32_t*)take(rows * 4);
+        D.chain = (int32_t*)take(rows * 4);
+        D.stack = (int32_t*)take(rows * 4);
+        D.tri = (int32_t*)take(3 * tmax * 4);
+        D.opp = (int32_t*)take(3 * tmax * 4);
+        D.lock = (uint32_t*)take(tmax * 4);
+        D.fwd = (int32_t*)take(3 * tmax * 4);
+        D.cand = (int32_t*)take(2 * tmax * 4);
+        D.ctr = (int32_t*)take(8 * 4);
+        D.hkey = (unsigned long long*)take(hmax * 8);
+        D.hcnt = (int32_t*)take(hmax * 4);
+        D.hval = (int32_t*)take(2 * hmax * 4);
+        D.hslot = (int32_t*)take(3 * tmax * 4);
+        D.Tmax = int(tmax);
+        D.Hmax = uint32_t(hmax);
+    }
+    h->prior0 = (unsigned long long*)take(px * 8);
+    h->prior1 = (unsigned long long*)take(px * 8);
+    h->raw0 = (float*)take(px * 4);
+    h->raw1 = (float*)take(px * 4);
+    h->lr0 = (float*)take(px * 4);
+    h->lr1 = (float*)take(px * 4);
+    h->tmp = (float*)take(px * 4);
+    h->out0 = (float*)take(px * 4);
+    h->out1 = (float*)take(px * 4);
+    h->lab = (int32_t*)take(px * 4);
+    h->usize = (int32_t*)take(px * 4);
+    h->err = (unsigned*)take(64);
+    return off;
+}
+
+int ensure_workspace(elas_handle* h, const Geom& g) {
+    size_t need = layout(h, g, nullptr);
+    if (need > h->arena_bytes) {
+        if (h->arena) {
+            CK(cudaDeviceSynchronize());
+            CK(cudaFree(h->arena));
+            h->arena = nullptr;
+            h->arena_bytes = 0;
+        }
+        cudaError_t e = cudaMalloc(&h->arena, need);
+        if (e != cudaSuccess) {
+            h->arena = nullptr;
+            return fail(h, ELAS_ERR_OOM, std::string("workspace allocation of ") + std::to_string(need) +
+                                             " bytes failed: " + cudaGetErrorString(e));
+        }
+        h->arena_bytes = need;
+        CK(cudaMemset(h->arena, 0, need));
+    }
+    layout(h, g, (char*)h->arena);
+    for (int k = 0; k < 2; ++k) {
+        h->del[k].x = k == 0 ? h->x0 : h->x1;
+        h->del[k].y = h->y;
+    }
+    return ELAS_OK;
+}
+
+int check_dims(elas_handle* h, const int32_t* dims, int& W, int& H) {
+    if (!dims) return fail(h, ELAS_ERR_INVALID_ARG, "dims is null");
+    W = dims[0];
+    H = dims[1];
+    if (W < 16 || H < 16) return fail(h, ELAS_ERR_INVALID_ARG, "images must be at least 16x16");
+    if (W > 14000 || H > 16384) return fail(h, ELAS_ERR_UNSUPPORTED, "images wider than 14000 or taller than 16384");
+    if (W / h->params.candidate_stepsize > 2048)
+        return fail(h, ELAS_ERR_UNSUPPORTED, "more than 2048 candidates per lattice row");
+    return ELAS_OK;
+}
+
+// The whole pipeline on device buffers (inputs img0/img1 already on the device).
+int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float* out0, float* out1, int W, int H,
+                 cudaStream_t st) {
+    const elas_params& p = h->params;
+    Geom g = geom_of(W, H, p);
+    DevParams dp = dev_params(p);
+    int rc = ensure_workspace(h, g);
+    if (rc != ELAS_OK) return rc;
+    h->g = g;
+    int n = 0;
+    CK(cudaMemsetAsync(h->err, 0, sizeof(unsigned), st));
+    CK(launch_descriptor(img0, img1, h->desc0, h->desc1, W, H, st));
+    n += 1;
+    CK(launch_support(h->desc0, h->desc1, h->can_lr, nullptr, h->can, g, dp, h->num_sms, st));
+    n += 4;
+    CK(launch_compact(h->can, h->row_cnt, h->row_off, h->uvd, h->x0, h->x1, h->y, g, st));
+    n += 3;
+    CK(launch_grid(h->can, h->gtmp0, h->gtmp1, h->grid0, h->grid1, g, st));
+    n += 2;
+    CK(launch_delaunay(h->del[0], h->del[1], h->row_off, g.ch, h->num_sms, h->flip_blocks, h->err, st, &n));
+    CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
+                    h->prior0, h->prior1, g, h->num_sms, st));
+    n += 1;
+    CK(launch_dense(h->desc0, h->desc1, h->prior0, h->prior1, h->grid0, h->grid1, h->raw0, h->raw1, g, dp, st));
+    n += 1;
+    CK(launch_lr(h->raw0, h->raw1, h->lr0, h->lr1, g, p.lr_threshold, st));
+    n += 1;
+    CK(cudaMemcpyAsync(out0, h->lr0, size_t(W) * H * 4, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(out1, h->lr1, size_t(W) * H * 4, cudaMemcpyDeviceToDevice, st));
+    CK(launch_post(out0, h->tmp, h->lab, h->usize, g, dp, p.filter_median, p.filter_adaptive_mean, h->err, st, &n));
+    if (!p.postprocess_only_left)
+        CK(launch_post(out1, h->tmp, h->lab, h->usize, g, dp, p.filter_median, p.filter_adaptive_mean, h->err, st, &n));
+    h->launches += n;
+    h->have_last = true;
+    return ELAS_OK;
+}
+
+int check_device_errors(elas_handle* h, cudaStream_t st) {
+    unsigned e = 0;
+    CK(cudaMemcpyAsync(&e, h->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (e & ERRF_FLIP_LIMIT) return fail(h, ELAS_ERR_TIMEOUT, "edge flipping hit its round limit");
+    if (e) return fail(h, ELAS_ERR_INTERNAL, "device consistency check failed, flags " + std::to_string(e));
+    return ELAS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void elas_params_default(elas_params* p) {
+    if (!p) return;
+    // src/Elas.h:42-66
+    p->disp_min = 0;
+    p->disp_max = 255;
+    p->support_threshold = 0.95f;
+    p->support_texture = 10;
+    p->candidate_stepsize = 5;
+    p->incon_window_size = 5;
+    p->incon_threshold = 5;
+    p->incon_min_support = 5;
+    p->add_corners = true;
+    p->grid_size = 20;
+    p->beta = 0.02f;
+    p->gamma = 5;
+    p->sigma = 1;
+    p->sradius = 3;
+    p->match_texture = 0;
+    p->lr_threshold = 2;
+    p->speckle_sim_threshold = 1;
+    p->speckle_size = 200;
+    p->ipol_gap_width = 5000;
+    p->filter_median = true;
+    p->filter_adaptive_mean = false;
+    p->postprocess_only_left = false;
+    p->subsampling = false;
+}
+
+void elas_params_reference(elas_params* p) {
+    if (!p) return;
+    elas_params_default(p);
+    // src/Kernels/KernelsCommon.h:8-27
+    p->disp_min = 0;
+    p->disp_max = 255;
+    p->support_threshold = 0.85f;
+    p->support_texture = 10;
+    p->candidate_stepsize = 5;
+    p->incon_window_size = 5;
+    p->incon_threshold = 5;
+    p->incon_min_support = 5;
+    p->add_corners = false;
+    p->grid_size = 20;
+    p->beta = 0.02f;
+    p->gamma = 3;
+    p->sigma = 1;
+    p->sradius = 2;
+    p->match_texture = 0;
+    p->lr_threshold = 2;
+    p->speckle_sim_threshold = 1;
+    // the reference runs no post-filter (src/Elas.cu:107-119)
+    p->speckle_size = 0;
+    p->ipol_gap_width = 0;
+    p->filter_median = false;
+    p->filter_adaptive_mean = false;
+    p->postprocess_only_left = false;
+    p->subsampling = false;
+}
+
+const char* elas_b200_status_string(int s) {
+    switch (s) {
+    case ELAS_OK: return "ok";
+    case ELAS_ERR_INVALID_ARG: return "invalid argument";
+    case ELAS_ERR_UNSUPPORTED: return "unsupported";
+    case ELAS_ERR_CUDA: return "CUDA error";
+    case ELAS_ERR_OOM: return "out of memory";
+    case ELAS_ERR_INTERNAL: return "internal consistency check failed";
+    case ELAS_ERR_NO_DEVICE: return "no usable sm_100 device";
+    case ELAS_ERR_TIMEOUT: return "bounded device loop hit its limit";
+    default: return "unknown status";
+    }
+}
+
+int elas_b200_create(const elas_params* params, int device, elas_handle** out) {
+    if (!out) return ELAS_ERR_INVALID_ARG;
+    *out = nullptr;
+    elas_params p;
+    if (params) p = *params;
+    else elas_params_default(&p);
+    std::string why;
+    int rc = check_params(p, why);
+    if (rc != ELAS_OK) return rc;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return ELAS_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return ELAS_ERR_NO_DEVICE;
+    if (prop.major != 10 || prop.minor != 0) return ELAS_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return ELAS_ERR_NO_DEVICE;
+    elas_handle* h = new elas_handle();
+    h->params = p;
+    h->device = device;
+    h->num_sms = prop.multiProcessorCount;
+    h->flip_blocks = flip_blocks_for(h->num_sms);
+    *out = h;
+    return ELAS_OK;
+}
+
+int elas_b200_destroy(elas_handle* h) {
+    if (!h) return ELAS_ERR_INVALID_ARG;
+    if (h->arena) {
+        cudaSetDevice(h->device);
+        cudaDeviceSynchronize();
+        cudaFree(h->arena);
+    }
+    delete h;
+    return ELAS_OK;
+}
+
+int elas_b200_set_params(elas_handle* h, const elas_params* params) {
+    if (!h || !params) return ELAS_ERR_INVALID_ARG;
+    std::string why;
+    int rc = check_params(*params, why);
+    if (rc != ELAS_OK) return fail(h, rc, why);
+    h->params = *params;
+    return ELAS_OK;
+}
+
+int elas_b200_get_params(const elas_handle* h, elas_params* out) {
+    if (!h || !out) return ELAS_ERR_INVALID_ARG;
+    *out = h->params;
+    return ELAS_OK;
+}
+
+const char* elas_b200_last_error(const elas_handle* h) { return h ? h->last_error.c_str() : ""; }
+
+int64_t elas_b200_launch_count(const elas_handle* h) { return h ? h->launches : 0; }
+
+int elas_b200_process_device(elas_handle* h, const uint8_t* d_left, const uint8_t* d_right, float* d_disp_left,
+                             float* d_disp_right, const int32_t* dims, void* stream) {
+    if (!h) return ELAS_ERR_INVALID_ARG;
+    if (!d_left || !d_right || !d_disp_left || !d_disp_right) return fail(h, ELAS_ERR_INVALID_ARG, "null buffer");
+    int W, H;
+    int rc = check_dims(h, dims, W, H);
+    if (rc != ELAS_OK) return rc;
+    CK(cudaSetDevice(h->device));
+    return run_pipeline(h, d_left, d_right, d_disp_left, d_disp_right, W, H, (cudaStream_t)stream);
+}
+
+int elas_b200_process(elas_handle* h, const uint8_t* left, const uint8_t* right, float* disp_left,
+                      float* disp_right, const int32_t* dims, void* stream) {
+    if (!h) return ELAS_ERR_INVALID_ARG;
+    if (!left || !right || !disp_left || !disp_right) return fail(h, ELAS_ERR_INVALID_ARG, "null buffer");
+    int W, H;
+    int rc = check_dims(h, dims, W, H);
+    if (rc != ELAS_OK) return rc;
+    CK(cudaSetDevice(h->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    rc = ensure_workspace(h, geom_of(W, H, h->params));
+    if (rc != ELAS_OK) return rc;
+    const size_t px = size_t(W) * H;
+    CK(cudaMemcpyAsync(h->img0, left, px, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(h->img1, right, px, cudaMemcpyHostToDevice, st));
+    rc = run_pipeline(h, h->img0, h->img1, h->out0, h->out1, W, H, st);
+    if (rc != ELAS_OK) return rc;
+    CK(cudaMemcpyAsync(disp_left, h->out0, px * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(disp_right, h->out1, px * 4, cudaMemcpyDeviceToHost, st));
+    return check_device_errors(h, st);
+}
+
+int elas_b200_process_batch(elas_handle* h, int n, const uint8_t* const* lefts, const uint8_t* const* rights,
+                            float* const* disp_lefts, float* const* disp_rights, const int32_t* dims,
+                            const int32_t* disp_max_per_pair, void* stream) {
+    if (!h || n < 0 || (n > 0 && (!lefts || !rights || !disp_lefts || !disp_rights || !dims)))
+        return ELAS_ERR_INVALID_ARG;
+    elas_params saved = h->params;
+    int rc = ELAS_OK;
+    for (int i = 0; i < n && rc == ELAS_OK; ++i) {
+        if (disp_max_per_pair) {
+            elas_params q = saved;
+            q.disp_max = disp_max_per_pair[i];
+            rc = elas_b200_set_params(h, &q);
+            if (rc != ELAS_OK) break;
+        }
+        rc = elas_b200_process(h, lefts[i], rights[i], disp_lefts[i], disp_rights[i], dims + 2 * i, stream);
+    }
+    h->params = saved;
+    return rc;
+}
+
+int elas_b200_get_stage(elas_handle* h, int stage, void* dst, size_t bytes, size_t* needed) {
+    if (!h) return ELAS_ERR_INVALID_ARG;
+    if (!h->have_last) return fail(h, ELAS_ERR_INVALID_ARG, "no previous call");
+    if (stage < 0 || stage >= ELAS_STAGE_COUNT) return fail(h, ELAS_ERR_INVALID_ARG, "bad stage");
+    CK(cudaSetDevice(h->device));
+    CK(cudaDeviceSynchronize());
+    const Geom& g = h->g;
+    const size_t px = size_t(g.W) * g.H;
+    const size_t can_n = size_t(g.cw) * g.ch;
+    const size_t cells = size_t(g.gw) * g.gh;
+    size_t need = 0;
+    int32_t nsup = 0, ntri = 0;
+    switch (stage) {
+    case ELAS_STAGE_DESC_LEFT: case ELAS_STAGE_DESC_RIGHT: need = px * 16; break;
+    case ELAS_STAGE_CAN_LR: case ELAS_STAGE_CAN: need = can_n * 4; break;
+    case ELAS_STAGE_SUPPORT:
+        CK(cudaMemcpy(&nsup, h->row_off + g.ch, 4, cudaMemcpyDeviceToHost));
+        need = size_t(nsup) * 12;
+        break;
+    case ELAS_STAGE_GRID_LEFT: case ELAS_STAGE_GRID_RIGHT: need = cells * (g.D + 2) * 4; break;
+    case ELAS_STAGE_TRI_LEFT: case ELAS_STAGE_TRI_RIGHT:
+        CK(cudaMemcpy(&ntri, h->del[stage - ELAS_STAGE_TRI_LEFT].ctr, 4, cudaMemcpyDeviceToHost));
+        need = size_t(ntri) * 12;
+        break;
+    case ELAS_STAGE_PRIOR_LEFT: case ELAS_STAGE_PRIOR_RIGHT: need = px * 4; break;
+    default: need = px * 4; break;
+    }
+    if (needed) *needed = need;
+    if (!dst) return ELAS_OK;
+    if (bytes < need) return fail(h, ELAS_ERR_INVALID_ARG, "destination too small");
+    switch (stage) {
+    case ELAS_STAGE_DESC_LEFT: CK(cudaMemcpy(dst, h->desc0, need, cudaMemcpyDeviceToHost)); break;
+    case ELAS_STAGE_DESC_RIGHT: CK(cudaMemcpy(dst, h->desc1, need, cudaMemcpyDeviceToHost)); break;
+    case ELAS_STAGE_CAN_LR: CK(cudaMemcpy(dst, h->can_lr, need, cudaMemcpyDeviceToHost)); break;
+    case ELAS_STAGE_CAN: CK(cudaMemcpy(dst, h->can, need, cudaMemcpyDeviceToHost)); break;
+    case ELAS_STAGE_SUPPORT: CK(cudaMemcpy(dst, h->uvd, need, cudaMemcpyDeviceToHost)); break;
+    case ELAS_STAGE_GRID_LEFT: case ELAS_STAGE_GRID_RIGHT: {
+        std::vector<uint32_t> bits(cells * g.words);
+        CK(cudaMemcpy(bits.data(), stage == ELAS_STAGE_GRID_LEFT ? h->grid0 : h->grid1, bits.size() * 4,
+                      cudaMemcpyDeviceToHost));
+        int32_t* o = (int32_t*)dst;
+        std::memset(o, 0, need);
+        for (size_t c = 0; c < cells; ++c) {
+            int32_t* cell = o + c * (g.D + 2);
+            int k = 1;
+            for (int d = 0; d <= g.D; ++d)
+                if (bits[c * g.words + d / 32] >> (d % 32) & 1u) cell[k++] = d;
+            cell[0] = k - 1;
+        }
+        break;
+    }
+    case ELAS_STAGE_TRI_LEFT: CK(cudaMemcpy(dst, h->del[0].tri, need, cudaMemcpyDeviceToHost)); break;
+    case ELAS_STAGE_TRI_RIGHT: CK(cudaMemcpy(dst, h->del[1].tri, need, cudaMemcpyDeviceToHost)); break;
+    case ELAS_STAGE_PRIOR_LEFT: case ELAS_STAGE_PRIOR_RIGHT: {
+        std::vector<unsigned long long> pk(px);
+        CK(cudaMemcpy(pk.data(), stage == ELAS_STAGE_PRIOR_LEFT ? h->prior0 : h->prior1, px * 8,
+                      cudaMemcpyDeviceToHost));
+        int32_t* o = (int32_t*)dst;
+        for (size_t i = 0; i < px; ++i) o[i] = (pk[i] >> 32) ? int32_t(uint32_t(pk[i])) : -1;
+        break;
+    }
+    case ELAS_STAGE_DISP_LEFT: CK(cudaMemcpy(dst, h->raw0, need, cudaMemcpyDeviceToHost)); break;
+    case ELAS_STAGE_DISP_RIGHT: CK(cudaMemcpy(dst, h->raw1, need, cudaMemcpyDeviceToHost)); break;
+    case ELAS_STAGE_LR_LEFT: CK(cudaMemcpy(dst, h->lr0, need, cudaMemcpyDeviceToHost)); break;
+    case ELAS_STAGE_LR_RIGHT: CK(cudaMemcpy(dst, h->lr1, need, cudaMemcpyDeviceToHost)); break;
+    default: return fail(h, ELAS_ERR_INVALID_ARG, "bad stage");
+    }
+    return ELAS_OK;
+}
+
+}  // extern "C"

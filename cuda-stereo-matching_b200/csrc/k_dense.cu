@@ -1,0 +1,277 @@
+// Plane prior, dense matching and the left/right check.
+//
+// Prior: replaces kerComputeDepthApproximation
+// (src/Kernels/KerComputeDisparity.cu:9-152), one thread per triangle with
+// long serial scanline loops.  Here a warp takes a triangle: every lane
+// solves the plane (same double Gauss-Jordan as kerSolve, :321-375) and the
+// lanes split the triangle's columns.  A pixel covered by more than one
+// triangle (rounding at shared vertices) must keep the last triangle in
+// list order, as a sequential rasteriser would; the prior is therefore
+// written with a 64-bit atomicMax of (triangle+1) << 32 | d_plane, which
+// makes the result independent of scheduling.
+//
+// Floating point follows the reference expressions with the contraction
+// nvcc applies to them made explicit (fma where a*b+c occurs); the CPU
+// oracle evaluates the identical operation sequence.
+//
+// Dense: replaces kerComputeDisparity (KerComputeDisparity.cu:155-316).
+// One CTA per image row and view; the other view's descriptor row is
+// staged in shared memory; the candidate list of the pixel's grid cell is a
+// bitset walked in ascending order (the reference's sorted int list),
+// skipping the plane window, then the plane window with the penalty added.
+// Strict '<' keeps the first minimum in that order, as the reference does.
+#include <cuda_runtime.h>
+#include "common.cuh"
+#include "kernels.h"
+
+namespace elas {
+
+namespace {
+
+__device__ __forceinline__ int sad16(const uint4& a, const uint4& b) {
+    return int(__vsadu4(a.x, b.x) + __vsadu4(a.y, b.y) + __vsadu4(a.z, b.z) + __vsadu4(a.w, b.w));
+}
+__device__ __forceinline__ int texture16(const uint4& a) {
+    const unsigned k = 0x80808080u;
+    return int(__vsadu4(a.x, k) + __vsadu4(a.y, k) + __vsadu4(a.z, k) + __vsadu4(a.w, k));
+}
+
+// kerSolve with the row update written as fma(-y, dum, x).
+__device__ bool solve3(double A[3][3], double B[3]) {
+    const double eps = 1e-20;
+    int ipiv[3] = {0, 0, 0};
+    int irow = 0, icol = 0;
+#pragma unroll 1
+    for (int i = 0; i < 3; ++i) {
+        double big = 0.0;
+        for (int j = 0; j < 3; ++j)
+            if (ipiv[j] != 1)
+                for (int k = 0; k < 3; ++k)
+                    if (ipiv[k] == 0)
+                        if (fabs(A[j][k]) >= big) { big = fabs(A[j][k]); irow = j; icol = k; }
+        ++ipiv[icol];
+        if (irow != icol) {
+            for (int l = 0; l < 3; ++l) { double t = A[irow][l]; A[irow][l] = A[icol][l]; A[icol][l] = t; }
+            double t = B[irow]; B[irow] = B[icol]; B[icol] = t;
+        }
+        if (fabs(A[icol][icol]) < eps) return false;
+        double pivinv = __ddiv_rn(1.0, A[icol][icol]);
+        A[icol][icol] = 1.0;
+        for (int l = 0; l < 3; ++l) A[icol][l] = __dmul_rn(A[icol][l], pivinv);
+        B[icol] = __dmul_rn(B[icol], pivinv);
+        for (int ll = 0; ll < 3; ++ll)
+            if (ll != icol) {
+                double dum = A[ll][icol];
+                A[ll][icol] = 0.0;
+                for (int l = 0; l < 3; ++l) A[ll][l] = __fma_rn(-A[icol][l], dum, A[ll][l]);
+                B[ll] = __fma_rn(-B[icol], dum, B[ll]);
+            }
+    }
+    return true;
+}
+
+struct Raster {
+    float pa, pb, pc;
+    float A_u, B_u, C_u;
+    float AB_a, AC_a, BC_a, AB_b, AC_b, BC_b;
+};
+
+__device__ void setup_triangle(const int32_t* tri, const int32_t* can, const int32_t* uvd, int cw, int step,
+                               bool right, Raster& R) {
+    int tu[3], tv[3], td[3];
+    for (int k = 0; k < 3; ++k) {
+        int c = tri[k];
+        tu[k] = uvd[3 * c];
+        tv[k] = uvd[3 * c + 1];
+        td[k] = can[(tv[k] * cw + tu[k]) / step];
+    }
+    double A[3][3], B[3];
+    for (int k = 0; k < 3; ++k) {
+        A[k][0] = right ? double(tu[k] - td[k]) : double(tu[k]);
+        A[k][1] = double(tv[k]);
+        A[k][2] = 1.0;
+        B[k] = double(td[k]);
+    }
+    R.pa = R.pb = R.pc = 0.0f;
+    if (solve3(A, B)) {
+        R.pa = __double2float_rn(B[0]);
+        R.pb = __double2float_rn(B[1]);
+        R.pc = __double2float_rn(B[2]);
+    }
+    if (right)
+        for (int k = 0; k < 3; ++k) tu[k] -= td[k];
+    for (int j = 0; j < 3; ++j)
+        for (int k = 0; k < j; ++k)
+            if (tu[k] > tu[j]) {
+                int t = tu[j]; tu[j] = tu[k]; tu[k] = t;
+                t = tv[j]; tv[j] = tv[k]; tv[k] = t;
+            }
+    float A_u = float(tu[0]), A_v = float(tv[0]);
+    float B_u = float(tu[1]), B_v = float(tv[1]);
+    float C_u = float(tu[2]), C_v = float(tv[2]);
+    R.A_u = A_u; R.B_u = B_u; R.C_u = C_u;
+    R.AB_a = 0.0f; R.AC_a = 0.0f; R.BC_a = 0.0f;
+    if (int(A_u) != int(B_u)) R.AB_a = __fdiv_rn(__fsub_rn(A_v, B_v), __fsub_rn(A_u, B_u));
+    if (int(A_u) != int(C_u)) R.AC_a = __fdiv_rn(__fsub_rn(A_v, C_v), __fsub_rn(A_u, C_u));
+    if (int(B_u) != int(C_u)) R.BC_a = __fdiv_rn(__fsub_rn(B_v, C_v), __fsub_rn(B_u, C_u));
+    R.AB_b = __fmaf_rn(-R.AB_a, A_u, A_v);
+    R.AC_b = __fmaf_rn(-R.AC_a, A_u, A_v);
+    R.BC_b = __fmaf_rn(-R.BC_a, B_u, B_v);
+}
+
+__device__ __forceinline__ void raster_part(const Raster& R, int u0, int u1, float ea, float eb, int W, int H,
+                                            unsigned long long tag, unsigned long long* prior, int lane) {
+    for (int u = imax(u0, 0) + lane; u < imin(u1, W); u += 32) {
+        float fu = float(u);
+        int v1 = int(__float2uint_rz(__fmaf_rn(R.AC_a, fu, R.AC_b)));
+        int v2 = int(__float2uint_rz(__fmaf_rn(ea, fu, eb)));
+        int va = imin(v1, v2), vb = imax(v1, v2);
+        float au = __fmul_rn(R.pa, fu);
+        (void)au;
+        for (int v = va; v < vb; ++v) {
+            if (v < 0 || v >= H) continue;
+            float dp = __fadd_rn(__fmaf_rn(R.pa, fu, __fmul_rn(R.pb, float(v))), R.pc);
+            int d = __float2int_rz(dp);
+            atomicMax(&prior[size_t(v) * W + u], tag | (unsigned long long)uint32_t(d));
+        }
+    }
+}
+
+// One warp per (view, triangle).
+__global__ void __launch_bounds__(256) k_prior(const int32_t* __restrict__ tri0, const int32_t* __restrict__ tri1,
+                                               const int32_t* __restrict__ ctr0, const int32_t* __restrict__ ctr1,
+                                               const int32_t* __restrict__ can, const int32_t* __restrict__ uvd,
+                                               unsigned long long* prior0, unsigned long long* prior1, Geom g) {
+    const int lane = threadIdx.x & 31;
+    const int T0 = ctr0[0], T1 = ctr1[0];
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int i = wid; i < T0 + T1; i += nw) {
+        const bool right = i >= T0;
+        const int t = right ? i - T0 : i;
+        const int32_t* tri = (right ? tri1 : tri0) + 3 * size_t(t);
+        Raster R;
+        setup_triangle(tri, can, uvd, g.cw, g.step, right, R);
+        unsigned long long tag = (unsigned long long)(t + 1) << 32;
+        unsigned long long* prior = right ? prior1 : prior0;
+        if (int(R.A_u) != int(R.B_u)) raster_part(R, int(R.A_u), int(R.B_u), R.AB_a, R.AB_b, g.W, g.H, tag, prior, lane);
+        if (int(R.B_u) != int(R.C_u)) raster_part(R, int(R.B_u), int(R.C_u), R.BC_a, R.BC_b, g.W, g.H, tag, prior, lane);
+    }
+}
+
+// blockIdx.x = row, blockIdx.y = view (0 left, 1 right).
+__global__ void __launch_bounds__(512) k_dense(const uint4* __restrict__ desc0, const uint4* __restrict__ desc1,
+                                               const unsigned long long* __restrict__ prior0,
+                                               const unsigned long long* __restrict__ prior1,
+                                               const uint32_t* __restrict__ grid0, const uint32_t* __restrict__ grid1,
+                                               float* __restrict__ disp0, float* __restrict__ disp1, Geom g,
+                                               DevParams p) {
+    extern __shared__ uint4 row[];
+    const int v = blockIdx.x;
+    const bool right = blockIdx.y != 0;
+    const int W = g.W, H = g.H;
+    const uint4* self = (right ? desc1 : desc0) + size_t(v) * W;
+    const uint4* other = (right ? desc0 : desc1) + size_t(v) * W;
+    const unsigned long long* prior = (right ? prior1 : prior0) + size_t(v) * W;
+    const uint32_t* grid = right ? grid1 : grid0;
+    float* disp = (right ? disp1 : disp0) + size_t(v) * W;
+    for (int i = threadIdx.x; i < W; i += blockDim.x) row[i] = other[i];
+    __syncthreads();
+    const int dir = right ? 1 : -1;
+    const int r = p.plane_radius;
+    const bool v_ok = v > 3 && v < H - 3;
+    const int gy = floordiv(v, g.gs);
+    for (int u = threadIdx.x; u < W; u += blockDim.x) {
+        float out = -1.0f;
+        if (v_ok && u > 3 && u < W - 3) {
+            unsigned long long pk = prior[u];
+            int dp = int(uint32_t(pk & 0xffffffffull));
+            if ((pk >> 32) != 0 && dp > 0) {
+                uint4 I1 = self[u];
+                if (texture16(I1) >= p.match_texture) {
+                    int dpmin = imax(dp - r, 0);
+                    long long dpmax_l = (long long)dp + r;
+                    int dpmax = dpmax_l > g.D ? g.D : int(dpmax_l);
+                    const uint32_t* cell = grid + (size_t(gy) * g.gw + floordiv(u, g.gs)) * g.words;
+                    int min_val = 10000, min_d = -1;
+                    for (int w = 0; w < g.words; ++w) {
+                        uint32_t bits = cell[w];
+                        while (bits) {
+                            int d = 32 * w + __ffs(bits) - 1;
+                            bits &= bits - 1;
+                            if (d >= dpmin && d <= dpmax) continue;
+                            int uw = u + dir * d;
+                            if (uw < 3 || uw >= W - 3) continue;
+                            int e = sad16(I1, row[uw]);
+                            if (e < min_val) { min_val = e; min_d = d; }
+                        }
+                    }
+                    for (int d = dpmin; d <= dpmax; ++d) {
+                        int uw = u + dir * d;
+                        if (uw < 3 || uw >= W - 3) continue;
+                        int e = p.penalty[abs(d - dp)] + sad16(I1, row[uw]);
+                        if (e < min_val) { min_val = e; min_d = d; }
+                    }
+                    out = min_d >= 0 ? float(min_d) : -1.0f;
+                }
+            }
+        }
+        disp[u] = out;
+    }
+}
+
+// kerLeftRightConsistencyCheck (src/Kernels/KerLeftRightConsistencyCheck.cu:7-64)
+// reading the dense results and writing separate outputs (the reference's
+// snapshot copies, src/Elas.cu:542-546).
+__global__ void k_lr(const float* __restrict__ D1, const float* __restrict__ D2, float* __restrict__ O1,
+                     float* __restrict__ O2, int W, int H, float thr) {
+    int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (u >= W || v >= H) return;
+    size_t a = size_t(v) * W + u;
+    float d1 = D1[a], d2 = D2[a];
+    float uw1 = float(u) - d1, uw2 = float(u) + d2;
+    float o1 = d1, o2 = d2;
+    if (d1 >= 0 && uw1 >= 0 && uw1 < W) {
+        if (fabsf(D2[size_t(v) * W + int(uw1)] - d1) > thr) o1 = -1;
+    } else {
+        o1 = -1;
+    }
+    if (d2 >= 0 && uw2 >= 0 && uw2 < W) {
+        if (fabsf(D1[size_t(v) * W + int(uw2)] - d2) > thr) o2 = -1;
+    } else {
+        o2 = -1;
+    }
+    O1[a] = o1;
+    O2[a] = o2;
+}
+
+}  // namespace
+
+cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
+                         int Tmax, const int32_t* can, const int32_t* uvd, unsigned long long* prior0,
+                         unsigned long long* prior1, const Geom& g, int num_sms, cudaStream_t st) {
+    size_t n = size_t(g.W) * g.H * sizeof(unsigned long long);
+    cudaMemsetAsync(prior0, 0, n, st);
+    cudaMemsetAsync(prior1, 0, n, st);
+    int blocks = imax(1, imin(16 * num_sms, (2 * Tmax + 7) / 8));
+    k_prior<<<blocks, 256, 0, st>>>(tri0, tri1, ctr0, ctr1, can, uvd, prior0, prior1, g);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const unsigned long long* prior0,
+                         const unsigned long long* prior1, const uint32_t* grid0, const uint32_t* grid1,
+                         float* disp0, float* disp1, const Geom& g, const DevParams& p, cudaStream_t st) {
+    size_t smem = size_t(g.W) * sizeof(uint4);
+    cudaFuncSetAttribute(k_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    int threads = g.W >= 512 ? 512 : ((g.W + 31) / 32) * 32;
+    k_dense<<<dim3(g.H, 2), threads, smem, st>>>(desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lr(const float* d0, const float* d1, float* o0, float* o1, const Geom& g, int lr_threshold,
+                      cudaStream_t st) {
+    k_lr<<<dim3((g.W + 255) / 256, g.H), 256, 0, st>>>(d0, d1, o0, o1, g.W, g.H, float(lr_threshold));
+    return cudaGetLastError();
+}
+
+}  // namespace elas

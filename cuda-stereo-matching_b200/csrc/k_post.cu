@@ -1,0 +1,186 @@
+// Post-filters: speckle removal, gap interpolation, adaptive mean, median.
+//
+// The reference declares these only as parameters (src/Elas.h:31-36,
+// KernelsCommon.h:19-21) and its process() stops after the left/right check
+// (src/Elas.cu:107-119).  The semantics are the project's own and are
+// written out in the CPU oracle (oracle/elas_oracle.cpp, orc_postprocess):
+//   speckle   4-connected segments (|d_p - d_q| <= speckle_sim_threshold);
+//             segments smaller than speckle_size become invalid.  Union-find
+//             with atomic hooking of the larger root under the smaller.
+//   gap       rows, then columns: a run of <= ipol_gap_width invalid pixels
+//             between valid a and b becomes (a+b)/2 if |a-b| <= 3 else
+//             min(a,b).  One thread per line.
+//   mean      5x5 weighted mean of valid pixels, w = 1/(1+(d_q-d_p)^2).
+//   median    lower median of the valid pixels of the 3x3 window.
+#include <cuda_runtime.h>
+#include "common.cuh"
+#include "kernels.h"
+
+namespace elas {
+
+namespace {
+
+constexpr int UF_LIMIT = 1 << 20;   // bound on any union-find walk / retry loop
+
+__device__ __forceinline__ int uf_find(const int32_t* lab, int x, unsigned* err) {
+    for (int it = 0; it < UF_LIMIT; ++it) {
+        int p = lab[x];
+        if (p == x) return x;
+        x = p;
+    }
+    atomicOr(err, ERRF_BOUNDS);
+    return x;
+}
+
+__global__ void k_uf_init(const float* __restrict__ D, int32_t* __restrict__ lab, int32_t* __restrict__ sz, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    lab[i] = D[i] >= 0 ? i : -1;
+    sz[i] = 0;
+}
+
+__device__ void uf_union(int32_t* lab, int a, int b, unsigned* err) {
+    for (int it = 0; it < UF_LIMIT; ++it) {
+        int ra = uf_find(lab, a, err), rb = uf_find(lab, b, err);
+        if (ra == rb) return;
+        if (ra < rb) { int t = ra; ra = rb; rb = t; }
+        int old = atomicCAS(&lab[ra], ra, rb);
+        if (old == ra) return;
+        a = old;
+    }
+    atomicOr(err, ERRF_BOUNDS);
+}
+
+__global__ void k_uf_union(const float* __restrict__ D, int32_t* lab, int W, int H, float thr, unsigned* err) {
+    int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (u >= W || v >= H) return;
+    int i = v * W + u;
+    float d = D[i];
+    if (d < 0) return;
+    if (u + 1 < W) {
+        float q = D[i + 1];
+        if (q >= 0 && fabsf(q - d) <= thr) uf_union(lab, i, i + 1, err);
+    }
+    if (v + 1 < H) {
+        float q = D[i + W];
+        if (q >= 0 && fabsf(q - d) <= thr) uf_union(lab, i, i + W, err);
+    }
+}
+
+__global__ void k_uf_count(int32_t* lab, int32_t* sz, int n, unsigned* err) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || lab[i] < 0) return;
+    int r = uf_find(lab, i, err);
+    atomicAdd(&sz[r], 1);
+}
+
+__global__ void k_uf_apply(float* D, const int32_t* lab, const int32_t* sz, int n, int min_size, unsigned* err) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || lab[i] < 0) return;
+    int r = uf_find(lab, i, err);
+    if (sz[r] < min_size) D[i] = -1.0f;
+}
+
+// horizontal = 1: one thread per row; 0: one thread per column.
+__global__ void k_gap(float* D, int W, int H, int gap, int horizontal) {
+    int l = blockIdx.x * blockDim.x + threadIdx.x;
+    int lines = horizontal ? H : W, len = horizontal ? W : H;
+    if (l >= lines) return;
+    size_t base = horizontal ? size_t(l) * W : size_t(l);
+    size_t stride = horizontal ? 1 : size_t(W);
+    int k = 0;
+    while (k < len) {
+        if (D[base + k * stride] >= 0) { ++k; continue; }
+        int k0 = k;
+        while (k < len && D[base + k * stride] < 0) ++k;
+        if (k0 > 0 && k < len && k - k0 <= gap) {
+            float a = D[base + (k0 - 1) * stride], b = D[base + k * stride];
+            float f = fabsf(a - b) <= 3.0f ? __fmul_rn(0.5f, __fadd_rn(a, b)) : fminf(a, b);
+            for (int q = k0; q < k; ++q) D[base + q * stride] = f;
+        }
+    }
+}
+
+__global__ void k_mean(const float* __restrict__ S, float* __restrict__ D, int W, int H) {
+    int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (u >= W || v >= H) return;
+    float dp = S[size_t(v) * W + u];
+    float out = dp;
+    if (dp >= 0) {
+        float num = 0.0f, den = 0.0f;
+        for (int dy = -2; dy <= 2; ++dy)
+            for (int dx = -2; dx <= 2; ++dx) {
+                int x = u + dx, y = v + dy;
+                if (x < 0 || x >= W || y < 0 || y >= H) continue;
+                float dq = S[size_t(y) * W + x];
+                if (dq < 0) continue;
+                float diff = __fsub_rn(dq, dp);
+                float w = __fdiv_rn(1.0f, __fmaf_rn(diff, diff, 1.0f));
+                num = __fmaf_rn(w, dq, num);
+                den = __fadd_rn(den, w);
+            }
+        out = __fdiv_rn(num, den);
+    }
+    D[size_t(v) * W + u] = out;
+}
+
+__global__ void k_median(const float* __restrict__ S, float* __restrict__ D, int W, int H) {
+    int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (u >= W || v >= H) return;
+    float c = S[size_t(v) * W + u];
+    float out = c;
+    if (c >= 0) {
+        float a[9];
+        int n = 0;
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                int x = u + dx, y = v + dy;
+                if (x < 0 || x >= W || y < 0 || y >= H) continue;
+                float q = S[size_t(y) * W + x];
+                if (q >= 0) a[n++] = q;
+            }
+        for (int i = 1; i < n; ++i) {   // insertion sort, n <= 9
+            float x = a[i];
+            int j = i - 1;
+            while (j >= 0 && a[j] > x) { a[j + 1] = a[j]; --j; }
+            a[j + 1] = x;
+        }
+        out = a[(n - 1) / 2];
+    }
+    D[size_t(v) * W + u] = out;
+}
+
+}  // namespace
+
+cudaError_t launch_post(float* disp, float* tmp, int32_t* lab, int32_t* size, const Geom& g, const DevParams& p,
+                        bool median, bool adaptive_mean, unsigned* err, cudaStream_t st, int* nlaunch) {
+    const int W = g.W, H = g.H, n = W * H;
+    const int tb = 256;
+    int launched = 0;
+    if (p.speckle_size > 0) {
+        k_uf_init<<<(n + tb - 1) / tb, tb, 0, st>>>(disp, lab, size, n);
+        k_uf_union<<<dim3((W + tb - 1) / tb, H), tb, 0, st>>>(disp, lab, W, H, p.speckle_sim_threshold, err);
+        k_uf_count<<<(n + tb - 1) / tb, tb, 0, st>>>(lab, size, n, err);
+        k_uf_apply<<<(n + tb - 1) / tb, tb, 0, st>>>(disp, lab, size, n, p.speckle_size, err);
+        launched += 4;
+    }
+    if (p.ipol_gap_width > 0) {
+        k_gap<<<(H + 127) / 128, 128, 0, st>>>(disp, W, H, p.ipol_gap_width, 1);
+        k_gap<<<(W + 127) / 128, 128, 0, st>>>(disp, W, H, p.ipol_gap_width, 0);
+        launched += 2;
+    }
+    if (adaptive_mean) {
+        k_mean<<<dim3((W + tb - 1) / tb, H), tb, 0, st>>>(disp, tmp, W, H);
+        cudaMemcpyAsync(disp, tmp, size_t(n) * sizeof(float), cudaMemcpyDeviceToDevice, st);
+        launched += 1;
+    }
+    if (median) {
+        k_median<<<dim3((W + tb - 1) / tb, H), tb, 0, st>>>(disp, tmp, W, H);
+        cudaMemcpyAsync(disp, tmp, size_t(n) * sizeof(float), cudaMemcpyDeviceToDevice, st);
+        launched += 1;
+    }
+    if (nlaunch) *nlaunch += launched;
+    return cudaGetLastError();
+}
+
+}  // namespace elas

@@ -1,0 +1,382 @@
+// Support-point matching and the filters on the candidate lattice.
+//
+// Replaces kerComputeSupportMatches (src/Kernels/KerSupportMatches.cu:12-193,
+// launched L->R then R->L from src/Elas.cu:200-225), the inconsistency and
+// redundancy filters (:195-357), the compaction (kerFlag + cub scan +
+// kerCompact, :360-421 and src/Elas.cu:338-394) and the disparity grid
+// (kerLoadGridValues + kerCreateGird, src/Kernels/KerGrid.cu:8-126).
+//
+// Sweep design.  A CTA owns a segment of one candidate row and stages the
+// four descriptor rows every candidate of that row reads (rows v-2 and v+2
+// of both images) in shared memory, so the d-sweep reads shared memory only.
+// A warp sweeps one candidate: lane l takes d = dmin + l + 32k, as the
+// reference's 32-thread block does, and per-lane states are merged with
+// shuffles.  The SAD of a 16-byte descriptor pair is four __vsadu4.
+//
+// Reduction.  The reference keeps (best, second best) per lane with strict
+// '<' and lets lane 0 merge its own registers and then all 32 lanes' pairs
+// from shared memory -- lane 0's pair a second time.  Its outcome is a
+// function of a commutative state (E1 = min energy, key = (lane, d) of the
+// first minimum in merge order, c = number of minima capped at 2,
+// E2 = smallest energy among the other disparities):
+//   second = (c >= 2 or lane(d*) == 0) ? E1 : E2
+//   accept iff c >= 1 and (float)E1 < support_threshold * (float)second
+// which is what the warp computes; the oracle restates the reference's
+// lane-by-lane merge literally and the tests compare the two.
+#include <cuda_runtime.h>
+#include "common.cuh"
+#include "kernels.h"
+
+namespace elas {
+
+namespace {
+
+constexpr int INF_E = 0x7fffffff;
+
+struct Top2 {
+    int e1, key, c, e2;
+};
+
+__device__ __forceinline__ void top2_add(Top2& s, int e, int key) {
+    if (e < s.e1) { s.e2 = s.e1; s.e1 = e; s.key = key; s.c = 1; }
+    else if (e == s.e1) { s.c = s.c >= 1 ? 2 : 1; s.e2 = e; s.key = min(s.key, key); }
+    else if (e < s.e2) { s.e2 = e; }
+}
+
+__device__ __forceinline__ void top2_merge(Top2& a, const Top2& b) {
+    if (b.e1 < a.e1) {
+        a.e2 = min(a.e1, b.e2);
+        a.e1 = b.e1; a.key = b.key; a.c = b.c;
+    } else if (b.e1 == a.e1) {
+        if (a.e1 != INF_E) {
+            a.c = min(a.c + b.c, 2);
+            a.e2 = a.e1;
+            a.key = min(a.key, b.key);
+        }
+    } else {
+        a.e2 = min(a.e2, b.e1);
+    }
+}
+
+__device__ __forceinline__ int sad16(const uint4& a, const uint4& b) {
+    return int(__vsadu4(a.x, b.x) + __vsadu4(a.y, b.y) + __vsadu4(a.z, b.z) + __vsadu4(a.w, b.w));
+}
+
+__device__ __forceinline__ int texture16(const uint4& a) {
+    const unsigned k = 0x80808080u;
+    return int(__vsadu4(a.x, k) + __vsadu4(a.y, k) + __vsadu4(a.z, k) + __vsadu4(a.w, k));
+}
+
+// One candidate sweep by a full warp.  self_m2/self_p2: rows v-2/v+2 of the
+// image the candidate lives in; oth_m2/oth_p2: the same rows of the other
+// image.  dir = -1 (left view: u_warp = u - d) or +1 (right view).
+// Returns the accepted disparity or -1 (lane 0's value is authoritative,
+// all lanes return the same value).
+__device__ __forceinline__ int sweep_candidate(const uint4* self_m2, const uint4* self_p2,
+                                               const uint4* oth_m2, const uint4* oth_p2, int u, int dmin,
+                                               int dmax, int dir, float thr) {
+    const int lane = threadIdx.x & 31;
+    const uint4 c0 = self_m2[u - 2], c1 = self_m2[u + 2], c2 = self_p2[u - 2], c3 = self_p2[u + 2];
+    Top2 s{INF_E, 0x7fffffff, 0, INF_E};
+    for (int d = dmin + lane; d <= dmax; d += 32) {
+        int uw = u + dir * d;
+        int e = sad16(c0, oth_m2[uw - 2]) + sad16(c1, oth_m2[uw + 2]) +
+                sad16(c2, oth_p2[uw - 2]) + sad16(c3, oth_p2[uw + 2]);
+        top2_add(s, e, (((d - dmin) & 31) << 16) | d);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        Top2 t;
+        t.e1 = __shfl_xor_sync(0xffffffffu, s.e1, o);
+        t.key = __shfl_xor_sync(0xffffffffu, s.key, o);
+        t.c = __shfl_xor_sync(0xffffffffu, s.c, o);
+        t.e2 = __shfl_xor_sync(0xffffffffu, s.e2, o);
+        top2_merge(s, t);
+    }
+    if (s.c < 1) return -1;
+    int second = (s.c >= 2 || (s.key >> 16) == 0) ? s.e1 : s.e2;
+    if (float(s.e1) < thr * float(second)) return s.key & 0xffff;
+    return -1;
+}
+
+// Block: 256 threads (8 warps).  grid.x = segments per candidate row,
+// grid.y = candidate rows.  SMEM: stage the four rows when they fit.
+template <bool SMEM>
+__global__ void __launch_bounds__(256) k_support_sweep(const uint4* __restrict__ desc0,
+                                                       const uint4* __restrict__ desc1,
+                                                       int32_t* __restrict__ can_out, Geom g, DevParams p,
+                                                       int seg) {
+    extern __shared__ uint4 rows[];
+    __shared__ int res[256];
+    const int W = g.W, H = g.H;
+    const int vc = blockIdx.y;
+    const int v = vc * g.step;
+    const int c_begin = blockIdx.x * seg, c_end = min(g.cw, c_begin + seg);
+    if (c_begin >= c_end) return;
+    const bool row_ok = v >= 5 && v <= H - 6;
+    const uint4 *L_m2, *L_p2, *R_m2, *R_p2;
+    if (row_ok) {
+        if (SMEM) {
+            const uint4* src[4] = {desc0 + size_t(v - 2) * W, desc0 + size_t(v + 2) * W,
+                                   desc1 + size_t(v - 2) * W, desc1 + size_t(v + 2) * W};
+            for (int r = 0; r < 4; ++r)
+                for (int i = threadIdx.x; i < W; i += blockDim.x) rows[r * W + i] = src[r][i];
+            L_m2 = rows; L_p2 = rows + W; R_m2 = rows + 2 * W; R_p2 = rows + 3 * W;
+        } else {
+            L_m2 = desc0 + size_t(v - 2) * W; L_p2 = desc0 + size_t(v + 2) * W;
+            R_m2 = desc1 + size_t(v - 2) * W; R_p2 = desc1 + size_t(v + 2) * W;
+        }
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    // left view: candidates of the segment
+    for (int ci = c_begin + warp; ci < c_end; ci += nw) {
+        int u = ci * g.step;
+        int r = -1;
+        if (row_ok && u >= 5 && u <= W - 6) {
+            uint4 ctr = desc0[size_t(v) * W + u];
+            if (texture16(ctr) >= p.support_texture) {
+                int dmax = min(g.D, u - 5);
+                if (dmax - g.dmin >= 10)
+                    r = sweep_candidate(L_m2, L_p2, R_m2, R_p2, u, g.dmin, dmax, -1, p.support_threshold);
+            }
+        }
+        if (lane == 0) res[ci - c_begin] = r;
+    }
+    __syncthreads();
+    // right view: re-match accepted candidates from u - d
+    for (int ci = c_begin + warp; ci < c_end; ci += nw) {
+        int dl = res[ci - c_begin];
+        if (dl < 0) continue;
+        int u = ci * g.step - dl;
+        int r = -1;
+        uint4 ctr = desc1[size_t(v) * W + u];
+        if (texture16(ctr) >= p.support_texture) {
+            int dmax = min(g.D, W - u - 5);
+            if (dmax - g.dmin >= 10) {
+                int dr = sweep_candidate(R_m2, R_p2, L_m2, L_p2, u, g.dmin, dmax, +1, p.support_threshold);
+                if (dr >= 0 && abs(dl - dr) <= p.lr_threshold) r = dl;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) res[ci - c_begin] = r;
+    }
+    __syncthreads();
+    for (int ci = c_begin + threadIdx.x; ci < c_end; ci += blockDim.x)
+        can_out[size_t(vc) * g.cw + ci] = res[ci - c_begin];
+}
+
+// removeInconsistentSupportPoints with snapshot semantics: reads can_in,
+// writes can_out.  The reference's bound `y < can_width`
+// (KerSupportMatches.cu:208) is kept: rows y >= cw pass through.
+__global__ void k_incon(const int32_t* __restrict__ cin, int32_t* __restrict__ cout, Geom g, DevParams p) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= g.cw || y >= g.ch) return;
+    int d = cin[size_t(y) * g.cw + x];
+    int out = d;
+    if (d >= 0 && y < g.cw) {
+        const int ws = p.incon_window;
+        int support = 0;
+        for (int y2 = max(0, y - ws); y2 <= min(g.ch - 1, y + ws); ++y2)
+            for (int x2 = max(0, x - ws); x2 <= min(g.cw - 1, x + ws); ++x2) {
+                int d2 = cin[size_t(y2) * g.cw + x2];
+                if (d2 >= 0 && abs(d - d2) <= p.incon_threshold) ++support;
+            }
+        if (support < p.incon_min_support) out = -1;
+    }
+    cout[size_t(y) * g.cw + x] = out;
+}
+
+// Redundancy filter along one line held in shared memory (serial, in place,
+// exactly the reference's per-line order).
+__device__ void redundant_line(int* a, int len) {
+    for (int k = 0; k < len; ++k) {
+        int d = a[k];
+        if (d < 0) continue;
+        bool redundant = true;
+        for (int dir = -1; dir <= 1 && redundant; dir += 2) {
+            bool support = false;
+            int k2 = k;
+            for (int j = 0; j < 5; ++j) {
+                k2 += dir;
+                if (k2 < 0 || k2 >= len) break;
+                int d2 = a[k2];
+                if (d2 >= 0 && abs(d - d2) <= 1) { support = true; break; }
+            }
+            if (!support) redundant = false;
+        }
+        if (redundant) a[k] = -1;
+    }
+}
+
+// One warp per line; horizontal = 1: rows, 0: columns.
+__global__ void k_redundant(int32_t* __restrict__ can, Geom g, int horizontal) {
+    extern __shared__ int lines[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nlines = horizontal ? g.ch : g.cw;
+    const int len = horizontal ? g.cw : g.ch;
+    int l = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (l >= nlines) return;
+    int* a = lines + warp * len;
+    for (int k = lane; k < len; k += 32)
+        a[k] = horizontal ? can[size_t(l) * g.cw + k] : can[size_t(k) * g.cw + l];
+    __syncwarp();
+    if (lane == 0) redundant_line(a, len);
+    __syncwarp();
+    for (int k = lane; k < len; k += 32) {
+        if (horizontal) can[size_t(l) * g.cw + k] = a[k];
+        else can[size_t(k) * g.cw + l] = a[k];
+    }
+}
+
+// Count valid candidates per row.
+__global__ void k_row_count(const int32_t* __restrict__ can, int32_t* __restrict__ row_cnt, Geom g) {
+    __shared__ int s;
+    if (threadIdx.x == 0) s = 0;
+    __syncthreads();
+    int cnt = 0;
+    for (int x = threadIdx.x; x < g.cw; x += blockDim.x) cnt += can[size_t(blockIdx.x) * g.cw + x] >= 0;
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&s, cnt);
+    __syncthreads();
+    if (threadIdx.x == 0) row_cnt[blockIdx.x] = s;
+}
+
+// Exclusive scan of the row counts (single block); row_off[ch] = total.
+__global__ void k_row_scan(const int32_t* __restrict__ row_cnt, int32_t* __restrict__ row_off, int n) {
+    __shared__ int part[1024];
+    const int t = threadIdx.x;
+    const int per = (n + blockDim.x - 1) / blockDim.x;
+    const int b = t * per, e = min(n, b + per);
+    int s = 0;
+    for (int i = b; i < e; ++i) s += row_cnt[i];
+    part[t] = s;
+    __syncthreads();
+    for (int o = 1; o < blockDim.x; o <<= 1) {
+        int x = t >= o ? part[t - o] : 0;
+        __syncthreads();
+        part[t] += x;
+        __syncthreads();
+    }
+    int run = part[t] - s;
+    for (int i = b; i < e; ++i) { row_off[i] = run; run += row_cnt[i]; }
+    if (t == blockDim.x - 1) row_off[n] = part[t];
+}
+
+// Write the support list in raster order: uvd (u, v, d), and the point
+// coordinates of both views (x0 = u, x1 = u - d, y = v).
+__global__ void k_compact(const int32_t* __restrict__ can, const int32_t* __restrict__ row_off,
+                          int32_t* __restrict__ uvd, int32_t* __restrict__ x0, int32_t* __restrict__ x1,
+                          int32_t* __restrict__ y, Geom g) {
+    __shared__ int warp_tot[32];
+    __shared__ int base;
+    const int r = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) base = row_off[r];
+    __syncthreads();
+    for (int x0c = 0; x0c < g.cw; x0c += blockDim.x) {
+        int x = x0c + threadIdx.x;
+        int d = x < g.cw ? can[size_t(r) * g.cw + x] : -1;
+        unsigned m = __ballot_sync(0xffffffffu, d >= 0);
+        if (lane == 0) warp_tot[warp] = __popc(m);
+        __syncthreads();
+        int off = 0, tot = 0;
+        for (int w = 0; w < nw; ++w) { if (w < warp) off += warp_tot[w]; tot += warp_tot[w]; }
+        if (d >= 0) {
+            int i = base + off + __popc(m & ((1u << lane) - 1));
+            int u = x * g.step, vv = r * g.step;
+            uvd[3 * i] = u; uvd[3 * i + 1] = vv; uvd[3 * i + 2] = d;
+            x0[i] = u; x1[i] = u - d; y[i] = vv;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) base += tot;
+        __syncthreads();
+    }
+}
+
+// kerLoadGridValues as bitsets: for every support point set bits d-1..d+1
+// (clamped to [0, D]) in its left cell floor(u/gs) and right cell
+// floor((u-d)/gs) of row floor(v/gs).
+__global__ void k_grid_load(const int32_t* __restrict__ can, uint32_t* __restrict__ t0,
+                            uint32_t* __restrict__ t1, Geom g) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= g.cw || y >= g.ch) return;
+    int dc = can[size_t(y) * g.cw + x];
+    if (dc < 0) return;
+    int u = x * g.step, v = y * g.step;
+    int ug0 = floordiv(u, g.gs), ug1 = floordiv(u - dc, g.gs), vg = floordiv(v, g.gs);
+    if (vg < 0 || vg >= g.gh) return;
+    for (int d = max(dc - 1, 0); d <= min(dc + 1, g.D); ++d) {
+        uint32_t bit = 1u << (d & 31);
+        if (ug0 >= 0 && ug0 < g.gw) atomicOr(&t0[(size_t(vg) * g.gw + ug0) * g.words + (d >> 5)], bit);
+        if (ug1 >= 0 && ug1 < g.gw) atomicOr(&t1[(size_t(vg) * g.gw + ug1) * g.words + (d >> 5)], bit);
+    }
+}
+
+// kerCreateGird: 3x3 OR-diffusion for interior cells; border cells empty.
+// One thread per (cell, word); blockIdx.z selects the view.
+__global__ void k_grid_diffuse(const uint32_t* __restrict__ t0, const uint32_t* __restrict__ t1,
+                               uint32_t* __restrict__ g0, uint32_t* __restrict__ g1, Geom g) {
+    const uint32_t* t = blockIdx.z ? t1 : t0;
+    uint32_t* out = blockIdx.z ? g1 : g0;
+    size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    size_t n = size_t(g.gw) * g.gh * g.words;
+    if (i >= n) return;
+    int w = int(i % g.words);
+    int cell = int(i / g.words);
+    int ug = cell % g.gw, vg = cell / g.gw;
+    uint32_t o = 0;
+    if (ug > 0 && ug < g.gw - 1 && vg > 0 && vg < g.gh - 1)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) o |= t[(size_t(vg + dy) * g.gw + ug + dx) * g.words + w];
+    out[i] = o;
+}
+
+}  // namespace
+
+cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_lr, int32_t* can_tmp,
+                           int32_t* can, const Geom& g, const DevParams& p, int num_sms, cudaStream_t st) {
+    // segments: about 4 CTAs per SM in flight
+    int rows = g.ch;
+    int segs = imax(1, (4 * num_sms + rows - 1) / imax(rows, 1));
+    int seg = imin(256, imax(8, (g.cw + segs - 1) / segs));
+    segs = (g.cw + seg - 1) / seg;
+    size_t smem = size_t(4) * g.W * sizeof(uint4);
+    dim3 grid(segs, rows);
+    if (smem <= 200 * 1024) {
+        cudaFuncSetAttribute(k_support_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        k_support_sweep<true><<<grid, 256, smem, st>>>(desc0, desc1, can_lr, g, p, seg);
+    } else {
+        k_support_sweep<false><<<grid, 256, 0, st>>>(desc0, desc1, can_lr, g, p, seg);
+    }
+    k_incon<<<dim3((g.cw + 127) / 128, g.ch), 128, 0, st>>>(can_lr, can, g, p);
+    {
+        int wpb = 4;
+        size_t sm = size_t(wpb) * g.cw * sizeof(int);
+        k_redundant<<<(g.ch + wpb - 1) / wpb, 32 * wpb, sm, st>>>(can, g, 1);
+        sm = size_t(wpb) * g.ch * sizeof(int);
+        k_redundant<<<(g.cw + wpb - 1) / wpb, 32 * wpb, sm, st>>>(can, g, 0);
+    }
+    (void)can_tmp;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_off, int32_t* uvd, int32_t* x0,
+                           int32_t* x1, int32_t* y, const Geom& g, cudaStream_t st) {
+    k_row_count<<<g.ch, 128, 0, st>>>(can, row_cnt, g);
+    k_row_scan<<<1, 1024, 0, st>>>(row_cnt, row_off, g.ch);
+    k_compact<<<g.ch, 256, 0, st>>>(can, row_off, uvd, x0, x1, y, g);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grid(const int32_t* can, uint32_t* tmp0, uint32_t* tmp1, uint32_t* grid0, uint32_t* grid1,
+                        const Geom& g, cudaStream_t st) {
+    size_t n = size_t(g.gw) * g.gh * g.words;
+    cudaMemsetAsync(tmp0, 0, n * sizeof(uint32_t), st);
+    cudaMemsetAsync(tmp1, 0, n * sizeof(uint32_t), st);
+    k_grid_load<<<dim3((g.cw + 127) / 128, g.ch), 128, 0, st>>>(can, tmp0, tmp1, g);
+    k_grid_diffuse<<<dim3(unsigned((n + 255) / 256), 1, 2), 256, 0, st>>>(tmp0, tmp1, grid0, grid1, g);
+    return cudaGetLastError();
+}
+
+}  // namespace elas

@@ -1,0 +1,68 @@
+// Launchers of the ELAS B200 kernels (internal interface of the library).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "common.cuh"
+
+namespace elas {
+
+// Device view of one triangulation problem (see delaunay_core.h).
+struct DelDev {
+    const int32_t* x;      // [Nmax] point x (u for the left view, u-d for the right)
+    const int32_t* y;      // [Nmax] point y (v)
+    int32_t* srt;          // [Nmax] per-row sorted unique point indices (at row_off offsets)
+    int32_t* rcnt;         // [rows] unique points per row
+    int32_t* ne;           // [rows] non-empty rows
+    int32_t* soff;         // [rows] strip triangle offsets
+    int32_t* chain;        // [rows]
+    int32_t* stack;        // [rows]
+    int32_t* tri;          // [3*Tmax]
+    int32_t* opp;          // [3*Tmax]
+    uint32_t* lock;        // [Tmax]
+    int32_t* fwd;          // [3*Tmax]
+    int32_t* cand;         // [2*Tmax]
+    int32_t* ctr;          // [8]
+    unsigned long long* hkey;  // [Hmax]
+    int32_t* hcnt;         // [Hmax]
+    int32_t* hval;         // [2*Hmax]
+    int32_t* hslot;        // [3*Tmax]
+    int Tmax;
+    uint32_t Hmax;         // power of two
+};
+
+cudaError_t launch_descriptor(const uint8_t* img0, const uint8_t* img1, uint4* desc0, uint4* desc1,
+                              int W, int H, cudaStream_t st);
+
+cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_lr, int32_t* can_tmp,
+                           int32_t* can, const Geom& g, const DevParams& p, int num_sms, cudaStream_t st);
+
+cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_off, int32_t* uvd, int32_t* x0,
+                           int32_t* x1, int32_t* y, const Geom& g, cudaStream_t st);
+
+cudaError_t launch_grid(const int32_t* can, uint32_t* tmp0, uint32_t* tmp1, uint32_t* grid0, uint32_t* grid1,
+                        const Geom& g, cudaStream_t st);
+
+cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int num_sms,
+                            int flip_blocks, unsigned* err, cudaStream_t st, int* nlaunch);
+int flip_blocks_for(int num_sms);
+
+// Plane prior of both views: prior[v*W+u] = (triangle+1) << 32 | uint32(d_plane),
+// 0 where no triangle covers the pixel.  Buffers must be zeroed first.
+cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
+                         int Tmax, const int32_t* can, const int32_t* uvd, unsigned long long* prior0,
+                         unsigned long long* prior1, const Geom& g, int num_sms, cudaStream_t st);
+
+cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const unsigned long long* prior0,
+                         const unsigned long long* prior1, const uint32_t* grid0, const uint32_t* grid1,
+                         float* disp0, float* disp1, const Geom& g, const DevParams& p, cudaStream_t st);
+
+cudaError_t launch_lr(const float* d0, const float* d1, float* o0, float* o1, const Geom& g, int lr_threshold,
+                      cudaStream_t st);
+
+// Post-filters on one disparity image in place (tmp: W*H floats, lab/size:
+// W*H int32 each).  Returns the number of kernels launched via *nlaunch.
+cudaError_t launch_post(float* disp, float* tmp, int32_t* lab, int32_t* size, const Geom& g, const DevParams& p,
+                        bool median, bool adaptive_mean, unsigned* err, cudaStream_t st, int* nlaunch);
+
+}  // namespace elas

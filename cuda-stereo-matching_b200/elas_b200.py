@@ -1,0 +1,233 @@
+"""Python binding of the ELAS B200 library (ctypes over include/elas_b200.h).
+
+Mirrors the reference's interface (src/Elas.h): an ``Elas`` object built
+from an ``Elas.parameters``-compatible block whose ``process(left, right)``
+returns the left and right disparity maps (float32, -1 = invalid).  All work
+runs in ``libelas_b200.so``; there is no CPU fallback: if the library or a
+B200 is missing the calls raise.
+"""
+import ctypes
+import os
+from ctypes import POINTER, c_bool, c_float, c_int, c_int32, c_int64, c_size_t, c_uint64, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libelas_b200.so")
+
+ELAS_OK = 0
+STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported", 3: "CUDA error", 4: "out of memory",
+          5: "internal consistency check failed", 6: "no usable sm_100 device", 7: "bounded device loop hit its limit"}
+
+STAGES = {
+    "desc_left": 0, "desc_right": 1, "can_lr": 2, "can": 3, "support": 4, "grid_left": 5, "grid_right": 6,
+    "tri_left": 7, "tri_right": 8, "prior_left": 9, "prior_right": 10, "disp_left": 11, "disp_right": 12,
+    "lr_left": 13, "lr_right": 14,
+}
+
+
+class ElasParams(ctypes.Structure):
+    """Byte-compatible with Elas::parameters (reference src/Elas.h:14-40)."""
+
+    _fields_ = [
+        ("disp_min", c_int32), ("disp_max", c_int32), ("support_threshold", c_float),
+        ("support_texture", c_int32), ("candidate_stepsize", c_int32), ("incon_window_size", c_int32),
+        ("incon_threshold", c_int32), ("incon_min_support", c_int32), ("add_corners", c_bool),
+        ("grid_size", c_int32), ("beta", c_float), ("gamma", c_float), ("sigma", c_float), ("sradius", c_float),
+        ("match_texture", c_int32), ("lr_threshold", c_int32), ("speckle_sim_threshold", c_float),
+        ("speckle_size", c_int32), ("ipol_gap_width", c_int32), ("filter_median", c_bool),
+        ("filter_adaptive_mean", c_bool), ("postprocess_only_left", c_bool), ("subsampling", c_bool),
+    ]
+
+    def copy(self):
+        p = ElasParams()
+        ctypes.pointer(p)[0] = self
+        return p
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class ElasError(RuntimeError):
+    def __init__(self, status, msg=""):
+        super().__init__(f"{STATUS.get(status, status)} ({status}){': ' + msg if msg else ''}")
+        self.status = status
+
+
+_lib = None
+
+
+def library():
+    """Load libelas_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ElasError(1, f"{LIB_PATH} is missing; run __graft_entry__.build()")
+        lib = ctypes.CDLL(LIB_PATH)
+        pp = POINTER(ElasParams)
+        lib.elas_params_default.argtypes = [pp]
+        lib.elas_params_reference.argtypes = [pp]
+        lib.elas_b200_status_string.restype = ctypes.c_char_p
+        lib.elas_b200_status_string.argtypes = [c_int]
+        lib.elas_b200_create.argtypes = [pp, c_int, POINTER(c_void_p)]
+        lib.elas_b200_destroy.argtypes = [c_void_p]
+        lib.elas_b200_set_params.argtypes = [c_void_p, pp]
+        lib.elas_b200_get_params.argtypes = [c_void_p, pp]
+        lib.elas_b200_last_error.restype = ctypes.c_char_p
+        lib.elas_b200_last_error.argtypes = [c_void_p]
+        lib.elas_b200_process.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+        lib.elas_b200_process_device.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                                 c_void_p]
+        lib.elas_b200_process_batch.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                                c_void_p, c_void_p]
+        lib.elas_b200_get_stage.argtypes = [c_void_p, c_int, c_void_p, c_size_t, POINTER(c_size_t)]
+        lib.elas_b200_launch_count.restype = c_int64
+        lib.elas_b200_launch_count.argtypes = [c_void_p]
+        lib.elas_b200_synth_pair.argtypes = [c_int, c_uint64, c_int32, c_int32, c_int32, c_void_p, c_void_p,
+                                             c_void_p, c_void_p]
+        lib.elas_b200_synth_dims.argtypes = [c_int, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]
+        _lib = lib
+    return _lib
+
+
+def params_default():
+    """Elas::parameters() defaults (reference src/Elas.h:42-66)."""
+    p = ElasParams()
+    library().elas_params_default(ctypes.byref(p))
+    return p
+
+
+def params_reference():
+    """The values the reference kernels are compiled with, post-filters off."""
+    p = ElasParams()
+    library().elas_params_reference(ctypes.byref(p))
+    return p
+
+
+def params_config(disp_max, post=True):
+    """Parameters of the benchmark configurations: the reference kernel
+    constants with the configured disparity range; post-filters (speckle 200,
+    gap width 3, median and adaptive mean) on unless ``post`` is False."""
+    p = params_reference()
+    p.disp_max = int(disp_max)
+    if post:
+        p.speckle_size = 200
+        p.ipol_gap_width = 3
+        p.filter_median = True
+        p.filter_adaptive_mean = True
+    return p
+
+
+def _ptr(a):
+    return a.ctypes.data_as(c_void_p)
+
+
+def synth_dims(preset):
+    w, h, d = c_int32(), c_int32(), c_int32()
+    rc = library().elas_b200_synth_dims(preset, ctypes.byref(w), ctypes.byref(h), ctypes.byref(d))
+    if rc:
+        raise ElasError(rc)
+    return w.value, h.value, d.value
+
+
+def synth_pair(preset, seed, width=0, height=0, disp_max=0, gt=True):
+    """Seeded synthetic pair: (left, right, gt_left, gt_right) (gt None if not asked)."""
+    W, H, D = synth_dims(preset)
+    W = width or W
+    H = height or H
+    left = np.empty((H, W), np.uint8)
+    right = np.empty((H, W), np.uint8)
+    gl = np.empty((H, W), np.float32) if gt else None
+    gr = np.empty((H, W), np.float32) if gt else None
+    rc = library().elas_b200_synth_pair(preset, seed, W, H, disp_max, _ptr(left), _ptr(right),
+                                        _ptr(gl) if gt else None, _ptr(gr) if gt else None)
+    if rc:
+        raise ElasError(rc)
+    return left, right, gl, gr
+
+
+class Elas:
+    """Drop-in for the reference's ``Elas`` class (src/Elas.h:11-83)."""
+
+    def __init__(self, params=None, device=0):
+        self._lib = library()
+        self._h = c_void_p()
+        self.params = (params or params_default()).copy()
+        rc = self._lib.elas_b200_create(ctypes.byref(self.params), device, ctypes.byref(self._h))
+        if rc != ELAS_OK:
+            raise ElasError(rc)
+
+    def close(self):
+        if self._h:
+            self._lib.elas_b200_destroy(self._h)
+            self._h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != ELAS_OK:
+            msg = self._lib.elas_b200_last_error(self._h)
+            raise ElasError(rc, msg.decode() if msg else "")
+
+    def set_params(self, params):
+        self._check(self._lib.elas_b200_set_params(self._h, ctypes.byref(params)))
+        self.params = params.copy()
+
+    def process(self, left, right, stream=None):
+        """left, right: uint8 (H, W) arrays.  Returns (D1, D2) float32."""
+        left = np.ascontiguousarray(left, np.uint8)
+        right = np.ascontiguousarray(right, np.uint8)
+        if left.shape != right.shape or left.ndim != 2:
+            raise ElasError(1, "images must be 2-D and of the same size")
+        H, W = left.shape
+        d1 = np.empty((H, W), np.float32)
+        d2 = np.empty((H, W), np.float32)
+        dims = np.array([W, H, W], np.int32)
+        self._check(self._lib.elas_b200_process(self._h, _ptr(left), _ptr(right), _ptr(d1), _ptr(d2), _ptr(dims),
+                                                stream))
+        return d1, d2
+
+    def process_device(self, left_ptr, right_ptr, d1_ptr, d2_ptr, width, height, stream=None):
+        """Device-pointer form (ints); asynchronous on `stream` (a cudaStream_t int)."""
+        dims = np.array([width, height, width], np.int32)
+        self._dims_keepalive = dims
+        self._check(self._lib.elas_b200_process_device(self._h, c_void_p(left_ptr), c_void_p(right_ptr),
+                                                       c_void_p(d1_ptr), c_void_p(d2_ptr), _ptr(dims),
+                                                       c_void_p(stream) if stream else None))
+
+    def process_batch(self, lefts, rights, disp_max=None):
+        n = len(lefts)
+        outs1, outs2 = [], []
+        dims = np.zeros(2 * n, np.int32)
+        keep = []
+        for i, (l, r) in enumerate(zip(lefts, rights)):
+            l = np.ascontiguousarray(l, np.uint8)
+            r = np.ascontiguousarray(r, np.uint8)
+            keep += [l, r]
+            dims[2 * i] = l.shape[1]
+            dims[2 * i + 1] = l.shape[0]
+            outs1.append(np.empty(l.shape, np.float32))
+            outs2.append(np.empty(l.shape, np.float32))
+        arr = lambda xs: (c_void_p * n)(*[x.ctypes.data for x in xs])
+        dm = np.asarray(disp_max, np.int32) if disp_max is not None else None
+        self._check(self._lib.elas_b200_process_batch(self._h, n, arr(keep[0::2]), arr(keep[1::2]), arr(outs1),
+                                                      arr(outs2), _ptr(dims), _ptr(dm) if dm is not None else None,
+                                                      None))
+        return outs1, outs2
+
+    def stage(self, name):
+        """Copy an intermediate stage of the last single-pair call."""
+        sid = STAGES[name]
+        need = c_size_t()
+        self._check(self._lib.elas_b200_get_stage(self._h, sid, None, 0, ctypes.byref(need)))
+        buf = np.empty(need.value, np.uint8)
+        self._check(self._lib.elas_b200_get_stage(self._h, sid, _ptr(buf), need.value, ctypes.byref(need)))
+        return buf
+
+    @property
+    def launch_count(self):
+        return int(self._lib.elas_b200_launch_count(self._h))

@@ -1,0 +1,184 @@
+/*
+ * elas_b200.h -- C ABI of the B200-native ELAS stereo matcher.
+ *
+ * The library replaces the GPU pipeline behind the reference's
+ *   void Elas::process(uint8_t* h_img0, uint8_t* h_img1,
+ *                      float* h_disp0, float* h_disp1, const int32_t* dims)
+ * (reference src/Elas.h:76-83, body src/Elas.cu:19-120).  Every entry point
+ * takes plain pointers and sizes, returns an int status (ELAS_OK == 0) and
+ * never exits the process (the reference calls exit() on any CUDA error,
+ * src/Utils.h:11-38).
+ *
+ * Threading: a handle owns its device workspaces and is used by one host
+ * thread at a time.  Work is enqueued on the stream passed to each call
+ * (NULL = the legacy default stream); host-buffer calls return after the
+ * results are in host memory.
+ */
+#ifndef ELAS_B200_H
+#define ELAS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#ifndef __cplusplus
+#include <stdbool.h>
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ELAS_B200_VERSION 1
+
+/* status codes */
+#define ELAS_OK                 0
+#define ELAS_ERR_INVALID_ARG    1  /* null pointer, bad size, bad parameter */
+#define ELAS_ERR_UNSUPPORTED    2  /* parameter combination not implemented */
+#define ELAS_ERR_CUDA           3  /* a CUDA runtime call failed */
+#define ELAS_ERR_OOM            4  /* device or host allocation failed */
+#define ELAS_ERR_INTERNAL       5  /* a device-side consistency check failed */
+#define ELAS_ERR_NO_DEVICE      6  /* no usable sm_100 device */
+#define ELAS_ERR_TIMEOUT        7  /* a bounded device loop hit its limit */
+
+/*
+ * Parameter block.  Field order, types and meaning are those of
+ * Elas::parameters (reference src/Elas.h:14-40) so the struct is
+ * byte-compatible with it.  Unlike the reference, whose kernels read
+ * compile-time macros (src/Kernels/KernelsCommon.h:8-27), every field that
+ * has a macro counterpart is honoured at run time.
+ */
+typedef struct elas_params {
+    int32_t disp_min;               /* min disparity (support sweep starts at max(disp_min,0)) */
+    int32_t disp_max;               /* max disparity */
+    float   support_threshold;      /* max uniqueness ratio best / second best */
+    int32_t support_texture;        /* min texture for support points */
+    int32_t candidate_stepsize;     /* step of the support candidate lattice */
+    int32_t incon_window_size;      /* half window of the inconsistency filter */
+    int32_t incon_threshold;        /* disparity similarity of the inconsistency filter */
+    int32_t incon_min_support;      /* min number of consistent support points */
+    bool    add_corners;            /* unimplemented in the reference; ignored here as there */
+    int32_t grid_size;              /* cell size of the disparity candidate grid */
+    float   beta;                   /* image likelihood parameter */
+    float   gamma;                  /* prior constant */
+    float   sigma;                  /* prior sigma */
+    float   sradius;                /* prior sigma radius */
+    int32_t match_texture;          /* min texture for dense matching */
+    int32_t lr_threshold;           /* left/right consistency threshold */
+    float   speckle_sim_threshold;  /* similarity threshold for speckle segmentation */
+    int32_t speckle_size;           /* speckles smaller than this are removed (0 = off) */
+    int32_t ipol_gap_width;         /* gaps up to this width are interpolated (0 = off) */
+    bool    filter_median;          /* 3x3 median filter */
+    bool    filter_adaptive_mean;   /* edge-preserving adaptive mean filter */
+    bool    postprocess_only_left;  /* post-filters on D1 only */
+    bool    subsampling;            /* not supported: returns ELAS_ERR_UNSUPPORTED */
+} elas_params;
+
+/* Defaults of the Elas::parameters constructor (reference src/Elas.h:42-66). */
+void elas_params_default(elas_params* p);
+
+/* The values the reference kernels are compiled with
+ * (src/Kernels/KernelsCommon.h:8-27: DISP_MAX 255, SUPPORT_THRESHOLD 0.85,
+ * GAMMA 3, SRADIUS 2, ...) with every post-filter off, because the
+ * reference's process() stops after the left/right check
+ * (src/Elas.cu:107-119).  With these parameters the output equals the
+ * reference's. */
+void elas_params_reference(elas_params* p);
+
+/* Human-readable text for a status code. */
+const char* elas_b200_status_string(int status);
+
+typedef struct elas_handle elas_handle;
+
+/* Create a matcher bound to CUDA device `device` (reference: the Elas()
+ * constructor, src/Elas.h:70-72, which reads device 0's properties).
+ * `params` may be NULL for elas_params_default(). */
+int elas_b200_create(const elas_params* params, int device, elas_handle** out);
+
+/* Release the handle and its device workspaces. */
+int elas_b200_destroy(elas_handle* h);
+
+/* Replace the parameter block used by subsequent calls. */
+int elas_b200_set_params(elas_handle* h, const elas_params* params);
+int elas_b200_get_params(const elas_handle* h, elas_params* out);
+
+/* Text of the last error on this handle ("" when none). */
+const char* elas_b200_last_error(const elas_handle* h);
+
+/*
+ * Drop-in for Elas::process (src/Elas.h:76-83, src/Elas.cu:19-120).
+ *   left, right : host uint8 images, dims[0] x dims[1], row-major, stride dims[0]
+ *   disp_left, disp_right : host float outputs of dims[0]*dims[1] values;
+ *                 -1 marks an invalid pixel, as in the reference.
+ *   dims        : only dims[0] (width) and dims[1] (height) are read
+ *                 (the reference ignores a libelas-style dims[2]).
+ *   stream      : cudaStream_t (NULL = legacy default stream).
+ * Blocks until the outputs are in host memory.
+ */
+int elas_b200_process(elas_handle* h, const uint8_t* left, const uint8_t* right,
+                      float* disp_left, float* disp_right, const int32_t* dims,
+                      void* stream);
+
+/* Same computation on caller-owned device buffers; asynchronous on `stream`
+ * (no host synchronisation except the one-off workspace growth). */
+int elas_b200_process_device(elas_handle* h, const uint8_t* d_left, const uint8_t* d_right,
+                             float* d_disp_left, float* d_disp_right, const int32_t* dims,
+                             void* stream);
+
+/*
+ * Batched form: n independent pairs of possibly different sizes.  lefts[i],
+ * rights[i], disp_lefts[i], disp_rights[i] are host pointers; dims holds
+ * 2*n int32 (w_i, h_i); disp_max_per_pair (nullable) overrides the handle's
+ * disp_max per pair.  Outputs equal n single elas_b200_process calls.
+ */
+int elas_b200_process_batch(elas_handle* h, int n,
+                            const uint8_t* const* lefts, const uint8_t* const* rights,
+                            float* const* disp_lefts, float* const* disp_rights,
+                            const int32_t* dims, const int32_t* disp_max_per_pair,
+                            void* stream);
+
+/* ---- introspection of the last call (for stage-wise parity checks) ---- */
+
+/* Stages that can be copied out after a process call. */
+#define ELAS_STAGE_DESC_LEFT     0   /* uint8  [h][w][16] */
+#define ELAS_STAGE_DESC_RIGHT    1   /* uint8  [h][w][16] */
+#define ELAS_STAGE_CAN_LR        2   /* int32  [ch][cw] after the L->R and R->L sweeps */
+#define ELAS_STAGE_CAN           3   /* int32  [ch][cw] after inconsistency + redundancy filters */
+#define ELAS_STAGE_SUPPORT       4   /* int32  [n][3] (u, v, d) in candidate raster order */
+#define ELAS_STAGE_GRID_LEFT     5   /* int32  [gh][gw][disp_max+2] {count, d0 < d1 < ...} */
+#define ELAS_STAGE_GRID_RIGHT    6   /* int32  [gh][gw][disp_max+2] */
+#define ELAS_STAGE_TRI_LEFT      7   /* int32  [t][3] support indices, CCW, smallest index first */
+#define ELAS_STAGE_TRI_RIGHT     8   /* int32  [t][3] */
+#define ELAS_STAGE_PRIOR_LEFT    9   /* int32  [h][w] plane prior d_plane, -1 = not covered */
+#define ELAS_STAGE_PRIOR_RIGHT  10   /* int32  [h][w] */
+#define ELAS_STAGE_DISP_LEFT    11   /* float  [h][w] dense result before the L/R check */
+#define ELAS_STAGE_DISP_RIGHT   12   /* float  [h][w] */
+#define ELAS_STAGE_LR_LEFT      13   /* float  [h][w] after the L/R check, before post-filters */
+#define ELAS_STAGE_LR_RIGHT     14   /* float  [h][w] */
+#define ELAS_STAGE_COUNT        15
+
+/* Copy stage `stage` of the last single-pair call into host memory `dst`
+ * of `bytes` bytes.  *needed receives the size in bytes (call with
+ * dst == NULL to query).  Returns ELAS_ERR_INVALID_ARG if bytes is too small. */
+int elas_b200_get_stage(elas_handle* h, int stage, void* dst, size_t bytes, size_t* needed);
+
+/* Number of kernels this handle has launched since creation. */
+int64_t elas_b200_launch_count(const elas_handle* h);
+
+/* ---- seeded synthetic stereo pairs (the benchmark inputs) ---- */
+
+/* Scene presets: 0 = 450x375 D 0-63 (6 planes, two 40x40 textureless
+ * patches); 1 = 1242x375 D 0-255 (12 planes incl. a ground plane, 8%
+ * textureless); 2 = 2880x1988 D 0-511 (40 planes + 2 px sinusoidal ripple);
+ * 3 = batch member (size and disp_max from the arguments).  w/h/disp_max
+ * <= 0 take the preset's values.  gt_left / gt_right (nullable) receive the
+ * float ground-truth disparity of each view. */
+int elas_b200_synth_pair(int preset, uint64_t seed, int32_t w, int32_t h, int32_t disp_max,
+                         uint8_t* left, uint8_t* right, float* gt_left, float* gt_right);
+
+/* Preset geometry (width, height, disp_max) for a scene preset. */
+int elas_b200_synth_dims(int preset, int32_t* w, int32_t* h, int32_t* disp_max);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ELAS_B200_H */

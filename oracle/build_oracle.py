@@ -1,0 +1,47 @@
+"""Build recipe for the oracle (test infrastructure only).
+
+* oracle/liboracle.so      -- the CPU restatement in elas_oracle.cpp
+* oracle/_ref/libreftriangle.so -- the reference's own Triangle
+  (src/triangle.cpp) compiled from the reference tree, with the C shim
+  tri_ref_shim.cpp.  Built only where the reference tree is present; the
+  prebuilt file travels with the repository snapshot.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SRC = "/root/reference/src"
+
+
+def _run(cmd):
+    subprocess.run(cmd, check=True)
+
+
+def build_oracle(force=False):
+    out = os.path.join(HERE, "liboracle.so")
+    src = os.path.join(HERE, "elas_oracle.cpp")
+    if force or not os.path.exists(out) or os.path.getmtime(out) < os.path.getmtime(src):
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
+              src, "-o", out, "-ldl"])
+    return out
+
+
+def build_ref(force=False):
+    out_dir = os.path.join(HERE, "_ref")
+    out = os.path.join(out_dir, "libreftriangle.so")
+    tri = os.path.join(REF_SRC, "triangle.cpp")
+    if not os.path.exists(tri):
+        return out if os.path.exists(out) else None
+    os.makedirs(out_dir, exist_ok=True)
+    shim = os.path.join(HERE, "tri_ref_shim.cpp")
+    if force or not os.path.exists(out) or os.path.getmtime(out) < os.path.getmtime(shim):
+        _run(["g++", "-O2", "-fPIC", "-shared", "-w", "-DREAL_TYPE_FP32", "-I" + REF_SRC,
+              tri, shim, "-o", out])
+    return out
+
+
+if __name__ == "__main__":
+    force = "--force" in sys.argv
+    print(build_oracle(force))
+    print(build_ref(force))

@@ -1,0 +1,101 @@
+"""The GPU Delaunay algorithm (delaunay_core.h), run by its sequential host
+emulation, against the exact checker and the reference's Triangle."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+import elas_b200 as eb
+
+
+def emu_triangulate(lib, xy, row_of):
+    """xy: (n,2) int32 in lattice-row order; row_of: lattice row per point."""
+    n = xy.shape[0]
+    nrows = int(row_of.max()) + 1 if n else 1
+    row_off = np.zeros(nrows + 1, np.int32)
+    np.add.at(row_off, row_of + 1, 1)
+    row_off = np.cumsum(row_off).astype(np.int32)
+    x = np.ascontiguousarray(xy[:, 0], np.int32)
+    y = np.ascontiguousarray(xy[:, 1], np.int32)
+    cap = 2 * n + 16
+    out = np.zeros((cap, 3), np.int32)
+    st = np.zeros(2, np.int64)
+    T = lib.emu_delaunay(x.ctypes.data_as(ctypes.c_void_p), y.ctypes.data_as(ctypes.c_void_p), n,
+                         row_off.ctypes.data_as(ctypes.c_void_p), nrows, out.ctypes.data_as(ctypes.c_void_p), cap,
+                         st.ctypes.data_as(ctypes.c_void_p))
+    assert T >= 0
+    return out[:T], st
+
+
+def check_case(lib, xy, row_of, compare=True):
+    tris, st = emu_triangulate(lib, xy, row_of)
+    ok, stats = oracle.delaunay_check(xy, tris)
+    assert ok, stats
+    if compare and oracle.have_triangle() and xy.shape[0] >= 3:
+        ref = oracle.triangulate_ref(xy.astype(np.float32))
+        assert ref.shape[0] == tris.shape[0]
+        cmp = oracle.tri_compare(xy, tris, ref)
+        assert cmp[4] == 0, cmp      # every difference is a co-circular tie
+    return tris
+
+
+def lattice_points(rng, rows, cols, step, keep, jitter_d=0):
+    pts, row_of = [], []
+    for r in range(rows):
+        for c in range(cols):
+            if rng.random() < keep:
+                d = int(rng.integers(0, jitter_d + 1)) if jitter_d else 0
+                pts.append((c * step - d, r * step))
+                row_of.append(r)
+    return np.array(pts, np.int32).reshape(-1, 2), np.array(row_of, np.int64)
+
+
+@pytest.mark.parametrize("preset", [0, 1])
+def test_support_points_of_synthetic_pairs(emu_lib, preset):
+    L, R, _, _ = eb.synth_pair(preset, 5)
+    p = eb.params_config(eb.synth_dims(preset)[2])
+    _, _, st = oracle.process(L, R, p, dumps=True)
+    uvd = st["support"]
+    for right in (0, 1):
+        check_case(emu_lib, oracle.support_points(uvd, right), uvd[:, 1] // 5)
+
+
+@pytest.mark.parametrize("keep", [1.0, 0.6, 0.2, 0.05])
+def test_lattice_subsets_cocircular_heavy(emu_lib, keep):
+    rng = np.random.default_rng(int(keep * 100))
+    xy, row_of = lattice_points(rng, 30, 40, 5, keep)
+    if xy.shape[0] >= 3:
+        check_case(emu_lib, xy, row_of)
+
+
+def test_shifted_rows_with_duplicates(emu_lib):
+    rng = np.random.default_rng(1)
+    xy, row_of = lattice_points(rng, 25, 30, 5, 0.7, jitter_d=12)
+    assert len(np.unique(xy, axis=0)) < len(xy)          # duplicates present
+    check_case(emu_lib, xy, row_of)
+
+
+def test_degenerate_inputs(emu_lib):
+    # one row: collinear -> no triangles
+    xy = np.array([[0, 0], [5, 0], [10, 0]], np.int32)
+    tris, _ = emu_triangulate(emu_lib, xy, np.zeros(3, np.int64))
+    assert tris.shape[0] == 0
+    # two points, one point, nothing
+    for n in (0, 1, 2):
+        xy = np.array([[5 * i, 5 * i] for i in range(n)], np.int32).reshape(-1, 2)
+        tris, _ = emu_triangulate(emu_lib, xy, np.arange(n))
+        assert tris.shape[0] == 0
+    # single-point rows on a vertical line -> collinear
+    xy = np.array([[10, 5 * i] for i in range(6)], np.int32)
+    tris, _ = emu_triangulate(emu_lib, xy, np.arange(6))
+    assert tris.shape[0] == 0
+    # a column of single points with wide rows above and below
+    xy = np.array([[0, 0], [100, 0], [50, 5], [50, 10], [0, 15], [100, 15]], np.int32)
+    check_case(emu_lib, xy, np.array([0, 0, 1, 2, 3, 3]))
+
+
+def test_random_large(emu_lib):
+    rng = np.random.default_rng(9)
+    xy, row_of = lattice_points(rng, 120, 150, 5, 0.3, jitter_d=40)
+    check_case(emu_lib, xy, row_of)
