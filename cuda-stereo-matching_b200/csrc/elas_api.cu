@@ -47,6 +47,10 @@ struct elas_handle {
     float *out0 = nullptr, *out1 = nullptr;
     int32_t *lab = nullptr, *usize = nullptr;
     unsigned* err = nullptr;
+
+    // per-stage timing
+    bool timing = false;
+    cudaEvent_t ev[ELAS_TIME_COUNT + 1] = {};
 };
 
 namespace {
@@ -244,28 +248,39 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     if (rc != ELAS_OK) return rc;
     h->g = g;
     int n = 0;
+    auto mark = [&](int i) -> cudaError_t { return h->timing ? cudaEventRecord(h->ev[i], st) : cudaSuccess; };
     CK(cudaMemsetAsync(h->err, 0, sizeof(unsigned), st));
+    CK(mark(ELAS_TIME_DESCRIPTOR));
     CK(launch_descriptor(img0, img1, h->desc0, h->desc1, W, H, st));
     n += 1;
+    CK(mark(ELAS_TIME_SUPPORT));
     CK(launch_support(h->desc0, h->desc1, h->can_lr, nullptr, h->can, g, dp, h->num_sms, st));
     n += 4;
+    CK(mark(ELAS_TIME_COMPACT));
     CK(launch_compact(h->can, h->row_cnt, h->row_off, h->uvd, h->x0, h->x1, h->y, g, st));
     n += 3;
+    CK(mark(ELAS_TIME_GRID));
     CK(launch_grid(h->can, h->gtmp0, h->gtmp1, h->grid0, h->grid1, g, st));
     n += 2;
+    CK(mark(ELAS_TIME_DELAUNAY));
     CK(launch_delaunay(h->del[0], h->del[1], h->row_off, g.ch, h->num_sms, h->flip_blocks, h->err, st, &n));
+    CK(mark(ELAS_TIME_PRIOR));
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
                     h->prior0, h->prior1, g, h->num_sms, st));
     n += 1;
+    CK(mark(ELAS_TIME_DENSE));
     CK(launch_dense(h->desc0, h->desc1, h->prior0, h->prior1, h->grid0, h->grid1, h->raw0, h->raw1, g, dp, st));
     n += 1;
+    CK(mark(ELAS_TIME_LR));
     CK(launch_lr(h->raw0, h->raw1, h->lr0, h->lr1, g, p.lr_threshold, st));
     n += 1;
+    CK(mark(ELAS_TIME_POST));
     CK(cudaMemcpyAsync(out0, h->lr0, size_t(W) * H * 4, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(out1, h->lr1, size_t(W) * H * 4, cudaMemcpyDeviceToDevice, st));
     CK(launch_post(out0, h->tmp, h->lab, h->usize, g, dp, p.filter_median, p.filter_adaptive_mean, h->err, st, &n));
     if (!p.postprocess_only_left)
         CK(launch_post(out1, h->tmp, h->lab, h->usize, g, dp, p.filter_median, p.filter_adaptive_mean, h->err, st, &n));
+    CK(mark(ELAS_TIME_COUNT));
     h->launches += n;
     h->have_last = true;
     return ELAS_OK;
@@ -383,8 +398,27 @@ int elas_b200_create(const elas_params* params, int device, elas_handle** out) {
     return ELAS_OK;
 }
 
+int elas_b200_set_timing(elas_handle* h, int enable) {
+    if (!h) return ELAS_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    if (enable && !h->ev[0])
+        for (int i = 0; i <= ELAS_TIME_COUNT; ++i) CK(cudaEventCreate(&h->ev[i]));
+    h->timing = enable != 0;
+    return ELAS_OK;
+}
+
+int elas_b200_get_timing(elas_handle* h, float* ms_out, int n) {
+    if (!h || !ms_out || n < ELAS_TIME_COUNT) return ELAS_ERR_INVALID_ARG;
+    if (!h->timing || !h->have_last) return fail(h, ELAS_ERR_INVALID_ARG, "timing not enabled or no call yet");
+    CK(cudaEventSynchronize(h->ev[ELAS_TIME_COUNT]));
+    for (int i = 0; i < ELAS_TIME_COUNT; ++i) CK(cudaEventElapsedTime(&ms_out[i], h->ev[i], h->ev[i + 1]));
+    return ELAS_OK;
+}
+
 int elas_b200_destroy(elas_handle* h) {
     if (!h) return ELAS_ERR_INVALID_ARG;
+    for (int i = 0; i <= ELAS_TIME_COUNT; ++i)
+        if (h->ev[i]) cudaEventDestroy(h->ev[i]);
     if (h->arena) {
         cudaSetDevice(h->device);
         cudaDeviceSynchronize();

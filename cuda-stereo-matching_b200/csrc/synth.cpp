@@ -326,8 +326,14 @@ extern "C" int elas_b200_synth_pair(int preset, uint64_t seed, int32_t w, int32_
             double bd = -1e300, bu = 0;
             for (int k = 0; k < NP; ++k) {
                 const Plane& p = s.planes[k];
-                double u = x + disp_of(p, x, v);
-                for (int it = 0; it < 8; ++it) u = x + disp_of(p, u, v);
+                // closed-form solution of u = x + a*u + b*v + c, refined for the ripple
+                double u = (x + p.b * v + p.c) / (1.0 - p.a);
+                if (p.shape == 1 || p.shape == 2) {
+                    double m = 2.0 * std::fabs(p.ripple) + 1.0;
+                    if (u < p.cx - p.rx - m || u > p.cx + p.rx + m || v < p.cy - p.ry || v > p.cy + p.ry) continue;
+                }
+                if (p.ripple != 0.0)
+                    for (int it = 0; it < 6; ++it) u = x + disp_of(p, u, v);
                 if (!covers(p, u, v, H)) continue;
                 double d = u - x;
                 if (d > bd) { bd = d; best = k; bu = u; }

@@ -81,6 +81,8 @@ def library():
         lib.elas_b200_process_batch.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                                 c_void_p, c_void_p]
         lib.elas_b200_get_stage.argtypes = [c_void_p, c_int, c_void_p, c_size_t, POINTER(c_size_t)]
+        lib.elas_b200_set_timing.argtypes = [c_void_p, c_int]
+        lib.elas_b200_get_timing.argtypes = [c_void_p, c_void_p, c_int]
         lib.elas_b200_launch_count.restype = c_int64
         lib.elas_b200_launch_count.argtypes = [c_void_p]
         lib.elas_b200_synth_pair.argtypes = [c_int, c_uint64, c_int32, c_int32, c_int32, c_void_p, c_void_p,
@@ -227,6 +229,17 @@ class Elas:
         buf = np.empty(need.value, np.uint8)
         self._check(self._lib.elas_b200_get_stage(self._h, sid, _ptr(buf), need.value, ctypes.byref(need)))
         return buf
+
+    TIME_STAGES = ["descriptor", "support", "compact", "grid", "delaunay", "prior", "dense", "lr", "post"]
+
+    def set_timing(self, enable=True):
+        self._check(self._lib.elas_b200_set_timing(self._h, int(enable)))
+
+    def timing(self):
+        """Per-stage device times (ms) of the last call, as a dict."""
+        out = np.zeros(len(self.TIME_STAGES), np.float32)
+        self._check(self._lib.elas_b200_get_timing(self._h, _ptr(out), len(out)))
+        return dict(zip(self.TIME_STAGES, out.tolist()))
 
     @property
     def launch_count(self):

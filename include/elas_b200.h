@@ -163,6 +163,26 @@ int elas_b200_get_stage(elas_handle* h, int stage, void* dst, size_t bytes, size
 /* Number of kernels this handle has launched since creation. */
 int64_t elas_b200_launch_count(const elas_handle* h);
 
+/* ---- per-stage device timing (CUDA events on the launch stream) ---- */
+
+#define ELAS_TIME_DESCRIPTOR  0   /* fused Sobel + descriptor, both views */
+#define ELAS_TIME_SUPPORT     1   /* support sweep L->R and R->L + filters */
+#define ELAS_TIME_COMPACT     2   /* support list compaction */
+#define ELAS_TIME_GRID        3   /* disparity grid, both views */
+#define ELAS_TIME_DELAUNAY    4   /* triangulation, both views */
+#define ELAS_TIME_PRIOR       5   /* plane prior, both views */
+#define ELAS_TIME_DENSE       6   /* dense matching, both views */
+#define ELAS_TIME_LR          7   /* left/right check */
+#define ELAS_TIME_POST        8   /* post-filters */
+#define ELAS_TIME_COUNT       9
+
+/* Enable (1) or disable (0) recording of per-stage events. */
+int elas_b200_set_timing(elas_handle* h, int enable);
+
+/* Wait for the last call and write its per-stage device times in ms
+ * (ELAS_TIME_COUNT values) to ms_out. */
+int elas_b200_get_timing(elas_handle* h, float* ms_out, int n);
+
 /* ---- seeded synthetic stereo pairs (the benchmark inputs) ---- */
 
 /* Scene presets: 0 = 450x375 D 0-63 (6 planes, two 40x40 textureless

@@ -1,0 +1,197 @@
+"""Parity of the CUDA pipeline with the CPU oracle, stage by stage.
+
+Every stage is bit-exact except the post-filtered output (float, 1e-4).
+The oracle consumes the GPU's triangle list, so the dense stages are
+compared on identical triangulations; the triangulation itself is checked
+exactly (valid, empty-circumcircle under the symbolic perturbation) and
+against the reference's Triangle (equal wherever no four points are
+co-circular).
+"""
+import numpy as np
+import pytest
+
+import elas_b200 as eb
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+POST_TOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def elas():
+    e = eb.Elas(eb.params_reference())
+    yield e
+    e.close()
+
+
+def gpu_stages(e, W, H, p):
+    cw, ch, gw, gh = oracle.geom(W, H, p)
+    st = {}
+    st["desc_left"] = e.stage("desc_left").reshape(H, W, 16)
+    st["desc_right"] = e.stage("desc_right").reshape(H, W, 16)
+    st["can_lr"] = e.stage("can_lr").view(np.int32).reshape(ch, cw)
+    st["can"] = e.stage("can").view(np.int32).reshape(ch, cw)
+    st["support"] = e.stage("support").view(np.int32).reshape(-1, 3)
+    st["grid_left"] = e.stage("grid_left").view(np.int32).reshape(gh, gw, p.disp_max + 2)
+    st["grid_right"] = e.stage("grid_right").view(np.int32).reshape(gh, gw, p.disp_max + 2)
+    st["tri_left"] = e.stage("tri_left").view(np.int32).reshape(-1, 3)
+    st["tri_right"] = e.stage("tri_right").view(np.int32).reshape(-1, 3)
+    for k in ("prior_left", "prior_right"):
+        st[k] = e.stage(k).view(np.int32).reshape(H, W)
+    for k in ("disp_left", "disp_right", "lr_left", "lr_right"):
+        st[k] = e.stage(k).view(np.float32).reshape(H, W)
+    return st
+
+
+def run_and_compare(e, L, R, p, check_triangle=True):
+    e.set_params(p)
+    H, W = L.shape
+    D1, D2 = e.process(L, R)
+    g = gpu_stages(e, W, H, p)
+    o1, o2, o = oracle.process(L, R, p, tri_left=g["tri_left"], tri_right=g["tri_right"], dumps=True)
+    for k in ("desc_left", "desc_right", "can_lr", "can", "support", "grid_left", "grid_right", "prior_left",
+              "prior_right"):
+        assert g[k].shape == o[k].shape, k
+        mism = np.count_nonzero(g[k] != o[k])
+        assert mism == 0, f"{k}: {mism} mismatches"
+    for k in ("disp_left", "disp_right", "lr_left", "lr_right"):
+        assert np.array_equal(g[k], o[k]), f"{k}: {np.count_nonzero(g[k] != o[k])} mismatches"
+    np.testing.assert_allclose(D1, o1, atol=POST_TOL, rtol=0)
+    np.testing.assert_allclose(D2, o2, atol=POST_TOL, rtol=0)
+    uvd = g["support"]
+    for right, key in ((0, "tri_left"), (1, "tri_right")):
+        xy = oracle.support_points(uvd, right)
+        ok, stats = oracle.delaunay_check(xy, g[key])
+        assert ok, (key, stats)
+        if check_triangle and oracle.have_triangle() and len(uvd) >= 3:
+            ref = oracle.triangulate_ref(xy.astype(np.float32))
+            assert ref.shape[0] == g[key].shape[0], key
+            cmp = oracle.tri_compare(xy, g[key], ref)
+            assert cmp[4] == 0, (key, cmp)
+    return D1, D2, g
+
+
+def test_stagewise_parity_config0(elas):
+    L, R, gt, _ = eb.synth_pair(0, 1)
+    D1, D2, g = run_and_compare(elas, L, R, eb.params_config(63))
+    valid = D1 >= 0
+    assert valid.mean() > 0.5
+    assert (np.abs(D1 - gt) > 2)[valid].mean() < 0.2
+
+
+def test_reference_parameters_config0(elas):
+    L, R, _, _ = eb.synth_pair(0, 2)
+    run_and_compare(elas, L, R, eb.params_reference())
+
+
+def test_stagewise_parity_config1(elas):
+    L, R, _, _ = eb.synth_pair(1, 1)
+    run_and_compare(elas, L, R, eb.params_config(255))
+
+
+@pytest.mark.parametrize("W,H,D", [(97, 61, 31), (160, 120, 47), (333, 211, 95), (16, 16, 8)])
+def test_odd_sizes(elas, W, H, D):
+    L, R, _, _ = eb.synth_pair(3, 7, width=W, height=H, disp_max=D)
+    run_and_compare(elas, L, R, eb.params_config(D))
+
+
+def test_non_default_parameters(elas):
+    L, R, _, _ = eb.synth_pair(3, 9, width=400, height=300, disp_max=80)
+    p = eb.params_config(80)
+    p.candidate_stepsize = 4
+    p.grid_size = 16
+    p.disp_min = 3
+    p.support_threshold = 0.95
+    p.incon_window_size = 3
+    p.lr_threshold = 1
+    p.match_texture = 6
+    p.sradius = 3
+    p.gamma = 5
+    p.postprocess_only_left = True
+    run_and_compare(elas, L, R, p)
+
+
+def test_textureless_and_tiny_inputs(elas):
+    flat = np.full((64, 80), 128, np.uint8)
+    elas.set_params(eb.params_config(31))
+    D1, D2 = elas.process(flat, flat)
+    assert (D1 == -1).all() and (D2 == -1).all()
+    assert elas.stage("support").size == 0
+    noise = np.random.default_rng(0).integers(0, 256, (16, 16), dtype=np.uint8)
+    run_and_compare(elas, noise, noise, eb.params_config(8))
+
+
+def test_end_to_end_against_triangle(elas):
+    """Same pair through the oracle with the reference's Triangle: only pixels
+    whose plane prior comes from a co-circular or duplicate-point choice may
+    differ."""
+    if not oracle.have_triangle():
+        pytest.skip("reference Triangle not built")
+    L, R, _, _ = eb.synth_pair(1, 4)
+    p = eb.params_reference()
+    elas.set_params(p)
+    D1, D2 = elas.process(L, R)
+    o1, o2, _ = oracle.process(L, R, p)
+    diff = (np.count_nonzero(D1 != o1) + np.count_nonzero(D2 != o2)) / (2.0 * D1.size)
+    print(f"pixels differing from the Triangle pipeline: {diff:.5f}")
+    assert diff < 0.02
+
+
+def test_deterministic_repeat(elas):
+    L, R, _, _ = eb.synth_pair(1, 8)
+    p = eb.params_config(255)
+    elas.set_params(p)
+    a1, a2 = elas.process(L, R)
+    sa = gpu_stages(elas, L.shape[1], L.shape[0], p)
+    b1, b2 = elas.process(L, R)
+    sb = gpu_stages(elas, L.shape[1], L.shape[0], p)
+    assert np.array_equal(a1, b1) and np.array_equal(a2, b2)
+    for k in sa:
+        assert np.array_equal(sa[k], sb[k]), k
+
+
+def test_batch_equals_singles(elas):
+    pairs = [eb.synth_pair(3, s, width=w, height=h, disp_max=d)
+             for s, (w, h, d) in enumerate([(320, 240, 64), (480, 272, 128), (400, 304, 64)])]
+    dmax = [64, 128, 64]
+    elas.set_params(eb.params_config(64))
+    b1, b2 = elas.process_batch([x[0] for x in pairs], [x[1] for x in pairs], disp_max=dmax)
+    for (L, R, _, _), d, x1, x2 in zip(pairs, dmax, b1, b2):
+        elas.set_params(eb.params_config(d))
+        s1, s2 = elas.process(L, R)
+        assert np.array_equal(s1, x1) and np.array_equal(s2, x2)
+
+
+def test_device_api_matches_host_api(elas):
+    import torch
+
+    L, R, _, _ = eb.synth_pair(0, 5)
+    p = eb.params_config(63)
+    elas.set_params(p)
+    h1, h2 = elas.process(L, R)
+    H, W = L.shape
+    dl = torch.from_numpy(L).cuda()
+    dr = torch.from_numpy(R).cuda()
+    o1 = torch.empty((H, W), dtype=torch.float32, device="cuda")
+    o2 = torch.empty_like(o1)
+    torch.cuda.synchronize()
+    elas.process_device(dl.data_ptr(), dr.data_ptr(), o1.data_ptr(), o2.data_ptr(), W, H,
+                        stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(o1.cpu().numpy(), h1) and np.array_equal(o2.cpu().numpy(), h2)
+
+
+def test_cpp_drop_in_class_runs(tmp_path):
+    import os
+    import subprocess
+
+    from conftest import REPO
+    exe = tmp_path / "demo"
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(REPO, "include"),
+                    os.path.join(REPO, "tests", "native", "elas_class_demo.cpp"), "-o", str(exe),
+                    "-L", os.path.dirname(eb.LIB_PATH), "-lelas_b200",
+                    "-Wl,-rpath," + os.path.dirname(eb.LIB_PATH)], check=True)
+    out = subprocess.run([str(exe), "run"], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "density" in out.stdout
