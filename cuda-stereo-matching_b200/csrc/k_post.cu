@@ -20,22 +20,39 @@ namespace elas {
 
 namespace {
 
-constexpr int UF_LIMIT = 1 << 20;   // bound on any union-find walk / retry loop
+constexpr int UF_LIMIT = 1 << 22;   // bound on any union-find walk / retry loop
 
-__device__ __forceinline__ int uf_find(const int32_t* lab, int x, unsigned* err) {
+// Root of x with path halving (labels only ever move to a smaller index, so
+// concurrent halving keeps every node in its tree).
+__device__ __forceinline__ int uf_find(int32_t* lab, int x, unsigned* err) {
     for (int it = 0; it < UF_LIMIT; ++it) {
         int p = lab[x];
         if (p == x) return x;
+        int gp = lab[p];
+        if (gp != p) lab[x] = gp;
         x = p;
     }
     atomicOr(err, ERRF_BOUNDS);
     return x;
 }
 
-__global__ void k_uf_init(const float* __restrict__ D, int32_t* __restrict__ lab, int32_t* __restrict__ sz, int n) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    lab[i] = D[i] >= 0 ? i : -1;
+// Labels start at the left neighbour when it is connected (the most common
+// union), else at the pixel itself.
+__global__ void k_uf_init(const float* __restrict__ D, int32_t* __restrict__ lab, int32_t* __restrict__ sz, int W,
+                          int H, float thr) {
+    int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (u >= W || v >= H) return;
+    int i = v * W + u;
+    float d = D[i];
+    int l = -1;
+    if (d >= 0) {
+        l = i;
+        if (u > 0) {
+            float q = D[i - 1];
+            if (q >= 0 && fabsf(q - d) <= thr) l = i - 1;
+        }
+    }
+    lab[i] = l;
     sz[i] = 0;
 }
 
@@ -43,10 +60,13 @@ __device__ void uf_union(int32_t* lab, int a, int b, unsigned* err) {
     for (int it = 0; it < UF_LIMIT; ++it) {
         int ra = uf_find(lab, a, err), rb = uf_find(lab, b, err);
         if (ra == rb) return;
-        if (ra < rb) { int t = ra; ra = rb; rb = t; }
+        if (ra < rb) {   // keep (a, ra) and (b, rb) paired: hook the larger root
+            int t = ra; ra = rb; rb = t;
+            t = a; a = b; b = t;
+        }
         int old = atomicCAS(&lab[ra], ra, rb);
         if (old == ra) return;
-        a = old;
+        a = old;         // ra gained a parent meanwhile: continue from it
     }
     atomicOr(err, ERRF_BOUNDS);
 }
@@ -67,21 +87,57 @@ __global__ void k_uf_union(const float* __restrict__ D, int32_t* lab, int W, int
     }
 }
 
+// Flatten every label to its root and count segment sizes; lanes of a warp
+// that share a root add once (segments are large, so this removes most of
+// the contention on the root counters).
 __global__ void k_uf_count(int32_t* lab, int32_t* sz, int n, unsigned* err) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || lab[i] < 0) return;
-    int r = uf_find(lab, i, err);
-    atomicAdd(&sz[r], 1);
+    int r = -1;
+    if (i < n && lab[i] >= 0) {
+        r = uf_find(lab, i, err);
+        lab[i] = r;
+    }
+    unsigned peers = __match_any_sync(0xffffffffu, r);
+    int leader = __ffs(peers) - 1;
+    if (r >= 0 && (threadIdx.x & 31) == leader) atomicAdd(&sz[r], __popc(peers));
 }
 
-__global__ void k_uf_apply(float* D, const int32_t* lab, const int32_t* sz, int n, int min_size, unsigned* err) {
+__global__ void k_uf_apply(float* D, const int32_t* lab, const int32_t* sz, int n, int min_size) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || lab[i] < 0) return;
-    int r = uf_find(lab, i, err);
-    if (sz[r] < min_size) D[i] = -1.0f;
+    if (i >= n) return;
+    int r = lab[i];
+    if (r >= 0 && sz[r] < min_size) D[i] = -1.0f;
 }
 
-// horizontal = 1: one thread per row; 0: one thread per column.
+// Gap interpolation, one pixel per thread: an invalid pixel looks for the
+// nearest valid pixel on each side within `gap`; both found and the run
+// between them no longer than `gap` -> fill.  Equivalent to the serial
+// per-line scan because filled runs never touch the pixels that bound
+// other runs.  S = pass input, O = pass output.
+__global__ void k_gap_px(const float* __restrict__ S, float* __restrict__ O, int W, int H, int gap, int horizontal) {
+    int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (u >= W || v >= H) return;
+    size_t i = size_t(v) * W + u;
+    float c = S[i];
+    if (c < 0) {
+        const int len = horizontal ? W : H, k = horizontal ? u : v;
+        const long stride = horizontal ? 1 : W;
+        int lo = -1, hi = -1;
+        for (int j = 1; j <= gap && k - j >= 0; ++j)
+            if (S[i - j * stride] >= 0) { lo = k - j; break; }
+        if (lo >= 0)
+            for (int j = 1; j <= gap && k + j < len; ++j)
+                if (S[i + j * stride] >= 0) { hi = k + j; break; }
+        if (lo >= 0 && hi >= 0 && hi - lo - 1 <= gap) {
+            float a = S[i - (k - lo) * stride], b = S[i + (hi - k) * stride];
+            c = fabsf(a - b) <= 3.0f ? __fmul_rn(0.5f, __fadd_rn(a, b)) : fminf(a, b);
+        }
+    }
+    O[i] = c;
+}
+
+// horizontal = 1: one thread per row; 0: one thread per column (used for
+// gap widths too large for the per-pixel search).
 __global__ void k_gap(float* D, int W, int H, int gap, int horizontal) {
     int l = blockIdx.x * blockDim.x + threadIdx.x;
     int lines = horizontal ? H : W, len = horizontal ? W : H;
@@ -157,16 +213,22 @@ cudaError_t launch_post(float* disp, float* tmp, int32_t* lab, int32_t* size, co
     const int W = g.W, H = g.H, n = W * H;
     const int tb = 256;
     int launched = 0;
+    const dim3 grid2((W + tb - 1) / tb, H);
     if (p.speckle_size > 0) {
-        k_uf_init<<<(n + tb - 1) / tb, tb, 0, st>>>(disp, lab, size, n);
-        k_uf_union<<<dim3((W + tb - 1) / tb, H), tb, 0, st>>>(disp, lab, W, H, p.speckle_sim_threshold, err);
+        k_uf_init<<<grid2, tb, 0, st>>>(disp, lab, size, W, H, p.speckle_sim_threshold);
+        k_uf_union<<<grid2, tb, 0, st>>>(disp, lab, W, H, p.speckle_sim_threshold, err);
         k_uf_count<<<(n + tb - 1) / tb, tb, 0, st>>>(lab, size, n, err);
-        k_uf_apply<<<(n + tb - 1) / tb, tb, 0, st>>>(disp, lab, size, n, p.speckle_size, err);
+        k_uf_apply<<<(n + tb - 1) / tb, tb, 0, st>>>(disp, lab, size, n, p.speckle_size);
         launched += 4;
     }
     if (p.ipol_gap_width > 0) {
-        k_gap<<<(H + 127) / 128, 128, 0, st>>>(disp, W, H, p.ipol_gap_width, 1);
-        k_gap<<<(W + 127) / 128, 128, 0, st>>>(disp, W, H, p.ipol_gap_width, 0);
+        if (p.ipol_gap_width <= 64) {
+            k_gap_px<<<grid2, tb, 0, st>>>(disp, tmp, W, H, p.ipol_gap_width, 1);
+            k_gap_px<<<grid2, tb, 0, st>>>(tmp, disp, W, H, p.ipol_gap_width, 0);
+        } else {
+            k_gap<<<(H + 127) / 128, 128, 0, st>>>(disp, W, H, p.ipol_gap_width, 1);
+            k_gap<<<(W + 127) / 128, 128, 0, st>>>(disp, W, H, p.ipol_gap_width, 0);
+        }
         launched += 2;
     }
     if (adaptive_mean) {

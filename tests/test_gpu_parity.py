@@ -112,6 +112,30 @@ def test_non_default_parameters(elas):
     run_and_compare(elas, L, R, p)
 
 
+@pytest.mark.parametrize("filt", ["speckle", "gap", "gap_wide", "mean", "median"])
+def test_post_filters_individually(elas, filt):
+    L, R, _, _ = eb.synth_pair(1, 3)
+    p = eb.params_reference()
+    if filt == "speckle":
+        p.speckle_size = 200
+    elif filt == "gap":
+        p.ipol_gap_width = 3
+    elif filt == "gap_wide":
+        p.ipol_gap_width = 5000
+    elif filt == "mean":
+        p.filter_adaptive_mean = True
+    else:
+        p.filter_median = True
+    run_and_compare(elas, L, R, p, check_triangle=False)
+
+
+def test_constructor_default_parameters(elas):
+    """Elas::parameters() defaults (support_threshold 0.95, gamma 5, sradius 3,
+    ipol_gap_width 5000, median on)."""
+    L, R, _, _ = eb.synth_pair(1, 6)
+    run_and_compare(elas, L, R, eb.params_default(), check_triangle=False)
+
+
 def test_textureless_and_tiny_inputs(elas):
     flat = np.full((64, 80), 128, np.uint8)
     elas.set_params(eb.params_config(31))
