@@ -8,16 +8,19 @@
 //     coordinates (the lowest support index of a group is kept; Triangle
 //     keeps the first of its randomised sort, src/triangle.cpp divconqdelaunay).
 //  2. Insert the points row by row: the strip between two consecutive
-//     non-empty rows is triangulated by one merge ("zipper") pass, choosing
-//     at each step the diagonal that the incircle test prefers.
+//     non-empty rows is triangulated by merging the two rows by x; every
+//     point finds its own triangle by a binary search in the other row
+//     (merge path), so the strips are built fully in parallel.
 //  3. Fill the pockets between the rows' first (last) points and the convex
 //     hull with the monotone-chain stack walk.
 //  4. Build edge adjacency with an open-addressing hash of undirected edges.
-//  5. Lawson edge flipping in parallel rounds: every non-locally-Delaunay
-//     interior edge proposes itself, an edge flips when it holds the minimum
-//     priority on both of its triangles, neighbour links are repaired through
-//     a forwarding table.  Converges to the unique Delaunay triangulation
-//     under the symbolic perturbation below.
+//  5. Lawson edge flipping in rounds driven by a worklist: round 0 tests
+//     every interior edge; later rounds test only the four outer edges of
+//     each quad flipped in the previous round and the proposals that lost
+//     their lock.  An edge flips when it holds the minimum priority on both
+//     of its triangles; neighbour links are repaired through a forwarding
+//     table in two phases (resolve, then write).  Converges to the unique
+//     Delaunay triangulation under the symbolic perturbation below.
 //
 // Predicates: orientation and incircle on integer coordinates in int64 --
 // exact for |coordinates| < 2^15 (terms stay below 2^62).  Ties (four
@@ -70,50 +73,65 @@ HD bool inside_sos(Pts P, int a, int b, int c, int d) {
     return orient(P, a, b, d) < 0;
 }
 
-// Triangulate the strip between an upper row A[0..m) and a lower row
-// B[0..n), both sorted by strictly increasing x.  Writes (m-1)+(n-1)
-// counter-clockwise triangles.
-HD void zipper(Pts P, const int32_t* A, int m, const int32_t* B, int n, int32_t* tri) {
-    int i = 0, j = 0, k = 0;
-    while (i < m - 1 || j < n - 1) {
-        bool adv_a;
-        if (i == m - 1) adv_a = false;
-        else if (j == n - 1) adv_a = true;
-        else adv_a = incircle(P, A[i], A[i + 1], B[j], B[j + 1]) <= 0;
-        if (adv_a) {
-            tri[3 * k] = A[i]; tri[3 * k + 1] = A[i + 1]; tri[3 * k + 2] = B[j];
-            ++i;
-        } else {
-            tri[3 * k] = A[i]; tri[3 * k + 1] = B[j + 1]; tri[3 * k + 2] = B[j];
-            ++j;
-        }
-        ++k;
+// Strip between an upper row A[0..m) and a lower row B[0..n), both sorted
+// by strictly increasing x: walking the merge of A[1..m) and B[1..n) by x
+// (A first on equal x), each element advances its row by one point and
+// creates one counter-clockwise triangle.  These two functions give the
+// triangle of one element and its position in the strip, so every point
+// can emit its triangles independently.
+//
+// Number of elements of the sorted X[0..n) with x < v (strict) or x <= v.
+HD int count_below(Pts P, const int32_t* X, int n, int32_t v, bool inclusive) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        int32_t x = P.x[X[mid]];
+        if (inclusive ? (x <= v) : (x < v)) lo = mid + 1;
+        else hi = mid;
     }
+    return lo;
+}
+
+// Element A[k], 1 <= k < m: triangle (A[k-1], A[k], B[j]); returns its position.
+HD int strip_tri_upper(Pts P, const int32_t* A, const int32_t* B, int n, int k, int32_t* tri) {
+    int cl = count_below(P, B, n, P.x[A[k]], false);
+    int j = cl > 0 ? cl - 1 : 0;
+    tri[0] = A[k - 1]; tri[1] = A[k]; tri[2] = B[j];
+    return (k - 1) + j;
+}
+
+// Element B[k], 1 <= k < n: triangle (A[i], B[k], B[k-1]); returns its position.
+HD int strip_tri_lower(Pts P, const int32_t* A, int m, const int32_t* B, int k, int32_t* tri) {
+    int cl = count_below(P, A, m, P.x[B[k]], true);
+    int i = cl > 0 ? cl - 1 : 0;
+    tri[0] = A[i]; tri[1] = B[k]; tri[2] = B[k - 1];
+    return i + (k - 1);
 }
 
 // Fill the pocket between a boundary chain (one point per non-empty row,
-// top to bottom) and its convex hull.  side = +1 for the left chain (first
-// points), -1 for the right chain (last points).  `stack` has room for
-// `len` entries.  Returns the number of triangles written.
-HD int fill_pockets(Pts P, const int32_t* chain, int len, int side, int32_t* stack, int32_t* tri) {
+// top to bottom: point index ci[k] at (cx[k], cy[k])) and its convex hull.
+// side = +1 for the left chain (first points), -1 for the right chain
+// (last points).  `stack` (chain positions) has room for `len` entries.
+// Returns the number of counter-clockwise triangles written.
+HD int fill_pockets(const int32_t* ci, const int32_t* cx, const int32_t* cy, int len, int side, int32_t* stack,
+                    int32_t* tri) {
     int sp = 0, k = 0;
     for (int i = 0; i < len; ++i) {
-        int p = chain[i];
         while (sp >= 2) {
-            int64_t o = orient(P, stack[sp - 2], stack[sp - 1], p);
+            int a = stack[sp - 2], b = stack[sp - 1];
+            int64_t o = (int64_t(cx[b]) - cx[a]) * (int64_t(cy[i]) - cy[a]) -
+                        (int64_t(cy[b]) - cy[a]) * (int64_t(cx[i]) - cx[a]);
             if (side > 0 ? (o > 0) : (o < 0)) {
-                if (side > 0) {
-                    tri[3 * k] = stack[sp - 2]; tri[3 * k + 1] = stack[sp - 1]; tri[3 * k + 2] = p;
-                } else {
-                    tri[3 * k] = stack[sp - 2]; tri[3 * k + 1] = p; tri[3 * k + 2] = stack[sp - 1];
-                }
+                tri[3 * k] = ci[a];
+                tri[3 * k + 1] = side > 0 ? ci[b] : ci[i];
+                tri[3 * k + 2] = side > 0 ? ci[i] : ci[b];
                 ++k;
                 --sp;
             } else {
                 break;
             }
         }
-        stack[sp++] = p;
+        stack[sp++] = i;
     }
     return k;
 }
@@ -144,55 +162,53 @@ constexpr int32_t FINAL = 1 << 30;          // opp entry already refers to the n
 constexpr uint32_t LOCK_FREE = 0xFFFFFFFFu;
 constexpr unsigned long long HASH_EMPTY = ~0ull;
 
-// Per-problem state of one triangulation.
-struct Tri {
+// Per-problem state of one triangulation during flipping.
+struct Flip {
     Pts P;
     int32_t* tri;       // [3*Tmax] vertex triples, counter-clockwise
     int32_t* opp;       // [3*Tmax] neighbour half-edge (3*t+s) across edge (v_s, v_s+1), -1 = hull
-    uint32_t* lock;     // [Tmax]
-    int32_t* fwd;       // [3*Tmax] old half-edge -> new half-edge within a flip round
-    int32_t* cand;      // [2*Tmax] candidate half-edges of the current round
-    int32_t* ctr;       // counters: [0] triangles, [1] strip triangles, [2],[3] candidates (round parity),
-                        //           [4] rounds used, [5] flips done, [6] non-empty rows
+    uint32_t* lock;     // [Tmax]   minimum proposal priority on the triangle this round
+    int32_t* fround;    // [Tmax]   last round the triangle was flipped (-1 = never)
+    int32_t* fwd;       // [3*Tmax] old half-edge -> new half-edge, valid for one round
+    int32_t* cand;      // [2*3*Tmax] proposals of the round: (half-edge, neighbour triangle)
+    int32_t* flips;     // [Tmax]   flipped pairs of the round: (t, n)
+    int32_t* res;       // [2*Tmax] resolved outer neighbours of the flipped pairs (4 per pair)
+    int32_t* fwdl;      // [2*Tmax] forwarding entries written this round (to clear next round)
+    int32_t* wl[2];     // [6*Tmax] worklists of half-edges
     int Tmax;
 };
 
-// Phase A of a flip round for triangle t: clear forwarding, test the edges
-// this triangle owns (neighbour index larger), propose the illegal ones.
-// Returns false if an index is out of range.
-template <class AtomicMin, class AtomicAdd>
-HD bool flip_propose(Tri& S, int t, int T, uint32_t round, AtomicMin amin, AtomicAdd aadd) {
-    for (int s = 0; s < 3; ++s) S.fwd[3 * t + s] = -1;
-    bool ok = true;
-    for (int s = 0; s < 3; ++s) {
-        int o = S.opp[3 * t + s];
-        if (o < 0) continue;
-        int n = o / 3;
-        if (n <= t) continue;
-        if (n >= T) { ok = false; continue; }
-        int sn = o % 3;
-        int a = S.tri[3 * t + s], b = S.tri[3 * t + (s + 1) % 3], c = S.tri[3 * t + (s + 2) % 3];
-        int d = S.tri[3 * n + (sn + 2) % 3];
-        if (inside_sos(S.P, a, b, c, d)) {
-            uint32_t p = prio(uint32_t(3 * t + s), round);
-            amin(&S.lock[t], p);
-            amin(&S.lock[n], p);
-            int idx = aadd(&S.ctr[2 + (round & 1)], 1);
-            if (idx < 2 * S.Tmax) S.cand[idx] = 3 * t + s;
-            else ok = false;
-        }
+// Phase A: test half-edge h; propose it if its edge is not locally Delaunay.
+// `owner`: only the triangle with the smaller index tests a shared edge
+// (round 0 walks every half-edge).
+template <class AtomicMin, class Append>
+HD bool flip_propose(Flip& S, int h, int T, uint32_t round, bool owner, AtomicMin amin, Append append_cand) {
+    int t = h / 3, s = h % 3;
+    int o = S.opp[h];
+    if (o < 0) return true;
+    int n = o / 3;
+    if (n >= T || t >= T) return false;
+    if (owner && n <= t) return true;
+    int sn = o % 3;
+    int a = S.tri[3 * t + s], b = S.tri[3 * t + (s + 1) % 3], c = S.tri[3 * t + (s + 2) % 3];
+    int d = S.tri[3 * n + (sn + 2) % 3];
+    if (inside_sos(S.P, a, b, c, d)) {
+        uint32_t p = prio(uint32_t(h), round);
+        amin(&S.lock[t], p);
+        amin(&S.lock[n], p);
+        append_cand(h, n);
     }
-    return ok;
+    return true;
 }
 
-// Phase B for one candidate half-edge e: flip if it won both locks.
-HD bool flip_apply(Tri& S, int e, uint32_t round) {
-    int t = e / 3, s = e % 3;
-    int o = S.opp[e];
-    if (o < 0) return false;
-    int n = o / 3, sn = o % 3;
-    uint32_t p = prio(uint32_t(e), round);
+// Phase B: flip the proposal (h, n) if it won both locks.  Returns true if
+// flipped; the caller records the pair and the four forwarding slots.
+HD bool flip_apply(Flip& S, int h, int n, uint32_t round, int32_t* fwd_slots) {
+    int t = h / 3, s = h % 3;
+    uint32_t p = prio(uint32_t(h), round);
     if (S.lock[t] != p || S.lock[n] != p) return false;
+    int o = S.opp[h];
+    int sn = o % 3;
     int a = S.tri[3 * t + s], b = S.tri[3 * t + (s + 1) % 3], c = S.tri[3 * t + (s + 2) % 3];
     int d = S.tri[3 * n + (sn + 2) % 3];
     int O_bc = S.opp[3 * t + (s + 1) % 3], O_ca = S.opp[3 * t + (s + 2) % 3];
@@ -202,27 +218,46 @@ HD bool flip_apply(Tri& S, int e, uint32_t round) {
     S.tri[3 * n] = d; S.tri[3 * n + 1] = b; S.tri[3 * n + 2] = c;
     S.opp[3 * t] = O_ca; S.opp[3 * t + 1] = O_ad; S.opp[3 * t + 2] = FINAL | (3 * n + 2);
     S.opp[3 * n] = O_db; S.opp[3 * n + 1] = O_bc; S.opp[3 * n + 2] = FINAL | (3 * t + 2);
-    S.fwd[3 * t + (s + 2) % 3] = 3 * t;        // edge c-a  -> t' slot 0
-    S.fwd[3 * t + (s + 1) % 3] = 3 * n + 1;    // edge b-c  -> n' slot 1
-    S.fwd[3 * n + (sn + 1) % 3] = 3 * t + 1;   // edge a-d  -> t' slot 1
-    S.fwd[3 * n + (sn + 2) % 3] = 3 * n;       // edge d-b  -> n' slot 0
+    fwd_slots[0] = 3 * t + (s + 2) % 3; S.fwd[fwd_slots[0]] = 3 * t;        // edge c-a -> t' slot 0
+    fwd_slots[1] = 3 * t + (s + 1) % 3; S.fwd[fwd_slots[1]] = 3 * n + 1;    // edge b-c -> n' slot 1
+    fwd_slots[2] = 3 * n + (sn + 1) % 3; S.fwd[fwd_slots[2]] = 3 * t + 1;   // edge a-d -> t' slot 1
+    fwd_slots[3] = 3 * n + (sn + 2) % 3; S.fwd[fwd_slots[3]] = 3 * n;       // edge d-b -> n' slot 0
+    S.fround[t] = int32_t(round);
+    S.fround[n] = int32_t(round);
     return true;
 }
 
-// Phase C for triangle t: resolve neighbour links through the forwarding
-// table and release the lock.
-HD void flip_repair(Tri& S, int t) {
-    for (int s = 0; s < 3; ++s) {
-        int o = S.opp[3 * t + s];
-        if (o < 0) continue;
-        if (o & FINAL) {
-            S.opp[3 * t + s] = o & ~FINAL;
-        } else {
-            int f = S.fwd[o];
-            if (f >= 0) S.opp[3 * t + s] = f;
+// The four outer half-edges of a flipped pair (t, n): t' slots 0,1 and n' slots 0,1.
+HD int outer_slot(int t, int n, int k) { return k < 2 ? 3 * t + k : 3 * n + (k - 2); }
+
+// Phase C1 (read only): resolve where the outer neighbours of pair f now live.
+HD void flip_resolve(Flip& S, int f) {
+    int t = S.flips[2 * f], n = S.flips[2 * f + 1];
+    for (int k = 0; k < 4; ++k) {
+        int o = S.opp[outer_slot(t, n, k)];
+        int r = o;
+        if (o >= 0) {
+            int fw = S.fwd[o];
+            if (fw >= 0) r = fw;
         }
+        S.res[4 * f + k] = r;
     }
-    S.lock[t] = LOCK_FREE;
+}
+
+// Phase C2: write the links in both directions, clear the FINAL marks and
+// queue the outer edges for the next round.
+template <class Append>
+HD void flip_relink(Flip& S, int f, Append append_next) {
+    int t = S.flips[2 * f], n = S.flips[2 * f + 1];
+    for (int k = 0; k < 4; ++k) {
+        int x = outer_slot(t, n, k);
+        int r = S.res[4 * f + k];
+        S.opp[x] = r;
+        if (r >= 0) S.opp[r] = x;
+        append_next(x);
+    }
+    S.opp[3 * t + 2] &= ~FINAL;
+    S.opp[3 * n + 2] &= ~FINAL;
 }
 
 // Rotate a triangle so its smallest vertex index comes first.

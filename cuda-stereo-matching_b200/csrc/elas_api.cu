@@ -26,7 +26,6 @@ struct elas_handle {
     elas_params params;
     int device = 0;
     int num_sms = 0;
-    int flip_blocks = 0;
     std::string last_error;
     int64_t launches = 0;
 
@@ -171,14 +170,19 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         D.rcnt = (int32_t*)take(rows * 4);
         D.ne = (int32_t*)take(rows * 4);
         D.soff = (int32_t*)take(rows * 4);
-        D.chain = (int32_t*)take(rows * 4);
-        D.stack = (int32_t*)take(rows * 4);
+        D.chain = (int32_t*)take(4 * rows * 4);
         D.tri = (int32_t*)take(3 * tmax * 4);
         D.opp = (int32_t*)take(3 * tmax * 4);
         D.lock = (uint32_t*)take(tmax * 4);
+        D.fround = (int32_t*)take(tmax * 4);
         D.fwd = (int32_t*)take(3 * tmax * 4);
-        D.cand = (int32_t*)take(2 * tmax * 4);
-        D.ctr = (int32_t*)take(8 * 4);
+        D.cand = (int32_t*)take(6 * tmax * 4);
+        D.flips = (int32_t*)take(tmax * 4);
+        D.res = (int32_t*)take(2 * tmax * 4);
+        D.fwdl = (int32_t*)take(2 * tmax * 4);
+        D.wl0 = (int32_t*)take(6 * tmax * 4);
+        D.wl1 = (int32_t*)take(6 * tmax * 4);
+        D.ctr = (int32_t*)take(16 * 4);
         D.hkey = (unsigned long long*)take(hmax * 8);
         D.hcnt = (int32_t*)take(hmax * 4);
         D.hval = (int32_t*)take(2 * hmax * 4);
@@ -263,7 +267,7 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     CK(launch_grid(h->can, h->gtmp0, h->gtmp1, h->grid0, h->grid1, g, st));
     n += 2;
     CK(mark(ELAS_TIME_DELAUNAY));
-    CK(launch_delaunay(h->del[0], h->del[1], h->row_off, g.ch, h->num_sms, h->flip_blocks, h->err, st, &n));
+    CK(launch_delaunay(h->del[0], h->del[1], h->row_off, g.ch, g.cw * g.ch, h->num_sms, h->err, st, &n));
     CK(mark(ELAS_TIME_PRIOR));
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
                     h->prior0, h->prior1, g, h->num_sms, st));
@@ -393,7 +397,6 @@ int elas_b200_create(const elas_params* params, int device, elas_handle** out) {
     h->params = p;
     h->device = device;
     h->num_sms = prop.multiProcessorCount;
-    h->flip_blocks = flip_blocks_for(h->num_sms);
     *out = h;
     return ELAS_OK;
 }

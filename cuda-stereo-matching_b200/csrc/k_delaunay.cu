@@ -5,13 +5,10 @@
 //
 // Both views run as two independent problems inside the same launches:
 // problem 0 triangulates (u, v), problem 1 triangulates (u - d, v).
-#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include "common.cuh"
 #include "delaunay_core.h"
 #include "kernels.h"
-
-namespace cg = cooperative_groups;
 
 namespace elas {
 
@@ -20,8 +17,39 @@ using namespace del;
 namespace {
 
 constexpr int SORT_CAP = 2048;   // max candidates per lattice row
+constexpr int FLIP_THREADS = 1024;
 
 __device__ __forceinline__ void set_err(unsigned* err, unsigned f) { atomicOr(err, f); }
+
+// Exclusive scan of one int per thread over a 1024-thread block; *total
+// receives the sum.  `warp_sums` has 32 entries.
+__device__ int block_scan(int v, int* warp_sums, int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < (blockDim.x >> 5) ? warp_sums[lane] : 0;
+        int ws = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, ws, o);
+            if (lane >= o) ws += y;
+        }
+        warp_sums[lane] = ws - w;
+        if (lane == 31) warp_sums[32] = ws;
+    }
+    __syncthreads();
+    int r = x - v + warp_sums[warp];
+    *total = warp_sums[32];
+    __syncthreads();
+    return r;
+}
 
 // Per lattice row: sort the row's points by (x, index), drop repeated x
 // (keeps the lowest index), write the unique list to srt[row_off[r] ..] and
@@ -29,7 +57,7 @@ __device__ __forceinline__ void set_err(unsigned* err, unsigned f) { atomicOr(er
 __global__ void __launch_bounds__(512) k_rowsort(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off,
                                                  int nrows, unsigned* err) {
     __shared__ unsigned long long key[SORT_CAP];
-    __shared__ int keep_scan[SORT_CAP];
+    __shared__ int keep[SORT_CAP];
     const DelDev& D = blockIdx.y ? d1 : d0;
     const int r = blockIdx.x;
     if (r >= nrows) return;
@@ -56,55 +84,125 @@ __global__ void __launch_bounds__(512) k_rowsort(DelDev d0, DelDev d1, const int
             __syncthreads();
         }
     for (int i = threadIdx.x; i < n; i += blockDim.x)
-        keep_scan[i] = (i == 0 || (key[i] >> 32) != (key[i - 1] >> 32)) ? 1 : 0;
+        keep[i] = (i == 0 || (key[i] >> 32) != (key[i - 1] >> 32)) ? 1 : 0;
     __syncthreads();
-    if (threadIdx.x == 0) {   // n <= 2048: serial compaction is short
-        int m = 0;
-        for (int i = 0; i < n; ++i)
-            if (keep_scan[i]) D.srt[b + m++] = int32_t(key[i] & 0xffffffffu);
-        D.rcnt[r] = m;
+    // compaction: each warp counts its span, warp 0 turns the counts into offsets
+    __shared__ int wcnt[17];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int span = (n + nw - 1) / nw;
+    int c = 0;
+    for (int i = warp * span + lane; i < min(n, (warp + 1) * span); i += 32) c += keep[i];
+    c = __reduce_add_sync(0xffffffffu, c);
+    if (lane == 0) wcnt[warp] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int w = 0; w < nw; ++w) { int t = wcnt[w]; wcnt[w] = run; run += t; }
+        wcnt[16] = run;
+        D.rcnt[r] = run;
+    }
+    __syncthreads();
+    int base = wcnt[warp];
+    for (int i0 = warp * span; i0 < min(n, (warp + 1) * span); i0 += 32) {
+        int i = i0 + lane;
+        bool k = i < min(n, (warp + 1) * span) && keep[i];
+        unsigned m = __ballot_sync(0xffffffffu, k);
+        if (k) D.srt[b + base + __popc(m & ((1u << lane) - 1))] = int32_t(key[i] & 0xffffffffu);
+        base += __popc(m);
     }
 }
 
-// Non-empty rows, strip offsets and the two hull pockets (one thread per
-// problem; the chains are one point per lattice row).
-__global__ void k_plan(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off, int nrows, unsigned* err) {
-    if (threadIdx.x != 0) return;
+// Non-empty rows (list + rank), strip offsets and the two hull pockets.
+// One 1024-thread block per problem; dynamic shared memory holds the chain
+// (index, x, y) and the stack of the pocket walk when it fits.
+__global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off,
+                                               int nrows, int smem_rows, unsigned* err) {
+    extern __shared__ int32_t sh[];
+    __shared__ int ws[33];
     DelDev D = blockIdx.x ? d1 : d0;
-    int R = 0;
-    for (int r = 0; r < nrows; ++r)
-        if (D.rcnt[r] > 0) D.ne[R++] = r;
+    int R = 0, total = 0;
+    // non-empty rows in order, and each row's rank
+    for (int r0 = 0; r0 < nrows; r0 += blockDim.x) {
+        int r = r0 + threadIdx.x;
+        int f = (r < nrows && D.rcnt[r] > 0) ? 1 : 0;
+        int pos = block_scan(f, ws, &total);
+        if (f) D.ne[R + pos] = r;
+        R += total;
+    }
+    __syncthreads();
+    // strip s between ne[s] and ne[s+1] holds rcnt[ne[s]] + rcnt[ne[s+1]] - 2 triangles
     int off = 0;
-    for (int s = 0; s + 1 < R; ++s) {
-        D.soff[s] = off;
-        off += D.rcnt[D.ne[s]] + D.rcnt[D.ne[s + 1]] - 2;
+    for (int s0 = 0; s0 < R - 1; s0 += blockDim.x) {
+        int s = s0 + threadIdx.x;
+        int c = s < R - 1 ? D.rcnt[D.ne[s]] + D.rcnt[D.ne[s + 1]] - 2 : 0;
+        int pos = block_scan(c, ws, &total);
+        if (s < R - 1) D.soff[s] = off + pos;
+        off += total;
     }
-    D.ctr[1] = off;
-    D.ctr[6] = R;
-    if (R >= 2 && off + 2 * R <= D.Tmax) {
-        Pts P{D.x, D.y};
-        for (int s = 0; s < R; ++s) D.chain[s] = D.srt[row_off[D.ne[s]]];
-        off += fill_pockets(P, D.chain, R, +1, D.stack, D.tri + 3 * size_t(off));
-        for (int s = 0; s < R; ++s) D.chain[s] = D.srt[row_off[D.ne[s]] + D.rcnt[D.ne[s]] - 1];
-        off += fill_pockets(P, D.chain, R, -1, D.stack, D.tri + 3 * size_t(off));
+    const bool in_smem = R <= smem_rows;
+    int32_t* ci = in_smem ? sh : D.chain;
+    int32_t* cx = ci + (in_smem ? smem_rows : nrows);
+    int32_t* cy = cx + (in_smem ? smem_rows : nrows);
+    int32_t* stk = cy + (in_smem ? smem_rows : nrows);
+    int pockets = 0;
+    if (R >= 2 && off + 2 * R > D.Tmax) {
+        if (threadIdx.x == 0) set_err(err, ERRF_TRI_COUNT);
     } else if (R >= 2) {
-        set_err(err, ERRF_TRI_COUNT);
-        off = 0;
+        for (int side = 0; side < 2; ++side) {
+            for (int s = threadIdx.x; s < R; s += blockDim.x) {
+                int r = D.ne[s];
+                int i = D.srt[row_off[r] + (side ? D.rcnt[r] - 1 : 0)];
+                ci[s] = i; cx[s] = D.x[i]; cy[s] = D.y[i];
+            }
+            __syncthreads();
+            if (threadIdx.x == 0)
+                pockets += fill_pockets(ci, cx, cy, R, side ? -1 : +1, stk, D.tri + 3 * size_t(off + pockets));
+            __syncthreads();
+        }
     }
-    D.ctr[0] = off;
-    D.ctr[2] = 0;
-    D.ctr[3] = 0;
+    if (threadIdx.x == 0) {
+        D.ctr[0] = (R >= 2 && off + 2 * R <= D.Tmax) ? off + pockets : 0;
+        D.ctr[1] = off;
+        D.ctr[6] = R;
+    }
 }
 
-// One thread per strip: zipper between consecutive non-empty rows.
-__global__ void k_strips(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off, int max_strips) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+// One thread per sorted point of a non-empty row: the point's triangle in
+// the strip below its row (as the upper row) and in the strip above (as the
+// lower row), placed by merge path.
+__global__ void k_strips(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off, int nmax) {
     const DelDev& D = blockIdx.y ? d1 : d0;
-    int R = D.ctr[6];
-    if (i >= max_strips || i + 1 >= R) return;
-    int ra = D.ne[i], rb = D.ne[i + 1];
+    const int R = D.ctr[6];
+    if (D.ctr[0] == 0) return;
     Pts P{D.x, D.y};
-    zipper(P, D.srt + row_off[ra], D.rcnt[ra], D.srt + row_off[rb], D.rcnt[rb], D.tri + 3 * size_t(D.soff[i]));
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nmax; g += gridDim.x * blockDim.x) {
+        // g walks the support index space; map it to (row, position) through the row offsets
+        int lo = 0, hi = R;    // find the non-empty row whose range holds g
+        // rows are in support-index order, so binary search ne by row_off
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (row_off[D.ne[mid] + 1] <= g) lo = mid + 1;
+            else hi = mid;
+        }
+        if (lo >= R) continue;
+        int r = D.ne[lo];
+        int k = g - row_off[r];
+        if (k < 1 || k >= D.rcnt[r]) continue;
+        const int32_t* A_row = D.srt + row_off[r];
+        int32_t tri[3];
+        if (lo + 1 < R) {       // as the upper row of strip lo
+            int rb = D.ne[lo + 1];
+            int pos = strip_tri_upper(P, A_row, D.srt + row_off[rb], D.rcnt[rb], k, tri);
+            int32_t* o = D.tri + 3 * size_t(D.soff[lo] + pos);
+            o[0] = tri[0]; o[1] = tri[1]; o[2] = tri[2];
+        }
+        if (lo >= 1) {          // as the lower row of strip lo-1
+            int ra = D.ne[lo - 1];
+            int pos = strip_tri_lower(P, D.srt + row_off[ra], D.rcnt[ra], A_row, k, tri);
+            int32_t* o = D.tri + 3 * size_t(D.soff[lo - 1] + pos);
+            o[0] = tri[0]; o[1] = tri[1]; o[2] = tri[2];
+        }
+    }
 }
 
 __device__ __forceinline__ uint32_t hash_cap(int T) {
@@ -149,6 +247,7 @@ __global__ void k_hash_insert(DelDev d0, DelDev d1, unsigned* err) {
     }
 }
 
+// Neighbour links from the hash, and the per-triangle flip state.
 __global__ void k_link(DelDev d0, DelDev d1, unsigned* err) {
     const DelDev& D = blockIdx.y ? d1 : d0;
     const int T = D.ctr[0];
@@ -161,66 +260,102 @@ __global__ void k_link(DelDev d0, DelDev d1, unsigned* err) {
         else if (c != 1) set_err(err, ERRF_HASH);
         if (o >= 3 * T) { set_err(err, ERRF_BOUNDS); o = -1; }
         D.opp[h] = o;
+        D.fwd[h] = -1;
     }
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x)
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
         D.lock[t] = LOCK_FREE;
+        D.fround[t] = -1;
+    }
 }
 
-struct AMin {
+struct SAMin {
     __device__ void operator()(uint32_t* p, uint32_t v) const { atomicMin(p, v); }
 };
-struct AAdd {
-    __device__ int operator()(int32_t* p, int v) const { return atomicAdd(p, v); }
-};
 
-// Parallel Lawson flipping, all rounds in one cooperative launch.  Every
-// loop is bounded: `max_rounds` rounds at most, after which ERRF_FLIP_LIMIT
-// is raised and the kernel returns.
-__global__ void k_flip(DelDev d0, DelDev d1, int max_rounds, unsigned* err) {
-    cg::grid_group grid = cg::this_grid();
-    const int T0 = d0.ctr[0], T1 = d1.ctr[0];
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int gstride = gridDim.x * blockDim.x;
-    Tri S0{Pts{d0.x, d0.y}, d0.tri, d0.opp, d0.lock, d0.fwd, d0.cand, d0.ctr, d0.Tmax};
-    Tri S1{Pts{d1.x, d1.y}, d1.tri, d1.opp, d1.lock, d1.fwd, d1.cand, d1.ctr, d1.Tmax};
-    bool converged = false;
+// Worklist-driven Lawson flipping, one 1024-thread CTA per problem, every
+// phase separated by __syncthreads.  At most `max_rounds` rounds; hitting the
+// limit raises ERRF_FLIP_LIMIT.
+__global__ void __launch_bounds__(FLIP_THREADS) k_flip(DelDev d0, DelDev d1, int max_rounds, unsigned* err) {
+    __shared__ int n_cand, n_flip, n_fwd, n_next, n_cur, stop, prev_fwd;
+    const DelDev& D = blockIdx.x ? d1 : d0;
+    const int T = D.ctr[0];
+    Flip S{Pts{D.x, D.y}, D.tri, D.opp, D.lock, D.fround, D.fwd, D.cand, D.flips, D.res, D.fwdl,
+           {D.wl0, D.wl1}, D.Tmax};
+    const int cand_cap = 3 * D.Tmax, wl_cap = 6 * D.Tmax;
+    const int tid = threadIdx.x;
+    if (tid == 0) { n_cur = 3 * T; n_fwd = 0; prev_fwd = 0; stop = 0; }
+    __syncthreads();
     int round = 0;
+    int flips_total = 0;
     for (; round < max_rounds; ++round) {
-        for (int i = gtid; i < T0 + T1; i += gstride) {
-            bool ok = i < T0 ? flip_propose(S0, i, T0, round, AMin(), AAdd())
-                             : flip_propose(S1, i - T0, T1, round, AMin(), AAdd());
+        int32_t* cur = S.wl[round & 1];
+        int32_t* nxt = S.wl[(round + 1) & 1];
+        if (tid == 0) { n_cand = 0; n_next = 0; }
+        // clear the forwarding entries of the previous round
+        for (int k = tid; k < prev_fwd; k += FLIP_THREADS) S.fwd[S.fwdl[k]] = -1;
+        __syncthreads();
+        // A: propose
+        const int items = n_cur;
+        for (int k = tid; k < items; k += FLIP_THREADS) {
+            int h = round == 0 ? k : cur[k];
+            bool ok = flip_propose(S, h, T, uint32_t(round), round == 0, SAMin(), [&](int hh, int nn) {
+                int idx = atomicAdd(&n_cand, 1);
+                if (idx < cand_cap) { S.cand[2 * idx] = hh; S.cand[2 * idx + 1] = nn; }
+            });
             if (!ok) set_err(err, ERRF_BOUNDS);
         }
-        grid.sync();
-        const int n0 = imin(((volatile int32_t*)d0.ctr)[2 + (round & 1)], 2 * d0.Tmax);
-        const int n1 = imin(((volatile int32_t*)d1.ctr)[2 + (round & 1)], 2 * d1.Tmax);
-        if (n0 + n1 == 0) { converged = true; break; }
-        for (int i = gtid; i < n0 + n1; i += gstride) {
-            if (i < n0) flip_apply(S0, d0.cand[i], round);
-            else flip_apply(S1, d1.cand[i - n0], round);
-        }
-        grid.sync();
-        for (int i = gtid; i < T0 + T1; i += gstride) {
-            Tri& S = i < T0 ? S0 : S1;
-            int t = i < T0 ? i : i - T0;
-            int T = i < T0 ? T0 : T1;
-            // validate links before the forwarding lookup
-            for (int s = 0; s < 3; ++s) {
-                int o = S.opp[3 * t + s];
-                if (o >= 0 && (o & ~FINAL) >= 3 * T) { set_err(err, ERRF_BOUNDS); S.opp[3 * t + s] = -1; }
+        __syncthreads();
+        const int nc = n_cand;
+        if (nc > cand_cap) { if (tid == 0) { set_err(err, ERRF_BOUNDS); stop = 1; } }
+        if (tid == 0) { n_flip = 0; n_fwd = 0; }
+        __syncthreads();
+        if (nc == 0 || stop) break;
+        // B: flip the winners
+        for (int c = tid; c < nc; c += FLIP_THREADS) {
+            int slots[4];
+            if (flip_apply(S, S.cand[2 * c], S.cand[2 * c + 1], uint32_t(round), slots)) {
+                int f = atomicAdd(&n_flip, 1);
+                int h = S.cand[2 * c];
+                S.flips[2 * f] = h / 3;
+                S.flips[2 * f + 1] = S.cand[2 * c + 1];
+                int q = atomicAdd(&n_fwd, 4);
+                for (int k = 0; k < 4; ++k) S.fwdl[q + k] = slots[k];
             }
-            flip_repair(S, t);
         }
-        if (gtid == 0) {
-            d0.ctr[2 + ((round + 1) & 1)] = 0;
-            d1.ctr[2 + ((round + 1) & 1)] = 0;
+        __syncthreads();
+        const int nf = n_flip;
+        // C1: resolve the outer neighbours (read only)
+        for (int f = tid; f < nf; f += FLIP_THREADS) flip_resolve(S, f);
+        __syncthreads();
+        // C2: relink, queue the outer edges, release locks, requeue lost proposals
+        for (int f = tid; f < nf; f += FLIP_THREADS)
+            flip_relink(S, f, [&](int x) {
+                int idx = atomicAdd(&n_next, 1);
+                if (idx < wl_cap) nxt[idx] = x;
+            });
+        for (int c = tid; c < nc; c += FLIP_THREADS) {
+            int h = S.cand[2 * c], n = S.cand[2 * c + 1], t = h / 3;
+            S.lock[t] = LOCK_FREE;
+            S.lock[n] = LOCK_FREE;
+            if (S.fround[t] != round && S.fround[n] != round) {
+                int idx = atomicAdd(&n_next, 1);
+                if (idx < wl_cap) nxt[idx] = h;
+            }
         }
-        grid.sync();
+        flips_total += nf;
+        __syncthreads();
+        if (tid == 0) {
+            if (n_next > wl_cap) { set_err(err, ERRF_BOUNDS); stop = 1; }
+            n_cur = min(n_next, wl_cap);
+            prev_fwd = n_fwd;
+        }
+        __syncthreads();
+        if (stop) break;
     }
-    if (gtid == 0) {
-        d0.ctr[4] = round + 1;
-        d1.ctr[4] = round + 1;
-        if (!converged) set_err(err, ERRF_FLIP_LIMIT);
+    if (tid == 0) {
+        D.ctr[4] = round + 1;
+        D.ctr[5] = flips_total;
+        if (round >= max_rounds) set_err(err, ERRF_FLIP_LIMIT);
     }
 }
 
@@ -233,29 +368,22 @@ __global__ void k_normalise(DelDev d0, DelDev d1) {
 
 }  // namespace
 
-cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int num_sms,
-                            int flip_blocks, unsigned* err, cudaStream_t st, int* nlaunch) {
+cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int nmax, int num_sms,
+                            unsigned* err, cudaStream_t st, int* nlaunch) {
     k_rowsort<<<dim3(nrows, 2), 512, 0, st>>>(d0, d1, row_off, nrows, err);
-    k_plan<<<2, 32, 0, st>>>(d0, d1, row_off, nrows, err);
-    k_strips<<<dim3((nrows + 127) / 128, 2), 128, 0, st>>>(d0, d1, row_off, nrows);
+    int smem_rows = imin(nrows, (96 * 1024) / 16);
+    size_t smem = size_t(smem_rows) * 16;
+    cudaFuncSetAttribute(k_plan, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    k_plan<<<2, 1024, smem, st>>>(d0, d1, row_off, nrows, smem_rows, err);
     int blocks = 4 * num_sms;
+    k_strips<<<dim3(imax(1, imin(blocks, (nmax + 255) / 256)), 2), 256, 0, st>>>(d0, d1, row_off, nmax);
     k_hash_clear<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1);
     k_hash_insert<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1, err);
     k_link<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1, err);
-    int max_rounds = 4096;
-    void* args[] = {&d0, &d1, &max_rounds, &err};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_flip, dim3(flip_blocks), dim3(256), args, 0, st);
-    if (e != cudaSuccess) return e;
+    k_flip<<<2, FLIP_THREADS, 0, st>>>(d0, d1, 100000, err);
     k_normalise<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1);
     if (nlaunch) *nlaunch += 8;
     return cudaGetLastError();
-}
-
-int flip_blocks_for(int num_sms) {
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flip, 256, 0);
-    if (per_sm < 1) per_sm = 1;
-    return per_sm * num_sms;
 }
 
 }  // namespace elas

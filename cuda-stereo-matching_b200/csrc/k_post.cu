@@ -87,25 +87,24 @@ __global__ void k_uf_union(const float* __restrict__ D, int32_t* lab, int W, int
     }
 }
 
-// Flatten every label to its root and count segment sizes; lanes of a warp
-// that share a root add once (segments are large, so this removes most of
-// the contention on the root counters).
-__global__ void k_uf_count(int32_t* lab, int32_t* sz, int n, unsigned* err) {
+// Root of every pixel into `root` (written only by its own thread: `lab`
+// itself may still receive path-halving writes from other threads) and
+// segment sizes; lanes of a warp that share a root add once (segments are
+// large, so this removes most of the contention on the root counters).
+__global__ void k_uf_count(int32_t* lab, int32_t* __restrict__ root, int32_t* sz, int n, unsigned* err) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int r = -1;
-    if (i < n && lab[i] >= 0) {
-        r = uf_find(lab, i, err);
-        lab[i] = r;
-    }
+    if (i < n && lab[i] >= 0) r = uf_find(lab, i, err);
+    if (i < n) root[i] = r;
     unsigned peers = __match_any_sync(0xffffffffu, r);
     int leader = __ffs(peers) - 1;
     if (r >= 0 && (threadIdx.x & 31) == leader) atomicAdd(&sz[r], __popc(peers));
 }
 
-__global__ void k_uf_apply(float* D, const int32_t* lab, const int32_t* sz, int n, int min_size) {
+__global__ void k_uf_apply(float* D, const int32_t* __restrict__ root, const int32_t* sz, int n, int min_size) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    int r = lab[i];
+    int r = root[i];
     if (r >= 0 && sz[r] < min_size) D[i] = -1.0f;
 }
 
@@ -217,8 +216,9 @@ cudaError_t launch_post(float* disp, float* tmp, int32_t* lab, int32_t* size, co
     if (p.speckle_size > 0) {
         k_uf_init<<<grid2, tb, 0, st>>>(disp, lab, size, W, H, p.speckle_sim_threshold);
         k_uf_union<<<grid2, tb, 0, st>>>(disp, lab, W, H, p.speckle_sim_threshold, err);
-        k_uf_count<<<(n + tb - 1) / tb, tb, 0, st>>>(lab, size, n, err);
-        k_uf_apply<<<(n + tb - 1) / tb, tb, 0, st>>>(disp, lab, size, n, p.speckle_size);
+        int32_t* root = reinterpret_cast<int32_t*>(tmp);   // tmp is free during speckle removal
+        k_uf_count<<<(n + tb - 1) / tb, tb, 0, st>>>(lab, root, size, n, err);
+        k_uf_apply<<<(n + tb - 1) / tb, tb, 0, st>>>(disp, root, size, n, p.speckle_size);
         launched += 4;
     }
     if (p.ipol_gap_width > 0) {

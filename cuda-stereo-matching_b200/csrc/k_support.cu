@@ -187,26 +187,41 @@ __global__ void k_incon(const int32_t* __restrict__ cin, int32_t* __restrict__ c
     cout[size_t(y) * g.cw + x] = out;
 }
 
-// Redundancy filter along one line held in shared memory (serial, in place,
-// exactly the reference's per-line order).
-__device__ void redundant_line(int* a, int len) {
-    for (int k = 0; k < len; ++k) {
+// Redundancy filter along one line (removeRedundantSupportPoints*,
+// KerSupportMatches.cu:241-357): point k is removed when it has a similar
+// (|d - d2| <= 1) valid point within 5 cells on BOTH sides, the left side
+// seen after the removals already made on this line, the right side as it
+// was.  The lanes precompute, per point, "valid", "right support" and the
+// 5-bit mask of similar valid points on the left; the serial part then only
+// carries the 5-bit history of removals.
+__device__ void redundant_line(int* a, uint8_t* code, int len, int lane) {
+    for (int k = lane; k < len; k += 32) {
         int d = a[k];
-        if (d < 0) continue;
-        bool redundant = true;
-        for (int dir = -1; dir <= 1 && redundant; dir += 2) {
-            bool support = false;
-            int k2 = k;
-            for (int j = 0; j < 5; ++j) {
-                k2 += dir;
-                if (k2 < 0 || k2 >= len) break;
-                int d2 = a[k2];
-                if (d2 >= 0 && abs(d - d2) <= 1) { support = true; break; }
+        int c = 0;
+        if (d >= 0) {
+            c = 1;
+            for (int j = 1; j <= 5 && k + j < len; ++j) {
+                int d2 = a[k + j];
+                if (d2 >= 0 && abs(d - d2) <= 1) { c |= 2; break; }
             }
-            if (!support) redundant = false;
+            for (int b = 0; b < 5 && k - 1 - b >= 0; ++b) {
+                int d2 = a[k - 1 - b];
+                if (d2 >= 0 && abs(d - d2) <= 1) c |= 4 << b;
+            }
         }
-        if (redundant) a[k] = -1;
+        code[k] = uint8_t(c);
     }
+    __syncwarp();
+    if (lane == 0) {
+        unsigned hist = 0;   // bit b: point k-1-b was removed
+        for (int k = 0; k < len; ++k) {
+            unsigned c = code[k];
+            unsigned rem = (c & 1u) && (c & 2u) && ((c >> 2) & ~hist & 31u) ? 1u : 0u;
+            hist = ((hist << 1) | rem) & 31u;
+            if (rem) a[k] = -1;
+        }
+    }
+    __syncwarp();
 }
 
 // One warp per line; horizontal = 1: rows, 0: columns.
@@ -218,11 +233,11 @@ __global__ void k_redundant(int32_t* __restrict__ can, Geom g, int horizontal) {
     int l = blockIdx.x * (blockDim.x >> 5) + warp;
     if (l >= nlines) return;
     int* a = lines + warp * len;
+    uint8_t* code = reinterpret_cast<uint8_t*>(lines + (blockDim.x >> 5) * len) + warp * len;
     for (int k = lane; k < len; k += 32)
         a[k] = horizontal ? can[size_t(l) * g.cw + k] : can[size_t(k) * g.cw + l];
     __syncwarp();
-    if (lane == 0) redundant_line(a, len);
-    __syncwarp();
+    redundant_line(a, code, len, lane);
     for (int k = lane; k < len; k += 32) {
         if (horizontal) can[size_t(l) * g.cw + k] = a[k];
         else can[size_t(k) * g.cw + l] = a[k];
@@ -352,9 +367,9 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
     k_incon<<<dim3((g.cw + 127) / 128, g.ch), 128, 0, st>>>(can_lr, can, g, p);
     {
         int wpb = 4;
-        size_t sm = size_t(wpb) * g.cw * sizeof(int);
+        size_t sm = size_t(wpb) * g.cw * (sizeof(int) + 1);
         k_redundant<<<(g.ch + wpb - 1) / wpb, 32 * wpb, sm, st>>>(can, g, 1);
-        sm = size_t(wpb) * g.ch * sizeof(int);
+        sm = size_t(wpb) * g.ch * (sizeof(int) + 1);
         k_redundant<<<(g.cw + wpb - 1) / wpb, 32 * wpb, sm, st>>>(can, g, 0);
     }
     (void)can_tmp;

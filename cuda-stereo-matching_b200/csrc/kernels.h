@@ -15,14 +15,19 @@ struct DelDev {
     int32_t* rcnt;         // [rows] unique points per row
     int32_t* ne;           // [rows] non-empty rows
     int32_t* soff;         // [rows] strip triangle offsets
-    int32_t* chain;        // [rows]
-    int32_t* stack;        // [rows]
+    int32_t* chain;        // [4*rows] pocket walk scratch when it does not fit in shared memory
     int32_t* tri;          // [3*Tmax]
     int32_t* opp;          // [3*Tmax]
     uint32_t* lock;        // [Tmax]
+    int32_t* fround;       // [Tmax]
     int32_t* fwd;          // [3*Tmax]
-    int32_t* cand;         // [2*Tmax]
-    int32_t* ctr;          // [8]
+    int32_t* cand;         // [6*Tmax]
+    int32_t* flips;        // [Tmax]
+    int32_t* res;          // [2*Tmax]
+    int32_t* fwdl;         // [2*Tmax]
+    int32_t* wl0;          // [6*Tmax]
+    int32_t* wl1;          // [6*Tmax]
+    int32_t* ctr;          // [16]: 0 triangles, 1 strip triangles, 4 flip rounds, 5 flips, 6 non-empty rows
     unsigned long long* hkey;  // [Hmax]
     int32_t* hcnt;         // [Hmax]
     int32_t* hval;         // [2*Hmax]
@@ -43,9 +48,8 @@ cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_of
 cudaError_t launch_grid(const int32_t* can, uint32_t* tmp0, uint32_t* tmp1, uint32_t* grid0, uint32_t* grid1,
                         const Geom& g, cudaStream_t st);
 
-cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int num_sms,
-                            int flip_blocks, unsigned* err, cudaStream_t st, int* nlaunch);
-int flip_blocks_for(int num_sms);
+cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int nmax, int num_sms,
+                            unsigned* err, cudaStream_t st, int* nlaunch);
 
 // Plane prior of both views: prior[v*W+u] = (triangle+1) << 32 | uint32(d_plane),
 // 0 where no triangle covers the pixel.  Buffers must be zeroed first.

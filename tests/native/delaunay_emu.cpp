@@ -1,8 +1,8 @@
-// Test helper: sequential host emulation of the CUDA Delaunay pipeline.
-// Every data-parallel phase of the device code runs here as a loop over its
-// items, calling the same __host__ __device__ functions
-// (cuda-stereo-matching_b200/csrc/delaunay_core.h), so the algorithm can be
-// checked on the CPU against the exact checker and Triangle.
+// Test helper: sequential host emulation of the CUDA Delaunay pipeline
+// (cuda-stereo-matching_b200/csrc/k_delaunay.cu).  Every data-parallel
+// phase of the device code runs here as a loop over its items and calls the
+// same __host__ __device__ functions (delaunay_core.h), so the algorithm can
+// be checked on the CPU against the exact checker and Triangle.
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
@@ -13,79 +13,128 @@
 
 using namespace elas::del;
 
-// px, py: n points; row_off: nrows+1 offsets of points per lattice row
-// (points of a row share y).  tris_out: capacity cap triangles.  Returns the
-// triangle count, or -1 on an internal error.  stats (nullable):
-// [0] rounds, [1] flips.
-extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const int32_t* row_off,
-                            int nrows, int32_t* tris_out, int cap, long long* stats) {
+// px, py: n points; row_off: nrows+1 offsets of the points of each lattice
+// row (points of a row share y).  tris_out: room for cap triangles.  Returns
+// the triangle count, or -1 on an internal error.  stats (nullable):
+// [0] flip rounds, [1] flips.
+extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const int32_t* row_off, int nrows,
+                            int32_t* tris_out, int cap, long long* stats) {
     Pts P{px, py};
-    // 1. per-row sort + dedup
-    std::vector<std::vector<int32_t>> rows(nrows);
+    // 1. per-row sort + dedup (k_rowsort)
+    std::vector<int32_t> srt(std::max(n, 1)), rcnt(nrows, 0);
     for (int r = 0; r < nrows; ++r) {
         std::vector<int32_t> v;
         for (int i = row_off[r]; i < row_off[r + 1]; ++i) v.push_back(i);
-        std::sort(v.begin(), v.end(), [&](int a, int b) {
-            return px[a] != px[b] ? px[a] < px[b] : a < b;
-        });
+        std::sort(v.begin(), v.end(), [&](int a, int b) { return px[a] != px[b] ? px[a] < px[b] : a < b; });
+        int m = 0;
         for (size_t k = 0; k < v.size(); ++k)
-            if (k == 0 || px[v[k]] != px[v[k - 1]]) rows[r].push_back(v[k]);
+            if (k == 0 || px[v[k]] != px[v[k - 1]]) srt[row_off[r] + m++] = v[k];
+        rcnt[r] = m;
     }
-    std::vector<int> ne;
+    // 2. plan (k_plan)
+    std::vector<int> ne, soff;
     for (int r = 0; r < nrows; ++r)
-        if (!rows[r].empty()) ne.push_back(r);
-    int Tmax = 2 * n + 8;
-    std::vector<int32_t> tri(3 * size_t(Tmax)), opp(3 * size_t(Tmax)), fwd(3 * size_t(Tmax), -1),
-        cand(2 * size_t(Tmax));
-    std::vector<uint32_t> lock(Tmax, LOCK_FREE);
-    int32_t ctr[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (rcnt[r] > 0) ne.push_back(r);
+    const int R = int(ne.size());
+    int off = 0;
+    for (int s = 0; s + 1 < R; ++s) { soff.push_back(off); off += rcnt[ne[s]] + rcnt[ne[s + 1]] - 2; }
+    const int Tmax = 2 * n + 16;
+    std::vector<int32_t> tri(3 * size_t(Tmax), -1);
     int T = 0;
-    // 2. strips
-    for (size_t s = 0; s + 1 < ne.size(); ++s) {
-        auto& A = rows[ne[s]];
-        auto& B = rows[ne[s + 1]];
-        int cnt = int(A.size()) + int(B.size()) - 2;
-        if (T + cnt > Tmax) return -1;
-        zipper(P, A.data(), int(A.size()), B.data(), int(B.size()), &tri[3 * size_t(T)]);
-        T += cnt;
+    if (R >= 2) {
+        if (off + 2 * R > Tmax) return -1;
+        std::vector<int32_t> ci(R), cx(R), cy(R), stk(R);
+        int pockets = 0;
+        for (int side = 0; side < 2; ++side) {
+            for (int s = 0; s < R; ++s) {
+                int r = ne[s];
+                int i = srt[row_off[r] + (side ? rcnt[r] - 1 : 0)];
+                ci[s] = i; cx[s] = px[i]; cy[s] = py[i];
+            }
+            pockets += fill_pockets(ci.data(), cx.data(), cy.data(), R, side ? -1 : +1, stk.data(),
+                                    &tri[3 * size_t(off + pockets)]);
+        }
+        T = off + pockets;
+        // 3. strips (k_strips), every point of every non-empty row
+        for (int lo = 0; lo < R; ++lo) {
+            int r = ne[lo];
+            const int32_t* A = &srt[row_off[r]];
+            for (int k = 1; k < rcnt[r]; ++k) {
+                int32_t t3[3];
+                if (lo + 1 < R) {
+                    int rb = ne[lo + 1];
+                    int pos = strip_tri_upper(P, A, &srt[row_off[rb]], rcnt[rb], k, t3);
+                    std::memcpy(&tri[3 * size_t(soff[lo] + pos)], t3, 12);
+                }
+                if (lo >= 1) {
+                    int ra = ne[lo - 1];
+                    int pos = strip_tri_lower(P, &srt[row_off[ra]], rcnt[ra], A, k, t3);
+                    std::memcpy(&tri[3 * size_t(soff[lo - 1] + pos)], t3, 12);
+                }
+            }
+        }
     }
-    // 3. pockets
-    if (ne.size() >= 2) {
-        std::vector<int32_t> chain(ne.size()), stack(ne.size());
-        for (size_t s = 0; s < ne.size(); ++s) chain[s] = rows[ne[s]].front();
-        T += fill_pockets(P, chain.data(), int(chain.size()), +1, stack.data(), &tri[3 * size_t(T)]);
-        for (size_t s = 0; s < ne.size(); ++s) chain[s] = rows[ne[s]].back();
-        T += fill_pockets(P, chain.data(), int(chain.size()), -1, stack.data(), &tri[3 * size_t(T)]);
-    }
-    if (T > Tmax) return -1;
-    // 4. adjacency
+    for (int i = 0; i < 3 * T; ++i)
+        if (tri[i] < 0) return -1;   // a strip slot nobody wrote
+    // 4. adjacency (k_hash_insert + k_link)
+    std::vector<int32_t> opp(3 * size_t(Tmax), -1);
     std::unordered_map<uint64_t, std::vector<int>> edges;
     for (int h = 0; h < 3 * T; ++h) {
         int t = h / 3, s = h % 3;
         edges[edge_key(tri[3 * t + s], tri[3 * t + (s + 1) % 3])].push_back(h);
     }
     for (auto& kv : edges) {
-        if (kv.second.size() == 1) opp[kv.second[0]] = -1;
-        else if (kv.second.size() == 2) { opp[kv.second[0]] = kv.second[1]; opp[kv.second[1]] = kv.second[0]; }
-        else return -1;
+        if (kv.second.size() == 2) { opp[kv.second[0]] = kv.second[1]; opp[kv.second[1]] = kv.second[0]; }
+        else if (kv.second.size() != 1) return -1;
     }
-    // 5. flip rounds
-    Tri S{P, tri.data(), opp.data(), lock.data(), fwd.data(), cand.data(), ctr, Tmax};
+    // 5. flips (k_flip)
+    std::vector<uint32_t> lock(Tmax, LOCK_FREE);
+    std::vector<int32_t> fround(Tmax, -1), fwd(3 * size_t(Tmax), -1), cand(6 * size_t(Tmax)), flips(Tmax),
+        res(2 * size_t(Tmax)), fwdl(2 * size_t(Tmax)), wl0(6 * size_t(Tmax)), wl1(6 * size_t(Tmax));
+    Flip S{P, tri.data(), opp.data(), lock.data(), fround.data(), fwd.data(), cand.data(), flips.data(), res.data(),
+           fwdl.data(), {wl0.data(), wl1.data()}, Tmax};
     auto amin = [](uint32_t* p, uint32_t v) { if (v < *p) *p = v; };
-    auto aadd = [](int32_t* p, int v) { int o = *p; *p += v; return o; };
-    long long rounds = 0, flips = 0;
-    for (uint32_t round = 0; round < 100000; ++round) {
-        for (int t = 0; t < T; ++t)
-            if (!flip_propose(S, t, T, round, amin, aadd)) return -1;
-        int nc = ctr[2 + (round & 1)];
+    int n_cur = 3 * T, prev_fwd = 0;
+    long long rounds = 0, nflips = 0;
+    for (int round = 0; round < 100000; ++round) {
+        int32_t* cur = S.wl[round & 1];
+        int32_t* nxt = S.wl[(round + 1) & 1];
+        for (int k = 0; k < prev_fwd; ++k) fwd[fwdl[k]] = -1;
+        int nc = 0;
+        for (int k = 0; k < n_cur; ++k) {
+            int h = round == 0 ? k : cur[k];
+            if (!flip_propose(S, h, T, uint32_t(round), round == 0, amin, [&](int hh, int nn) {
+                    cand[2 * nc] = hh; cand[2 * nc + 1] = nn; ++nc;
+                }))
+                return -1;
+        }
         ++rounds;
         if (nc == 0) break;
-        for (int c = 0; c < nc; ++c) flips += flip_apply(S, cand[c], round) ? 1 : 0;
-        for (int t = 0; t < T; ++t) flip_repair(S, t);
-        ctr[2 + ((round + 1) & 1)] = 0;
+        int nf = 0, nfw = 0;
+        for (int c = 0; c < nc; ++c) {
+            int slots[4];
+            if (flip_apply(S, cand[2 * c], cand[2 * c + 1], uint32_t(round), slots)) {
+                flips[2 * nf] = cand[2 * c] / 3;
+                flips[2 * nf + 1] = cand[2 * c + 1];
+                ++nf;
+                for (int k = 0; k < 4; ++k) fwdl[nfw++] = slots[k];
+            }
+        }
+        for (int f = 0; f < nf; ++f) flip_resolve(S, f);
+        int nn = 0;
+        for (int f = 0; f < nf; ++f) flip_relink(S, f, [&](int x) { nxt[nn++] = x; });
+        for (int c = 0; c < nc; ++c) {
+            int h = cand[2 * c], m = cand[2 * c + 1], t = h / 3;
+            lock[t] = LOCK_FREE;
+            lock[m] = LOCK_FREE;
+            if (fround[t] != round && fround[m] != round) nxt[nn++] = h;
+        }
+        nflips += nf;
+        n_cur = nn;
+        prev_fwd = nfw;
     }
     for (int t = 0; t < T; ++t) normalise(&tri[3 * size_t(t)]);
     if (T <= cap) std::memcpy(tris_out, tri.data(), sizeof(int32_t) * 3 * size_t(T));
-    if (stats) { stats[0] = rounds; stats[1] = flips; }
+    if (stats) { stats[0] = rounds; stats[1] = nflips; }
     return T;
 }
