@@ -371,6 +371,7 @@ const char* elas_b200_status_string(int s) {
     case ELAS_ERR_INTERNAL: return "internal consistency check failed";
     case ELAS_ERR_NO_DEVICE: return "no usable sm_100 device";
     case ELAS_ERR_TIMEOUT: return "bounded device loop hit its limit";
+    case ELAS_ERR_TOO_LARGE: return "input exceeds the fixed scratch capacity of the allocation-free entry point";
     default: return "unknown status";
     }
 }

@@ -13,6 +13,8 @@
 //   mean      5x5 weighted mean of valid pixels, w = 1/(1+(d_q-d_p)^2).
 //   median    lower median of the valid pixels of the 3x3 window.
 #include <cuda_runtime.h>
+#include <mutex>
+#include "../../include/elas_b200.h"
 #include "common.cuh"
 #include "kernels.h"
 
@@ -245,4 +247,63 @@ cudaError_t launch_post(float* disp, float* tmp, int32_t* lab, int32_t* size, co
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free speckle removal (elas_b200_speckle_noalloc).
+//
+// For callers that must not allocate device memory -- code inside a CUDA
+// stream capture (cudaMalloc cannot be captured), plugin hosts and real-time
+// loops that forbid allocation after start-up.  Its scratch (labels, roots,
+// segment sizes and an error word) is this one file-scope array, resident on
+// every GPU that loads the library until the process exits.  In host code
+// the array's name is only a host-side stand-in, so its device address is
+// looked up once per device with cudaGetSymbolAddress (the first call on a
+// device, which should therefore happen outside any stream capture) and
+// cached.  Every call reuses the array; the kernels initialise all of it
+// that must start at zero, and calls that overlap on the GPU race.
+static __device__ __align__(256) int32_t g_noalloc_scratch[3 * ELAS_NOALLOC_MAX_PIXELS + 64];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+int32_t* g_noalloc_base[kNoallocMaxDevices] = {};
+std::mutex g_noalloc_mutex;
+}  // namespace
+
 }  // namespace elas
+
+extern "C" int elas_b200_speckle_noalloc(const float* d_in, float* d_out, int32_t width, int32_t height,
+                                         float sim_threshold, int32_t min_size, void* stream) {
+    using namespace elas;
+    if (!d_in || !d_out || width <= 0 || height <= 0 || min_size < 0) return ELAS_ERR_INVALID_ARG;
+    if (int64_t(width) * height > ELAS_NOALLOC_MAX_PIXELS) return ELAS_ERR_TOO_LARGE;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices) return ELAS_ERR_NO_DEVICE;
+    int32_t* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_base[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return ELAS_ERR_CUDA;
+            g_noalloc_base[dev] = static_cast<int32_t*>(p);
+        }
+        base = g_noalloc_base[dev];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int W = width, H = height, n = W * H, tb = 256;
+    int32_t* lab = base;
+    int32_t* root = base + ELAS_NOALLOC_MAX_PIXELS;
+    int32_t* sz = base + 2 * ELAS_NOALLOC_MAX_PIXELS;
+    unsigned* err = reinterpret_cast<unsigned*>(base + 3 * ELAS_NOALLOC_MAX_PIXELS);
+    if (d_out != d_in &&
+        cudaMemcpyAsync(d_out, d_in, size_t(n) * sizeof(float), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return ELAS_ERR_CUDA;
+    if (cudaMemsetAsync(err, 0, sizeof(unsigned), st) != cudaSuccess) return ELAS_ERR_CUDA;
+    if (min_size > 0) {
+        const dim3 grid2((W + tb - 1) / tb, H);
+        k_uf_init<<<grid2, tb, 0, st>>>(d_out, lab, sz, W, H, sim_threshold);
+        k_uf_union<<<grid2, tb, 0, st>>>(d_out, lab, W, H, sim_threshold, err);
+        k_uf_count<<<(n + tb - 1) / tb, tb, 0, st>>>(lab, root, sz, n, err);
+        k_uf_apply<<<(n + tb - 1) / tb, tb, 0, st>>>(d_out, root, sz, n, min_size);
+    }
+    return cudaGetLastError() == cudaSuccess ? ELAS_OK : ELAS_ERR_CUDA;
+}
+

@@ -17,7 +17,8 @@ LIB_PATH = os.path.join(HERE, "libelas_b200.so")
 
 ELAS_OK = 0
 STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported", 3: "CUDA error", 4: "out of memory",
-          5: "internal consistency check failed", 6: "no usable sm_100 device", 7: "bounded device loop hit its limit"}
+          5: "internal consistency check failed", 6: "no usable sm_100 device", 7: "bounded device loop hit its limit",
+          8: "input exceeds the fixed scratch capacity of the allocation-free entry point"}
 
 STAGES = {
     "desc_left": 0, "desc_right": 1, "can_lr": 2, "can": 3, "support": 4, "grid_left": 5, "grid_right": 6,

@@ -38,6 +38,7 @@ extern "C" {
 #define ELAS_ERR_INTERNAL       5  /* a device-side consistency check failed */
 #define ELAS_ERR_NO_DEVICE      6  /* no usable sm_100 device */
 #define ELAS_ERR_TIMEOUT        7  /* a bounded device loop hit its limit */
+#define ELAS_ERR_TOO_LARGE      8  /* input exceeds the fixed scratch of elas_b200_speckle_noalloc */
 
 /*
  * Parameter block.  Field order, types and meaning are those of
@@ -182,6 +183,39 @@ int elas_b200_set_timing(elas_handle* h, int enable);
 /* Wait for the last call and write its per-stage device times in ms
  * (ELAS_TIME_COUNT values) to ms_out. */
 int elas_b200_get_timing(elas_handle* h, float* ms_out, int n);
+
+/* ---- allocation-free speckle removal ---- */
+
+/* Largest image (width * height) elas_b200_speckle_noalloc accepts. */
+#define ELAS_NOALLOC_MAX_PIXELS (1 << 19)
+
+/*
+ * Speckle removal on one disparity map without any memory allocation, for
+ * callers that may not call cudaMalloc: code running while a stream is
+ * being captured into a CUDA graph (cudaMalloc is not capturable), plugin
+ * hosts and real-time loops that forbid allocation after start-up, and
+ * tools that must not touch the device allocator.  No counterpart in the
+ * reference, which has no post-filters.
+ *
+ *   d_in, d_out   : device float maps of width*height values (-1 = invalid);
+ *                   they may be the same buffer.
+ *   sim_threshold : neighbours with |d_p - d_q| <= sim_threshold connect.
+ *   min_size      : 4-connected segments smaller than this become -1.
+ *   stream        : cudaStream_t (NULL = legacy default stream); asynchronous.
+ * The result equals the speckle stage of elas_b200_process run with
+ * speckle_size = min_size and speckle_sim_threshold = sim_threshold.
+ *
+ * Scratch lives in one fixed array of 3 * ELAS_NOALLOC_MAX_PIXELS int32
+ * (6 MiB) in the library's device image; every GPU that loads the library
+ * holds it until the process exits.  width * height above
+ * ELAS_NOALLOC_MAX_PIXELS returns ELAS_ERR_TOO_LARGE.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress), so
+ * make that first call outside any stream capture.  All calls share the
+ * array: calls that overlap on the GPU (other streams, other threads) race
+ * and give wrong results; serialise them.
+ */
+int elas_b200_speckle_noalloc(const float* d_in, float* d_out, int32_t width, int32_t height,
+                              float sim_threshold, int32_t min_size, void* stream);
 
 /* ---- seeded synthetic stereo pairs (the benchmark inputs) ---- */
 
