@@ -162,103 +162,155 @@ constexpr int32_t FINAL = 1 << 30;          // opp entry already refers to the n
 constexpr uint32_t LOCK_FREE = 0xFFFFFFFFu;
 constexpr unsigned long long HASH_EMPTY = ~0ull;
 
-// Per-problem state of one triangulation during flipping.
-struct Flip {
-    Pts P;
-    int32_t* tri;       // [3*Tmax] vertex triples, counter-clockwise
-    int32_t* opp;       // [3*Tmax] neighbour half-edge (3*t+s) across edge (v_s, v_s+1), -1 = hull
-    uint32_t* lock;     // [Tmax]   minimum proposal priority on the triangle this round
-    int32_t* fround;    // [Tmax]   last round the triangle was flipped (-1 = never)
-    int32_t* fwd;       // [3*Tmax] old half-edge -> new half-edge, valid for one round
-    int32_t* cand;      // [2*3*Tmax] proposals of the round: (half-edge, neighbour triangle)
-    int32_t* flips;     // [Tmax]   flipped pairs of the round: (t, n)
-    int32_t* res;       // [2*Tmax] resolved outer neighbours of the flipped pairs (4 per pair)
-    int32_t* fwdl;      // [2*Tmax] forwarding entries written this round (to clear next round)
-    int32_t* wl[2];     // [6*Tmax] worklists of half-edges
-    int Tmax;
-};
+// Packed point coordinates, 16 bits each with a bias of 2^15 (coordinates
+// in [-32768, 32767]; the predicates are translation invariant): every
+// triangle record carries its vertices' coordinates, so the predicates
+// never chase the point arrays.
+HD uint32_t pack_xy(int32_t x, int32_t y) {
+    return (uint32_t(x + 32768) & 0xffffu) | ((uint32_t(y + 32768) & 0xffffu) << 16);
+}
+HD int32_t px_of(uint32_t p) { return int32_t(p & 0xffffu) - 32768; }
+HD int32_t py_of(uint32_t p) { return int32_t(p >> 16) - 32768; }
 
+HD int64_t orient_p(uint32_t a, uint32_t b, uint32_t c) {
+    int64_t ax = px_of(a), ay = py_of(a);
+    return (int64_t(px_of(b)) - ax) * (int64_t(py_of(c)) - ay) - (int64_t(py_of(b)) - ay) * (int64_t(px_of(c)) - ax);
+}
+
+HD int64_t incircle_p(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    int64_t dx = px_of(d), dy = py_of(d);
+    int64_t adx = px_of(a) - dx, ady = py_of(a) - dy;
+    int64_t bdx = px_of(b) - dx, bdy = py_of(b) - dy;
+    int64_t cdx = px_of(c) - dx, cdy = py_of(c) - dy;
+    int64_t al = adx * adx + ady * ady, bl = bdx * bdx + bdy * bdy, cl = cdx * cdx + cdy * cdy;
+    return adx * (bdy * cl - bl * cdy) - ady * (bdx * cl - bl * cdx) + al * (bdx * cdy - bdy * cdx);
+}
+
+// inside_sos on packed coordinates; ia..id are the point indices that order
+// the symbolic perturbation.
+HD bool inside_sos_p(int ia, uint32_t a, int ib, uint32_t b, int ic, uint32_t c, int id, uint32_t d) {
+    int64_t det = incircle_p(a, b, c, d);
+    if (det != 0) return det > 0;
+    int m = imin(imin(ia, ib), imin(ic, id));
+    if (m == id) return true;
+    if (m == ia) return orient_p(d, b, c) < 0;
+    if (m == ib) return orient_p(a, d, c) < 0;
+    return orient_p(a, b, d) < 0;
+}
+
+// Flip rounds are written against an accessor M that stores, per triangle t:
+// v(t,k) vertex indices, xy(t,k) packed coordinates, opp(3t+k) neighbour
+// half-edges, a lock word and the last round t was flipped in.  The flat
+// accessor (global memory, host emulation) and the cluster accessor
+// (distributed shared memory) share this code.
+//
 // Phase A: test half-edge h; propose it if its edge is not locally Delaunay.
-// `owner`: only the triangle with the smaller index tests a shared edge
-// (round 0 walks every half-edge).
-template <class AtomicMin, class Append>
-HD bool flip_propose(Flip& S, int h, int T, uint32_t round, bool owner, AtomicMin amin, Append append_cand) {
+// `owner`: only the triangle with the smaller index tests a shared edge.
+template <class M, class Append>
+HD bool flip_propose(M& m, int h, int T, uint32_t round, bool owner, Append append_cand) {
     int t = h / 3, s = h % 3;
-    int o = S.opp[h];
+    int o = m.opp(h);
     if (o < 0) return true;
     int n = o / 3;
     if (n >= T || t >= T) return false;
     if (owner && n <= t) return true;
     int sn = o % 3;
-    int a = S.tri[3 * t + s], b = S.tri[3 * t + (s + 1) % 3], c = S.tri[3 * t + (s + 2) % 3];
-    int d = S.tri[3 * n + (sn + 2) % 3];
-    if (inside_sos(S.P, a, b, c, d)) {
+    int s1 = s == 2 ? 0 : s + 1, s2 = s1 == 2 ? 0 : s1 + 1, sd = sn == 0 ? 2 : sn - 1;
+    if (inside_sos_p(m.v(t, s), m.xy(t, s), m.v(t, s1), m.xy(t, s1), m.v(t, s2), m.xy(t, s2), m.v(n, sd),
+                     m.xy(n, sd))) {
         uint32_t p = prio(uint32_t(h), round);
-        amin(&S.lock[t], p);
-        amin(&S.lock[n], p);
+        m.lock_min(t, p);
+        m.lock_min(n, p);
         append_cand(h, n);
     }
     return true;
 }
 
-// Phase B: flip the proposal (h, n) if it won both locks.  Returns true if
-// flipped; the caller records the pair and the four forwarding slots.
-HD bool flip_apply(Flip& S, int h, int n, uint32_t round, int32_t* fwd_slots) {
+// Phase B: flip the proposal (h, n) if it won both locks.
+template <class M>
+HD bool flip_apply(M& m, int h, int n, uint32_t round) {
     int t = h / 3, s = h % 3;
     uint32_t p = prio(uint32_t(h), round);
-    if (S.lock[t] != p || S.lock[n] != p) return false;
-    int o = S.opp[h];
-    int sn = o % 3;
-    int a = S.tri[3 * t + s], b = S.tri[3 * t + (s + 1) % 3], c = S.tri[3 * t + (s + 2) % 3];
-    int d = S.tri[3 * n + (sn + 2) % 3];
-    int O_bc = S.opp[3 * t + (s + 1) % 3], O_ca = S.opp[3 * t + (s + 2) % 3];
-    int O_ad = S.opp[3 * n + (sn + 1) % 3], O_db = S.opp[3 * n + (sn + 2) % 3];
-    // t' = (c, a, d), n' = (d, b, c); the new diagonal (d,c)/(c,d) is slot 2 of both
-    S.tri[3 * t] = c; S.tri[3 * t + 1] = a; S.tri[3 * t + 2] = d;
-    S.tri[3 * n] = d; S.tri[3 * n + 1] = b; S.tri[3 * n + 2] = c;
-    S.opp[3 * t] = O_ca; S.opp[3 * t + 1] = O_ad; S.opp[3 * t + 2] = FINAL | (3 * n + 2);
-    S.opp[3 * n] = O_db; S.opp[3 * n + 1] = O_bc; S.opp[3 * n + 2] = FINAL | (3 * t + 2);
-    fwd_slots[0] = 3 * t + (s + 2) % 3; S.fwd[fwd_slots[0]] = 3 * t;        // edge c-a -> t' slot 0
-    fwd_slots[1] = 3 * t + (s + 1) % 3; S.fwd[fwd_slots[1]] = 3 * n + 1;    // edge b-c -> n' slot 1
-    fwd_slots[2] = 3 * n + (sn + 1) % 3; S.fwd[fwd_slots[2]] = 3 * t + 1;   // edge a-d -> t' slot 1
-    fwd_slots[3] = 3 * n + (sn + 2) % 3; S.fwd[fwd_slots[3]] = 3 * n;       // edge d-b -> n' slot 0
-    S.fround[t] = int32_t(round);
-    S.fround[n] = int32_t(round);
+    if (m.lock(t) != p || m.lock(n) != p) return false;
+    int sn = m.opp(h) % 3;
+    int s1 = s == 2 ? 0 : s + 1, s2 = s1 == 2 ? 0 : s1 + 1;
+    int sn1 = sn == 2 ? 0 : sn + 1, sn2 = sn1 == 2 ? 0 : sn1 + 1;
+    int a = m.v(t, s), b = m.v(t, s1), c = m.v(t, s2), d = m.v(n, sn2);
+    uint32_t pa = m.xy(t, s), pb = m.xy(t, s1), pc = m.xy(t, s2), pd = m.xy(n, sn2);
+    int O_bc = m.opp(3 * t + s1), O_ca = m.opp(3 * t + s2);
+    int O_ad = m.opp(3 * n + sn1), O_db = m.opp(3 * n + sn2);
+    // t' = (c, a, d), n' = (d, b, c); the new diagonal is slot 2 of both
+    m.set_v(t, c, a, d, pc, pa, pd);
+    m.set_v(n, d, b, c, pd, pb, pc);
+    m.set_opp(3 * t, O_ca); m.set_opp(3 * t + 1, O_ad); m.set_opp(3 * t + 2, FINAL | (3 * n + 2));
+    m.set_opp(3 * n, O_db); m.set_opp(3 * n + 1, O_bc); m.set_opp(3 * n + 2, FINAL | (3 * t + 2));
+    m.set_fround(t, int32_t(round));
+    m.set_fround(n, int32_t(round));
     return true;
 }
 
 // The four outer half-edges of a flipped pair (t, n): t' slots 0,1 and n' slots 0,1.
 HD int outer_slot(int t, int n, int k) { return k < 2 ? 3 * t + k : 3 * n + (k - 2); }
 
-// Phase C1 (read only): resolve where the outer neighbours of pair f now live.
-HD void flip_resolve(Flip& S, int f) {
-    int t = S.flips[2 * f], n = S.flips[2 * f + 1];
-    for (int k = 0; k < 4; ++k) {
-        int o = S.opp[outer_slot(t, n, k)];
-        int r = o;
-        if (o >= 0) {
-            int fw = S.fwd[o];
-            if (fw >= 0) r = fw;
+// Phase C1 (read only): where does the neighbour across outer slot x of a
+// flipped pair live now?  Its old reference o still holds if o's triangle
+// did not flip this round; otherwise the edge is one of the outer slots of
+// that triangle's new pair, found by matching the reversed edge.  Returns
+// the half-edge, -1 for the hull, or -2 if nothing matched (corrupt state).
+template <class M>
+HD int flip_resolve_slot(M& m, int x, uint32_t round) {
+    int o = m.opp(x);
+    if (o < 0) return -1;
+    int mt = o / 3;
+    if (m.fround(mt) != int32_t(round)) return o;
+    int xt = x / 3, xk = x % 3;
+    int a = m.v(xt, xk), b = m.v(xt, xk == 2 ? 0 : xk + 1);
+    int mt2 = (m.opp(3 * mt + 2) & ~FINAL) / 3;
+    const int cand_t[2] = {mt, mt2};
+    for (int i = 0; i < 2; ++i)
+        for (int k = 0; k < 2; ++k) {
+            int tt = cand_t[i];
+            if (m.v(tt, k) == b && m.v(tt, k + 1) == a) return 3 * tt + k;
         }
-        S.res[4 * f + k] = r;
-    }
+    return -2;
 }
 
-// Phase C2: write the links in both directions, clear the FINAL marks and
-// queue the outer edges for the next round.
-template <class Append>
-HD void flip_relink(Flip& S, int f, Append append_next) {
-    int t = S.flips[2 * f], n = S.flips[2 * f + 1];
+// Phase C2: write the links both ways and clear the FINAL marks.
+template <class M>
+HD void flip_relink(M& m, int t, int n, const int32_t* res) {
     for (int k = 0; k < 4; ++k) {
         int x = outer_slot(t, n, k);
-        int r = S.res[4 * f + k];
-        S.opp[x] = r;
-        if (r >= 0) S.opp[r] = x;
-        append_next(x);
+        int r = res[k];
+        m.set_opp(x, r);
+        if (r >= 0) m.set_opp(r, x);
     }
-    S.opp[3 * t + 2] &= ~FINAL;
-    S.opp[3 * n + 2] &= ~FINAL;
+    m.set_opp(3 * t + 2, m.opp(3 * t + 2) & ~FINAL);
+    m.set_opp(3 * n + 2, m.opp(3 * n + 2) & ~FINAL);
 }
+
+// Flat storage: plain arrays (global memory on the device, host memory in
+// the emulation).  AMin performs the lock's atomic minimum.
+template <class AMin>
+struct FlatTri {
+    int32_t* tv;      // [3T] vertex indices
+    uint32_t* txy;    // [3T] packed coordinates
+    int32_t* topp;    // [3T]
+    uint32_t* tlock;  // [T]
+    int32_t* tround;  // [T]
+    AMin amin;
+    HD int v(int t, int k) const { return tv[3 * t + k]; }
+    HD uint32_t xy(int t, int k) const { return txy[3 * t + k]; }
+    HD int opp(int h) const { return topp[h]; }
+    HD uint32_t lock(int t) const { return tlock[t]; }
+    HD int32_t fround(int t) const { return tround[t]; }
+    HD void lock_min(int t, uint32_t p) { amin(&tlock[t], p); }
+    HD void set_v(int t, int a, int b, int c, uint32_t pa, uint32_t pb, uint32_t pc) {
+        tv[3 * t] = a; tv[3 * t + 1] = b; tv[3 * t + 2] = c;
+        txy[3 * t] = pa; txy[3 * t + 1] = pb; txy[3 * t + 2] = pc;
+    }
+    HD void set_opp(int h, int o) { topp[h] = o; }
+    HD void set_fround(int t, int32_t r) { tround[t] = r; }
+};
 
 // Rotate a triangle so its smallest vertex index comes first.
 HD void normalise(int32_t* v) {

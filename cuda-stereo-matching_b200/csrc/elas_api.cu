@@ -26,6 +26,7 @@ struct elas_handle {
     elas_params params;
     int device = 0;
     int num_sms = 0;
+    int cluster_size = 0;   // CTAs per cluster of the Delaunay flip kernel (0 = global fallback only)
     std::string last_error;
     int64_t launches = 0;
 
@@ -173,15 +174,17 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         D.chain = (int32_t*)take(4 * rows * 4);
         D.tri = (int32_t*)take(3 * tmax * 4);
         D.opp = (int32_t*)take(3 * tmax * 4);
+        D.txy = (uint32_t*)take(3 * tmax * 4);
         D.lock = (uint32_t*)take(tmax * 4);
         D.fround = (int32_t*)take(tmax * 4);
-        D.fwd = (int32_t*)take(3 * tmax * 4);
         D.cand = (int32_t*)take(6 * tmax * 4);
-        D.flips = (int32_t*)take(tmax * 4);
-        D.res = (int32_t*)take(2 * tmax * 4);
-        D.fwdl = (int32_t*)take(2 * tmax * 4);
+        D.flips = (int32_t*)take(3 * tmax * 4);
         D.wl0 = (int32_t*)take(6 * tmax * 4);
         D.wl1 = (int32_t*)take(6 * tmax * 4);
+        const size_t per_cta = 6 * 4096;
+        D.cwl = (int32_t*)take(16 * 2 * per_cta * 4);
+        D.ccand = (int32_t*)take(16 * 2 * per_cta * 4);
+        D.cflips = (int32_t*)take(16 * per_cta * 4);
         D.ctr = (int32_t*)take(16 * 4);
         D.hkey = (unsigned long long*)take(hmax * 8);
         D.hcnt = (int32_t*)take(hmax * 4);
@@ -267,7 +270,8 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     CK(launch_grid(h->can, h->gtmp0, h->gtmp1, h->grid0, h->grid1, g, st));
     n += 2;
     CK(mark(ELAS_TIME_DELAUNAY));
-    CK(launch_delaunay(h->del[0], h->del[1], h->row_off, g.ch, g.cw * g.ch, h->num_sms, h->err, st, &n));
+    CK(launch_delaunay(h->del[0], h->del[1], h->row_off, g.ch, g.cw * g.ch, h->num_sms, h->cluster_size, h->err,
+                       st, &n));
     CK(mark(ELAS_TIME_PRIOR));
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
                     h->prior0, h->prior1, g, h->num_sms, st));
@@ -398,6 +402,7 @@ int elas_b200_create(const elas_params* params, int device, elas_handle** out) {
     h->params = p;
     h->device = device;
     h->num_sms = prop.multiProcessorCount;
+    h->cluster_size = cluster_size_for_flip();
     *out = h;
     return ELAS_OK;
 }

@@ -5,6 +5,7 @@
 //
 // Both views run as two independent problems inside the same launches:
 // problem 0 triangulates (u, v), problem 1 triangulates (u - d, v).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include "common.cuh"
 #include "delaunay_core.h"
@@ -13,6 +14,7 @@
 namespace elas {
 
 using namespace del;
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -164,6 +166,7 @@ __global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32
         D.ctr[0] = (R >= 2 && off + 2 * R <= D.Tmax) ? off + pockets : 0;
         D.ctr[1] = off;
         D.ctr[6] = R;
+        D.ctr[8] = 0;    // set to 1 by the cluster flip kernel when it handles the problem
     }
 }
 
@@ -260,94 +263,101 @@ __global__ void k_link(DelDev d0, DelDev d1, unsigned* err) {
         else if (c != 1) set_err(err, ERRF_HASH);
         if (o >= 3 * T) { set_err(err, ERRF_BOUNDS); o = -1; }
         D.opp[h] = o;
-        D.fwd[h] = -1;
-    }
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
-        D.lock[t] = LOCK_FREE;
-        D.fround[t] = -1;
     }
 }
 
-struct SAMin {
+struct GAMin {
     __device__ void operator()(uint32_t* p, uint32_t v) const { atomicMin(p, v); }
 };
 
-// Worklist-driven Lawson flipping, one 1024-thread CTA per problem, every
-// phase separated by __syncthreads.  At most `max_rounds` rounds; hitting the
-// limit raises ERRF_FLIP_LIMIT.
-__global__ void __launch_bounds__(FLIP_THREADS) k_flip(DelDev d0, DelDev d1, int max_rounds, unsigned* err) {
-    __shared__ int n_cand, n_flip, n_fwd, n_next, n_cur, stop, prev_fwd;
-    const DelDev& D = blockIdx.x ? d1 : d0;
+// Packed coordinates of every triangle corner (flat storage of the fallback).
+__global__ void k_tri_xy(DelDev d0, DelDev d1) {
+    const DelDev& D = blockIdx.y ? d1 : d0;
+    if (D.ctr[8] != 0) return;            // the cluster kernel handled this problem
     const int T = D.ctr[0];
-    Flip S{Pts{D.x, D.y}, D.tri, D.opp, D.lock, D.fround, D.fwd, D.cand, D.flips, D.res, D.fwdl,
-           {D.wl0, D.wl1}, D.Tmax};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * T; i += gridDim.x * blockDim.x) {
+        int v = D.tri[i];
+        D.txy[i] = pack_xy(D.x[v], D.y[v]);
+    }
+}
+
+// Shared round driver: one "group" (a CTA, or a cluster of CTAs) runs the
+// rounds; `Sync` is its barrier.  Lists live in global memory; their
+// counters in shared memory of the owning CTA.
+//
+// Fallback: one 1024-thread CTA per problem on global memory, for
+// triangulations larger than the cluster kernel holds.  Every loop is
+// bounded: `max_rounds` rounds at most (ERRF_FLIP_LIMIT).
+__global__ void __launch_bounds__(FLIP_THREADS) k_flip_global(DelDev d0, DelDev d1, int max_rounds, unsigned* err) {
+    __shared__ int n_cand, n_flip, n_next, n_cur, stop;
+    const DelDev& D = blockIdx.x ? d1 : d0;
+    if (D.ctr[8] != 0) return;            // the cluster kernel handled this problem
+    const int T = D.ctr[0];
+    FlatTri<GAMin> m{D.tri, D.txy, D.opp, D.lock, D.fround, GAMin()};
     const int cand_cap = 3 * D.Tmax, wl_cap = 6 * D.Tmax;
     const int tid = threadIdx.x;
-    if (tid == 0) { n_cur = 3 * T; n_fwd = 0; prev_fwd = 0; stop = 0; }
+    for (int t = tid; t < T; t += FLIP_THREADS) { D.lock[t] = LOCK_FREE; D.fround[t] = -1; }
+    if (tid == 0) { n_cur = 3 * T; stop = 0; }
     __syncthreads();
-    int round = 0;
-    int flips_total = 0;
+    int round = 0, flips_total = 0;
     for (; round < max_rounds; ++round) {
-        int32_t* cur = S.wl[round & 1];
-        int32_t* nxt = S.wl[(round + 1) & 1];
-        if (tid == 0) { n_cand = 0; n_next = 0; }
-        // clear the forwarding entries of the previous round
-        for (int k = tid; k < prev_fwd; k += FLIP_THREADS) S.fwd[S.fwdl[k]] = -1;
+        const int32_t* cur = (round & 1) ? D.wl1 : D.wl0;
+        int32_t* nxt = (round & 1) ? D.wl0 : D.wl1;
+        if (tid == 0) { n_cand = 0; n_next = 0; n_flip = 0; }
         __syncthreads();
-        // A: propose
         const int items = n_cur;
         for (int k = tid; k < items; k += FLIP_THREADS) {
             int h = round == 0 ? k : cur[k];
-            bool ok = flip_propose(S, h, T, uint32_t(round), round == 0, SAMin(), [&](int hh, int nn) {
-                int idx = atomicAdd(&n_cand, 1);
-                if (idx < cand_cap) { S.cand[2 * idx] = hh; S.cand[2 * idx + 1] = nn; }
-            });
-            if (!ok) set_err(err, ERRF_BOUNDS);
+            if (!flip_propose(m, h, T, uint32_t(round), round == 0, [&](int hh, int nn) {
+                    int idx = atomicAdd(&n_cand, 1);
+                    if (idx < cand_cap) { D.cand[2 * idx] = hh; D.cand[2 * idx + 1] = nn; }
+                }))
+                set_err(err, ERRF_BOUNDS);
         }
         __syncthreads();
         const int nc = n_cand;
-        if (nc > cand_cap) { if (tid == 0) { set_err(err, ERRF_BOUNDS); stop = 1; } }
-        if (tid == 0) { n_flip = 0; n_fwd = 0; }
+        if (tid == 0 && nc > cand_cap) { set_err(err, ERRF_BOUNDS); stop = 1; }
         __syncthreads();
         if (nc == 0 || stop) break;
-        // B: flip the winners
         for (int c = tid; c < nc; c += FLIP_THREADS) {
-            int slots[4];
-            if (flip_apply(S, S.cand[2 * c], S.cand[2 * c + 1], uint32_t(round), slots)) {
+            int h = D.cand[2 * c], n = D.cand[2 * c + 1];
+            if (flip_apply(m, h, n, uint32_t(round))) {
                 int f = atomicAdd(&n_flip, 1);
-                int h = S.cand[2 * c];
-                S.flips[2 * f] = h / 3;
-                S.flips[2 * f + 1] = S.cand[2 * c + 1];
-                int q = atomicAdd(&n_fwd, 4);
-                for (int k = 0; k < 4; ++k) S.fwdl[q + k] = slots[k];
+                D.flips[6 * f] = h / 3;
+                D.flips[6 * f + 1] = n;
             }
         }
         __syncthreads();
         const int nf = n_flip;
-        // C1: resolve the outer neighbours (read only)
-        for (int f = tid; f < nf; f += FLIP_THREADS) flip_resolve(S, f);
-        __syncthreads();
-        // C2: relink, queue the outer edges, release locks, requeue lost proposals
-        for (int f = tid; f < nf; f += FLIP_THREADS)
-            flip_relink(S, f, [&](int x) {
-                int idx = atomicAdd(&n_next, 1);
-                if (idx < wl_cap) nxt[idx] = x;
-            });
-        for (int c = tid; c < nc; c += FLIP_THREADS) {
-            int h = S.cand[2 * c], n = S.cand[2 * c + 1], t = h / 3;
-            S.lock[t] = LOCK_FREE;
-            S.lock[n] = LOCK_FREE;
-            if (S.fround[t] != round && S.fround[n] != round) {
-                int idx = atomicAdd(&n_next, 1);
-                if (idx < wl_cap) nxt[idx] = h;
+        for (int f = tid; f < nf; f += FLIP_THREADS) {
+            int t = D.flips[6 * f], n = D.flips[6 * f + 1];
+            for (int k = 0; k < 4; ++k) {
+                int r = flip_resolve_slot(m, outer_slot(t, n, k), uint32_t(round));
+                if (r == -2) { set_err(err, ERRF_BOUNDS); r = -1; }
+                D.flips[6 * f + 2 + k] = r;
             }
+        }
+        __syncthreads();
+        auto push = [&](int x) {
+            int idx = atomicAdd(&n_next, 1);
+            if (idx < wl_cap) nxt[idx] = x;
+        };
+        for (int f = tid; f < nf; f += FLIP_THREADS) {
+            int t = D.flips[6 * f], n = D.flips[6 * f + 1];
+            flip_relink(m, t, n, D.flips + 6 * f + 2);
+            for (int k = 0; k < 4; ++k) push(outer_slot(t, n, k));
+        }
+        for (int c = tid; c < nc; c += FLIP_THREADS) {
+            int h = D.cand[2 * c], n = D.cand[2 * c + 1], t = h / 3;
+            D.lock[t] = LOCK_FREE;
+            D.lock[n] = LOCK_FREE;
+            if (D.fround[t] != round && D.fround[n] != round) push(h);
         }
         flips_total += nf;
         __syncthreads();
         if (tid == 0) {
             if (n_next > wl_cap) { set_err(err, ERRF_BOUNDS); stop = 1; }
             n_cur = min(n_next, wl_cap);
-            prev_fwd = n_fwd;
         }
         __syncthreads();
         if (stop) break;
@@ -359,6 +369,172 @@ __global__ void __launch_bounds__(FLIP_THREADS) k_flip(DelDev d0, DelDev d1, int
     }
 }
 
+// ---------------------------------------------------------------------------
+// Cluster kernel: the triangulation of one problem lives in the distributed
+// shared memory of a cluster of CL_MAX CTAs.  Triangle t sits in CTA
+// t >> shift at slot t & mask (a power-of-two slice); a record is 44 bytes
+// (3 vertex indices, 3 packed coordinates, 3 links, lock, flip round), so a
+// cluster of 16 CTAs holds up to 65536 triangles.  Every access to another
+// CTA's triangle is a distributed-shared-memory load, store or atomic; the
+// phases are separated by cluster barriers.
+constexpr int CL_THREADS = 1024;
+constexpr int SLICE_MAX_LOG2 = 12;                 // 4096 triangles per CTA
+constexpr int SLICE_MAX = 1 << SLICE_MAX_LOG2;
+constexpr int WL_PER_CTA = 6 * SLICE_MAX;           // worklist entries per CTA and round
+constexpr int CAND_PER_CTA = 6 * SLICE_MAX;         // proposals per CTA and round
+constexpr int FLIP_PER_CTA = SLICE_MAX;             // flipped pairs per CTA and round
+
+struct ClusterTri {
+    int32_t* lv;      // [3*SLICE_MAX] in this CTA's shared memory
+    uint32_t* lxy;    // [3*SLICE_MAX]
+    int32_t* lopp;    // [3*SLICE_MAX]
+    uint32_t* llock;  // [SLICE_MAX]
+    int32_t* lround;  // [SLICE_MAX]
+    int shift, mask;
+    template <class X>
+    __device__ __forceinline__ X* at(X* base, int t) const {
+        return cg::this_cluster().map_shared_rank(base, unsigned(t >> shift));
+    }
+    __device__ int v(int t, int k) const { return at(lv, t)[3 * (t & mask) + k]; }
+    __device__ uint32_t xy(int t, int k) const { return at(lxy, t)[3 * (t & mask) + k]; }
+    __device__ int opp(int h) const { int t = h / 3; return at(lopp, t)[3 * (t & mask) + h - 3 * t]; }
+    __device__ uint32_t lock(int t) const { return *((volatile uint32_t*)at(llock, t) + (t & mask)); }
+    __device__ int32_t fround(int t) const { return at(lround, t)[t & mask]; }
+    __device__ void lock_min(int t, uint32_t p) { atomicMin(at(llock, t) + (t & mask), p); }
+    __device__ void set_v(int t, int a, int b, int c, uint32_t pa, uint32_t pb, uint32_t pc) {
+        int32_t* V = at(lv, t) + 3 * (t & mask);
+        uint32_t* X = at(lxy, t) + 3 * (t & mask);
+        V[0] = a; V[1] = b; V[2] = c;
+        X[0] = pa; X[1] = pb; X[2] = pc;
+    }
+    __device__ void set_opp(int h, int o) { int t = h / 3; at(lopp, t)[3 * (t & mask) + h - 3 * t] = o; }
+    __device__ void set_fround(int t, int32_t r) { at(lround, t)[t & mask] = r; }
+};
+
+__global__ void __launch_bounds__(CL_THREADS) k_flip_cluster(DelDev d0, DelDev d1, int csize, int max_rounds,
+                                                             unsigned* err) {
+    extern __shared__ __align__(16) uint8_t csm[];
+    __shared__ int n_cand[2], n_flip, n_wl[2], stop;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = int(cluster.block_rank());
+    const int prob = blockIdx.x / csize;
+    const DelDev& D = prob ? d1 : d0;
+    const int T = D.ctr[0];
+    if (T > csize * SLICE_MAX) {            // too large: the global kernel takes it
+        if (rank == 0 && threadIdx.x == 0) D.ctr[8] = 0;
+        return;                              // uniform over the cluster
+    }
+    int shift = 6;
+    while ((csize << shift) < T) ++shift;
+    ClusterTri m;
+    m.lv = reinterpret_cast<int32_t*>(csm);
+    m.lxy = reinterpret_cast<uint32_t*>(m.lv + 3 * SLICE_MAX);
+    m.lopp = reinterpret_cast<int32_t*>(m.lxy + 3 * SLICE_MAX);
+    m.llock = reinterpret_cast<uint32_t*>(m.lopp + 3 * SLICE_MAX);
+    m.lround = reinterpret_cast<int32_t*>(m.llock + SLICE_MAX);
+    m.shift = shift;
+    m.mask = (1 << shift) - 1;
+    const int t0 = rank << shift, t1 = min(T, (rank + 1) << shift);
+    const int tid = threadIdx.x;
+    for (int t = t0 + tid; t < t1; t += CL_THREADS) {
+        int l = t - t0;
+        for (int k = 0; k < 3; ++k) {
+            int v = D.tri[3 * t + k];
+            m.lv[3 * l + k] = v;
+            m.lxy[3 * l + k] = pack_xy(D.x[v], D.y[v]);
+            m.lopp[3 * l + k] = D.opp[3 * t + k];
+        }
+        m.llock[l] = LOCK_FREE;
+        m.lround[l] = -1;
+    }
+    if (tid == 0) { n_cand[0] = n_cand[1] = 0; n_flip = 0; n_wl[0] = n_wl[1] = 0; stop = 0; }
+    // per-CTA list regions in global memory
+    int32_t* wl[2] = {D.cwl + size_t(rank) * 2 * WL_PER_CTA, D.cwl + size_t(rank) * 2 * WL_PER_CTA + WL_PER_CTA};
+    int32_t* cand = D.ccand + size_t(rank) * 2 * CAND_PER_CTA;
+    int32_t* flips = D.cflips + size_t(rank) * 6 * FLIP_PER_CTA;
+    cluster.sync();
+    int round = 0, flips_total = 0;
+    bool converged = false;
+    for (; round < max_rounds; ++round) {
+        const int cur = round & 1, nxt = cur ^ 1;
+        // A: propose (round 0: every own half-edge, owner rule)
+        const int items = round == 0 ? 3 * (t1 - t0) : min(n_wl[cur], WL_PER_CTA);
+        auto add_cand = [&](int hh, int nn) {
+            int idx = atomicAdd(&n_cand[cur], 1);
+            if (idx < CAND_PER_CTA) { cand[2 * idx] = hh; cand[2 * idx + 1] = nn; }
+        };
+        for (int k = tid; k < items; k += CL_THREADS) {
+            int h = round == 0 ? 3 * t0 + k : wl[cur][k];
+            if (!flip_propose(m, h, T, uint32_t(round), round == 0, add_cand)) set_err(err, ERRF_BOUNDS);
+        }
+        if (tid == 0) n_wl[nxt] = 0;       // nobody appends to it before phase C2
+        cluster.sync();
+        int total = 0;
+        for (int r = 0; r < csize; ++r) total += *cluster.map_shared_rank(&n_cand[cur], unsigned(r));
+        const int nc = min(n_cand[cur], CAND_PER_CTA);
+        if (tid == 0 && n_cand[cur] > CAND_PER_CTA) { set_err(err, ERRF_BOUNDS); stop = 1; }
+        if (total == 0) { converged = true; break; }
+        // B: flip the winners
+        for (int c = tid; c < nc; c += CL_THREADS) {
+            int h = cand[2 * c], n = cand[2 * c + 1];
+            if (flip_apply(m, h, n, uint32_t(round))) {
+                int f = atomicAdd(&n_flip, 1);
+                if (f < FLIP_PER_CTA) { flips[6 * f] = h / 3; flips[6 * f + 1] = n; }
+            }
+        }
+        cluster.sync();
+        const int nf = min(n_flip, FLIP_PER_CTA);
+        // C1: resolve the outer neighbours (read only)
+        for (int f = tid; f < nf; f += CL_THREADS) {
+            int t = flips[6 * f], n = flips[6 * f + 1];
+            for (int k = 0; k < 4; ++k) {
+                int r = flip_resolve_slot(m, outer_slot(t, n, k), uint32_t(round));
+                if (r == -2) { set_err(err, ERRF_BOUNDS); r = -1; }
+                flips[6 * f + 2 + k] = r;
+            }
+        }
+        cluster.sync();
+        // C2: relink, queue the outer edges at their owners, release locks, requeue lost proposals
+        auto push = [&](int x) {
+            int t = x / 3;
+            int* cnt = cluster.map_shared_rank(&n_wl[nxt], unsigned(t >> shift));
+            int idx = atomicAdd(cnt, 1);
+            if (idx < WL_PER_CTA) D.cwl[size_t(t >> shift) * 2 * WL_PER_CTA + size_t(nxt) * WL_PER_CTA + idx] = x;
+        };
+        for (int f = tid; f < nf; f += CL_THREADS) {
+            int t = flips[6 * f], n = flips[6 * f + 1];
+            flip_relink(m, t, n, flips + 6 * f + 2);
+            for (int k = 0; k < 4; ++k) push(outer_slot(t, n, k));
+        }
+        for (int c = tid; c < nc; c += CL_THREADS) {
+            int h = cand[2 * c], n = cand[2 * c + 1], t = h / 3;
+            *(m.at(m.llock, t) + (t & m.mask)) = LOCK_FREE;
+            *(m.at(m.llock, n) + (n & m.mask)) = LOCK_FREE;
+            if (m.fround(t) != round && m.fround(n) != round) push(h);
+        }
+        flips_total += nf;
+        if (tid == 0) { n_cand[nxt] = 0; n_flip = 0; }
+        cluster.sync();
+        if (tid == 0 && n_wl[nxt] > WL_PER_CTA) { set_err(err, ERRF_BOUNDS); stop = 1; }
+        // every CTA's stop flag is final after this barrier and unchanged until
+        // the next round's proposals, so all CTAs take the same decision
+        cluster.sync();
+        int any_stop = 0;
+        for (int r = 0; r < csize; ++r) any_stop |= *cluster.map_shared_rank(&stop, unsigned(r));
+        if (any_stop) break;
+    }
+    // write back this CTA's slice
+    for (int t = t0 + tid; t < t1; t += CL_THREADS)
+        for (int k = 0; k < 3; ++k) D.tri[3 * t + k] = m.lv[3 * (t - t0) + k];
+    if (rank == 0 && tid == 0) {
+        D.ctr[8] = 1;
+        D.ctr[4] = round + 1;
+        D.ctr[5] = flips_total;
+        if (!converged) set_err(err, ERRF_FLIP_LIMIT);
+    }
+    cluster.sync();   // keep every CTA's shared memory alive until remote readers are done
+}
+
 __global__ void k_normalise(DelDev d0, DelDev d1) {
     const DelDev& D = blockIdx.y ? d1 : d0;
     const int T = D.ctr[0];
@@ -368,8 +544,32 @@ __global__ void k_normalise(DelDev d0, DelDev d1) {
 
 }  // namespace
 
+int cluster_size_for_flip() {
+    int sizes[2] = {16, 8};
+    size_t smem = size_t(SLICE_MAX) * 44;
+    cudaFuncSetAttribute(k_flip_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaFuncSetAttribute(k_flip_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    for (int cs : sizes) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2 * cs);
+        cfg.blockDim = dim3(CL_THREADS);
+        cfg.dynamicSmemBytes = smem;
+        cudaLaunchAttribute attr;
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = cs;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, k_flip_cluster, &cfg) == cudaSuccess && n >= 2) return cs;
+        cudaGetLastError();
+    }
+    return 0;
+}
+
 cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int nmax, int num_sms,
-                            unsigned* err, cudaStream_t st, int* nlaunch) {
+                            int csize, unsigned* err, cudaStream_t st, int* nlaunch) {
     k_rowsort<<<dim3(nrows, 2), 512, 0, st>>>(d0, d1, row_off, nrows, err);
     int smem_rows = imin(nrows, (96 * 1024) / 16);
     size_t smem = size_t(smem_rows) * 16;
@@ -380,9 +580,30 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
     k_hash_clear<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1);
     k_hash_insert<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1, err);
     k_link<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1, err);
-    k_flip<<<2, FLIP_THREADS, 0, st>>>(d0, d1, 100000, err);
+    int launched = 6;
+    const int max_rounds = 100000;
+    if (csize > 0) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2 * csize);
+        cfg.blockDim = dim3(CL_THREADS);
+        cfg.dynamicSmemBytes = size_t(SLICE_MAX) * 44;
+        cfg.stream = st;
+        cudaLaunchAttribute attr;
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = csize;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        cudaError_t e = cudaLaunchKernelEx(&cfg, k_flip_cluster, d0, d1, csize, max_rounds, err);
+        if (e != cudaSuccess) return e;
+        ++launched;
+    }
+    k_tri_xy<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1);
+    k_flip_global<<<2, FLIP_THREADS, 0, st>>>(d0, d1, max_rounds, err);
     k_normalise<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1);
-    if (nlaunch) *nlaunch += 8;
+    launched += 3;
+    if (nlaunch) *nlaunch += launched;
     return cudaGetLastError();
 }
 

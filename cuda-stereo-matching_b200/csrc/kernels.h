@@ -18,16 +18,18 @@ struct DelDev {
     int32_t* chain;        // [4*rows] pocket walk scratch when it does not fit in shared memory
     int32_t* tri;          // [3*Tmax]
     int32_t* opp;          // [3*Tmax]
+    uint32_t* txy;         // [3*Tmax] packed corner coordinates (global flip kernel)
     uint32_t* lock;        // [Tmax]
     int32_t* fround;       // [Tmax]
-    int32_t* fwd;          // [3*Tmax]
     int32_t* cand;         // [6*Tmax]
-    int32_t* flips;        // [Tmax]
-    int32_t* res;          // [2*Tmax]
-    int32_t* fwdl;         // [2*Tmax]
+    int32_t* flips;        // [3*Tmax]
     int32_t* wl0;          // [6*Tmax]
     int32_t* wl1;          // [6*Tmax]
-    int32_t* ctr;          // [16]: 0 triangles, 1 strip triangles, 4 flip rounds, 5 flips, 6 non-empty rows
+    int32_t* cwl;          // cluster kernel: per-CTA worklists  [16 * 2 * 6 * 4096]
+    int32_t* ccand;        // cluster kernel: per-CTA proposals  [16 * 2 * 6 * 4096]
+    int32_t* cflips;       // cluster kernel: per-CTA flips      [16 * 6 * 4096]
+    int32_t* ctr;          // [16]: 0 triangles, 1 strip triangles, 4 flip rounds, 5 flips,
+                           //       6 non-empty rows, 8 handled by the cluster kernel
     unsigned long long* hkey;  // [Hmax]
     int32_t* hcnt;         // [Hmax]
     int32_t* hval;         // [2*Hmax]
@@ -49,7 +51,10 @@ cudaError_t launch_grid(const int32_t* can, uint32_t* tmp0, uint32_t* tmp1, uint
                         const Geom& g, cudaStream_t st);
 
 cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int nmax, int num_sms,
-                            unsigned* err, cudaStream_t st, int* nlaunch);
+                            int cluster_size, unsigned* err, cudaStream_t st, int* nlaunch);
+// Largest cluster (16 or 8 CTAs) with two co-resident copies for the flip
+// kernel, or 0 if none fits.
+int cluster_size_for_flip();
 
 // Plane prior of both views: prior[v*W+u] = (triangle+1) << 32 | uint32(d_plane),
 // 0 where no triangle covers the pixel.  Buffers must be zeroed first.

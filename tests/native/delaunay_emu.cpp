@@ -87,51 +87,56 @@ extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const i
         if (kv.second.size() == 2) { opp[kv.second[0]] = kv.second[1]; opp[kv.second[1]] = kv.second[0]; }
         else if (kv.second.size() != 1) return -1;
     }
-    // 5. flips (k_flip)
-    std::vector<uint32_t> lock(Tmax, LOCK_FREE);
-    std::vector<int32_t> fround(Tmax, -1), fwd(3 * size_t(Tmax), -1), cand(6 * size_t(Tmax)), flips(Tmax),
-        res(2 * size_t(Tmax)), fwdl(2 * size_t(Tmax)), wl0(6 * size_t(Tmax)), wl1(6 * size_t(Tmax));
-    Flip S{P, tri.data(), opp.data(), lock.data(), fround.data(), fwd.data(), cand.data(), flips.data(), res.data(),
-           fwdl.data(), {wl0.data(), wl1.data()}, Tmax};
+    // 5. flips (k_flip_global / k_flip_cluster)
+    std::vector<uint32_t> txy(3 * size_t(Tmax)), lock(Tmax, LOCK_FREE);
+    std::vector<int32_t> fround(Tmax, -1), cand(6 * size_t(Tmax)), flips(6 * size_t(Tmax)), wl[2];
+    wl[0].resize(6 * size_t(Tmax));
+    wl[1].resize(6 * size_t(Tmax));
+    for (int i = 0; i < 3 * T; ++i) txy[i] = pack_xy(px[tri[i]], py[tri[i]]);
     auto amin = [](uint32_t* p, uint32_t v) { if (v < *p) *p = v; };
-    int n_cur = 3 * T, prev_fwd = 0;
+    FlatTri<decltype(amin)> m{tri.data(), txy.data(), opp.data(), lock.data(), fround.data(), amin};
+    int n_cur = 3 * T;
     long long rounds = 0, nflips = 0;
     for (int round = 0; round < 100000; ++round) {
-        int32_t* cur = S.wl[round & 1];
-        int32_t* nxt = S.wl[(round + 1) & 1];
-        for (int k = 0; k < prev_fwd; ++k) fwd[fwdl[k]] = -1;
+        const std::vector<int32_t>& cur = wl[round & 1];
+        std::vector<int32_t>& nxt = wl[(round + 1) & 1];
         int nc = 0;
         for (int k = 0; k < n_cur; ++k) {
             int h = round == 0 ? k : cur[k];
-            if (!flip_propose(S, h, T, uint32_t(round), round == 0, amin, [&](int hh, int nn) {
+            if (!flip_propose(m, h, T, uint32_t(round), round == 0, [&](int hh, int nn) {
                     cand[2 * nc] = hh; cand[2 * nc + 1] = nn; ++nc;
                 }))
                 return -1;
         }
         ++rounds;
         if (nc == 0) break;
-        int nf = 0, nfw = 0;
-        for (int c = 0; c < nc; ++c) {
-            int slots[4];
-            if (flip_apply(S, cand[2 * c], cand[2 * c + 1], uint32_t(round), slots)) {
-                flips[2 * nf] = cand[2 * c] / 3;
-                flips[2 * nf + 1] = cand[2 * c + 1];
+        int nf = 0;
+        for (int c = 0; c < nc; ++c)
+            if (flip_apply(m, cand[2 * c], cand[2 * c + 1], uint32_t(round))) {
+                flips[6 * nf] = cand[2 * c] / 3;
+                flips[6 * nf + 1] = cand[2 * c + 1];
                 ++nf;
-                for (int k = 0; k < 4; ++k) fwdl[nfw++] = slots[k];
             }
-        }
-        for (int f = 0; f < nf; ++f) flip_resolve(S, f);
+        for (int f = 0; f < nf; ++f)
+            for (int k = 0; k < 4; ++k) {
+                int r = flip_resolve_slot(m, outer_slot(flips[6 * f], flips[6 * f + 1], k), uint32_t(round));
+                if (r == -2) return -1;
+                flips[6 * f + 2 + k] = r;
+            }
         int nn = 0;
-        for (int f = 0; f < nf; ++f) flip_relink(S, f, [&](int x) { nxt[nn++] = x; });
+        for (int f = 0; f < nf; ++f) {
+            int t = flips[6 * f], n2 = flips[6 * f + 1];
+            flip_relink(m, t, n2, &flips[6 * f + 2]);
+            for (int k = 0; k < 4; ++k) nxt[nn++] = outer_slot(t, n2, k);
+        }
         for (int c = 0; c < nc; ++c) {
-            int h = cand[2 * c], m = cand[2 * c + 1], t = h / 3;
+            int h = cand[2 * c], n2 = cand[2 * c + 1], t = h / 3;
             lock[t] = LOCK_FREE;
-            lock[m] = LOCK_FREE;
-            if (fround[t] != round && fround[m] != round) nxt[nn++] = h;
+            lock[n2] = LOCK_FREE;
+            if (fround[t] != round && fround[n2] != round) nxt[nn++] = h;
         }
         nflips += nf;
         n_cur = nn;
-        prev_fwd = nfw;
     }
     for (int t = 0; t < T; ++t) normalise(&tri[3 * size_t(t)]);
     if (T <= cap) std::memcpy(tris_out, tri.data(), sizeof(int32_t) * 3 * size_t(T));
