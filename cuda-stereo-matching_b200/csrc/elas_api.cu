@@ -43,9 +43,12 @@ struct elas_handle {
     uint32_t *gtmp0 = nullptr, *gtmp1 = nullptr, *grid0 = nullptr, *grid1 = nullptr;
     DelDev del[2]{};
     unsigned long long *prior0 = nullptr, *prior1 = nullptr;
-    float *raw0 = nullptr, *raw1 = nullptr, *lr0 = nullptr, *lr1 = nullptr, *tmp = nullptr;
+    float *raw0 = nullptr, *raw1 = nullptr, *lr0 = nullptr, *lr1 = nullptr;
     float *out0 = nullptr, *out1 = nullptr;
-    int32_t *lab = nullptr, *usize = nullptr;
+    float* tmp[2] = {nullptr, nullptr};          // post-filter ping-pong buffer per view
+    int32_t* lab[2] = {nullptr, nullptr};        // union-find labels per view
+    int32_t* root[2] = {nullptr, nullptr};       // union-find roots per view
+    int32_t* usize[2] = {nullptr, nullptr};      // segment sizes per view
     unsigned* err = nullptr;
 
     // per-stage timing
@@ -199,11 +202,14 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
     h->raw1 = (float*)take(px * 4);
     h->lr0 = (float*)take(px * 4);
     h->lr1 = (float*)take(px * 4);
-    h->tmp = (float*)take(px * 4);
     h->out0 = (float*)take(px * 4);
     h->out1 = (float*)take(px * 4);
-    h->lab = (int32_t*)take(px * 4);
-    h->usize = (int32_t*)take(px * 4);
+    for (int k = 0; k < 2; ++k) {
+        h->tmp[k] = (float*)take(px * 4);
+        h->lab[k] = (int32_t*)take(px * 4);
+        h->root[k] = (int32_t*)take(px * 4);
+        h->usize[k] = (int32_t*)take(px * 4);
+    }
     h->err = (unsigned*)take(64);
     return off;
 }
@@ -285,9 +291,18 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     CK(mark(ELAS_TIME_POST));
     CK(cudaMemcpyAsync(out0, h->lr0, size_t(W) * H * 4, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(out1, h->lr1, size_t(W) * H * 4, cudaMemcpyDeviceToDevice, st));
-    CK(launch_post(out0, h->tmp, h->lab, h->usize, g, dp, p.filter_median, p.filter_adaptive_mean, h->err, st, &n));
-    if (!p.postprocess_only_left)
-        CK(launch_post(out1, h->tmp, h->lab, h->usize, g, dp, p.filter_median, p.filter_adaptive_mean, h->err, st, &n));
+    PostViews pv;
+    float* outs[2] = {out0, out1};
+    for (int k = 0; k < 2; ++k) {
+        pv.cur[k] = outs[k];
+        pv.nxt[k] = h->tmp[k];
+        pv.out[k] = outs[k];
+        pv.lab[k] = h->lab[k];
+        pv.root[k] = h->root[k];
+        pv.sz[k] = h->usize[k];
+    }
+    CK(launch_post(pv, p.postprocess_only_left ? 1 : 2, g, dp, p.filter_median, p.filter_adaptive_mean, h->err, st,
+                   &n));
     CK(mark(ELAS_TIME_COUNT));
     h->launches += n;
     h->have_last = true;

@@ -6,6 +6,7 @@
 // Both views run as two independent problems inside the same launches:
 // problem 0 triangulates (u, v), problem 1 triangulates (u - d, v).
 #include <cooperative_groups.h>
+#include <type_traits>
 #include <cuda_runtime.h>
 #include "common.cuh"
 #include "delaunay_core.h"
@@ -411,22 +412,65 @@ struct ClusterTri {
     __device__ void set_fround(int t, int32_t r) { at(lround, t)[t & mask] = r; }
 };
 
-__global__ void __launch_bounds__(CL_THREADS) k_flip_cluster(DelDev d0, DelDev d1, int csize, int max_rounds,
-                                                             unsigned* err) {
+// The same record layout in this CTA's own shared memory, for problems that
+// fit one SM (plain shared-memory accesses, __syncthreads between phases).
+struct LocalTri {
+    int32_t* lv;
+    uint32_t* lxy;
+    int32_t* lopp;
+    uint32_t* llock;
+    int32_t* lround;
+    int shift, mask;
+    template <class X>
+    __device__ __forceinline__ X* at(X* base, int) const { return base; }
+    __device__ int v(int t, int k) const { return lv[3 * t + k]; }
+    __device__ uint32_t xy(int t, int k) const { return lxy[3 * t + k]; }
+    __device__ int opp(int h) const { return lopp[h]; }
+    __device__ uint32_t lock(int t) const { return *((volatile uint32_t*)llock + t); }
+    __device__ int32_t fround(int t) const { return lround[t]; }
+    __device__ void lock_min(int t, uint32_t p) { atomicMin(llock + t, p); }
+    __device__ void set_v(int t, int a, int b, int c, uint32_t pa, uint32_t pb, uint32_t pc) {
+        lv[3 * t] = a; lv[3 * t + 1] = b; lv[3 * t + 2] = c;
+        lxy[3 * t] = pa; lxy[3 * t + 1] = pb; lxy[3 * t + 2] = pc;
+    }
+    __device__ void set_opp(int h, int o) { lopp[h] = o; }
+    __device__ void set_fround(int t, int32_t r) { lround[t] = r; }
+};
+
+struct ClusterSync {
+    __device__ void operator()() const { cg::this_cluster().sync(); }
+    template <class X>
+    __device__ X* remote(X* p, int r) const { return cg::this_cluster().map_shared_rank(p, unsigned(r)); }
+    __device__ int rank() const { return int(cg::this_cluster().block_rank()); }
+};
+struct BlockSync {
+    __device__ void operator()() const { __syncthreads(); }
+    template <class X>
+    __device__ X* remote(X* p, int) const { return p; }
+    __device__ int rank() const { return 0; }
+};
+
+// Shared-memory flip rounds.  LOCAL: one CTA per problem holding at most
+// SLICE_MAX triangles; otherwise a cluster of csize CTAs (csize * SLICE_MAX).
+// A kernel whose range does not contain T returns at once; the first one
+// that handles a problem sets ctr[8].
+template <bool LOCAL>
+__global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, int csize, int max_rounds,
+                                                          unsigned* err) {
+    using Acc = typename std::conditional<LOCAL, LocalTri, ClusterTri>::type;
+    using Sync = typename std::conditional<LOCAL, BlockSync, ClusterSync>::type;
     extern __shared__ __align__(16) uint8_t csm[];
     __shared__ int n_cand[2], n_flip, n_wl[2], stop;
-    cg::cluster_group cluster = cg::this_cluster();
-    const int rank = int(cluster.block_rank());
+    Sync sync;
+    const int rank = sync.rank();
     const int prob = blockIdx.x / csize;
     const DelDev& D = prob ? d1 : d0;
     const int T = D.ctr[0];
-    if (T > csize * SLICE_MAX) {            // too large: the global kernel takes it
-        if (rank == 0 && threadIdx.x == 0) D.ctr[8] = 0;
-        return;                              // uniform over the cluster
-    }
+    // uniform over the CTAs of a problem: no barrier has been passed yet
+    if (D.ctr[8] != 0 || T > csize * SLICE_MAX || (!LOCAL && T <= SLICE_MAX)) return;
     int shift = 6;
     while ((csize << shift) < T) ++shift;
-    ClusterTri m;
+    Acc m;
     m.lv = reinterpret_cast<int32_t*>(csm);
     m.lxy = reinterpret_cast<uint32_t*>(m.lv + 3 * SLICE_MAX);
     m.lopp = reinterpret_cast<int32_t*>(m.lxy + 3 * SLICE_MAX);
@@ -452,7 +496,7 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_cluster(DelDev d0, DelDev d
     int32_t* wl[2] = {D.cwl + size_t(rank) * 2 * WL_PER_CTA, D.cwl + size_t(rank) * 2 * WL_PER_CTA + WL_PER_CTA};
     int32_t* cand = D.ccand + size_t(rank) * 2 * CAND_PER_CTA;
     int32_t* flips = D.cflips + size_t(rank) * 6 * FLIP_PER_CTA;
-    cluster.sync();
+    sync();
     int round = 0, flips_total = 0;
     bool converged = false;
     for (; round < max_rounds; ++round) {
@@ -468,9 +512,9 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_cluster(DelDev d0, DelDev d
             if (!flip_propose(m, h, T, uint32_t(round), round == 0, add_cand)) set_err(err, ERRF_BOUNDS);
         }
         if (tid == 0) n_wl[nxt] = 0;       // nobody appends to it before phase C2
-        cluster.sync();
+        sync();
         int total = 0;
-        for (int r = 0; r < csize; ++r) total += *cluster.map_shared_rank(&n_cand[cur], unsigned(r));
+        for (int r = 0; r < csize; ++r) total += *sync.remote(&n_cand[cur], r);
         const int nc = min(n_cand[cur], CAND_PER_CTA);
         if (tid == 0 && n_cand[cur] > CAND_PER_CTA) { set_err(err, ERRF_BOUNDS); stop = 1; }
         if (total == 0) { converged = true; break; }
@@ -482,7 +526,7 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_cluster(DelDev d0, DelDev d
                 if (f < FLIP_PER_CTA) { flips[6 * f] = h / 3; flips[6 * f + 1] = n; }
             }
         }
-        cluster.sync();
+        sync();
         const int nf = min(n_flip, FLIP_PER_CTA);
         // C1: resolve the outer neighbours (read only)
         for (int f = tid; f < nf; f += CL_THREADS) {
@@ -493,11 +537,11 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_cluster(DelDev d0, DelDev d
                 flips[6 * f + 2 + k] = r;
             }
         }
-        cluster.sync();
+        sync();
         // C2: relink, queue the outer edges at their owners, release locks, requeue lost proposals
         auto push = [&](int x) {
             int t = x / 3;
-            int* cnt = cluster.map_shared_rank(&n_wl[nxt], unsigned(t >> shift));
+            int* cnt = sync.remote(&n_wl[nxt], t >> shift);
             int idx = atomicAdd(cnt, 1);
             if (idx < WL_PER_CTA) D.cwl[size_t(t >> shift) * 2 * WL_PER_CTA + size_t(nxt) * WL_PER_CTA + idx] = x;
         };
@@ -514,13 +558,13 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_cluster(DelDev d0, DelDev d
         }
         flips_total += nf;
         if (tid == 0) { n_cand[nxt] = 0; n_flip = 0; }
-        cluster.sync();
+        sync();
         if (tid == 0 && n_wl[nxt] > WL_PER_CTA) { set_err(err, ERRF_BOUNDS); stop = 1; }
         // every CTA's stop flag is final after this barrier and unchanged until
         // the next round's proposals, so all CTAs take the same decision
-        cluster.sync();
+        sync();
         int any_stop = 0;
-        for (int r = 0; r < csize; ++r) any_stop |= *cluster.map_shared_rank(&stop, unsigned(r));
+        for (int r = 0; r < csize; ++r) any_stop |= *sync.remote(&stop, r);
         if (any_stop) break;
     }
     // write back this CTA's slice
@@ -532,7 +576,7 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_cluster(DelDev d0, DelDev d
         D.ctr[5] = flips_total;
         if (!converged) set_err(err, ERRF_FLIP_LIMIT);
     }
-    cluster.sync();   // keep every CTA's shared memory alive until remote readers are done
+    sync();   // keep every CTA's shared memory alive until remote readers are done
 }
 
 __global__ void k_normalise(DelDev d0, DelDev d1) {
@@ -547,8 +591,9 @@ __global__ void k_normalise(DelDev d0, DelDev d1) {
 int cluster_size_for_flip() {
     int sizes[2] = {16, 8};
     size_t smem = size_t(SLICE_MAX) * 44;
-    cudaFuncSetAttribute(k_flip_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    cudaFuncSetAttribute(k_flip_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaFuncSetAttribute(k_flip_smem<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaFuncSetAttribute(k_flip_smem<false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaFuncSetAttribute(k_flip_smem<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     for (int cs : sizes) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(2 * cs);
@@ -562,7 +607,7 @@ int cluster_size_for_flip() {
         cfg.attrs = &attr;
         cfg.numAttrs = 1;
         int n = 0;
-        if (cudaOccupancyMaxActiveClusters(&n, k_flip_cluster, &cfg) == cudaSuccess && n >= 2) return cs;
+        if (cudaOccupancyMaxActiveClusters(&n, k_flip_smem<false>, &cfg) == cudaSuccess && n >= 2) return cs;
         cudaGetLastError();
     }
     return 0;
@@ -582,6 +627,8 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
     k_link<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1, err);
     int launched = 6;
     const int max_rounds = 100000;
+    k_flip_smem<true><<<2, CL_THREADS, size_t(SLICE_MAX) * 44, st>>>(d0, d1, 1, max_rounds, err);
+    ++launched;
     if (csize > 0) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(2 * csize);
@@ -595,7 +642,7 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
         attr.val.clusterDim.z = 1;
         cfg.attrs = &attr;
         cfg.numAttrs = 1;
-        cudaError_t e = cudaLaunchKernelEx(&cfg, k_flip_cluster, d0, d1, csize, max_rounds, err);
+        cudaError_t e = cudaLaunchKernelEx(&cfg, k_flip_smem<false>, d0, d1, csize, max_rounds, err);
         if (e != cudaSuccess) return e;
         ++launched;
     }

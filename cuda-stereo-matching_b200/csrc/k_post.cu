@@ -38,6 +38,39 @@ __device__ __forceinline__ int uf_find(int32_t* lab, int x, unsigned* err) {
     return x;
 }
 
+// Labels start as stars over the runs of each row: every pixel points at the
+// first pixel of its connected run (one warp per row, ballot scan over
+// 32-pixel chunks).  Only vertical unions remain for k_uf_union_v.
+__global__ void k_uf_init_rows(PostViews pv, int W, int H, float thr) {
+    const int view = blockIdx.z;
+    const float* D = pv.cur[view];
+    int32_t* lab = pv.lab[view];
+    int32_t* sz = pv.sz[view];
+    const int lane = threadIdx.x & 31;
+    const int v = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (v >= H) return;
+    int carry = -1;
+    float prev = -1.0f;
+    for (int u0 = 0; u0 < W; u0 += 32) {
+        const int u = u0 + lane;
+        const size_t i = size_t(v) * W + u;
+        float d = u < W ? D[i] : -1.0f;
+        float dl = __shfl_up_sync(0xffffffffu, d, 1);
+        if (lane == 0) dl = prev;
+        const bool valid = d >= 0;
+        const bool conn = valid && u > 0 && dl >= 0 && fabsf(d - dl) <= thr;
+        const unsigned starts = __ballot_sync(0xffffffffu, valid && !conn);
+        const unsigned mine = starts & (0xffffffffu >> (31 - lane));
+        const int rs = mine ? int(size_t(v) * W + u0 + 31 - __clz(mine)) : carry;
+        if (u < W) {
+            lab[i] = valid ? rs : -1;
+            sz[i] = 0;
+        }
+        carry = __shfl_sync(0xffffffffu, rs, 31);
+        prev = __shfl_sync(0xffffffffu, d, 31);
+    }
+}
+
 // Labels start at the left neighbour when it is connected (the most common
 // union), else at the pixel itself.
 __global__ void k_uf_init(const float* __restrict__ D, int32_t* __restrict__ lab, int32_t* __restrict__ sz, int W,
@@ -73,6 +106,19 @@ __device__ void uf_union(int32_t* lab, int a, int b, unsigned* err) {
     atomicOr(err, ERRF_BOUNDS);
 }
 
+__global__ void k_uf_union_v(PostViews pv, int W, int H, float thr, unsigned* err) {
+    const int view = blockIdx.z;
+    const float* D = pv.cur[view];
+    int32_t* lab = pv.lab[view];
+    int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (u >= W || v + 1 >= H) return;
+    int i = v * W + u;
+    float d = D[i];
+    if (d < 0) return;
+    float q = D[i + W];
+    if (q >= 0 && fabsf(q - d) <= thr) uf_union(lab, i, i + W, err);
+}
+
 __global__ void k_uf_union(const float* __restrict__ D, int32_t* lab, int W, int H, float thr, unsigned* err) {
     int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
     if (u >= W || v >= H) return;
@@ -103,6 +149,31 @@ __global__ void k_uf_count(int32_t* lab, int32_t* __restrict__ root, int32_t* sz
     if (r >= 0 && (threadIdx.x & 31) == leader) atomicAdd(&sz[r], __popc(peers));
 }
 
+__global__ void k_uf_count_v(PostViews pv, int n, unsigned* err) {
+    const int view = blockIdx.z;
+    int32_t* lab = pv.lab[view];
+    int32_t* root = pv.root[view];
+    int32_t* sz = pv.sz[view];
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int r = -1;
+    if (i < n && lab[i] >= 0) r = uf_find(lab, i, err);
+    if (i < n) root[i] = r;
+    unsigned peers = __match_any_sync(0xffffffffu, r);
+    int leader = __ffs(peers) - 1;
+    if (r >= 0 && (threadIdx.x & 31) == leader) atomicAdd(&sz[r], __popc(peers));
+}
+
+__global__ void k_uf_apply_v(PostViews pv, int n, int min_size) {
+    const int view = blockIdx.z;
+    float* D = pv.cur[view];
+    const int32_t* root = pv.root[view];
+    const int32_t* sz = pv.sz[view];
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int r = root[i];
+    if (r >= 0 && sz[r] < min_size) D[i] = -1.0f;
+}
+
 __global__ void k_uf_apply(float* D, const int32_t* __restrict__ root, const int32_t* sz, int n, int min_size) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -115,7 +186,9 @@ __global__ void k_uf_apply(float* D, const int32_t* __restrict__ root, const int
 // between them no longer than `gap` -> fill.  Equivalent to the serial
 // per-line scan because filled runs never touch the pixels that bound
 // other runs.  S = pass input, O = pass output.
-__global__ void k_gap_px(const float* __restrict__ S, float* __restrict__ O, int W, int H, int gap, int horizontal) {
+__global__ void k_gap_px(PostViews pv, int W, int H, int gap, int horizontal) {
+    const float* __restrict__ S = pv.cur[blockIdx.z];
+    float* __restrict__ O = pv.nxt[blockIdx.z];
     int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
     if (u >= W || v >= H) return;
     size_t i = size_t(v) * W + u;
@@ -139,7 +212,8 @@ __global__ void k_gap_px(const float* __restrict__ S, float* __restrict__ O, int
 
 // horizontal = 1: one thread per row; 0: one thread per column (used for
 // gap widths too large for the per-pixel search).
-__global__ void k_gap(float* D, int W, int H, int gap, int horizontal) {
+__global__ void k_gap(PostViews pv, int W, int H, int gap, int horizontal) {
+    float* D = pv.cur[blockIdx.z];
     int l = blockIdx.x * blockDim.x + threadIdx.x;
     int lines = horizontal ? H : W, len = horizontal ? W : H;
     if (l >= lines) return;
@@ -158,91 +232,112 @@ __global__ void k_gap(float* D, int W, int H, int gap, int horizontal) {
     }
 }
 
-__global__ void k_mean(const float* __restrict__ S, float* __restrict__ D, int W, int H) {
-    int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
-    if (u >= W || v >= H) return;
-    float dp = S[size_t(v) * W + u];
-    float out = dp;
-    if (dp >= 0) {
-        float num = 0.0f, den = 0.0f;
-        for (int dy = -2; dy <= 2; ++dy)
-            for (int dx = -2; dx <= 2; ++dx) {
-                int x = u + dx, y = v + dy;
-                if (x < 0 || x >= W || y < 0 || y >= H) continue;
-                float dq = S[size_t(y) * W + x];
-                if (dq < 0) continue;
-                float diff = __fsub_rn(dq, dp);
-                float w = __fdiv_rn(1.0f, __fmaf_rn(diff, diff, 1.0f));
-                num = __fmaf_rn(w, dq, num);
-                den = __fadd_rn(den, w);
-            }
-        out = __fdiv_rn(num, den);
+// Adaptive mean and/or median in one pass over a 32x8 output tile: the
+// input tile (halo 3) and the mean of the tile plus halo 1 live in shared
+// memory; the median reads the mean.  Same arithmetic as k_mean/k_median.
+template <bool MEAN, bool MEDIAN>
+__global__ void __launch_bounds__(256) k_mean_median(PostViews pv, int W, int H) {
+    constexpr int TXo = 32, TYo = 8, HX = TXo + 6, HY = TYo + 6, MX = TXo + 2, MY = TYo + 2;
+    __shared__ float in[HY][HX];
+    __shared__ float mn[MY][MX];
+    const float* __restrict__ S = pv.cur[blockIdx.z];
+    float* __restrict__ O = pv.nxt[blockIdx.z];
+    const int u0 = blockIdx.x * TXo, v0 = blockIdx.y * TYo, tid = threadIdx.x;
+    for (int i = tid; i < HY * HX; i += 256) {
+        int r = i / HX, c = i % HX;
+        int x = u0 - 3 + c, y = v0 - 3 + r;
+        in[r][c] = (x >= 0 && x < W && y >= 0 && y < H) ? S[size_t(y) * W + x] : -2.0f;   // -2: outside
     }
-    D[size_t(v) * W + u] = out;
-}
-
-__global__ void k_median(const float* __restrict__ S, float* __restrict__ D, int W, int H) {
-    int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
-    if (u >= W || v >= H) return;
-    float c = S[size_t(v) * W + u];
-    float out = c;
-    if (c >= 0) {
-        float a[9];
-        int n = 0;
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) {
-                int x = u + dx, y = v + dy;
-                if (x < 0 || x >= W || y < 0 || y >= H) continue;
-                float q = S[size_t(y) * W + x];
-                if (q >= 0) a[n++] = q;
-            }
-        for (int i = 1; i < n; ++i) {   // insertion sort, n <= 9
-            float x = a[i];
-            int j = i - 1;
-            while (j >= 0 && a[j] > x) { a[j + 1] = a[j]; --j; }
-            a[j + 1] = x;
+    __syncthreads();
+    for (int i = tid; i < MY * MX; i += 256) {
+        int r = i / MX, c = i % MX;       // mean at (u0-1+c, v0-1+r) = in[r+2][c+2]
+        float dp = in[r + 2][c + 2];
+        float out = dp;
+        if (MEAN && dp >= 0) {
+            float num = 0.0f, den = 0.0f;
+            for (int dy = -2; dy <= 2; ++dy)
+                for (int dx = -2; dx <= 2; ++dx) {
+                    float dq = in[r + 2 + dy][c + 2 + dx];
+                    if (dq < 0) continue;      // invalid (-1) or outside (-2)
+                    float diff = __fsub_rn(dq, dp);
+                    float w = __fdiv_rn(1.0f, __fmaf_rn(diff, diff, 1.0f));
+                    num = __fmaf_rn(w, dq, num);
+                    den = __fadd_rn(den, w);
+                }
+            out = __fdiv_rn(num, den);
         }
-        out = a[(n - 1) / 2];
+        mn[r][c] = out;
     }
-    D[size_t(v) * W + u] = out;
+    __syncthreads();
+    {
+        int ty = tid / TXo, tx = tid % TXo;
+        int u = u0 + tx, v = v0 + ty;
+        if (u < W && v < H) {
+            float c = mn[ty + 1][tx + 1];
+            float out = c;
+            if (MEDIAN && c >= 0) {
+                float a[9];
+                int n = 0;
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        float q = mn[ty + 1 + dy][tx + 1 + dx];
+                        if (q >= 0) a[n++] = q;
+                    }
+                for (int i = 1; i < n; ++i) {
+                    float x = a[i];
+                    int j = i - 1;
+                    while (j >= 0 && a[j] > x) { a[j + 1] = a[j]; --j; }
+                    a[j + 1] = x;
+                }
+                out = a[(n - 1) / 2];
+            }
+            O[size_t(v) * W + u] = out;
+        }
+    }
 }
 
 }  // namespace
 
-cudaError_t launch_post(float* disp, float* tmp, int32_t* lab, int32_t* size, const Geom& g, const DevParams& p,
-                        bool median, bool adaptive_mean, unsigned* err, cudaStream_t st, int* nlaunch) {
+cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams& p, bool median,
+                        bool adaptive_mean, unsigned* err, cudaStream_t st, int* nlaunch) {
     const int W = g.W, H = g.H, n = W * H;
     const int tb = 256;
     int launched = 0;
-    const dim3 grid2((W + tb - 1) / tb, H);
+    const dim3 grid2((W + tb - 1) / tb, H, nviews);
+    auto flip = [&]() {
+        for (int k = 0; k < 2; ++k) { float* t = pv.cur[k]; pv.cur[k] = pv.nxt[k]; pv.nxt[k] = t; }
+    };
     if (p.speckle_size > 0) {
-        k_uf_init<<<grid2, tb, 0, st>>>(disp, lab, size, W, H, p.speckle_sim_threshold);
-        k_uf_union<<<grid2, tb, 0, st>>>(disp, lab, W, H, p.speckle_sim_threshold, err);
-        int32_t* root = reinterpret_cast<int32_t*>(tmp);   // tmp is free during speckle removal
-        k_uf_count<<<(n + tb - 1) / tb, tb, 0, st>>>(lab, root, size, n, err);
-        k_uf_apply<<<(n + tb - 1) / tb, tb, 0, st>>>(disp, root, size, n, p.speckle_size);
+        const int wpb = 8;
+        k_uf_init_rows<<<dim3((H + wpb - 1) / wpb, 1, nviews), 32 * wpb, 0, st>>>(pv, W, H, p.speckle_sim_threshold);
+        k_uf_union_v<<<grid2, tb, 0, st>>>(pv, W, H, p.speckle_sim_threshold, err);
+        k_uf_count_v<<<dim3((n + tb - 1) / tb, 1, nviews), tb, 0, st>>>(pv, n, err);
+        k_uf_apply_v<<<dim3((n + tb - 1) / tb, 1, nviews), tb, 0, st>>>(pv, n, p.speckle_size);
         launched += 4;
     }
     if (p.ipol_gap_width > 0) {
         if (p.ipol_gap_width <= 64) {
-            k_gap_px<<<grid2, tb, 0, st>>>(disp, tmp, W, H, p.ipol_gap_width, 1);
-            k_gap_px<<<grid2, tb, 0, st>>>(tmp, disp, W, H, p.ipol_gap_width, 0);
+            k_gap_px<<<grid2, tb, 0, st>>>(pv, W, H, p.ipol_gap_width, 1);
+            flip();
+            k_gap_px<<<grid2, tb, 0, st>>>(pv, W, H, p.ipol_gap_width, 0);
+            flip();
         } else {
-            k_gap<<<(H + 127) / 128, 128, 0, st>>>(disp, W, H, p.ipol_gap_width, 1);
-            k_gap<<<(W + 127) / 128, 128, 0, st>>>(disp, W, H, p.ipol_gap_width, 0);
+            k_gap<<<dim3((H + 127) / 128, 1, nviews), 128, 0, st>>>(pv, W, H, p.ipol_gap_width, 1);
+            k_gap<<<dim3((W + 127) / 128, 1, nviews), 128, 0, st>>>(pv, W, H, p.ipol_gap_width, 0);
         }
         launched += 2;
     }
-    if (adaptive_mean) {
-        k_mean<<<dim3((W + tb - 1) / tb, H), tb, 0, st>>>(disp, tmp, W, H);
-        cudaMemcpyAsync(disp, tmp, size_t(n) * sizeof(float), cudaMemcpyDeviceToDevice, st);
+    if (adaptive_mean || median) {
+        dim3 grid((W + 31) / 32, (H + 7) / 8, nviews);
+        if (adaptive_mean && median) k_mean_median<true, true><<<grid, 256, 0, st>>>(pv, W, H);
+        else if (adaptive_mean) k_mean_median<true, false><<<grid, 256, 0, st>>>(pv, W, H);
+        else k_mean_median<false, true><<<grid, 256, 0, st>>>(pv, W, H);
+        flip();
         launched += 1;
     }
-    if (median) {
-        k_median<<<dim3((W + tb - 1) / tb, H), tb, 0, st>>>(disp, tmp, W, H);
-        cudaMemcpyAsync(disp, tmp, size_t(n) * sizeof(float), cudaMemcpyDeviceToDevice, st);
-        launched += 1;
-    }
+    for (int k = 0; k < nviews; ++k)
+        if (pv.cur[k] != pv.out[k])
+            cudaMemcpyAsync(pv.out[k], pv.cur[k], size_t(n) * sizeof(float), cudaMemcpyDeviceToDevice, st);
     if (nlaunch) *nlaunch += launched;
     return cudaGetLastError();
 }

@@ -99,10 +99,12 @@ __device__ __forceinline__ int sweep_candidate(const uint4* self_m2, const uint4
     return -1;
 }
 
-// Block: 256 threads (8 warps).  grid.x = segments per candidate row,
-// grid.y = candidate rows.  SMEM: stage the four rows when they fit.
+// Block: SWEEP_THREADS threads (one candidate per warp at a time).  grid.x =
+// segments per candidate row, grid.y = candidate rows.  SMEM: stage the four
+// rows when they fit.
+constexpr int SWEEP_THREADS = 1024;
 template <bool SMEM>
-__global__ void __launch_bounds__(256) k_support_sweep(const uint4* __restrict__ desc0,
+__global__ void __launch_bounds__(SWEEP_THREADS) k_support_sweep(const uint4* __restrict__ desc0,
                                                        const uint4* __restrict__ desc1,
                                                        int32_t* __restrict__ can_out, Geom g, DevParams p,
                                                        int seg) {
@@ -360,9 +362,9 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
     dim3 grid(segs, rows);
     if (smem <= 200 * 1024) {
         cudaFuncSetAttribute(k_support_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        k_support_sweep<true><<<grid, 256, smem, st>>>(desc0, desc1, can_lr, g, p, seg);
+        k_support_sweep<true><<<grid, SWEEP_THREADS, smem, st>>>(desc0, desc1, can_lr, g, p, seg);
     } else {
-        k_support_sweep<false><<<grid, 256, 0, st>>>(desc0, desc1, can_lr, g, p, seg);
+        k_support_sweep<false><<<grid, SWEEP_THREADS, 0, st>>>(desc0, desc1, can_lr, g, p, seg);
     }
     k_incon<<<dim3((g.cw + 127) / 128, g.ch), 128, 0, st>>>(can_lr, can, g, p);
     {

@@ -69,9 +69,20 @@ cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const unsigned 
 cudaError_t launch_lr(const float* d0, const float* d1, float* o0, float* o1, const Geom& g, int lr_threshold,
                       cudaStream_t st);
 
-// Post-filters on one disparity image in place (tmp: W*H floats, lab/size:
-// W*H int32 each).  Returns the number of kernels launched via *nlaunch.
-cudaError_t launch_post(float* disp, float* tmp, int32_t* lab, int32_t* size, const Geom& g, const DevParams& p,
-                        bool median, bool adaptive_mean, unsigned* err, cudaStream_t st, int* nlaunch);
+// Buffers of the post-filter chain, per view: the filters ping-pong between
+// cur and nxt (the chain starts in cur; the result is copied to out if it
+// does not end there); lab/root/sz are union-find scratch (W*H int32 each).
+struct PostViews {
+    float* cur[2];
+    float* nxt[2];
+    float* out[2];
+    int32_t* lab[2];
+    int32_t* root[2];
+    int32_t* sz[2];
+};
+
+// Post-filters on nviews (1 or 2) disparity images.
+cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams& p, bool median, bool adaptive_mean,
+                        unsigned* err, cudaStream_t st, int* nlaunch);
 
 }  // namespace elas
