@@ -48,7 +48,73 @@ enum : unsigned {
     ERRF_HASH = 2u,         // adjacency hash table overflow / non-manifold edge
     ERRF_FLIP_LIMIT = 4u,   // edge flipping did not converge within its round limit
     ERRF_TRI_COUNT = 8u,    // triangle count mismatch (Euler)
+    ERRF_TMA_TIMEOUT = 16u, // a bulk copy did not complete within its bounded wait
 };
+
+#if defined(__CUDACC__)
+// Sum of absolute differences of two 16-byte descriptors: four
+// vabsdiff4.u32.u32.u32.add (byte-wise |a-b| summed into the accumulator),
+// the fastest of the packed-byte forms on sm_100a.
+__device__ __forceinline__ int sad16(const uint4& a, const uint4& b, int acc = 0) {
+    unsigned r = unsigned(acc);
+    asm("vabsdiff4.u32.u32.u32.add %0, %1, %2, %0;" : "+r"(r) : "r"(a.x), "r"(b.x));
+    asm("vabsdiff4.u32.u32.u32.add %0, %1, %2, %0;" : "+r"(r) : "r"(a.y), "r"(b.y));
+    asm("vabsdiff4.u32.u32.u32.add %0, %1, %2, %0;" : "+r"(r) : "r"(a.z), "r"(b.z));
+    asm("vabsdiff4.u32.u32.u32.add %0, %1, %2, %0;" : "+r"(r) : "r"(a.w), "r"(b.w));
+    return int(r);
+}
+
+// sum over the 16 bytes of |b - 128| (the texture measure of the reference)
+__device__ __forceinline__ int texture16(const uint4& a) {
+    return sad16(a, make_uint4(0x80808080u, 0x80808080u, 0x80808080u, 0x80808080u));
+}
+
+// ---- bulk (TMA) copies global -> shared, completed on an mbarrier ----
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return uint32_t(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// One bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+// Copy `bytes` in chunks of at most 32 KiB; call from one thread after
+// mbar_expect_tx(bar, bytes).
+__device__ __forceinline__ void bulk_g2s_chunked(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    const unsigned chunk = 32768;
+    for (unsigned off = 0; off < bytes; off += chunk) {
+        unsigned n = bytes - off < chunk ? bytes - off : chunk;
+        bulk_g2s(static_cast<char*>(dst) + off, static_cast<const char*>(src) + off, n, bar);
+    }
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for phase `parity` of the barrier: false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, int limit) {
+    for (int i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+constexpr int MBAR_WAIT_LIMIT = 1 << 22;
+#endif
 
 HD int imin(int a, int b) { return a < b ? a : b; }
 HD int imax(int a, int b) { return a > b ? a : b; }

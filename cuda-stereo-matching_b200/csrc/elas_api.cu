@@ -42,7 +42,7 @@ struct elas_handle {
     int32_t *uvd = nullptr, *x0 = nullptr, *x1 = nullptr, *y = nullptr;
     uint32_t *gtmp0 = nullptr, *gtmp1 = nullptr, *grid0 = nullptr, *grid1 = nullptr;
     DelDev del[2]{};
-    unsigned long long *prior0 = nullptr, *prior1 = nullptr;
+    uint32_t *prior0 = nullptr, *prior1 = nullptr;
     float *raw0 = nullptr, *raw1 = nullptr, *lr0 = nullptr, *lr1 = nullptr;
     float *out0 = nullptr, *out1 = nullptr;
     float* tmp[2] = {nullptr, nullptr};          // post-filter ping-pong buffer per view
@@ -138,6 +138,14 @@ Geom geom_of(int W, int H, const elas_params& p) {
     return g;
 }
 
+// Bits of the packed prior word that hold d_plane: enough for
+// [0, disp_max + plane_radius + 1]; the rest numbers the triangle.
+int prior_shift(const Geom& g, const DevParams& dp) {
+    int need = g.D + dp.plane_radius + 2, b = 1;
+    while ((1 << b) < need) ++b;
+    return b;
+}
+
 // Lay out (and, if `base` is non-null, assign) every workspace buffer.
 size_t layout(elas_handle* h, const Geom& g, char* base) {
     size_t off = 0;
@@ -196,8 +204,8 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         D.Tmax = int(tmax);
         D.Hmax = uint32_t(hmax);
     }
-    h->prior0 = (unsigned long long*)take(px * 8);
-    h->prior1 = (unsigned long long*)take(px * 8);
+    h->prior0 = (uint32_t*)take(px * 4);
+    h->prior1 = (uint32_t*)take(px * 4);
     h->raw0 = (float*)take(px * 4);
     h->raw1 = (float*)take(px * 4);
     h->lr0 = (float*)take(px * 4);
@@ -248,6 +256,15 @@ int check_dims(elas_handle* h, const int32_t* dims, int& W, int& H) {
     if (W > 14000 || H > 16384) return fail(h, ELAS_ERR_UNSUPPORTED, "images wider than 14000 or taller than 16384");
     if (W / h->params.candidate_stepsize > 2048)
         return fail(h, ELAS_ERR_UNSUPPORTED, "more than 2048 candidates per lattice row");
+    {
+        Geom g = geom_of(W, H, h->params);
+        DevParams dp = dev_params(h->params);
+        int64_t tmax = 2LL * g.cw * g.ch + 16;
+        if ((tmax + 1) >> (32 - prior_shift(g, dp)) != 0)
+            return fail(h, ELAS_ERR_UNSUPPORTED, "too many candidate points for the packed plane prior");
+        if (dense_smem_bytes(g) > 220 * 1024)
+            return fail(h, ELAS_ERR_UNSUPPORTED, "image too wide for the dense row in shared memory");
+    }
     return ELAS_OK;
 }
 
@@ -267,7 +284,7 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     CK(launch_descriptor(img0, img1, h->desc0, h->desc1, W, H, st));
     n += 1;
     CK(mark(ELAS_TIME_SUPPORT));
-    CK(launch_support(h->desc0, h->desc1, h->can_lr, nullptr, h->can, g, dp, h->num_sms, st));
+    CK(launch_support(h->desc0, h->desc1, h->can_lr, nullptr, h->can, g, dp, h->num_sms, h->err, st));
     n += 4;
     CK(mark(ELAS_TIME_COMPACT));
     CK(launch_compact(h->can, h->row_cnt, h->row_off, h->uvd, h->x0, h->x1, h->y, g, st));
@@ -280,10 +297,11 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
                        st, &n));
     CK(mark(ELAS_TIME_PRIOR));
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
-                    h->prior0, h->prior1, g, h->num_sms, st));
+                    h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1, h->num_sms, st));
     n += 1;
     CK(mark(ELAS_TIME_DENSE));
-    CK(launch_dense(h->desc0, h->desc1, h->prior0, h->prior1, h->grid0, h->grid1, h->raw0, h->raw1, g, dp, st));
+    CK(launch_dense(h->desc0, h->desc1, h->prior0, h->prior1, h->grid0, h->grid1, h->raw0, h->raw1, g, dp,
+                    prior_shift(g, dp), h->err, st));
     n += 1;
     CK(mark(ELAS_TIME_LR));
     CK(launch_lr(h->raw0, h->raw1, h->lr0, h->lr1, g, p.lr_threshold, st));
@@ -577,11 +595,15 @@ int elas_b200_get_stage(elas_handle* h, int stage, void* dst, size_t bytes, size
     case ELAS_STAGE_TRI_LEFT: CK(cudaMemcpy(dst, h->del[0].tri, need, cudaMemcpyDeviceToHost)); break;
     case ELAS_STAGE_TRI_RIGHT: CK(cudaMemcpy(dst, h->del[1].tri, need, cudaMemcpyDeviceToHost)); break;
     case ELAS_STAGE_PRIOR_LEFT: case ELAS_STAGE_PRIOR_RIGHT: {
-        std::vector<unsigned long long> pk(px);
-        CK(cudaMemcpy(pk.data(), stage == ELAS_STAGE_PRIOR_LEFT ? h->prior0 : h->prior1, px * 8,
+        std::vector<uint32_t> pk(px);
+        CK(cudaMemcpy(pk.data(), stage == ELAS_STAGE_PRIOR_LEFT ? h->prior0 : h->prior1, px * 4,
                       cudaMemcpyDeviceToHost));
+        const int sh = prior_shift(g, dev_params(h->params));
         int32_t* o = (int32_t*)dst;
-        for (size_t i = 0; i < px; ++i) o[i] = (pk[i] >> 32) ? int32_t(uint32_t(pk[i])) : -1;
+        for (size_t i = 0; i < px; ++i) {
+            int32_t d = int32_t(pk[i] & ((1u << sh) - 1u));
+            o[i] = ((pk[i] >> sh) != 0 && d > 0) ? d : -1;
+        }
         break;
     }
     case ELAS_STAGE_DISP_LEFT: CK(cudaMemcpy(dst, h->raw0, need, cudaMemcpyDeviceToHost)); break;

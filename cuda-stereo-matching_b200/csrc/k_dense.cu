@@ -7,8 +7,10 @@
 // lanes split the triangle's columns.  A pixel covered by more than one
 // triangle (rounding at shared vertices) must keep the last triangle in
 // list order, as a sequential rasteriser would; the prior is therefore
-// written with a 64-bit atomicMax of (triangle+1) << 32 | d_plane, which
-// makes the result independent of scheduling.
+// written with a 32-bit atomicMax of (triangle+1) << pshift | d_plane, which
+// makes the result independent of scheduling.  d_plane is stored clamped to
+// [0, disp_max + plane_radius + 1] (0 standing for every d_plane <= 0): the
+// dense step treats all values beyond either end alike.
 //
 // Floating point follows the reference expressions with the contraction
 // nvcc applies to them made explicit (fma where a*b+c occurs); the CPU
@@ -27,14 +29,6 @@
 namespace elas {
 
 namespace {
-
-__device__ __forceinline__ int sad16(const uint4& a, const uint4& b) {
-    return int(__vsadu4(a.x, b.x) + __vsadu4(a.y, b.y) + __vsadu4(a.z, b.z) + __vsadu4(a.w, b.w));
-}
-__device__ __forceinline__ int texture16(const uint4& a) {
-    const unsigned k = 0x80808080u;
-    return int(__vsadu4(a.x, k) + __vsadu4(a.y, k) + __vsadu4(a.z, k) + __vsadu4(a.w, k));
-}
 
 // kerSolve with the row update written as fma(-y, dum, x).
 __device__ bool solve3(double A[3][3], double B[3]) {
@@ -120,19 +114,17 @@ __device__ void setup_triangle(const int32_t* tri, const int32_t* can, const int
 }
 
 __device__ __forceinline__ void raster_part(const Raster& R, int u0, int u1, float ea, float eb, int W, int H,
-                                            unsigned long long tag, unsigned long long* prior, int lane) {
+                                            uint32_t tag, int dcap, uint32_t* prior, int lane) {
     for (int u = imax(u0, 0) + lane; u < imin(u1, W); u += 32) {
         float fu = float(u);
         int v1 = int(__float2uint_rz(__fmaf_rn(R.AC_a, fu, R.AC_b)));
         int v2 = int(__float2uint_rz(__fmaf_rn(ea, fu, eb)));
-        int va = imin(v1, v2), vb = imax(v1, v2);
-        float au = __fmul_rn(R.pa, fu);
-        (void)au;
+        int va = imax(imin(v1, v2), 0), vb = imin(imax(v1, v2), H);
         for (int v = va; v < vb; ++v) {
-            if (v < 0 || v >= H) continue;
             float dp = __fadd_rn(__fmaf_rn(R.pa, fu, __fmul_rn(R.pb, float(v))), R.pc);
             int d = __float2int_rz(dp);
-            atomicMax(&prior[size_t(v) * W + u], tag | (unsigned long long)uint32_t(d));
+            d = d <= 0 ? 0 : (d > dcap ? dcap : d);
+            atomicMax(&prior[size_t(v) * W + u], tag | uint32_t(d));
         }
     }
 }
@@ -141,7 +133,7 @@ __device__ __forceinline__ void raster_part(const Raster& R, int u0, int u1, flo
 __global__ void __launch_bounds__(256) k_prior(const int32_t* __restrict__ tri0, const int32_t* __restrict__ tri1,
                                                const int32_t* __restrict__ ctr0, const int32_t* __restrict__ ctr1,
                                                const int32_t* __restrict__ can, const int32_t* __restrict__ uvd,
-                                               unsigned long long* prior0, unsigned long long* prior1, Geom g) {
+                                               uint32_t* prior0, uint32_t* prior1, Geom g, int pshift, int dcap) {
     const int lane = threadIdx.x & 31;
     const int T0 = ctr0[0], T1 = ctr1[0];
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -152,68 +144,115 @@ __global__ void __launch_bounds__(256) k_prior(const int32_t* __restrict__ tri0,
         const int32_t* tri = (right ? tri1 : tri0) + 3 * size_t(t);
         Raster R;
         setup_triangle(tri, can, uvd, g.cw, g.step, right, R);
-        unsigned long long tag = (unsigned long long)(t + 1) << 32;
-        unsigned long long* prior = right ? prior1 : prior0;
-        if (int(R.A_u) != int(R.B_u)) raster_part(R, int(R.A_u), int(R.B_u), R.AB_a, R.AB_b, g.W, g.H, tag, prior, lane);
-        if (int(R.B_u) != int(R.C_u)) raster_part(R, int(R.B_u), int(R.C_u), R.BC_a, R.BC_b, g.W, g.H, tag, prior, lane);
+        uint32_t tag = uint32_t(t + 1) << pshift;
+        uint32_t* prior = right ? prior1 : prior0;
+        if (int(R.A_u) != int(R.B_u))
+            raster_part(R, int(R.A_u), int(R.B_u), R.AB_a, R.AB_b, g.W, g.H, tag, dcap, prior, lane);
+        if (int(R.B_u) != int(R.C_u))
+            raster_part(R, int(R.B_u), int(R.C_u), R.BC_a, R.BC_b, g.W, g.H, tag, dcap, prior, lane);
     }
 }
 
-// blockIdx.x = row, blockIdx.y = view (0 left, 1 right).
+// Candidate-list entries per grid cell kept in shared memory; cells with
+// more candidates walk their bitset instead.
+constexpr int LMAX = 48;
+
+// blockIdx.x = row, blockIdx.y = view (0 left, 1 right).  The other view's
+// descriptor row arrives by bulk copy (TMA) while the CTA expands the
+// candidate lists of the row's grid cells into shared memory.
 __global__ void __launch_bounds__(512) k_dense(const uint4* __restrict__ desc0, const uint4* __restrict__ desc1,
-                                               const unsigned long long* __restrict__ prior0,
-                                               const unsigned long long* __restrict__ prior1,
+                                               const uint32_t* __restrict__ prior0, const uint32_t* __restrict__ prior1,
                                                const uint32_t* __restrict__ grid0, const uint32_t* __restrict__ grid1,
                                                float* __restrict__ disp0, float* __restrict__ disp1, Geom g,
-                                               DevParams p) {
-    extern __shared__ uint4 row[];
+                                               DevParams p, int pshift, unsigned* err) {
+    extern __shared__ __align__(128) uint8_t sm[];
+    __shared__ uint64_t bar;
     const int v = blockIdx.x;
     const bool right = blockIdx.y != 0;
     const int W = g.W, H = g.H;
+    uint4* row = reinterpret_cast<uint4*>(sm);
+    int16_t* lst = reinterpret_cast<int16_t*>(sm + size_t(W) * 16);
+    uint8_t* lcnt = reinterpret_cast<uint8_t*>(lst + size_t(g.gw) * LMAX);
     const uint4* self = (right ? desc1 : desc0) + size_t(v) * W;
     const uint4* other = (right ? desc0 : desc1) + size_t(v) * W;
-    const unsigned long long* prior = (right ? prior1 : prior0) + size_t(v) * W;
+    const uint32_t* prior = (right ? prior1 : prior0) + size_t(v) * W;
     const uint32_t* grid = right ? grid1 : grid0;
     float* disp = (right ? disp1 : disp0) + size_t(v) * W;
-    for (int i = threadIdx.x; i < W; i += blockDim.x) row[i] = other[i];
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        mbar_expect_tx(&bar, unsigned(W) * 16u);
+        bulk_g2s_chunked(row, other, unsigned(W) * 16u, &bar);
+    }
+    const int gy = floordiv(v, g.gs);
+    for (int c = tid; c < g.gw; c += blockDim.x) {
+        const uint32_t* cell = grid + (size_t(gy) * g.gw + c) * g.words;
+        int n = 0;
+        for (int w = 0; w < g.words; ++w) {
+            uint32_t bits = cell[w];
+            while (bits) {
+                int d = 32 * w + __ffs(bits) - 1;
+                bits &= bits - 1;
+                if (n < LMAX) lst[c * LMAX + n] = int16_t(d);
+                ++n;
+            }
+        }
+        lcnt[c] = uint8_t(n > LMAX ? 255 : n);
+    }
     __syncthreads();
+    if (!mbar_wait_bounded(&bar, 0, MBAR_WAIT_LIMIT)) {
+        if (tid == 0) atomicOr(err, ERRF_TMA_TIMEOUT);
+        mbar_wait_bounded(&bar, 0, MBAR_WAIT_LIMIT);   // let the copy in flight land before exiting
+        return;
+    }
     const int dir = right ? 1 : -1;
     const int r = p.plane_radius;
     const bool v_ok = v > 3 && v < H - 3;
-    const int gy = floordiv(v, g.gs);
-    for (int u = threadIdx.x; u < W; u += blockDim.x) {
+    const uint32_t dmask = (1u << pshift) - 1u;
+    for (int u = tid; u < W; u += blockDim.x) {
         float out = -1.0f;
-        if (v_ok && u > 3 && u < W - 3) {
-            unsigned long long pk = prior[u];
-            int dp = int(uint32_t(pk & 0xffffffffull));
-            if ((pk >> 32) != 0 && dp > 0) {
-                uint4 I1 = self[u];
-                if (texture16(I1) >= p.match_texture) {
-                    int dpmin = imax(dp - r, 0);
-                    long long dpmax_l = (long long)dp + r;
-                    int dpmax = dpmax_l > g.D ? g.D : int(dpmax_l);
-                    const uint32_t* cell = grid + (size_t(gy) * g.gw + floordiv(u, g.gs)) * g.words;
-                    int min_val = 10000, min_d = -1;
+        const uint32_t pk = prior[u];
+        const int dp = int(pk & dmask);
+        if (v_ok && u > 3 && u < W - 3 && (pk >> pshift) != 0 && dp > 0) {
+            const uint4 I1 = self[u];
+            if (p.match_texture <= 0 || texture16(I1) >= p.match_texture) {
+                const int dpmin = imax(dp - r, 0);
+                const int dpmax = imin(dp + r, g.D);
+                const int c = floordiv(u, g.gs);
+                int min_val = 10000, min_d = -1;
+                const int n = lcnt[c];
+                if (n != 255) {
+                    const int16_t* L = lst + c * LMAX;
+                    for (int i = 0; i < n; ++i) {
+                        const int d = L[i];
+                        if (d >= dpmin && d <= dpmax) continue;
+                        const int uw = u + dir * d;
+                        if (uw < 3 || uw >= W - 3) continue;
+                        const int e = sad16(I1, row[uw]);
+                        if (e < min_val) { min_val = e; min_d = d; }
+                    }
+                } else {
+                    const uint32_t* cell = grid + (size_t(gy) * g.gw + c) * g.words;
                     for (int w = 0; w < g.words; ++w) {
                         uint32_t bits = cell[w];
                         while (bits) {
-                            int d = 32 * w + __ffs(bits) - 1;
+                            const int d = 32 * w + __ffs(bits) - 1;
                             bits &= bits - 1;
                             if (d >= dpmin && d <= dpmax) continue;
-                            int uw = u + dir * d;
+                            const int uw = u + dir * d;
                             if (uw < 3 || uw >= W - 3) continue;
-                            int e = sad16(I1, row[uw]);
+                            const int e = sad16(I1, row[uw]);
                             if (e < min_val) { min_val = e; min_d = d; }
                         }
                     }
-                    for (int d = dpmin; d <= dpmax; ++d) {
-                        int uw = u + dir * d;
-                        if (uw < 3 || uw >= W - 3) continue;
-                        int e = p.penalty[abs(d - dp)] + sad16(I1, row[uw]);
-                        if (e < min_val) { min_val = e; min_d = d; }
-                    }
-                    out = min_d >= 0 ? float(min_d) : -1.0f;
                 }
+                for (int d = dpmin; d <= dpmax; ++d) {
+                    const int uw = u + dir * d;
+                    if (uw < 3 || uw >= W - 3) continue;
+                    const int e = sad16(I1, row[uw], p.penalty[d > dp ? d - dp : dp - d]);
+                    if (e < min_val) { min_val = e; min_d = d; }
+                }
+                out = min_d >= 0 ? float(min_d) : -1.0f;
             }
         }
         disp[u] = out;
@@ -248,23 +287,26 @@ __global__ void k_lr(const float* __restrict__ D1, const float* __restrict__ D2,
 }  // namespace
 
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
-                         int Tmax, const int32_t* can, const int32_t* uvd, unsigned long long* prior0,
-                         unsigned long long* prior1, const Geom& g, int num_sms, cudaStream_t st) {
-    size_t n = size_t(g.W) * g.H * sizeof(unsigned long long);
+                         int Tmax, const int32_t* can, const int32_t* uvd, uint32_t* prior0, uint32_t* prior1,
+                         const Geom& g, int pshift, int dcap, int num_sms, cudaStream_t st) {
+    size_t n = size_t(g.W) * g.H * sizeof(uint32_t);
     cudaMemsetAsync(prior0, 0, n, st);
     cudaMemsetAsync(prior1, 0, n, st);
     int blocks = imax(1, imin(16 * num_sms, (2 * Tmax + 7) / 8));
-    k_prior<<<blocks, 256, 0, st>>>(tri0, tri1, ctr0, ctr1, can, uvd, prior0, prior1, g);
+    k_prior<<<blocks, 256, 0, st>>>(tri0, tri1, ctr0, ctr1, can, uvd, prior0, prior1, g, pshift, dcap);
     return cudaGetLastError();
 }
 
-cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const unsigned long long* prior0,
-                         const unsigned long long* prior1, const uint32_t* grid0, const uint32_t* grid1,
-                         float* disp0, float* disp1, const Geom& g, const DevParams& p, cudaStream_t st) {
-    size_t smem = size_t(g.W) * sizeof(uint4);
+size_t dense_smem_bytes(const Geom& g) { return size_t(g.W) * 16 + size_t(g.gw) * (LMAX * 2 + 1); }
+
+cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t* prior0, const uint32_t* prior1,
+                         const uint32_t* grid0, const uint32_t* grid1, float* disp0, float* disp1, const Geom& g,
+                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st) {
+    size_t smem = dense_smem_bytes(g);
     cudaFuncSetAttribute(k_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     int threads = g.W >= 512 ? 512 : ((g.W + 31) / 32) * 32;
-    k_dense<<<dim3(g.H, 2), threads, smem, st>>>(desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p);
+    k_dense<<<dim3(g.H, 2), threads, smem, st>>>(desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
+                                                  pshift, err);
     return cudaGetLastError();
 }
 

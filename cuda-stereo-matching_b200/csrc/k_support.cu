@@ -11,7 +11,8 @@
 // of both images) in shared memory, so the d-sweep reads shared memory only.
 // A warp sweeps one candidate: lane l takes d = dmin + l + 32k, as the
 // reference's 32-thread block does, and per-lane states are merged with
-// shuffles.  The SAD of a 16-byte descriptor pair is four __vsadu4.
+// shuffles.  The SAD of a 16-byte descriptor pair is four chained
+// vabsdiff4.add; the four rows arrive in shared memory by bulk copy (TMA).
 //
 // Reduction.  The reference keeps (best, second best) per lane with strict
 // '<' and lets lane 0 merge its own registers and then all 32 lanes' pairs
@@ -58,15 +59,6 @@ __device__ __forceinline__ void top2_merge(Top2& a, const Top2& b) {
     }
 }
 
-__device__ __forceinline__ int sad16(const uint4& a, const uint4& b) {
-    return int(__vsadu4(a.x, b.x) + __vsadu4(a.y, b.y) + __vsadu4(a.z, b.z) + __vsadu4(a.w, b.w));
-}
-
-__device__ __forceinline__ int texture16(const uint4& a) {
-    const unsigned k = 0x80808080u;
-    return int(__vsadu4(a.x, k) + __vsadu4(a.y, k) + __vsadu4(a.z, k) + __vsadu4(a.w, k));
-}
-
 // One candidate sweep by a full warp.  self_m2/self_p2: rows v-2/v+2 of the
 // image the candidate lives in; oth_m2/oth_p2: the same rows of the other
 // image.  dir = -1 (left view: u_warp = u - d) or +1 (right view).
@@ -80,8 +72,10 @@ __device__ __forceinline__ int sweep_candidate(const uint4* self_m2, const uint4
     Top2 s{INF_E, 0x7fffffff, 0, INF_E};
     for (int d = dmin + lane; d <= dmax; d += 32) {
         int uw = u + dir * d;
-        int e = sad16(c0, oth_m2[uw - 2]) + sad16(c1, oth_m2[uw + 2]) +
-                sad16(c2, oth_p2[uw - 2]) + sad16(c3, oth_p2[uw + 2]);
+        int e = sad16(c0, oth_m2[uw - 2]);
+        e = sad16(c1, oth_m2[uw + 2], e);
+        e = sad16(c2, oth_p2[uw - 2], e);
+        e = sad16(c3, oth_p2[uw + 2], e);
         top2_add(s, e, (((d - dmin) & 31) << 16) | d);
     }
 #pragma unroll
@@ -107,9 +101,10 @@ template <bool SMEM>
 __global__ void __launch_bounds__(SWEEP_THREADS) k_support_sweep(const uint4* __restrict__ desc0,
                                                        const uint4* __restrict__ desc1,
                                                        int32_t* __restrict__ can_out, Geom g, DevParams p,
-                                                       int seg) {
-    extern __shared__ uint4 rows[];
+                                                       int seg, unsigned* err) {
+    extern __shared__ __align__(128) uint4 rows[];
     __shared__ int res[256];
+    __shared__ uint64_t bar;
     const int W = g.W, H = g.H;
     const int vc = blockIdx.y;
     const int v = vc * g.step;
@@ -119,10 +114,13 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_support_sweep(const uint4* __
     const uint4 *L_m2, *L_p2, *R_m2, *R_p2;
     if (row_ok) {
         if (SMEM) {
-            const uint4* src[4] = {desc0 + size_t(v - 2) * W, desc0 + size_t(v + 2) * W,
-                                   desc1 + size_t(v - 2) * W, desc1 + size_t(v + 2) * W};
-            for (int r = 0; r < 4; ++r)
-                for (int i = threadIdx.x; i < W; i += blockDim.x) rows[r * W + i] = src[r][i];
+            if (threadIdx.x == 0) {
+                const uint4* src[4] = {desc0 + size_t(v - 2) * W, desc0 + size_t(v + 2) * W,
+                                       desc1 + size_t(v - 2) * W, desc1 + size_t(v + 2) * W};
+                mbar_init(&bar, 1);
+                mbar_expect_tx(&bar, 4u * unsigned(W) * 16u);
+                for (int r = 0; r < 4; ++r) bulk_g2s_chunked(rows + r * W, src[r], unsigned(W) * 16u, &bar);
+            }
             L_m2 = rows; L_p2 = rows + W; R_m2 = rows + 2 * W; R_p2 = rows + 3 * W;
         } else {
             L_m2 = desc0 + size_t(v - 2) * W; L_p2 = desc0 + size_t(v + 2) * W;
@@ -130,6 +128,11 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_support_sweep(const uint4* __
         }
     }
     __syncthreads();
+    if (SMEM && row_ok && !mbar_wait_bounded(&bar, 0, MBAR_WAIT_LIMIT)) {
+        if (threadIdx.x == 0) atomicOr(err, ERRF_TMA_TIMEOUT);
+        mbar_wait_bounded(&bar, 0, MBAR_WAIT_LIMIT);   // let the copies in flight land before exiting
+        return;
+    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     // left view: candidates of the segment
     for (int ci = c_begin + warp; ci < c_end; ci += nw) {
@@ -352,7 +355,8 @@ __global__ void k_grid_diffuse(const uint32_t* __restrict__ t0, const uint32_t* 
 }  // namespace
 
 cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_lr, int32_t* can_tmp,
-                           int32_t* can, const Geom& g, const DevParams& p, int num_sms, cudaStream_t st) {
+                           int32_t* can, const Geom& g, const DevParams& p, int num_sms, unsigned* err,
+                           cudaStream_t st) {
     // segments: about 4 CTAs per SM in flight
     int rows = g.ch;
     int segs = imax(1, (4 * num_sms + rows - 1) / imax(rows, 1));
@@ -362,9 +366,9 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
     dim3 grid(segs, rows);
     if (smem <= 200 * 1024) {
         cudaFuncSetAttribute(k_support_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        k_support_sweep<true><<<grid, SWEEP_THREADS, smem, st>>>(desc0, desc1, can_lr, g, p, seg);
+        k_support_sweep<true><<<grid, SWEEP_THREADS, smem, st>>>(desc0, desc1, can_lr, g, p, seg, err);
     } else {
-        k_support_sweep<false><<<grid, SWEEP_THREADS, 0, st>>>(desc0, desc1, can_lr, g, p, seg);
+        k_support_sweep<false><<<grid, SWEEP_THREADS, 0, st>>>(desc0, desc1, can_lr, g, p, seg, err);
     }
     k_incon<<<dim3((g.cw + 127) / 128, g.ch), 128, 0, st>>>(can_lr, can, g, p);
     {

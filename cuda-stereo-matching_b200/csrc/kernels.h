@@ -42,7 +42,8 @@ cudaError_t launch_descriptor(const uint8_t* img0, const uint8_t* img1, uint4* d
                               int W, int H, cudaStream_t st);
 
 cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_lr, int32_t* can_tmp,
-                           int32_t* can, const Geom& g, const DevParams& p, int num_sms, cudaStream_t st);
+                           int32_t* can, const Geom& g, const DevParams& p, int num_sms, unsigned* err,
+                           cudaStream_t st);
 
 cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_off, int32_t* uvd, int32_t* x0,
                            int32_t* x1, int32_t* y, const Geom& g, cudaStream_t st);
@@ -56,15 +57,17 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
 // kernel, or 0 if none fits.
 int cluster_size_for_flip();
 
-// Plane prior of both views: prior[v*W+u] = (triangle+1) << 32 | uint32(d_plane),
-// 0 where no triangle covers the pixel.  Buffers must be zeroed first.
+// Plane prior of both views: prior[v*W+u] = (triangle+1) << pshift | d,
+// d = d_plane clamped to [0, dcap] (dcap = disp_max + plane_radius + 1),
+// 0 where no triangle covers the pixel.  The buffers are zeroed here.
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
-                         int Tmax, const int32_t* can, const int32_t* uvd, unsigned long long* prior0,
-                         unsigned long long* prior1, const Geom& g, int num_sms, cudaStream_t st);
+                         int Tmax, const int32_t* can, const int32_t* uvd, uint32_t* prior0, uint32_t* prior1,
+                         const Geom& g, int pshift, int dcap, int num_sms, cudaStream_t st);
 
-cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const unsigned long long* prior0,
-                         const unsigned long long* prior1, const uint32_t* grid0, const uint32_t* grid1,
-                         float* disp0, float* disp1, const Geom& g, const DevParams& p, cudaStream_t st);
+size_t dense_smem_bytes(const Geom& g);
+cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t* prior0, const uint32_t* prior1,
+                         const uint32_t* grid0, const uint32_t* grid1, float* disp0, float* disp1, const Geom& g,
+                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st);
 
 cudaError_t launch_lr(const float* d0, const float* d1, float* o0, float* o1, const Geom& g, int lr_threshold,
                       cudaStream_t st);

@@ -148,7 +148,9 @@ int elas_b200_process_batch(elas_handle* h, int n,
 #define ELAS_STAGE_GRID_RIGHT    6   /* int32  [gh][gw][disp_max+2] */
 #define ELAS_STAGE_TRI_LEFT      7   /* int32  [t][3] support indices, CCW, smallest index first */
 #define ELAS_STAGE_TRI_RIGHT     8   /* int32  [t][3] */
-#define ELAS_STAGE_PRIOR_LEFT    9   /* int32  [h][w] plane prior d_plane, -1 = not covered */
+#define ELAS_STAGE_PRIOR_LEFT    9   /* int32  [h][w] plane prior d_plane clamped to at most
+                                        disp_max + plane_radius + 1; -1 where no triangle covers
+                                        the pixel or d_plane <= 0 (the dense step skips both) */
 #define ELAS_STAGE_PRIOR_RIGHT  10   /* int32  [h][w] */
 #define ELAS_STAGE_DISP_LEFT    11   /* float  [h][w] dense result before the L/R check */
 #define ELAS_STAGE_DISP_RIGHT   12   /* float  [h][w] */

@@ -50,6 +50,11 @@ def run_and_compare(e, L, R, p, check_triangle=True):
     D1, D2 = e.process(L, R)
     g = gpu_stages(e, W, H, p)
     o1, o2, o = oracle.process(L, R, p, tri_left=g["tri_left"], tri_right=g["tri_right"], dumps=True)
+    # the library stores the plane prior clamped (every d_plane <= 0 and every
+    # d_plane > disp_max + radius act alike in the dense step)
+    dcap = p.disp_max + max(int(np.ceil(np.float32(p.sigma) * np.float32(p.sradius))), 2) + 1
+    for k in ("prior_left", "prior_right"):
+        o[k] = np.where(o[k] <= 0, -1, np.minimum(o[k], dcap)).astype(np.int32)
     for k in ("desc_left", "desc_right", "can_lr", "can", "support", "grid_left", "grid_right", "prior_left",
               "prior_right"):
         assert g[k].shape == o[k].shape, k
