@@ -9,7 +9,8 @@
 //             with atomic hooking of the larger root under the smaller.
 //   gap       rows, then columns: a run of <= ipol_gap_width invalid pixels
 //             between valid a and b becomes (a+b)/2 if |a-b| <= 3 else
-//             min(a,b).  One thread per line.
+//             min(a,b).  Widths up to 8 run inside the fused tile kernel,
+//             wider gaps as one thread per line.
 //   mean      5x5 weighted mean of valid pixels, w = 1/(1+(d_q-d_p)^2).
 //   median    lower median of the valid pixels of the 3x3 window.
 #include <cuda_runtime.h>
@@ -116,7 +117,14 @@ __global__ void k_uf_union_v(PostViews pv, int W, int H, float thr, unsigned* er
     float d = D[i];
     if (d < 0) return;
     float q = D[i + W];
-    if (q >= 0 && fabsf(q - d) <= thr) uf_union(lab, i, i + W, err);
+    if (!(q >= 0 && fabsf(q - d) <= thr)) return;
+    // the two row runs were already joined one column to the left when that
+    // column links them too (both pixels belong to the same runs)
+    if (u > 0) {
+        float dl = D[i - 1], ql = D[i + W - 1];
+        if (dl >= 0 && ql >= 0 && fabsf(dl - d) <= thr && fabsf(ql - q) <= thr && fabsf(ql - dl) <= thr) return;
+    }
+    uf_union(lab, i, i + W, err);
 }
 
 __global__ void k_uf_union(const float* __restrict__ D, int32_t* lab, int W, int H, float thr, unsigned* err) {
@@ -149,29 +157,50 @@ __global__ void k_uf_count(int32_t* lab, int32_t* __restrict__ root, int32_t* sz
     if (r >= 0 && (threadIdx.x & 31) == leader) atomicAdd(&sz[r], __popc(peers));
 }
 
-__global__ void k_uf_count_v(PostViews pv, int n, unsigned* err) {
+// Roots and segment sizes.  Warps merge equal roots with match_any, then a
+// small per-block table merges them again, so a large segment costs one
+// global atomic per block instead of one per pixel.
+constexpr int CNT_SLOTS = 128;
+__global__ void __launch_bounds__(1024) k_uf_count_v(PostViews pv, int n, unsigned* err) {
+    __shared__ int keys[CNT_SLOTS], vals[CNT_SLOTS];
     const int view = blockIdx.z;
     int32_t* lab = pv.lab[view];
     int32_t* root = pv.root[view];
     int32_t* sz = pv.sz[view];
+    for (int k = threadIdx.x; k < CNT_SLOTS; k += blockDim.x) { keys[k] = -1; vals[k] = 0; }
+    __syncthreads();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int r = -1;
     if (i < n && lab[i] >= 0) r = uf_find(lab, i, err);
     if (i < n) root[i] = r;
     unsigned peers = __match_any_sync(0xffffffffu, r);
     int leader = __ffs(peers) - 1;
-    if (r >= 0 && (threadIdx.x & 31) == leader) atomicAdd(&sz[r], __popc(peers));
+    if (r >= 0 && (threadIdx.x & 31) == leader) {
+        int c = __popc(peers);
+        int slot = int((unsigned(r) * 2654435761u) >> 25) & (CNT_SLOTS - 1);
+        bool done = false;
+        for (int probe = 0; probe < 8 && !done; ++probe, slot = (slot + 1) & (CNT_SLOTS - 1)) {
+            int prev = atomicCAS(&keys[slot], -1, r);
+            if (prev == -1 || prev == r) { atomicAdd(&vals[slot], c); done = true; }
+        }
+        if (!done) atomicAdd(&sz[r], c);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < CNT_SLOTS; k += blockDim.x)
+        if (keys[k] >= 0) atomicAdd(&sz[keys[k]], vals[k]);
 }
 
+// out = in with the pixels of small segments set invalid.
 __global__ void k_uf_apply_v(PostViews pv, int n, int min_size) {
     const int view = blockIdx.z;
-    float* D = pv.cur[view];
+    const float* D = pv.cur[view];
+    float* O = pv.nxt[view];
     const int32_t* root = pv.root[view];
     const int32_t* sz = pv.sz[view];
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int r = root[i];
-    if (r >= 0 && sz[r] < min_size) D[i] = -1.0f;
+    O[i] = (r >= 0 && sz[r] < min_size) ? -1.0f : D[i];
 }
 
 __global__ void k_uf_apply(float* D, const int32_t* __restrict__ root, const int32_t* sz, int n, int min_size) {
@@ -179,35 +208,6 @@ __global__ void k_uf_apply(float* D, const int32_t* __restrict__ root, const int
     if (i >= n) return;
     int r = root[i];
     if (r >= 0 && sz[r] < min_size) D[i] = -1.0f;
-}
-
-// Gap interpolation, one pixel per thread: an invalid pixel looks for the
-// nearest valid pixel on each side within `gap`; both found and the run
-// between them no longer than `gap` -> fill.  Equivalent to the serial
-// per-line scan because filled runs never touch the pixels that bound
-// other runs.  S = pass input, O = pass output.
-__global__ void k_gap_px(PostViews pv, int W, int H, int gap, int horizontal) {
-    const float* __restrict__ S = pv.cur[blockIdx.z];
-    float* __restrict__ O = pv.nxt[blockIdx.z];
-    int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
-    if (u >= W || v >= H) return;
-    size_t i = size_t(v) * W + u;
-    float c = S[i];
-    if (c < 0) {
-        const int len = horizontal ? W : H, k = horizontal ? u : v;
-        const long stride = horizontal ? 1 : W;
-        int lo = -1, hi = -1;
-        for (int j = 1; j <= gap && k - j >= 0; ++j)
-            if (S[i - j * stride] >= 0) { lo = k - j; break; }
-        if (lo >= 0)
-            for (int j = 1; j <= gap && k + j < len; ++j)
-                if (S[i + j * stride] >= 0) { hi = k + j; break; }
-        if (lo >= 0 && hi >= 0 && hi - lo - 1 <= gap) {
-            float a = S[i - (k - lo) * stride], b = S[i + (hi - k) * stride];
-            c = fabsf(a - b) <= 3.0f ? __fmul_rn(0.5f, __fadd_rn(a, b)) : fminf(a, b);
-        }
-    }
-    O[i] = c;
 }
 
 // horizontal = 1: one thread per row; 0: one thread per column (used for
@@ -232,55 +232,95 @@ __global__ void k_gap(PostViews pv, int W, int H, int gap, int horizontal) {
     }
 }
 
-// Adaptive mean and/or median in one pass over a 32x8 output tile: the
-// input tile (halo 3) and the mean of the tile plus halo 1 live in shared
-// memory; the median reads the mean.  Same arithmetic as k_mean/k_median.
-template <bool MEAN, bool MEDIAN>
-__global__ void __launch_bounds__(256) k_mean_median(PostViews pv, int W, int H) {
-    constexpr int TXo = 32, TYo = 8, HX = TXo + 6, HY = TYo + 6, MX = TXo + 2, MY = TYo + 2;
-    __shared__ float in[HY][HX];
-    __shared__ float mn[MY][MX];
-    const float* __restrict__ S = pv.cur[blockIdx.z];
-    float* __restrict__ O = pv.nxt[blockIdx.z];
-    const int u0 = blockIdx.x * TXo, v0 = blockIdx.y * TYo, tid = threadIdx.x;
-    for (int i = tid; i < HY * HX; i += 256) {
-        int r = i / HX, c = i % HX;
-        int x = u0 - 3 + c, y = v0 - 3 + r;
-        in[r][c] = (x >= 0 && x < W && y >= 0 && y < H) ? S[size_t(y) * W + x] : -2.0f;   // -2: outside
+// Gap interpolation (rows, then columns), adaptive mean and median in one
+// pass over a 32x32 output tile, every intermediate in shared memory.  The
+// input region carries a halo of gap + 3 (the column pass needs the row
+// pass gap rows away, the mean 2 more, the median 1 more).  Each stage is
+// computed exactly as its separate kernel (k_gap_px, k_mean_median) does.
+constexpr int PT = 32, PGMAX = 8, PHALO = PGMAX + 3, PS = PT + 2 * PHALO;   // S tile side
+__device__ __forceinline__ float gap_fill(const float* line, int stride, int k, int len, int gap, float c) {
+    // line[k*stride] is the pixel; positions < 0 or >= len are outside the image
+    if (c >= 0) return c;
+    int lo = -1, hi = -1;
+    for (int j = 1; j <= gap && k - j >= 0; ++j)
+        if (line[-j * stride] >= 0) { lo = k - j; break; }
+    if (lo >= 0)
+        for (int j = 1; j <= gap && k + j < len; ++j)
+            if (line[j * stride] >= 0) { hi = k + j; break; }
+    if (lo >= 0 && hi >= 0 && hi - lo - 1 <= gap) {
+        float a = line[-(k - lo) * stride], b = line[(hi - k) * stride];
+        return fabsf(a - b) <= 3.0f ? __fmul_rn(0.5f, __fadd_rn(a, b)) : fminf(a, b);
+    }
+    return c;
+}
+
+template <bool GAP, bool MEAN, bool MEDIAN>
+__global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, int gap) {
+    __shared__ float S[PS][PS];                 // input, halo PHALO
+    __shared__ float G[PS][PT + 6];             // after the row pass: columns [-3, 35)
+    __shared__ float V[PT + 6][PT + 6];         // after the column pass: [-3, 35)^2
+    __shared__ float M[PT + 2][PT + 2];         // after the mean: [-1, 33)^2
+    const float* __restrict__ src = pv.cur[blockIdx.z];
+    float* __restrict__ dst = pv.nxt[blockIdx.z];
+    const int u0 = blockIdx.x * PT, v0 = blockIdx.y * PT, tid = threadIdx.x;
+    const float OUT = -2.0f;                    // outside the image (never valid, never filled)
+    for (int i = tid; i < PS * PS; i += 1024) {
+        int r = i / PS, c = i % PS;
+        int x = u0 - PHALO + c, y = v0 - PHALO + r;
+        S[r][c] = (x >= 0 && x < W && y >= 0 && y < H) ? src[size_t(y) * W + x] : OUT;
     }
     __syncthreads();
-    for (int i = tid; i < MY * MX; i += 256) {
-        int r = i / MX, c = i % MX;       // mean at (u0-1+c, v0-1+r) = in[r+2][c+2]
-        float dp = in[r + 2][c + 2];
+    // row pass on rows [-PHALO, 32+PHALO), columns [-3, 35)
+    for (int i = tid; i < PS * (PT + 6); i += 1024) {
+        int r = i / (PT + 6), c = i % (PT + 6);
+        int x = u0 - 3 + c;
+        float val = S[r][c + PHALO - 3];
+        if (GAP && val != OUT && val < 0) val = gap_fill(&S[r][c + PHALO - 3], 1, x, W, gap, val);
+        G[r][c] = val;
+    }
+    __syncthreads();
+    // column pass on [-3, 35)^2
+    for (int i = tid; i < (PT + 6) * (PT + 6); i += 1024) {
+        int r = i / (PT + 6), c = i % (PT + 6);
+        int y = v0 - 3 + r;
+        float val = G[r + PHALO - 3][c];
+        if (GAP && val != OUT && val < 0) val = gap_fill(&G[r + PHALO - 3][c], PT + 6, y, H, gap, val);
+        V[r][c] = val;
+    }
+    __syncthreads();
+    // mean on [-1, 33)^2
+    for (int i = tid; i < (PT + 2) * (PT + 2); i += 1024) {
+        int r = i / (PT + 2), c = i % (PT + 2);
+        float dp = V[r + 2][c + 2];
         float out = dp;
         if (MEAN && dp >= 0) {
             float num = 0.0f, den = 0.0f;
             for (int dy = -2; dy <= 2; ++dy)
                 for (int dx = -2; dx <= 2; ++dx) {
-                    float dq = in[r + 2 + dy][c + 2 + dx];
-                    if (dq < 0) continue;      // invalid (-1) or outside (-2)
+                    float dq = V[r + 2 + dy][c + 2 + dx];
+                    if (dq < 0) continue;
                     float diff = __fsub_rn(dq, dp);
-                    float w = __fdiv_rn(1.0f, __fmaf_rn(diff, diff, 1.0f));
+                    float w = __frcp_rn(__fmaf_rn(diff, diff, 1.0f));
                     num = __fmaf_rn(w, dq, num);
                     den = __fadd_rn(den, w);
                 }
             out = __fdiv_rn(num, den);
         }
-        mn[r][c] = out;
+        M[r][c] = out;
     }
     __syncthreads();
     {
-        int ty = tid / TXo, tx = tid % TXo;
+        int ty = tid / PT, tx = tid % PT;
         int u = u0 + tx, v = v0 + ty;
         if (u < W && v < H) {
-            float c = mn[ty + 1][tx + 1];
+            float c = M[ty + 1][tx + 1];
             float out = c;
             if (MEDIAN && c >= 0) {
                 float a[9];
                 int n = 0;
                 for (int dy = -1; dy <= 1; ++dy)
                     for (int dx = -1; dx <= 1; ++dx) {
-                        float q = mn[ty + 1 + dy][tx + 1 + dx];
+                        float q = M[ty + 1 + dy][tx + 1 + dx];
                         if (q >= 0) a[n++] = q;
                     }
                 for (int i = 1; i < n; ++i) {
@@ -291,7 +331,7 @@ __global__ void __launch_bounds__(256) k_mean_median(PostViews pv, int W, int H)
                 }
                 out = a[(n - 1) / 2];
             }
-            O[size_t(v) * W + u] = out;
+            dst[size_t(v) * W + u] = out;
         }
     }
 }
@@ -311,27 +351,30 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         const int wpb = 8;
         k_uf_init_rows<<<dim3((H + wpb - 1) / wpb, 1, nviews), 32 * wpb, 0, st>>>(pv, W, H, p.speckle_sim_threshold);
         k_uf_union_v<<<grid2, tb, 0, st>>>(pv, W, H, p.speckle_sim_threshold, err);
-        k_uf_count_v<<<dim3((n + tb - 1) / tb, 1, nviews), tb, 0, st>>>(pv, n, err);
+        k_uf_count_v<<<dim3((n + 1023) / 1024, 1, nviews), 1024, 0, st>>>(pv, n, err);
         k_uf_apply_v<<<dim3((n + tb - 1) / tb, 1, nviews), tb, 0, st>>>(pv, n, p.speckle_size);
+        flip();
         launched += 4;
     }
-    if (p.ipol_gap_width > 0) {
-        if (p.ipol_gap_width <= 64) {
-            k_gap_px<<<grid2, tb, 0, st>>>(pv, W, H, p.ipol_gap_width, 1);
-            flip();
-            k_gap_px<<<grid2, tb, 0, st>>>(pv, W, H, p.ipol_gap_width, 0);
-            flip();
-        } else {
-            k_gap<<<dim3((H + 127) / 128, 1, nviews), 128, 0, st>>>(pv, W, H, p.ipol_gap_width, 1);
-            k_gap<<<dim3((W + 127) / 128, 1, nviews), 128, 0, st>>>(pv, W, H, p.ipol_gap_width, 0);
-        }
+    const int gap = p.ipol_gap_width;
+    const bool tile_gap = gap > 0 && gap <= PGMAX;
+    if (gap > PGMAX) {   // wide gaps: serial scans per line, in place
+        k_gap<<<dim3((H + 127) / 128, 1, nviews), 128, 0, st>>>(pv, W, H, gap, 1);
+        k_gap<<<dim3((W + 127) / 128, 1, nviews), 128, 0, st>>>(pv, W, H, gap, 0);
         launched += 2;
     }
-    if (adaptive_mean || median) {
-        dim3 grid((W + 31) / 32, (H + 7) / 8, nviews);
-        if (adaptive_mean && median) k_mean_median<true, true><<<grid, 256, 0, st>>>(pv, W, H);
-        else if (adaptive_mean) k_mean_median<true, false><<<grid, 256, 0, st>>>(pv, W, H);
-        else k_mean_median<false, true><<<grid, 256, 0, st>>>(pv, W, H);
+    if (tile_gap || adaptive_mean || median) {
+        dim3 grid((W + PT - 1) / PT, (H + PT - 1) / PT, nviews);
+        const int key = (tile_gap ? 4 : 0) | (adaptive_mean ? 2 : 0) | (median ? 1 : 0);
+        switch (key) {
+        case 1: k_post_tile<false, false, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+        case 2: k_post_tile<false, true, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+        case 3: k_post_tile<false, true, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+        case 4: k_post_tile<true, false, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+        case 5: k_post_tile<true, false, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+        case 6: k_post_tile<true, true, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+        default: k_post_tile<true, true, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+        }
         flip();
         launched += 1;
     }
