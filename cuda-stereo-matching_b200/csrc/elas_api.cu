@@ -43,6 +43,7 @@ struct elas_handle {
     uint32_t *gtmp0 = nullptr, *gtmp1 = nullptr, *grid0 = nullptr, *grid1 = nullptr;
     DelDev del[2]{};
     uint32_t *prior0 = nullptr, *prior1 = nullptr;
+    void* rast = nullptr;   // per-triangle plane/edge set-up of both views
     float *raw0 = nullptr, *raw1 = nullptr, *lr0 = nullptr, *lr1 = nullptr;
     float *out0 = nullptr, *out1 = nullptr;
     float* tmp[2] = {nullptr, nullptr};          // post-filter ping-pong buffer per view
@@ -204,6 +205,7 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         D.Tmax = int(tmax);
         D.Hmax = uint32_t(hmax);
     }
+    h->rast = take(2 * tmax * raster_bytes());
     h->prior0 = (uint32_t*)take(px * 4);
     h->prior1 = (uint32_t*)take(px * 4);
     h->raw0 = (float*)take(px * 4);
@@ -297,8 +299,8 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
                        st, &n));
     CK(mark(ELAS_TIME_PRIOR));
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
-                    h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1, h->num_sms, st));
-    n += 1;
+                    h->rast, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1, h->num_sms, st));
+    n += 3;
     CK(mark(ELAS_TIME_DENSE));
     CK(launch_dense(h->desc0, h->desc1, h->prior0, h->prior1, h->grid0, h->grid1, h->raw0, h->raw1, g, dp,
                     prior_shift(g, dp), h->err, st));

@@ -113,43 +113,63 @@ __device__ void setup_triangle(const int32_t* tri, const int32_t* can, const int
     R.BC_b = __fmaf_rn(-R.BC_a, B_u, B_v);
 }
 
-__device__ __forceinline__ void raster_part(const Raster& R, int u0, int u1, float ea, float eb, int W, int H,
-                                            uint32_t tag, int dcap, uint32_t* prior, int lane) {
-    for (int u = imax(u0, 0) + lane; u < imin(u1, W); u += 32) {
-        float fu = float(u);
-        int v1 = int(__float2uint_rz(__fmaf_rn(R.AC_a, fu, R.AC_b)));
-        int v2 = int(__float2uint_rz(__fmaf_rn(ea, fu, eb)));
-        int va = imax(imin(v1, v2), 0), vb = imin(imax(v1, v2), H);
-        for (int v = va; v < vb; ++v) {
-            float dp = __fadd_rn(__fmaf_rn(R.pa, fu, __fmul_rn(R.pb, float(v))), R.pc);
-            int d = __float2int_rz(dp);
-            d = d <= 0 ? 0 : (d > dcap ? dcap : d);
-            atomicMax(&prior[size_t(v) * W + u], tag | uint32_t(d));
-        }
+// One thread per (view, triangle): plane and edge set-up, once.
+__global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__ tri0,
+                                                     const int32_t* __restrict__ tri1,
+                                                     const int32_t* __restrict__ ctr0,
+                                                     const int32_t* __restrict__ ctr1,
+                                                     const int32_t* __restrict__ can, const int32_t* __restrict__ uvd,
+                                                     Raster* __restrict__ rast, int Tmax, Geom g) {
+    const int T0 = ctr0[0], T1 = ctr1[0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T0 + T1; i += gridDim.x * blockDim.x) {
+        const bool right = i >= T0;
+        const int t = right ? i - T0 : i;
+        Raster R;
+        setup_triangle((right ? tri1 : tri0) + 3 * size_t(t), can, uvd, g.cw, g.step, right, R);
+        rast[(right ? Tmax : 0) + t] = R;
     }
 }
 
-// One warp per (view, triangle).
-__global__ void __launch_bounds__(256) k_prior(const int32_t* __restrict__ tri0, const int32_t* __restrict__ tri1,
-                                               const int32_t* __restrict__ ctr0, const int32_t* __restrict__ ctr1,
-                                               const int32_t* __restrict__ can, const int32_t* __restrict__ uvd,
-                                               uint32_t* prior0, uint32_t* prior1, Geom g, int pshift, int dcap) {
+// One warp per (view, triangle), lanes over columns.  PASS 0 stores the
+// packed value; PASS 1 re-reads each pixel and, where a later triangle lost
+// the race of pass 0, raises it with atomicMax -- so every pixel ends with
+// the last covering triangle, as with sequential rasterisation, while
+// uncontested pixels (nearly all) cost a plain store and a load.
+template <int PASS>
+__global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict__ ctr0,
+                                                      const int32_t* __restrict__ ctr1,
+                                                      const Raster* __restrict__ rast, int Tmax,
+                                                      uint32_t* prior0, uint32_t* prior1, Geom g, int pshift,
+                                                      int dcap) {
     const int lane = threadIdx.x & 31;
     const int T0 = ctr0[0], T1 = ctr1[0];
-    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int i = wid; i < T0 + T1; i += nw) {
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < T0 + T1; i += nw) {
         const bool right = i >= T0;
         const int t = right ? i - T0 : i;
-        const int32_t* tri = (right ? tri1 : tri0) + 3 * size_t(t);
-        Raster R;
-        setup_triangle(tri, can, uvd, g.cw, g.step, right, R);
-        uint32_t tag = uint32_t(t + 1) << pshift;
+        const Raster R = rast[(right ? Tmax : 0) + t];
+        const uint32_t tag = uint32_t(t + 1) << pshift;
         uint32_t* prior = right ? prior1 : prior0;
-        if (int(R.A_u) != int(R.B_u))
-            raster_part(R, int(R.A_u), int(R.B_u), R.AB_a, R.AB_b, g.W, g.H, tag, dcap, prior, lane);
-        if (int(R.B_u) != int(R.C_u))
-            raster_part(R, int(R.B_u), int(R.C_u), R.BC_a, R.BC_b, g.W, g.H, tag, dcap, prior, lane);
+        for (int part = 0; part < 2; ++part) {
+            const int ua = part ? int(R.B_u) : int(R.A_u), ub = part ? int(R.C_u) : int(R.B_u);
+            if (ua == ub) continue;
+            const float ea = part ? R.BC_a : R.AB_a, eb = part ? R.BC_b : R.AB_b;
+            for (int u = imax(ua, 0) + lane; u < imin(ub, g.W); u += 32) {
+                const float fu = float(u);
+                const int v1 = int(__float2uint_rz(__fmaf_rn(R.AC_a, fu, R.AC_b)));
+                const int v2 = int(__float2uint_rz(__fmaf_rn(ea, fu, eb)));
+                const int va = imax(imin(v1, v2), 0), vb = imin(imax(v1, v2), g.H);
+                for (int v = va; v < vb; ++v) {
+                    const float dp = __fadd_rn(__fmaf_rn(R.pa, fu, __fmul_rn(R.pb, float(v))), R.pc);
+                    int d = __float2int_rz(dp);
+                    d = d <= 0 ? 0 : (d > dcap ? dcap : d);
+                    const uint32_t val = tag | uint32_t(d);
+                    uint32_t* px = &prior[size_t(v) * g.W + u];
+                    if (PASS == 0) *px = val;
+                    else if (*px < val) atomicMax(px, val);
+                }
+            }
+        }
     }
 }
 
@@ -287,15 +307,21 @@ __global__ void k_lr(const float* __restrict__ D1, const float* __restrict__ D2,
 }  // namespace
 
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
-                         int Tmax, const int32_t* can, const int32_t* uvd, uint32_t* prior0, uint32_t* prior1,
-                         const Geom& g, int pshift, int dcap, int num_sms, cudaStream_t st) {
+                         int Tmax, const int32_t* can, const int32_t* uvd, void* rast, uint32_t* prior0,
+                         uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms, cudaStream_t st) {
     size_t n = size_t(g.W) * g.H * sizeof(uint32_t);
     cudaMemsetAsync(prior0, 0, n, st);
     cudaMemsetAsync(prior1, 0, n, st);
+    Raster* R = static_cast<Raster*>(rast);
+    k_prior_setup<<<imax(1, imin(8 * num_sms, (2 * Tmax + 255) / 256)), 256, 0, st>>>(tri0, tri1, ctr0, ctr1, can,
+                                                                                      uvd, R, Tmax, g);
     int blocks = imax(1, imin(16 * num_sms, (2 * Tmax + 7) / 8));
-    k_prior<<<blocks, 256, 0, st>>>(tri0, tri1, ctr0, ctr1, can, uvd, prior0, prior1, g, pshift, dcap);
+    k_prior_raster<0><<<blocks, 256, 0, st>>>(ctr0, ctr1, R, Tmax, prior0, prior1, g, pshift, dcap);
+    k_prior_raster<1><<<blocks, 256, 0, st>>>(ctr0, ctr1, R, Tmax, prior0, prior1, g, pshift, dcap);
     return cudaGetLastError();
 }
+
+size_t raster_bytes() { return sizeof(Raster); }
 
 size_t dense_smem_bytes(const Geom& g) { return size_t(g.W) * 16 + size_t(g.gw) * (LMAX * 2 + 1); }
 

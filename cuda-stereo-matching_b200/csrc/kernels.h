@@ -60,9 +60,11 @@ int cluster_size_for_flip();
 // Plane prior of both views: prior[v*W+u] = (triangle+1) << pshift | d,
 // d = d_plane clamped to [0, dcap] (dcap = disp_max + plane_radius + 1),
 // 0 where no triangle covers the pixel.  The buffers are zeroed here.
+// rast: scratch of 2 * Tmax * raster_bytes() for the per-triangle set-up.
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
-                         int Tmax, const int32_t* can, const int32_t* uvd, uint32_t* prior0, uint32_t* prior1,
-                         const Geom& g, int pshift, int dcap, int num_sms, cudaStream_t st);
+                         int Tmax, const int32_t* can, const int32_t* uvd, void* rast, uint32_t* prior0,
+                         uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms, cudaStream_t st);
+size_t raster_bytes();
 
 size_t dense_smem_bytes(const Geom& g);
 cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t* prior0, const uint32_t* prior1,
