@@ -159,14 +159,29 @@ __global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict_
                 const int v1 = int(__float2uint_rz(__fmaf_rn(R.AC_a, fu, R.AC_b)));
                 const int v2 = int(__float2uint_rz(__fmaf_rn(ea, fu, eb)));
                 const int va = imax(imin(v1, v2), 0), vb = imin(imax(v1, v2), g.H);
-                for (int v = va; v < vb; ++v) {
+                auto value = [&](int v) {
                     const float dp = __fadd_rn(__fmaf_rn(R.pa, fu, __fmul_rn(R.pb, float(v))), R.pc);
                     int d = __float2int_rz(dp);
                     d = d <= 0 ? 0 : (d > dcap ? dcap : d);
-                    const uint32_t val = tag | uint32_t(d);
-                    uint32_t* px = &prior[size_t(v) * g.W + u];
-                    if (PASS == 0) *px = val;
-                    else if (*px < val) atomicMax(px, val);
+                    return tag | uint32_t(d);
+                };
+                if (PASS == 0) {
+                    for (int v = va; v < vb; ++v) prior[size_t(v) * g.W + u] = value(v);
+                } else {
+                    // eight independent loads in flight before any compare
+                    constexpr int B = 8;
+                    for (int v0 = va; v0 < vb; v0 += B) {
+                        uint32_t got[B];
+#pragma unroll
+                        for (int k = 0; k < B; ++k)
+                            got[k] = v0 + k < vb ? __ldcg(&prior[size_t(v0 + k) * g.W + u]) : 0xffffffffu;
+#pragma unroll
+                        for (int k = 0; k < B; ++k) {
+                            if (v0 + k >= vb) break;
+                            const uint32_t val = value(v0 + k);
+                            if (got[k] < val) atomicMax(&prior[size_t(v0 + k) * g.W + u], val);
+                        }
+                    }
                 }
             }
         }
