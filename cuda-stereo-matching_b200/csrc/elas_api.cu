@@ -50,6 +50,7 @@ struct elas_handle {
     int32_t* lab[2] = {nullptr, nullptr};        // union-find labels per view
     int32_t* root[2] = {nullptr, nullptr};       // union-find roots per view
     int32_t* usize[2] = {nullptr, nullptr};      // segment sizes per view
+    float* wtab = nullptr;                       // adaptive-mean weight table
     unsigned* err = nullptr;
 
     // per-stage timing
@@ -220,6 +221,7 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         h->root[k] = (int32_t*)take(px * 4);
         h->usize[k] = (int32_t*)take(px * 4);
     }
+    h->wtab = (float*)take(WTAB_SIZE * 4);
     h->err = (unsigned*)take(64);
     return off;
 }
@@ -300,7 +302,7 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     CK(mark(ELAS_TIME_PRIOR));
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
                     h->rast, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1, h->num_sms, st));
-    n += 3;
+    n += 2;
     CK(mark(ELAS_TIME_DENSE));
     CK(launch_dense(h->desc0, h->desc1, h->prior0, h->prior1, h->grid0, h->grid1, h->raw0, h->raw1, g, dp,
                     prior_shift(g, dp), h->err, st));
@@ -312,6 +314,7 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     CK(cudaMemcpyAsync(out0, h->lr0, size_t(W) * H * 4, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(out1, h->lr1, size_t(W) * H * 4, cudaMemcpyDeviceToDevice, st));
     PostViews pv;
+    pv.wtab = h->wtab;
     float* outs[2] = {out0, out1};
     for (int k = 0; k < 2; ++k) {
         pv.cur[k] = outs[k];

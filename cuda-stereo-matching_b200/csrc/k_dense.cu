@@ -2,9 +2,9 @@
 //
 // Prior: replaces kerComputeDepthApproximation
 // (src/Kernels/KerComputeDisparity.cu:9-152), one thread per triangle with
-// long serial scanline loops.  Here a warp takes a triangle: every lane
-// solves the plane (same double Gauss-Jordan as kerSolve, :321-375) and the
-// lanes split the triangle's columns.  A pixel covered by more than one
+// long serial scanline loops.  Here one thread per triangle solves the plane
+// (same double Gauss-Jordan as kerSolve, :321-375) and sets up the edges,
+// then a warp per triangle splits its columns.  A pixel covered by more than one
 // triangle (rounding at shared vertices) must keep the last triangle in
 // list order, as a sequential rasteriser would; the prior is therefore
 // written with a 32-bit atomicMax of (triangle+1) << pshift | d_plane, which
@@ -130,12 +130,8 @@ __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__
     }
 }
 
-// One warp per (view, triangle), lanes over columns.  PASS 0 stores the
-// packed value; PASS 1 re-reads each pixel and, where a later triangle lost
-// the race of pass 0, raises it with atomicMax -- so every pixel ends with
-// the last covering triangle, as with sequential rasterisation, while
-// uncontested pixels (nearly all) cost a plain store and a load.
-template <int PASS>
+// One warp per (view, triangle), lanes over columns; every pixel keeps the
+// last covering triangle through atomicMax on the packed value.
 __global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict__ ctr0,
                                                       const int32_t* __restrict__ ctr1,
                                                       const Raster* __restrict__ rast, int Tmax,
@@ -165,24 +161,7 @@ __global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict_
                     d = d <= 0 ? 0 : (d > dcap ? dcap : d);
                     return tag | uint32_t(d);
                 };
-                if (PASS == 0) {
-                    for (int v = va; v < vb; ++v) prior[size_t(v) * g.W + u] = value(v);
-                } else {
-                    // eight independent loads in flight before any compare
-                    constexpr int B = 8;
-                    for (int v0 = va; v0 < vb; v0 += B) {
-                        uint32_t got[B];
-#pragma unroll
-                        for (int k = 0; k < B; ++k)
-                            got[k] = v0 + k < vb ? __ldcg(&prior[size_t(v0 + k) * g.W + u]) : 0xffffffffu;
-#pragma unroll
-                        for (int k = 0; k < B; ++k) {
-                            if (v0 + k >= vb) break;
-                            const uint32_t val = value(v0 + k);
-                            if (got[k] < val) atomicMax(&prior[size_t(v0 + k) * g.W + u], val);
-                        }
-                    }
-                }
+                for (int v = va; v < vb; ++v) atomicMax(&prior[size_t(v) * g.W + u], value(v));
             }
         }
     }
@@ -331,8 +310,7 @@ cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t
     k_prior_setup<<<imax(1, imin(8 * num_sms, (2 * Tmax + 255) / 256)), 256, 0, st>>>(tri0, tri1, ctr0, ctr1, can,
                                                                                       uvd, R, Tmax, g);
     int blocks = imax(1, imin(16 * num_sms, (2 * Tmax + 7) / 8));
-    k_prior_raster<0><<<blocks, 256, 0, st>>>(ctr0, ctr1, R, Tmax, prior0, prior1, g, pshift, dcap);
-    k_prior_raster<1><<<blocks, 256, 0, st>>>(ctr0, ctr1, R, Tmax, prior0, prior1, g, pshift, dcap);
+    k_prior_raster<<<blocks, 256, 0, st>>>(ctr0, ctr1, R, Tmax, prior0, prior1, g, pshift, dcap);
     return cudaGetLastError();
 }
 

@@ -191,16 +191,33 @@ __global__ void __launch_bounds__(1024) k_uf_count_v(PostViews pv, int n, unsign
 }
 
 // out = in with the pixels of small segments set invalid.
+// Four pixels per thread, their loads issued together.
 __global__ void k_uf_apply_v(PostViews pv, int n, int min_size) {
     const int view = blockIdx.z;
     const float* D = pv.cur[view];
     float* O = pv.nxt[view];
     const int32_t* root = pv.root[view];
     const int32_t* sz = pv.sz[view];
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int r = root[i];
-    O[i] = (r >= 0 && sz[r] < min_size) ? -1.0f : D[i];
+    const int i0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    int r[4], s4[4];
+    float d[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        r[k] = i0 + k < n ? root[i0 + k] : -1;
+        d[k] = i0 + k < n ? D[i0 + k] : 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) s4[k] = r[k] >= 0 ? sz[r[k]] : min_size;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (i0 + k < n) O[i0 + k] = s4[k] < min_size ? -1.0f : d[k];
+}
+
+__global__ void k_wtab(float* wtab) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= WTAB_SIZE) return;
+    float q = float(k) * 0.25f;
+    wtab[k] = __frcp_rn(__fmaf_rn(q, q, 1.0f));
 }
 
 __global__ void k_uf_apply(float* D, const int32_t* __restrict__ root, const int32_t* sz, int n, int min_size) {
@@ -300,7 +317,12 @@ __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, 
                     float dq = V[r + 2 + dy][c + 2 + dx];
                     if (dq < 0) continue;
                     float diff = __fsub_rn(dq, dp);
-                    float w = __frcp_rn(__fmaf_rn(diff, diff, 1.0f));
+                    // disparities here are multiples of 1/4, so the weight is a
+                    // table entry computed by the same correctly rounded operation
+                    float k4 = fabsf(diff) * 4.0f;
+                    int ki = int(k4);
+                    float w = (float(ki) == k4 && ki < WTAB_SIZE) ? __ldg(&pv.wtab[ki])
+                                                                  : __frcp_rn(__fmaf_rn(diff, diff, 1.0f));
                     num = __fmaf_rn(w, dq, num);
                     den = __fadd_rn(den, w);
                 }
@@ -352,7 +374,7 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         k_uf_init_rows<<<dim3((H + wpb - 1) / wpb, 1, nviews), 32 * wpb, 0, st>>>(pv, W, H, p.speckle_sim_threshold);
         k_uf_union_v<<<grid2, tb, 0, st>>>(pv, W, H, p.speckle_sim_threshold, err);
         k_uf_count_v<<<dim3((n + 1023) / 1024, 1, nviews), 1024, 0, st>>>(pv, n, err);
-        k_uf_apply_v<<<dim3((n + tb - 1) / tb, 1, nviews), tb, 0, st>>>(pv, n, p.speckle_size);
+        k_uf_apply_v<<<dim3((n + 4 * tb - 1) / (4 * tb), 1, nviews), tb, 0, st>>>(pv, n, p.speckle_size);
         flip();
         launched += 4;
     }
@@ -364,6 +386,10 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         launched += 2;
     }
     if (tile_gap || adaptive_mean || median) {
+        if (adaptive_mean) {
+            k_wtab<<<(WTAB_SIZE + 255) / 256, 256, 0, st>>>(pv.wtab);
+            launched += 1;
+        }
         dim3 grid((W + PT - 1) / PT, (H + PT - 1) / PT, nviews);
         const int key = (tile_gap ? 4 : 0) | (adaptive_mean ? 2 : 0) | (median ? 1 : 0);
         switch (key) {

@@ -84,7 +84,9 @@ struct PostViews {
     int32_t* lab[2];
     int32_t* root[2];
     int32_t* sz[2];
+    float* wtab;     // adaptive-mean weights 1/(1 + (k/4)^2), k = 0 .. WTAB_SIZE-1
 };
+constexpr int WTAB_SIZE = 4 * 4096 + 8;
 
 // Post-filters on nviews (1 or 2) disparity images.
 cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams& p, bool median, bool adaptive_mean,
