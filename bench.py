@@ -284,6 +284,8 @@ def run_ours(args):
         out["cpu_baseline"] = cpu_baseline(L, R, p, args.cpu_seconds)
     if rank == 0 and world == 1 and not args.no_large:
         out["large"] = run_large(torch, args, flush, stream, hbm, peak_kind)
+    if rank == 0 and world == 1 and not args.no_batch:
+        out["batch"] = run_batch(torch, args, flush, stream)
     e.close()
     del flush
     if rank == 0:
@@ -312,6 +314,68 @@ def run_large(torch, args, flush, stream, hbm, peak_kind):
                                "unit": "GB/s", "frac": dense_bytes / (stage_ms["dense"] / 1e3) / 1e9 / hbm,
                                "peak_kind": peak_kind, "traffic": profile_traffic("k_dense_2880x1988")},
             "gpu_launches": launches, "quality": quality(D1, gt)}
+
+
+def batch_workload(n=64, seed=7):
+    """Heterogeneous batch: widths 320-1920, heights 240-1080 (multiples of
+    16), disparity ranges 64/128/256, drawn from a fixed seed."""
+    rng = np.random.default_rng(seed)
+    shapes = []
+    for _ in range(n):
+        w = int(rng.integers(20, 121)) * 16
+        h = int(rng.integers(15, 68)) * 16
+        d = int(rng.choice([64, 128, 256]))
+        shapes.append((w, h, d))
+    return shapes
+
+
+def run_batch(torch, args, flush, stream):
+    """64 independent pairs per step through the batched device call: one
+    worker stream per pair, the whole batch replayed as one CUDA graph."""
+    shapes = batch_workload()
+    n = len(shapes)
+    bufs, pix = [], 0
+    for i, (w, h, d) in enumerate(shapes):
+        L, R, _, _ = eb.synth_pair(3, 5000 + i, width=w, height=h, disp_max=d, gt=False)
+        bufs.append([torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda(),
+                     torch.empty((h, w), dtype=torch.float32, device="cuda"),
+                     torch.empty((h, w), dtype=torch.float32, device="cuda")])
+        pix += w * h
+    dims = [(w, h) for (w, h, _) in shapes]
+    dmax = [d for (_, _, d) in shapes]
+    ptrs = [[b[k].data_ptr() for b in bufs] for k in range(4)]
+    e = eb.Elas(eb.params_config(64))
+    s = stream.cuda_stream
+    out = {"workload": f"batch_{n}_pairs_w320-1920_h240-1080_disp64-256", "pairs_per_step": n,
+           "megapixels_per_step": pix / 1e6}
+    steps = max(3, min(args.steps, 10))
+    for mode, graphs in (("graph", True), ("eager", False)):
+        e.set_graphs(graphs)
+        l0 = e.launch_count
+        for _ in range(3):
+            flush.zero_()
+            e.process_batch_device(*ptrs, dims, dmax, stream=s)
+        torch.cuda.synchronize()
+        lat = []
+        total = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            e.process_batch_device(*ptrs, dims, dmax, stream=s)
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+            lat.extend(e.batch_latency(n).tolist())
+        v = steps * n / (total / 1e3)
+        out[mode] = {"value": v, "unit": "pairs/s", "ms_per_step": total / steps,
+                     "megapixels_per_s": v * pix / n / 1e6,
+                     "latency_ms_p50": float(np.percentile(lat, 50)), "latency_ms_p99": float(np.percentile(lat, 99)),
+                     "steps": steps}
+    out["dense_shapes"] = sorted({f"{(w + 127) // 128 * 128}/{d}:{e.dense_shape(w, d)}" for (w, _, d) in shapes})
+    e.close()
+    return out
 
 
 def run_reference(args):
@@ -355,6 +419,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

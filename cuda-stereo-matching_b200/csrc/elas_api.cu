@@ -13,7 +13,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/elas_b200.h"
@@ -56,6 +58,23 @@ struct elas_handle {
     // per-stage timing
     bool timing = false;
     cudaEvent_t ev[ELAS_TIME_COUNT + 1] = {};
+
+    // dense-matching autotuner: (width class, disp_max) -> threads per CTA
+    std::map<std::pair<int, int>, int> dense_threads;
+
+    // batch execution: one worker (own workspace and stream) per pair
+    std::vector<elas_handle*> slots;
+    std::vector<cudaStream_t> slot_streams;
+    std::vector<cudaEvent_t> slot_done;
+    cudaEvent_t batch_start = nullptr;
+    cudaEvent_t lat_start = nullptr;          // per-pair latency marks (graph nodes when captured)
+    std::vector<cudaEvent_t> lat_done;
+    cudaStream_t own_stream = nullptr;
+    bool use_graphs = true;
+    cudaGraphExec_t graph_exec = nullptr;
+    std::vector<int64_t> graph_sig;   // what the cached graph was captured for
+    int last_batch = 0;
+    elas_handle* owner = nullptr;     // the user's handle, for a batch worker
 };
 
 namespace {
@@ -272,6 +291,48 @@ int check_dims(elas_handle* h, const int32_t* dims, int& W, int& H) {
     return ELAS_OK;
 }
 
+// Dense-matching autotuner.  The CTA shape (threads per row CTA) changes
+// only how the row's pixels are spread over threads, never the result; the
+// first call with a new (width class, disp_max) times each shape on its own
+// data (CUDA events on the stream) and keeps the fastest.  Inside a stream
+// capture an untuned class uses 512 threads.
+constexpr int DENSE_SHAPES[4] = {128, 256, 512, 1024};
+
+int dense_threads_for(elas_handle* h, const Geom& g, const DevParams& dp, cudaStream_t st, int* nlaunch, int* out) {
+    elas_handle* t = h->owner ? h->owner : h;
+    const std::pair<int, int> key((g.W + 127) / 128, g.D);
+    auto it = t->dense_threads.find(key);
+    if (it != t->dense_threads.end()) { *out = it->second; return ELAS_OK; }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) { *out = 512; return ELAS_OK; }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    int best = 512;
+    float best_ms = 1e30f;
+    for (int shape : DENSE_SHAPES) {
+        float shape_ms = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            CK(cudaEventRecord(e0, st));
+            CK(launch_dense(h->desc0, h->desc1, h->prior0, h->prior1, h->grid0, h->grid1, h->raw0, h->raw1, g, dp,
+                            prior_shift(g, dp), h->err, st, shape));
+            CK(cudaEventRecord(e1, st));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            shape_ms = std::min(shape_ms, ms);
+            *nlaunch += 1;
+        }
+        if (shape_ms < best_ms) { best_ms = shape_ms; best = shape; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    t->dense_threads[key] = best;
+    *out = best;
+    return ELAS_OK;
+}
+
 // The whole pipeline on device buffers (inputs img0/img1 already on the device).
 int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float* out0, float* out1, int W, int H,
                  cudaStream_t st) {
@@ -303,9 +364,12 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
                     h->rast, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1, h->num_sms, st));
     n += 2;
+    int shape = 512;
+    rc = dense_threads_for(h, g, dp, st, &n, &shape);
+    if (rc != ELAS_OK) return rc;
     CK(mark(ELAS_TIME_DENSE));
     CK(launch_dense(h->desc0, h->desc1, h->prior0, h->prior1, h->grid0, h->grid1, h->raw0, h->raw1, g, dp,
-                    prior_shift(g, dp), h->err, st));
+                    prior_shift(g, dp), h->err, st, shape));
     n += 1;
     CK(mark(ELAS_TIME_LR));
     CK(launch_lr(h->raw0, h->raw1, h->lr0, h->lr1, g, p.lr_threshold, st));
@@ -329,6 +393,102 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     CK(mark(ELAS_TIME_COUNT));
     h->launches += n;
     h->have_last = true;
+    return ELAS_OK;
+}
+
+// Batch workers: one handle (own workspace) and one stream per pair.
+int ensure_slots(elas_handle* h, int n) {
+    while (int(h->slots.size()) < n) {
+        elas_handle* w = new elas_handle();
+        w->params = h->params;
+        w->device = h->device;
+        w->num_sms = h->num_sms;
+        w->cluster_size = h->cluster_size;
+        w->owner = h;
+        cudaStream_t st;
+        cudaEvent_t ev;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) { delete w; return ELAS_ERR_CUDA; }
+        if (cudaEventCreate(&ev) != cudaSuccess) { cudaStreamDestroy(st); delete w; return ELAS_ERR_CUDA; }
+        cudaEvent_t lev;
+        if (cudaEventCreate(&lev) != cudaSuccess) {
+            cudaEventDestroy(ev);
+            cudaStreamDestroy(st);
+            delete w;
+            return ELAS_ERR_CUDA;
+        }
+        h->lat_done.push_back(lev);
+        h->slots.push_back(w);
+        h->slot_streams.push_back(st);
+        h->slot_done.push_back(ev);
+    }
+    if (!h->batch_start) CK(cudaEventCreate(&h->batch_start));
+    if (!h->lat_start) CK(cudaEventCreate(&h->lat_start));
+    if (!h->own_stream) CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    return ELAS_OK;
+}
+
+// Fork from `st`, run pair i on worker stream i, join back into `st`.  With
+// host buffers (hl/hr/hd1/hd2 non-null) the copies in both directions go on
+// the worker streams as well.  Works inside a stream capture (the workers
+// join it through the fork event) as long as every workspace is sized.
+// lat_start / lat_done are recorded as event nodes of a captured graph, so
+// per-pair latencies stay readable after a replay.
+int issue_batch(elas_handle* h, int n, const uint8_t* const* l, const uint8_t* const* r, float* const* d1,
+                float* const* d2, const int32_t* dims, const int32_t* dmax, bool host, cudaStream_t st,
+                bool capturing = false) {
+    const unsigned lat_flags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    CK(cudaEventRecordWithFlags(h->lat_start, st, lat_flags));
+    CK(cudaEventRecord(h->batch_start, st));
+    for (int i = 0; i < n; ++i) {
+        elas_handle* w = h->slots[i];
+        cudaStream_t ws = h->slot_streams[i];
+        w->params = h->params;
+        if (dmax) w->params.disp_max = dmax[i];
+        const int W = dims[2 * i], H = dims[2 * i + 1];
+        const size_t px = size_t(W) * H;
+        CK(cudaStreamWaitEvent(ws, h->batch_start, 0));
+        int rc = ensure_workspace(w, geom_of(W, H, w->params));
+        if (rc != ELAS_OK) return fail(h, rc, w->last_error);
+        const uint8_t* il = l[i];
+        const uint8_t* ir = r[i];
+        float* o1 = d1[i];
+        float* o2 = d2[i];
+        if (host) {
+            CK(cudaMemcpyAsync(w->img0, l[i], px, cudaMemcpyHostToDevice, ws));
+            CK(cudaMemcpyAsync(w->img1, r[i], px, cudaMemcpyHostToDevice, ws));
+            il = w->img0;
+            ir = w->img1;
+            o1 = w->out0;
+            o2 = w->out1;
+        }
+        rc = run_pipeline(w, il, ir, o1, o2, W, H, ws);
+        if (rc != ELAS_OK) return fail(h, rc, w->last_error);
+        if (host) {
+            CK(cudaMemcpyAsync(d1[i], w->out0, px * 4, cudaMemcpyDeviceToHost, ws));
+            CK(cudaMemcpyAsync(d2[i], w->out1, px * 4, cudaMemcpyDeviceToHost, ws));
+        }
+        CK(cudaEventRecordWithFlags(h->lat_done[i], ws, lat_flags));
+        CK(cudaEventRecord(h->slot_done[i], ws));
+        CK(cudaStreamWaitEvent(st, h->slot_done[i], 0));
+    }
+    h->last_batch = n;
+    return ELAS_OK;
+}
+
+int check_batch(elas_handle* h, int n, const int32_t* dims, const int32_t* dmax) {
+    for (int i = 0; i < n; ++i) {
+        elas_params q = h->params;
+        if (dmax) q.disp_max = dmax[i];
+        std::string why;
+        int rc = check_params(q, why);
+        if (rc != ELAS_OK) return fail(h, rc, "pair " + std::to_string(i) + ": " + why);
+        elas_params saved = h->params;
+        h->params = q;
+        int W, H;
+        rc = check_dims(h, dims + 2 * i, W, H);
+        h->params = saved;
+        if (rc != ELAS_OK) return rc;
+    }
     return ELAS_OK;
 }
 
@@ -464,6 +624,18 @@ int elas_b200_get_timing(elas_handle* h, float* ms_out, int n) {
 
 int elas_b200_destroy(elas_handle* h) {
     if (!h) return ELAS_ERR_INVALID_ARG;
+    cudaSetDevice(h->device);
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    for (size_t i = 0; i < h->slots.size(); ++i) {
+        cudaStreamSynchronize(h->slot_streams[i]);
+        elas_b200_destroy(h->slots[i]);
+        cudaStreamDestroy(h->slot_streams[i]);
+        cudaEventDestroy(h->slot_done[i]);
+        cudaEventDestroy(h->lat_done[i]);
+    }
+    if (h->batch_start) cudaEventDestroy(h->batch_start);
+    if (h->lat_start) cudaEventDestroy(h->lat_start);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
     for (int i = 0; i <= ELAS_TIME_COUNT; ++i)
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);
     if (h->arena) {
@@ -531,19 +703,98 @@ int elas_b200_process_batch(elas_handle* h, int n, const uint8_t* const* lefts, 
                             const int32_t* disp_max_per_pair, void* stream) {
     if (!h || n < 0 || (n > 0 && (!lefts || !rights || !disp_lefts || !disp_rights || !dims)))
         return ELAS_ERR_INVALID_ARG;
-    elas_params saved = h->params;
-    int rc = ELAS_OK;
-    for (int i = 0; i < n && rc == ELAS_OK; ++i) {
-        if (disp_max_per_pair) {
-            elas_params q = saved;
-            q.disp_max = disp_max_per_pair[i];
-            rc = elas_b200_set_params(h, &q);
-            if (rc != ELAS_OK) break;
-        }
-        rc = elas_b200_process(h, lefts[i], rights[i], disp_lefts[i], disp_rights[i], dims + 2 * i, stream);
+    if (n == 0) return ELAS_OK;
+    CK(cudaSetDevice(h->device));
+    int rc = check_batch(h, n, dims, disp_max_per_pair);
+    if (rc != ELAS_OK) return rc;
+    rc = ensure_slots(h, n);
+    if (rc != ELAS_OK) return fail(h, rc, "creating batch workers failed");
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->own_stream;
+    rc = issue_batch(h, n, lefts, rights, disp_lefts, disp_rights, dims, disp_max_per_pair, true, st);
+    if (rc != ELAS_OK) return rc;
+    CK(cudaStreamSynchronize(st));
+    for (int i = 0; i < n; ++i) {
+        rc = check_device_errors(h->slots[i], h->slot_streams[i]);
+        if (rc != ELAS_OK) return fail(h, rc, h->slots[i]->last_error);
     }
-    h->params = saved;
-    return rc;
+    return ELAS_OK;
+}
+
+int elas_b200_process_batch_device(elas_handle* h, int n, const uint8_t* const* d_lefts,
+                                   const uint8_t* const* d_rights, float* const* d_disp_lefts,
+                                   float* const* d_disp_rights, const int32_t* dims,
+                                   const int32_t* disp_max_per_pair, void* stream) {
+    if (!h || n < 0 || (n > 0 && (!d_lefts || !d_rights || !d_disp_lefts || !d_disp_rights || !dims)))
+        return ELAS_ERR_INVALID_ARG;
+    if (n == 0) return ELAS_OK;
+    CK(cudaSetDevice(h->device));
+    int rc = check_batch(h, n, dims, disp_max_per_pair);
+    if (rc != ELAS_OK) return rc;
+    rc = ensure_slots(h, n);
+    if (rc != ELAS_OK) return fail(h, rc, "creating batch workers failed");
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->own_stream;
+    // what a captured graph depends on: sizes, disparity ranges, buffers, parameters
+    std::vector<int64_t> sig;
+    sig.push_back(n);
+    for (int i = 0; i < n; ++i) {
+        sig.push_back(dims[2 * i]);
+        sig.push_back(dims[2 * i + 1]);
+        sig.push_back(disp_max_per_pair ? disp_max_per_pair[i] : h->params.disp_max);
+        sig.push_back(int64_t(d_lefts[i]));
+        sig.push_back(int64_t(d_rights[i]));
+        sig.push_back(int64_t(d_disp_lefts[i]));
+        sig.push_back(int64_t(d_disp_rights[i]));
+    }
+    int64_t pw[sizeof(elas_params) / 8 + 1] = {};
+    std::memcpy(pw, &h->params, sizeof(elas_params));
+    for (int64_t x : pw) sig.push_back(x);
+    sig.push_back(int64_t(st));
+    if (h->use_graphs && h->graph_exec && sig == h->graph_sig) {
+        CK(cudaGraphLaunch(h->graph_exec, st));
+    } else {
+        // eager run: sizes every workspace, tunes the dense shape, produces the result
+        rc = issue_batch(h, n, d_lefts, d_rights, d_disp_lefts, d_disp_rights, dims, disp_max_per_pair, false, st);
+        if (rc != ELAS_OK) return rc;
+        if (h->use_graphs) {
+            CK(cudaStreamSynchronize(st));
+            if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            rc = issue_batch(h, n, d_lefts, d_rights, d_disp_lefts, d_disp_rights, dims, disp_max_per_pair, false,
+                             st, true);
+            cudaGraph_t graph = nullptr;
+            cudaError_t e = cudaStreamEndCapture(st, &graph);
+            if (rc != ELAS_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
+            if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&h->graph_exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) { h->graph_exec = nullptr; return cuda_fail(h, e, "cudaGraphInstantiate"); }
+            h->graph_sig = sig;
+        }
+    }
+    if (!stream) CK(cudaStreamSynchronize(st));
+    return ELAS_OK;
+}
+
+int elas_b200_set_graphs(elas_handle* h, int enable) {
+    if (!h) return ELAS_ERR_INVALID_ARG;
+    h->use_graphs = enable != 0;
+    return ELAS_OK;
+}
+
+int elas_b200_batch_latency(elas_handle* h, float* ms_out, int n) {
+    if (!h || !ms_out || n < h->last_batch) return -ELAS_ERR_INVALID_ARG;
+    for (int i = 0; i < h->last_batch; ++i) {
+        if (cudaEventSynchronize(h->lat_done[i]) != cudaSuccess ||
+            cudaEventElapsedTime(&ms_out[i], h->lat_start, h->lat_done[i]) != cudaSuccess)
+            return -ELAS_ERR_CUDA;
+    }
+    return h->last_batch;
+}
+
+int elas_b200_dense_shape(const elas_handle* h, int32_t width, int32_t disp_max) {
+    if (!h) return 0;
+    auto it = h->dense_threads.find(std::make_pair((width + 127) / 128, int(disp_max)));
+    return it == h->dense_threads.end() ? 0 : it->second;
 }
 
 int elas_b200_get_stage(elas_handle* h, int stage, void* dst, size_t bytes, size_t* needed) {

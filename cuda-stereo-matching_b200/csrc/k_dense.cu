@@ -174,7 +174,7 @@ constexpr int LMAX = 48;
 // blockIdx.x = row, blockIdx.y = view (0 left, 1 right).  The other view's
 // descriptor row arrives by bulk copy (TMA) while the CTA expands the
 // candidate lists of the row's grid cells into shared memory.
-__global__ void __launch_bounds__(512) k_dense(const uint4* __restrict__ desc0, const uint4* __restrict__ desc1,
+__global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0, const uint4* __restrict__ desc1,
                                                const uint32_t* __restrict__ prior0, const uint32_t* __restrict__ prior1,
                                                const uint32_t* __restrict__ grid0, const uint32_t* __restrict__ grid1,
                                                float* __restrict__ disp0, float* __restrict__ disp1, Geom g,
@@ -320,10 +320,11 @@ size_t dense_smem_bytes(const Geom& g) { return size_t(g.W) * 16 + size_t(g.gw) 
 
 cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t* prior0, const uint32_t* prior1,
                          const uint32_t* grid0, const uint32_t* grid1, float* disp0, float* disp1, const Geom& g,
-                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st) {
+                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads) {
     size_t smem = dense_smem_bytes(g);
     cudaFuncSetAttribute(k_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    int threads = g.W >= 512 ? 512 : ((g.W + 31) / 32) * 32;
+    if (threads <= 0) threads = 512;
+    threads = imin(threads, ((g.W + 31) / 32) * 32);
     k_dense<<<dim3(g.H, 2), threads, smem, st>>>(desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
                                                   pshift, err);
     return cudaGetLastError();

@@ -69,7 +69,7 @@ size_t raster_bytes();
 size_t dense_smem_bytes(const Geom& g);
 cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t* prior0, const uint32_t* prior1,
                          const uint32_t* grid0, const uint32_t* grid1, float* disp0, float* disp1, const Geom& g,
-                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st);
+                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads);
 
 cudaError_t launch_lr(const float* d0, const float* d1, float* o0, float* o1, const Geom& g, int lr_threshold,
                       cudaStream_t st);

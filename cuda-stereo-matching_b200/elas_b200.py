@@ -81,6 +81,11 @@ def library():
                                                  c_void_p]
         lib.elas_b200_process_batch.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                                 c_void_p, c_void_p]
+        lib.elas_b200_process_batch_device.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                                       c_void_p, c_void_p, c_void_p]
+        lib.elas_b200_set_graphs.argtypes = [c_void_p, c_int]
+        lib.elas_b200_batch_latency.argtypes = [c_void_p, c_void_p, c_int]
+        lib.elas_b200_dense_shape.argtypes = [c_void_p, c_int32, c_int32]
         lib.elas_b200_get_stage.argtypes = [c_void_p, c_int, c_void_p, c_size_t, POINTER(c_size_t)]
         lib.elas_b200_set_timing.argtypes = [c_void_p, c_int]
         lib.elas_b200_get_timing.argtypes = [c_void_p, c_void_p, c_int]
@@ -221,6 +226,32 @@ class Elas:
                                                       arr(outs2), _ptr(dims), _ptr(dm) if dm is not None else None,
                                                       None))
         return outs1, outs2
+
+    def process_batch_device(self, lefts, rights, outs1, outs2, dims, disp_max=None, stream=None):
+        """Batch on device pointers (ints); dims is a sequence of (width, height).
+        Replays a cached CUDA graph when sizes, buffers, parameters and stream
+        repeat."""
+        n = len(lefts)
+        d = np.asarray(dims, np.int32).reshape(-1)
+        arr = lambda xs: (c_void_p * n)(*[int(x) for x in xs])
+        dm = np.asarray(disp_max, np.int32) if disp_max is not None else None
+        self._check(self._lib.elas_b200_process_batch_device(self._h, n, arr(lefts), arr(rights), arr(outs1),
+                                                             arr(outs2), _ptr(d), _ptr(dm) if dm is not None else None,
+                                                             c_void_p(stream) if stream else None))
+
+    def set_graphs(self, enable=True):
+        self._check(self._lib.elas_b200_set_graphs(self._h, int(bool(enable))))
+
+    def batch_latency(self, n):
+        """Milliseconds from the last batch's start to each pair's completion."""
+        out = np.zeros(max(n, 1), np.float32)
+        rc = self._lib.elas_b200_batch_latency(self._h, _ptr(out), n)
+        if rc < 0:
+            self._check(-rc)
+        return out[:rc]
+
+    def dense_shape(self, width, disp_max):
+        return self._lib.elas_b200_dense_shape(self._h, width, disp_max)
 
     def stage(self, name):
         """Copy an intermediate stage of the last single-pair call."""

@@ -136,6 +136,34 @@ int elas_b200_process_batch(elas_handle* h, int n,
                             const int32_t* dims, const int32_t* disp_max_per_pair,
                             void* stream);
 
+/*
+ * Batched form on device buffers (pointer arrays in host memory).  Pair i
+ * runs on its own worker (workspace + stream); the whole batch -- fork, n
+ * pipelines, join -- is captured once into a CUDA graph and later calls with
+ * the same sizes, disparity ranges, buffers, parameters and stream replay it
+ * with a single graph launch.  The first call of a new signature runs
+ * eagerly (sizing workspaces, tuning the dense kernel) and then captures.
+ * stream NULL: an internal stream, and the call returns when done.
+ * No counterpart in the reference (one pair per call, src/Elas.cu:19).
+ */
+int elas_b200_process_batch_device(elas_handle* h, int n,
+                                   const uint8_t* const* d_lefts, const uint8_t* const* d_rights,
+                                   float* const* d_disp_lefts, float* const* d_disp_rights,
+                                   const int32_t* dims, const int32_t* disp_max_per_pair,
+                                   void* stream);
+
+/* Capture and replay batches as CUDA graphs (1, default) or run eagerly (0). */
+int elas_b200_set_graphs(elas_handle* h, int enable);
+
+/* Per-pair latency (ms from the batch's start to the pair's completion) of
+ * the last batch.  Returns the number of pairs (>= 0), or minus a status
+ * code (too small an output, a failed event query). */
+int elas_b200_batch_latency(elas_handle* h, float* ms_out, int n);
+
+/* Threads per CTA the dense-matching autotuner chose for this width class
+ * and disparity range (0 = not tuned yet). */
+int elas_b200_dense_shape(const elas_handle* h, int32_t width, int32_t disp_max);
+
 /* ---- introspection of the last call (for stage-wise parity checks) ---- */
 
 /* Stages that can be copied out after a process call. */

@@ -224,3 +224,42 @@ def test_cpp_drop_in_class_runs(tmp_path):
     out = subprocess.run([str(exe), "run"], capture_output=True, text=True, timeout=120)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "density" in out.stdout
+
+
+def test_batch_device_graph_replay_equals_singles(elas):
+    """Batched device call: the first call runs eagerly and captures a CUDA
+    graph, the second (same buffers, new image contents) replays it; both
+    must equal single-pair runs with each pair's own disparity range."""
+    import torch
+
+    shapes = [(320, 240, 64), (640, 480, 128), (480, 272, 256), (336, 256, 64)]
+    p = eb.params_config(64)
+    elas.set_params(p)
+    bufs = []
+    for (w, h, _) in shapes:
+        bufs.append([torch.empty((h, w), dtype=torch.uint8, device="cuda"),
+                     torch.empty((h, w), dtype=torch.uint8, device="cuda"),
+                     torch.empty((h, w), dtype=torch.float32, device="cuda"),
+                     torch.empty((h, w), dtype=torch.float32, device="cuda")])
+    dims = [(w, h) for (w, h, _) in shapes]
+    dmax = [d for (_, _, d) in shapes]
+    elas.set_graphs(True)
+    for seed in (11, 12, 13):
+        pairs = [eb.synth_pair(3, seed * 10 + i, width=w, height=h, disp_max=d, gt=False)
+                 for i, (w, h, d) in enumerate(shapes)]
+        for b, (L, R, _, _) in zip(bufs, pairs):
+            b[0].copy_(torch.from_numpy(L))
+            b[1].copy_(torch.from_numpy(R))
+        torch.cuda.synchronize()
+        elas.process_batch_device([b[0].data_ptr() for b in bufs], [b[1].data_ptr() for b in bufs],
+                                  [b[2].data_ptr() for b in bufs], [b[3].data_ptr() for b in bufs], dims, dmax)
+        lat = elas.batch_latency(len(shapes))
+        assert lat.shape == (len(shapes),) and (lat > 0).all()
+        got = [(b[2].cpu().numpy(), b[3].cpu().numpy()) for b in bufs]
+        for (L, R, _, _), d, (x1, x2) in zip(pairs, dmax, got):
+            elas.set_params(eb.params_config(d))
+            s1, s2 = elas.process(L, R)
+            assert np.array_equal(s1, x1) and np.array_equal(s2, x2)
+        elas.set_params(p)
+    for (w, _, d) in shapes:
+        assert elas.dense_shape(w, d) in (128, 256, 512, 1024)
