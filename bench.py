@@ -378,6 +378,20 @@ def run_batch(torch, args, flush, stream):
     return out
 
 
+def run_only(args):
+    import torch
+
+    torch.cuda.set_device(0)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    hbm, peak_kind = peaks()
+    if args.only == "large":
+        out = run_large(torch, args, flush, stream, hbm, peak_kind)
+    else:
+        out = run_batch(torch, args, flush, stream)
+    print(json.dumps(out))
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -420,11 +434,15 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--only", choices=["large", "batch"], default=None,
+                    help="run one secondary workload alone (for profiling) and print its block")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.only:
+        run_only(args)
     else:
         run_ours(args)
 
