@@ -112,7 +112,17 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup(args):
+def replica_seed(rank):
+    """Seed of the pair rank `rank` processes: every replica works on its own pair."""
+    return 1000 + rank
+
+
+def aggregate_rate(units_per_rank, max_seconds, world):
+    """Whole-job throughput: the units all ranks processed over the slowest rank's time."""
+    return units_per_rank * world / max_seconds
+
+
+def dist_setup(args, backend=None):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -122,7 +132,7 @@ def dist_setup(args):
         import torch
         import torch.distributed as dist
 
-        backend = "nccl" if args.impl == "ours" else "gloo"
+        backend = backend or ("nccl" if args.impl == "ours" else "gloo")
         if backend == "nccl":
             torch.cuda.set_device(local)
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
@@ -233,7 +243,7 @@ def run_ours(args):
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
     W, H, D = eb.synth_dims(PRESET)
-    L, R, gt, _ = eb.synth_pair(PRESET, 1000 + rank)
+    L, R, gt, _ = eb.synth_pair(PRESET, replica_seed(rank))
     p = eb.params_config(D)
     e = eb.Elas(p, device=local)
     e.set_timing(True)
@@ -249,7 +259,7 @@ def run_ours(args):
     clk = clocks.stop()
     max_ms = max_over_ranks(total_ms, world, device="cuda")
     pairs = args.steps * world
-    value = pairs / (max_ms / 1e3)
+    value = aggregate_rate(args.steps, max_ms / 1e3, world)
     ms_per_step = max_ms / args.steps
 
     e2e_s, e2e_bytes = time_e2e(e, L, R, args.steps, torch, flush)
