@@ -115,23 +115,33 @@ HD int strip_tri_lower(Pts P, const int32_t* A, int m, const int32_t* B, int k, 
 // Returns the number of counter-clockwise triangles written.
 HD int fill_pockets(const int32_t* ci, const int32_t* cx, const int32_t* cy, int len, int side, int32_t* stack,
                     int32_t* tri) {
+    // the two top stack entries are kept in registers: (a, b) = stack[sp-2], stack[sp-1]
     int sp = 0, k = 0;
+    int32_t ia = 0, ib = 0;
+    int64_t ax = 0, ay = 0, bx = 0, by = 0;
     for (int i = 0; i < len; ++i) {
+        const int64_t x = cx[i], y = cy[i];
+        const int32_t ii = ci[i];
         while (sp >= 2) {
-            int a = stack[sp - 2], b = stack[sp - 1];
-            int64_t o = (int64_t(cx[b]) - cx[a]) * (int64_t(cy[i]) - cy[a]) -
-                        (int64_t(cy[b]) - cy[a]) * (int64_t(cx[i]) - cx[a]);
+            const int64_t o = (bx - ax) * (y - ay) - (by - ay) * (x - ax);
             if (side > 0 ? (o > 0) : (o < 0)) {
-                tri[3 * k] = ci[a];
-                tri[3 * k + 1] = side > 0 ? ci[b] : ci[i];
-                tri[3 * k + 2] = side > 0 ? ci[i] : ci[b];
+                tri[3 * k] = ia;
+                tri[3 * k + 1] = side > 0 ? ib : ii;
+                tri[3 * k + 2] = side > 0 ? ii : ib;
                 ++k;
                 --sp;
+                ib = ia; bx = ax; by = ay;
+                if (sp >= 2) {
+                    const int a = stack[sp - 2];
+                    ia = ci[a]; ax = cx[a]; ay = cy[a];
+                }
             } else {
                 break;
             }
         }
         stack[sp++] = i;
+        ia = ib; ax = bx; ay = by;
+        ib = ii; bx = x; by = y;
     }
     return k;
 }

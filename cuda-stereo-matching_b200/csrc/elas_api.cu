@@ -52,7 +52,6 @@ struct elas_handle {
     int32_t* lab[2] = {nullptr, nullptr};        // union-find labels per view
     int32_t* root[2] = {nullptr, nullptr};       // union-find roots per view
     int32_t* usize[2] = {nullptr, nullptr};      // segment sizes per view
-    float* wtab = nullptr;                       // adaptive-mean weight table
     unsigned* err = nullptr;
 
     // per-stage timing
@@ -203,7 +202,7 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         D.rcnt = (int32_t*)take(rows * 4);
         D.ne = (int32_t*)take(rows * 4);
         D.soff = (int32_t*)take(rows * 4);
-        D.chain = (int32_t*)take(4 * rows * 4);
+        D.chain = (int32_t*)take(8 * rows * 4);
         D.tri = (int32_t*)take(3 * tmax * 4);
         D.opp = (int32_t*)take(3 * tmax * 4);
         D.txy = (uint32_t*)take(3 * tmax * 4);
@@ -240,7 +239,6 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         h->root[k] = (int32_t*)take(px * 4);
         h->usize[k] = (int32_t*)take(px * 4);
     }
-    h->wtab = (float*)take(WTAB_SIZE * 4);
     h->err = (unsigned*)take(64);
     return off;
 }
@@ -378,7 +376,6 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     CK(cudaMemcpyAsync(out0, h->lr0, size_t(W) * H * 4, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(out1, h->lr1, size_t(W) * H * 4, cudaMemcpyDeviceToDevice, st));
     PostViews pv;
-    pv.wtab = h->wtab;
     float* outs[2] = {out0, out1};
     for (int k = 0; k < 2; ++k) {
         pv.cur[k] = outs[k];

@@ -142,26 +142,43 @@ __global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32
         if (s < R - 1) D.soff[s] = off + pos;
         off += total;
     }
+    // the two pockets are walked at once by lanes 0 of warps 0 and 1, each on
+    // its own copy of the chain; the right side writes behind the left one's
+    // room (at most R-2 triangles) and is moved down when both are done
     const bool in_smem = R <= smem_rows;
-    int32_t* ci = in_smem ? sh : D.chain;
-    int32_t* cx = ci + (in_smem ? smem_rows : nrows);
-    int32_t* cy = cx + (in_smem ? smem_rows : nrows);
-    int32_t* stk = cy + (in_smem ? smem_rows : nrows);
+    const int cap = in_smem ? smem_rows : nrows;
     int pockets = 0;
+    __shared__ int npk[2];
     if (R >= 2 && off + 2 * R > D.Tmax) {
         if (threadIdx.x == 0) set_err(err, ERRF_TRI_COUNT);
     } else if (R >= 2) {
-        for (int side = 0; side < 2; ++side) {
-            for (int s = threadIdx.x; s < R; s += blockDim.x) {
-                int r = D.ne[s];
-                int i = D.srt[row_off[r] + (side ? D.rcnt[r] - 1 : 0)];
-                ci[s] = i; cx[s] = D.x[i]; cy[s] = D.y[i];
-            }
+        for (int e = threadIdx.x; e < 2 * R; e += blockDim.x) {
+            const int side = e >= R, s = e - side * R;
+            int32_t* ci = (in_smem ? sh : D.chain) + side * 4 * cap;
+            const int r = D.ne[s];
+            const int i = D.srt[row_off[r] + (side ? D.rcnt[r] - 1 : 0)];
+            ci[s] = i; ci[cap + s] = D.x[i]; ci[2 * cap + s] = D.y[i];
+        }
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0 && threadIdx.x < 64) {
+            const int side = threadIdx.x >> 5;
+            int32_t* ci = (in_smem ? sh : D.chain) + side * 4 * cap;
+            npk[side] = fill_pockets(ci, ci + cap, ci + 2 * cap, R, side ? -1 : +1, ci + 3 * cap,
+                                     D.tri + 3 * size_t(off + side * R));
+        }
+        __syncthreads();
+        const int k0 = npk[0], k1 = npk[1];
+        // move the right side's triangles from off+R to off+k0 (k0 <= R-2, so
+        // a forward copy in rounds of one block never overwrites unread data)
+        for (int b0 = 0; b0 < 3 * k1; b0 += blockDim.x) {
+            const int j = b0 + threadIdx.x;
+            int32_t v = 0;
+            if (j < 3 * k1) v = D.tri[3 * size_t(off + R) + j];
             __syncthreads();
-            if (threadIdx.x == 0)
-                pockets += fill_pockets(ci, cx, cy, R, side ? -1 : +1, stk, D.tri + 3 * size_t(off + pockets));
+            if (j < 3 * k1) D.tri[3 * size_t(off + k0) + j] = v;
             __syncthreads();
         }
+        pockets = k0 + k1;
     }
     if (threadIdx.x == 0) {
         D.ctr[0] = (R >= 2 && off + 2 * R <= D.Tmax) ? off + pockets : 0;
@@ -616,8 +633,8 @@ int cluster_size_for_flip() {
 cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int nmax, int num_sms,
                             int csize, unsigned* err, cudaStream_t st, int* nlaunch) {
     k_rowsort<<<dim3(nrows, 2), 512, 0, st>>>(d0, d1, row_off, nrows, err);
-    int smem_rows = imin(nrows, (96 * 1024) / 16);
-    size_t smem = size_t(smem_rows) * 16;
+    int smem_rows = imin(nrows, (96 * 1024) / 32);     // 2 sides x (index, x, y, stack)
+    size_t smem = size_t(smem_rows) * 32;
     cudaFuncSetAttribute(k_plan, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     k_plan<<<2, 1024, smem, st>>>(d0, d1, row_off, nrows, smem_rows, err);
     int blocks = 4 * num_sms;

@@ -213,12 +213,6 @@ __global__ void k_uf_apply_v(PostViews pv, int n, int min_size) {
         if (i0 + k < n) O[i0 + k] = s4[k] < min_size ? -1.0f : d[k];
 }
 
-__global__ void k_wtab(float* wtab) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= WTAB_SIZE) return;
-    float q = float(k) * 0.25f;
-    wtab[k] = __frcp_rn(__fmaf_rn(q, q, 1.0f));
-}
 
 __global__ void k_uf_apply(float* D, const int32_t* __restrict__ root, const int32_t* sz, int n, int min_size) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -271,8 +265,25 @@ __device__ __forceinline__ float gap_fill(const float* line, int stride, int k, 
     return c;
 }
 
+// 9-input sorting network (25 compare-exchanges, depth 7; checked by the
+// 0-1 principle on all 512 binary inputs).
+__device__ __forceinline__ void sort9(float* a) {
+    constexpr int NET[25][2] = {{0, 3}, {1, 7}, {2, 5}, {4, 8}, {0, 7}, {2, 4}, {3, 8}, {5, 6}, {0, 2},
+                                {1, 3}, {4, 5}, {7, 8}, {1, 4}, {3, 6}, {5, 7}, {0, 1}, {2, 4}, {3, 5},
+                                {6, 8}, {2, 3}, {4, 5}, {6, 7}, {1, 2}, {3, 4}, {5, 6}};
+#pragma unroll
+    for (int k = 0; k < 25; ++k) {
+        float x = a[NET[k][0]], y = a[NET[k][1]];
+        a[NET[k][0]] = fminf(x, y);
+        a[NET[k][1]] = fmaxf(x, y);
+    }
+}
+
+constexpr int WT_SMEM = 1024;                   // adaptive-mean weights for |diff| = k/4, k < 1024
+
 template <bool GAP, bool MEAN, bool MEDIAN>
 __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, int gap) {
+    __shared__ float WT[MEAN ? WT_SMEM : 1];
     __shared__ float S[PS][PS];                 // input, halo PHALO
     __shared__ float G[PS][PT + 6];             // after the row pass: columns [-3, 35)
     __shared__ float V[PT + 6][PT + 6];         // after the column pass: [-3, 35)^2
@@ -281,6 +292,10 @@ __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, 
     float* __restrict__ dst = pv.nxt[blockIdx.z];
     const int u0 = blockIdx.x * PT, v0 = blockIdx.y * PT, tid = threadIdx.x;
     const float OUT = -2.0f;                    // outside the image (never valid, never filled)
+    if (MEAN) {
+        float q = float(tid) * 0.25f;
+        WT[tid] = __frcp_rn(__fmaf_rn(q, q, 1.0f));
+    }
     for (int i = tid; i < PS * PS; i += 1024) {
         int r = i / PS, c = i % PS;
         int x = u0 - PHALO + c, y = v0 - PHALO + r;
@@ -317,12 +332,11 @@ __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, 
                     float dq = V[r + 2 + dy][c + 2 + dx];
                     if (dq < 0) continue;
                     float diff = __fsub_rn(dq, dp);
-                    // disparities here are multiples of 1/4, so the weight is a
-                    // table entry computed by the same correctly rounded operation
+                    // |diff| = k/4 for small k almost everywhere: the weight is then a
+                    // table entry made by the same correctly rounded operation
                     float k4 = fabsf(diff) * 4.0f;
                     int ki = int(k4);
-                    float w = (float(ki) == k4 && ki < WTAB_SIZE) ? __ldg(&pv.wtab[ki])
-                                                                  : __frcp_rn(__fmaf_rn(diff, diff, 1.0f));
+                    float w = (float(ki) == k4 && ki < WT_SMEM) ? WT[ki] : __frcp_rn(__fmaf_rn(diff, diff, 1.0f));
                     num = __fmaf_rn(w, dq, num);
                     den = __fadd_rn(den, w);
                 }
@@ -338,20 +352,21 @@ __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, 
             float c = M[ty + 1][tx + 1];
             float out = c;
             if (MEDIAN && c >= 0) {
+                // invalid neighbours sort last as +inf; the lower median of the
+                // n valid values is then element (n-1)/2 (all in registers)
                 float a[9];
                 int n = 0;
-                for (int dy = -1; dy <= 1; ++dy)
-                    for (int dx = -1; dx <= 1; ++dx) {
-                        float q = M[ty + 1 + dy][tx + 1 + dx];
-                        if (q >= 0) a[n++] = q;
-                    }
-                for (int i = 1; i < n; ++i) {
-                    float x = a[i];
-                    int j = i - 1;
-                    while (j >= 0 && a[j] > x) { a[j + 1] = a[j]; --j; }
-                    a[j + 1] = x;
+#pragma unroll
+                for (int k = 0; k < 9; ++k) {
+                    float q = M[ty + k / 3][tx + k % 3];
+                    n += q >= 0 ? 1 : 0;
+                    a[k] = q >= 0 ? q : INFINITY;
                 }
-                out = a[(n - 1) / 2];
+                sort9(a);
+                const int m = (n - 1) >> 1;     // n >= 1 (the centre), so m in [0, 4]
+                out = a[0];
+#pragma unroll
+                for (int k = 1; k < 5; ++k) out = m == k ? a[k] : out;
             }
             dst[size_t(v) * W + u] = out;
         }
@@ -386,10 +401,6 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         launched += 2;
     }
     if (tile_gap || adaptive_mean || median) {
-        if (adaptive_mean) {
-            k_wtab<<<(WTAB_SIZE + 255) / 256, 256, 0, st>>>(pv.wtab);
-            launched += 1;
-        }
         dim3 grid((W + PT - 1) / PT, (H + PT - 1) / PT, nviews);
         const int key = (tile_gap ? 4 : 0) | (adaptive_mean ? 2 : 0) | (median ? 1 : 0);
         switch (key) {

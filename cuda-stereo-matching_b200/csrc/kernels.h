@@ -15,7 +15,7 @@ struct DelDev {
     int32_t* rcnt;         // [rows] unique points per row
     int32_t* ne;           // [rows] non-empty rows
     int32_t* soff;         // [rows] strip triangle offsets
-    int32_t* chain;        // [4*rows] pocket walk scratch when it does not fit in shared memory
+    int32_t* chain;        // [8*rows] pocket walk scratch (2 sides) when it does not fit in shared memory
     int32_t* tri;          // [3*Tmax]
     int32_t* opp;          // [3*Tmax]
     uint32_t* txy;         // [3*Tmax] packed corner coordinates (global flip kernel)
@@ -84,9 +84,7 @@ struct PostViews {
     int32_t* lab[2];
     int32_t* root[2];
     int32_t* sz[2];
-    float* wtab;     // adaptive-mean weights 1/(1 + (k/4)^2), k = 0 .. WTAB_SIZE-1
 };
-constexpr int WTAB_SIZE = 4 * 4096 + 8;
 
 // Post-filters on nviews (1 or 2) disparity images.
 cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams& p, bool median, bool adaptive_mean,
