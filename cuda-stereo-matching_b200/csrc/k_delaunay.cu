@@ -184,7 +184,8 @@ __global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32
         D.ctr[0] = (R >= 2 && off + 2 * R <= D.Tmax) ? off + pockets : 0;
         D.ctr[1] = off;
         D.ctr[6] = R;
-        D.ctr[8] = 0;    // set to 1 by the cluster flip kernel when it handles the problem
+        D.ctr[8] = 0;    // set to 1 by the flip kernel that handles the problem
+        D.ctr[9] = row_off[nrows];   // support points (vertex ids) of the problem
     }
 }
 
@@ -429,30 +430,158 @@ struct ClusterTri {
     __device__ void set_fround(int t, int32_t r) { at(lround, t)[t & mask] = r; }
 };
 
-// The same record layout in this CTA's own shared memory, for problems that
-// fit one SM (plain shared-memory accesses, __syncthreads between phases).
-struct LocalTri {
+// Point-table accessor for a problem that fits one SM: corner coordinates
+// are looked up per vertex (4 bytes per support point instead of 12 per
+// triangle), which leaves shared memory for the round lists.
+struct PtTri {
     int32_t* lv;
-    uint32_t* lxy;
+    const uint32_t* pxy;
     int32_t* lopp;
     uint32_t* llock;
     int32_t* lround;
-    int shift, mask;
-    template <class X>
-    __device__ __forceinline__ X* at(X* base, int) const { return base; }
     __device__ int v(int t, int k) const { return lv[3 * t + k]; }
-    __device__ uint32_t xy(int t, int k) const { return lxy[3 * t + k]; }
+    __device__ uint32_t xy(int t, int k) const { return pxy[lv[3 * t + k]]; }
     __device__ int opp(int h) const { return lopp[h]; }
     __device__ uint32_t lock(int t) const { return *((volatile uint32_t*)llock + t); }
     __device__ int32_t fround(int t) const { return lround[t]; }
     __device__ void lock_min(int t, uint32_t p) { atomicMin(llock + t, p); }
-    __device__ void set_v(int t, int a, int b, int c, uint32_t pa, uint32_t pb, uint32_t pc) {
+    __device__ void set_v(int t, int a, int b, int c, uint32_t, uint32_t, uint32_t) {
         lv[3 * t] = a; lv[3 * t + 1] = b; lv[3 * t + 2] = c;
-        lxy[3 * t] = pa; lxy[3 * t + 1] = pb; lxy[3 * t + 2] = pc;
     }
     __device__ void set_opp(int h, int o) { lopp[h] = o; }
     __device__ void set_fround(int t, int32_t r) { lround[t] = r; }
 };
+
+// A round list whose first entries live in shared memory and the rest in
+// global memory (records of `width` ints).
+struct List2 {
+    int32_t* s;
+    int32_t* g;
+    int scap, gcap, width;
+    __device__ int32_t* slot(int i) const { return i < scap ? s + width * i : g + width * (i - scap); }
+    __device__ int cap() const { return scap + gcap; }
+};
+
+constexpr int LOC_T = 4096;        // triangles of a one-SM problem
+constexpr int LOC_PTS = 4096;      // support points (vertex ids) of a one-SM problem
+constexpr int LOC_WL = 3072;       // worklist entries per buffer in shared memory
+constexpr int LOC_CAND = 2048;     // proposals in shared memory
+constexpr int LOC_FLIP = 1280;     // flipped pairs in shared memory
+constexpr size_t LOC_SMEM = size_t(32) * LOC_T + size_t(4) * LOC_PTS + size_t(8) * LOC_WL + size_t(8) * LOC_CAND +
+                            size_t(24) * LOC_FLIP;
+
+// Flip rounds of one problem in one CTA: triangles, points and the round
+// lists in shared memory, __syncthreads between the phases.  Problems with
+// more triangles or points are left (ctr[8] stays 0) to the cluster kernel.
+__global__ void __launch_bounds__(1024) k_flip_local(DelDev d0, DelDev d1, int max_rounds, unsigned* err) {
+    extern __shared__ __align__(16) uint8_t lsm[];
+    __shared__ int n_cand, n_flip, n_wl[2], stop;
+    const DelDev& D = blockIdx.x ? d1 : d0;
+    const int T = D.ctr[0], NP = D.ctr[9];
+    if (D.ctr[8] != 0 || T > LOC_T || NP > LOC_PTS) return;
+    const int tid = threadIdx.x, NT = blockDim.x;
+    PtTri m;
+    m.lv = reinterpret_cast<int32_t*>(lsm);
+    m.lopp = m.lv + 3 * LOC_T;
+    m.llock = reinterpret_cast<uint32_t*>(m.lopp + 3 * LOC_T);
+    m.lround = reinterpret_cast<int32_t*>(m.llock + LOC_T);
+    uint32_t* pxy = reinterpret_cast<uint32_t*>(m.lround + LOC_T);
+    m.pxy = pxy;
+    int32_t* sw = reinterpret_cast<int32_t*>(pxy + LOC_PTS);
+    List2 wl[2] = {{sw, D.cwl, LOC_WL, WL_PER_CTA, 1}, {sw + LOC_WL, D.cwl + WL_PER_CTA, LOC_WL, WL_PER_CTA, 1}};
+    List2 cand{sw + 2 * LOC_WL, D.ccand, LOC_CAND, CAND_PER_CTA, 2};
+    List2 flips{sw + 2 * LOC_WL + 2 * LOC_CAND, D.cflips, LOC_FLIP, FLIP_PER_CTA, 6};
+    for (int i = tid; i < NP; i += NT) pxy[i] = pack_xy(D.x[i], D.y[i]);
+    for (int t = tid; t < T; t += NT) {
+        for (int k = 0; k < 3; ++k) {
+            m.lv[3 * t + k] = D.tri[3 * t + k];
+            m.lopp[3 * t + k] = D.opp[3 * t + k];
+        }
+        m.llock[t] = LOCK_FREE;
+        m.lround[t] = -1;
+    }
+    if (tid == 0) { n_cand = 0; n_flip = 0; n_wl[0] = n_wl[1] = 0; stop = 0; }
+    __syncthreads();
+    int round = 0, flips_total = 0;
+    bool converged = false;
+    for (; round < max_rounds; ++round) {
+        const int cur = round & 1, nxt = cur ^ 1;
+        // A: propose (round 0: every half-edge, owner rule)
+        const int items = round == 0 ? 3 * T : min(n_wl[cur], wl[cur].cap());
+        auto add_cand = [&](int hh, int nn) {
+            int idx = atomicAdd(&n_cand, 1);
+            if (idx < cand.cap()) { int32_t* c = cand.slot(idx); c[0] = hh; c[1] = nn; }
+        };
+        for (int k = tid; k < items; k += NT) {
+            int h = round == 0 ? k : *wl[cur].slot(k);
+            if (!flip_propose(m, h, T, uint32_t(round), round == 0, add_cand)) set_err(err, ERRF_BOUNDS);
+        }
+        if (tid == 0) n_wl[nxt] = 0;       // nobody appends to it before phase C2
+        __syncthreads();
+        const int ncand = n_cand;
+        if (ncand == 0) { converged = true; break; }
+        const int nc = min(ncand, cand.cap());
+        if (tid == 0 && ncand > cand.cap()) { set_err(err, ERRF_BOUNDS); stop = 1; }
+        // B: flip the winners
+        for (int c = tid; c < nc; c += NT) {
+            const int32_t* cc = cand.slot(c);
+            int h = cc[0], n = cc[1];
+            if (flip_apply(m, h, n, uint32_t(round))) {
+                int f = atomicAdd(&n_flip, 1);     // at most T/2 <= flips.cap()
+                int32_t* q = flips.slot(f);
+                q[0] = h / 3; q[1] = n;
+            }
+        }
+        __syncthreads();
+        const int nf = n_flip;
+        // C1: resolve the outer neighbours (read only)
+        for (int f = tid; f < nf; f += NT) {
+            int32_t* q = flips.slot(f);
+            int t = q[0], n = q[1];
+            for (int k = 0; k < 4; ++k) {
+                int r = flip_resolve_slot(m, outer_slot(t, n, k), uint32_t(round));
+                if (r == -2) { set_err(err, ERRF_BOUNDS); r = -1; }
+                q[2 + k] = r;
+            }
+        }
+        __syncthreads();
+        // C2: relink, queue the outer edges, release locks, requeue lost proposals
+        auto push = [&](int x) {
+            int idx = atomicAdd(&n_wl[nxt], 1);
+            if (idx < wl[nxt].cap()) *wl[nxt].slot(idx) = x;
+        };
+        for (int f = tid; f < nf; f += NT) {
+            int32_t* q = flips.slot(f);
+            int t = q[0], n = q[1];
+            flip_relink(m, t, n, q + 2);
+            for (int k = 0; k < 4; ++k) push(outer_slot(t, n, k));
+        }
+        for (int c = tid; c < nc; c += NT) {
+            const int32_t* cc = cand.slot(c);
+            int h = cc[0], n = cc[1], t = h / 3;
+            m.llock[t] = LOCK_FREE;
+            m.llock[n] = LOCK_FREE;
+            if (m.fround(t) != round && m.fround(n) != round) push(h);
+        }
+        flips_total += nf;
+        __syncthreads();
+        if (tid == 0) {
+            n_cand = 0;
+            n_flip = 0;
+            if (n_wl[nxt] > wl[nxt].cap()) { set_err(err, ERRF_BOUNDS); stop = 1; }
+        }
+        __syncthreads();
+        if (stop) break;
+    }
+    for (int t = tid; t < T; t += NT)
+        for (int k = 0; k < 3; ++k) D.tri[3 * t + k] = m.lv[3 * t + k];
+    if (tid == 0) {
+        D.ctr[8] = 1;
+        D.ctr[4] = round + 1;
+        D.ctr[5] = flips_total;
+        if (!converged) set_err(err, ERRF_FLIP_LIMIT);
+    }
+}
 
 struct ClusterSync {
     __device__ void operator()() const { cg::this_cluster().sync(); }
@@ -460,22 +589,15 @@ struct ClusterSync {
     __device__ X* remote(X* p, int r) const { return cg::this_cluster().map_shared_rank(p, unsigned(r)); }
     __device__ int rank() const { return int(cg::this_cluster().block_rank()); }
 };
-struct BlockSync {
-    __device__ void operator()() const { __syncthreads(); }
-    template <class X>
-    __device__ X* remote(X* p, int) const { return p; }
-    __device__ int rank() const { return 0; }
-};
 
-// Shared-memory flip rounds.  LOCAL: one CTA per problem holding at most
-// SLICE_MAX triangles; otherwise a cluster of csize CTAs (csize * SLICE_MAX).
-// A kernel whose range does not contain T returns at once; the first one
-// that handles a problem sets ctr[8].
-template <bool LOCAL>
+// Flip rounds in distributed shared memory: a cluster of csize CTAs, each
+// holding a slice of at most SLICE_MAX triangles.  A problem already handled
+// (ctr[8] set by the one-SM kernel) or larger than csize * SLICE_MAX is
+// skipped; the kernel that handles a problem sets ctr[8].
 __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, int csize, int max_rounds,
                                                           unsigned* err) {
-    using Acc = typename std::conditional<LOCAL, LocalTri, ClusterTri>::type;
-    using Sync = typename std::conditional<LOCAL, BlockSync, ClusterSync>::type;
+    using Acc = ClusterTri;
+    using Sync = ClusterSync;
     extern __shared__ __align__(16) uint8_t csm[];
     __shared__ int n_cand[2], n_flip, n_wl[2], stop;
     Sync sync;
@@ -484,7 +606,7 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, 
     const DelDev& D = prob ? d1 : d0;
     const int T = D.ctr[0];
     // uniform over the CTAs of a problem: no barrier has been passed yet
-    if (D.ctr[8] != 0 || T > csize * SLICE_MAX || (!LOCAL && T <= SLICE_MAX)) return;
+    if (D.ctr[8] != 0 || T > csize * SLICE_MAX) return;
     int shift = 6;
     while ((csize << shift) < T) ++shift;
     Acc m;
@@ -608,9 +730,8 @@ __global__ void k_normalise(DelDev d0, DelDev d1) {
 int cluster_size_for_flip() {
     int sizes[2] = {16, 8};
     size_t smem = size_t(SLICE_MAX) * 44;
-    cudaFuncSetAttribute(k_flip_smem<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    cudaFuncSetAttribute(k_flip_smem<false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    cudaFuncSetAttribute(k_flip_smem<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaFuncSetAttribute(k_flip_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaFuncSetAttribute(k_flip_smem, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     for (int cs : sizes) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(2 * cs);
@@ -624,7 +745,7 @@ int cluster_size_for_flip() {
         cfg.attrs = &attr;
         cfg.numAttrs = 1;
         int n = 0;
-        if (cudaOccupancyMaxActiveClusters(&n, k_flip_smem<false>, &cfg) == cudaSuccess && n >= 2) return cs;
+        if (cudaOccupancyMaxActiveClusters(&n, k_flip_smem, &cfg) == cudaSuccess && n >= 2) return cs;
         cudaGetLastError();
     }
     return 0;
@@ -644,7 +765,8 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
     k_link<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1, err);
     int launched = 6;
     const int max_rounds = 100000;
-    k_flip_smem<true><<<2, CL_THREADS, size_t(SLICE_MAX) * 44, st>>>(d0, d1, 1, max_rounds, err);
+    cudaFuncSetAttribute(k_flip_local, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LOC_SMEM));
+    k_flip_local<<<2, 1024, LOC_SMEM, st>>>(d0, d1, max_rounds, err);
     ++launched;
     if (csize > 0) {
         cudaLaunchConfig_t cfg = {};
@@ -659,7 +781,7 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
         attr.val.clusterDim.z = 1;
         cfg.attrs = &attr;
         cfg.numAttrs = 1;
-        cudaError_t e = cudaLaunchKernelEx(&cfg, k_flip_smem<false>, d0, d1, csize, max_rounds, err);
+        cudaError_t e = cudaLaunchKernelEx(&cfg, k_flip_smem, d0, d1, csize, max_rounds, err);
         if (e != cudaSuccess) return e;
         ++launched;
     }
