@@ -208,31 +208,6 @@ HD bool inside_sos_p(int ia, uint32_t a, int ib, uint32_t b, int ic, uint32_t c,
     return orient_p(a, b, d) < 0;
 }
 
-// Zipper triangulation of the strip between sorted rows A (na points) and B
-// (nb points, the next non-empty row): from the edge (A[0], B[0]) advance on
-// A with (A[i], A[i+1], B[j]) unless B[j+1] lies inside that triangle's
-// circumcircle (symbolic perturbation), else on B with (A[i], B[j+1], B[j]).
-// The step from state (i, j) is triangle i + j of the strip, as in the
-// merge-path placement; only the choice of triangles differs.
-constexpr int ZIP_MAX = 96;    // longest strip (points of both rows) given to strip_zip
-
-HD void strip_zip(Pts P, const int32_t* A, int na, const int32_t* B, int nb, int32_t* tri) {
-    int i = 0, j = 0;
-    while (i + 1 < na || j + 1 < nb) {
-        bool adv_a;
-        if (i + 1 >= na) adv_a = false;
-        else if (j + 1 >= nb) adv_a = true;
-        else {
-            const int a = A[i], a1 = A[i + 1], b = B[j], b1 = B[j + 1];
-            adv_a = !inside_sos_p(a, pack_xy(P.x[a], P.y[a]), a1, pack_xy(P.x[a1], P.y[a1]), b,
-                                  pack_xy(P.x[b], P.y[b]), b1, pack_xy(P.x[b1], P.y[b1]));
-        }
-        int32_t* t = tri + 3 * (i + j);
-        if (adv_a) { t[0] = A[i]; t[1] = A[i + 1]; t[2] = B[j]; ++i; }
-        else { t[0] = A[i]; t[1] = B[j + 1]; t[2] = B[j]; ++j; }
-    }
-}
-
 // Flip rounds are written against an accessor M that stores, per triangle t:
 // v(t,k) vertex indices, xy(t,k) packed coordinates, opp(3t+k) neighbour
 // half-edges, a lock word and the last round t was flipped in.  The flat

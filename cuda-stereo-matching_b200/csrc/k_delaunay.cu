@@ -212,34 +212,18 @@ __global__ void k_strips(DelDev d0, DelDev d1, const int32_t* __restrict__ row_o
         if (k < 1 || k >= D.rcnt[r]) continue;
         const int32_t* A_row = D.srt + row_off[r];
         int32_t tri[3];
-        if (lo + 1 < R && D.rcnt[r] + D.rcnt[D.ne[lo + 1]] > ZIP_MAX) {   // as the upper row of strip lo
+        if (lo + 1 < R) {       // as the upper row of strip lo
             int rb = D.ne[lo + 1];
             int pos = strip_tri_upper(P, A_row, D.srt + row_off[rb], D.rcnt[rb], k, tri);
             int32_t* o = D.tri + 3 * size_t(D.soff[lo] + pos);
             o[0] = tri[0]; o[1] = tri[1]; o[2] = tri[2];
         }
-        if (lo >= 1 && D.rcnt[D.ne[lo - 1]] + D.rcnt[r] > ZIP_MAX) {       // as the lower row of strip lo-1
+        if (lo >= 1) {          // as the lower row of strip lo-1
             int ra = D.ne[lo - 1];
             int pos = strip_tri_lower(P, D.srt + row_off[ra], D.rcnt[ra], A_row, k, tri);
             int32_t* o = D.tri + 3 * size_t(D.soff[lo - 1] + pos);
             o[0] = tri[0]; o[1] = tri[1]; o[2] = tri[2];
         }
-    }
-}
-
-// Strips of at most ZIP_MAX points are triangulated sequentially by one
-// thread with the zipper (closer to Delaunay: fewer flip rounds); longer
-// strips by merge path above (one thread per point).
-__global__ void k_strips_zip(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off) {
-    const DelDev& D = blockIdx.y ? d1 : d0;
-    const int R = D.ctr[6];
-    if (D.ctr[0] == 0) return;
-    Pts P{D.x, D.y};
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s + 1 < R; s += gridDim.x * blockDim.x) {
-        const int ra = D.ne[s], rb = D.ne[s + 1];
-        const int na = D.rcnt[ra], nb = D.rcnt[rb];
-        if (na + nb > ZIP_MAX) continue;
-        strip_zip(P, D.srt + row_off[ra], na, D.srt + row_off[rb], nb, D.tri + 3 * size_t(D.soff[s]));
     }
 }
 
@@ -776,11 +760,10 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
     k_plan<<<2, 1024, smem, st>>>(d0, d1, row_off, nrows, smem_rows, err);
     int blocks = 4 * num_sms;
     k_strips<<<dim3(imax(1, imin(blocks, (nmax + 255) / 256)), 2), 256, 0, st>>>(d0, d1, row_off, nmax);
-    k_strips_zip<<<dim3((nrows + 63) / 64, 2), 64, 0, st>>>(d0, d1, row_off);
     k_hash_clear<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1);
     k_hash_insert<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1, err);
     k_link<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1, err);
-    int launched = 7;
+    int launched = 6;
     const int max_rounds = 100000;
     cudaFuncSetAttribute(k_flip_local, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LOC_SMEM));
     k_flip_local<<<2, 1024, LOC_SMEM, st>>>(d0, d1, max_rounds, err);

@@ -55,23 +55,18 @@ extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const i
                                     &tri[3 * size_t(off + pockets)]);
         }
         T = off + pockets;
-        // 3. strips: short ones by the zipper (k_strips_zip), the rest by
-        // merge path (k_strips, every point of every non-empty row)
-        for (int lo = 0; lo + 1 < R; ++lo)
-            if (rcnt[ne[lo]] + rcnt[ne[lo + 1]] <= ZIP_MAX)
-                strip_zip(P, &srt[row_off[ne[lo]]], rcnt[ne[lo]], &srt[row_off[ne[lo + 1]]], rcnt[ne[lo + 1]],
-                          &tri[3 * size_t(soff[lo])]);
+        // 3. strips (k_strips), every point of every non-empty row
         for (int lo = 0; lo < R; ++lo) {
             int r = ne[lo];
             const int32_t* A = &srt[row_off[r]];
             for (int k = 1; k < rcnt[r]; ++k) {
                 int32_t t3[3];
-                if (lo + 1 < R && rcnt[r] + rcnt[ne[lo + 1]] > ZIP_MAX) {
+                if (lo + 1 < R) {
                     int rb = ne[lo + 1];
                     int pos = strip_tri_upper(P, A, &srt[row_off[rb]], rcnt[rb], k, t3);
                     std::memcpy(&tri[3 * size_t(soff[lo] + pos)], t3, 12);
                 }
-                if (lo >= 1 && rcnt[ne[lo - 1]] + rcnt[r] > ZIP_MAX) {
+                if (lo >= 1) {
                     int ra = ne[lo - 1];
                     int pos = strip_tri_lower(P, &srt[row_off[ra]], rcnt[ra], A, k, t3);
                     std::memcpy(&tri[3 * size_t(soff[lo - 1] + pos)], t3, 12);
