@@ -13,7 +13,8 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libelas_b200.so")
 OBJ_DIR = os.path.join(HERE, "_build")
 
-CU_SOURCES = ["k_descriptor.cu", "k_support.cu", "k_delaunay.cu", "k_dense.cu", "k_post.cu", "elas_api.cu"]
+CU_SOURCES = ["k_descriptor.cu", "k_support.cu", "k_delaunay.cu", "k_dense.cu", "k_post.cu", "k_proposal.cu",
+              "k_proposal_tc.cu", "elas_api.cu"]
 CPP_SOURCES = ["synth.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -21,6 +21,7 @@
 #include "../../include/elas_b200.h"
 #include "common.cuh"
 #include "kernels.h"
+#include "proposal.h"
 
 using namespace elas;
 
@@ -74,6 +75,17 @@ struct elas_handle {
     std::vector<int64_t> graph_sig;   // what the cached graph was captured for
     int last_batch = 0;
     elas_handle* owner = nullptr;     // the user's handle, for a batch worker
+
+    // learned support-point proposal (off until weights are set)
+    bool prop = false;
+    int prop_version = 0;             // bumped by every elas_b200_set_proposal
+    std::vector<float> prop_params;   // host copy (batch workers upload it)
+    pn::InferWeights pw{};
+    __nv_bfloat16 *pn_in = nullptr, *pn_a0 = nullptr, *pn_a1 = nullptr, *pn_out = nullptr;
+    uint32_t* pn_bins = nullptr;
+    int32_t* pn_stats = nullptr;      // [4]: settled by the proposal, fell back, -, -
+    size_t pn_map_elems = 0, pn_cands = 0;
+    bool pn_used = false;             // the last call ran the proposal
 };
 
 namespace {
@@ -332,6 +344,64 @@ int dense_threads_for(elas_handle* h, const Geom& g, const DevParams& dp, cudaSt
 }
 
 // The whole pipeline on device buffers (inputs img0/img1 already on the device).
+// Proposal buffers: four [2][H/4][W/4][32] bf16 maps and the packed bins of
+// every candidate; grown on demand (outside any stream capture: the first
+// call of a batch runs eagerly).
+int ensure_pn(elas_handle* h, const Geom& g) {
+    const size_t elems = size_t(2) * (g.H / 4) * (g.W / 4) * pn::CH;
+    const size_t cands = size_t(g.cw) * g.ch;
+    if (elems > h->pn_map_elems) {
+        CK(cudaDeviceSynchronize());
+        __nv_bfloat16** bufs[4] = {&h->pn_in, &h->pn_a0, &h->pn_a1, &h->pn_out};
+        for (auto b : bufs) {
+            if (*b) cudaFree(*b);
+            *b = nullptr;
+            if (cudaMalloc(reinterpret_cast<void**>(b), elems * sizeof(__nv_bfloat16)) != cudaSuccess)
+                return fail(h, ELAS_ERR_OOM, "proposal feature maps");
+        }
+        h->pn_map_elems = elems;
+    }
+    if (cands > h->pn_cands) {
+        CK(cudaDeviceSynchronize());
+        if (h->pn_bins) cudaFree(h->pn_bins);
+        h->pn_bins = nullptr;
+        if (cudaMalloc(&h->pn_bins, cands * sizeof(uint32_t)) != cudaSuccess)
+            return fail(h, ELAS_ERR_OOM, "proposal bins");
+        h->pn_cands = cands;
+    }
+    return ELAS_OK;
+}
+
+int set_proposal_weights(elas_handle* h, const float* params, int n) {
+    if (n == 0) { h->prop = false; ++h->prop_version; return ELAS_OK; }
+    if (!params || n != pn::NPARAMS) return fail(h, ELAS_ERR_INVALID_ARG, "proposal parameter count");
+    for (int i = 0; i < n; ++i)
+        if (!std::isfinite(params[i])) return fail(h, ELAS_ERR_INVALID_ARG, "non-finite proposal parameter");
+    if (!h->pw.w) {
+        if (cudaMalloc(&h->pw.w, size_t(pn::LAYERS) * pn::TAPS * pn::CH * pn::CH * sizeof(__nv_bfloat16)) !=
+                cudaSuccess ||
+            cudaMalloc(&h->pw.b, size_t(pn::LAYERS) * pn::CH * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&h->pn_stats, 4 * sizeof(int32_t)) != cudaSuccess)
+            return fail(h, ELAS_ERR_OOM, "proposal weights");
+        CK(cudaMemset(h->pn_stats, 0, 4 * sizeof(int32_t)));
+    }
+    CK(pn::upload_weights(params, h->pw, nullptr));
+    h->prop_params.assign(params, params + n);
+    h->prop = true;
+    ++h->prop_version;
+    return ELAS_OK;
+}
+
+void free_pn(elas_handle* h) {
+    __nv_bfloat16* bufs[4] = {h->pn_in, h->pn_a0, h->pn_a1, h->pn_out};
+    for (auto b : bufs)
+        if (b) cudaFree(b);
+    if (h->pn_bins) cudaFree(h->pn_bins);
+    if (h->pn_stats) cudaFree(h->pn_stats);
+    if (h->pw.w) cudaFree(h->pw.w);
+    if (h->pw.b) cudaFree(h->pw.b);
+}
+
 int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float* out0, float* out1, int W, int H,
                  cudaStream_t st) {
     const elas_params& p = h->params;
@@ -347,7 +417,20 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     CK(launch_descriptor(img0, img1, h->desc0, h->desc1, W, H, st));
     n += 1;
     CK(mark(ELAS_TIME_SUPPORT));
-    CK(launch_support(h->desc0, h->desc1, h->can_lr, nullptr, h->can, g, dp, h->num_sms, h->err, st));
+    const uint32_t* bins = nullptr;
+    h->pn_used = h->prop && H >= 4 && W >= 4 && g.cw > 0 && g.ch > 0;
+    if (h->pn_used) {
+        rc = ensure_pn(h, g);
+        if (rc != ELAS_OK) return rc;
+        CK(cudaMemsetAsync(h->pn_stats, 0, 4 * sizeof(int32_t), st));
+        CK(pn::launch_features(h->desc0, h->desc1, h->pn_in, W, H, st));
+        CK(pn::launch_infer(h->pw, h->pn_in, h->pn_a0, h->pn_a1, h->pn_out, H / 4, W / 4, h->num_sms, h->err, st));
+        CK(pn::launch_topk(h->pn_out, h->pn_bins, H / 4, W / 4, g.cw, g.ch, g.step, g.D, st));
+        bins = h->pn_bins;
+        n += 6;
+    }
+    CK(launch_support(h->desc0, h->desc1, h->can_lr, nullptr, h->can, g, dp, h->num_sms, h->err, st, bins,
+                      h->pn_used ? h->pn_stats : nullptr));
     n += 4;
     CK(mark(ELAS_TIME_COMPACT));
     CK(launch_compact(h->can, h->row_cnt, h->row_off, h->uvd, h->x0, h->x1, h->y, g, st));
@@ -441,6 +524,12 @@ int issue_batch(elas_handle* h, int n, const uint8_t* const* l, const uint8_t* c
         cudaStream_t ws = h->slot_streams[i];
         w->params = h->params;
         if (dmax) w->params.disp_max = dmax[i];
+        if (w->prop_version != h->prop_version) {
+            int rc = set_proposal_weights(w, h->prop ? h->prop_params.data() : nullptr,
+                                          h->prop ? int(h->prop_params.size()) : 0);
+            if (rc != ELAS_OK) return fail(h, rc, w->last_error);
+            w->prop_version = h->prop_version;
+        }
         const int W = dims[2 * i], H = dims[2 * i + 1];
         const size_t px = size_t(W) * H;
         CK(cudaStreamWaitEvent(ws, h->batch_start, 0));
@@ -632,6 +721,7 @@ int elas_b200_destroy(elas_handle* h) {
     }
     if (h->batch_start) cudaEventDestroy(h->batch_start);
     if (h->lat_start) cudaEventDestroy(h->lat_start);
+    free_pn(h);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     for (int i = 0; i <= ELAS_TIME_COUNT; ++i)
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);
@@ -819,6 +909,14 @@ int elas_b200_get_stage(elas_handle* h, int stage, void* dst, size_t bytes, size
         need = size_t(ntri) * 12;
         break;
     case ELAS_STAGE_PRIOR_LEFT: case ELAS_STAGE_PRIOR_RIGHT: need = px * 4; break;
+    case ELAS_STAGE_PN_FEATURES: case ELAS_STAGE_PN_OUTPUT:
+        if (!h->pn_used) return fail(h, ELAS_ERR_INVALID_ARG, "the last call did not run the proposal");
+        need = size_t(2) * (g.H / 4) * (g.W / 4) * pn::CH * 2;
+        break;
+    case ELAS_STAGE_PN_BINS:
+        if (!h->pn_used) return fail(h, ELAS_ERR_INVALID_ARG, "the last call did not run the proposal");
+        need = can_n * 4;
+        break;
     default: need = px * 4; break;
     }
     if (needed) *needed = need;
@@ -863,9 +961,109 @@ int elas_b200_get_stage(elas_handle* h, int stage, void* dst, size_t bytes, size
     case ELAS_STAGE_DISP_RIGHT: CK(cudaMemcpy(dst, h->raw1, need, cudaMemcpyDeviceToHost)); break;
     case ELAS_STAGE_LR_LEFT: CK(cudaMemcpy(dst, h->lr0, need, cudaMemcpyDeviceToHost)); break;
     case ELAS_STAGE_LR_RIGHT: CK(cudaMemcpy(dst, h->lr1, need, cudaMemcpyDeviceToHost)); break;
+    case ELAS_STAGE_PN_FEATURES: CK(cudaMemcpy(dst, h->pn_in, need, cudaMemcpyDeviceToHost)); break;
+    case ELAS_STAGE_PN_OUTPUT: CK(cudaMemcpy(dst, h->pn_out, need, cudaMemcpyDeviceToHost)); break;
+    case ELAS_STAGE_PN_BINS: CK(cudaMemcpy(dst, h->pn_bins, need, cudaMemcpyDeviceToHost)); break;
     default: return fail(h, ELAS_ERR_INVALID_ARG, "bad stage");
     }
     return ELAS_OK;
+}
+
+int elas_b200_set_proposal(elas_handle* h, const float* params, int32_t n) {
+    if (!h) return ELAS_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    return set_proposal_weights(h, params, n);
+}
+
+int elas_b200_proposal_stats(elas_handle* h, int32_t* out, int32_t n) {
+    if (!h || !out || n < 2) return ELAS_ERR_INVALID_ARG;
+    if (!h->pn_used) { out[0] = out[1] = 0; return ELAS_OK; }
+    CK(cudaSetDevice(h->device));
+    CK(cudaDeviceSynchronize());
+    int32_t st[4];
+    CK(cudaMemcpy(st, h->pn_stats, sizeof(st), cudaMemcpyDeviceToHost));
+    out[0] = st[0];
+    out[1] = st[1];
+    return ELAS_OK;
+}
+
+int elas_b200_pn_infer(elas_handle* h, const void* d_in, void* d_out, int32_t hd, int32_t wd, void* stream) {
+    if (!h || !d_in || !d_out || hd <= 0 || wd <= 0) return ELAS_ERR_INVALID_ARG;
+    if (!h->prop) return fail(h, ELAS_ERR_INVALID_ARG, "no proposal weights set");
+    CK(cudaSetDevice(h->device));
+    Geom g{};
+    g.W = 4 * wd;
+    g.H = 4 * hd;
+    g.cw = g.ch = 0;
+    int rc = ensure_pn(h, g);
+    if (rc != ELAS_OK) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned* err = reinterpret_cast<unsigned*>(h->pn_stats + 2);
+    CK(cudaMemsetAsync(err, 0, sizeof(unsigned), st));
+    CK(pn::launch_infer(h->pw, static_cast<const __nv_bfloat16*>(d_in), h->pn_a0, h->pn_a1,
+                        static_cast<__nv_bfloat16*>(d_out), hd, wd, h->num_sms, err, st));
+    h->launches += pn::LAYERS;
+    unsigned e = 0;
+    CK(cudaMemcpyAsync(&e, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (e) return fail(h, ELAS_ERR_TIMEOUT, "proposal inference: a bounded wait ran out");
+    return ELAS_OK;
+}
+
+int elas_b200_pn_features(elas_handle* h, void* d_out, void* stream) {
+    if (!h || !d_out) return ELAS_ERR_INVALID_ARG;
+    if (!h->have_last) return fail(h, ELAS_ERR_INVALID_ARG, "no previous call");
+    CK(cudaSetDevice(h->device));
+    CK(pn::launch_features(h->desc0, h->desc1, static_cast<__nv_bfloat16*>(d_out), h->g.W, h->g.H,
+                           static_cast<cudaStream_t>(stream)));
+    h->launches += 1;
+    return ELAS_OK;
+}
+
+int elas_b200_pn_bf16_to_f32(const void* d_in, float* d_out, size_t n, void* stream) {
+    if (!d_in || !d_out) return ELAS_ERR_INVALID_ARG;
+    cudaError_t e = pn::launch_bf16_to_f32(static_cast<const __nv_bfloat16*>(d_in), d_out, n,
+                                           static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? ELAS_OK : ELAS_ERR_CUDA;
+}
+
+int elas_b200_pn_conv_forward(const float* x, const float* w, const float* b, float* y, int32_t nimg, int32_t hd,
+                              int32_t wd, int32_t relu, void* stream) {
+    if (!x || !w || !y || nimg <= 0 || hd <= 0 || wd <= 0) return ELAS_ERR_INVALID_ARG;
+    cudaError_t e = pn::launch_conv_f32(x, nullptr, w, b, y, nimg, hd, wd, relu, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? ELAS_OK : ELAS_ERR_CUDA;
+}
+
+int elas_b200_pn_conv_backward(const float* x, const float* y, const float* w, const float* dy, float* dx,
+                               float* dw, float* db, float* w_scratch, int32_t nimg, int32_t hd, int32_t wd,
+                               int32_t relu, void* stream) {
+    if (!x || !y || !w || !dy || !dw || !db || !w_scratch || nimg <= 0 || hd <= 0 || wd <= 0)
+        return ELAS_ERR_INVALID_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const float* mask = relu ? y : nullptr;
+    cudaError_t e = pn::launch_conv_wgrad(x, dy, mask, dw, db, nimg, hd, wd, st);
+    if (e == cudaSuccess && dx) {
+        e = pn::launch_flip_weights(w, w_scratch, st);
+        if (e == cudaSuccess) e = pn::launch_conv_f32(dy, mask, w_scratch, nullptr, dx, nimg, hd, wd, 0, st);
+    }
+    return e == cudaSuccess ? ELAS_OK : ELAS_ERR_CUDA;
+}
+
+int elas_b200_pn_corr_loss(const float* f, const int32_t* labels, int32_t nlab, int32_t hd, int32_t wd,
+                           int32_t disp_max, float* df, float* loss_sum, int32_t* correct, void* stream) {
+    if (!f || !df || !loss_sum || !correct || nlab < 0 || (nlab > 0 && !labels) || hd <= 0 || wd <= 0 ||
+        disp_max < 1)
+        return ELAS_ERR_INVALID_ARG;
+    cudaError_t e = pn::launch_corr_loss(f, labels, nlab, hd, wd, disp_max, df, loss_sum, correct,
+                                         static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? ELAS_OK : ELAS_ERR_CUDA;
+}
+
+int elas_b200_pn_adam(float* p, const float* g, float* m, float* v, int32_t n, float lr, float beta1, float beta2,
+                      float eps, int32_t step, void* stream) {
+    if (!p || !g || !m || !v || n <= 0 || step < 1) return ELAS_ERR_INVALID_ARG;
+    cudaError_t e = pn::launch_adam(p, g, m, v, n, lr, beta1, beta2, eps, step, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? ELAS_OK : ELAS_ERR_CUDA;
 }
 
 }  // extern "C"

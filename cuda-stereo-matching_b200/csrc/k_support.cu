@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 #include "common.cuh"
 #include "kernels.h"
+#include "proposal.h"
 
 namespace elas {
 
@@ -93,15 +94,68 @@ __device__ __forceinline__ int sweep_candidate(const uint4* self_m2, const uint4
     return -1;
 }
 
+// Learned-proposal sweep of one candidate by a full warp: only the
+// disparities of the packed bin set `bins` (up to four bins of width w, each
+// widened by pn::MARGIN pixels on both sides, clipped to [dmin, dmax]) are
+// matched.  Accepted iff the minimum energy is attained once and
+// (float)E1 < thr * (float)E2, E2 the smallest energy of the other
+// disparities of the set; returns the disparity or -1.
+__device__ __forceinline__ int sweep_restricted(const uint4* self_m2, const uint4* self_p2, const uint4* oth_m2,
+                                                const uint4* oth_p2, int u, int dmin, int dmax, int dir, float thr,
+                                                uint32_t bins, int w) {
+    const int lane = threadIdx.x & 31;
+    const int L = w + 2 * pn::MARGIN;
+    int lo[pn::TOPK];
+#pragma unroll
+    for (int r = 0; r < pn::TOPK; ++r) {
+        const uint32_t b = (bins >> (8 * r)) & 0xffu;
+        lo[r] = b == pn::NO_BIN ? INT32_MIN / 2 : int(b) * w - pn::MARGIN;
+    }
+    const uint4 c0 = self_m2[u - 2], c1 = self_m2[u + 2], c2 = self_p2[u - 2], c3 = self_p2[u + 2];
+    int e1 = INF_E, d1 = 0x7fffffff, c = 0, e2 = INF_E;
+    for (int e = lane; e < pn::TOPK * L; e += 32) {
+        const int r = e / L;
+        const int lor = r == 0 ? lo[0] : r == 1 ? lo[1] : r == 2 ? lo[2] : lo[3];
+        if (lor == INT32_MIN / 2) continue;
+        const int d = lor + (e - r * L);
+        if (d < dmin || d > dmax) continue;
+        bool dup = false;
+#pragma unroll
+        for (int q = 0; q < pn::TOPK - 1; ++q)
+            if (q < r && d >= lo[q] && d < lo[q] + L) dup = true;
+        if (dup) continue;
+        const int uw = u + dir * d;
+        int en = sad16(c0, oth_m2[uw - 2]);
+        en = sad16(c1, oth_m2[uw + 2], en);
+        en = sad16(c2, oth_p2[uw - 2], en);
+        en = sad16(c3, oth_p2[uw + 2], en);
+        if (en < e1) { e2 = e1; e1 = en; d1 = d; c = 1; }
+        else if (en == e1) { e2 = en; c = 2; d1 = min(d1, d); }
+        else if (en < e2) { e2 = en; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const int oe1 = __shfl_xor_sync(0xffffffffu, e1, o), od1 = __shfl_xor_sync(0xffffffffu, d1, o);
+        const int oc = __shfl_xor_sync(0xffffffffu, c, o), oe2 = __shfl_xor_sync(0xffffffffu, e2, o);
+        if (oe1 < e1) { e2 = min(e1, oe2); e1 = oe1; d1 = od1; c = oc; }
+        else if (oe1 == e1) { if (e1 != INF_E) { c = min(c + oc, 2); e2 = e1; d1 = min(d1, od1); } }
+        else { e2 = min(e2, oe1); }
+    }
+    if (c != 1) return -1;
+    return float(e1) < thr * float(e2) ? d1 : -1;
+}
+
 // Block: SWEEP_THREADS threads (one candidate per warp at a time).  grid.x =
 // segments per candidate row, grid.y = candidate rows.  SMEM: stage the four
 // rows when they fit.
 constexpr int SWEEP_THREADS = 1024;
-template <bool SMEM>
+constexpr int PROP_FINAL = 1 << 20;     // res[] flag: accepted by the learned proposal, no R->L pass
+template <bool SMEM, bool PROP>
 __global__ void __launch_bounds__(SWEEP_THREADS) k_support_sweep(const uint4* __restrict__ desc0,
                                                        const uint4* __restrict__ desc1,
                                                        int32_t* __restrict__ can_out, Geom g, DevParams p,
-                                                       int seg, unsigned* err) {
+                                                       int seg, unsigned* err, const uint32_t* __restrict__ bins,
+                                                       int32_t* __restrict__ stats) {
     extern __shared__ __align__(128) uint4 rows[];
     __shared__ int res[256];
     __shared__ uint64_t bar;
@@ -142,8 +196,34 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_support_sweep(const uint4* __
             uint4 ctr = desc0[size_t(v) * W + u];
             if (texture16(ctr) >= p.support_texture) {
                 int dmax = min(g.D, u - 5);
-                if (dmax - g.dmin >= 10)
-                    r = sweep_candidate(L_m2, L_p2, R_m2, R_p2, u, g.dmin, dmax, -1, p.support_threshold);
+                if (dmax - g.dmin >= 10) {
+                    bool done = false;
+                    if (PROP) {
+                        // learned search set first: accepted only if the same
+                        // uniqueness and left/right tests pass on it
+                        const uint32_t bset = bins[size_t(vc) * g.cw + ci];
+                        const int w = pn::bin_width(g.D);
+                        const int rl = bset == 0xffffffffu ? -1
+                                           : sweep_restricted(L_m2, L_p2, R_m2, R_p2, u, g.dmin, dmax, -1,
+                                                              p.support_threshold, bset, w);
+                        if (rl >= 0) {
+                            const int ur = u - rl;
+                            const uint4 cr = desc1[size_t(v) * W + ur];
+                            const int dmaxr = min(g.D, W - ur - 5);
+                            if (texture16(cr) >= p.support_texture && dmaxr - g.dmin >= 10) {
+                                const int rr = sweep_restricted(R_m2, R_p2, L_m2, L_p2, ur, g.dmin, dmaxr, +1,
+                                                                p.support_threshold, bset, w);
+                                if (rr >= 0 && abs(rl - rr) <= p.lr_threshold) {
+                                    r = rl | PROP_FINAL;
+                                    done = true;
+                                }
+                            }
+                        }
+                        if (lane == 0) atomicAdd(&stats[done ? 0 : 1], 1);
+                    }
+                    if (!done)   // the full sweep
+                        r = sweep_candidate(L_m2, L_p2, R_m2, R_p2, u, g.dmin, dmax, -1, p.support_threshold);
+                }
             }
         }
         if (lane == 0) res[ci - c_begin] = r;
@@ -153,6 +233,10 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_support_sweep(const uint4* __
     for (int ci = c_begin + warp; ci < c_end; ci += nw) {
         int dl = res[ci - c_begin];
         if (dl < 0) continue;
+        if (PROP && (dl & PROP_FINAL)) {
+            if (lane == 0) res[ci - c_begin] = dl & ~PROP_FINAL;
+            continue;
+        }
         int u = ci * g.step - dl;
         int r = -1;
         uint4 ctr = desc1[size_t(v) * W + u];
@@ -356,7 +440,7 @@ __global__ void k_grid_diffuse(const uint32_t* __restrict__ t0, const uint32_t* 
 
 cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_lr, int32_t* can_tmp,
                            int32_t* can, const Geom& g, const DevParams& p, int num_sms, unsigned* err,
-                           cudaStream_t st) {
+                           cudaStream_t st, const uint32_t* bins, int32_t* stats) {
     // segments: about 4 CTAs per SM in flight
     int rows = g.ch;
     int segs = imax(1, (4 * num_sms + rows - 1) / imax(rows, 1));
@@ -365,10 +449,23 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
     size_t smem = size_t(4) * g.W * sizeof(uint4);
     dim3 grid(segs, rows);
     if (smem <= 200 * 1024) {
-        cudaFuncSetAttribute(k_support_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        k_support_sweep<true><<<grid, SWEEP_THREADS, smem, st>>>(desc0, desc1, can_lr, g, p, seg, err);
+        if (bins) {
+            cudaFuncSetAttribute(k_support_sweep<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            k_support_sweep<true, true><<<grid, SWEEP_THREADS, smem, st>>>(desc0, desc1, can_lr, g, p, seg, err, bins,
+                                                                           stats);
+        } else {
+            cudaFuncSetAttribute(k_support_sweep<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(smem));
+            k_support_sweep<true, false><<<grid, SWEEP_THREADS, smem, st>>>(desc0, desc1, can_lr, g, p, seg, err,
+                                                                            nullptr, nullptr);
+        }
     } else {
-        k_support_sweep<false><<<grid, SWEEP_THREADS, 0, st>>>(desc0, desc1, can_lr, g, p, seg, err);
+        if (bins)
+            k_support_sweep<false, true><<<grid, SWEEP_THREADS, 0, st>>>(desc0, desc1, can_lr, g, p, seg, err, bins,
+                                                                         stats);
+        else
+            k_support_sweep<false, false><<<grid, SWEEP_THREADS, 0, st>>>(desc0, desc1, can_lr, g, p, seg, err,
+                                                                          nullptr, nullptr);
     }
     k_incon<<<dim3((g.cw + 127) / 128, g.ch), 128, 0, st>>>(can_lr, can, g, p);
     {

@@ -41,9 +41,12 @@ struct DelDev {
 cudaError_t launch_descriptor(const uint8_t* img0, const uint8_t* img1, uint4* desc0, uint4* desc1,
                               int W, int H, cudaStream_t st);
 
+// bins (nullable): packed learned search sets per candidate; then stats[0]
+// counts candidates the proposal settled and stats[1] those that fell back
+// to the full sweep.
 cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_lr, int32_t* can_tmp,
                            int32_t* can, const Geom& g, const DevParams& p, int num_sms, unsigned* err,
-                           cudaStream_t st);
+                           cudaStream_t st, const uint32_t* bins = nullptr, int32_t* stats = nullptr);
 
 cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_off, int32_t* uvd, int32_t* x0,
                            int32_t* x1, int32_t* y, const Geom& g, cudaStream_t st);

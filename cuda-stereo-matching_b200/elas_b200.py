@@ -23,8 +23,25 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported", 3: "CUDA error", 4: 
 STAGES = {
     "desc_left": 0, "desc_right": 1, "can_lr": 2, "can": 3, "support": 4, "grid_left": 5, "grid_right": 6,
     "tri_left": 7, "tri_right": 8, "prior_left": 9, "prior_right": 10, "disp_left": 11, "disp_right": 12,
-    "lr_left": 13, "lr_right": 14,
+    "lr_left": 13, "lr_right": 14, "pn_features": 15, "pn_output": 16, "pn_bins": 17,
 }
+
+PN_PARAMS = 36992
+PN_WEIGHTS = os.path.join(HERE, "weights", "proposal.f32")
+
+
+def bf16_to_f32(raw):
+    """bf16 values (raw uint16 / bytes) -> float32."""
+    u = np.frombuffer(np.ascontiguousarray(raw).tobytes(), np.uint16).astype(np.uint32) << 16
+    return u.view(np.float32)
+
+
+def load_proposal(path=PN_WEIGHTS):
+    """Trained proposal parameters (ELAS_PN_PARAMS little-endian float32)."""
+    w = np.fromfile(path, np.float32)
+    if w.size != PN_PARAMS:
+        raise ElasError(1, f"{path}: {w.size} values, expected {PN_PARAMS}")
+    return w
 
 
 class ElasParams(ctypes.Structure):
@@ -86,6 +103,18 @@ def library():
         lib.elas_b200_set_graphs.argtypes = [c_void_p, c_int]
         lib.elas_b200_batch_latency.argtypes = [c_void_p, c_void_p, c_int]
         lib.elas_b200_dense_shape.argtypes = [c_void_p, c_int32, c_int32]
+        lib.elas_b200_set_proposal.argtypes = [c_void_p, c_void_p, c_int32]
+        lib.elas_b200_proposal_stats.argtypes = [c_void_p, c_void_p, c_int32]
+        lib.elas_b200_pn_infer.argtypes = [c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p]
+        lib.elas_b200_pn_features.argtypes = [c_void_p, c_void_p, c_void_p]
+        lib.elas_b200_pn_bf16_to_f32.argtypes = [c_void_p, c_void_p, c_size_t, c_void_p]
+        lib.elas_b200_pn_conv_forward.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32,
+                                                  c_int32, c_void_p]
+        lib.elas_b200_pn_conv_backward.argtypes = [c_void_p] * 8 + [c_int32] * 4 + [c_void_p]
+        lib.elas_b200_pn_corr_loss.argtypes = [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p,
+                                               c_void_p, c_void_p, c_void_p]
+        lib.elas_b200_pn_adam.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_float, c_float, c_float,
+                                          c_float, c_int32, c_void_p]
         lib.elas_b200_get_stage.argtypes = [c_void_p, c_int, c_void_p, c_size_t, POINTER(c_size_t)]
         lib.elas_b200_set_timing.argtypes = [c_void_p, c_int]
         lib.elas_b200_get_timing.argtypes = [c_void_p, c_void_p, c_int]
@@ -262,6 +291,28 @@ class Elas:
         self._check(self._lib.elas_b200_get_stage(self._h, sid, _ptr(buf), need.value, ctypes.byref(need)))
         return buf
 
+    def set_proposal(self, params):
+        """Enable the learned support-point proposal with these parameters
+        (ELAS_PN_PARAMS float32), or disable it with None."""
+        if params is None:
+            self._check(self._lib.elas_b200_set_proposal(self._h, None, 0))
+            return
+        w = np.ascontiguousarray(params, np.float32)
+        self._check(self._lib.elas_b200_set_proposal(self._h, _ptr(w), w.size))
+
+    def proposal_stats(self):
+        """(settled by the proposal, sent to the full sweep) for the last call."""
+        out = np.zeros(2, np.int32)
+        self._check(self._lib.elas_b200_proposal_stats(self._h, _ptr(out), 2))
+        return int(out[0]), int(out[1])
+
+    def pn_infer(self, in_ptr, out_ptr, hd, wd, stream=None):
+        self._check(self._lib.elas_b200_pn_infer(self._h, c_void_p(in_ptr), c_void_p(out_ptr), hd, wd,
+                                                 c_void_p(stream) if stream else None))
+
+    def pn_features(self, out_ptr, stream=None):
+        self._check(self._lib.elas_b200_pn_features(self._h, c_void_p(out_ptr), c_void_p(stream) if stream else None))
+
     TIME_STAGES = ["descriptor", "support", "compact", "grid", "delaunay", "prior", "dense", "lr", "post"]
 
     def set_timing(self, enable=True):
@@ -276,3 +327,37 @@ class Elas:
     @property
     def launch_count(self):
         return int(self._lib.elas_b200_launch_count(self._h))
+
+
+# ---- training kernels of the proposal network (device pointers as ints) ----
+
+def _pn_check(rc):
+    if rc != ELAS_OK:
+        raise ElasError(rc)
+
+
+def pn_bf16_to_f32(src, dst, n, stream=None):
+    _pn_check(library().elas_b200_pn_bf16_to_f32(c_void_p(src), c_void_p(dst), n, c_void_p(stream) if stream else None))
+
+
+def pn_conv_forward(x, w, b, y, nimg, hd, wd, relu, stream=None):
+    _pn_check(library().elas_b200_pn_conv_forward(c_void_p(x), c_void_p(w), c_void_p(b) if b else None, c_void_p(y),
+                                                  nimg, hd, wd, int(relu), c_void_p(stream) if stream else None))
+
+
+def pn_conv_backward(x, y, w, dy, dx, dw, db, w_scratch, nimg, hd, wd, relu, stream=None):
+    _pn_check(library().elas_b200_pn_conv_backward(c_void_p(x), c_void_p(y), c_void_p(w), c_void_p(dy),
+                                                   c_void_p(dx) if dx else None, c_void_p(dw), c_void_p(db),
+                                                   c_void_p(w_scratch), nimg, hd, wd, int(relu),
+                                                   c_void_p(stream) if stream else None))
+
+
+def pn_corr_loss(f, labels, nlab, hd, wd, disp_max, df, loss_sum, correct, stream=None):
+    _pn_check(library().elas_b200_pn_corr_loss(c_void_p(f), c_void_p(labels), nlab, hd, wd, disp_max, c_void_p(df),
+                                               c_void_p(loss_sum), c_void_p(correct),
+                                               c_void_p(stream) if stream else None))
+
+
+def pn_adam(p, g, m, v, n, lr, beta1, beta2, eps, step, stream=None):
+    _pn_check(library().elas_b200_pn_adam(c_void_p(p), c_void_p(g), c_void_p(m), c_void_p(v), n, lr, beta1, beta2,
+                                          eps, step, c_void_p(stream) if stream else None))

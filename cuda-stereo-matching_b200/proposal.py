@@ -1,0 +1,201 @@
+"""Training and evaluation of the learned support-point proposal.
+
+The network (4 layers of 3x3 convolutions, 32 channels) and its loss are
+computed by the library's own CUDA kernels (elas_b200_pn_*); PyTorch only
+holds device memory.  Training data are support points that plain ELAS
+accepts on seeded synthetic pairs: for every pair the library runs the
+plain pipeline, the pooled descriptor features of that run are kept on the
+device, and every support point (u, v, d) becomes a target: the cell
+(u // 4, v // 4) of the left view should score bin d // w highest.
+
+Usage (writes the trained parameters, ELAS_PN_PARAMS float32):
+    python proposal.py --pairs 2000 --epochs 8 --out weights/proposal.f32
+"""
+import argparse
+import concurrent.futures as cf
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+import elas_b200 as eb  # noqa: E402
+
+CH, TAPS, LAYERS, NBINS = 32, 9, 4, 64
+LAYER_PARAMS = TAPS * CH * CH + CH
+NPARAMS = LAYERS * LAYER_PARAMS
+
+# seeds of the synthetic pairs: training and the two held-out evaluation sets
+TRAIN_SEED0 = 200000
+EVAL_SEED0_1242 = 300000
+EVAL_SEED0_2880 = 400000
+
+
+def init_params(seed=0):
+    """He-style initialisation, per layer W[tap][ci][co] then b[co]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(LAYERS):
+        out.append(rng.normal(0.0, np.sqrt(2.0 / (TAPS * CH)), TAPS * CH * CH))
+        out.append(np.zeros(CH))
+    return np.concatenate(out).astype(np.float32)
+
+
+def bin_width(D):
+    return (D + 1 + NBINS - 1) // NBINS
+
+
+def labels_of(uvd, D, hd, wd, pair):
+    """Support points -> (pair, cx, cy, bin) rows inside the cell grid."""
+    w = bin_width(D)
+    cx, cy = uvd[:, 0] // 4, uvd[:, 1] // 4
+    keep = (cx < wd) & (cy < hd)
+    n = int(keep.sum())
+    out = np.empty((n, 4), np.int32)
+    out[:, 0] = pair
+    out[:, 1] = cx[keep]
+    out[:, 2] = cy[keep]
+    out[:, 3] = np.minimum(uvd[keep, 2] // w, NBINS - 1)
+    return out
+
+
+class Net:
+    """Forward / backward of the proposal network over a batch of pairs,
+    with buffers sized for `max_pairs` pairs of hd x wd cells."""
+
+    def __init__(self, torch, hd, wd, max_pairs):
+        self.torch, self.hd, self.wd = torch, hd, wd
+        shape = (2 * max_pairs, hd, wd, CH)
+        f32 = dict(dtype=torch.float32, device="cuda")
+        self.x = torch.empty(shape, **f32)
+        self.acts = [torch.empty(shape, **f32) for _ in range(LAYERS)]
+        self.g = [torch.empty(shape, **f32) for _ in range(2)]
+        self.scratch = torch.empty(TAPS * CH * CH, **f32)
+        self.loss = torch.zeros(1, **f32)
+        self.correct = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def forward_backward(self, theta, grad, x, labels, npairs, D):
+        """x: fp32 [2*npairs][hd][wd][32] (device); labels: int32 [n][4]
+        (device).  Accumulates dL/dtheta into grad; returns (loss sum, hits)."""
+        nimg, hd, wd = 2 * npairs, self.hd, self.wd
+        p0, g0 = theta.data_ptr(), grad.data_ptr()
+        W = [p0 + 4 * l * LAYER_PARAMS for l in range(LAYERS)]
+        B = [w + 4 * TAPS * CH * CH for w in W]
+        dW = [g0 + 4 * l * LAYER_PARAMS for l in range(LAYERS)]
+        dB = [w + 4 * TAPS * CH * CH for w in dW]
+        ins = [x.data_ptr()] + [a.data_ptr() for a in self.acts[:-1]]
+        for l in range(LAYERS):
+            eb.pn_conv_forward(ins[l], W[l], B[l], self.acts[l].data_ptr(), nimg, hd, wd, l < LAYERS - 1)
+        self.loss.zero_()
+        self.correct.zero_()
+        gcur, gnext = self.g
+        gcur[:nimg].zero_()
+        eb.pn_corr_loss(self.acts[-1].data_ptr(), labels.data_ptr(), int(labels.shape[0]), hd, wd, D,
+                        gcur.data_ptr(), self.loss.data_ptr(), self.correct.data_ptr())
+        for l in range(LAYERS - 1, -1, -1):
+            dx = gnext.data_ptr() if l > 0 else 0
+            eb.pn_conv_backward(ins[l], self.acts[l].data_ptr(), W[l], gcur.data_ptr(), dx, dW[l], dB[l],
+                                self.scratch.data_ptr(), nimg, hd, wd, l < LAYERS - 1)
+            gcur, gnext = gnext, gcur
+        return float(self.loss.item()), int(self.correct.item())
+
+
+def collect(torch, n, seed0, preset=1, log=None):
+    """Plain ELAS on n seeded pairs: bf16 features [2n][hd][wd][32] on the
+    device and the label rows of every pair."""
+    W, H, D = eb.synth_dims(preset)
+    hd, wd = H // 4, W // 4
+    feats = torch.empty((2 * n, hd, wd, CH), dtype=torch.bfloat16, device="cuda")
+    e = eb.Elas(eb.params_config(D))
+    dl = torch.empty((H, W), dtype=torch.uint8, device="cuda")
+    dr = torch.empty_like(dl)
+    o1 = torch.empty((H, W), dtype=torch.float32, device="cuda")
+    o2 = torch.empty_like(o1)
+    labels = []
+    t0 = time.time()
+    with cf.ThreadPoolExecutor(8) as ex:
+        futs = [ex.submit(eb.synth_pair, preset, seed0 + i, gt=False) for i in range(min(n, 16))]
+        for i in range(n):
+            L, R, _, _ = futs[i].result()
+            if i + 16 < n:
+                futs.append(ex.submit(eb.synth_pair, preset, seed0 + i + 16, gt=False))
+            futs[i] = None
+            dl.copy_(torch.from_numpy(L))
+            dr.copy_(torch.from_numpy(R))
+            e.process_device(dl.data_ptr(), dr.data_ptr(), o1.data_ptr(), o2.data_ptr(), W, H)
+            e.pn_features(feats[2 * i].data_ptr())
+            uvd = e.stage("support").view(np.int32).reshape(-1, 3)
+            labels.append(labels_of(uvd, D, hd, wd, i))
+            if log and (i + 1) % 250 == 0:
+                log(f"collected {i + 1}/{n} pairs, {time.time() - t0:.1f} s")
+    torch.cuda.synchronize()
+    e.close()
+    return feats, labels, (hd, wd, D)
+
+
+def train(torch, feats, labels, geom, epochs=8, batch=16, lr=2e-3, seed=0, log=print):
+    hd, wd, D = geom
+    n = len(labels)
+    theta = torch.from_numpy(init_params(seed)).cuda()
+    grad = torch.zeros_like(theta)
+    m = torch.zeros_like(theta)
+    v = torch.zeros_like(theta)
+    net = Net(torch, hd, wd, batch)
+    rng = np.random.default_rng(seed)
+    steps_per_epoch = (n + batch - 1) // batch
+    total = epochs * steps_per_epoch
+    step = 0
+    history = []
+    for ep in range(epochs):
+        order = rng.permutation(n)
+        tl, tc, tn, t0 = 0.0, 0, 0, time.time()
+        for k in range(0, n, batch):
+            idx = order[k:k + batch]
+            nb = len(idx)
+            for j, i in enumerate(idx):
+                net.x[2 * j:2 * j + 2].copy_(feats[2 * i:2 * i + 2])     # bf16 -> fp32
+            lab = np.concatenate([labels[i] for i in idx])
+            lab[:, 0] = np.repeat(np.arange(nb), [len(labels[i]) for i in idx])
+            lab_d = torch.from_numpy(lab).cuda()
+            grad.zero_()
+            loss, hits = net.forward_backward(theta, grad, net.x, lab_d, nb, D)
+            step += 1
+            lr_t = lr * 0.5 * (1.0 + np.cos(np.pi * (step - 1) / total))
+            eb.pn_adam(theta.data_ptr(), grad.data_ptr(), m.data_ptr(), v.data_ptr(), NPARAMS, lr_t, 0.9, 0.999,
+                       1e-8, step)
+            tl += loss
+            tc += hits
+            tn += len(lab)
+        torch.cuda.synchronize()
+        rec = {"epoch": ep + 1, "loss": tl / max(tn, 1), "top1": tc / max(tn, 1), "s": time.time() - t0}
+        history.append(rec)
+        log(f"epoch {ep + 1}: loss {rec['loss']:.4f} top-1 {rec['top1']:.3f} ({rec['s']:.1f} s)")
+    return theta.cpu().numpy(), history
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--pairs", type=int, default=2000)
+    ap.add_argument("--epochs", type=int, default=8)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--out", default=eb.PN_WEIGHTS)
+    args = ap.parse_args()
+    import torch
+
+    torch.cuda.set_device(0)
+    t0 = time.time()
+    feats, labels, geom = collect(torch, args.pairs, TRAIN_SEED0, log=print)
+    print(f"data: {args.pairs} pairs, {sum(len(x) for x in labels)} support points, {time.time() - t0:.1f} s",
+          flush=True)
+    theta, hist = train(torch, feats, labels, geom, args.epochs, args.batch, args.lr)
+    os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
+    theta.astype(np.float32).tofile(args.out)
+    print(f"wrote {args.out}; total {time.time() - t0:.1f} s")
+
+
+if __name__ == "__main__":
+    main()

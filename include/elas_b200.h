@@ -164,6 +164,49 @@ int elas_b200_batch_latency(elas_handle* h, float* ms_out, int n);
  * and disparity range (0 = not tuned yet). */
 int elas_b200_dense_shape(const elas_handle* h, int32_t width, int32_t disp_max);
 
+/* ---- learned support-point proposal (no counterpart in the reference) ----
+ *
+ * A 4-layer 3x3 CNN (32 channels, bf16 with fp32 accumulation, tcgen05
+ * implicit-GEMM kernels) over the descriptors pooled to 4x4-pixel cells
+ * scores 64 disparity bins per support candidate; the candidate is first
+ * matched only on its 4 best bins (each widened by 2 pixels) and must pass
+ * the same uniqueness and left/right tests there, else it falls back to the
+ * full sweep of the reference (src/Kernels/KerSupportMatches.cu:12-193).
+ * Parameters: ELAS_PN_PARAMS floats, per layer W[tap][ci][co] then b[co]. */
+#define ELAS_PN_PARAMS 36992
+
+/* Enable the proposal with these parameters (n == ELAS_PN_PARAMS) or
+ * disable it (n == 0). */
+int elas_b200_set_proposal(elas_handle* h, const float* params, int32_t n);
+
+/* Candidates of the last call settled by the proposal (out[0]) and sent to
+ * the full sweep (out[1]); zeros when the proposal did not run. */
+int elas_b200_proposal_stats(elas_handle* h, int32_t* out, int32_t n);
+
+/* The network alone on caller features (bf16 [2][hd][wd][32] in and out,
+ * device memory), with the handle's weights; blocks until done. */
+int elas_b200_pn_infer(elas_handle* h, const void* d_in, void* d_out, int32_t hd, int32_t wd, void* stream);
+
+/* Training kernels (fp32, device pointers, asynchronous on `stream`).
+ * Feature maps are [nimg][hd][wd][32]; a pair's left image is 2*pair and
+ * its right image 2*pair+1. */
+int elas_b200_pn_features(elas_handle* h, void* d_out, void* stream);  /* bf16 input features of the last call */
+int elas_b200_pn_bf16_to_f32(const void* d_in, float* d_out, size_t n, void* stream);
+int elas_b200_pn_conv_forward(const float* x, const float* w, const float* b, float* y, int32_t nimg, int32_t hd,
+                              int32_t wd, int32_t relu, void* stream);
+/* dw, db accumulate (+=); dx (nullable) is overwritten; w_scratch holds
+ * 9*32*32 floats. */
+int elas_b200_pn_conv_backward(const float* x, const float* y, const float* w, const float* dy, float* dx,
+                               float* dw, float* db, float* w_scratch, int32_t nimg, int32_t hd, int32_t wd,
+                               int32_t relu, void* stream);
+/* Mean softmax cross-entropy over labels (nlab x {pair, cx, cy, bin}):
+ * adds the summed loss to *loss_sum, the count of top-1 hits to *correct
+ * and the gradient to df (accumulated). */
+int elas_b200_pn_corr_loss(const float* f, const int32_t* labels, int32_t nlab, int32_t hd, int32_t wd,
+                           int32_t disp_max, float* df, float* loss_sum, int32_t* correct, void* stream);
+int elas_b200_pn_adam(float* p, const float* g, float* m, float* v, int32_t n, float lr, float beta1, float beta2,
+                      float eps, int32_t step, void* stream);
+
 /* ---- introspection of the last call (for stage-wise parity checks) ---- */
 
 /* Stages that can be copied out after a process call. */
@@ -184,7 +227,11 @@ int elas_b200_dense_shape(const elas_handle* h, int32_t width, int32_t disp_max)
 #define ELAS_STAGE_DISP_RIGHT   12   /* float  [h][w] */
 #define ELAS_STAGE_LR_LEFT      13   /* float  [h][w] after the L/R check, before post-filters */
 #define ELAS_STAGE_LR_RIGHT     14   /* float  [h][w] */
-#define ELAS_STAGE_COUNT        15
+#define ELAS_STAGE_PN_FEATURES  15   /* bf16   [2][h/4][w/4][32] proposal input (left, right) */
+#define ELAS_STAGE_PN_OUTPUT    16   /* bf16   [2][h/4][w/4][32] proposal network output */
+#define ELAS_STAGE_PN_BINS      17   /* uint32 [ch][cw] top-4 bins per candidate, one byte each
+                                      * (best first, 0xff = none) */
+#define ELAS_STAGE_COUNT        18
 
 /* Copy stage `stage` of the last single-pair call into host memory `dst`
  * of `bytes` bytes.  *needed receives the size in bytes (call with
