@@ -296,6 +296,8 @@ def run_ours(args):
         out["large"] = run_large(torch, args, flush, stream, hbm, peak_kind)
     if rank == 0 and world == 1 and not args.no_batch:
         out["batch"] = run_batch(torch, args, flush, stream)
+    if rank == 0 and world == 1 and not args.no_learned:
+        out["learned"] = run_learned(torch)
     e.close()
     del flush
     if rank == 0:
@@ -324,6 +326,19 @@ def run_large(torch, args, flush, stream, hbm, peak_kind):
                                "unit": "GB/s", "frac": dense_bytes / (stage_ms["dense"] / 1e3) / 1e9 / hbm,
                                "peak_kind": peak_kind, "traffic": profile_traffic("k_dense_2880x1988")},
             "gpu_launches": launches, "quality": quality(D1, gt)}
+
+
+def run_learned(torch, n1=10, n2=3):
+    """Plain ELAS against the learned support-point proposal on held-out
+    seeds (the first n1 of the 1242x375 set, the first n2 of the 2880x1988
+    set), with the trained weights shipped in the package."""
+    if not os.path.exists(eb.PN_WEIGHTS):
+        return {"unavailable": "no trained proposal weights in the package"}
+    import proposal
+
+    theta = eb.load_proposal()
+    return [proposal.evaluate(torch, theta, 1, list(range(proposal.EVAL_SEED0_1242, proposal.EVAL_SEED0_1242 + n1))),
+            proposal.evaluate(torch, theta, 2, list(range(proposal.EVAL_SEED0_2880, proposal.EVAL_SEED0_2880 + n2)))]
 
 
 def batch_workload(n=64, seed=7):
@@ -444,6 +459,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--only", choices=["large", "batch"], default=None,
                     help="run one secondary workload alone (for profiling) and print its block")
     args = ap.parse_args()

@@ -176,6 +176,79 @@ def train(torch, feats, labels, geom, epochs=8, batch=16, lr=2e-3, seed=0, log=p
     return theta.cpu().numpy(), history
 
 
+def bad2px(D, gt):
+    """Fraction of ground-truth-valid pixels with |D - gt| > 2; invalid
+    pixels (D < 0) count as bad."""
+    valid = np.isfinite(gt) & (gt > 0)
+    bad = (np.abs(D - gt) > 2) | (D < 0)
+    return float(bad[valid].mean())
+
+
+def evaluate(torch, theta, preset, seeds, log=None, flush_bytes=256 << 20):
+    """Plain ELAS against the learned proposal on held-out seeded pairs.
+
+    Both paths run on the same device-resident inputs; each call is timed
+    alone with CUDA events after an L2 flush.  Returns the fallback rate
+    (candidates the proposal sent back to the full sweep), bad-2px of both
+    paths against the ground truth, the fraction of pixels where the two
+    maps differ by more than 2 px (or in validity), and pairs/s of both."""
+    W, H, D = eb.synth_dims(preset)
+    p = eb.params_config(D)
+    plain, learned = eb.Elas(p), eb.Elas(p)
+    learned.set_proposal(theta)
+    dl = torch.empty((H, W), dtype=torch.uint8, device="cuda")
+    dr = torch.empty_like(dl)
+    outs = {k: (torch.empty((H, W), dtype=torch.float32, device="cuda"),
+                torch.empty((H, W), dtype=torch.float32, device="cuda")) for k in ("plain", "learned")}
+    flush = torch.empty(flush_bytes // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    engines = {"plain": plain, "learned": learned}
+    ms = {"plain": [], "learned": []}
+    bad = {"plain": [], "learned": []}
+    disagree, settled, fell = [], 0, 0
+    with cf.ThreadPoolExecutor(4) as ex:
+        futs = [ex.submit(eb.synth_pair, preset, s) for s in seeds]
+        for i, f in enumerate(futs):
+            L, R, gt, _ = f.result()
+            futs[i] = None
+            dl.copy_(torch.from_numpy(L))
+            dr.copy_(torch.from_numpy(R))
+            maps = {}
+            for name, e in engines.items():
+                o1, o2 = outs[name]
+                args = (dl.data_ptr(), dr.data_ptr(), o1.data_ptr(), o2.data_ptr(), W, H)
+                if i == 0:                       # grows the workspaces outside the timing
+                    e.process_device(*args, stream=stream.cuda_stream)
+                flush.zero_()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                e.process_device(*args, stream=stream.cuda_stream)
+                b.record(stream)
+                b.synchronize()
+                ms[name].append(a.elapsed_time(b))
+                maps[name] = o1.cpu().numpy()
+                bad[name].append(bad2px(maps[name], gt))
+            st, fl = learned.proposal_stats()
+            settled += st
+            fell += fl
+            dp, dq = maps["plain"], maps["learned"]
+            disagree.append(float(((np.abs(dp - dq) > 2) | ((dp < 0) != (dq < 0))).mean()))
+            if log and (i + 1) % 50 == 0:
+                log(f"evaluated {i + 1}/{len(seeds)} pairs")
+    plain.close()
+    learned.close()
+    out = {"workload": f"{W}x{H}_disp0-{D}", "pairs": len(seeds), "seeds": f"{seeds[0]}..{seeds[-1]}",
+           "fallback_rate": fell / max(settled + fell, 1), "candidates_settled": settled, "candidates_fell_back": fell,
+           "bad2px_plain": float(np.mean(bad["plain"])), "bad2px_learned": float(np.mean(bad["learned"])),
+           "disagree_2px": float(np.mean(disagree))}
+    for name in ("plain", "learned"):
+        out[f"pairs_per_s_{name}"] = len(seeds) / (sum(ms[name]) / 1e3)
+        out[f"ms_per_pair_{name}"] = float(np.mean(ms[name]))
+    out["speedup"] = out["pairs_per_s_learned"] / out["pairs_per_s_plain"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--pairs", type=int, default=2000)
@@ -183,10 +256,27 @@ def main():
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--out", default=eb.PN_WEIGHTS)
+    ap.add_argument("--eval", action="store_true",
+                    help="evaluate the weights in --out on the held-out seeds instead of training")
+    ap.add_argument("--eval-pairs", default="200,20",
+                    help="held-out pairs at 1242x375 and at 2880x1988")
     args = ap.parse_args()
     import torch
 
     torch.cuda.set_device(0)
+    if args.eval:
+        import json
+
+        theta = eb.load_proposal(args.out)
+        n1, n2 = (int(x) for x in args.eval_pairs.split(","))
+        res = []
+        if n1:
+            res.append(evaluate(torch, theta, 1, list(range(EVAL_SEED0_1242, EVAL_SEED0_1242 + n1)), log=print))
+        if n2:
+            res.append(evaluate(torch, theta, 2, list(range(EVAL_SEED0_2880, EVAL_SEED0_2880 + n2)), log=print))
+        for r in res:
+            print(json.dumps(r), flush=True)
+        return
     t0 = time.time()
     feats, labels, geom = collect(torch, args.pairs, TRAIN_SEED0, log=print)
     print(f"data: {args.pairs} pairs, {sum(len(x) for x in labels)} support points, {time.time() - t0:.1f} s",
