@@ -37,6 +37,7 @@ struct DevParams {
     int match_texture;
     int plane_radius;       // (int)max(ceil(sigma*sradius), 2)   (KerComputeDisparity.cu:194)
     int penalty[16];        // P(|d - d_plane|) for |d - d_plane| <= plane_radius
+    int window_negative;    // every penalty[0..plane_radius] is < 0
     float speckle_sim_threshold;
     int speckle_size;
     int ipol_gap_width;

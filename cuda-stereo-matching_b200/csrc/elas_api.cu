@@ -149,6 +149,9 @@ DevParams dev_params(const elas_params& p) {
     d.match_texture = p.match_texture;
     d.plane_radius = int32_t(std::max(float(std::ceil(p.sigma * p.sradius)), 2.0f));
     for (int i = 0; i < 16; ++i) d.penalty[i] = i <= d.plane_radius ? penalty(i, p) : 0;
+    d.window_negative = 1;
+    for (int i = 0; i <= d.plane_radius; ++i)
+        if (d.penalty[i] >= 0) d.window_negative = 0;
     d.speckle_sim_threshold = p.speckle_sim_threshold;
     d.speckle_size = p.speckle_size;
     d.ipol_gap_width = p.ipol_gap_width;
@@ -917,6 +920,7 @@ int elas_b200_get_stage(elas_handle* h, int stage, void* dst, size_t bytes, size
         if (!h->pn_used) return fail(h, ELAS_ERR_INVALID_ARG, "the last call did not run the proposal");
         need = can_n * 4;
         break;
+    case ELAS_STAGE_DEL_COUNTERS: need = 2 * 16 * 4; break;
     default: need = px * 4; break;
     }
     if (needed) *needed = need;
@@ -964,6 +968,10 @@ int elas_b200_get_stage(elas_handle* h, int stage, void* dst, size_t bytes, size
     case ELAS_STAGE_PN_FEATURES: CK(cudaMemcpy(dst, h->pn_in, need, cudaMemcpyDeviceToHost)); break;
     case ELAS_STAGE_PN_OUTPUT: CK(cudaMemcpy(dst, h->pn_out, need, cudaMemcpyDeviceToHost)); break;
     case ELAS_STAGE_PN_BINS: CK(cudaMemcpy(dst, h->pn_bins, need, cudaMemcpyDeviceToHost)); break;
+    case ELAS_STAGE_DEL_COUNTERS:
+        CK(cudaMemcpy(dst, h->del[0].ctr, 16 * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(static_cast<char*>(dst) + 64, h->del[1].ctr, 16 * 4, cudaMemcpyDeviceToHost));
+        break;
     default: return fail(h, ELAS_ERR_INVALID_ARG, "bad stage");
     }
     return ELAS_OK;

@@ -171,9 +171,31 @@ __global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict_
 // more candidates walk their bitset instead.
 constexpr int LMAX = 48;
 
+// Energy update with the reference's strict '<' (the first minimum in
+// evaluation order wins).
+__device__ __forceinline__ void take_min(int e, int d, int& min_val, int& min_d) {
+    if (e < min_val) { min_val = e; min_d = d; }
+}
+
 // blockIdx.x = row, blockIdx.y = view (0 left, 1 right).  The other view's
 // descriptor row arrives by bulk copy (TMA) while the CTA expands the
 // candidate lists of the row's grid cells into shared memory.
+//
+// Per pixel u the reference evaluates the cell's sorted list, skipping the
+// plane window [d_plane - r, d_plane + r] and every d whose warped column
+// leaves [3, W - 3), then the window with the penalty added.  Here:
+//   * the warped-column test is one bound on d (dlim below): the left view
+//     needs d <= u - 3, the right view d <= W - 4 - u, every other bound
+//     holds for 3 < u < W - 3; the list is ascending, so the walk stops at
+//     the first d > dlim;
+//   * when every window penalty is negative (the usual parameters), the
+//     window entries need no skipping in the list walk: the window pass
+//     re-evaluates each of them with a strictly lower energy, so it ends
+//     at the same (value, first index) as the reference's walk;
+//   * RFIX > 0 unrolls the window for plane_radius == RFIX;
+//   * the own descriptor and the prior of the thread's next pixel are
+//     loaded before the current pixel is matched.
+template <int RFIX>
 __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0, const uint4* __restrict__ desc1,
                                                const uint32_t* __restrict__ prior0, const uint32_t* __restrict__ prior1,
                                                const uint32_t* __restrict__ grid0, const uint32_t* __restrict__ grid1,
@@ -184,6 +206,12 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
     const int v = blockIdx.x;
     const bool right = blockIdx.y != 0;
     const int W = g.W, H = g.H;
+    const int tid = threadIdx.x, NT = blockDim.x;
+    float* disp = (right ? disp1 : disp0) + size_t(v) * W;
+    if (!(v > 3 && v < H - 3)) {           // CTA-uniform: no copy is issued for these rows
+        for (int u = tid; u < W; u += NT) disp[u] = -1.0f;
+        return;
+    }
     uint4* row = reinterpret_cast<uint4*>(sm);
     int16_t* lst = reinterpret_cast<int16_t*>(sm + size_t(W) * 16);
     uint8_t* lcnt = reinterpret_cast<uint8_t*>(lst + size_t(g.gw) * LMAX);
@@ -191,15 +219,13 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
     const uint4* other = (right ? desc0 : desc1) + size_t(v) * W;
     const uint32_t* prior = (right ? prior1 : prior0) + size_t(v) * W;
     const uint32_t* grid = right ? grid1 : grid0;
-    float* disp = (right ? disp1 : disp0) + size_t(v) * W;
-    const int tid = threadIdx.x;
     if (tid == 0) {
         mbar_init(&bar, 1);
         mbar_expect_tx(&bar, unsigned(W) * 16u);
         bulk_g2s_chunked(row, other, unsigned(W) * 16u, &bar);
     }
     const int gy = floordiv(v, g.gs);
-    for (int c = tid; c < g.gw; c += blockDim.x) {
+    for (int c = tid; c < g.gw; c += NT) {
         const uint32_t* cell = grid + (size_t(gy) * g.gw + c) * g.words;
         int n = 0;
         for (int w = 0; w < g.words; ++w) {
@@ -213,6 +239,10 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
         }
         lcnt[c] = uint8_t(n > LMAX ? 255 : n);
     }
+    // first pixel of this thread and its prefetch
+    int u = tid;
+    uint32_t pk_next = u < W ? prior[u] : 0u;
+    uint4 I_next = u < W ? self[u] : make_uint4(0, 0, 0, 0);
     __syncthreads();
     if (!mbar_wait_bounded(&bar, 0, MBAR_WAIT_LIMIT)) {
         if (tid == 0) atomicOr(err, ERRF_TMA_TIMEOUT);
@@ -220,54 +250,86 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
         return;
     }
     const int dir = right ? 1 : -1;
-    const int r = p.plane_radius;
-    const bool v_ok = v > 3 && v < H - 3;
+    const int r = RFIX > 0 ? RFIX : p.plane_radius;
     const uint32_t dmask = (1u << pshift) - 1u;
-    for (int u = tid; u < W; u += blockDim.x) {
+    const int gs = g.gs;
+    // cell of u, advanced incrementally (u grows by NT per iteration)
+    int cell = u / gs, rem = u - cell * gs;
+    const int cstep = NT / gs, rstep = NT - cstep * gs;
+    for (; u < W; u += NT) {
+        const uint32_t pk = pk_next;
+        const uint4 I1 = I_next;
+        const int c = cell;
+        {
+            const int un = u + NT;
+            if (un < W) { pk_next = prior[un]; I_next = self[un]; }
+            cell += cstep;
+            rem += rstep;
+            if (rem >= gs) { rem -= gs; ++cell; }
+        }
         float out = -1.0f;
-        const uint32_t pk = prior[u];
         const int dp = int(pk & dmask);
-        if (v_ok && u > 3 && u < W - 3 && (pk >> pshift) != 0 && dp > 0) {
-            const uint4 I1 = self[u];
-            if (p.match_texture <= 0 || texture16(I1) >= p.match_texture) {
-                const int dpmin = imax(dp - r, 0);
-                const int dpmax = imin(dp + r, g.D);
-                const int c = floordiv(u, g.gs);
-                int min_val = 10000, min_d = -1;
-                const int n = lcnt[c];
-                if (n != 255) {
-                    const int16_t* L = lst + c * LMAX;
-                    for (int i = 0; i < n; ++i) {
-                        const int d = L[i];
-                        if (d >= dpmin && d <= dpmax) continue;
-                        const int uw = u + dir * d;
-                        if (uw < 3 || uw >= W - 3) continue;
-                        const int e = sad16(I1, row[uw]);
-                        if (e < min_val) { min_val = e; min_d = d; }
+        if (u > 3 && u < W - 3 && (pk >> pshift) != 0 && dp > 0 &&
+            (p.match_texture <= 0 || texture16(I1) >= p.match_texture)) {
+            const int dlim = right ? W - 4 - u : u - 3;
+            const int dpmin = imax(dp - r, 0);
+            const int dpmax = imin(dp + r, g.D);
+            int min_val = 10000, min_d = -1;
+            const int n = lcnt[c];
+            if (n != 255) {
+                const int16_t* Ls = lst + c * LMAX;
+                int i = 0;
+                if (p.window_negative) {
+                    const uint32_t* L2 = reinterpret_cast<const uint32_t*>(Ls);
+                    for (; i + 1 < n; i += 2) {
+                        const uint32_t pr = L2[i >> 1];
+                        const int da = int(pr & 0xffffu), db = int(pr >> 16);
+                        if (db > dlim) break;
+                        const int ea = sad16(I1, row[u + dir * da]);
+                        const int eb = sad16(I1, row[u + dir * db]);
+                        take_min(ea, da, min_val, min_d);
+                        take_min(eb, db, min_val, min_d);
+                    }
+                    for (; i < n; ++i) {
+                        const int d = Ls[i];
+                        if (d > dlim) break;
+                        take_min(sad16(I1, row[u + dir * d]), d, min_val, min_d);
                     }
                 } else {
-                    const uint32_t* cell = grid + (size_t(gy) * g.gw + c) * g.words;
-                    for (int w = 0; w < g.words; ++w) {
-                        uint32_t bits = cell[w];
-                        while (bits) {
-                            const int d = 32 * w + __ffs(bits) - 1;
-                            bits &= bits - 1;
-                            if (d >= dpmin && d <= dpmax) continue;
-                            const int uw = u + dir * d;
-                            if (uw < 3 || uw >= W - 3) continue;
-                            const int e = sad16(I1, row[uw]);
-                            if (e < min_val) { min_val = e; min_d = d; }
-                        }
+                    for (; i < n; ++i) {
+                        const int d = Ls[i];
+                        if (d > dlim) break;
+                        if (d >= dpmin && d <= dpmax) continue;
+                        take_min(sad16(I1, row[u + dir * d]), d, min_val, min_d);
                     }
                 }
-                for (int d = dpmin; d <= dpmax; ++d) {
-                    const int uw = u + dir * d;
-                    if (uw < 3 || uw >= W - 3) continue;
-                    const int e = sad16(I1, row[uw], p.penalty[d > dp ? d - dp : dp - d]);
-                    if (e < min_val) { min_val = e; min_d = d; }
+            } else {
+                const uint32_t* cw = grid + (size_t(gy) * g.gw + c) * g.words;
+                bool done = false;
+                for (int w = 0; w < g.words && !done; ++w) {
+                    uint32_t bits = cw[w];
+                    while (bits) {
+                        const int d = 32 * w + __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        if (d > dlim) { done = true; break; }
+                        if (d >= dpmin && d <= dpmax) continue;
+                        take_min(sad16(I1, row[u + dir * d]), d, min_val, min_d);
+                    }
                 }
-                out = min_d >= 0 ? float(min_d) : -1.0f;
             }
+            if (RFIX > 0) {
+#pragma unroll
+                for (int k = -RFIX; k <= RFIX; ++k) {
+                    const int d = dp + k;
+                    if (d >= 0 && d <= g.D && d <= dlim)
+                        take_min(sad16(I1, row[u + dir * d], p.penalty[k < 0 ? -k : k]), d, min_val, min_d);
+                }
+            } else {
+                const int dhi = imin(dpmax, dlim);
+                for (int d = dpmin; d <= dhi; ++d)
+                    take_min(sad16(I1, row[u + dir * d], p.penalty[d > dp ? d - dp : dp - d]), d, min_val, min_d);
+            }
+            out = min_d >= 0 ? float(min_d) : -1.0f;
         }
         disp[u] = out;
     }
@@ -322,11 +384,18 @@ cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t*
                          const uint32_t* grid0, const uint32_t* grid1, float* disp0, float* disp1, const Geom& g,
                          const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads) {
     size_t smem = dense_smem_bytes(g);
-    cudaFuncSetAttribute(k_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (threads <= 0) threads = 512;
     threads = imin(threads, ((g.W + 31) / 32) * 32);
-    k_dense<<<dim3(g.H, 2), threads, smem, st>>>(desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
-                                                  pshift, err);
+    const dim3 grid(g.H, 2);
+    if (p.plane_radius == 2) {
+        cudaFuncSetAttribute(k_dense<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        k_dense<2><<<grid, threads, smem, st>>>(desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
+                                                pshift, err);
+    } else {
+        cudaFuncSetAttribute(k_dense<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        k_dense<0><<<grid, threads, smem, st>>>(desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
+                                                pshift, err);
+    }
     return cudaGetLastError();
 }
 

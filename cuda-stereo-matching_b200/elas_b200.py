@@ -23,7 +23,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported", 3: "CUDA error", 4: 
 STAGES = {
     "desc_left": 0, "desc_right": 1, "can_lr": 2, "can": 3, "support": 4, "grid_left": 5, "grid_right": 6,
     "tri_left": 7, "tri_right": 8, "prior_left": 9, "prior_right": 10, "disp_left": 11, "disp_right": 12,
-    "lr_left": 13, "lr_right": 14, "pn_features": 15, "pn_output": 16, "pn_bins": 17,
+    "lr_left": 13, "lr_right": 14, "pn_features": 15, "pn_output": 16, "pn_bins": 17, "del_counters": 18,
 }
 
 PN_PARAMS = 36992

@@ -231,7 +231,10 @@ int elas_b200_pn_adam(float* p, const float* g, float* m, float* v, int32_t n, f
 #define ELAS_STAGE_PN_OUTPUT    16   /* bf16   [2][h/4][w/4][32] proposal network output */
 #define ELAS_STAGE_PN_BINS      17   /* uint32 [ch][cw] top-4 bins per candidate, one byte each
                                       * (best first, 0xff = none) */
-#define ELAS_STAGE_COUNT        18
+#define ELAS_STAGE_DEL_COUNTERS 18   /* int32  [2][16] Delaunay counters per view: [0] triangles,
+                                      * [4] flip rounds, [5] flips, [6] non-empty lattice rows,
+                                      * [8] set by the flip kernel that ran, [9] support points */
+#define ELAS_STAGE_COUNT        19
 
 /* Copy stage `stage` of the last single-pair call into host memory `dst`
  * of `bytes` bytes.  *needed receives the size in bytes (call with
