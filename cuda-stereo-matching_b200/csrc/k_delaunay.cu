@@ -54,6 +54,32 @@ __device__ int block_scan(int v, int* warp_sums, int* total) {
     return r;
 }
 
+// Reserve one slot per calling lane in a list whose length counter `ctr`
+// is shared by many threads: one atomic per converged group of lanes
+// instead of one per lane (shared-memory atomics on one address serialise).
+// The order of entries within a list carries no meaning.
+__device__ __forceinline__ int agg_inc(int* ctr) {
+    const unsigned mask = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(ctr, __popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+// As agg_inc, for lanes whose counters may differ (grouped by address).
+__device__ __forceinline__ int agg_inc_keyed(int* ctr) {
+    const unsigned mask = __activemask();
+    const unsigned peers = __match_any_sync(mask, reinterpret_cast<unsigned long long>(ctr));
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(ctr, __popc(peers));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(peers & ((1u << lane) - 1u));
+}
+
 // Per lattice row: sort the row's points by (x, index), drop repeated x
 // (keeps the lowest index), write the unique list to srt[row_off[r] ..] and
 // its length to rcnt[r].
@@ -328,7 +354,7 @@ __global__ void __launch_bounds__(FLIP_THREADS) k_flip_global(DelDev d0, DelDev 
         for (int k = tid; k < items; k += FLIP_THREADS) {
             int h = round == 0 ? k : cur[k];
             if (!flip_propose(m, h, T, uint32_t(round), round == 0, [&](int hh, int nn) {
-                    int idx = atomicAdd(&n_cand, 1);
+                    int idx = agg_inc(&n_cand);
                     if (idx < cand_cap) { D.cand[2 * idx] = hh; D.cand[2 * idx + 1] = nn; }
                 }))
                 set_err(err, ERRF_BOUNDS);
@@ -341,7 +367,7 @@ __global__ void __launch_bounds__(FLIP_THREADS) k_flip_global(DelDev d0, DelDev 
         for (int c = tid; c < nc; c += FLIP_THREADS) {
             int h = D.cand[2 * c], n = D.cand[2 * c + 1];
             if (flip_apply(m, h, n, uint32_t(round))) {
-                int f = atomicAdd(&n_flip, 1);
+                int f = agg_inc(&n_flip);
                 D.flips[6 * f] = h / 3;
                 D.flips[6 * f + 1] = n;
             }
@@ -358,7 +384,7 @@ __global__ void __launch_bounds__(FLIP_THREADS) k_flip_global(DelDev d0, DelDev 
         }
         __syncthreads();
         auto push = [&](int x) {
-            int idx = atomicAdd(&n_next, 1);
+            int idx = agg_inc(&n_next);
             if (idx < wl_cap) nxt[idx] = x;
         };
         for (int f = tid; f < nf; f += FLIP_THREADS) {
@@ -509,7 +535,7 @@ __global__ void __launch_bounds__(1024) k_flip_local(DelDev d0, DelDev d1, int m
         // A: propose (round 0: every half-edge, owner rule)
         const int items = round == 0 ? 3 * T : min(n_wl[cur], wl[cur].cap());
         auto add_cand = [&](int hh, int nn) {
-            int idx = atomicAdd(&n_cand, 1);
+            int idx = agg_inc(&n_cand);
             if (idx < cand.cap()) { int32_t* c = cand.slot(idx); c[0] = hh; c[1] = nn; }
         };
         for (int k = tid; k < items; k += NT) {
@@ -527,7 +553,7 @@ __global__ void __launch_bounds__(1024) k_flip_local(DelDev d0, DelDev d1, int m
             const int32_t* cc = cand.slot(c);
             int h = cc[0], n = cc[1];
             if (flip_apply(m, h, n, uint32_t(round))) {
-                int f = atomicAdd(&n_flip, 1);     // at most T/2 <= flips.cap()
+                int f = agg_inc(&n_flip);     // at most T/2 <= flips.cap()
                 int32_t* q = flips.slot(f);
                 q[0] = h / 3; q[1] = n;
             }
@@ -547,7 +573,7 @@ __global__ void __launch_bounds__(1024) k_flip_local(DelDev d0, DelDev d1, int m
         __syncthreads();
         // C2: relink, queue the outer edges, release locks, requeue lost proposals
         auto push = [&](int x) {
-            int idx = atomicAdd(&n_wl[nxt], 1);
+            int idx = agg_inc(&n_wl[nxt]);
             if (idx < wl[nxt].cap()) *wl[nxt].slot(idx) = x;
         };
         for (int f = tid; f < nf; f += NT) {
@@ -643,7 +669,7 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, 
         // A: propose (round 0: every own half-edge, owner rule)
         const int items = round == 0 ? 3 * (t1 - t0) : min(n_wl[cur], WL_PER_CTA);
         auto add_cand = [&](int hh, int nn) {
-            int idx = atomicAdd(&n_cand[cur], 1);
+            int idx = agg_inc(&n_cand[cur]);
             if (idx < CAND_PER_CTA) { cand[2 * idx] = hh; cand[2 * idx + 1] = nn; }
         };
         for (int k = tid; k < items; k += CL_THREADS) {
@@ -661,7 +687,7 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, 
         for (int c = tid; c < nc; c += CL_THREADS) {
             int h = cand[2 * c], n = cand[2 * c + 1];
             if (flip_apply(m, h, n, uint32_t(round))) {
-                int f = atomicAdd(&n_flip, 1);
+                int f = agg_inc(&n_flip);
                 if (f < FLIP_PER_CTA) { flips[6 * f] = h / 3; flips[6 * f + 1] = n; }
             }
         }
@@ -681,7 +707,7 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, 
         auto push = [&](int x) {
             int t = x / 3;
             int* cnt = sync.remote(&n_wl[nxt], t >> shift);
-            int idx = atomicAdd(cnt, 1);
+            int idx = agg_inc_keyed(cnt);
             if (idx < WL_PER_CTA) D.cwl[size_t(t >> shift) * 2 * WL_PER_CTA + size_t(nxt) * WL_PER_CTA + idx] = x;
         };
         for (int f = tid; f < nf; f += CL_THREADS) {

@@ -286,6 +286,80 @@ __global__ void k_topk(const __nv_bfloat16* __restrict__ F, uint32_t* __restrict
     if (lane == 0) bins[warp] = packed;
 }
 
+// Top-4 bins with the right view's feature row in shared memory: one CTA
+// per candidate row, one thread per candidate.  A thread keeps its left
+// cell's 32 features in registers, walks the 64 bins in ascending order and
+// keeps the four best (score descending, lower bin first on ties) -- the
+// same order k_topk's repeated warp maximum yields.  Scores are the same
+// fp32 FMA chain over channels 0..31.  The row is stored with the four
+// 16-byte chunks of cell x rotated by (x >> 1) & 3, which spreads the
+// chunks that neighbouring candidates read over distinct banks.
+__device__ __forceinline__ int topk_slot(int x, int q) { return 4 * x + (q ^ ((x >> 1) & 3)); }
+
+__global__ void __launch_bounds__(256) k_topk_rows(const __nv_bfloat16* __restrict__ F, uint32_t* __restrict__ bins,
+                                                   int Hd, int Wd, int cw, int step, int D) {
+    extern __shared__ __align__(16) uint4 frow[];
+    const int vc = blockIdx.x;
+    const int v = vc * step;
+    const int cy = min(v / 4, Hd - 1);
+    const uint4* src = reinterpret_cast<const uint4*>(F + ((size_t(1) * Hd + cy) * Wd) * CH);
+    for (int i = threadIdx.x; i < 4 * Wd; i += blockDim.x) frow[topk_slot(i >> 2, i & 3)] = src[i];
+    __syncthreads();
+    const int w = bin_width(D);
+    const uint4* lrow = reinterpret_cast<const uint4*>(F + ((size_t(0) * Hd + cy) * Wd) * CH);
+    for (int ci = threadIdx.x; ci < cw; ci += blockDim.x) {
+        const int cx = min((ci * step) / 4, Wd - 1);
+        float fl[CH];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint4 a = lrow[size_t(cx) * 4 + q];
+            const __nv_bfloat162* a2 = reinterpret_cast<const __nv_bfloat162*>(&a);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                float2 f = __bfloat1622float2(a2[j]);
+                fl[8 * q + 2 * j] = f.x;
+                fl[8 * q + 2 * j + 1] = f.y;
+            }
+        }
+        float ts[TOPK];
+        int tb[TOPK];
+#pragma unroll
+        for (int r = 0; r < TOPK; ++r) { ts[r] = -INFINITY; tb[r] = int(NO_BIN); }
+        for (int b = 0; b < NBINS; ++b) {
+            const int x2 = cx - bin_shift(b, w);
+            if (x2 < 0) break;            // the shift grows with b
+            float acc = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                uint4 c = frow[topk_slot(x2, q)];
+                const __nv_bfloat162* c2 = reinterpret_cast<const __nv_bfloat162*>(&c);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float2 fc = __bfloat1622float2(c2[j]);
+                    acc = fmaf(fl[8 * q + 2 * j], fc.x, acc);
+                    acc = fmaf(fl[8 * q + 2 * j + 1], fc.y, acc);
+                }
+            }
+            const float sc = SCALE * acc;
+            if (tb[TOPK - 1] != int(NO_BIN) && !(sc > ts[TOPK - 1])) continue;
+            // insert (sc, b) behind every kept entry with a score >= sc
+#pragma unroll
+            for (int r = TOPK - 1; r >= 0; --r) {
+                const bool above = r > 0 && (tb[r - 1] == int(NO_BIN) || sc > ts[r - 1]);
+                const bool here = tb[r] == int(NO_BIN) || sc > ts[r];
+                if (here) {
+                    if (above) { ts[r] = ts[r - 1]; tb[r] = tb[r - 1]; }
+                    else { ts[r] = sc; tb[r] = b; }
+                }
+            }
+        }
+        uint32_t packed = 0;
+#pragma unroll
+        for (int r = 0; r < TOPK; ++r) packed |= uint32_t(tb[r] & 0xff) << (8 * r);
+        bins[size_t(vc) * cw + ci] = packed;
+    }
+}
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against libcuda).
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -367,7 +441,14 @@ cudaError_t launch_topk(const __nv_bfloat16* F, uint32_t* bins, int Hd, int Wd, 
                         cudaStream_t st) {
     const int n = cw * ch;
     if (n <= 0) return cudaSuccess;
-    k_topk<<<(n * 32 + 255) / 256, 256, 0, st>>>(F, bins, Hd, Wd, cw, ch, step, D);
+    const size_t smem = size_t(Wd) * CH * sizeof(__nv_bfloat16);
+    if (smem <= 200 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_topk_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+        k_topk_rows<<<ch, 256, smem, st>>>(F, bins, Hd, Wd, cw, step, D);
+    } else {
+        k_topk<<<(n * 32 + 255) / 256, 256, 0, st>>>(F, bins, Hd, Wd, cw, ch, step, D);
+    }
     return cudaGetLastError();
 }
 

@@ -114,7 +114,8 @@ __device__ __forceinline__ int sweep_restricted(const uint4* self_m2, const uint
     const uint4 c0 = self_m2[u - 2], c1 = self_m2[u + 2], c2 = self_p2[u - 2], c3 = self_p2[u + 2];
     int e1 = INF_E, d1 = 0x7fffffff, c = 0, e2 = INF_E;
     for (int e = lane; e < pn::TOPK * L; e += 32) {
-        const int r = e / L;
+        static_assert(pn::TOPK == 4, "e / L below assumes four bins");
+        const int r = int(e >= L) + int(e >= 2 * L) + int(e >= 3 * L);   // e / L, as e < 4 L
         const int lor = r == 0 ? lo[0] : r == 1 ? lo[1] : r == 2 ? lo[2] : lo[3];
         if (lor == INT32_MIN / 2) continue;
         const int d = lor + (e - r * L);

@@ -158,3 +158,48 @@ def test_trained_proposal_gain():
     assert np.mean(fb_t) < 0.5
     assert np.mean(fb_u) > np.mean(fb_t) + 0.1
     assert np.mean(bad_l) - np.mean(bad_p) < 0.01
+
+
+@pytest.mark.parametrize("preset,seed", [(1, 33), (2, 34)])
+def test_topk_bins_match_float64_scores(preset, seed):
+    """The packed top-4 bins of every candidate, from the GPU's own network
+    output: valid, distinct, as many as there are valid bins (up to four),
+    and the four best of the float64 scores.  Where two scores lie within
+    float rounding of each other either order is accepted, so the check
+    compares the scores of the chosen bins, not the bin numbers."""
+    L, R, _, _ = eb.synth_pair(preset, seed)
+    W, H, D = eb.synth_dims(preset)
+    p = eb.params_config(D)
+    e = eb.Elas(p)
+    e.set_proposal(_weights_or_random())
+    e.process(L, R)
+    step = p.candidate_stepsize
+    ch, cw = H // step, W // step
+    hd, wd = H // 4, W // 4
+    F = eb.bf16_to_f32(e.stage("pn_output")).reshape(2, hd, wd, 32).astype(np.float64)
+    bins = e.stage("pn_bins").view(np.uint32).reshape(ch, cw)
+    e.close()
+    sh = po.bin_shifts(D)
+    cys = np.minimum(np.arange(ch) * step // 4, hd - 1)
+    cxs = np.minimum(np.arange(cw) * step // 4, wd - 1)
+    worst = 0.0
+    for vc in range(ch):
+        cy = cys[vc]
+        xr = cxs[:, None] - sh[None, :]                       # (cw, 64)
+        valid = xr >= 0
+        s = po.SCALE * np.einsum("ck,cbk->cb", F[0, cy, cxs], F[1, cy, np.maximum(xr, 0)])
+        s = np.where(valid, s, -np.inf)
+        exp_sorted = -np.sort(-s, axis=1)[:, :po.TOPK]
+        for ci in range(cw):
+            got = po.unpack_bins(bins[vc, ci])
+            nvalid = int(valid[ci].sum())
+            assert len(got) == min(po.TOPK, nvalid)
+            assert len(set(got)) == len(got)
+            assert all(valid[ci, b] for b in got)
+            gs = s[ci, got]
+            es = exp_sorted[ci, :len(got)]
+            tol = 1e-5 * (1.0 + np.abs(es))
+            assert np.all(np.diff(gs) <= tol[1:]), (vc, ci, got, gs)
+            if len(got):
+                worst = max(worst, float(np.max(np.abs(gs - es) / tol)))
+    assert worst <= 1.0, worst
