@@ -256,6 +256,240 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_support_sweep(const uint4* __
         can_out[size_t(vc) * g.cw + ci] = res[ci - c_begin];
 }
 
+// ---------------------------------------------------------------------------
+// Plain sweep with Q threads per candidate.  Thread j of a candidate's group
+// takes a contiguous slice of its disparity range and keeps a commutative
+// state of its slice (Best2 below, equivalent to Top2); the Q states merge
+// by shuffles and the closed form above decides, so the result equals the
+// reference's lane-by-lane merge whatever the slicing.  Inside a slice the
+// other view's descriptors slide: the column read fresh at disparity d
+// (u + dir (d + 2)) is the one the four-rows energy needs again at d + 4
+// (u + dir (d - 2) then), so each disparity loads one descriptor per row
+// instead of two; the last loads live in two register banks.
+//
+// Packed state of the plain sweep: the two smallest values of
+// energy << 17 | lane << 12 | d over the disparities seen (energy < 2^14,
+// d < 2^12, lane = (d - dmin) & 31).  The smallest value is the Top2
+// state's (E1, first minimum in merge order); the second smallest carries
+// the smallest energy among the other disparities, and it equals E1
+// exactly when the minimum is attained more than once.  Updates are three
+// min/max operations and the state merges by the same rule.
+constexpr uint32_t PK_INF = 0xffffffffu;
+struct Best2 {
+    uint32_t v1, v2;
+};
+__device__ __forceinline__ uint32_t pack_ek(int e, int d, int dmin) {
+    return (uint32_t(e) << 17) | (uint32_t((d - dmin) & 31) << 12) | uint32_t(d);
+}
+__device__ __forceinline__ void best2_add(Best2& b, uint32_t v) {
+    const uint32_t hi = max(b.v1, v);
+    b.v1 = min(b.v1, v);
+    b.v2 = min(b.v2, hi);
+}
+__device__ __forceinline__ void best2_merge(Best2& a, const Best2& b) {
+    const uint32_t lo = min(a.v1, b.v1), hi = max(a.v1, b.v1);
+    a.v2 = min(hi, min(a.v2, b.v2));
+    a.v1 = lo;
+}
+// The reference's decision on a merged state: the disparity, or -1.
+__device__ __forceinline__ int best2_decide(const Best2& b, float thr) {
+    if (b.v1 == PK_INF) return -1;
+    const int e1 = int(b.v1 >> 17);
+    const int e2 = b.v2 == PK_INF ? INF_E : int(b.v2 >> 17);
+    const int second = ((b.v1 >> 12) & 31u) == 0 ? e1 : e2;
+    return float(e1) < thr * float(second) ? int(b.v1 & 0xfffu) : -1;
+}
+
+// Energy of disparity d from the fresh and the lagging columns of both rows.
+template <int DIR>
+__device__ __forceinline__ int slice_energy(const uint4& c0, const uint4& c1, const uint4& c2, const uint4& c3,
+                                            const uint4& fm, const uint4& fp, const uint4& lm, const uint4& lp) {
+    // c0 / c2 pair with column u + dir d - 2, c1 / c3 with u + dir d + 2
+    const int em = DIR < 0 ? sad16(c1, lm, sad16(c0, fm)) : sad16(c1, fm, sad16(c0, lm));
+    const int ep = DIR < 0 ? sad16(c3, lp, sad16(c2, fp)) : sad16(c3, fp, sad16(c2, lp));
+    return em + ep;
+}
+
+template <int DIR>
+__device__ __forceinline__ Best2 sweep_slice(const uint4* self_m2, const uint4* self_p2, const uint4* oth_m2,
+                                             const uint4* oth_p2, int u, int dmin, int da, int db) {
+    Best2 s{PK_INF, PK_INF};
+    if (da > db) return s;
+    const uint4 c0 = self_m2[u - 2], c1 = self_m2[u + 2], c2 = self_p2[u - 2], c3 = self_p2[u + 2];
+    // two register banks of lagging columns: bank A serves d = d0 .. d0+3
+    // and receives the fresh columns of d0+4 .. d0+7, which serve the next
+    // block; no register is copied
+    uint4 Am[4], Ap[4], Bm[4], Bp[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int d = da + k;
+        if (d <= db) {
+            const int x = u + DIR * (d - 2);
+            Am[k] = oth_m2[x];
+            Ap[k] = oth_p2[x];
+        }
+    }
+    int d0 = da;
+    for (; d0 + 7 <= db; d0 += 8) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int d = d0 + k;
+            const int x = u + DIR * (d + 2);
+            Bm[k] = oth_m2[x];
+            Bp[k] = oth_p2[x];
+            best2_add(s, pack_ek(slice_energy<DIR>(c0, c1, c2, c3, Bm[k], Bp[k], Am[k], Ap[k]), d, dmin));
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int d = d0 + 4 + k;
+            const int x = u + DIR * (d + 2);
+            Am[k] = oth_m2[x];
+            Ap[k] = oth_p2[x];
+            best2_add(s, pack_ek(slice_energy<DIR>(c0, c1, c2, c3, Am[k], Ap[k], Bm[k], Bp[k]), d, dmin));
+        }
+    }
+    // tail: fewer than 8 disparities left (bank A lags d0 .. d0+3)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int d = d0 + k;
+        if (d <= db) {
+            const int x = u + DIR * (d + 2);
+            Bm[k] = oth_m2[x];
+            Bp[k] = oth_p2[x];
+            best2_add(s, pack_ek(slice_energy<DIR>(c0, c1, c2, c3, Bm[k], Bp[k], Am[k], Ap[k]), d, dmin));
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int d = d0 + 4 + k;
+        if (d <= db) {
+            const int x = u + DIR * (d + 2);
+            const uint4 fm = oth_m2[x], fp = oth_p2[x];
+            best2_add(s, pack_ek(slice_energy<DIR>(c0, c1, c2, c3, fm, fp, Bm[k], Bp[k]), d, dmin));
+        }
+    }
+    return s;
+}
+
+// Merge the states of a group of Q consecutive lanes and decide; every
+// lane of the group returns the same value.
+template <int Q>
+__device__ __forceinline__ int group_decide(Best2 s, float thr) {
+#pragma unroll
+    for (int o = Q / 2; o > 0; o >>= 1) {
+        Best2 t;
+        t.v1 = __shfl_xor_sync(0xffffffffu, s.v1, o);
+        t.v2 = __shfl_xor_sync(0xffffffffu, s.v2, o);
+        best2_merge(s, t);
+    }
+    return best2_decide(s, thr);
+}
+
+// Slice [da, db] of thread j of Q over the range [lo, hi].  The slice
+// length is odd, so the eight slices of a candidate start in eight
+// different 16-byte bank groups and one shared-memory phase (8 lanes of a
+// 16-byte load) is free of conflicts.
+__device__ __forceinline__ void slice_of(int lo, int hi, int j, int Q, int& da, int& db) {
+    const int n = hi - lo + 1;
+    int per = (n + Q - 1) / Q;
+    per |= 1;
+    da = lo + j * per;
+    db = imin(hi, da + per - 1);
+}
+
+// grid.x = segments of a candidate row, grid.y = candidate rows; blockDim =
+// Q x candidates per pass.  SMEM: the four descriptor rows arrive by bulk
+// copy (TMA); otherwise they are read through L1 from global memory.
+constexpr int SWEEP_Q_THREADS = 512;   // at most 64 candidates x 8 threads per pass (128 registers)
+template <int Q, bool SMEM>
+__global__ void __launch_bounds__(SWEEP_Q_THREADS) k_support_sweep_q(const uint4* __restrict__ desc0,
+                                                          const uint4* __restrict__ desc1,
+                                                          int32_t* __restrict__ can_out, Geom g, DevParams p,
+                                                          int seg, unsigned* err) {
+    extern __shared__ __align__(128) uint4 rows[];
+    __shared__ int res[256];
+    __shared__ uint64_t bar;
+    const int W = g.W, H = g.H;
+    const int vc = blockIdx.y;
+    const int v = vc * g.step;
+    const int c_begin = blockIdx.x * seg, c_end = min(g.cw, c_begin + seg);
+    if (c_begin >= c_end) return;
+    const bool row_ok = v >= 5 && v <= H - 6;
+    if (!row_ok) {                       // CTA-uniform: no copy is issued for these rows
+        for (int ci = c_begin + threadIdx.x; ci < c_end; ci += blockDim.x) can_out[size_t(vc) * g.cw + ci] = -1;
+        return;
+    }
+    const uint4 *L_m2, *L_p2, *R_m2, *R_p2;
+    if (SMEM) {
+        if (threadIdx.x == 0) {
+            const uint4* src[4] = {desc0 + size_t(v - 2) * W, desc0 + size_t(v + 2) * W,
+                                   desc1 + size_t(v - 2) * W, desc1 + size_t(v + 2) * W};
+            mbar_init(&bar, 1);
+            mbar_expect_tx(&bar, 4u * unsigned(W) * 16u);
+            for (int r = 0; r < 4; ++r) bulk_g2s_chunked(rows + r * W, src[r], unsigned(W) * 16u, &bar);
+        }
+        L_m2 = rows; L_p2 = rows + W; R_m2 = rows + 2 * W; R_p2 = rows + 3 * W;
+    } else {
+        L_m2 = desc0 + size_t(v - 2) * W; L_p2 = desc0 + size_t(v + 2) * W;
+        R_m2 = desc1 + size_t(v - 2) * W; R_p2 = desc1 + size_t(v + 2) * W;
+    }
+    __syncthreads();
+    if (SMEM && !mbar_wait_bounded(&bar, 0, MBAR_WAIT_LIMIT)) {
+        if (threadIdx.x == 0) atomicOr(err, ERRF_TMA_TIMEOUT);
+        mbar_wait_bounded(&bar, 0, MBAR_WAIT_LIMIT);   // let the copies in flight land before exiting
+        return;
+    }
+    const int j = threadIdx.x % Q, per_pass = blockDim.x / Q;
+    const int n_seg = c_end - c_begin;
+    const int passes = (n_seg + per_pass - 1) / per_pass;   // uniform: every lane joins the shuffles
+    // left view: candidates of the segment, swept L->R
+    for (int pass = 0; pass < passes; ++pass) {
+        const int ci = c_begin + pass * per_pass + int(threadIdx.x) / Q;
+        const int u = ci * g.step;
+        bool active = false;
+        int dmax = 0;
+        if (ci < c_end && u >= 5 && u <= W - 6 && texture16(desc0[size_t(v) * W + u]) >= p.support_texture) {
+            dmax = min(g.D, u - 5);
+            active = dmax - g.dmin >= 10;
+        }
+        Best2 st{PK_INF, PK_INF};
+        if (active) {
+            int da, db;
+            slice_of(g.dmin, dmax, j, Q, da, db);
+            st = sweep_slice<-1>(L_m2, L_p2, R_m2, R_p2, u, g.dmin, da, db);
+        }
+        const int r = group_decide<Q>(st, p.support_threshold);
+        if (ci < c_end && j == 0) res[ci - c_begin] = active ? r : -1;
+    }
+    __syncthreads();
+    // right view: re-match accepted candidates from u - d
+    for (int pass = 0; pass < passes; ++pass) {
+        const int ci = c_begin + pass * per_pass + int(threadIdx.x) / Q;
+        const int dl = ci < c_end ? res[ci - c_begin] : -1;
+        bool active = false;
+        int ur = 0, dmax = 0;
+        if (dl >= 0) {
+            ur = ci * g.step - dl;
+            if (texture16(desc1[size_t(v) * W + ur]) >= p.support_texture) {
+                dmax = min(g.D, W - ur - 5);
+                active = dmax - g.dmin >= 10;
+            }
+        }
+        Best2 st{PK_INF, PK_INF};
+        if (active) {
+            int da, db;
+            slice_of(g.dmin, dmax, j, Q, da, db);
+            st = sweep_slice<1>(R_m2, R_p2, L_m2, L_p2, ur, g.dmin, da, db);
+        }
+        const int dr = group_decide<Q>(st, p.support_threshold);
+        __syncwarp();
+        if (ci < c_end && j == 0) res[ci - c_begin] = (active && dr >= 0 && abs(dl - dr) <= p.lr_threshold) ? dl : -1;
+    }
+    __syncthreads();
+    for (int ci = c_begin + threadIdx.x; ci < c_end; ci += blockDim.x)
+        can_out[size_t(vc) * g.cw + ci] = res[ci - c_begin];
+}
+
 // removeInconsistentSupportPoints with snapshot semantics: reads can_in,
 // writes can_out.  The reference's bound `y < can_width`
 // (KerSupportMatches.cu:208) is kept: rows y >= cw pass through.
@@ -449,7 +683,22 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
     segs = (g.cw + seg - 1) / seg;
     size_t smem = size_t(4) * g.W * sizeof(uint4);
     dim3 grid(segs, rows);
-    if (smem <= 200 * 1024) {
+    if (!bins && smem <= 200 * 1024) {
+        // plain sweep: 8 threads per candidate, segments of 32..128
+        // candidates sized for about two CTAs per SM
+        // plain sweep: 8 threads per candidate; segments of at most 256
+        // candidates (each CTA stages the four rows once), sized for about
+        // two CTAs per SM over the whole lattice
+        constexpr int Q = 8;
+        const long long cands = (long long)g.cw * imax(rows, 1);
+        const int want = int(imin(256, imax(32, int((cands + 2 * num_sms - 1) / (2 * num_sms)))));
+        const int qsegs = imax(1, (g.cw + want - 1) / want);
+        int qseg = imax(1, (g.cw + qsegs - 1) / qsegs);
+        qseg = (qseg + 3) & ~3;
+        const int threads = imin(qseg, SWEEP_Q_THREADS / Q) * Q;
+        cudaFuncSetAttribute(k_support_sweep_q<Q, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        k_support_sweep_q<Q, true><<<dim3(qsegs, rows), threads, smem, st>>>(desc0, desc1, can_lr, g, p, qseg, err);
+    } else if (smem <= 200 * 1024) {
         if (bins) {
             cudaFuncSetAttribute(k_support_sweep<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
             k_support_sweep<true, true><<<grid, SWEEP_THREADS, smem, st>>>(desc0, desc1, can_lr, g, p, seg, err, bins,
