@@ -516,8 +516,13 @@ __global__ void k_incon(const int32_t* __restrict__ cin, int32_t* __restrict__ c
 // (|d - d2| <= 1) valid point within 5 cells on BOTH sides, the left side
 // seen after the removals already made on this line, the right side as it
 // was.  The lanes precompute, per point, "valid", "right support" and the
-// 5-bit mask of similar valid points on the left; the serial part then only
-// carries the 5-bit history of removals.
+// 5-bit mask of similar valid points on the left; what remains serial is a
+// 32-state automaton over the 5-bit history of removals
+// (hist' = (hist << 1 | rem) & 31, rem = valid & right & (left & ~hist)).
+// Each lane runs the automaton over its chunk of the line for all 32
+// entry states at once (bit s of H[b] = history bit b when the chunk was
+// entered in state s), the lanes then chain their entry states in order,
+// and each lane replays its chunk from its actual entry state.
 __device__ void redundant_line(int* a, uint8_t* code, int len, int lane) {
     for (int k = lane; k < len; k += 32) {
         int d = a[k];
@@ -536,14 +541,37 @@ __device__ void redundant_line(int* a, uint8_t* code, int len, int lane) {
         code[k] = uint8_t(c);
     }
     __syncwarp();
-    if (lane == 0) {
-        unsigned hist = 0;   // bit b: point k-1-b was removed
-        for (int k = 0; k < len; ++k) {
-            unsigned c = code[k];
-            unsigned rem = (c & 1u) && (c & 2u) && ((c >> 2) & ~hist & 31u) ? 1u : 0u;
-            hist = ((hist << 1) | rem) & 31u;
-            if (rem) a[k] = -1;
+    const int chunk = (len + 31) / 32;
+    const int k0 = imin(len, lane * chunk), k1 = imin(len, k0 + chunk);
+    uint32_t H0 = 0xAAAAAAAAu, H1 = 0xCCCCCCCCu, H2 = 0xF0F0F0F0u, H3 = 0xFF00FF00u, H4 = 0xFFFF0000u;
+    for (int k = k0; k < k1; ++k) {
+        const unsigned c = code[k];
+        uint32_t R = 0;
+        if ((c & 3u) == 3u) {
+            if (c & 4u) R |= ~H0;
+            if (c & 8u) R |= ~H1;
+            if (c & 16u) R |= ~H2;
+            if (c & 32u) R |= ~H3;
+            if (c & 64u) R |= ~H4;
         }
+        H4 = H3; H3 = H2; H2 = H1; H1 = H0; H0 = R;
+    }
+    // entry state of every lane: chain the lanes' maps from state 0
+    unsigned s = 0, mine = 0;
+    for (int i = 0; i < 32; ++i) {
+        const uint32_t h0 = __shfl_sync(0xffffffffu, H0, i), h1 = __shfl_sync(0xffffffffu, H1, i),
+                       h2 = __shfl_sync(0xffffffffu, H2, i), h3 = __shfl_sync(0xffffffffu, H3, i),
+                       h4 = __shfl_sync(0xffffffffu, H4, i);
+        if (lane == i) mine = s;
+        s = ((h0 >> s) & 1u) | (((h1 >> s) & 1u) << 1) | (((h2 >> s) & 1u) << 2) | (((h3 >> s) & 1u) << 3) |
+            (((h4 >> s) & 1u) << 4);
+    }
+    unsigned hist = mine;   // bit b: point k-1-b was removed
+    for (int k = k0; k < k1; ++k) {
+        const unsigned c = code[k];
+        const unsigned rem = (c & 1u) && (c & 2u) && ((c >> 2) & ~hist & 31u) ? 1u : 0u;
+        hist = ((hist << 1) | rem) & 31u;
+        if (rem) a[k] = -1;
     }
     __syncwarp();
 }
