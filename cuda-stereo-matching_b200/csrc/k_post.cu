@@ -245,10 +245,11 @@ __global__ void k_gap(PostViews pv, int W, int H, int gap, int horizontal) {
 
 // Gap interpolation (rows, then columns), adaptive mean and median in one
 // pass over a 32x32 output tile, every intermediate in shared memory.  The
-// input region carries a halo of gap + 3 (the column pass needs the row
-// pass gap rows away, the mean 2 more, the median 1 more).  Each stage is
-// computed exactly as its separate kernel (k_gap_px, k_mean_median) does.
-constexpr int PT = 32, PGMAX = 8, PHALO = PGMAX + 3, PS = PT + 2 * PHALO;   // S tile side
+// input region carries a halo of G + 3 for gaps up to G (the column pass
+// needs the row pass G rows away, the mean 2 more, the median 1 more).
+// Each stage is computed exactly as its separate kernel (k_gap_px,
+// k_mean_median) does.
+constexpr int PT = 32, PGMAX = 8;
 __device__ __forceinline__ float gap_fill(const float* line, int stride, int k, int len, int gap, float c) {
     // line[k*stride] is the pixel; positions < 0 or >= len are outside the image
     if (c >= 0) return c;
@@ -267,25 +268,27 @@ __device__ __forceinline__ float gap_fill(const float* line, int stride, int k, 
 
 // 9-input sorting network (25 compare-exchanges, depth 7; checked by the
 // 0-1 principle on all 512 binary inputs).
+template <int I, int J>
+__device__ __forceinline__ void cex(float* a) {
+    const float x = a[I], y = a[J];
+    a[I] = fminf(x, y);
+    a[J] = fmaxf(x, y);
+}
 __device__ __forceinline__ void sort9(float* a) {
-    constexpr int NET[25][2] = {{0, 3}, {1, 7}, {2, 5}, {4, 8}, {0, 7}, {2, 4}, {3, 8}, {5, 6}, {0, 2},
-                                {1, 3}, {4, 5}, {7, 8}, {1, 4}, {3, 6}, {5, 7}, {0, 1}, {2, 4}, {3, 5},
-                                {6, 8}, {2, 3}, {4, 5}, {6, 7}, {1, 2}, {3, 4}, {5, 6}};
-#pragma unroll
-    for (int k = 0; k < 25; ++k) {
-        float x = a[NET[k][0]], y = a[NET[k][1]];
-        a[NET[k][0]] = fminf(x, y);
-        a[NET[k][1]] = fmaxf(x, y);
-    }
+    cex<0, 3>(a); cex<1, 7>(a); cex<2, 5>(a); cex<4, 8>(a); cex<0, 7>(a); cex<2, 4>(a); cex<3, 8>(a);
+    cex<5, 6>(a); cex<0, 2>(a); cex<1, 3>(a); cex<4, 5>(a); cex<7, 8>(a); cex<1, 4>(a); cex<3, 6>(a);
+    cex<5, 7>(a); cex<0, 1>(a); cex<2, 4>(a); cex<3, 5>(a); cex<6, 8>(a); cex<2, 3>(a); cex<4, 5>(a);
+    cex<6, 7>(a); cex<1, 2>(a); cex<3, 4>(a); cex<5, 6>(a);
 }
 
 constexpr int WT_SMEM = 1024;                   // adaptive-mean weights for |diff| = k/4, k < 1024
 
-template <bool GAP, bool MEAN, bool MEDIAN>
+template <int G, bool GAP, bool MEAN, bool MEDIAN>
 __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, int gap) {
+    constexpr int PHALO = G + 3, PS = PT + 2 * PHALO;   // S tile side
     __shared__ float WT[MEAN ? WT_SMEM : 1];
     __shared__ float S[PS][PS];                 // input, halo PHALO
-    __shared__ float G[PS][PT + 6];             // after the row pass: columns [-3, 35)
+    __shared__ float G2[PS][PT + 6];            // after the row pass: columns [-3, 35)
     __shared__ float V[PT + 6][PT + 6];         // after the column pass: [-3, 35)^2
     __shared__ float M[PT + 2][PT + 2];         // after the mean: [-1, 33)^2
     const float* __restrict__ src = pv.cur[blockIdx.z];
@@ -308,35 +311,44 @@ __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, 
         int x = u0 - 3 + c;
         float val = S[r][c + PHALO - 3];
         if (GAP && val != OUT && val < 0) val = gap_fill(&S[r][c + PHALO - 3], 1, x, W, gap, val);
-        G[r][c] = val;
+        G2[r][c] = val;
     }
     __syncthreads();
     // column pass on [-3, 35)^2
     for (int i = tid; i < (PT + 6) * (PT + 6); i += 1024) {
         int r = i / (PT + 6), c = i % (PT + 6);
         int y = v0 - 3 + r;
-        float val = G[r + PHALO - 3][c];
-        if (GAP && val != OUT && val < 0) val = gap_fill(&G[r + PHALO - 3][c], PT + 6, y, H, gap, val);
+        float val = G2[r + PHALO - 3][c];
+        if (GAP && val != OUT && val < 0) val = gap_fill(&G2[r + PHALO - 3][c], PT + 6, y, H, gap, val);
         V[r][c] = val;
     }
     __syncthreads();
-    // mean on [-1, 33)^2
+    // mean on [-1, 33)^2.  An invalid neighbour adds weight 0 (num and den
+    // unchanged, bit for bit), so the loop has no branch.  The weight table
+    // holds 1/(1 + (k/4)^2) for k < WT_SMEM, made by the same correctly
+    // rounded operations as the direct formula; k = 4|diff| is recovered
+    // without a float-to-int conversion: t = 4|diff| + 2^23 puts the
+    // integer part in the low mantissa bits, and t - 2^23 == 4|diff| holds
+    // exactly when 4|diff| is an integer below 2^23.
     for (int i = tid; i < (PT + 2) * (PT + 2); i += 1024) {
         int r = i / (PT + 2), c = i % (PT + 2);
         float dp = V[r + 2][c + 2];
         float out = dp;
         if (MEAN && dp >= 0) {
             float num = 0.0f, den = 0.0f;
+#pragma unroll
             for (int dy = -2; dy <= 2; ++dy)
+#pragma unroll
                 for (int dx = -2; dx <= 2; ++dx) {
-                    float dq = V[r + 2 + dy][c + 2 + dx];
-                    if (dq < 0) continue;
-                    float diff = __fsub_rn(dq, dp);
-                    // |diff| = k/4 for small k almost everywhere: the weight is then a
-                    // table entry made by the same correctly rounded operation
-                    float k4 = fabsf(diff) * 4.0f;
-                    int ki = int(k4);
-                    float w = (float(ki) == k4 && ki < WT_SMEM) ? WT[ki] : __frcp_rn(__fmaf_rn(diff, diff, 1.0f));
+                    const float dq = V[r + 2 + dy][c + 2 + dx];
+                    const float diff = __fsub_rn(dq, dp);
+                    const float k4 = dq >= 0 ? fabsf(diff) * 4.0f : 0.0f;   // invalid: any table entry
+                    const float t = __fadd_rn(k4, 8388608.0f);
+                    const int ki = __float_as_int(t) - 0x4B000000;
+                    float w;
+                    if (__fsub_rn(t, 8388608.0f) == k4 && ki < WT_SMEM) w = WT[ki];
+                    else w = __frcp_rn(__fmaf_rn(diff, diff, 1.0f));
+                    w = dq >= 0 ? w : 0.0f;
                     num = __fmaf_rn(w, dq, num);
                     den = __fadd_rn(den, w);
                 }
@@ -403,14 +415,23 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
     if (tile_gap || adaptive_mean || median) {
         dim3 grid((W + PT - 1) / PT, (H + PT - 1) / PT, nviews);
         const int key = (tile_gap ? 4 : 0) | (adaptive_mean ? 2 : 0) | (median ? 1 : 0);
-        switch (key) {
-        case 1: k_post_tile<false, false, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-        case 2: k_post_tile<false, true, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-        case 3: k_post_tile<false, true, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-        case 4: k_post_tile<true, false, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-        case 5: k_post_tile<true, false, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-        case 6: k_post_tile<true, true, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-        default: k_post_tile<true, true, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+        if (!tile_gap || gap <= 3) {   // halo 6
+            switch (key) {
+            case 1: k_post_tile<3, false, false, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+            case 2: k_post_tile<3, false, true, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+            case 3: k_post_tile<3, false, true, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+            case 4: k_post_tile<3, true, false, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+            case 5: k_post_tile<3, true, false, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+            case 6: k_post_tile<3, true, true, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+            default: k_post_tile<3, true, true, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+            }
+        } else {                       // gaps 4..8: halo 11
+            switch (key) {
+            case 4: k_post_tile<PGMAX, true, false, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+            case 5: k_post_tile<PGMAX, true, false, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+            case 6: k_post_tile<PGMAX, true, true, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+            default: k_post_tile<PGMAX, true, true, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+            }
         }
         flip();
         launched += 1;
