@@ -152,7 +152,11 @@ int elas_b200_process_batch_device(elas_handle* h, int n,
                                    const int32_t* dims, const int32_t* disp_max_per_pair,
                                    void* stream);
 
-/* Capture and replay batches as CUDA graphs (1, default) or run eagerly (0). */
+/* Capture and replay as CUDA graphs (1, default) or run eagerly (0): batches,
+ * and single pairs through elas_b200_process / _process_device, whose second
+ * call with the same buffers, size, parameters and settings is captured (on
+ * the handle's own stream) and whose later calls replay the graph.  A caller
+ * that is itself capturing a stream gets plain launches. */
 int elas_b200_set_graphs(elas_handle* h, int enable);
 
 /* Per-pair latency (ms from the batch's start to the pair's completion) of
