@@ -11,6 +11,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libelas_b200.so")
+CLI = os.path.join(HERE, "elas_b200_cli")
+CLI_SOURCES = [os.path.join(HERE, "cli", "elas_cli.cpp"), os.path.join(HERE, "cli", "pnm_io.h")]
 OBJ_DIR = os.path.join(HERE, "_build")
 
 CU_SOURCES = ["k_descriptor.cu", "k_support.cu", "k_delaunay.cu", "k_dense.cu", "k_post.cu", "k_proposal.cu",
@@ -48,6 +50,13 @@ def build(force=False, verbose=False, ptxas_info=False):
             subprocess.run(cmd, check=True)
     if force or _stale(OUT, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lgomp"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    # the command-line front end (host code linked against the library)
+    if force or _stale(CLI, CLI_SOURCES + [OUT, os.path.join(HERE, "..", "include", "elas_b200.h")]):
+        cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(HERE, "..", "include"), CLI_SOURCES[0], "-o", CLI,
+               "-L", HERE, "-lelas_b200", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -120,7 +120,6 @@ uint32_t next_pow2(size_t x) {
 }
 
 int check_params(const elas_params& p, std::string& why) {
-    if (p.subsampling) { why = "subsampling is not supported"; return ELAS_ERR_UNSUPPORTED; }
     if (p.candidate_stepsize < 1) { why = "candidate_stepsize must be >= 1"; return ELAS_ERR_INVALID_ARG; }
     if (p.grid_size < 1) { why = "grid_size must be >= 1"; return ELAS_ERR_INVALID_ARG; }
     if (p.disp_max < 1 || p.disp_max > 4095) { why = "disp_max must be in [1, 4095]"; return ELAS_ERR_INVALID_ARG; }
@@ -185,6 +184,11 @@ int prior_shift(const Geom& g, const DevParams& dp) {
     int need = g.D + dp.plane_radius + 2, b = 1;
     while ((1 << b) < need) ++b;
     return b;
+}
+
+// Pixels of one output map: W x H, or (W / 2) x (H / 2) when subsampling.
+size_t out_pixels(int W, int H, const elas_params& p) {
+    return p.subsampling ? size_t(W / 2) * (H / 2) : size_t(W) * H;
 }
 
 // Lay out (and, if `base` is non-null, assign) every workspace buffer.
@@ -319,7 +323,8 @@ constexpr int DENSE_SHAPES[4] = {128, 256, 512, 1024};
 
 int dense_threads_for(elas_handle* h, const Geom& g, const DevParams& dp, cudaStream_t st, int* nlaunch, int* out) {
     elas_handle* t = h->owner ? h->owner : h;
-    const std::pair<int, int> key((g.W + 127) / 128, g.D);
+    const int sub = h->params.subsampling ? 1 : 0;
+    const std::pair<int, int> key(((g.W >> sub) + 127) / 128, g.D);
     auto it = t->dense_threads.find(key);
     if (it != t->dense_threads.end()) { *out = it->second; return ELAS_OK; }
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -335,7 +340,7 @@ int dense_threads_for(elas_handle* h, const Geom& g, const DevParams& dp, cudaSt
         for (int rep = 0; rep < 3; ++rep) {
             CK(cudaEventRecord(e0, st));
             CK(launch_dense(h->desc0, h->desc1, h->prior0, h->prior1, h->grid0, h->grid1, h->raw0, h->raw1, g, dp,
-                            prior_shift(g, dp), h->err, st, shape));
+                            prior_shift(g, dp), h->err, st, shape, sub));
             CK(cudaEventRecord(e1, st));
             CK(cudaEventSynchronize(e1));
             float ms = 0;
@@ -464,15 +469,20 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     rc = dense_threads_for(h, g, dp, st, &n, &shape);
     if (rc != ELAS_OK) return rc;
     CK(mark(ELAS_TIME_DENSE));
+    // subsampling: dense, L/R and post-filters on every second row and column
+    const int sub = p.subsampling ? 1 : 0;
+    Geom go = g;
+    go.W = W >> sub;
+    go.H = H >> sub;
     CK(launch_dense(h->desc0, h->desc1, h->prior0, h->prior1, h->grid0, h->grid1, h->raw0, h->raw1, g, dp,
-                    prior_shift(g, dp), h->err, st, shape));
+                    prior_shift(g, dp), h->err, st, shape, sub));
     n += 1;
     CK(mark(ELAS_TIME_LR));
-    CK(launch_lr(h->raw0, h->raw1, h->lr0, h->lr1, g, p.lr_threshold, st));
+    CK(launch_lr(h->raw0, h->raw1, h->lr0, h->lr1, g, p.lr_threshold, st, sub));
     n += 1;
     CK(mark(ELAS_TIME_POST));
-    CK(cudaMemcpyAsync(out0, h->lr0, size_t(W) * H * 4, cudaMemcpyDeviceToDevice, st));
-    CK(cudaMemcpyAsync(out1, h->lr1, size_t(W) * H * 4, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(out0, h->lr0, size_t(go.W) * go.H * 4, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(out1, h->lr1, size_t(go.W) * go.H * 4, cudaMemcpyDeviceToDevice, st));
     PostViews pv;
     float* outs[2] = {out0, out1};
     for (int k = 0; k < 2; ++k) {
@@ -483,7 +493,7 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
         pv.root[k] = h->root[k];
         pv.sz[k] = h->usize[k];
     }
-    CK(launch_post(pv, p.postprocess_only_left ? 1 : 2, g, dp, p.filter_median, p.filter_adaptive_mean, h->err, st,
+    CK(launch_post(pv, p.postprocess_only_left ? 1 : 2, go, dp, p.filter_median, p.filter_adaptive_mean, h->err, st,
                    &n));
     CK(mark(ELAS_TIME_COUNT));
     h->launches += n;
@@ -620,8 +630,9 @@ int issue_batch(elas_handle* h, int n, const uint8_t* const* l, const uint8_t* c
         rc = run_pipeline(w, il, ir, o1, o2, W, H, ws);
         if (rc != ELAS_OK) return fail(h, rc, w->last_error);
         if (host) {
-            CK(cudaMemcpyAsync(d1[i], w->out0, px * 4, cudaMemcpyDeviceToHost, ws));
-            CK(cudaMemcpyAsync(d2[i], w->out1, px * 4, cudaMemcpyDeviceToHost, ws));
+            const size_t po = out_pixels(W, H, w->params);
+            CK(cudaMemcpyAsync(d1[i], w->out0, po * 4, cudaMemcpyDeviceToHost, ws));
+            CK(cudaMemcpyAsync(d2[i], w->out1, po * 4, cudaMemcpyDeviceToHost, ws));
         }
         CK(cudaEventRecordWithFlags(h->lat_done[i], ws, lat_flags));
         CK(cudaEventRecord(h->slot_done[i], ws));
@@ -851,8 +862,9 @@ int elas_b200_process(elas_handle* h, const uint8_t* left, const uint8_t* right,
     CK(cudaMemcpyAsync(h->img1, right, px, cudaMemcpyHostToDevice, st));
     rc = run_pipeline_graphed(h, h->img0, h->img1, h->out0, h->out1, W, H, st);
     if (rc != ELAS_OK) return rc;
-    CK(cudaMemcpyAsync(disp_left, h->out0, px * 4, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(disp_right, h->out1, px * 4, cudaMemcpyDeviceToHost, st));
+    const size_t po = out_pixels(W, H, h->params);
+    CK(cudaMemcpyAsync(disp_left, h->out0, po * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(disp_right, h->out1, po * 4, cudaMemcpyDeviceToHost, st));
     return check_device_errors(h, st);
 }
 
@@ -989,6 +1001,9 @@ int elas_b200_get_stage(elas_handle* h, int stage, void* dst, size_t bytes, size
         need = can_n * 4;
         break;
     case ELAS_STAGE_DEL_COUNTERS: need = 2 * 16 * 4; break;
+    case ELAS_STAGE_DISP_LEFT: case ELAS_STAGE_DISP_RIGHT: case ELAS_STAGE_LR_LEFT: case ELAS_STAGE_LR_RIGHT:
+        need = out_pixels(g.W, g.H, h->params) * 4;
+        break;
     default: need = px * 4; break;
     }
     if (needed) *needed = need;

@@ -200,16 +200,18 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
                                                const uint32_t* __restrict__ prior0, const uint32_t* __restrict__ prior1,
                                                const uint32_t* __restrict__ grid0, const uint32_t* __restrict__ grid1,
                                                float* __restrict__ disp0, float* __restrict__ disp1, Geom g,
-                                               DevParams p, int pshift, unsigned* err) {
+                                               DevParams p, int pshift, int sub, unsigned* err) {
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ uint64_t bar;
-    const int v = blockIdx.x;
+    // sub = 1: every second row and column (output (W/2) x (H/2))
+    const int v = int(blockIdx.x) << sub;
     const bool right = blockIdx.y != 0;
     const int W = g.W, H = g.H;
     const int tid = threadIdx.x, NT = blockDim.x;
-    float* disp = (right ? disp1 : disp0) + size_t(v) * W;
+    const int Wo = W >> sub;
+    float* disp = (right ? disp1 : disp0) + size_t(blockIdx.x) * Wo;
     if (!(v > 3 && v < H - 3)) {           // CTA-uniform: no copy is issued for these rows
-        for (int u = tid; u < W; u += NT) disp[u] = -1.0f;
+        for (int o = tid; o < Wo; o += NT) disp[o] = -1.0f;
         return;
     }
     uint4* row = reinterpret_cast<uint4*>(sm);
@@ -240,9 +242,9 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
         lcnt[c] = uint8_t(n > LMAX ? 255 : n);
     }
     // first pixel of this thread and its prefetch
-    int u = tid;
-    uint32_t pk_next = u < W ? prior[u] : 0u;
-    uint4 I_next = u < W ? self[u] : make_uint4(0, 0, 0, 0);
+    int o = tid, u = o << sub;
+    uint32_t pk_next = o < Wo ? prior[u] : 0u;
+    uint4 I_next = o < Wo ? self[u] : make_uint4(0, 0, 0, 0);
     __syncthreads();
     if (!mbar_wait_bounded(&bar, 0, MBAR_WAIT_LIMIT)) {
         if (tid == 0) atomicOr(err, ERRF_TMA_TIMEOUT);
@@ -255,14 +257,14 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
     const int gs = g.gs;
     // cell of u, advanced incrementally (u grows by NT per iteration)
     int cell = u / gs, rem = u - cell * gs;
-    const int cstep = NT / gs, rstep = NT - cstep * gs;
-    for (; u < W; u += NT) {
+    const int ustep = NT << sub;
+    const int cstep = ustep / gs, rstep = ustep - cstep * gs;
+    for (; o < Wo; o += NT, u += ustep) {
         const uint32_t pk = pk_next;
         const uint4 I1 = I_next;
         const int c = cell;
         {
-            const int un = u + NT;
-            if (un < W) { pk_next = prior[un]; I_next = self[un]; }
+            if (o + NT < Wo) { pk_next = prior[u + ustep]; I_next = self[u + ustep]; }
             cell += cstep;
             rem += rstep;
             if (rem >= gs) { rem -= gs; ++cell; }
@@ -331,20 +333,22 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
             }
             out = min_d >= 0 ? float(min_d) : -1.0f;
         }
-        disp[u] = out;
+        disp[o] = out;
     }
 }
 
 // kerLeftRightConsistencyCheck (src/Kernels/KerLeftRightConsistencyCheck.cu:7-64)
 // reading the dense results and writing separate outputs (the reference's
 // snapshot copies, src/Elas.cu:542-546).
+// scale = 0.5 on subsampled maps: a disparity (in full-resolution pixels)
+// moves d / 2 columns there.
 __global__ void k_lr(const float* __restrict__ D1, const float* __restrict__ D2, float* __restrict__ O1,
-                     float* __restrict__ O2, int W, int H, float thr) {
+                     float* __restrict__ O2, int W, int H, float thr, float scale) {
     int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
     if (u >= W || v >= H) return;
     size_t a = size_t(v) * W + u;
     float d1 = D1[a], d2 = D2[a];
-    float uw1 = float(u) - d1, uw2 = float(u) + d2;
+    float uw1 = float(u) - d1 * scale, uw2 = float(u) + d2 * scale;
     float o1 = d1, o2 = d2;
     if (d1 >= 0 && uw1 >= 0 && uw1 < W) {
         if (fabsf(D2[size_t(v) * W + int(uw1)] - d1) > thr) o1 = -1;
@@ -382,26 +386,27 @@ size_t dense_smem_bytes(const Geom& g) { return size_t(g.W) * 16 + size_t(g.gw) 
 
 cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t* prior0, const uint32_t* prior1,
                          const uint32_t* grid0, const uint32_t* grid1, float* disp0, float* disp1, const Geom& g,
-                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads) {
+                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads, int sub) {
     size_t smem = dense_smem_bytes(g);
     if (threads <= 0) threads = 512;
-    threads = imin(threads, ((g.W + 31) / 32) * 32);
-    const dim3 grid(g.H, 2);
+    threads = imin(threads, (((g.W >> sub) + 31) / 32) * 32);
+    const dim3 grid(g.H >> sub, 2);
     if (p.plane_radius == 2) {
         cudaFuncSetAttribute(k_dense<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         k_dense<2><<<grid, threads, smem, st>>>(desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
-                                                pshift, err);
+                                                pshift, sub, err);
     } else {
         cudaFuncSetAttribute(k_dense<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         k_dense<0><<<grid, threads, smem, st>>>(desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
-                                                pshift, err);
+                                                pshift, sub, err);
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_lr(const float* d0, const float* d1, float* o0, float* o1, const Geom& g, int lr_threshold,
-                      cudaStream_t st) {
-    k_lr<<<dim3((g.W + 255) / 256, g.H), 256, 0, st>>>(d0, d1, o0, o1, g.W, g.H, float(lr_threshold));
+                      cudaStream_t st, int sub) {
+    const int W = g.W >> sub, H = g.H >> sub;
+    k_lr<<<dim3((W + 255) / 256, H), 256, 0, st>>>(d0, d1, o0, o1, W, H, float(lr_threshold), sub ? 0.5f : 1.0f);
     return cudaGetLastError();
 }
 

@@ -423,9 +423,15 @@ cudaError_t launch_infer(const InferWeights& iw, const __nv_bfloat16* in, __nv_b
     const __nv_bfloat16* src[LAYERS] = {in, act0, act1, act0};
     __nv_bfloat16* dst[LAYERS] = {act0, act1, act0, out};
     const int tiles = 2 * Hd * ((Wd + TILE_M - 1) / TILE_M);
-    const int grid = imax(1, imin(tiles, num_sms));
     cudaError_t e = cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TC_SMEM));
     if (e != cudaSuccess) return e;
+    // persistent CTAs: as many per SM as shared memory allows (each holds its
+    // own 32-column accumulator), so one CTA's epilogue overlaps another's MMAs
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv_tc, TC_THREADS, TC_SMEM) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    const int grid = imax(1, imin(tiles, per_sm * num_sms));
     for (int l = 0; l < LAYERS; ++l) {
         CUtensorMap map;
         if (!make_act_map(&map, src[l], Hd, Wd)) return cudaErrorInvalidValue;

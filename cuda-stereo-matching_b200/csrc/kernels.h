@@ -72,10 +72,10 @@ size_t raster_bytes();
 size_t dense_smem_bytes(const Geom& g);
 cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t* prior0, const uint32_t* prior1,
                          const uint32_t* grid0, const uint32_t* grid1, float* disp0, float* disp1, const Geom& g,
-                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads);
+                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads, int sub = 0);
 
 cudaError_t launch_lr(const float* d0, const float* d1, float* o0, float* o1, const Geom& g, int lr_threshold,
-                      cudaStream_t st);
+                      cudaStream_t st, int sub = 0);
 
 // Buffers of the post-filter chain, per view: the filters ping-pong between
 // cur and nxt (the chain starts in cur; the result is copied to out if it

@@ -221,12 +221,18 @@ class Elas:
         if left.shape != right.shape or left.ndim != 2:
             raise ElasError(1, "images must be 2-D and of the same size")
         H, W = left.shape
-        d1 = np.empty((H, W), np.float32)
-        d2 = np.empty((H, W), np.float32)
+        shape = self.out_shape(W, H)
+        d1 = np.empty(shape, np.float32)
+        d2 = np.empty(shape, np.float32)
         dims = np.array([W, H, W], np.int32)
         self._check(self._lib.elas_b200_process(self._h, _ptr(left), _ptr(right), _ptr(d1), _ptr(d2), _ptr(dims),
                                                 stream))
         return d1, d2
+
+    def out_shape(self, width, height):
+        """(rows, columns) of the output maps: (H, W), or (H / 2, W / 2) when
+        the parameters ask for subsampling."""
+        return (height // 2, width // 2) if self.params.subsampling else (height, width)
 
     def process_device(self, left_ptr, right_ptr, d1_ptr, d2_ptr, width, height, stream=None):
         """Device-pointer form (ints); asynchronous on `stream` (a cudaStream_t int)."""
@@ -247,8 +253,8 @@ class Elas:
             keep += [l, r]
             dims[2 * i] = l.shape[1]
             dims[2 * i + 1] = l.shape[0]
-            outs1.append(np.empty(l.shape, np.float32))
-            outs2.append(np.empty(l.shape, np.float32))
+            outs1.append(np.empty(self.out_shape(l.shape[1], l.shape[0]), np.float32))
+            outs2.append(np.empty(self.out_shape(l.shape[1], l.shape[0]), np.float32))
         arr = lambda xs: (c_void_p * n)(*[x.ctypes.data for x in xs])
         dm = np.asarray(disp_max, np.int32) if disp_max is not None else None
         self._check(self._lib.elas_b200_process_batch(self._h, n, arr(keep[0::2]), arr(keep[1::2]), arr(outs1),

@@ -70,7 +70,10 @@ typedef struct elas_params {
     bool    filter_median;          /* 3x3 median filter */
     bool    filter_adaptive_mean;   /* edge-preserving adaptive mean filter */
     bool    postprocess_only_left;  /* post-filters on D1 only */
-    bool    subsampling;            /* not supported: returns ELAS_ERR_UNSUPPORTED */
+    bool    subsampling;            /* outputs at every second row and column: (W/2) x (H/2) maps
+                                     * (disparities in full-resolution pixels); L/R check and
+                                     * post-filters on the half-size maps.  The reference declares
+                                     * the field only (src/Elas.h:37-39); this is the project's mode */
 } elas_params;
 
 /* Defaults of the Elas::parameters constructor (reference src/Elas.h:42-66). */
@@ -107,7 +110,8 @@ const char* elas_b200_last_error(const elas_handle* h);
 /*
  * Drop-in for Elas::process (src/Elas.h:76-83, src/Elas.cu:19-120).
  *   left, right : host uint8 images, dims[0] x dims[1], row-major, stride dims[0]
- *   disp_left, disp_right : host float outputs of dims[0]*dims[1] values;
+ *   disp_left, disp_right : host float outputs of dims[0]*dims[1] values
+ *                 ((dims[0]/2)*(dims[1]/2) with subsampling, row stride dims[0]/2);
  *                 -1 marks an invalid pixel, as in the reference.
  *   dims        : only dims[0] (width) and dims[1] (height) are read
  *                 (the reference ignores a libelas-style dims[2]).

@@ -44,7 +44,8 @@ public:
     Elas& operator=(const Elas&) = delete;
 
     // Drop-in for Elas::process (src/Elas.h:76-83).  dims[0] = width,
-    // dims[1] = height; D1/D2 receive width*height floats, -1 = invalid.
+    // dims[1] = height; D1/D2 receive width*height floats ((width/2)*(height/2)
+    // with param.subsampling), -1 = invalid.
     void process(uint8_t* h_img0, uint8_t* h_img1, float* h_disp0, float* h_disp1, const int32_t* dims) {
         int rc = elas_b200_set_params(h_, &param);
         if (rc == ELAS_OK) rc = elas_b200_process(h_, h_img0, h_img1, h_disp0, h_disp1, dims, nullptr);

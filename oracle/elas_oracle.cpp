@@ -493,7 +493,10 @@ int orc_dense(const int32_t* grid, const uint8_t* desc0, const uint8_t* desc1, c
 // Left/right consistency: kerLeftRightConsistencyCheck
 // (src/Kernels/KerLeftRightConsistencyCheck.cu:7-64) against snapshot copies
 // (src/Elas.cu:542-546).
-int orc_lr(float* D1, float* D2, int W, int H, const elas_params* p) {
+// scale 0.5 on subsampled maps (the project's subsampling mode: a
+// disparity in full-resolution pixels moves d / 2 columns of the half-size
+// map).
+int orc_lr_scaled(float* D1, float* D2, int W, int H, const elas_params* p, float scale) {
     if (!D1 || !D2 || !p) return ELAS_ERR_INVALID_ARG;
     std::vector<float> c1(D1, D1 + size_t(W) * H), c2(D2, D2 + size_t(W) * H);
     const float thr = float(p->lr_threshold);
@@ -501,7 +504,7 @@ int orc_lr(float* D1, float* D2, int W, int H, const elas_params* p) {
         for (int u = 0; u < W; ++u) {
             size_t a = size_t(v) * W + u;
             float d1 = c1[a], d2 = c2[a];
-            float uw1 = float(u) - d1, uw2 = float(u) + d2;
+            float uw1 = float(u) - d1 * scale, uw2 = float(u) + d2 * scale;
             if (d1 >= 0 && uw1 >= 0 && uw1 < W) {
                 if (std::fabs(c2[size_t(v) * W + int32_t(uw1)] - d1) > thr) D1[a] = -1;
             } else {
@@ -515,6 +518,8 @@ int orc_lr(float* D1, float* D2, int W, int H, const elas_params* p) {
         }
     return ELAS_OK;
 }
+
+int orc_lr(float* D1, float* D2, int W, int H, const elas_params* p) { return orc_lr_scaled(D1, D2, W, H, p, 1.0f); }
 
 // ---------------------------------------------------------------------------
 // Post-filters.  The reference has none (its process() ends after the L/R
@@ -733,6 +738,20 @@ int orc_process(const uint8_t* L, const uint8_t* R, int W, int H, const elas_par
     orc_prior(can.data(), g.cw, g.step, uvd.data(), tr, ntr, 1, W, H, pr1.data());
     orc_dense(grid0.data(), d0.data(), d1.data(), pr0.data(), 0, W, H, &p, D1);
     orc_dense(grid1.data(), d0.data(), d1.data(), pr1.data(), 1, W, H, &p, D2);
+    // Subsampling (the project's own definition; the reference declares only
+    // the parameter, src/Elas.h:37-39): the maps keep every second row and
+    // column, (W / 2) x (H / 2), each value the full-resolution MAP
+    // disparity of pixel (2u, 2v); L/R check and post-filters then run on
+    // the half-size maps.  D1 / D2 then hold (W / 2) * (H / 2) values.
+    const int Wo = p.subsampling ? W / 2 : W, Ho = p.subsampling ? H / 2 : H;
+    const size_t No = size_t(Wo) * Ho;
+    if (p.subsampling) {
+        for (int v = 0; v < Ho; ++v)
+            for (int u = 0; u < Wo; ++u) {
+                D1[size_t(v) * Wo + u] = D1[size_t(2 * v) * W + 2 * u];
+                D2[size_t(v) * Wo + u] = D2[size_t(2 * v) * W + 2 * u];
+            }
+    }
     if (dumps) {
         if (dumps->desc_left) std::copy(d0.begin(), d0.end(), dumps->desc_left);
         if (dumps->desc_right) std::copy(d1.begin(), d1.end(), dumps->desc_right);
@@ -747,16 +766,16 @@ int orc_process(const uint8_t* L, const uint8_t* R, int W, int H, const elas_par
         if (dumps->tri_right && ntr <= dumps->tri_cap) std::copy(tr, tr + size_t(3) * ntr, dumps->tri_right);
         if (dumps->prior_left) std::copy(pr0.begin(), pr0.end(), dumps->prior_left);
         if (dumps->prior_right) std::copy(pr1.begin(), pr1.end(), dumps->prior_right);
-        if (dumps->disp_left) std::copy(D1, D1 + N, dumps->disp_left);
-        if (dumps->disp_right) std::copy(D2, D2 + N, dumps->disp_right);
+        if (dumps->disp_left) std::copy(D1, D1 + No, dumps->disp_left);
+        if (dumps->disp_right) std::copy(D2, D2 + No, dumps->disp_right);
     }
-    orc_lr(D1, D2, W, H, &p);
+    orc_lr_scaled(D1, D2, Wo, Ho, &p, p.subsampling ? 0.5f : 1.0f);
     if (dumps) {
-        if (dumps->lr_left) std::copy(D1, D1 + N, dumps->lr_left);
-        if (dumps->lr_right) std::copy(D2, D2 + N, dumps->lr_right);
+        if (dumps->lr_left) std::copy(D1, D1 + No, dumps->lr_left);
+        if (dumps->lr_right) std::copy(D2, D2 + No, dumps->lr_right);
     }
-    orc_postprocess(D1, W, H, &p);
-    if (!p.postprocess_only_left) orc_postprocess(D2, W, H, &p);
+    orc_postprocess(D1, Wo, Ho, &p);
+    if (!p.postprocess_only_left) orc_postprocess(D2, Wo, Ho, &p);
     return ELAS_OK;
 }
 

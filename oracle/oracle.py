@@ -194,6 +194,13 @@ def process(left, right, p, tri_left=None, tri_right=None, dumps=False, threads=
         st["support"] = st["support"][:st["n_support"][0]]
         st["tri_left"] = st["tri_left"][:st["n_tri_left"][0]]
         st["tri_right"] = st["tri_right"][:st["n_tri_right"][0]]
+    if p.subsampling:   # (H / 2) x (W / 2) maps in the leading values
+        Ho, Wo = H // 2, W // 2
+        D1 = D1.reshape(-1)[:Ho * Wo].reshape(Ho, Wo).copy()
+        D2 = D2.reshape(-1)[:Ho * Wo].reshape(Ho, Wo).copy()
+        if st is not None:
+            for k in ("disp_left", "disp_right", "lr_left", "lr_right"):
+                st[k] = st[k].reshape(-1)[:Ho * Wo].reshape(Ho, Wo).copy()
     return D1, D2, st
 
 

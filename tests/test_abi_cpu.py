@@ -69,9 +69,6 @@ def test_invalid_parameters_rejected_before_device_use():
     lib = eb.library()
     h = ctypes.c_void_p()
     p = eb.params_reference()
-    p.subsampling = True
-    assert lib.elas_b200_create(ctypes.byref(p), 0, ctypes.byref(h)) == 2
-    p = eb.params_reference()
     p.candidate_stepsize = 0
     assert lib.elas_b200_create(ctypes.byref(p), 0, ctypes.byref(h)) == 1
     p = eb.params_reference()

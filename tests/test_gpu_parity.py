@@ -39,8 +39,9 @@ def gpu_stages(e, W, H, p):
     st["tri_right"] = e.stage("tri_right").view(np.int32).reshape(-1, 3)
     for k in ("prior_left", "prior_right"):
         st[k] = e.stage(k).view(np.int32).reshape(H, W)
+    Ho, Wo = (H // 2, W // 2) if p.subsampling else (H, W)
     for k in ("disp_left", "disp_right", "lr_left", "lr_right"):
-        st[k] = e.stage(k).view(np.float32).reshape(H, W)
+        st[k] = e.stage(k).view(np.float32).reshape(Ho, Wo)
     return st
 
 
@@ -263,3 +264,64 @@ def test_batch_device_graph_replay_equals_singles(elas):
         elas.set_params(p)
     for (w, _, d) in shapes:
         assert elas.dense_shape(w, d) in (128, 256, 512, 1024)
+
+
+def _read_pfm(path):
+    with open(path, "rb") as f:
+        assert f.readline().strip() == b"Pf"
+        w, h = (int(x) for x in f.readline().split())
+        assert float(f.readline()) < 0
+        return np.frombuffer(f.read(), "<f4").reshape(h, w)[::-1]
+
+
+def test_cli_matches_library(tmp_path):
+    """The command-line front end on PGM files: its PFM output equals the
+    library's maps for the same pair and parameters, bit for bit; the demo
+    mode runs a synthetic pair and reports bad-2px."""
+    import os
+    import subprocess
+
+    cli = os.path.join(os.path.dirname(eb.LIB_PATH), "elas_b200_cli")
+    L, R, _, _ = eb.synth_pair(0, 7)
+    for path, img in ((tmp_path / "l.pgm", L), (tmp_path / "r.pgm", R)):
+        with open(path, "wb") as f:
+            f.write(b"P5\n%d %d\n255\n" % (img.shape[1], img.shape[0]))
+            f.write(img.tobytes())
+    out = subprocess.run([cli, str(tmp_path / "l.pgm"), str(tmp_path / "r.pgm"), "--out", str(tmp_path / "o"),
+                          "--disp-max", "63"], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    p = eb.params_default()
+    p.disp_max = 63
+    e = eb.Elas(p)
+    try:
+        D1, D2 = e.process(L, R)
+    finally:
+        e.close()
+    assert np.array_equal(_read_pfm(tmp_path / "o_left.pfm"), D1)
+    assert np.array_equal(_read_pfm(tmp_path / "o_right.pfm"), D2)
+    assert (tmp_path / "o_left.pgm").stat().st_size == L.size + len(b"P5\n450 375\n255\n")
+    out = subprocess.run([cli, "demo", "0", "--out", str(tmp_path / "demo")], capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "bad-2px" in out.stdout
+
+
+@pytest.mark.parametrize("preset,seed,D,size", [(0, 3, 63, None), (1, 4, 255, None), (3, 9, 31, (97, 61))])
+def test_subsampling_parity(elas, preset, seed, D, size):
+    """Subsampling (every second row and column, the project's mode for the
+    reference's declared-only parameter): stage-wise parity with the oracle,
+    and the half-size dense maps equal the full-resolution ones at even
+    pixels."""
+    kw = dict(width=size[0], height=size[1], disp_max=D) if size else {}
+    L, R, _, _ = eb.synth_pair(preset, seed, **kw)
+    H, W = L.shape
+    p = eb.params_config(D)
+    p.subsampling = True
+    D1, D2, g = run_and_compare(elas, L, R, p)
+    assert D1.shape == (H // 2, W // 2) and D2.shape == (H // 2, W // 2)
+    p.subsampling = False
+    elas.set_params(p)
+    elas.process(L, R)
+    for k in ("disp_left", "disp_right"):
+        full = elas.stage(k).view(np.float32).reshape(H, W)
+        assert np.array_equal(g[k], full[0:2 * (H // 2):2, 0:2 * (W // 2):2]), k

@@ -145,3 +145,28 @@ def test_triangle_known_answers():
     dup = np.array([[0, 0], [10, 0], [0, 10], [10, 0]], np.float32)
     t = oracle.triangulate_ref(dup)
     assert t.shape[0] == 1
+
+
+def test_subsampling_keeps_every_second_pixel():
+    """Subsampling in the oracle: the maps before the L/R check are the
+    full-resolution dense maps at even rows and columns; the L/R check and
+    the post-filters then run on the half-size maps."""
+    L, R, _, _ = eb.synth_pair(0, 5)
+    H, W = L.shape
+    p = eb.params_config(63)
+    _, _, full = oracle.process(L, R, p, dumps=True)
+    p.subsampling = True
+    D1, D2, sub = oracle.process(L, R, p, tri_left=full["tri_left"], tri_right=full["tri_right"], dumps=True)
+    assert D1.shape == (H // 2, W // 2) and D2.shape == (H // 2, W // 2)
+    assert np.array_equal(sub["disp_left"], full["disp_left"][0:2 * (H // 2):2, 0:2 * (W // 2):2])
+    assert np.array_equal(sub["disp_right"], full["disp_right"][0:2 * (H // 2):2, 0:2 * (W // 2):2])
+    # L/R on the half-size maps warps by d / 2
+    a, b = sub["disp_left"], sub["disp_right"]
+    exp = a.copy()
+    for v in range(a.shape[0]):
+        for u in range(a.shape[1]):
+            d = a[v, u]
+            uw = np.float32(u) - d * np.float32(0.5)
+            if not (d >= 0 and 0 <= uw < a.shape[1]) or abs(b[v, int(uw)] - d) > p.lr_threshold:
+                exp[v, u] = -1
+    assert np.array_equal(sub["lr_left"], exp)
