@@ -266,16 +266,21 @@ HD int outer_slot(int t, int n, int k) { return k < 2 ? 3 * t + k : 3 * n + (k -
 // flipped pair live now?  Its old reference o still holds if o's triangle
 // did not flip this round; otherwise the edge is one of the outer slots of
 // that triangle's new pair, found by matching the reversed edge.  Returns
-// the half-edge, -1 for the hull, or -2 if nothing matched (corrupt state).
+// the half-edge, -1 for the hull, or -2 if nothing matched or an index left
+// [0, T) (corrupt state).
 template <class M>
-HD int flip_resolve_slot(M& m, int x, uint32_t round) {
+HD int flip_resolve_slot(M& m, int x, uint32_t round, int T) {
     int o = m.opp(x);
     if (o < 0) return -1;
     int mt = o / 3;
+    if (mt >= T) return -2;
     if (m.fround(mt) != int32_t(round)) return o;
     int xt = x / 3, xk = x % 3;
     int a = m.v(xt, xk), b = m.v(xt, xk == 2 ? 0 : xk + 1);
-    int mt2 = (m.opp(3 * mt + 2) & ~FINAL) / 3;
+    const int o2 = m.opp(3 * mt + 2);
+    if (o2 < 0) return -2;
+    int mt2 = (o2 & ~FINAL) / 3;
+    if (mt2 >= T) return -2;
     const int cand_t[2] = {mt, mt2};
     for (int i = 0; i < 2; ++i)
         for (int k = 0; k < 2; ++k) {

@@ -200,8 +200,10 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         return p;
     };
     const size_t px = size_t(g.W) * g.H;
-    const size_t nmax = size_t(std::max(g.cw, 1)) * std::max(g.ch, 1);
-    const size_t rows = size_t(std::max(g.ch, 1));
+    // support points: the lattice plus six corner points (add_corners),
+    // rows: the lattice rows plus the corners' extra row
+    const size_t nmax = size_t(std::max(g.cw, 1)) * std::max(g.ch, 1) + 6;
+    const size_t rows = size_t(std::max(g.ch, 1)) + 1;
     const size_t tmax = 2 * nmax + 16;
     const size_t hmax = next_pow2(6 * tmax);
     const size_t cells = size_t(g.gw) * g.gh * g.words;
@@ -453,14 +455,15 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
                       h->pn_used ? h->pn_stats : nullptr));
     n += 4;
     CK(mark(ELAS_TIME_COMPACT));
-    CK(launch_compact(h->can, h->row_cnt, h->row_off, h->uvd, h->x0, h->x1, h->y, g, st));
-    n += 3;
+    const int corners = p.add_corners ? 1 : 0;
+    CK(launch_compact(h->can, h->row_cnt, h->row_off, h->uvd, h->x0, h->x1, h->y, g, st, corners));
+    n += 3 + corners;
     CK(mark(ELAS_TIME_GRID));
     CK(launch_grid(h->can, h->gtmp0, h->gtmp1, h->grid0, h->grid1, g, st));
     n += 2;
     CK(mark(ELAS_TIME_DELAUNAY));
-    CK(launch_delaunay(h->del[0], h->del[1], h->row_off, g.ch, g.cw * g.ch, h->num_sms, h->cluster_size, h->err,
-                       st, &n));
+    CK(launch_delaunay(h->del[0], h->del[1], h->row_off, g.ch + corners, g.cw * g.ch + 6 * corners, h->num_sms,
+                       h->cluster_size, h->err, st, &n));
     CK(mark(ELAS_TIME_PRIOR));
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
                     h->rast, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1, h->num_sms, st));
@@ -983,7 +986,7 @@ int elas_b200_get_stage(elas_handle* h, int stage, void* dst, size_t bytes, size
     case ELAS_STAGE_DESC_LEFT: case ELAS_STAGE_DESC_RIGHT: need = px * 16; break;
     case ELAS_STAGE_CAN_LR: case ELAS_STAGE_CAN: need = can_n * 4; break;
     case ELAS_STAGE_SUPPORT:
-        CK(cudaMemcpy(&nsup, h->row_off + g.ch, 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&nsup, h->row_off + g.ch + (h->params.add_corners ? 1 : 0), 4, cudaMemcpyDeviceToHost));
         need = size_t(nsup) * 12;
         break;
     case ELAS_STAGE_GRID_LEFT: case ELAS_STAGE_GRID_RIGHT: need = cells * (g.D + 2) * 4; break;

@@ -98,7 +98,9 @@ __global__ void __launch_bounds__(512) k_rowsort(DelDev d0, DelDev d1, const int
     int np = 1;
     while (np < n) np <<= 1;
     for (int i = threadIdx.x; i < np; i += blockDim.x)
-        key[i] = i < n ? (uint64_t(uint32_t(D.x[b + i])) << 32 | uint32_t(b + i)) : ~0ull;
+        // x with its sign bit flipped orders signed coordinates as unsigned keys
+        // (the right view's corner points of add_corners lie left of x = 0)
+        key[i] = i < n ? (uint64_t(uint32_t(D.x[b + i]) ^ 0x80000000u) << 32 | uint32_t(b + i)) : ~0ull;
     __syncthreads();
     for (int k = 2; k <= np; k <<= 1)
         for (int j = k >> 1; j > 0; j >>= 1) {
@@ -377,7 +379,7 @@ __global__ void __launch_bounds__(FLIP_THREADS) k_flip_global(DelDev d0, DelDev 
         for (int f = tid; f < nf; f += FLIP_THREADS) {
             int t = D.flips[6 * f], n = D.flips[6 * f + 1];
             for (int k = 0; k < 4; ++k) {
-                int r = flip_resolve_slot(m, outer_slot(t, n, k), uint32_t(round));
+                int r = flip_resolve_slot(m, outer_slot(t, n, k), uint32_t(round), T);
                 if (r == -2) { set_err(err, ERRF_BOUNDS); r = -1; }
                 D.flips[6 * f + 2 + k] = r;
             }
@@ -565,7 +567,7 @@ __global__ void __launch_bounds__(1024) k_flip_local(DelDev d0, DelDev d1, int m
             int32_t* q = flips.slot(f);
             int t = q[0], n = q[1];
             for (int k = 0; k < 4; ++k) {
-                int r = flip_resolve_slot(m, outer_slot(t, n, k), uint32_t(round));
+                int r = flip_resolve_slot(m, outer_slot(t, n, k), uint32_t(round), T);
                 if (r == -2) { set_err(err, ERRF_BOUNDS); r = -1; }
                 q[2 + k] = r;
             }
@@ -697,7 +699,7 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, 
         for (int f = tid; f < nf; f += CL_THREADS) {
             int t = flips[6 * f], n = flips[6 * f + 1];
             for (int k = 0; k < 4; ++k) {
-                int r = flip_resolve_slot(m, outer_slot(t, n, k), uint32_t(round));
+                int r = flip_resolve_slot(m, outer_slot(t, n, k), uint32_t(round), T);
                 if (r == -2) { set_err(err, ERRF_BOUNDS); r = -1; }
                 flips[6 * f + 2 + k] = r;
             }

@@ -77,7 +77,10 @@ __device__ void setup_triangle(const int32_t* tri, const int32_t* can, const int
         int c = tri[k];
         tu[k] = uvd[3 * c];
         tv[k] = uvd[3 * c + 1];
-        td[k] = can[(tv[k] * cw + tu[k]) / step];
+        // the point's own disparity: for a lattice point the value the
+        // reference reads at can[(v * cw + u) / step]; corner points
+        // (add_corners) have no lattice cell
+        td[k] = uvd[3 * c + 2];
     }
     double A[3][3], B[3];
     for (int k = 0; k < 3; ++k) {

@@ -610,7 +610,9 @@ __global__ void k_row_count(const int32_t* __restrict__ can, int32_t* __restrict
 }
 
 // Exclusive scan of the row counts (single block); row_off[ch] = total.
-__global__ void k_row_scan(const int32_t* __restrict__ row_cnt, int32_t* __restrict__ row_off, int n) {
+// corners: three corner points lead row 0 and three more form the extra
+// row ch (row_off[ch + 1] = total + 6).
+__global__ void k_row_scan(const int32_t* __restrict__ row_cnt, int32_t* __restrict__ row_off, int n, int corners) {
     __shared__ int part[1024];
     const int t = threadIdx.x;
     const int per = (n + blockDim.x - 1) / blockDim.x;
@@ -625,21 +627,25 @@ __global__ void k_row_scan(const int32_t* __restrict__ row_cnt, int32_t* __restr
         part[t] += x;
         __syncthreads();
     }
+    const int front = corners ? 3 : 0;
     int run = part[t] - s;
-    for (int i = b; i < e; ++i) { row_off[i] = run; run += row_cnt[i]; }
-    if (t == blockDim.x - 1) row_off[n] = part[t];
+    for (int i = b; i < e; ++i) { row_off[i] = run + (i > 0 ? front : 0); run += row_cnt[i]; }
+    if (t == blockDim.x - 1) {
+        row_off[n] = part[t] + front;
+        if (corners) row_off[n + 1] = part[t] + 6;
+    }
 }
 
 // Write the support list in raster order: uvd (u, v, d), and the point
 // coordinates of both views (x0 = u, x1 = u - d, y = v).
 __global__ void k_compact(const int32_t* __restrict__ can, const int32_t* __restrict__ row_off,
                           int32_t* __restrict__ uvd, int32_t* __restrict__ x0, int32_t* __restrict__ x1,
-                          int32_t* __restrict__ y, Geom g) {
+                          int32_t* __restrict__ y, Geom g, int lead) {
     __shared__ int warp_tot[32];
     __shared__ int base;
     const int r = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (threadIdx.x == 0) base = row_off[r];
+    if (threadIdx.x == 0) base = row_off[r] + (r == 0 ? lead : 0);
     __syncthreads();
     for (int x0c = 0; x0c < g.cw; x0c += blockDim.x) {
         int x = x0c + threadIdx.x;
@@ -658,6 +664,59 @@ __global__ void k_compact(const int32_t* __restrict__ can, const int32_t* __rest
         __syncthreads();
         if (threadIdx.x == 0) base += tot;
         __syncthreads();
+    }
+}
+
+// add_corners (the reference declares the parameter only, src/Elas.h:23):
+// support points at the image corners with the disparity of the nearest
+// support point (squared distance, the first one in list order on ties; 0
+// when there is none), and, for the right view, the two right corners moved
+// by their disparity (u = W - 1 + d, so that u - d = W - 1).  Layout: the
+// three points of row 0 -- (0, 0), (W-1, 0), (W-1+d, 0) -- lead the list,
+// the three of row H-1 -- (0, H-1), (W-1, H-1), (W-1+d, H-1) -- end it as
+// the extra row ch.  Every corner lies in a border cell of the grid, which
+// the grid leaves empty, so only the triangulations change.
+__global__ void __launch_bounds__(1024) k_corners(const int32_t* __restrict__ row_off, int32_t* __restrict__ uvd,
+                                                  int32_t* __restrict__ x0, int32_t* __restrict__ x1,
+                                                  int32_t* __restrict__ y, Geom g) {
+    __shared__ unsigned long long best[4][32];
+    const int n0 = 3, n1 = row_off[g.ch];          // regular points are [3, n1)
+    const int cu[4] = {0, g.W - 1, 0, g.W - 1}, cv[4] = {0, 0, g.H - 1, g.H - 1};
+    unsigned long long b[4] = {~0ull, ~0ull, ~0ull, ~0ull};
+    for (int i = n0 + threadIdx.x; i < n1; i += blockDim.x) {
+        const int u = uvd[3 * i], v = uvd[3 * i + 1];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const long long du = u - cu[k], dv = v - cv[k];
+            const unsigned long long key = (unsigned long long)(du * du + dv * dv) << 32 | unsigned(i);
+            b[k] = b[k] < key ? b[k] : key;
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long x = __shfl_xor_sync(0xffffffffu, b[k], o);
+            b[k] = b[k] < x ? b[k] : x;
+        }
+        if (lane == 0) best[k][warp] = b[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int d[4];
+        for (int k = 0; k < 4; ++k) {
+            unsigned long long m = ~0ull;
+            for (int w = 0; w < int(blockDim.x >> 5); ++w) m = best[k][w] < m ? best[k][w] : m;
+            d[k] = m == ~0ull ? 0 : uvd[3 * int(m & 0xffffffffu) + 2];
+        }
+        const int top[3][3] = {{0, 0, d[0]}, {g.W - 1, 0, d[1]}, {g.W - 1 + d[1], 0, d[1]}};
+        const int bot[3][3] = {{0, g.H - 1, d[2]}, {g.W - 1, g.H - 1, d[3]}, {g.W - 1 + d[3], g.H - 1, d[3]}};
+        for (int k = 0; k < 6; ++k) {
+            const int* q = k < 3 ? top[k] : bot[k - 3];
+            const int i = k < 3 ? k : n1 + (k - 3);
+            uvd[3 * i] = q[0]; uvd[3 * i + 1] = q[1]; uvd[3 * i + 2] = q[2];
+            x0[i] = q[0]; x1[i] = q[0] - q[2]; y[i] = q[1];
+        }
     }
 }
 
@@ -758,10 +817,11 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
 }
 
 cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_off, int32_t* uvd, int32_t* x0,
-                           int32_t* x1, int32_t* y, const Geom& g, cudaStream_t st) {
+                           int32_t* x1, int32_t* y, const Geom& g, cudaStream_t st, int corners) {
     k_row_count<<<g.ch, 128, 0, st>>>(can, row_cnt, g);
-    k_row_scan<<<1, 1024, 0, st>>>(row_cnt, row_off, g.ch);
-    k_compact<<<g.ch, 256, 0, st>>>(can, row_off, uvd, x0, x1, y, g);
+    k_row_scan<<<1, 1024, 0, st>>>(row_cnt, row_off, g.ch, corners);
+    k_compact<<<g.ch, 256, 0, st>>>(can, row_off, uvd, x0, x1, y, g, corners ? 3 : 0);
+    if (corners) k_corners<<<1, 1024, 0, st>>>(row_off, uvd, x0, x1, y, g);
     return cudaGetLastError();
 }
 

@@ -49,7 +49,7 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
                            cudaStream_t st, const uint32_t* bins = nullptr, int32_t* stats = nullptr);
 
 cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_off, int32_t* uvd, int32_t* x0,
-                           int32_t* x1, int32_t* y, const Geom& g, cudaStream_t st);
+                           int32_t* x1, int32_t* y, const Geom& g, cudaStream_t st, int corners = 0);
 
 cudaError_t launch_grid(const int32_t* can, uint32_t* tmp0, uint32_t* tmp1, uint32_t* grid0, uint32_t* grid1,
                         const Geom& g, cudaStream_t st);

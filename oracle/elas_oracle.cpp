@@ -376,7 +376,10 @@ int orc_prior(const int32_t* can, int cw, int step, const int32_t* uvd, const in
         for (int k = 0; k < 3; ++k) {
             tu[k] = uvd[3 * c[k]];
             tv[k] = uvd[3 * c[k] + 1];
-            td[k] = can[(tv[k] * cw + tu[k]) / step];   // KerComputeDisparity.cu:53-55
+            // KerComputeDisparity.cu:53-55 reads can[(v * cw + u) / step], the
+            // lattice point's disparity, which the list holds as well; corner
+            // points (add_corners) exist only in the list
+            td[k] = uvd[3 * c[k] + 2];
         }
         double A[3][3], B[3];
         for (int k = 0; k < 3; ++k) {
@@ -704,6 +707,34 @@ int orc_process(const uint8_t* L, const uint8_t* R, int W, int H, const elas_par
     int n = orc_support_list(can.data(), g.cw, g.ch, g.step, nullptr);
     std::vector<int32_t> uvd(size_t(3) * std::max(n, 1));
     orc_support_list(can.data(), g.cw, g.ch, g.step, uvd.data());
+    if (p.add_corners) {
+        // add_corners (declared only in the reference, src/Elas.h:23): the
+        // image corners with the disparity of the nearest support point
+        // (squared distance, first in list order on ties, 0 without any),
+        // plus the two right corners moved by their disparity for the right
+        // view.  Row 0's three points lead the list, row H-1's three end it.
+        const int cu[4] = {0, W - 1, 0, W - 1}, cv[4] = {0, 0, H - 1, H - 1};
+        int d[4] = {0, 0, 0, 0};
+        for (int k = 0; k < 4; ++k) {
+            long long best = -1;
+            for (int i = 0; i < n; ++i) {
+                const long long du = uvd[3 * i] - cu[k], dv = uvd[3 * i + 1] - cv[k];
+                const long long dist = du * du + dv * dv;
+                if (best < 0 || dist < best) { best = dist; d[k] = uvd[3 * i + 2]; }
+            }
+        }
+        std::vector<int32_t> full(size_t(3) * (n + 6));
+        const int top[3][3] = {{0, 0, d[0]}, {W - 1, 0, d[1]}, {W - 1 + d[1], 0, d[1]}};
+        const int bot[3][3] = {{0, H - 1, d[2]}, {W - 1, H - 1, d[3]}, {W - 1 + d[3], H - 1, d[3]}};
+        for (int k = 0; k < 3; ++k)
+            for (int j = 0; j < 3; ++j) {
+                full[3 * k + j] = top[k][j];
+                full[3 * (n + 3 + k) + j] = bot[k][j];
+            }
+        std::copy(uvd.begin(), uvd.begin() + size_t(3) * n, full.begin() + 9);
+        uvd.swap(full);
+        n += 6;
+    }
     std::vector<int32_t> grid0(size_t(g.gw) * g.gh * (g.D + 2)), grid1(grid0.size());
     orc_grid(can.data(), W, H, &p, grid0.data(), grid1.data());
 

@@ -168,10 +168,10 @@ def process(left, right, p, tri_left=None, tri_right=None, dumps=False, threads=
     st = None
     dp = None
     if dumps:
-        cap = 2 * cw * ch + 16
+        cap = 2 * (cw * ch + 6) + 16
         st = {"desc_left": np.empty((H, W, 16), np.uint8), "desc_right": np.empty((H, W, 16), np.uint8),
               "can_lr": np.empty((ch, cw), np.int32), "can": np.empty((ch, cw), np.int32),
-              "support": np.empty((cw * ch, 3), np.int32), "n_support": np.zeros(1, np.int32),
+              "support": np.empty((cw * ch + 6, 3), np.int32), "n_support": np.zeros(1, np.int32),
               "grid_left": np.empty((gh, gw, p.disp_max + 2), np.int32),
               "grid_right": np.empty((gh, gw, p.disp_max + 2), np.int32),
               "tri_left": np.empty((cap, 3), np.int32), "n_tri_left": np.zeros(1, np.int32),

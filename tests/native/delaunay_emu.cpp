@@ -119,7 +119,7 @@ extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const i
             }
         for (int f = 0; f < nf; ++f)
             for (int k = 0; k < 4; ++k) {
-                int r = flip_resolve_slot(m, outer_slot(flips[6 * f], flips[6 * f + 1], k), uint32_t(round));
+                int r = flip_resolve_slot(m, outer_slot(flips[6 * f], flips[6 * f + 1], k), uint32_t(round), T);
                 if (r == -2) return -1;
                 flips[6 * f + 2 + k] = r;
             }

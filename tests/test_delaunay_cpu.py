@@ -99,3 +99,19 @@ def test_random_large(emu_lib):
     rng = np.random.default_rng(9)
     xy, row_of = lattice_points(rng, 120, 150, 5, 0.3, jitter_d=40)
     check_case(emu_lib, xy, row_of)
+
+
+@pytest.mark.parametrize("preset", [0, 1])
+def test_support_points_with_corners(emu_lib, preset):
+    """The GPU algorithm with add_corners: the corner points of row 0 join
+    lattice row 0, those of row H-1 form one more row after the lattice."""
+    W, H, D = eb.synth_dims(preset)
+    L, R, _, _ = eb.synth_pair(preset, 2)
+    p = eb.params_config(D)
+    p.add_corners = True
+    _, _, st = oracle.process(L, R, p, dumps=True)
+    uvd = st["support"]
+    ch = H // p.candidate_stepsize
+    row_of = np.where(uvd[:, 1] == H - 1, ch, uvd[:, 1] // p.candidate_stepsize)
+    for right in (0, 1):
+        check_case(emu_lib, oracle.support_points(uvd, right), row_of)

@@ -325,3 +325,18 @@ def test_subsampling_parity(elas, preset, seed, D, size):
     for k in ("disp_left", "disp_right"):
         full = elas.stage(k).view(np.float32).reshape(H, W)
         assert np.array_equal(g[k], full[0:2 * (H // 2):2, 0:2 * (W // 2):2]), k
+
+
+@pytest.mark.parametrize("preset,seed,D", [(0, 11, 63), (1, 12, 255)])
+def test_add_corners_parity(elas, preset, seed, D):
+    """add_corners (the project's mode for the reference's declared-only
+    parameter): the framed support list, both triangulations (exact check
+    and Triangle), the priors and every later stage against the oracle."""
+    L, R, _, _ = eb.synth_pair(preset, seed)
+    H, W = L.shape
+    p = eb.params_config(D)
+    p.add_corners = True
+    D1, D2, g = run_and_compare(elas, L, R, p)
+    uvd = g["support"]
+    assert uvd[:3, :2].tolist() == [[0, 0], [W - 1, 0], [W - 1 + int(uvd[2, 2]), 0]]
+    assert uvd[-3:, 1].tolist() == [H - 1, H - 1, H - 1]

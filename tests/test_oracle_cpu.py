@@ -170,3 +170,28 @@ def test_subsampling_keeps_every_second_pixel():
             if not (d >= 0 and 0 <= uw < a.shape[1]) or abs(b[v, int(uw)] - d) > p.lr_threshold:
                 exp[v, u] = -1
     assert np.array_equal(sub["lr_left"], exp)
+
+
+def test_add_corners_support_list():
+    """add_corners in the oracle: the regular list is framed by the corner
+    points (row 0's three first, row H-1's three last) with the disparity of
+    the nearest support point, the right corners also moved by it.  (The
+    triangulation of the framed list is checked on the GPU algorithm's
+    emulation in test_delaunay_cpu.py.)"""
+    L, R, _, _ = eb.synth_pair(0, 6)
+    H, W = L.shape
+    p = eb.params_config(63)
+    _, _, a = oracle.process(L, R, p, dumps=True)
+    p.add_corners = True
+    _, _, b = oracle.process(L, R, p, dumps=True)
+    reg, sb = a["support"], b["support"]
+    assert len(sb) == len(reg) + 6
+    assert np.array_equal(sb[3:-3], reg)
+
+    def nearest(u, v):
+        dist = (reg[:, 0].astype(np.int64) - u) ** 2 + (reg[:, 1].astype(np.int64) - v) ** 2
+        return int(reg[np.argmin(dist), 2])          # argmin: the first minimum in list order
+
+    d = [nearest(0, 0), nearest(W - 1, 0), nearest(0, H - 1), nearest(W - 1, H - 1)]
+    assert sb[:3].tolist() == [[0, 0, d[0]], [W - 1, 0, d[1]], [W - 1 + d[1], 0, d[1]]]
+    assert sb[-3:].tolist() == [[0, H - 1, d[2]], [W - 1, H - 1, d[3]], [W - 1 + d[3], H - 1, d[3]]]
