@@ -237,6 +237,39 @@ def cpu_baseline(L, R, p, budget_s=12.0):
                       f"(C++ restatement of the reference kernels + the reference's Triangle), {threads} threads"}
 
 
+def reference_gpu(L, R, runs=5):
+    """The reference's own Elas::process -- its CUDA kernels built for
+    sm_100a from the reference tree into oracle/_ref, host buffers, its
+    per-call allocations and CPU Triangle -- timed on the same GPU: a
+    comparator beside the CPU baseline, not the target.  Its kernels are
+    compiled with the disparity range 0-255 (KernelsCommon.h)."""
+    import ctypes
+
+    import oracle
+
+    if not oracle.have_ref_elas():
+        return {"unavailable": "the reference pipeline was not built (oracle/_ref/libelasref.so)"}
+    libc = ctypes.CDLL(None)
+    sys.stdout.flush()
+    saved, devnull = os.dup(1), os.open(os.devnull, os.O_WRONLY)
+    ts = []
+    try:
+        os.dup2(devnull, 1)              # the reference prints a per-stage profile to stdout
+        oracle.ref_elas_process(L, R)
+        for _ in range(runs):
+            t0 = time.perf_counter()
+            oracle.ref_elas_process(L, R)
+            ts.append(time.perf_counter() - t0)
+    finally:
+        libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
+    ms = 1e3 * statistics.median(ts)
+    return {"value": 1e3 / ms, "unit": "pairs/s", "ms_per_pair": ms, "runs": runs,
+            "what": "reference Elas::process built for sm_100a, host buffers, median of the runs"}
+
+
 def run_ours(args):
     import torch
 
@@ -292,6 +325,8 @@ def run_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(L, R, p, args.cpu_seconds)
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        out["reference_gpu"] = reference_gpu(L, R)
     if rank == 0 and world == 1 and not args.no_large:
         out["large"] = run_large(torch, args, flush, stream, hbm, peak_kind)
     if rank == 0 and world == 1 and not args.no_batch:
@@ -320,7 +355,9 @@ def run_large(torch, args, flush, stream, hbm, peak_kind):
     e.close()
     dense_bytes = 80.0 * W * H
     v = steps / (total_ms / 1e3)
+    ref = reference_gpu(L, R) if not args.no_ref_gpu else None
     return {"workload": "elas_pair_2880x1988_disp0-511", "steps": steps, "value": v, "unit": "pairs/s",
+            "reference_gpu_disp0-255": ref,
             "ms_per_step": total_ms / steps, "gpix_disp_per_s": v * W * H * (D + 1) / 1e9, "stages_ms": stage_ms,
             "roofline_dense": {"achieved": dense_bytes / (stage_ms["dense"] / 1e3) / 1e9, "peak": hbm,
                                "unit": "GB/s", "frac": dense_bytes / (stage_ms["dense"] / 1e3) / 1e9 / hbm,
@@ -452,14 +489,15 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--only", choices=["large", "batch"], default=None,
                     help="run one secondary workload alone (for profiling) and print its block")
     args = ap.parse_args()

@@ -3,8 +3,13 @@
 * oracle/liboracle.so      -- the CPU restatement in elas_oracle.cpp
 * oracle/_ref/libreftriangle.so -- the reference's own Triangle
   (src/triangle.cpp) compiled from the reference tree, with the C shim
-  tri_ref_shim.cpp.  Built only where the reference tree is present; the
-  prebuilt file travels with the repository snapshot.
+  tri_ref_shim.cpp.
+* oracle/_ref/libelasref.so -- the reference's own GPU pipeline
+  (src/Elas.cu, src/Kernels/*.cu, src/triangle.cpp, unmodified, with the
+  CPU Triangle path its default build takes) compiled for sm_100a with the C
+  shim ref_elas_shim.cu.
+The _ref libraries are built only where the reference tree is present; the
+prebuilt files travel with the repository snapshot.
 """
 import os
 import subprocess
@@ -41,7 +46,26 @@ def build_ref(force=False):
     return out
 
 
+def build_ref_elas(force=False):
+    out_dir = os.path.join(HERE, "_ref")
+    out = os.path.join(out_dir, "libelasref.so")
+    elas = os.path.join(REF_SRC, "Elas.cu")
+    if not os.path.exists(elas):
+        return out if os.path.exists(out) else None
+    os.makedirs(out_dir, exist_ok=True)
+    shim = os.path.join(HERE, "ref_elas_shim.cu")
+    if force or not os.path.exists(out) or os.path.getmtime(out) < os.path.getmtime(shim):
+        kernels = [os.path.join(REF_SRC, "Kernels", k) for k in
+                   ("KerComputeDisparity.cu", "KerDescriptor.cu", "KerGrid.cu", "KerLeftRightConsistencyCheck.cu",
+                    "KerSupportMatches.cu")]
+        _run([os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc"), "-gencode", "arch=compute_100a,code=sm_100a",
+              "-O2", "-std=c++14", "-Xcompiler", "-fPIC", "-shared", "-w", "-DREAL_TYPE_FP32", "-I" + REF_SRC,
+              elas] + kernels + [os.path.join(REF_SRC, "triangle.cpp"), shim, "-o", out])
+    return out
+
+
 if __name__ == "__main__":
     force = "--force" in sys.argv
     print(build_oracle(force))
     print(build_ref(force))
+    print(build_ref_elas(force))

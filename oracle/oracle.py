@@ -19,6 +19,7 @@ from elas_b200 import ElasParams  # noqa: E402  (pure ctypes struct, does not lo
 
 LIB = os.path.join(HERE, "liboracle.so")
 REF_TRI = os.path.join(HERE, "_ref", "libreftriangle.so")
+REF_ELAS = os.path.join(HERE, "_ref", "libelasref.so")
 
 
 class Dumps(ctypes.Structure):
@@ -50,6 +51,32 @@ def lib():
 
 def have_triangle():
     return os.path.exists(REF_TRI)
+
+
+_ref_elas = None
+
+
+def have_ref_elas():
+    return os.path.exists(REF_ELAS)
+
+
+def ref_elas_process(left, right):
+    """The reference's own GPU pipeline (Elas::process built from the
+    reference tree; needs a GPU).  Its kernels use the compile-time
+    constants of src/Kernels/KernelsCommon.h and it stops after the L/R
+    check.  Returns (D1, D2) float32."""
+    global _ref_elas
+    if _ref_elas is None:
+        _ref_elas = ctypes.CDLL(REF_ELAS)
+    left = np.ascontiguousarray(left, np.uint8)
+    right = np.ascontiguousarray(right, np.uint8)
+    H, W = left.shape
+    D1 = np.empty((H, W), np.float32)
+    D2 = np.empty((H, W), np.float32)
+    rc = _ref_elas.ref_elas_process(P(left), P(right), P(D1), P(D2), W, H)
+    if rc != 0:
+        raise RuntimeError(f"reference pipeline failed with status {rc}")
+    return D1, D2
 
 
 def P(a):
