@@ -39,39 +39,6 @@ __device__ __forceinline__ int uf_find(int32_t* lab, int x, unsigned* err) {
     return x;
 }
 
-// Labels start as stars over the runs of each row: every pixel points at the
-// first pixel of its connected run (one warp per row, ballot scan over
-// 32-pixel chunks).  Only vertical unions remain for k_uf_union_v.
-__global__ void k_uf_init_rows(PostViews pv, int W, int H, float thr) {
-    const int view = blockIdx.z;
-    const float* D = pv.cur[view];
-    int32_t* lab = pv.lab[view];
-    int32_t* sz = pv.sz[view];
-    const int lane = threadIdx.x & 31;
-    const int v = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (v >= H) return;
-    int carry = -1;
-    float prev = -1.0f;
-    for (int u0 = 0; u0 < W; u0 += 32) {
-        const int u = u0 + lane;
-        const size_t i = size_t(v) * W + u;
-        float d = u < W ? D[i] : -1.0f;
-        float dl = __shfl_up_sync(0xffffffffu, d, 1);
-        if (lane == 0) dl = prev;
-        const bool valid = d >= 0;
-        const bool conn = valid && u > 0 && dl >= 0 && fabsf(d - dl) <= thr;
-        const unsigned starts = __ballot_sync(0xffffffffu, valid && !conn);
-        const unsigned mine = starts & (0xffffffffu >> (31 - lane));
-        const int rs = mine ? int(size_t(v) * W + u0 + 31 - __clz(mine)) : carry;
-        if (u < W) {
-            lab[i] = valid ? rs : -1;
-            sz[i] = 0;
-        }
-        carry = __shfl_sync(0xffffffffu, rs, 31);
-        prev = __shfl_sync(0xffffffffu, d, 31);
-    }
-}
-
 // Labels start at the left neighbour when it is connected (the most common
 // union), else at the pixel itself.
 __global__ void k_uf_init(const float* __restrict__ D, int32_t* __restrict__ lab, int32_t* __restrict__ sz, int W,
@@ -107,26 +74,6 @@ __device__ void uf_union(int32_t* lab, int a, int b, unsigned* err) {
     atomicOr(err, ERRF_BOUNDS);
 }
 
-__global__ void k_uf_union_v(PostViews pv, int W, int H, float thr, unsigned* err) {
-    const int view = blockIdx.z;
-    const float* D = pv.cur[view];
-    int32_t* lab = pv.lab[view];
-    int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
-    if (u >= W || v + 1 >= H) return;
-    int i = v * W + u;
-    float d = D[i];
-    if (d < 0) return;
-    float q = D[i + W];
-    if (!(q >= 0 && fabsf(q - d) <= thr)) return;
-    // the two row runs were already joined one column to the left when that
-    // column links them too (both pixels belong to the same runs)
-    if (u > 0) {
-        float dl = D[i - 1], ql = D[i + W - 1];
-        if (dl >= 0 && ql >= 0 && fabsf(dl - d) <= thr && fabsf(ql - q) <= thr && fabsf(ql - dl) <= thr) return;
-    }
-    uf_union(lab, i, i + W, err);
-}
-
 __global__ void k_uf_union(const float* __restrict__ D, int32_t* lab, int W, int H, float thr, unsigned* err) {
     int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
     if (u >= W || v >= H) return;
@@ -157,62 +104,153 @@ __global__ void k_uf_count(int32_t* lab, int32_t* __restrict__ root, int32_t* sz
     if (r >= 0 && (threadIdx.x & 31) == leader) atomicAdd(&sz[r], __popc(peers));
 }
 
-// Roots and segment sizes.  Warps merge equal roots with match_any, then a
-// small per-block table merges them again, so a large segment costs one
-// global atomic per block instead of one per pixel.
-constexpr int CNT_SLOTS = 128;
-__global__ void __launch_bounds__(1024) k_uf_count_v(PostViews pv, int n, unsigned* err) {
-    __shared__ int keys[CNT_SLOTS], vals[CNT_SLOTS];
+// ---------------------------------------------------------------------------
+// Speckle segmentation in tiles.  The segments (4-connected valid pixels,
+// |d_p - d_q| <= thr) are labelled first inside every 32x32 tile with a
+// union-find in shared memory; only links across tile borders then go
+// through the global union-find, and sizes are counted once per tile-local
+// component.  The segments, hence the result, are those of a whole-image
+// union-find.
+//   lab[i]  the global index of i's tile-local root (-1 invalid); the local
+//           roots are the nodes of the global forest
+//   sz[i]   the pixel count of i's tile component if i is its local root, else 0;
+//           after the count, -(global root + 1) at every local root
+//   acc[g]  the segment size at global root g (zeroed by the tile kernel)
+constexpr int SPK_T = 32;
+
+__device__ __forceinline__ int lfind(int* L, int x) {
+    for (int it = 0; it < SPK_T * SPK_T; ++it) {
+        const int p = L[x];
+        if (p == x) return x;
+        const int gp = L[p];
+        if (gp != p) L[x] = gp;
+        x = p;
+    }
+    return x;
+}
+__device__ __forceinline__ void lunion(int* L, int a, int b) {
+    for (int it = 0; it < SPK_T * SPK_T; ++it) {
+        int ra = lfind(L, a), rb = lfind(L, b);
+        if (ra == rb) return;
+        if (ra < rb) { int t = ra; ra = rb; rb = t; t = a; a = b; b = t; }
+        const int old = atomicCAS(&L[ra], ra, rb);
+        if (old == ra) return;
+        a = old;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_spk_tile(PostViews pv, int W, int H, float thr) {
+    __shared__ float S[SPK_T][SPK_T];
+    __shared__ int L[SPK_T * SPK_T];
+    __shared__ int C[SPK_T * SPK_T];
+    const int view = blockIdx.z;
+    const float* __restrict__ D = pv.cur[view];
+    const int tx = threadIdx.x, ty = threadIdx.y, t = ty * SPK_T + tx;   // a warp per tile row
+    const int x = blockIdx.x * SPK_T + tx, y = blockIdx.y * SPK_T + ty;
+    const bool in = x < W && y < H;
+    const float d = in ? D[size_t(y) * W + x] : -1.0f;
+    const bool valid = d >= 0;
+    S[ty][tx] = d;
+    C[t] = 0;
+    // runs of the row: every pixel points at the first pixel of its run
+    const float dl = __shfl_up_sync(0xffffffffu, d, 1);
+    const bool conn_l = valid && tx > 0 && dl >= 0 && fabsf(d - dl) <= thr;
+    const unsigned starts = __ballot_sync(0xffffffffu, valid && !conn_l);
+    const unsigned mine = starts & (0xffffffffu >> (31 - tx));
+    L[t] = valid ? ty * SPK_T + (31 - __clz(mine)) : t;
+    __syncthreads();
+    // vertical links; a link is implied when the left neighbours make the same one
+    if (valid && ty + 1 < SPK_T) {
+        const float q = S[ty + 1][tx];
+        if (q >= 0 && fabsf(q - d) <= thr) {
+            bool implied = false;
+            if (tx > 0) {
+                const float ql = S[ty + 1][tx - 1];
+                implied = conn_l && ql >= 0 && fabsf(ql - q) <= thr && fabsf(ql - dl) <= thr;
+            }
+            if (!implied) lunion(L, t, t + SPK_T);
+        }
+    }
+    __syncthreads();
+    const int r = valid ? lfind(L, t) : -1;
+    {   // component sizes, one shared atomic per group of lanes with the same root
+        const unsigned peers = __match_any_sync(0xffffffffu, r);
+        if (r >= 0 && tx == __ffs(peers) - 1) atomicAdd(&C[r], __popc(peers));
+    }
+    __syncthreads();
+    if (in) {
+        const size_t i = size_t(y) * W + x;
+        const int rx = blockIdx.x * SPK_T + (r & (SPK_T - 1)), ry = blockIdx.y * SPK_T + (r / SPK_T);
+        pv.lab[view][i] = r >= 0 ? int(size_t(ry) * W + rx) : -1;
+        pv.sz[view][i] = (r == t) ? C[t] : 0;
+        pv.root[view][i] = 0;
+    }
+}
+
+// Links across tile borders: item k < H * tx_n is the right border of tile
+// column k % tx_n in row k / tx_n; the rest are bottom borders.
+__global__ void k_spk_border(PostViews pv, int W, int H, float thr, unsigned* err) {
+    const int view = blockIdx.z;
+    const float* __restrict__ D = pv.cur[view];
+    int32_t* lab = pv.lab[view];
+    const int txn = (W + SPK_T - 1) / SPK_T, tyn = (H + SPK_T - 1) / SPK_T;
+    const long long nr = (long long)H * (txn - 1), nb = (long long)W * (tyn - 1);
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nr + nb;
+         k += (long long)gridDim.x * blockDim.x) {
+        int x, y, x2, y2;
+        if (k < nr) {
+            y = int(k / (txn - 1));
+            x = int(k % (txn - 1)) * SPK_T + SPK_T - 1;
+            x2 = x + 1; y2 = y;
+        } else {
+            const long long kb = k - nr;
+            x = int(kb % W);
+            y = int(kb / W) * SPK_T + SPK_T - 1;
+            x2 = x; y2 = y + 1;
+        }
+        const size_t i = size_t(y) * W + x, j = size_t(y2) * W + x2;
+        const float d = D[i], q = D[j];
+        if (d >= 0 && q >= 0 && fabsf(q - d) <= thr) uf_union(lab, lab[i], lab[j], err);
+    }
+}
+
+// Sizes: every tile-local root adds its count at its global root g and
+// keeps -(g + 1) in its size slot (only this thread reads that slot).
+__global__ void k_spk_count(PostViews pv, int n, unsigned* err) {
     const int view = blockIdx.z;
     int32_t* lab = pv.lab[view];
-    int32_t* root = pv.root[view];
     int32_t* sz = pv.sz[view];
-    for (int k = threadIdx.x; k < CNT_SLOTS; k += blockDim.x) { keys[k] = -1; vals[k] = 0; }
-    __syncthreads();
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int r = -1;
-    if (i < n && lab[i] >= 0) r = uf_find(lab, i, err);
-    if (i < n) root[i] = r;
-    unsigned peers = __match_any_sync(0xffffffffu, r);
-    int leader = __ffs(peers) - 1;
-    if (r >= 0 && (threadIdx.x & 31) == leader) {
-        int c = __popc(peers);
-        int slot = int((unsigned(r) * 2654435761u) >> 25) & (CNT_SLOTS - 1);
-        bool done = false;
-        for (int probe = 0; probe < 8 && !done; ++probe, slot = (slot + 1) & (CNT_SLOTS - 1)) {
-            int prev = atomicCAS(&keys[slot], -1, r);
-            if (prev == -1 || prev == r) { atomicAdd(&vals[slot], c); done = true; }
+    int32_t* acc = pv.root[view];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int c = sz[i];
+        if (c > 0) {
+            const int g = uf_find(lab, i, err);
+            atomicAdd(&acc[g], c);
+            sz[i] = -(g + 1);
         }
-        if (!done) atomicAdd(&sz[r], c);
     }
-    __syncthreads();
-    for (int k = threadIdx.x; k < CNT_SLOTS; k += blockDim.x)
-        if (keys[k] >= 0) atomicAdd(&sz[keys[k]], vals[k]);
 }
 
-// out = in with the pixels of small segments set invalid.
-// Four pixels per thread, their loads issued together.
-__global__ void k_uf_apply_v(PostViews pv, int n, int min_size) {
+// out = in with the pixels of segments smaller than min_size set invalid:
+// a pixel's tile-local root (itself, or lab[i]) holds -(global root + 1).
+__global__ void k_spk_apply(PostViews pv, int n, int min_size) {
     const int view = blockIdx.z;
-    const float* D = pv.cur[view];
-    float* O = pv.nxt[view];
-    const int32_t* root = pv.root[view];
-    const int32_t* sz = pv.sz[view];
-    const int i0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
-    int r[4], s4[4];
-    float d[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        r[k] = i0 + k < n ? root[i0 + k] : -1;
-        d[k] = i0 + k < n ? D[i0 + k] : 0.0f;
+    const float* __restrict__ D = pv.cur[view];
+    float* __restrict__ O = pv.nxt[view];
+    const int32_t* __restrict__ lab = pv.lab[view];
+    const int32_t* __restrict__ sz = pv.sz[view];
+    const int32_t* __restrict__ acc = pv.root[view];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float d = D[i];
+        float o = d;
+        if (d >= 0) {
+            int m = sz[i];
+            if (m >= 0) m = sz[lab[i]];
+            if (acc[-m - 1] < min_size) o = -1.0f;
+        }
+        O[i] = o;
     }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) s4[k] = r[k] >= 0 ? sz[r[k]] : min_size;
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-        if (i0 + k < n) O[i0 + k] = s4[k] < min_size ? -1.0f : d[k];
 }
-
 
 __global__ void k_uf_apply(float* D, const int32_t* __restrict__ root, const int32_t* sz, int n, int min_size) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -390,18 +428,19 @@ __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, 
 cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams& p, bool median,
                         bool adaptive_mean, unsigned* err, cudaStream_t st, int* nlaunch) {
     const int W = g.W, H = g.H, n = W * H;
-    const int tb = 256;
     int launched = 0;
-    const dim3 grid2((W + tb - 1) / tb, H, nviews);
     auto flip = [&]() {
         for (int k = 0; k < 2; ++k) { float* t = pv.cur[k]; pv.cur[k] = pv.nxt[k]; pv.nxt[k] = t; }
     };
     if (p.speckle_size > 0) {
-        const int wpb = 8;
-        k_uf_init_rows<<<dim3((H + wpb - 1) / wpb, 1, nviews), 32 * wpb, 0, st>>>(pv, W, H, p.speckle_sim_threshold);
-        k_uf_union_v<<<grid2, tb, 0, st>>>(pv, W, H, p.speckle_sim_threshold, err);
-        k_uf_count_v<<<dim3((n + 1023) / 1024, 1, nviews), 1024, 0, st>>>(pv, n, err);
-        k_uf_apply_v<<<dim3((n + 4 * tb - 1) / (4 * tb), 1, nviews), tb, 0, st>>>(pv, n, p.speckle_size);
+        const dim3 tiles((W + SPK_T - 1) / SPK_T, (H + SPK_T - 1) / SPK_T, nviews);
+        k_spk_tile<<<tiles, dim3(SPK_T, SPK_T), 0, st>>>(pv, W, H, p.speckle_sim_threshold);
+        const long long border = (long long)H * (tiles.x - 1) + (long long)W * (tiles.y - 1);
+        const int gb = int(border / 256 + 1 < 4096 ? border / 256 + 1 : 4096);
+        k_spk_border<<<dim3(gb, 1, nviews), 256, 0, st>>>(pv, W, H, p.speckle_sim_threshold, err);
+        const int gn = imax(1, imin(8 * 1024, (n + 255) / 256));
+        k_spk_count<<<dim3(gn, 1, nviews), 256, 0, st>>>(pv, n, err);
+        k_spk_apply<<<dim3(gn, 1, nviews), 256, 0, st>>>(pv, n, p.speckle_size);
         flip();
         launched += 4;
     }
