@@ -111,17 +111,21 @@ HD int strip_tri_lower(Pts P, const int32_t* A, int m, const int32_t* B, int k, 
 // Fill the pocket between a boundary chain (one point per non-empty row,
 // top to bottom: point index ci[k] at (cx[k], cy[k])) and its convex hull.
 // side = +1 for the left chain (first points), -1 for the right chain
-// (last points).  `stack` (chain positions) has room for `len` entries.
-// Returns the number of counter-clockwise triangles written.
+// (last points).  `stack` has room for 4 * len ints: an entry is the
+// record (point index, x, y, -) of a chain point, so a pop reads one
+// 16-byte record.  The next chain point is loaded one step ahead.  Returns
+// the number of counter-clockwise triangles written.
 HD int fill_pockets(const int32_t* ci, const int32_t* cx, const int32_t* cy, int len, int side, int32_t* stack,
                     int32_t* tri) {
     // the two top stack entries are kept in registers: (a, b) = stack[sp-2], stack[sp-1]
     int sp = 0, k = 0;
     int32_t ia = 0, ib = 0;
     int64_t ax = 0, ay = 0, bx = 0, by = 0;
+    int32_t nx = len > 0 ? cx[0] : 0, ny = len > 0 ? cy[0] : 0, ni = len > 0 ? ci[0] : 0;
     for (int i = 0; i < len; ++i) {
-        const int64_t x = cx[i], y = cy[i];
-        const int32_t ii = ci[i];
+        const int64_t x = nx, y = ny;
+        const int32_t ii = ni;
+        if (i + 1 < len) { nx = cx[i + 1]; ny = cy[i + 1]; ni = ci[i + 1]; }
         while (sp >= 2) {
             const int64_t o = (bx - ax) * (y - ay) - (by - ay) * (x - ax);
             if (side > 0 ? (o > 0) : (o < 0)) {
@@ -132,14 +136,16 @@ HD int fill_pockets(const int32_t* ci, const int32_t* cx, const int32_t* cy, int
                 --sp;
                 ib = ia; bx = ax; by = ay;
                 if (sp >= 2) {
-                    const int a = stack[sp - 2];
-                    ia = ci[a]; ax = cx[a]; ay = cy[a];
+                    const int32_t* q = stack + 4 * (sp - 2);
+                    ia = q[0]; ax = q[1]; ay = q[2];
                 }
             } else {
                 break;
             }
         }
-        stack[sp++] = i;
+        int32_t* e = stack + 4 * sp;
+        e[0] = ii; e[1] = int32_t(x); e[2] = int32_t(y); e[3] = 0;
+        ++sp;
         ia = ib; ax = bx; ay = by;
         ib = ii; bx = x; by = y;
     }

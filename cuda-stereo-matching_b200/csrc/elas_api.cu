@@ -229,7 +229,7 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         D.rcnt = (int32_t*)take(rows * 4);
         D.ne = (int32_t*)take(rows * 4);
         D.soff = (int32_t*)take(rows * 4);
-        D.chain = (int32_t*)take(8 * rows * 4);
+        D.chain = (int32_t*)take(14 * rows * 4);   // 2 sides x (index, x, y, 4-int stack records)
         D.tri = (int32_t*)take(3 * tmax * 4);
         D.opp = (int32_t*)take(3 * tmax * 4);
         D.txy = (uint32_t*)take(3 * tmax * 4);

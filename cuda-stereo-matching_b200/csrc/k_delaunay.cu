@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32
     } else if (R >= 2) {
         for (int e = threadIdx.x; e < 2 * R; e += blockDim.x) {
             const int side = e >= R, s = e - side * R;
-            int32_t* ci = (in_smem ? sh : D.chain) + side * 4 * cap;
+            int32_t* ci = (in_smem ? sh : D.chain) + side * 7 * cap;
             const int r = D.ne[s];
             const int i = D.srt[row_off[r] + (side ? D.rcnt[r] - 1 : 0)];
             ci[s] = i; ci[cap + s] = D.x[i]; ci[2 * cap + s] = D.y[i];
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32
         __syncthreads();
         if ((threadIdx.x & 31) == 0 && threadIdx.x < 64) {
             const int side = threadIdx.x >> 5;
-            int32_t* ci = (in_smem ? sh : D.chain) + side * 4 * cap;
+            int32_t* ci = (in_smem ? sh : D.chain) + side * 7 * cap;
             npk[side] = fill_pockets(ci, ci + cap, ci + 2 * cap, R, side ? -1 : +1, ci + 3 * cap,
                                      D.tri + 3 * size_t(off + side * R));
         }
@@ -782,8 +782,8 @@ int cluster_size_for_flip() {
 cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int nmax, int num_sms,
                             int csize, unsigned* err, cudaStream_t st, int* nlaunch) {
     k_rowsort<<<dim3(nrows, 2), 512, 0, st>>>(d0, d1, row_off, nrows, err);
-    int smem_rows = imin(nrows, (96 * 1024) / 32);     // 2 sides x (index, x, y, stack)
-    size_t smem = size_t(smem_rows) * 32;
+    int smem_rows = imin(nrows, (96 * 1024) / 56);     // 2 sides x (index, x, y, 4-int stack records)
+    size_t smem = size_t(smem_rows) * 56;
     cudaFuncSetAttribute(k_plan, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     k_plan<<<2, 1024, smem, st>>>(d0, d1, row_off, nrows, smem_rows, err);
     int blocks = 4 * num_sms;

@@ -172,7 +172,14 @@ __global__ void __launch_bounds__(1024) k_spk_tile(PostViews pv, int W, int H, f
         }
     }
     __syncthreads();
-    const int r = valid ? lfind(L, t) : -1;
+    // roots: the run heads (the only nodes of the forest) walk to their
+    // root and keep it; every pixel then reads its head's entry
+    const bool head = valid && !conn_l;
+    int r = head ? lfind(L, t) : -1;
+    __syncthreads();
+    if (head) L[t] = r;
+    __syncthreads();
+    if (valid && !head) r = L[L[t]];
     {   // component sizes, one shared atomic per group of lanes with the same root
         const unsigned peers = __match_any_sync(0xffffffffu, r);
         if (r >= 0 && tx == __ffs(peers) - 1) atomicAdd(&C[r], __popc(peers));

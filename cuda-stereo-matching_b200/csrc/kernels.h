@@ -15,7 +15,7 @@ struct DelDev {
     int32_t* rcnt;         // [rows] unique points per row
     int32_t* ne;           // [rows] non-empty rows
     int32_t* soff;         // [rows] strip triangle offsets
-    int32_t* chain;        // [8*rows] pocket walk scratch (2 sides) when it does not fit in shared memory
+    int32_t* chain;        // [14*rows] pocket walk scratch (2 sides) when it does not fit in shared memory
     int32_t* tri;          // [3*Tmax]
     int32_t* opp;          // [3*Tmax]
     uint32_t* txy;         // [3*Tmax] packed corner coordinates (global flip kernel)

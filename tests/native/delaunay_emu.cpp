@@ -43,7 +43,7 @@ extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const i
     int T = 0;
     if (R >= 2) {
         if (off + 2 * R > Tmax) return -1;
-        std::vector<int32_t> ci(R), cx(R), cy(R), stk(R);
+        std::vector<int32_t> ci(R), cx(R), cy(R), stk(4 * size_t(R));
         int pockets = 0;
         for (int side = 0; side < 2; ++side) {
             for (int s = 0; s < R; ++s) {
