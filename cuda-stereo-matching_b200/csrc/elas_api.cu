@@ -119,6 +119,8 @@ uint32_t next_pow2(size_t x) {
     return c;
 }
 
+int penalty(int dd, const elas_params& p);
+
 int check_params(const elas_params& p, std::string& why) {
     if (p.candidate_stepsize < 1) { why = "candidate_stepsize must be >= 1"; return ELAS_ERR_INVALID_ARG; }
     if (p.grid_size < 1) { why = "grid_size must be >= 1"; return ELAS_ERR_INVALID_ARG; }
@@ -130,6 +132,10 @@ int check_params(const elas_params& p, std::string& why) {
     }
     float r = std::max(std::ceil(p.sigma * p.sradius), 2.0f);
     if (r > 15.0f) { why = "sigma*sradius must be <= 15"; return ELAS_ERR_UNSUPPORTED; }
+    // dense matching packs energy * 4096 + d into an int: the prior penalty
+    // (negative, growing as 1/beta) must stay above -2^18
+    for (int dd = 0; dd <= int(r); ++dd)
+        if (penalty(dd, p) < -(1 << 18)) { why = "beta is too small (prior penalty below -2^18)"; return ELAS_ERR_UNSUPPORTED; }
     if (p.incon_window_size < 0) { why = "incon_window_size must be >= 0"; return ELAS_ERR_INVALID_ARG; }
     return ELAS_OK;
 }

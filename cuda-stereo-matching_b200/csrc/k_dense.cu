@@ -176,9 +176,14 @@ constexpr int LMAX = 48;
 
 // Energy update with the reference's strict '<' (the first minimum in
 // evaluation order wins).
-__device__ __forceinline__ void take_min(int e, int d, int& min_val, int& min_d) {
-    if (e < min_val) { min_val = e; min_d = d; }
-}
+// Both passes (the cell list, then the plane window) walk their
+// disparities in ascending order, so the reference's strict '<' keeps, per
+// pass, the smallest energy and among equal energies the smallest d: the
+// minimum of e * 4096 + d (d < 4096, energies above -2^18).  The window
+// result replaces the list result only with a strictly smaller energy.
+constexpr int PK_NONE = 10000 * 4096;   // the reference's start value: energy 10000, no disparity
+__device__ __forceinline__ int pk_ed(int e, int d) { return e * 4096 + d; }
+__device__ __forceinline__ void take_min(int e, int d, int& best) { best = min(best, pk_ed(e, d)); }
 
 // blockIdx.x = row, blockIdx.y = view (0 left, 1 right).  The other view's
 // descriptor row arrives by bulk copy (TMA) while the CTA expands the
@@ -279,7 +284,7 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
             const int dlim = right ? W - 4 - u : u - 3;
             const int dpmin = imax(dp - r, 0);
             const int dpmax = imin(dp + r, g.D);
-            int min_val = 10000, min_d = -1;
+            int best_l = PK_NONE, best_w = PK_NONE;
             const int n = lcnt[c];
             if (n != 255) {
                 const int16_t* Ls = lst + c * LMAX;
@@ -292,20 +297,20 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
                         if (db > dlim) break;
                         const int ea = sad16(I1, row[u + dir * da]);
                         const int eb = sad16(I1, row[u + dir * db]);
-                        take_min(ea, da, min_val, min_d);
-                        take_min(eb, db, min_val, min_d);
+                        take_min(ea, da, best_l);
+                        take_min(eb, db, best_l);
                     }
                     for (; i < n; ++i) {
                         const int d = Ls[i];
                         if (d > dlim) break;
-                        take_min(sad16(I1, row[u + dir * d]), d, min_val, min_d);
+                        take_min(sad16(I1, row[u + dir * d]), d, best_l);
                     }
                 } else {
                     for (; i < n; ++i) {
                         const int d = Ls[i];
                         if (d > dlim) break;
                         if (d >= dpmin && d <= dpmax) continue;
-                        take_min(sad16(I1, row[u + dir * d]), d, min_val, min_d);
+                        take_min(sad16(I1, row[u + dir * d]), d, best_l);
                     }
                 }
             } else {
@@ -318,7 +323,7 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
                         bits &= bits - 1;
                         if (d > dlim) { done = true; break; }
                         if (d >= dpmin && d <= dpmax) continue;
-                        take_min(sad16(I1, row[u + dir * d]), d, min_val, min_d);
+                        take_min(sad16(I1, row[u + dir * d]), d, best_l);
                     }
                 }
             }
@@ -327,14 +332,15 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
                 for (int k = -RFIX; k <= RFIX; ++k) {
                     const int d = dp + k;
                     if (d >= 0 && d <= g.D && d <= dlim)
-                        take_min(sad16(I1, row[u + dir * d], p.penalty[k < 0 ? -k : k]), d, min_val, min_d);
+                        take_min(sad16(I1, row[u + dir * d], p.penalty[k < 0 ? -k : k]), d, best_w);
                 }
             } else {
                 const int dhi = imin(dpmax, dlim);
                 for (int d = dpmin; d <= dhi; ++d)
-                    take_min(sad16(I1, row[u + dir * d], p.penalty[d > dp ? d - dp : dp - d]), d, min_val, min_d);
+                    take_min(sad16(I1, row[u + dir * d], p.penalty[d > dp ? d - dp : dp - d]), d, best_w);
             }
-            out = min_d >= 0 ? float(min_d) : -1.0f;
+            const int best = (best_w >> 12) < (best_l >> 12) ? best_w : best_l;
+            out = best < PK_NONE ? float(best & 4095) : -1.0f;
         }
         disp[o] = out;
     }
