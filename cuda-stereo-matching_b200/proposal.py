@@ -217,7 +217,8 @@ def evaluate(torch, theta, preset, seeds, log=None, flush_bytes=256 << 20):
             for name, e in engines.items():
                 o1, o2 = outs[name]
                 args = (dl.data_ptr(), dr.data_ptr(), o1.data_ptr(), o2.data_ptr(), W, H)
-                if i == 0:                       # grows the workspaces outside the timing
+                if i == 0:   # sizes the workspaces and captures the pair's graph outside the timing
+                    e.process_device(*args, stream=stream.cuda_stream)
                     e.process_device(*args, stream=stream.cuda_stream)
                 flush.zero_()
                 a = torch.cuda.Event(enable_timing=True)
