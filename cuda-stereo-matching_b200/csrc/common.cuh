@@ -53,6 +53,11 @@ enum : unsigned {
 };
 
 #if defined(__CUDACC__)
+// First statement of every kernel: wait until the preceding work of the
+// stream has completed and its writes are visible (programmatic dependent
+// launch; a no-op for a kernel launched without the attribute).
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Sum of absolute differences of two 16-byte descriptors: four
 // vabsdiff4.u32.u32.u32.add (byte-wise |a-b| summed into the accumulator),
 // the fastest of the packed-byte forms on sm_100a.

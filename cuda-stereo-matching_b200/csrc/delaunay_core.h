@@ -22,8 +22,9 @@
 //     table in two phases (resolve, then write).  Converges to the unique
 //     Delaunay triangulation under the symbolic perturbation below.
 //
-// Predicates: orientation and incircle on integer coordinates in int64 --
-// exact for |coordinates| < 2^15 (terms stay below 2^62).  Ties (four
+// Predicates: orientation and incircle on integer coordinates, exact in
+// int32 / int64 arithmetic for the library's image limits (pack_xy below).
+// Ties (four
 // co-circular points) are broken by simulation of simplicity: point i is
 // lifted to x^2+y^2 - eps^(i+1); then d is inside circle(a,b,c) iff the
 // lowest index m of {a,b,c,d} is d, or d's barycentric coordinate for m is
@@ -44,34 +45,6 @@ struct Pts {
     const int32_t* x;
     const int32_t* y;
 };
-
-HD int64_t orient(Pts P, int a, int b, int c) {
-    int64_t ax = P.x[a], ay = P.y[a];
-    return (int64_t(P.x[b]) - ax) * (int64_t(P.y[c]) - ay) -
-           (int64_t(P.y[b]) - ay) * (int64_t(P.x[c]) - ax);
-}
-
-// > 0 iff d lies inside the circumcircle of the counter-clockwise (a,b,c).
-HD int64_t incircle(Pts P, int a, int b, int c, int d) {
-    int64_t dx = P.x[d], dy = P.y[d];
-    int64_t adx = P.x[a] - dx, ady = P.y[a] - dy;
-    int64_t bdx = P.x[b] - dx, bdy = P.y[b] - dy;
-    int64_t cdx = P.x[c] - dx, cdy = P.y[c] - dy;
-    int64_t al = adx * adx + ady * ady;
-    int64_t bl = bdx * bdx + bdy * bdy;
-    int64_t cl = cdx * cdx + cdy * cdy;
-    return adx * (bdy * cl - bl * cdy) - ady * (bdx * cl - bl * cdx) + al * (bdx * cdy - bdy * cdx);
-}
-
-HD bool inside_sos(Pts P, int a, int b, int c, int d) {
-    int64_t det = incircle(P, a, b, c, d);
-    if (det != 0) return det > 0;
-    int m = imin(imin(a, b), imin(c, d));
-    if (m == d) return true;
-    if (m == a) return orient(P, d, b, c) < 0;
-    if (m == b) return orient(P, a, d, c) < 0;
-    return orient(P, a, b, d) < 0;
-}
 
 // Strip between an upper row A[0..m) and a lower row B[0..n), both sorted
 // by strictly increasing x: walking the merge of A[1..m) and B[1..n) by x
@@ -188,18 +161,31 @@ HD uint32_t pack_xy(int32_t x, int32_t y) {
 HD int32_t px_of(uint32_t p) { return int32_t(p & 0xffffu) - 32768; }
 HD int32_t py_of(uint32_t p) { return int32_t(p >> 16) - 32768; }
 
+// Coordinate differences of packed points (the bias cancels).
+HD int32_t dx_p(uint32_t a, uint32_t b) { return int32_t(a & 0xffffu) - int32_t(b & 0xffffu); }
+HD int32_t dy_p(uint32_t a, uint32_t b) { return int32_t(a >> 16) - int32_t(b >> 16); }
+
+// Narrow exact predicates.  The library accepts width <= 14000,
+// height <= 16384 and disp_max <= 4095, so point x lies in [-4095, 13999]
+// (right view: u - d) and y in [0, 16383]: |dx| <= 18094, |dy| <= 16383.
+// Then every square sum and every 2x2 orientation term is below 2^30 in
+// magnitude (int32), and the lifted determinant is a sum of three 32x32-bit
+// products below 2^59 each (int64).  Both are exact.
 HD int64_t orient_p(uint32_t a, uint32_t b, uint32_t c) {
-    int64_t ax = px_of(a), ay = py_of(a);
-    return (int64_t(px_of(b)) - ax) * (int64_t(py_of(c)) - ay) - (int64_t(py_of(b)) - ay) * (int64_t(px_of(c)) - ax);
+    return int64_t(dx_p(b, a) * dy_p(c, a) - dy_p(b, a) * dx_p(c, a));
 }
 
+// > 0 iff d lies inside the circumcircle of the counter-clockwise (a,b,c):
+// the 3x3 lifted determinant expanded along its lifted column,
+// |a-d|^2 * orient(b,c) + |b-d|^2 * orient(c,a) + |c-d|^2 * orient(a,b)
+// with every orientation taken relative to d.
 HD int64_t incircle_p(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-    int64_t dx = px_of(d), dy = py_of(d);
-    int64_t adx = px_of(a) - dx, ady = py_of(a) - dy;
-    int64_t bdx = px_of(b) - dx, bdy = py_of(b) - dy;
-    int64_t cdx = px_of(c) - dx, cdy = py_of(c) - dy;
-    int64_t al = adx * adx + ady * ady, bl = bdx * bdx + bdy * bdy, cl = cdx * cdx + cdy * cdy;
-    return adx * (bdy * cl - bl * cdy) - ady * (bdx * cl - bl * cdx) + al * (bdx * cdy - bdy * cdx);
+    const int32_t adx = dx_p(a, d), ady = dy_p(a, d);
+    const int32_t bdx = dx_p(b, d), bdy = dy_p(b, d);
+    const int32_t cdx = dx_p(c, d), cdy = dy_p(c, d);
+    const int32_t al = adx * adx + ady * ady, bl = bdx * bdx + bdy * bdy, cl = cdx * cdx + cdy * cdy;
+    const int32_t obc = bdx * cdy - bdy * cdx, oca = cdx * ady - cdy * adx, oab = adx * bdy - ady * bdx;
+    return int64_t(al) * obc + int64_t(bl) * oca + int64_t(cl) * oab;
 }
 
 // inside_sos on packed coordinates; ia..id are the point indices that order
@@ -220,20 +206,28 @@ HD bool inside_sos_p(int ia, uint32_t a, int ib, uint32_t b, int ic, uint32_t c,
 // accessor (global memory, host emulation) and the cluster accessor
 // (distributed shared memory) share this code.
 //
+// Is the edge of half-edge h (twin tw) not locally Delaunay?  Tested from
+// h's side: h's triangle (a, b, c) against the vertex of tw's triangle
+// opposite the edge.
+template <class M>
+HD bool edge_flippable(const M& m, int h, int tw) {
+    const int t = h / 3, s = h % 3, n = tw / 3, sn = tw % 3;
+    const int s1 = s == 2 ? 0 : s + 1, s2 = s1 == 2 ? 0 : s1 + 1, sd = sn == 0 ? 2 : sn - 1;
+    return inside_sos_p(m.v(t, s), m.xy(t, s), m.v(t, s1), m.xy(t, s1), m.v(t, s2), m.xy(t, s2), m.v(n, sd),
+                        m.xy(n, sd));
+}
+
 // Phase A: test half-edge h; propose it if its edge is not locally Delaunay.
 // `owner`: only the triangle with the smaller index tests a shared edge.
 template <class M, class Append>
 HD bool flip_propose(M& m, int h, int T, uint32_t round, bool owner, Append append_cand) {
-    int t = h / 3, s = h % 3;
+    int t = h / 3;
     int o = m.opp(h);
     if (o < 0) return true;
     int n = o / 3;
     if (n >= T || t >= T) return false;
     if (owner && n <= t) return true;
-    int sn = o % 3;
-    int s1 = s == 2 ? 0 : s + 1, s2 = s1 == 2 ? 0 : s1 + 1, sd = sn == 0 ? 2 : sn - 1;
-    if (inside_sos_p(m.v(t, s), m.xy(t, s), m.v(t, s1), m.xy(t, s1), m.v(t, s2), m.xy(t, s2), m.v(n, sd),
-                     m.xy(n, sd))) {
+    if (edge_flippable(m, h, o)) {
         uint32_t p = prio(uint32_t(h), round);
         m.lock_min(t, p);
         m.lock_min(n, p);

@@ -487,11 +487,10 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
                     prior_shift(g, dp), h->err, st, shape, sub));
     n += 1;
     CK(mark(ELAS_TIME_LR));
-    CK(launch_lr(h->raw0, h->raw1, h->lr0, h->lr1, g, p.lr_threshold, st, sub));
+    // the checked maps also land in the outputs, where the post-filters work in place
+    CK(launch_lr(h->raw0, h->raw1, h->lr0, h->lr1, out0, out1, g, p.lr_threshold, st, sub));
     n += 1;
     CK(mark(ELAS_TIME_POST));
-    CK(cudaMemcpyAsync(out0, h->lr0, size_t(go.W) * go.H * 4, cudaMemcpyDeviceToDevice, st));
-    CK(cudaMemcpyAsync(out1, h->lr1, size_t(go.W) * go.H * 4, cudaMemcpyDeviceToDevice, st));
     PostViews pv;
     float* outs[2] = {out0, out1};
     for (int k = 0; k < 2; ++k) {

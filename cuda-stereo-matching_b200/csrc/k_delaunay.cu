@@ -9,6 +9,7 @@
 #include <type_traits>
 #include <cuda_runtime.h>
 #include "common.cuh"
+#include "launch.cuh"
 #include "delaunay_core.h"
 #include "kernels.h"
 
@@ -80,11 +81,57 @@ __device__ __forceinline__ int agg_inc_keyed(int* ctr) {
     return base + __popc(peers & ((1u << lane) - 1u));
 }
 
+// Worklists hold every interior edge at most once per round, as its lower
+// half-edge c = min(x, r) (x a half-edge, r its twin; hull edges, r < 0,
+// never flip).  `mark` is the round's bitset over half-edges, cleared before
+// the round's pushes; the lane that sets c's bit queues it.  With one entry
+// per edge, no edge is proposed twice in a round.
+__device__ __forceinline__ bool claim_edge(uint32_t* mark, int x, int r, int& c) {
+    if (r < 0) return false;
+    c = min(x, r);
+    const uint32_t bit = 1u << (c & 31);
+    return (atomicOr(mark + (c >> 5), bit) & bit) == 0u;
+}
+
+// Round 0 of a flip kernel: propose every interior edge of the half-edges
+// [h0, h1) once (the owner rule: the half-edge whose triangle has the
+// smaller index).  Each warp compacts its owned half-edges through a
+// 64-entry ring in shared memory (`ring`, per warp) and proposes them 32 at
+// a time, so no lane idles on a twin.  `opp_of(h)` reads a link, `prop(h)`
+// proposes; all 32 lanes of every warp of the block must call this.
+template <class Opp, class Prop>
+__device__ __forceinline__ void propose_owned(int h0, int h1, int32_t* ring, Opp opp_of, Prop prop) {
+    const int lane = threadIdx.x & 31;
+    int head = 0, cnt = 0;
+    for (int base = h0 + int(threadIdx.x & ~31u); base < h1; base += int(blockDim.x)) {
+        const int h = base + lane;
+        bool own = false;
+        if (h < h1) {
+            const int o = opp_of(h);
+            own = o >= 0 && o / 3 > h / 3;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, own);
+        if (own) ring[(head + cnt + __popc(bal & ((1u << lane) - 1u))) & 63] = h;
+        cnt += __popc(bal);
+        __syncwarp();
+        if (cnt >= 32) {
+            const int hh = ring[(head + lane) & 63];
+            __syncwarp();
+            prop(hh);
+            head = (head + 32) & 63;
+            cnt -= 32;
+        }
+    }
+    __syncwarp();
+    if (lane < cnt) prop(ring[(head + lane) & 63]);
+}
+
 // Per lattice row: sort the row's points by (x, index), drop repeated x
 // (keeps the lowest index), write the unique list to srt[row_off[r] ..] and
 // its length to rcnt[r].
 __global__ void __launch_bounds__(512) k_rowsort(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off,
                                                  int nrows, unsigned* err) {
+    grid_dep_wait();
     __shared__ unsigned long long key[SORT_CAP];
     __shared__ int keep[SORT_CAP];
     const DelDev& D = blockIdx.y ? d1 : d0;
@@ -148,6 +195,7 @@ __global__ void __launch_bounds__(512) k_rowsort(DelDev d0, DelDev d1, const int
 // (index, x, y) and the stack of the pocket walk when it fits.
 __global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off,
                                                int nrows, int smem_rows, unsigned* err) {
+    grid_dep_wait();
     extern __shared__ int32_t sh[];
     __shared__ int ws[33];
     DelDev D = blockIdx.x ? d1 : d0;
@@ -221,6 +269,7 @@ __global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32
 // the strip below its row (as the upper row) and in the strip above (as the
 // lower row), placed by merge path.
 __global__ void k_strips(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off, int nmax) {
+    grid_dep_wait();
     const DelDev& D = blockIdx.y ? d1 : d0;
     const int R = D.ctr[6];
     if (D.ctr[0] == 0) return;
@@ -263,6 +312,7 @@ __device__ __forceinline__ uint32_t hash_cap(int T) {
 }
 
 __global__ void k_hash_clear(DelDev d0, DelDev d1) {
+    grid_dep_wait();
     const DelDev& D = blockIdx.y ? d1 : d0;
     uint32_t cap = hash_cap(D.ctr[0]);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cap && i < D.Hmax; i += gridDim.x * blockDim.x) {
@@ -272,6 +322,7 @@ __global__ void k_hash_clear(DelDev d0, DelDev d1) {
 }
 
 __global__ void k_hash_insert(DelDev d0, DelDev d1, unsigned* err) {
+    grid_dep_wait();
     const DelDev& D = blockIdx.y ? d1 : d0;
     const int T = D.ctr[0];
     const uint32_t cap = hash_cap(T), mask = cap - 1;
@@ -299,6 +350,7 @@ __global__ void k_hash_insert(DelDev d0, DelDev d1, unsigned* err) {
 
 // Neighbour links from the hash, and the per-triangle flip state.
 __global__ void k_link(DelDev d0, DelDev d1, unsigned* err) {
+    grid_dep_wait();
     const DelDev& D = blockIdx.y ? d1 : d0;
     const int T = D.ctr[0];
     for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < 3 * T; h += gridDim.x * blockDim.x) {
@@ -317,17 +369,6 @@ struct GAMin {
     __device__ void operator()(uint32_t* p, uint32_t v) const { atomicMin(p, v); }
 };
 
-// Packed coordinates of every triangle corner (flat storage of the fallback).
-__global__ void k_tri_xy(DelDev d0, DelDev d1) {
-    const DelDev& D = blockIdx.y ? d1 : d0;
-    if (D.ctr[8] != 0) return;            // the cluster kernel handled this problem
-    const int T = D.ctr[0];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * T; i += gridDim.x * blockDim.x) {
-        int v = D.tri[i];
-        D.txy[i] = pack_xy(D.x[v], D.y[v]);
-    }
-}
-
 // Shared round driver: one "group" (a CTA, or a cluster of CTAs) runs the
 // rounds; `Sync` is its barrier.  Lists live in global memory; their
 // counters in shared memory of the owning CTA.
@@ -336,6 +377,7 @@ __global__ void k_tri_xy(DelDev d0, DelDev d1) {
 // triangulations larger than the cluster kernel holds.  Every loop is
 // bounded: `max_rounds` rounds at most (ERRF_FLIP_LIMIT).
 __global__ void __launch_bounds__(FLIP_THREADS) k_flip_global(DelDev d0, DelDev d1, int max_rounds, unsigned* err) {
+    grid_dep_wait();
     __shared__ int n_cand, n_flip, n_next, n_cur, stop;
     const DelDev& D = blockIdx.x ? d1 : d0;
     if (D.ctr[8] != 0) return;            // the cluster kernel handled this problem
@@ -343,7 +385,15 @@ __global__ void __launch_bounds__(FLIP_THREADS) k_flip_global(DelDev d0, DelDev 
     FlatTri<GAMin> m{D.tri, D.txy, D.opp, D.lock, D.fround, GAMin()};
     const int cand_cap = 3 * D.Tmax, wl_cap = 6 * D.Tmax;
     const int tid = threadIdx.x;
+    // the two per-round push bitsets live in hslot, which k_link was the last to read
+    const int mark_words = (3 * D.Tmax + 31) / 32, used_words = (3 * T + 31) / 32;
+    uint32_t* const mark0 = reinterpret_cast<uint32_t*>(D.hslot);
+    uint32_t* const mark1 = mark0 + mark_words;
     for (int t = tid; t < T; t += FLIP_THREADS) { D.lock[t] = LOCK_FREE; D.fround[t] = -1; }
+    for (int i = tid; i < 3 * T; i += FLIP_THREADS) {     // packed corner coordinates of the flat storage
+        const int v = D.tri[i];
+        D.txy[i] = pack_xy(D.x[v], D.y[v]);
+    }
     if (tid == 0) { n_cur = 3 * T; stop = 0; }
     __syncthreads();
     int round = 0, flips_total = 0;
@@ -361,6 +411,9 @@ __global__ void __launch_bounds__(FLIP_THREADS) k_flip_global(DelDev d0, DelDev 
                 }))
                 set_err(err, ERRF_BOUNDS);
         }
+        // this round's push bitset was last used two rounds ago
+        uint32_t* const mark_nxt = (round & 1) ? mark0 : mark1;
+        for (int i = tid; i < used_words; i += FLIP_THREADS) mark_nxt[i] = 0u;
         __syncthreads();
         const int nc = n_cand;
         if (tid == 0 && nc > cand_cap) { set_err(err, ERRF_BOUNDS); stop = 1; }
@@ -385,20 +438,22 @@ __global__ void __launch_bounds__(FLIP_THREADS) k_flip_global(DelDev d0, DelDev 
             }
         }
         __syncthreads();
-        auto push = [&](int x) {
+        auto push = [&](int x, int r) {
+            int c;
+            if (!claim_edge(mark_nxt, x, r, c)) return;
             int idx = agg_inc(&n_next);
-            if (idx < wl_cap) nxt[idx] = x;
+            if (idx < wl_cap) nxt[idx] = c;
         };
         for (int f = tid; f < nf; f += FLIP_THREADS) {
             int t = D.flips[6 * f], n = D.flips[6 * f + 1];
             flip_relink(m, t, n, D.flips + 6 * f + 2);
-            for (int k = 0; k < 4; ++k) push(outer_slot(t, n, k));
+            for (int k = 0; k < 4; ++k) push(outer_slot(t, n, k), D.flips[6 * f + 2 + k]);
         }
         for (int c = tid; c < nc; c += FLIP_THREADS) {
             int h = D.cand[2 * c], n = D.cand[2 * c + 1], t = h / 3;
             D.lock[t] = LOCK_FREE;
             D.lock[n] = LOCK_FREE;
-            if (D.fround[t] != round && D.fround[n] != round) push(h);
+            if (D.fround[t] != round && D.fround[n] != round) push(h, D.opp[h]);
         }
         flips_total += nf;
         __syncthreads();
@@ -409,6 +464,8 @@ __global__ void __launch_bounds__(FLIP_THREADS) k_flip_global(DelDev d0, DelDev 
         __syncthreads();
         if (stop) break;
     }
+    __syncthreads();
+    for (int t = tid; t < T; t += FLIP_THREADS) normalise(D.tri + 3 * size_t(t));
     if (tid == 0) {
         D.ctr[4] = round + 1;
         D.ctr[5] = flips_total;
@@ -430,6 +487,10 @@ constexpr int SLICE_MAX = 1 << SLICE_MAX_LOG2;
 constexpr int WL_PER_CTA = 6 * SLICE_MAX;           // worklist entries per CTA and round
 constexpr int CAND_PER_CTA = 6 * SLICE_MAX;         // proposals per CTA and round
 constexpr int FLIP_PER_CTA = SLICE_MAX;             // flipped pairs per CTA and round
+constexpr int CL_MARK = 3 * SLICE_MAX / 32;         // words of a per-round half-edge bitset
+// shared memory: the triangle slice (44 bytes a triangle), two push bitsets
+// and the round-0 staging rings (64 entries per warp)
+constexpr size_t CL_SMEM = size_t(SLICE_MAX) * 44 + size_t(8) * CL_MARK + size_t(4) * 64 * (CL_THREADS / 32);
 
 struct ClusterTri {
     int32_t* lv;      // [3*SLICE_MAX] in this CTA's shared memory
@@ -492,18 +553,36 @@ struct List2 {
 
 constexpr int LOC_T = 4096;        // triangles of a one-SM problem
 constexpr int LOC_PTS = 4096;      // support points (vertex ids) of a one-SM problem
-constexpr int LOC_WL = 3072;       // worklist entries per buffer in shared memory
-constexpr int LOC_CAND = 2048;     // proposals in shared memory
+constexpr int LOC_CAND = 1536;     // proposals of a round in shared memory (two round lists)
 constexpr int LOC_FLIP = 1280;     // flipped pairs in shared memory
-constexpr size_t LOC_SMEM = size_t(32) * LOC_T + size_t(4) * LOC_PTS + size_t(8) * LOC_WL + size_t(8) * LOC_CAND +
-                            size_t(24) * LOC_FLIP;
+constexpr int LOC_MARK = (3 * LOC_T + 31) / 32;   // words of a per-round half-edge bitset
+constexpr size_t LOC_SMEM = size_t(36) * LOC_T + size_t(4) * LOC_PTS + size_t(16) * LOC_CAND +
+                            size_t(24) * LOC_FLIP + size_t(8) * LOC_MARK;
+// round 0 stages each warp's owned half-edges (64 entries) in the flip list's
+// shared part, which is unused until the first flips
+static_assert(6 * LOC_FLIP >= 64 * (1024 / 32), "round-0 staging does not fit");
 
 // Flip rounds of one problem in one CTA: triangles, points and the round
-// lists in shared memory, __syncthreads between the phases.  Problems with
-// more triangles or points are left (ctr[8] stays 0) to the cluster kernel.
+// lists in shared memory.  Problems with more triangles or points are left
+// (ctr[8] stays 0) to the cluster kernel.
+//
+// A round is three phases between barriers:
+//   B   flip the proposals that won both locks; release the locks of the
+//       round before; clear the next round's edge bitset;
+//   C1  resolve the outer neighbours of every flipped pair (read only) and
+//       propose, for the next round, each outer edge that is not locally
+//       Delaunay (vertices are final once B is over, so the test needs no
+//       links);
+//   C2  write the links; re-propose the proposals that lost a lock while
+//       neither of their triangles flipped (their test result is unchanged).
+// Proposals of consecutive rounds use two lock arrays, so the next round's
+// locks fill while this round's are still held.  The rounds, proposals and
+// flips are those of the propose / flip / resolve / relink formulation with
+// a worklist (the host emulation): only the tests move forward a phase.
 __global__ void __launch_bounds__(1024) k_flip_local(DelDev d0, DelDev d1, int max_rounds, unsigned* err) {
+    grid_dep_wait();
     extern __shared__ __align__(16) uint8_t lsm[];
-    __shared__ int n_cand, n_flip, n_wl[2], stop;
+    __shared__ int n_cand[2], n_flip;
     const DelDev& D = blockIdx.x ? d1 : d0;
     const int T = D.ctr[0], NP = D.ctr[9];
     if (D.ctr[8] != 0 || T > LOC_T || NP > LOC_PTS) return;
@@ -511,48 +590,60 @@ __global__ void __launch_bounds__(1024) k_flip_local(DelDev d0, DelDev d1, int m
     PtTri m;
     m.lv = reinterpret_cast<int32_t*>(lsm);
     m.lopp = m.lv + 3 * LOC_T;
-    m.llock = reinterpret_cast<uint32_t*>(m.lopp + 3 * LOC_T);
-    m.lround = reinterpret_cast<int32_t*>(m.llock + LOC_T);
+    uint32_t* const lock0 = reinterpret_cast<uint32_t*>(m.lopp + 3 * LOC_T);
+    uint32_t* const lock1 = lock0 + LOC_T;
+    m.lround = reinterpret_cast<int32_t*>(lock1 + LOC_T);
     uint32_t* pxy = reinterpret_cast<uint32_t*>(m.lround + LOC_T);
     m.pxy = pxy;
     int32_t* sw = reinterpret_cast<int32_t*>(pxy + LOC_PTS);
-    List2 wl[2] = {{sw, D.cwl, LOC_WL, WL_PER_CTA, 1}, {sw + LOC_WL, D.cwl + WL_PER_CTA, LOC_WL, WL_PER_CTA, 1}};
-    List2 cand{sw + 2 * LOC_WL, D.ccand, LOC_CAND, CAND_PER_CTA, 2};
-    List2 flips{sw + 2 * LOC_WL + 2 * LOC_CAND, D.cflips, LOC_FLIP, FLIP_PER_CTA, 6};
+    const List2 cand0{sw, D.ccand, LOC_CAND, CAND_PER_CTA, 2};
+    const List2 cand1{sw + 2 * LOC_CAND, D.ccand + 2 * CAND_PER_CTA, LOC_CAND, CAND_PER_CTA, 2};
+    const List2 flips{sw + 4 * LOC_CAND, D.cflips, LOC_FLIP, FLIP_PER_CTA, 6};
+    uint32_t* const mark0 = reinterpret_cast<uint32_t*>(sw + 4 * LOC_CAND + 6 * LOC_FLIP);
+    uint32_t* const mark1 = mark0 + LOC_MARK;
     for (int i = tid; i < NP; i += NT) pxy[i] = pack_xy(D.x[i], D.y[i]);
     for (int t = tid; t < T; t += NT) {
         for (int k = 0; k < 3; ++k) {
             m.lv[3 * t + k] = D.tri[3 * t + k];
             m.lopp[3 * t + k] = D.opp[3 * t + k];
         }
-        m.llock[t] = LOCK_FREE;
+        lock0[t] = LOCK_FREE;
+        lock1[t] = LOCK_FREE;
         m.lround[t] = -1;
     }
-    if (tid == 0) { n_cand = 0; n_flip = 0; n_wl[0] = n_wl[1] = 0; stop = 0; }
+    if (tid == 0) { n_cand[0] = 0; n_cand[1] = 0; n_flip = 0; }
     __syncthreads();
-    int round = 0, flips_total = 0;
+    // round 0's proposals: every interior edge once
+    m.llock = lock0;
+    {
+        auto add0 = [&](int hh, int nn) {
+            int idx = agg_inc(&n_cand[0]);
+            if (idx < cand0.cap()) { int32_t* c = cand0.slot(idx); c[0] = hh; c[1] = nn; }
+        };
+        propose_owned(0, 3 * T, flips.s + 64 * (tid >> 5), [&](int h) { return m.lopp[h]; }, [&](int h) {
+            if (!flip_propose(m, h, T, 0u, false, add0)) set_err(err, ERRF_BOUNDS);
+        });
+    }
+    __syncthreads();
+    int round = 0, flips_total = 0, nc_prev = 0;
     bool converged = false;
     for (; round < max_rounds; ++round) {
         const int cur = round & 1, nxt = cur ^ 1;
-        // A: propose (round 0: every half-edge, owner rule)
-        const int items = round == 0 ? 3 * T : min(n_wl[cur], wl[cur].cap());
-        auto add_cand = [&](int hh, int nn) {
-            int idx = agg_inc(&n_cand);
-            if (idx < cand.cap()) { int32_t* c = cand.slot(idx); c[0] = hh; c[1] = nn; }
-        };
-        for (int k = tid; k < items; k += NT) {
-            int h = round == 0 ? k : *wl[cur].slot(k);
-            if (!flip_propose(m, h, T, uint32_t(round), round == 0, add_cand)) set_err(err, ERRF_BOUNDS);
+        // selected by value: a dynamically indexed pair would live in local memory
+        const List2 cand_cur = cur ? cand1 : cand0, cand_nxt = cur ? cand0 : cand1;
+        uint32_t* const lock_cur = cur ? lock1 : lock0;
+        uint32_t* const lock_nxt = cur ? lock0 : lock1;
+        uint32_t* const mark_nxt = cur ? mark0 : mark1;
+        const int nc = n_cand[cur];             // final since the last barrier; equal in every thread
+        if (nc == 0) { converged = true; break; }
+        if (nc > cand_cur.cap()) {
+            if (tid == 0) set_err(err, ERRF_BOUNDS);
+            break;
         }
-        if (tid == 0) n_wl[nxt] = 0;       // nobody appends to it before phase C2
-        __syncthreads();
-        const int ncand = n_cand;
-        if (ncand == 0) { converged = true; break; }
-        const int nc = min(ncand, cand.cap());
-        if (tid == 0 && ncand > cand.cap()) { set_err(err, ERRF_BOUNDS); stop = 1; }
-        // B: flip the winners
+        // B: flip the winners; release the previous round's locks; clear the next round's bitset
+        m.llock = lock_cur;
         for (int c = tid; c < nc; c += NT) {
-            const int32_t* cc = cand.slot(c);
+            const int32_t* cc = cand_cur.slot(c);
             int h = cc[0], n = cc[1];
             if (flip_apply(m, h, n, uint32_t(round))) {
                 int f = agg_inc(&n_flip);     // at most T/2 <= flips.cap()
@@ -560,49 +651,91 @@ __global__ void __launch_bounds__(1024) k_flip_local(DelDev d0, DelDev d1, int m
                 q[0] = h / 3; q[1] = n;
             }
         }
+        for (int c = tid; c < nc_prev; c += NT) {
+            const int32_t* cc = cand_nxt.slot(c);
+            lock_nxt[cc[0] / 3] = LOCK_FREE;
+            lock_nxt[cc[1]] = LOCK_FREE;
+        }
+        for (int i = tid; i < LOC_MARK; i += NT) mark_nxt[i] = 0u;
         __syncthreads();
         const int nf = n_flip;
-        // C1: resolve the outer neighbours (read only)
+        auto add_next = [&](int hh, int nn, uint32_t p) {
+            atomicMin(lock_nxt + hh / 3, p);
+            atomicMin(lock_nxt + nn, p);
+            int idx = agg_inc(&n_cand[nxt]);
+            if (idx < cand_nxt.cap()) { int32_t* c = cand_nxt.slot(idx); c[0] = hh; c[1] = nn; }
+        };
+        // C1: resolve the outer neighbours (read only); propose the outer edges.
+        // The four edges of a pair go through each step together (claims,
+        // tests, one list reservation per warp), so their latencies overlap.
         for (int f = tid; f < nf; f += NT) {
             int32_t* q = flips.slot(f);
-            int t = q[0], n = q[1];
+            const int t = q[0], n = q[1];
+            int r[4], c[4], tw[4];
+#pragma unroll
             for (int k = 0; k < 4; ++k) {
-                int r = flip_resolve_slot(m, outer_slot(t, n, k), uint32_t(round), T);
-                if (r == -2) { set_err(err, ERRF_BOUNDS); r = -1; }
-                q[2 + k] = r;
+                r[k] = flip_resolve_slot(m, outer_slot(t, n, k), uint32_t(round), T);
+                if (r[k] == -2) { set_err(err, ERRF_BOUNDS); r[k] = -1; }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) q[2 + k] = r[k];
+            uint32_t old[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int x = outer_slot(t, n, k);
+                c[k] = min(x, r[k]);
+                tw[k] = c[k] == x ? r[k] : x;
+                old[k] = r[k] >= 0 ? atomicOr(mark_nxt + (c[k] >> 5), 1u << (c[k] & 31)) : ~0u;
+            }
+            unsigned want = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (!(old[k] & (1u << (c[k] & 31))) && edge_flippable(m, c[k], tw[k])) want |= 1u << k;
+            // reserve popc(want) entries per lane with one atomic per warp
+            const unsigned act = __activemask();
+            const int lane = tid & 31, cnt = __popc(want);
+            const unsigned b0 = __ballot_sync(act, cnt & 1), b1 = __ballot_sync(act, cnt & 2),
+                           b2 = __ballot_sync(act, cnt & 4);
+            const unsigned lt = (1u << lane) - 1u;
+            const int before = __popc(b0 & lt) + 2 * __popc(b1 & lt) + 4 * __popc(b2 & lt);
+            const int total = __popc(b0) + 2 * __popc(b1) + 4 * __popc(b2);
+            const int leader = __ffs(act) - 1;
+            int base = 0;
+            if (lane == leader && total > 0) base = atomicAdd(&n_cand[nxt], total);
+            base = __shfl_sync(act, base, leader) + before;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (!(want & (1u << k))) continue;
+                const uint32_t p = prio(uint32_t(c[k]), uint32_t(round + 1));
+                atomicMin(lock_nxt + c[k] / 3, p);
+                atomicMin(lock_nxt + tw[k] / 3, p);
+                if (base < cand_nxt.cap()) { int32_t* e = cand_nxt.slot(base); e[0] = c[k]; e[1] = tw[k] / 3; }
+                ++base;
             }
         }
         __syncthreads();
-        // C2: relink, queue the outer edges, release locks, requeue lost proposals
-        auto push = [&](int x) {
-            int idx = agg_inc(&n_wl[nxt]);
-            if (idx < wl[nxt].cap()) *wl[nxt].slot(idx) = x;
-        };
+        // C2: relink; re-propose the lost proposals (their edges are no outer
+        // edge of a flipped pair, so the bitset need not see them)
+        if (tid == 0) { n_flip = 0; n_cand[cur] = 0; }   // both were read before the last barrier
         for (int f = tid; f < nf; f += NT) {
             int32_t* q = flips.slot(f);
-            int t = q[0], n = q[1];
-            flip_relink(m, t, n, q + 2);
-            for (int k = 0; k < 4; ++k) push(outer_slot(t, n, k));
+            flip_relink(m, q[0], q[1], q + 2);
         }
         for (int c = tid; c < nc; c += NT) {
-            const int32_t* cc = cand.slot(c);
-            int h = cc[0], n = cc[1], t = h / 3;
-            m.llock[t] = LOCK_FREE;
-            m.llock[n] = LOCK_FREE;
-            if (m.fround(t) != round && m.fround(n) != round) push(h);
+            const int32_t* cc = cand_cur.slot(c);
+            const int h = cc[0], n = cc[1], t = h / 3;
+            if (m.fround(t) != round && m.fround(n) != round) add_next(h, n, prio(uint32_t(h), uint32_t(round + 1)));
         }
         flips_total += nf;
+        nc_prev = nc;
         __syncthreads();
-        if (tid == 0) {
-            n_cand = 0;
-            n_flip = 0;
-            if (n_wl[nxt] > wl[nxt].cap()) { set_err(err, ERRF_BOUNDS); stop = 1; }
-        }
-        __syncthreads();
-        if (stop) break;
     }
-    for (int t = tid; t < T; t += NT)
-        for (int k = 0; k < 3; ++k) D.tri[3 * t + k] = m.lv[3 * t + k];
+    __syncthreads();
+    for (int t = tid; t < T; t += NT) {
+        int32_t v[3] = {m.lv[3 * t], m.lv[3 * t + 1], m.lv[3 * t + 2]};
+        normalise(v);
+        for (int k = 0; k < 3; ++k) D.tri[3 * t + k] = v[k];
+    }
     if (tid == 0) {
         D.ctr[8] = 1;
         D.ctr[4] = round + 1;
@@ -624,10 +757,11 @@ struct ClusterSync {
 // skipped; the kernel that handles a problem sets ctr[8].
 __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, int csize, int max_rounds,
                                                           unsigned* err) {
+    grid_dep_wait();
     using Acc = ClusterTri;
     using Sync = ClusterSync;
     extern __shared__ __align__(16) uint8_t csm[];
-    __shared__ int n_cand[2], n_flip, n_wl[2], stop;
+    __shared__ int n_cand[2], n_flip, n_wl[2], stop, s_flips;
     Sync sync;
     const int rank = sync.rank();
     const int prob = blockIdx.x / csize;
@@ -643,6 +777,9 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, 
     m.lopp = reinterpret_cast<int32_t*>(m.lxy + 3 * SLICE_MAX);
     m.llock = reinterpret_cast<uint32_t*>(m.lopp + 3 * SLICE_MAX);
     m.lround = reinterpret_cast<int32_t*>(m.llock + SLICE_MAX);
+    uint32_t* const mark0 = reinterpret_cast<uint32_t*>(m.lround + SLICE_MAX);
+    uint32_t* const mark1 = mark0 + CL_MARK;
+    int32_t* const ring = reinterpret_cast<int32_t*>(mark1 + CL_MARK);
     m.shift = shift;
     m.mask = (1 << shift) - 1;
     const int t0 = rank << shift, t1 = min(T, (rank + 1) << shift);
@@ -660,7 +797,8 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, 
     }
     if (tid == 0) { n_cand[0] = n_cand[1] = 0; n_flip = 0; n_wl[0] = n_wl[1] = 0; stop = 0; }
     // per-CTA list regions in global memory
-    int32_t* wl[2] = {D.cwl + size_t(rank) * 2 * WL_PER_CTA, D.cwl + size_t(rank) * 2 * WL_PER_CTA + WL_PER_CTA};
+    int32_t* const wl0 = D.cwl + size_t(rank) * 2 * WL_PER_CTA;
+    int32_t* const wl1 = wl0 + WL_PER_CTA;
     int32_t* cand = D.ccand + size_t(rank) * 2 * CAND_PER_CTA;
     int32_t* flips = D.cflips + size_t(rank) * 6 * FLIP_PER_CTA;
     sync();
@@ -668,16 +806,24 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, 
     bool converged = false;
     for (; round < max_rounds; ++round) {
         const int cur = round & 1, nxt = cur ^ 1;
-        // A: propose (round 0: every own half-edge, owner rule)
-        const int items = round == 0 ? 3 * (t1 - t0) : min(n_wl[cur], WL_PER_CTA);
+        // A: propose (round 0: every interior edge of the own slice once; later: the worklist)
         auto add_cand = [&](int hh, int nn) {
             int idx = agg_inc(&n_cand[cur]);
             if (idx < CAND_PER_CTA) { cand[2 * idx] = hh; cand[2 * idx + 1] = nn; }
         };
-        for (int k = tid; k < items; k += CL_THREADS) {
-            int h = round == 0 ? 3 * t0 + k : wl[cur][k];
-            if (!flip_propose(m, h, T, uint32_t(round), round == 0, add_cand)) set_err(err, ERRF_BOUNDS);
+        auto prop = [&](int h) {
+            if (!flip_propose(m, h, T, uint32_t(round), false, add_cand)) set_err(err, ERRF_BOUNDS);
+        };
+        if (round == 0) {
+            propose_owned(3 * t0, 3 * t1, ring + 64 * (tid >> 5), [&](int h) { return m.opp(h); }, prop);
+        } else {
+            const int items = min(n_wl[cur], WL_PER_CTA);
+            const int32_t* wl_cur = cur ? wl1 : wl0;
+            for (int k = tid; k < items; k += CL_THREADS) prop(wl_cur[k]);
         }
+        // this round's push bitset was last used two rounds ago
+        uint32_t* const mark_nxt = cur ? mark0 : mark1;
+        for (int i = tid; i < CL_MARK; i += CL_THREADS) mark_nxt[i] = 0u;
         if (tid == 0) n_wl[nxt] = 0;       // nobody appends to it before phase C2
         sync();
         int total = 0;
@@ -706,22 +852,27 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, 
         }
         sync();
         // C2: relink, queue the outer edges at their owners, release locks, requeue lost proposals
-        auto push = [&](int x) {
-            int t = x / 3;
-            int* cnt = sync.remote(&n_wl[nxt], t >> shift);
+        // the edge's bit and list entry live at the CTA that owns its lower half-edge
+        auto push = [&](int x, int r) {
+            if (r < 0) return;
+            const int c = min(x, r), owner = (c / 3) >> shift;
+            const int lb = c - 3 * (owner << shift);
+            const uint32_t bit = 1u << (lb & 31);
+            if (atomicOr(sync.remote(mark_nxt, owner) + (lb >> 5), bit) & bit) return;
+            int* cnt = sync.remote(&n_wl[nxt], owner);
             int idx = agg_inc_keyed(cnt);
-            if (idx < WL_PER_CTA) D.cwl[size_t(t >> shift) * 2 * WL_PER_CTA + size_t(nxt) * WL_PER_CTA + idx] = x;
+            if (idx < WL_PER_CTA) D.cwl[size_t(owner) * 2 * WL_PER_CTA + size_t(nxt) * WL_PER_CTA + idx] = c;
         };
         for (int f = tid; f < nf; f += CL_THREADS) {
             int t = flips[6 * f], n = flips[6 * f + 1];
             flip_relink(m, t, n, flips + 6 * f + 2);
-            for (int k = 0; k < 4; ++k) push(outer_slot(t, n, k));
+            for (int k = 0; k < 4; ++k) push(outer_slot(t, n, k), flips[6 * f + 2 + k]);
         }
         for (int c = tid; c < nc; c += CL_THREADS) {
             int h = cand[2 * c], n = cand[2 * c + 1], t = h / 3;
             *(m.at(m.llock, t) + (t & m.mask)) = LOCK_FREE;
             *(m.at(m.llock, n) + (n & m.mask)) = LOCK_FREE;
-            if (m.fround(t) != round && m.fround(n) != round) push(h);
+            if (m.fround(t) != round && m.fround(n) != round) push(h, m.opp(h));
         }
         flips_total += nf;
         if (tid == 0) { n_cand[nxt] = 0; n_flip = 0; }
@@ -735,29 +886,30 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, 
         if (any_stop) break;
     }
     // write back this CTA's slice
-    for (int t = t0 + tid; t < t1; t += CL_THREADS)
-        for (int k = 0; k < 3; ++k) D.tri[3 * t + k] = m.lv[3 * (t - t0) + k];
+    for (int t = t0 + tid; t < t1; t += CL_THREADS) {
+        const int l = t - t0;
+        int32_t v[3] = {m.lv[3 * l], m.lv[3 * l + 1], m.lv[3 * l + 2]};
+        normalise(v);
+        for (int k = 0; k < 3; ++k) D.tri[3 * t + k] = v[k];
+    }
+    if (tid == 0) s_flips = flips_total;
+    sync();
     if (rank == 0 && tid == 0) {
+        int total = 0;
+        for (int r = 0; r < csize; ++r) total += *sync.remote(&s_flips, r);
         D.ctr[8] = 1;
         D.ctr[4] = round + 1;
-        D.ctr[5] = flips_total;
+        D.ctr[5] = total;
         if (!converged) set_err(err, ERRF_FLIP_LIMIT);
     }
     sync();   // keep every CTA's shared memory alive until remote readers are done
-}
-
-__global__ void k_normalise(DelDev d0, DelDev d1) {
-    const DelDev& D = blockIdx.y ? d1 : d0;
-    const int T = D.ctr[0];
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x)
-        normalise(D.tri + 3 * size_t(t));
 }
 
 }  // namespace
 
 int cluster_size_for_flip() {
     int sizes[2] = {16, 8};
-    size_t smem = size_t(SLICE_MAX) * 44;
+    size_t smem = CL_SMEM;
     cudaFuncSetAttribute(k_flip_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     cudaFuncSetAttribute(k_flip_smem, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     for (int cs : sizes) {
@@ -781,26 +933,26 @@ int cluster_size_for_flip() {
 
 cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int nmax, int num_sms,
                             int csize, unsigned* err, cudaStream_t st, int* nlaunch) {
-    k_rowsort<<<dim3(nrows, 2), 512, 0, st>>>(d0, d1, row_off, nrows, err);
+    launch_k(k_rowsort, dim3(nrows, 2), 512, 0, st, d0, d1, row_off, nrows, err);
     int smem_rows = imin(nrows, (96 * 1024) / 56);     // 2 sides x (index, x, y, 4-int stack records)
     size_t smem = size_t(smem_rows) * 56;
     cudaFuncSetAttribute(k_plan, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    k_plan<<<2, 1024, smem, st>>>(d0, d1, row_off, nrows, smem_rows, err);
+    launch_k(k_plan, 2, 1024, smem, st, d0, d1, row_off, nrows, smem_rows, err);
     int blocks = 4 * num_sms;
-    k_strips<<<dim3(imax(1, imin(blocks, (nmax + 255) / 256)), 2), 256, 0, st>>>(d0, d1, row_off, nmax);
-    k_hash_clear<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1);
-    k_hash_insert<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1, err);
-    k_link<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1, err);
+    launch_k(k_strips, dim3(imax(1, imin(blocks, (nmax + 255) / 256)), 2), 256, 0, st, d0, d1, row_off, nmax);
+    launch_k(k_hash_clear, dim3(blocks, 2), 256, 0, st, d0, d1);
+    launch_k(k_hash_insert, dim3(blocks, 2), 256, 0, st, d0, d1, err);
+    launch_k(k_link, dim3(blocks, 2), 256, 0, st, d0, d1, err);
     int launched = 6;
     const int max_rounds = 100000;
     cudaFuncSetAttribute(k_flip_local, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LOC_SMEM));
-    k_flip_local<<<2, 1024, LOC_SMEM, st>>>(d0, d1, max_rounds, err);
+    launch_k(k_flip_local, 2, 1024, LOC_SMEM, st, d0, d1, max_rounds, err);
     ++launched;
     if (csize > 0) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(2 * csize);
         cfg.blockDim = dim3(CL_THREADS);
-        cfg.dynamicSmemBytes = size_t(SLICE_MAX) * 44;
+        cfg.dynamicSmemBytes = CL_SMEM;
         cfg.stream = st;
         cudaLaunchAttribute attr;
         attr.id = cudaLaunchAttributeClusterDimension;
@@ -813,10 +965,10 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
         if (e != cudaSuccess) return e;
         ++launched;
     }
-    k_tri_xy<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1);
-    k_flip_global<<<2, FLIP_THREADS, 0, st>>>(d0, d1, max_rounds, err);
-    k_normalise<<<dim3(blocks, 2), 256, 0, st>>>(d0, d1);
-    launched += 3;
+    // the fallback packs the corner coordinates itself; every flip kernel
+    // writes its triangles rotated to start at their smallest vertex index
+    launch_k(k_flip_global, 2, FLIP_THREADS, 0, st, d0, d1, max_rounds, err);
+    ++launched;
     if (nlaunch) *nlaunch += launched;
     return cudaGetLastError();
 }

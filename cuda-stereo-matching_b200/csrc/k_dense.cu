@@ -24,6 +24,7 @@
 // Strict '<' keeps the first minimum in that order, as the reference does.
 #include <cuda_runtime.h>
 #include "common.cuh"
+#include "launch.cuh"
 #include "kernels.h"
 
 namespace elas {
@@ -123,6 +124,7 @@ __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__
                                                      const int32_t* __restrict__ ctr1,
                                                      const int32_t* __restrict__ can, const int32_t* __restrict__ uvd,
                                                      Raster* __restrict__ rast, int Tmax, Geom g) {
+    grid_dep_wait();
     const int T0 = ctr0[0], T1 = ctr1[0];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T0 + T1; i += gridDim.x * blockDim.x) {
         const bool right = i >= T0;
@@ -140,6 +142,7 @@ __global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict_
                                                       const Raster* __restrict__ rast, int Tmax,
                                                       uint32_t* prior0, uint32_t* prior1, Geom g, int pshift,
                                                       int dcap) {
+    grid_dep_wait();
     const int lane = threadIdx.x & 31;
     const int T0 = ctr0[0], T1 = ctr1[0];
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -209,6 +212,7 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
                                                const uint32_t* __restrict__ grid0, const uint32_t* __restrict__ grid1,
                                                float* __restrict__ disp0, float* __restrict__ disp1, Geom g,
                                                DevParams p, int pshift, int sub, unsigned* err) {
+    grid_dep_wait();
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ uint64_t bar;
     // sub = 1: every second row and column (output (W/2) x (H/2))
@@ -351,8 +355,12 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
 // snapshot copies, src/Elas.cu:542-546).
 // scale = 0.5 on subsampled maps: a disparity (in full-resolution pixels)
 // moves d / 2 columns there.
+// The checked maps go to O1/O2 and, where given, also to C1/C2 (the
+// buffers the post-filters then work on in place).
 __global__ void k_lr(const float* __restrict__ D1, const float* __restrict__ D2, float* __restrict__ O1,
-                     float* __restrict__ O2, int W, int H, float thr, float scale) {
+                     float* __restrict__ O2, float* __restrict__ C1, float* __restrict__ C2, int W, int H, float thr,
+                     float scale) {
+    grid_dep_wait();
     int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
     if (u >= W || v >= H) return;
     size_t a = size_t(v) * W + u;
@@ -371,6 +379,10 @@ __global__ void k_lr(const float* __restrict__ D1, const float* __restrict__ D2,
     }
     O1[a] = o1;
     O2[a] = o2;
+    if (C1) {
+        C1[a] = o1;
+        C2[a] = o2;
+    }
 }
 
 }  // namespace
@@ -382,10 +394,10 @@ cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t
     cudaMemsetAsync(prior0, 0, n, st);
     cudaMemsetAsync(prior1, 0, n, st);
     Raster* R = static_cast<Raster*>(rast);
-    k_prior_setup<<<imax(1, imin(8 * num_sms, (2 * Tmax + 255) / 256)), 256, 0, st>>>(tri0, tri1, ctr0, ctr1, can,
+    launch_k(k_prior_setup, imax(1, imin(8 * num_sms, (2 * Tmax + 255) / 256)), 256, 0, st, tri0, tri1, ctr0, ctr1, can,
                                                                                       uvd, R, Tmax, g);
     int blocks = imax(1, imin(16 * num_sms, (2 * Tmax + 7) / 8));
-    k_prior_raster<<<blocks, 256, 0, st>>>(ctr0, ctr1, R, Tmax, prior0, prior1, g, pshift, dcap);
+    launch_k(k_prior_raster, blocks, 256, 0, st, ctr0, ctr1, R, Tmax, prior0, prior1, g, pshift, dcap);
     return cudaGetLastError();
 }
 
@@ -402,20 +414,21 @@ cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t*
     const dim3 grid(g.H >> sub, 2);
     if (p.plane_radius == 2) {
         cudaFuncSetAttribute(k_dense<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        k_dense<2><<<grid, threads, smem, st>>>(desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
+        launch_k(k_dense<2>, grid, threads, smem, st, desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
                                                 pshift, sub, err);
     } else {
         cudaFuncSetAttribute(k_dense<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        k_dense<0><<<grid, threads, smem, st>>>(desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
+        launch_k(k_dense<0>, grid, threads, smem, st, desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
                                                 pshift, sub, err);
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_lr(const float* d0, const float* d1, float* o0, float* o1, const Geom& g, int lr_threshold,
-                      cudaStream_t st, int sub) {
+cudaError_t launch_lr(const float* d0, const float* d1, float* o0, float* o1, float* c0, float* c1, const Geom& g,
+                      int lr_threshold, cudaStream_t st, int sub) {
     const int W = g.W >> sub, H = g.H >> sub;
-    k_lr<<<dim3((W + 255) / 256, H), 256, 0, st>>>(d0, d1, o0, o1, W, H, float(lr_threshold), sub ? 0.5f : 1.0f);
+    launch_k(k_lr, dim3((W + 255) / 256, H), 256, 0, st, d0, d1, o0, o1, c0, c1, W, H, float(lr_threshold),
+             sub ? 0.5f : 1.0f);
     return cudaGetLastError();
 }
 

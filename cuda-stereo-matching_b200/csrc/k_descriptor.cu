@@ -16,6 +16,7 @@
 // them uninitialised.
 #include <cuda_runtime.h>
 #include "common.cuh"
+#include "launch.cuh"
 #include "kernels.h"
 
 namespace elas {
@@ -35,6 +36,7 @@ __global__ void __launch_bounds__(256) k_descriptor(const uint8_t* __restrict__ 
                                                     const uint8_t* __restrict__ img1,
                                                     uint4* __restrict__ desc0,
                                                     uint4* __restrict__ desc1, int W, int H) {
+    grid_dep_wait();
     __shared__ uint8_t im[IH][IW + 2];
     __shared__ uint8_t du[GH][GW];
     __shared__ uint8_t dv[GH][GW];
@@ -84,7 +86,7 @@ __global__ void __launch_bounds__(256) k_descriptor(const uint8_t* __restrict__ 
 cudaError_t launch_descriptor(const uint8_t* img0, const uint8_t* img1, uint4* desc0, uint4* desc1,
                               int W, int H, cudaStream_t st) {
     dim3 grid((W + TX - 1) / TX, (H + TY - 1) / TY, 2);
-    k_descriptor<<<grid, 256, 0, st>>>(img0, img1, desc0, desc1, W, H);
+    launch_k(k_descriptor, grid, 256, 0, st, img0, img1, desc0, desc1, W, H);
     return cudaGetLastError();
 }
 

@@ -17,6 +17,7 @@
 #include <mutex>
 #include "../../include/elas_b200.h"
 #include "common.cuh"
+#include "launch.cuh"
 #include "kernels.h"
 
 namespace elas {
@@ -43,6 +44,7 @@ __device__ __forceinline__ int uf_find(int32_t* lab, int x, unsigned* err) {
 // union), else at the pixel itself.
 __global__ void k_uf_init(const float* __restrict__ D, int32_t* __restrict__ lab, int32_t* __restrict__ sz, int W,
                           int H, float thr) {
+    grid_dep_wait();
     int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
     if (u >= W || v >= H) return;
     int i = v * W + u;
@@ -75,6 +77,7 @@ __device__ void uf_union(int32_t* lab, int a, int b, unsigned* err) {
 }
 
 __global__ void k_uf_union(const float* __restrict__ D, int32_t* lab, int W, int H, float thr, unsigned* err) {
+    grid_dep_wait();
     int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
     if (u >= W || v >= H) return;
     int i = v * W + u;
@@ -95,6 +98,7 @@ __global__ void k_uf_union(const float* __restrict__ D, int32_t* lab, int W, int
 // segment sizes; lanes of a warp that share a root add once (segments are
 // large, so this removes most of the contention on the root counters).
 __global__ void k_uf_count(int32_t* lab, int32_t* __restrict__ root, int32_t* sz, int n, unsigned* err) {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int r = -1;
     if (i < n && lab[i] >= 0) r = uf_find(lab, i, err);
@@ -140,6 +144,7 @@ __device__ __forceinline__ void lunion(int* L, int a, int b) {
 }
 
 __global__ void __launch_bounds__(1024) k_spk_tile(PostViews pv, int W, int H, float thr) {
+    grid_dep_wait();
     __shared__ float S[SPK_T][SPK_T];
     __shared__ int L[SPK_T * SPK_T];
     __shared__ int C[SPK_T * SPK_T];
@@ -197,6 +202,7 @@ __global__ void __launch_bounds__(1024) k_spk_tile(PostViews pv, int W, int H, f
 // Links across tile borders: item k < H * tx_n is the right border of tile
 // column k % tx_n in row k / tx_n; the rest are bottom borders.
 __global__ void k_spk_border(PostViews pv, int W, int H, float thr, unsigned* err) {
+    grid_dep_wait();
     const int view = blockIdx.z;
     const float* __restrict__ D = pv.cur[view];
     int32_t* lab = pv.lab[view];
@@ -224,6 +230,7 @@ __global__ void k_spk_border(PostViews pv, int W, int H, float thr, unsigned* er
 // Sizes: every tile-local root adds its count at its global root g and
 // keeps -(g + 1) in its size slot (only this thread reads that slot).
 __global__ void k_spk_count(PostViews pv, int n, unsigned* err) {
+    grid_dep_wait();
     const int view = blockIdx.z;
     int32_t* lab = pv.lab[view];
     int32_t* sz = pv.sz[view];
@@ -241,6 +248,7 @@ __global__ void k_spk_count(PostViews pv, int n, unsigned* err) {
 // out = in with the pixels of segments smaller than min_size set invalid:
 // a pixel's tile-local root (itself, or lab[i]) holds -(global root + 1).
 __global__ void k_spk_apply(PostViews pv, int n, int min_size) {
+    grid_dep_wait();
     const int view = blockIdx.z;
     const float* __restrict__ D = pv.cur[view];
     float* __restrict__ O = pv.nxt[view];
@@ -260,6 +268,7 @@ __global__ void k_spk_apply(PostViews pv, int n, int min_size) {
 }
 
 __global__ void k_uf_apply(float* D, const int32_t* __restrict__ root, const int32_t* sz, int n, int min_size) {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int r = root[i];
@@ -269,6 +278,7 @@ __global__ void k_uf_apply(float* D, const int32_t* __restrict__ root, const int
 // horizontal = 1: one thread per row; 0: one thread per column (used for
 // gap widths too large for the per-pixel search).
 __global__ void k_gap(PostViews pv, int W, int H, int gap, int horizontal) {
+    grid_dep_wait();
     float* D = pv.cur[blockIdx.z];
     int l = blockIdx.x * blockDim.x + threadIdx.x;
     int lines = horizontal ? H : W, len = horizontal ? W : H;
@@ -330,6 +340,7 @@ constexpr int WT_SMEM = 1024;                   // adaptive-mean weights for |di
 
 template <int G, bool GAP, bool MEAN, bool MEDIAN>
 __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, int gap) {
+    grid_dep_wait();
     constexpr int PHALO = G + 3, PS = PT + 2 * PHALO;   // S tile side
     __shared__ float WT[MEAN ? WT_SMEM : 1];
     __shared__ float S[PS][PS];                 // input, halo PHALO
@@ -441,21 +452,21 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
     };
     if (p.speckle_size > 0) {
         const dim3 tiles((W + SPK_T - 1) / SPK_T, (H + SPK_T - 1) / SPK_T, nviews);
-        k_spk_tile<<<tiles, dim3(SPK_T, SPK_T), 0, st>>>(pv, W, H, p.speckle_sim_threshold);
+        launch_k(k_spk_tile, tiles, dim3(SPK_T, SPK_T), 0, st, pv, W, H, p.speckle_sim_threshold);
         const long long border = (long long)H * (tiles.x - 1) + (long long)W * (tiles.y - 1);
         const int gb = int(border / 256 + 1 < 4096 ? border / 256 + 1 : 4096);
-        k_spk_border<<<dim3(gb, 1, nviews), 256, 0, st>>>(pv, W, H, p.speckle_sim_threshold, err);
+        launch_k(k_spk_border, dim3(gb, 1, nviews), 256, 0, st, pv, W, H, p.speckle_sim_threshold, err);
         const int gn = imax(1, imin(8 * 1024, (n + 255) / 256));
-        k_spk_count<<<dim3(gn, 1, nviews), 256, 0, st>>>(pv, n, err);
-        k_spk_apply<<<dim3(gn, 1, nviews), 256, 0, st>>>(pv, n, p.speckle_size);
+        launch_k(k_spk_count, dim3(gn, 1, nviews), 256, 0, st, pv, n, err);
+        launch_k(k_spk_apply, dim3(gn, 1, nviews), 256, 0, st, pv, n, p.speckle_size);
         flip();
         launched += 4;
     }
     const int gap = p.ipol_gap_width;
     const bool tile_gap = gap > 0 && gap <= PGMAX;
     if (gap > PGMAX) {   // wide gaps: serial scans per line, in place
-        k_gap<<<dim3((H + 127) / 128, 1, nviews), 128, 0, st>>>(pv, W, H, gap, 1);
-        k_gap<<<dim3((W + 127) / 128, 1, nviews), 128, 0, st>>>(pv, W, H, gap, 0);
+        launch_k(k_gap, dim3((H + 127) / 128, 1, nviews), 128, 0, st, pv, W, H, gap, 1);
+        launch_k(k_gap, dim3((W + 127) / 128, 1, nviews), 128, 0, st, pv, W, H, gap, 0);
         launched += 2;
     }
     if (tile_gap || adaptive_mean || median) {
@@ -463,20 +474,20 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         const int key = (tile_gap ? 4 : 0) | (adaptive_mean ? 2 : 0) | (median ? 1 : 0);
         if (!tile_gap || gap <= 3) {   // halo 6
             switch (key) {
-            case 1: k_post_tile<3, false, false, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-            case 2: k_post_tile<3, false, true, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-            case 3: k_post_tile<3, false, true, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-            case 4: k_post_tile<3, true, false, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-            case 5: k_post_tile<3, true, false, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-            case 6: k_post_tile<3, true, true, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-            default: k_post_tile<3, true, true, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+            case 1: launch_k(k_post_tile<3, false, false, true>, grid, 1024, 0, st, pv, W, H, gap); break;
+            case 2: launch_k(k_post_tile<3, false, true, false>, grid, 1024, 0, st, pv, W, H, gap); break;
+            case 3: launch_k(k_post_tile<3, false, true, true>, grid, 1024, 0, st, pv, W, H, gap); break;
+            case 4: launch_k(k_post_tile<3, true, false, false>, grid, 1024, 0, st, pv, W, H, gap); break;
+            case 5: launch_k(k_post_tile<3, true, false, true>, grid, 1024, 0, st, pv, W, H, gap); break;
+            case 6: launch_k(k_post_tile<3, true, true, false>, grid, 1024, 0, st, pv, W, H, gap); break;
+            default: launch_k(k_post_tile<3, true, true, true>, grid, 1024, 0, st, pv, W, H, gap); break;
             }
         } else {                       // gaps 4..8: halo 11
             switch (key) {
-            case 4: k_post_tile<PGMAX, true, false, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-            case 5: k_post_tile<PGMAX, true, false, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-            case 6: k_post_tile<PGMAX, true, true, false><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
-            default: k_post_tile<PGMAX, true, true, true><<<grid, 1024, 0, st>>>(pv, W, H, gap); break;
+            case 4: launch_k(k_post_tile<PGMAX, true, false, false>, grid, 1024, 0, st, pv, W, H, gap); break;
+            case 5: launch_k(k_post_tile<PGMAX, true, false, true>, grid, 1024, 0, st, pv, W, H, gap); break;
+            case 6: launch_k(k_post_tile<PGMAX, true, true, false>, grid, 1024, 0, st, pv, W, H, gap); break;
+            default: launch_k(k_post_tile<PGMAX, true, true, true>, grid, 1024, 0, st, pv, W, H, gap); break;
             }
         }
         flip();
@@ -541,10 +552,10 @@ extern "C" int elas_b200_speckle_noalloc(const float* d_in, float* d_out, int32_
     if (cudaMemsetAsync(err, 0, sizeof(unsigned), st) != cudaSuccess) return ELAS_ERR_CUDA;
     if (min_size > 0) {
         const dim3 grid2((W + tb - 1) / tb, H);
-        k_uf_init<<<grid2, tb, 0, st>>>(d_out, lab, sz, W, H, sim_threshold);
-        k_uf_union<<<grid2, tb, 0, st>>>(d_out, lab, W, H, sim_threshold, err);
-        k_uf_count<<<(n + tb - 1) / tb, tb, 0, st>>>(lab, root, sz, n, err);
-        k_uf_apply<<<(n + tb - 1) / tb, tb, 0, st>>>(d_out, root, sz, n, min_size);
+        launch_k(k_uf_init, grid2, tb, 0, st, d_out, lab, sz, W, H, sim_threshold);
+        launch_k(k_uf_union, grid2, tb, 0, st, d_out, lab, W, H, sim_threshold, err);
+        launch_k(k_uf_count, (n + tb - 1) / tb, tb, 0, st, lab, root, sz, n, err);
+        launch_k(k_uf_apply, (n + tb - 1) / tb, tb, 0, st, d_out, root, sz, n, min_size);
     }
     return cudaGetLastError() == cudaSuccess ? ELAS_OK : ELAS_ERR_CUDA;
 }

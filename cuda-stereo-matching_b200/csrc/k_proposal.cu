@@ -28,6 +28,7 @@ namespace {
 // rounding.
 __global__ void k_features(const uint4* __restrict__ desc0, const uint4* __restrict__ desc1,
                            __nv_bfloat16* __restrict__ out, int W, int Hd, int Wd) {
+    grid_dep_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, v = blockIdx.z;
     if (x >= Wd) return;
     const uint4* D = v ? desc1 : desc0;
@@ -60,6 +61,7 @@ __global__ void k_features(const uint4* __restrict__ desc0, const uint4* __restr
 }
 
 __global__ void k_bf16_to_f32(const __nv_bfloat16* __restrict__ in, float* __restrict__ out, size_t n) {
+    grid_dep_wait();
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
         out[i] = __bfloat162float(in[i]);
 }
@@ -78,6 +80,7 @@ constexpr size_t CONV_F32_SMEM = sizeof(float) * (TAPS * CH * CH + 3 * (SEG + 2)
 __global__ void __launch_bounds__(SEG * CH) k_conv_f32(const float* __restrict__ x, const float* __restrict__ mask,
                                                    const float* __restrict__ w, const float* __restrict__ b,
                                                    float* __restrict__ y, int Hd, int Wd, int relu) {
+    grid_dep_wait();
     extern __shared__ float conv_sm[];
     float* sw = conv_sm;                                                  // [TAPS*CH*CH]
     float(*sx)[SEG + 2][CH] = reinterpret_cast<float(*)[SEG + 2][CH]>(conv_sm + TAPS * CH * CH);
@@ -114,6 +117,7 @@ __global__ void __launch_bounds__(SEG * CH) k_conv_f32(const float* __restrict__
 // Wt[8 - t][co][ci] = W[t][ci][co]: the gradient of a layer input is the
 // same convolution of the output gradient with these weights.
 __global__ void k_flip_weights(const float* __restrict__ w, float* __restrict__ wt) {
+    grid_dep_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= TAPS * CH * CH) return;
     const int t = i / (CH * CH), ci = (i / CH) % CH, co = i % CH;
@@ -129,6 +133,7 @@ constexpr int WG_ROWS = 8;
 __global__ void __launch_bounds__(CH * CH) k_conv_wgrad(const float* __restrict__ x, const float* __restrict__ dy,
                                                       const float* __restrict__ y, float* __restrict__ dw,
                                                       float* __restrict__ db, int Hd, int Wd) {
+    grid_dep_wait();
     __shared__ float sx[3][SEG + 2][CH];
     __shared__ float sg[SEG][CH];
     const int n = blockIdx.z, x0 = blockIdx.x * SEG, r0 = blockIdx.y * WG_ROWS;
@@ -173,6 +178,7 @@ __global__ void __launch_bounds__(CH * CH) k_conv_wgrad(const float* __restrict_
 __global__ void k_corr_loss(const float* __restrict__ F, const int32_t* __restrict__ labels, int nlab, int Hd,
                             int Wd, int D, float inv_n, float* __restrict__ dF, float* __restrict__ loss_sum,
                             int32_t* __restrict__ correct) {
+    grid_dep_wait();
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= nlab) return;
     const int pair = labels[4 * warp], cx = labels[4 * warp + 1], cy = labels[4 * warp + 2],
@@ -251,6 +257,7 @@ __global__ void k_corr_loss(const float* __restrict__ F, const int32_t* __restri
 
 __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
                        float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1, float c2) {
+    grid_dep_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float gi = g[i];

@@ -109,6 +109,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     k_conv_tc(const __grid_constant__ CUtensorMap in_map, const __nv_bfloat16* __restrict__ wts,
               const float* __restrict__ bias, __nv_bfloat16* __restrict__ out, int Hd, int Wd, int relu,
               unsigned* err) {
+    grid_dep_wait();
     extern __shared__ uint8_t tc_raw[];
     __shared__ __align__(8) uint64_t full[STAGES];
     __shared__ __align__(8) uint64_t wbar, mbar;
@@ -230,6 +231,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 // l + 32 from the bf16 features (fp32 dot products).
 __global__ void k_topk(const __nv_bfloat16* __restrict__ F, uint32_t* __restrict__ bins, int Hd, int Wd, int cw,
                        int ch, int step, int D) {
+    grid_dep_wait();
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= cw * ch) return;
     const int u = (warp % cw) * step, v = (warp / cw) * step;
@@ -298,6 +300,7 @@ __device__ __forceinline__ int topk_slot(int x, int q) { return 4 * x + (q ^ ((x
 
 __global__ void __launch_bounds__(256) k_topk_rows(const __nv_bfloat16* __restrict__ F, uint32_t* __restrict__ bins,
                                                    int Hd, int Wd, int cw, int step, int D) {
+    grid_dep_wait();
     extern __shared__ __align__(16) uint4 frow[];
     const int vc = blockIdx.x;
     const int v = vc * step;

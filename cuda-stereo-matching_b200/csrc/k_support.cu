@@ -26,6 +26,7 @@
 // lane-by-lane merge literally and the tests compare the two.
 #include <cuda_runtime.h>
 #include "common.cuh"
+#include "launch.cuh"
 #include "kernels.h"
 #include "proposal.h"
 
@@ -157,6 +158,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_support_sweep(const uint4* __
                                                        int32_t* __restrict__ can_out, Geom g, DevParams p,
                                                        int seg, unsigned* err, const uint32_t* __restrict__ bins,
                                                        int32_t* __restrict__ stats) {
+    grid_dep_wait();
     extern __shared__ __align__(128) uint4 rows[];
     __shared__ int res[256];
     __shared__ uint64_t bar;
@@ -406,6 +408,7 @@ __global__ void __launch_bounds__(SWEEP_Q_THREADS) k_support_sweep_q(const uint4
                                                           const uint4* __restrict__ desc1,
                                                           int32_t* __restrict__ can_out, Geom g, DevParams p,
                                                           int seg, unsigned* err) {
+    grid_dep_wait();
     extern __shared__ __align__(128) uint4 rows[];
     __shared__ int res[256];
     __shared__ uint64_t bar;
@@ -494,6 +497,7 @@ __global__ void __launch_bounds__(SWEEP_Q_THREADS) k_support_sweep_q(const uint4
 // writes can_out.  The reference's bound `y < can_width`
 // (KerSupportMatches.cu:208) is kept: rows y >= cw pass through.
 __global__ void k_incon(const int32_t* __restrict__ cin, int32_t* __restrict__ cout, Geom g, DevParams p) {
+    grid_dep_wait();
     int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= g.cw || y >= g.ch) return;
     int d = cin[size_t(y) * g.cw + x];
@@ -578,6 +582,7 @@ __device__ void redundant_line(int* a, uint8_t* code, int len, int lane) {
 
 // One warp per line; horizontal = 1: rows, 0: columns.
 __global__ void k_redundant(int32_t* __restrict__ can, Geom g, int horizontal) {
+    grid_dep_wait();
     extern __shared__ int lines[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nlines = horizontal ? g.ch : g.cw;
@@ -598,6 +603,7 @@ __global__ void k_redundant(int32_t* __restrict__ can, Geom g, int horizontal) {
 
 // Count valid candidates per row.
 __global__ void k_row_count(const int32_t* __restrict__ can, int32_t* __restrict__ row_cnt, Geom g) {
+    grid_dep_wait();
     __shared__ int s;
     if (threadIdx.x == 0) s = 0;
     __syncthreads();
@@ -613,6 +619,7 @@ __global__ void k_row_count(const int32_t* __restrict__ can, int32_t* __restrict
 // corners: three corner points lead row 0 and three more form the extra
 // row ch (row_off[ch + 1] = total + 6).
 __global__ void k_row_scan(const int32_t* __restrict__ row_cnt, int32_t* __restrict__ row_off, int n, int corners) {
+    grid_dep_wait();
     __shared__ int part[1024];
     const int t = threadIdx.x;
     const int per = (n + blockDim.x - 1) / blockDim.x;
@@ -641,6 +648,7 @@ __global__ void k_row_scan(const int32_t* __restrict__ row_cnt, int32_t* __restr
 __global__ void k_compact(const int32_t* __restrict__ can, const int32_t* __restrict__ row_off,
                           int32_t* __restrict__ uvd, int32_t* __restrict__ x0, int32_t* __restrict__ x1,
                           int32_t* __restrict__ y, Geom g, int lead) {
+    grid_dep_wait();
     __shared__ int warp_tot[32];
     __shared__ int base;
     const int r = blockIdx.x;
@@ -679,6 +687,7 @@ __global__ void k_compact(const int32_t* __restrict__ can, const int32_t* __rest
 __global__ void __launch_bounds__(1024) k_corners(const int32_t* __restrict__ row_off, int32_t* __restrict__ uvd,
                                                   int32_t* __restrict__ x0, int32_t* __restrict__ x1,
                                                   int32_t* __restrict__ y, Geom g) {
+    grid_dep_wait();
     __shared__ unsigned long long best[4][32];
     const int n0 = 3, n1 = row_off[g.ch];          // regular points are [3, n1)
     const int cu[4] = {0, g.W - 1, 0, g.W - 1}, cv[4] = {0, 0, g.H - 1, g.H - 1};
@@ -725,6 +734,7 @@ __global__ void __launch_bounds__(1024) k_corners(const int32_t* __restrict__ ro
 // floor((u-d)/gs) of row floor(v/gs).
 __global__ void k_grid_load(const int32_t* __restrict__ can, uint32_t* __restrict__ t0,
                             uint32_t* __restrict__ t1, Geom g) {
+    grid_dep_wait();
     int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= g.cw || y >= g.ch) return;
     int dc = can[size_t(y) * g.cw + x];
@@ -743,6 +753,7 @@ __global__ void k_grid_load(const int32_t* __restrict__ can, uint32_t* __restric
 // One thread per (cell, word); blockIdx.z selects the view.
 __global__ void k_grid_diffuse(const uint32_t* __restrict__ t0, const uint32_t* __restrict__ t1,
                                uint32_t* __restrict__ g0, uint32_t* __restrict__ g1, Geom g) {
+    grid_dep_wait();
     const uint32_t* t = blockIdx.z ? t1 : t0;
     uint32_t* out = blockIdx.z ? g1 : g0;
     size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -784,33 +795,33 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
         qseg = (qseg + 3) & ~3;
         const int threads = imin(qseg, SWEEP_Q_THREADS / Q) * Q;
         cudaFuncSetAttribute(k_support_sweep_q<Q, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        k_support_sweep_q<Q, true><<<dim3(qsegs, rows), threads, smem, st>>>(desc0, desc1, can_lr, g, p, qseg, err);
+        launch_k(k_support_sweep_q<Q, true>, dim3(qsegs, rows), threads, smem, st, desc0, desc1, can_lr, g, p, qseg, err);
     } else if (smem <= 200 * 1024) {
         if (bins) {
             cudaFuncSetAttribute(k_support_sweep<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-            k_support_sweep<true, true><<<grid, SWEEP_THREADS, smem, st>>>(desc0, desc1, can_lr, g, p, seg, err, bins,
+            launch_k(k_support_sweep<true, true>, grid, SWEEP_THREADS, smem, st, desc0, desc1, can_lr, g, p, seg, err, bins,
                                                                            stats);
         } else {
             cudaFuncSetAttribute(k_support_sweep<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem));
-            k_support_sweep<true, false><<<grid, SWEEP_THREADS, smem, st>>>(desc0, desc1, can_lr, g, p, seg, err,
+            launch_k(k_support_sweep<true, false>, grid, SWEEP_THREADS, smem, st, desc0, desc1, can_lr, g, p, seg, err,
                                                                             nullptr, nullptr);
         }
     } else {
         if (bins)
-            k_support_sweep<false, true><<<grid, SWEEP_THREADS, 0, st>>>(desc0, desc1, can_lr, g, p, seg, err, bins,
+            launch_k(k_support_sweep<false, true>, grid, SWEEP_THREADS, 0, st, desc0, desc1, can_lr, g, p, seg, err, bins,
                                                                          stats);
         else
-            k_support_sweep<false, false><<<grid, SWEEP_THREADS, 0, st>>>(desc0, desc1, can_lr, g, p, seg, err,
+            launch_k(k_support_sweep<false, false>, grid, SWEEP_THREADS, 0, st, desc0, desc1, can_lr, g, p, seg, err,
                                                                           nullptr, nullptr);
     }
-    k_incon<<<dim3((g.cw + 127) / 128, g.ch), 128, 0, st>>>(can_lr, can, g, p);
+    launch_k(k_incon, dim3((g.cw + 127) / 128, g.ch), 128, 0, st, can_lr, can, g, p);
     {
         int wpb = 4;
         size_t sm = size_t(wpb) * g.cw * (sizeof(int) + 1);
-        k_redundant<<<(g.ch + wpb - 1) / wpb, 32 * wpb, sm, st>>>(can, g, 1);
+        launch_k(k_redundant, (g.ch + wpb - 1) / wpb, 32 * wpb, sm, st, can, g, 1);
         sm = size_t(wpb) * g.ch * (sizeof(int) + 1);
-        k_redundant<<<(g.cw + wpb - 1) / wpb, 32 * wpb, sm, st>>>(can, g, 0);
+        launch_k(k_redundant, (g.cw + wpb - 1) / wpb, 32 * wpb, sm, st, can, g, 0);
     }
     (void)can_tmp;
     return cudaGetLastError();
@@ -818,10 +829,10 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
 
 cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_off, int32_t* uvd, int32_t* x0,
                            int32_t* x1, int32_t* y, const Geom& g, cudaStream_t st, int corners) {
-    k_row_count<<<g.ch, 128, 0, st>>>(can, row_cnt, g);
-    k_row_scan<<<1, 1024, 0, st>>>(row_cnt, row_off, g.ch, corners);
-    k_compact<<<g.ch, 256, 0, st>>>(can, row_off, uvd, x0, x1, y, g, corners ? 3 : 0);
-    if (corners) k_corners<<<1, 1024, 0, st>>>(row_off, uvd, x0, x1, y, g);
+    launch_k(k_row_count, g.ch, 128, 0, st, can, row_cnt, g);
+    launch_k(k_row_scan, 1, 1024, 0, st, row_cnt, row_off, g.ch, corners);
+    launch_k(k_compact, g.ch, 256, 0, st, can, row_off, uvd, x0, x1, y, g, corners ? 3 : 0);
+    if (corners) launch_k(k_corners, 1, 1024, 0, st, row_off, uvd, x0, x1, y, g);
     return cudaGetLastError();
 }
 
@@ -830,8 +841,8 @@ cudaError_t launch_grid(const int32_t* can, uint32_t* tmp0, uint32_t* tmp1, uint
     size_t n = size_t(g.gw) * g.gh * g.words;
     cudaMemsetAsync(tmp0, 0, n * sizeof(uint32_t), st);
     cudaMemsetAsync(tmp1, 0, n * sizeof(uint32_t), st);
-    k_grid_load<<<dim3((g.cw + 127) / 128, g.ch), 128, 0, st>>>(can, tmp0, tmp1, g);
-    k_grid_diffuse<<<dim3(unsigned((n + 255) / 256), 1, 2), 256, 0, st>>>(tmp0, tmp1, grid0, grid1, g);
+    launch_k(k_grid_load, dim3((g.cw + 127) / 128, g.ch), 128, 0, st, can, tmp0, tmp1, g);
+    launch_k(k_grid_diffuse, dim3(unsigned((n + 255) / 256), 1, 2), 256, 0, st, tmp0, tmp1, grid0, grid1, g);
     return cudaGetLastError();
 }
 

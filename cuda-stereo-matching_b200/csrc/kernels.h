@@ -74,8 +74,9 @@ cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t*
                          const uint32_t* grid0, const uint32_t* grid1, float* disp0, float* disp1, const Geom& g,
                          const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads, int sub = 0);
 
-cudaError_t launch_lr(const float* d0, const float* d1, float* o0, float* o1, const Geom& g, int lr_threshold,
-                      cudaStream_t st, int sub = 0);
+// L/R check into o0/o1 and, where c0 is not null, also into c0/c1
+cudaError_t launch_lr(const float* d0, const float* d1, float* o0, float* o1, float* c0, float* c1, const Geom& g,
+                      int lr_threshold, cudaStream_t st, int sub);
 
 // Buffers of the post-filter chain, per view: the filters ping-pong between
 // cur and nxt (the chain starts in cur; the result is copied to out if it

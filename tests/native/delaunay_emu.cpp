@@ -87,7 +87,7 @@ extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const i
         if (kv.second.size() == 2) { opp[kv.second[0]] = kv.second[1]; opp[kv.second[1]] = kv.second[0]; }
         else if (kv.second.size() != 1) return -1;
     }
-    // 5. flips (k_flip_global / k_flip_cluster)
+    // 5. flips (k_flip_local / k_flip_smem / k_flip_global)
     std::vector<uint32_t> txy(3 * size_t(Tmax)), lock(Tmax, LOCK_FREE);
     std::vector<int32_t> fround(Tmax, -1), cand(6 * size_t(Tmax)), flips(6 * size_t(Tmax)), wl[2];
     wl[0].resize(6 * size_t(Tmax));
@@ -95,6 +95,7 @@ extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const i
     for (int i = 0; i < 3 * T; ++i) txy[i] = pack_xy(px[tri[i]], py[tri[i]]);
     auto amin = [](uint32_t* p, uint32_t v) { if (v < *p) *p = v; };
     FlatTri<decltype(amin)> m{tri.data(), txy.data(), opp.data(), lock.data(), fround.data(), amin};
+    std::vector<char> mark(3 * size_t(T), 0);
     int n_cur = 3 * T;
     long long rounds = 0, nflips = 0;
     for (int round = 0; round < 100000; ++round) {
@@ -123,17 +124,26 @@ extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const i
                 if (r == -2) return -1;
                 flips[6 * f + 2 + k] = r;
             }
+        // the next worklist holds each interior edge once, as its lower half-edge
         int nn = 0;
+        std::fill(mark.begin(), mark.end(), 0);
+        auto push = [&](int x, int r) {
+            if (r < 0) return;
+            const int c = std::min(x, r);
+            if (mark[c]) return;
+            mark[c] = 1;
+            nxt[nn++] = c;
+        };
         for (int f = 0; f < nf; ++f) {
             int t = flips[6 * f], n2 = flips[6 * f + 1];
             flip_relink(m, t, n2, &flips[6 * f + 2]);
-            for (int k = 0; k < 4; ++k) nxt[nn++] = outer_slot(t, n2, k);
+            for (int k = 0; k < 4; ++k) push(outer_slot(t, n2, k), flips[6 * f + 2 + k]);
         }
         for (int c = 0; c < nc; ++c) {
             int h = cand[2 * c], n2 = cand[2 * c + 1], t = h / 3;
             lock[t] = LOCK_FREE;
             lock[n2] = LOCK_FREE;
-            if (fround[t] != round && fround[n2] != round) nxt[nn++] = h;
+            if (fround[t] != round && fround[n2] != round) push(h, opp[h]);
         }
         nflips += nf;
         n_cur = nn;
@@ -142,4 +152,13 @@ extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const i
     if (T <= cap) std::memcpy(tris_out, tri.data(), sizeof(int32_t) * 3 * size_t(T));
     if (stats) { stats[0] = rounds; stats[1] = nflips; }
     return T;
+}
+
+// The flip predicates on packed coordinates, for checks against exact
+// integer arithmetic.  xy: (x, y) of a, b, c[, d].
+extern "C" long long emu_orient_p(const int32_t* xy) {
+    return orient_p(pack_xy(xy[0], xy[1]), pack_xy(xy[2], xy[3]), pack_xy(xy[4], xy[5]));
+}
+extern "C" long long emu_incircle_p(const int32_t* xy) {
+    return incircle_p(pack_xy(xy[0], xy[1]), pack_xy(xy[2], xy[3]), pack_xy(xy[4], xy[5]), pack_xy(xy[6], xy[7]));
 }

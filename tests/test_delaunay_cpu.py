@@ -115,3 +115,30 @@ def test_support_points_with_corners(emu_lib, preset):
     row_of = np.where(uvd[:, 1] == H - 1, ch, uvd[:, 1] // p.candidate_stepsize)
     for right in (0, 1):
         check_case(emu_lib, oracle.support_points(uvd, right), row_of)
+
+
+def test_packed_predicates_exact_at_the_size_limits(emu_lib):
+    """orient_p / incircle_p against Python integers over the coordinate
+    range the size limits allow: x in [-4095, 13999] (right view: u - d with
+    disp_max <= 4095, width <= 14000), y in [0, 16383] (height <= 16384)."""
+    import ctypes
+
+    emu_lib.emu_orient_p.restype = ctypes.c_longlong
+    emu_lib.emu_incircle_p.restype = ctypes.c_longlong
+    rng = np.random.default_rng(7)
+    lo, hi = np.array([-4095, 0]), np.array([13999, 16383])
+    for it in range(4000):
+        if it % 4 == 0:      # corners of the range: the largest terms
+            pts = np.stack([np.where(rng.random(2) < 0.5, lo, hi) for _ in range(4)])
+        else:
+            pts = rng.integers(lo, hi + 1, size=(4, 2))
+        pts = pts.astype(np.int32)
+        (ax, ay), (bx, by), (cx, cy), (dx, dy) = [tuple(int(v) for v in p) for p in pts]
+        o = (bx - ax) * (cy - ay) - (by - ay) * (cx - ax)
+        adx, ady, bdx, bdy, cdx, cdy = ax - dx, ay - dy, bx - dx, by - dy, cx - dx, cy - dy
+        det = (adx * (bdy * (cdx * cdx + cdy * cdy) - (bdx * bdx + bdy * bdy) * cdy)
+               - ady * (bdx * (cdx * cdx + cdy * cdy) - (bdx * bdx + bdy * bdy) * cdx)
+               + (adx * adx + ady * ady) * (bdx * cdy - bdy * cdx))
+        buf = np.ascontiguousarray(pts.reshape(-1))
+        assert emu_lib.emu_orient_p(buf.ctypes.data_as(ctypes.c_void_p)) == o
+        assert emu_lib.emu_incircle_p(buf.ctypes.data_as(ctypes.c_void_p)) == det

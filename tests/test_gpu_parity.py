@@ -340,3 +340,24 @@ def test_add_corners_parity(elas, preset, seed, D):
     uvd = g["support"]
     assert uvd[:3, :2].tolist() == [[0, 0], [W - 1, 0], [W - 1 + int(uvd[2, 2]), 0]]
     assert uvd[-3:, 1].tolist() == [H - 1, H - 1, H - 1]
+
+
+@pytest.mark.parametrize("preset", [1, 2])
+def test_flip_rounds_match_host_emulation(elas, emu_lib, preset):
+    """The flip kernels (one SM at 1242x375, a cluster at 2880x1988) take the
+    same rounds and flips as the sequential host emulation of the algorithm:
+    each round's outcome is fixed by the edge priorities, whatever the order
+    in which threads reach the lists."""
+    from test_delaunay_cpu import emu_triangulate
+
+    W, H, D = eb.synth_dims(preset)
+    L, R, _, _ = eb.synth_pair(preset, 1)
+    elas.set_params(eb.params_config(D))
+    elas.process(L, R)
+    uvd = elas.stage("support").view(np.int32).reshape(-1, 3)
+    ctr = elas.stage("del_counters").view(np.int32).reshape(2, 16)
+    for right in (0, 1):
+        xy = oracle.support_points(uvd, right)
+        tris, st = emu_triangulate(emu_lib, xy, uvd[:, 1] // 5)
+        assert ctr[right, 0] == tris.shape[0]
+        assert (ctr[right, 4], ctr[right, 5]) == (st[0], st[1]), (right, ctr[right], st)
