@@ -92,15 +92,17 @@ HD int fill_pockets(const int32_t* ci, const int32_t* cx, const int32_t* cy, int
                     int32_t* tri) {
     // the two top stack entries are kept in registers: (a, b) = stack[sp-2], stack[sp-1]
     int sp = 0, k = 0;
+    // orientations are exact in int32 within the library's coordinate range
+    // (|dx| <= 18094, |dy| <= 16383, see orient_p)
     int32_t ia = 0, ib = 0;
-    int64_t ax = 0, ay = 0, bx = 0, by = 0;
+    int32_t ax = 0, ay = 0, bx = 0, by = 0;
     int32_t nx = len > 0 ? cx[0] : 0, ny = len > 0 ? cy[0] : 0, ni = len > 0 ? ci[0] : 0;
     for (int i = 0; i < len; ++i) {
-        const int64_t x = nx, y = ny;
+        const int32_t x = nx, y = ny;
         const int32_t ii = ni;
         if (i + 1 < len) { nx = cx[i + 1]; ny = cy[i + 1]; ni = ci[i + 1]; }
         while (sp >= 2) {
-            const int64_t o = (bx - ax) * (y - ay) - (by - ay) * (x - ax);
+            const int32_t o = (bx - ax) * (y - ay) - (by - ay) * (x - ax);
             if (side > 0 ? (o > 0) : (o < 0)) {
                 tri[3 * k] = ia;
                 tri[3 * k + 1] = side > 0 ? ib : ii;
@@ -117,7 +119,7 @@ HD int fill_pockets(const int32_t* ci, const int32_t* cx, const int32_t* cy, int
             }
         }
         int32_t* e = stack + 4 * sp;
-        e[0] = ii; e[1] = int32_t(x); e[2] = int32_t(y); e[3] = 0;
+        e[0] = ii; e[1] = x; e[2] = y; e[3] = 0;
         ++sp;
         ia = ib; ax = bx; ay = by;
         ib = ii; bx = x; by = y;

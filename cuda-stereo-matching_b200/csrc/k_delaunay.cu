@@ -190,13 +190,13 @@ __global__ void __launch_bounds__(512) k_rowsort(DelDev d0, DelDev d1, const int
     }
 }
 
-// Non-empty rows (list + rank), strip offsets and the two hull pockets.
-// One 1024-thread block per problem; dynamic shared memory holds the chain
-// (index, x, y) and the stack of the pocket walk when it fits.
+// Non-empty rows (list + rank) and strip offsets.  One 1024-thread block
+// per problem.  ctr[7] = 1 when the plan holds (two non-empty rows at least,
+// strips and pockets within Tmax); the strips and pockets are then built by
+// k_strips, which also sets the triangle count ctr[0].
 __global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off,
-                                               int nrows, int smem_rows, unsigned* err) {
+                                               int nrows, unsigned* err) {
     grid_dep_wait();
-    extern __shared__ int32_t sh[];
     __shared__ int ws[33];
     DelDev D = blockIdx.x ? d1 : d0;
     int R = 0, total = 0;
@@ -218,63 +218,75 @@ __global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32
         if (s < R - 1) D.soff[s] = off + pos;
         off += total;
     }
-    // the two pockets are walked at once by lanes 0 of warps 0 and 1, each on
-    // its own copy of the chain; the right side writes behind the left one's
-    // room (at most R-2 triangles) and is moved down when both are done
-    const bool in_smem = R <= smem_rows;
-    const int cap = in_smem ? smem_rows : nrows;
-    int pockets = 0;
-    __shared__ int npk[2];
-    if (R >= 2 && off + 2 * R > D.Tmax) {
-        if (threadIdx.x == 0) set_err(err, ERRF_TRI_COUNT);
-    } else if (R >= 2) {
-        for (int e = threadIdx.x; e < 2 * R; e += blockDim.x) {
-            const int side = e >= R, s = e - side * R;
-            int32_t* ci = (in_smem ? sh : D.chain) + side * 7 * cap;
-            const int r = D.ne[s];
-            const int i = D.srt[row_off[r] + (side ? D.rcnt[r] - 1 : 0)];
-            ci[s] = i; ci[cap + s] = D.x[i]; ci[2 * cap + s] = D.y[i];
-        }
-        __syncthreads();
-        if ((threadIdx.x & 31) == 0 && threadIdx.x < 64) {
-            const int side = threadIdx.x >> 5;
-            int32_t* ci = (in_smem ? sh : D.chain) + side * 7 * cap;
-            npk[side] = fill_pockets(ci, ci + cap, ci + 2 * cap, R, side ? -1 : +1, ci + 3 * cap,
-                                     D.tri + 3 * size_t(off + side * R));
-        }
-        __syncthreads();
-        const int k0 = npk[0], k1 = npk[1];
-        // move the right side's triangles from off+R to off+k0 (k0 <= R-2, so
-        // a forward copy in rounds of one block never overwrites unread data)
-        for (int b0 = 0; b0 < 3 * k1; b0 += blockDim.x) {
-            const int j = b0 + threadIdx.x;
-            int32_t v = 0;
-            if (j < 3 * k1) v = D.tri[3 * size_t(off + R) + j];
-            __syncthreads();
-            if (j < 3 * k1) D.tri[3 * size_t(off + k0) + j] = v;
-            __syncthreads();
-        }
-        pockets = k0 + k1;
-    }
     if (threadIdx.x == 0) {
-        D.ctr[0] = (R >= 2 && off + 2 * R <= D.Tmax) ? off + pockets : 0;
+        const bool fits = off + 2 * R <= D.Tmax;
+        if (R >= 2 && !fits) set_err(err, ERRF_TRI_COUNT);
+        D.ctr[0] = 0;
         D.ctr[1] = off;
         D.ctr[6] = R;
+        D.ctr[7] = (R >= 2 && fits) ? 1 : 0;
         D.ctr[8] = 0;    // set to 1 by the flip kernel that handles the problem
         D.ctr[9] = row_off[nrows];   // support points (vertex ids) of the problem
     }
 }
 
-// One thread per sorted point of a non-empty row: the point's triangle in
-// the strip below its row (as the upper row) and in the strip above (as the
-// lower row), placed by merge path.
-__global__ void k_strips(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off, int nmax) {
+// The two hull pockets of one problem, walked at once by lanes 0 of warps 0
+// and 1, each on its own copy of the chain (in `sh` when R <= smem_rows,
+// else in D.chain); the right side writes behind the left one's room (at
+// most R-2 triangles) and is moved down when both are done.  Sets ctr[0].
+__device__ void pocket_block(const DelDev& D, const int32_t* __restrict__ row_off, int nrows, int smem_rows,
+                             int32_t* sh) {
+    __shared__ int npk[2];
+    const int R = D.ctr[6], off = D.ctr[1];
+    const bool in_smem = R <= smem_rows;
+    const int cap = in_smem ? smem_rows : nrows;
+    for (int e = threadIdx.x; e < 2 * R; e += blockDim.x) {
+        const int side = e >= R, s = e - side * R;
+        int32_t* ci = (in_smem ? sh : D.chain) + side * 7 * cap;
+        const int r = D.ne[s];
+        const int i = D.srt[row_off[r] + (side ? D.rcnt[r] - 1 : 0)];
+        ci[s] = i; ci[cap + s] = D.x[i]; ci[2 * cap + s] = D.y[i];
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0 && threadIdx.x < 64) {
+        const int side = threadIdx.x >> 5;
+        int32_t* ci = (in_smem ? sh : D.chain) + side * 7 * cap;
+        npk[side] = fill_pockets(ci, ci + cap, ci + 2 * cap, R, side ? -1 : +1, ci + 3 * cap,
+                                 D.tri + 3 * size_t(off + side * R));
+    }
+    __syncthreads();
+    const int k0 = npk[0], k1 = npk[1];
+    // move the right side's triangles from off+R to off+k0 (k0 <= R-2, so
+    // a forward copy in rounds of one block never overwrites unread data)
+    for (int b0 = 0; b0 < 3 * k1; b0 += blockDim.x) {
+        const int j = b0 + threadIdx.x;
+        int32_t v = 0;
+        if (j < 3 * k1) v = D.tri[3 * size_t(off + R) + j];
+        __syncthreads();
+        if (j < 3 * k1) D.tri[3 * size_t(off + k0) + j] = v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) D.ctr[0] = off + k0 + k1;
+}
+
+// Blocks [0, gridDim.x - 1): one thread per sorted point of a non-empty
+// row: the point's triangle in the strip below its row (as the upper row)
+// and in the strip above (as the lower row), placed by merge path.  The last
+// block walks the problem's two hull pockets meanwhile.
+__global__ void k_strips(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off, int nrows, int nmax,
+                         int smem_rows) {
     grid_dep_wait();
+    extern __shared__ int32_t sh[];
     const DelDev& D = blockIdx.y ? d1 : d0;
+    if (D.ctr[7] == 0) return;
+    if (blockIdx.x == gridDim.x - 1) {
+        pocket_block(D, row_off, nrows, smem_rows, sh);
+        return;
+    }
     const int R = D.ctr[6];
-    if (D.ctr[0] == 0) return;
     Pts P{D.x, D.y};
-    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nmax; g += gridDim.x * blockDim.x) {
+    const int nb = gridDim.x - 1;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nmax; g += nb * blockDim.x) {
         // g walks the support index space; map it to (row, position) through the row offsets
         int lo = 0, hi = R;    // find the non-empty row whose range holds g
         // rows are in support-index order, so binary search ne by row_off
@@ -683,14 +695,19 @@ __global__ void __launch_bounds__(1024) k_flip_local(DelDev d0, DelDev d1, int m
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const int x = outer_slot(t, n, k);
-                c[k] = min(x, r[k]);
-                tw[k] = c[k] == x ? r[k] : x;
+                // a hull edge (r < 0) tests against its own triangle, is never claimed, and is masked out
+                c[k] = r[k] >= 0 ? min(x, r[k]) : x;
+                tw[k] = r[k] >= 0 ? (c[k] == x ? r[k] : x) : x;
                 old[k] = r[k] >= 0 ? atomicOr(mark_nxt + (c[k] >> 5), 1u << (c[k] & 31)) : ~0u;
             }
+            // the four tests are independent (no branch between them), so their loads overlap
+            bool flippable[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) flippable[k] = edge_flippable(m, c[k], tw[k]);
             unsigned want = 0;
 #pragma unroll
             for (int k = 0; k < 4; ++k)
-                if (!(old[k] & (1u << (c[k] & 31))) && edge_flippable(m, c[k], tw[k])) want |= 1u << k;
+                if (!(old[k] & (1u << (c[k] & 31))) && flippable[k]) want |= 1u << k;
             // reserve popc(want) entries per lane with one atomic per warp
             const unsigned act = __activemask();
             const int lane = tid & 31, cnt = __popc(want);
@@ -934,12 +951,15 @@ int cluster_size_for_flip() {
 cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int nmax, int num_sms,
                             int csize, unsigned* err, cudaStream_t st, int* nlaunch) {
     launch_k(k_rowsort, dim3(nrows, 2), 512, 0, st, d0, d1, row_off, nrows, err);
-    int smem_rows = imin(nrows, (96 * 1024) / 56);     // 2 sides x (index, x, y, 4-int stack records)
-    size_t smem = size_t(smem_rows) * 56;
-    cudaFuncSetAttribute(k_plan, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    launch_k(k_plan, 2, 1024, smem, st, d0, d1, row_off, nrows, smem_rows, err);
+    launch_k(k_plan, 2, 1024, 0, st, d0, d1, row_off, nrows, err);
+    // the pocket walk's chain and stack (2 sides x (index, x, y, 4-int stack
+    // records) = 56 bytes a row) in shared memory up to 32 KiB; every block
+    // of k_strips carries it
+    const int smem_rows = imin(nrows, (32 * 1024) / 56);
+    const size_t smem = size_t(smem_rows) * 56;
     int blocks = 4 * num_sms;
-    launch_k(k_strips, dim3(imax(1, imin(blocks, (nmax + 255) / 256)), 2), 256, 0, st, d0, d1, row_off, nmax);
+    launch_k(k_strips, dim3(imax(1, imin(blocks, (nmax + 255) / 256)) + 1, 2), 256, smem, st, d0, d1, row_off,
+             nrows, nmax, smem_rows);
     launch_k(k_hash_clear, dim3(blocks, 2), 256, 0, st, d0, d1);
     launch_k(k_hash_insert, dim3(blocks, 2), 256, 0, st, d0, d1, err);
     launch_k(k_link, dim3(blocks, 2), 256, 0, st, d0, d1, err);
@@ -965,10 +985,14 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
         if (e != cudaSuccess) return e;
         ++launched;
     }
-    // the fallback packs the corner coordinates itself; every flip kernel
-    // writes its triangles rotated to start at their smallest vertex index
-    launch_k(k_flip_global, 2, FLIP_THREADS, 0, st, d0, d1, max_rounds, err);
-    ++launched;
+    // The fallback, for triangulations larger than a cluster holds; not
+    // launched when none can be (at most 2 * nmax + 16 triangles).  It packs
+    // the corner coordinates itself; every flip kernel writes its triangles
+    // rotated to start at their smallest vertex index.
+    if (csize == 0 || 2LL * nmax + 16 > (long long)csize * SLICE_MAX) {
+        launch_k(k_flip_global, 2, FLIP_THREADS, 0, st, d0, d1, max_rounds, err);
+        ++launched;
+    }
     if (nlaunch) *nlaunch += launched;
     return cudaGetLastError();
 }
