@@ -487,21 +487,28 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
                     prior_shift(g, dp), h->err, st, shape, sub));
     n += 1;
     CK(mark(ELAS_TIME_LR));
-    // the checked maps also land in the outputs, where the post-filters work in place
-    CK(launch_lr(h->raw0, h->raw1, h->lr0, h->lr1, out0, out1, g, p.lr_threshold, st, sub));
+    // The checked maps also land where the post-filter chain starts: in the
+    // outputs, or, when the chain's first pass cannot work in place (speckle
+    // removal applied inside the tile filter), in the scratch maps, so that
+    // the last pass writes the outputs.
+    const int nviews = p.postprocess_only_left ? 1 : 2;
+    const bool from_tmp = post_fuses_speckle(dp, p.filter_median, p.filter_adaptive_mean);
+    float* outs[2] = {out0, out1};
+    float* start[2];
+    for (int k = 0; k < 2; ++k) start[k] = from_tmp && k < nviews ? h->tmp[k] : outs[k];
+    CK(launch_lr(h->raw0, h->raw1, h->lr0, h->lr1, start[0], start[1], g, p.lr_threshold, st, sub));
     n += 1;
     CK(mark(ELAS_TIME_POST));
     PostViews pv;
-    float* outs[2] = {out0, out1};
     for (int k = 0; k < 2; ++k) {
-        pv.cur[k] = outs[k];
-        pv.nxt[k] = h->tmp[k];
+        pv.cur[k] = start[k];
+        pv.nxt[k] = start[k] == outs[k] ? h->tmp[k] : outs[k];
         pv.out[k] = outs[k];
         pv.lab[k] = h->lab[k];
         pv.root[k] = h->root[k];
         pv.sz[k] = h->usize[k];
     }
-    CK(launch_post(pv, p.postprocess_only_left ? 1 : 2, go, dp, p.filter_median, p.filter_adaptive_mean, h->err, st,
+    CK(launch_post(pv, nviews, go, dp, p.filter_median, p.filter_adaptive_mean, h->err, st,
                    &n));
     CK(mark(ELAS_TIME_COUNT));
     h->launches += n;

@@ -338,8 +338,11 @@ __device__ __forceinline__ void sort9(float* a) {
 
 constexpr int WT_SMEM = 1024;                   // adaptive-mean weights for |diff| = k/4, k < 1024
 
+// spk_min > 0: the input is the L/R result before speckle removal, and
+// every loaded pixel goes through the speckle decision of k_spk_apply
+// (segments smaller than spk_min become invalid) on the way in.
 template <int G, bool GAP, bool MEAN, bool MEDIAN>
-__global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, int gap) {
+__global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, int gap, int spk_min) {
     grid_dep_wait();
     constexpr int PHALO = G + 3, PS = PT + 2 * PHALO;   // S tile side
     __shared__ float WT[MEAN ? WT_SMEM : 1];
@@ -355,10 +358,23 @@ __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, 
         float q = float(tid) * 0.25f;
         WT[tid] = __frcp_rn(__fmaf_rn(q, q, 1.0f));
     }
+    const int32_t* __restrict__ lab = pv.lab[blockIdx.z];
+    const int32_t* __restrict__ sz = pv.sz[blockIdx.z];
+    const int32_t* __restrict__ acc = pv.root[blockIdx.z];
     for (int i = tid; i < PS * PS; i += 1024) {
         int r = i / PS, c = i % PS;
         int x = u0 - PHALO + c, y = v0 - PHALO + r;
-        S[r][c] = (x >= 0 && x < W && y >= 0 && y < H) ? src[size_t(y) * W + x] : OUT;
+        float d = OUT;
+        if (x >= 0 && x < W && y >= 0 && y < H) {
+            const size_t j = size_t(y) * W + x;
+            d = src[j];
+            if (spk_min > 0 && d >= 0) {     // as k_spk_apply
+                int m = sz[j];
+                if (m >= 0) m = sz[lab[j]];
+                if (acc[-m - 1] < spk_min) d = -1.0f;
+            }
+        }
+        S[r][c] = d;
     }
     __syncthreads();
     // row pass on rows [-PHALO, 32+PHALO), columns [-3, 35)
@@ -443,6 +459,11 @@ __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, 
 
 }  // namespace
 
+bool post_fuses_speckle(const DevParams& p, bool median, bool adaptive_mean) {
+    const int gap = p.ipol_gap_width;
+    return p.speckle_size > 0 && gap <= PGMAX && (gap > 0 || adaptive_mean || median);
+}
+
 cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams& p, bool median,
                         bool adaptive_mean, unsigned* err, cudaStream_t st, int* nlaunch) {
     const int W = g.W, H = g.H, n = W * H;
@@ -450,6 +471,8 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
     auto flip = [&]() {
         for (int k = 0; k < 2; ++k) { float* t = pv.cur[k]; pv.cur[k] = pv.nxt[k]; pv.nxt[k] = t; }
     };
+    // with the tile filter following, speckle removal is applied as it loads
+    const bool fuse = post_fuses_speckle(p, median, adaptive_mean);
     if (p.speckle_size > 0) {
         const dim3 tiles((W + SPK_T - 1) / SPK_T, (H + SPK_T - 1) / SPK_T, nviews);
         launch_k(k_spk_tile, tiles, dim3(SPK_T, SPK_T), 0, st, pv, W, H, p.speckle_sim_threshold);
@@ -458,11 +481,15 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         launch_k(k_spk_border, dim3(gb, 1, nviews), 256, 0, st, pv, W, H, p.speckle_sim_threshold, err);
         const int gn = imax(1, imin(8 * 1024, (n + 255) / 256));
         launch_k(k_spk_count, dim3(gn, 1, nviews), 256, 0, st, pv, n, err);
-        launch_k(k_spk_apply, dim3(gn, 1, nviews), 256, 0, st, pv, n, p.speckle_size);
-        flip();
-        launched += 4;
+        launched += 3;
+        if (!fuse) {
+            launch_k(k_spk_apply, dim3(gn, 1, nviews), 256, 0, st, pv, n, p.speckle_size);
+            flip();
+            launched += 1;
+        }
     }
     const int gap = p.ipol_gap_width;
+    const int spk = fuse ? p.speckle_size : 0;
     const bool tile_gap = gap > 0 && gap <= PGMAX;
     if (gap > PGMAX) {   // wide gaps: serial scans per line, in place
         launch_k(k_gap, dim3((H + 127) / 128, 1, nviews), 128, 0, st, pv, W, H, gap, 1);
@@ -474,20 +501,20 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         const int key = (tile_gap ? 4 : 0) | (adaptive_mean ? 2 : 0) | (median ? 1 : 0);
         if (!tile_gap || gap <= 3) {   // halo 6
             switch (key) {
-            case 1: launch_k(k_post_tile<3, false, false, true>, grid, 1024, 0, st, pv, W, H, gap); break;
-            case 2: launch_k(k_post_tile<3, false, true, false>, grid, 1024, 0, st, pv, W, H, gap); break;
-            case 3: launch_k(k_post_tile<3, false, true, true>, grid, 1024, 0, st, pv, W, H, gap); break;
-            case 4: launch_k(k_post_tile<3, true, false, false>, grid, 1024, 0, st, pv, W, H, gap); break;
-            case 5: launch_k(k_post_tile<3, true, false, true>, grid, 1024, 0, st, pv, W, H, gap); break;
-            case 6: launch_k(k_post_tile<3, true, true, false>, grid, 1024, 0, st, pv, W, H, gap); break;
-            default: launch_k(k_post_tile<3, true, true, true>, grid, 1024, 0, st, pv, W, H, gap); break;
+            case 1: launch_k(k_post_tile<3, false, false, true>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
+            case 2: launch_k(k_post_tile<3, false, true, false>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
+            case 3: launch_k(k_post_tile<3, false, true, true>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
+            case 4: launch_k(k_post_tile<3, true, false, false>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
+            case 5: launch_k(k_post_tile<3, true, false, true>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
+            case 6: launch_k(k_post_tile<3, true, true, false>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
+            default: launch_k(k_post_tile<3, true, true, true>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
             }
         } else {                       // gaps 4..8: halo 11
             switch (key) {
-            case 4: launch_k(k_post_tile<PGMAX, true, false, false>, grid, 1024, 0, st, pv, W, H, gap); break;
-            case 5: launch_k(k_post_tile<PGMAX, true, false, true>, grid, 1024, 0, st, pv, W, H, gap); break;
-            case 6: launch_k(k_post_tile<PGMAX, true, true, false>, grid, 1024, 0, st, pv, W, H, gap); break;
-            default: launch_k(k_post_tile<PGMAX, true, true, true>, grid, 1024, 0, st, pv, W, H, gap); break;
+            case 4: launch_k(k_post_tile<PGMAX, true, false, false>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
+            case 5: launch_k(k_post_tile<PGMAX, true, false, true>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
+            case 6: launch_k(k_post_tile<PGMAX, true, true, false>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
+            default: launch_k(k_post_tile<PGMAX, true, true, true>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
             }
         }
         flip();

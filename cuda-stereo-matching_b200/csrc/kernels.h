@@ -90,6 +90,12 @@ struct PostViews {
     int32_t* sz[2];
 };
 
+// True when launch_post applies the speckle result while loading the fused
+// tile filter instead of in a pass of its own; the filter chain then must
+// not start in the output buffer (it never writes in place), so the caller
+// starts it in pv.nxt.
+bool post_fuses_speckle(const DevParams& p, bool median, bool adaptive_mean);
+
 // Post-filters on nviews (1 or 2) disparity images.
 cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams& p, bool median, bool adaptive_mean,
                         unsigned* err, cudaStream_t st, int* nlaunch);
