@@ -361,6 +361,12 @@ __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, 
     const int32_t* __restrict__ lab = pv.lab[blockIdx.z];
     const int32_t* __restrict__ sz = pv.sz[blockIdx.z];
     const int32_t* __restrict__ acc = pv.root[blockIdx.z];
+    // The speckle decision of k_spk_apply: a pixel's tile-local root (the
+    // pixel itself when sz[j] < 0, else lab[j]) holds -(global root + 1),
+    // whose segment size is acc[global root].  The value, sz[j] and lab[j]
+    // are loaded together, so each pixel waits on three dependent loads, and
+    // the loop is unrolled so that two pixels' chains overlap.
+#pragma unroll 2
     for (int i = tid; i < PS * PS; i += 1024) {
         int r = i / PS, c = i % PS;
         int x = u0 - PHALO + c, y = v0 - PHALO + r;
@@ -368,10 +374,12 @@ __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, 
         if (x >= 0 && x < W && y >= 0 && y < H) {
             const size_t j = size_t(y) * W + x;
             d = src[j];
-            if (spk_min > 0 && d >= 0) {     // as k_spk_apply
-                int m = sz[j];
-                if (m >= 0) m = sz[lab[j]];
-                if (acc[-m - 1] < spk_min) d = -1.0f;
+            if (spk_min > 0) {
+                const int m0 = sz[j], l = lab[j];
+                if (d >= 0) {
+                    const int m = m0 < 0 ? m0 : sz[l];     // a valid pixel has l >= 0
+                    if (acc[-m - 1] < spk_min) d = -1.0f;
+                }
             }
         }
         S[r][c] = d;
