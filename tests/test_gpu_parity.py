@@ -356,8 +356,10 @@ def test_flip_rounds_match_host_emulation(elas, emu_lib, preset):
     elas.process(L, R)
     uvd = elas.stage("support").view(np.int32).reshape(-1, 3)
     ctr = elas.stage("del_counters").view(np.int32).reshape(2, 16)
-    for right in (0, 1):
+    for right, key in ((0, "tri_left"), (1, "tri_right")):
         xy = oracle.support_points(uvd, right)
         tris, st = emu_triangulate(emu_lib, xy, uvd[:, 1] // 5)
         assert ctr[right, 0] == tris.shape[0]
         assert (ctr[right, 4], ctr[right, 5]) == (st[0], st[1]), (right, ctr[right], st)
+        ok, stats = oracle.delaunay_check(xy, elas.stage(key).view(np.int32).reshape(-1, 3))
+        assert ok, (key, stats)
