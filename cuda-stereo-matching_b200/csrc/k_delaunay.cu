@@ -488,8 +488,8 @@ __global__ void __launch_bounds__(FLIP_THREADS) k_flip_global(DelDev d0, DelDev 
 // ---------------------------------------------------------------------------
 // Cluster kernel: the triangulation of one problem lives in the distributed
 // shared memory of a cluster of CL_MAX CTAs.  Triangle t sits in CTA
-// t >> shift at slot t & mask (a power-of-two slice); a record is 44 bytes
-// (3 vertex indices, 3 packed coordinates, 3 links, lock, flip round), so a
+// t >> shift at slot t & mask (a power-of-two slice); a record is 48 bytes
+// (3 vertex indices, 3 packed coordinates, 3 links, two locks, flip round), so a
 // cluster of 16 CTAs holds up to 65536 triangles.  Every access to another
 // CTA's triangle is a distributed-shared-memory load, store or atomic; the
 // phases are separated by cluster barriers.
@@ -500,9 +500,9 @@ constexpr int WL_PER_CTA = 6 * SLICE_MAX;           // worklist entries per CTA 
 constexpr int CAND_PER_CTA = 6 * SLICE_MAX;         // proposals per CTA and round
 constexpr int FLIP_PER_CTA = SLICE_MAX;             // flipped pairs per CTA and round
 constexpr int CL_MARK = 3 * SLICE_MAX / 32;         // words of a per-round half-edge bitset
-// shared memory: the triangle slice (44 bytes a triangle), two push bitsets
+// shared memory: the triangle slice (48 bytes a triangle), two push bitsets
 // and the round-0 staging rings (64 entries per warp)
-constexpr size_t CL_SMEM = size_t(SLICE_MAX) * 44 + size_t(8) * CL_MARK + size_t(4) * 64 * (CL_THREADS / 32);
+constexpr size_t CL_SMEM = size_t(SLICE_MAX) * 48 + size_t(8) * CL_MARK + size_t(4) * 64 * (CL_THREADS / 32);
 
 struct ClusterTri {
     int32_t* lv;      // [3*SLICE_MAX] in this CTA's shared memory
@@ -772,13 +772,19 @@ struct ClusterSync {
 // holding a slice of at most SLICE_MAX triangles.  A problem already handled
 // (ctr[8] set by the one-SM kernel) or larger than csize * SLICE_MAX is
 // skipped; the kernel that handles a problem sets ctr[8].
+//
+// The rounds are those of k_flip_local (three phases between cluster
+// barriers: B flip, C1 resolve + propose the outer edges, C2 relink +
+// re-propose the lost proposals; two lock arrays by round parity).  A
+// proposal is queued at the CTA that owns its lower half-edge, so a CTA
+// flips at most its own triangles in a round (f < FLIP_PER_CTA), and that
+// CTA releases the proposal's locks in the next round.
 __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, int csize, int max_rounds,
                                                           unsigned* err) {
     grid_dep_wait();
-    using Acc = ClusterTri;
     using Sync = ClusterSync;
     extern __shared__ __align__(16) uint8_t csm[];
-    __shared__ int n_cand[2], n_flip, n_wl[2], stop, s_flips;
+    __shared__ int n_cand[2], n_flip, s_flips;
     Sync sync;
     const int rank = sync.rank();
     const int prob = blockIdx.x / csize;
@@ -788,12 +794,13 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, 
     if (D.ctr[8] != 0 || T > csize * SLICE_MAX) return;
     int shift = 6;
     while ((csize << shift) < T) ++shift;
-    Acc m;
+    ClusterTri m;
     m.lv = reinterpret_cast<int32_t*>(csm);
     m.lxy = reinterpret_cast<uint32_t*>(m.lv + 3 * SLICE_MAX);
     m.lopp = reinterpret_cast<int32_t*>(m.lxy + 3 * SLICE_MAX);
-    m.llock = reinterpret_cast<uint32_t*>(m.lopp + 3 * SLICE_MAX);
-    m.lround = reinterpret_cast<int32_t*>(m.llock + SLICE_MAX);
+    uint32_t* const lock0 = reinterpret_cast<uint32_t*>(m.lopp + 3 * SLICE_MAX);
+    uint32_t* const lock1 = lock0 + SLICE_MAX;
+    m.lround = reinterpret_cast<int32_t*>(lock1 + SLICE_MAX);
     uint32_t* const mark0 = reinterpret_cast<uint32_t*>(m.lround + SLICE_MAX);
     uint32_t* const mark1 = mark0 + CL_MARK;
     int32_t* const ring = reinterpret_cast<int32_t*>(mark1 + CL_MARK);
@@ -809,98 +816,126 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, 
             m.lxy[3 * l + k] = pack_xy(D.x[v], D.y[v]);
             m.lopp[3 * l + k] = D.opp[3 * t + k];
         }
-        m.llock[l] = LOCK_FREE;
+        lock0[l] = LOCK_FREE;
+        lock1[l] = LOCK_FREE;
         m.lround[l] = -1;
     }
-    if (tid == 0) { n_cand[0] = n_cand[1] = 0; n_flip = 0; n_wl[0] = n_wl[1] = 0; stop = 0; }
-    // per-CTA list regions in global memory
-    int32_t* const wl0 = D.cwl + size_t(rank) * 2 * WL_PER_CTA;
-    int32_t* const wl1 = wl0 + WL_PER_CTA;
-    int32_t* cand = D.ccand + size_t(rank) * 2 * CAND_PER_CTA;
-    int32_t* flips = D.cflips + size_t(rank) * 6 * FLIP_PER_CTA;
+    if (tid == 0) { n_cand[0] = 0; n_cand[1] = 0; n_flip = 0; }
+    // the proposal lists of CTA r, by round parity, in global memory
+    auto cand_list = [&](int parity, int r) -> int32_t* {
+        return parity ? D.cwl + size_t(r) * 2 * WL_PER_CTA : D.ccand + size_t(r) * 2 * CAND_PER_CTA;
+    };
+    int32_t* const flips = D.cflips + size_t(rank) * 6 * FLIP_PER_CTA;
     sync();
-    int round = 0, flips_total = 0;
+    // round 0's proposals: every interior edge of the own slice once
+    m.llock = lock0;
+    {
+        int32_t* const c0 = cand_list(0, rank);
+        auto add0 = [&](int hh, int nn) {
+            int idx = agg_inc(&n_cand[0]);
+            if (idx < CAND_PER_CTA) { c0[2 * idx] = hh; c0[2 * idx + 1] = nn; }
+        };
+        propose_owned(3 * t0, 3 * t1, ring + 64 * (tid >> 5), [&](int h) { return m.opp(h); }, [&](int h) {
+            if (!flip_propose(m, h, T, 0u, false, add0)) set_err(err, ERRF_BOUNDS);
+        });
+    }
+    sync();
+    int round = 0, flips_total = 0, nc_prev = 0;
     bool converged = false;
     for (; round < max_rounds; ++round) {
         const int cur = round & 1, nxt = cur ^ 1;
-        // A: propose (round 0: every interior edge of the own slice once; later: the worklist)
-        auto add_cand = [&](int hh, int nn) {
-            int idx = agg_inc(&n_cand[cur]);
-            if (idx < CAND_PER_CTA) { cand[2 * idx] = hh; cand[2 * idx + 1] = nn; }
-        };
-        auto prop = [&](int h) {
-            if (!flip_propose(m, h, T, uint32_t(round), false, add_cand)) set_err(err, ERRF_BOUNDS);
-        };
-        if (round == 0) {
-            propose_owned(3 * t0, 3 * t1, ring + 64 * (tid >> 5), [&](int h) { return m.opp(h); }, prop);
-        } else {
-            const int items = min(n_wl[cur], WL_PER_CTA);
-            const int32_t* wl_cur = cur ? wl1 : wl0;
-            for (int k = tid; k < items; k += CL_THREADS) prop(wl_cur[k]);
-        }
-        // this round's push bitset was last used two rounds ago
+        int32_t* const cand_cur = cand_list(cur, rank);
+        int32_t* const cand_old = cand_list(nxt, rank);   // the previous round's list, until C1 refills it
+        uint32_t* const lock_cur = cur ? lock1 : lock0;
+        uint32_t* const lock_nxt = cur ? lock0 : lock1;
         uint32_t* const mark_nxt = cur ? mark0 : mark1;
-        for (int i = tid; i < CL_MARK; i += CL_THREADS) mark_nxt[i] = 0u;
-        if (tid == 0) n_wl[nxt] = 0;       // nobody appends to it before phase C2
-        sync();
+        // every CTA's count is final since the last barrier, so all CTAs take the same decision
         int total = 0;
-        for (int r = 0; r < csize; ++r) total += *sync.remote(&n_cand[cur], r);
-        const int nc = min(n_cand[cur], CAND_PER_CTA);
-        if (tid == 0 && n_cand[cur] > CAND_PER_CTA) { set_err(err, ERRF_BOUNDS); stop = 1; }
+        bool over = false;
+        for (int r = 0; r < csize; ++r) {
+            const int c = *sync.remote(&n_cand[cur], r);
+            total += c;
+            over |= c > CAND_PER_CTA;
+        }
+        if (over) {
+            if (tid == 0) set_err(err, ERRF_BOUNDS);
+            break;
+        }
         if (total == 0) { converged = true; break; }
-        // B: flip the winners
+        const int nc = n_cand[cur];
+        // B: flip the winners (own triangles); release the previous round's locks; clear the next bitset
+        m.llock = lock_cur;
         for (int c = tid; c < nc; c += CL_THREADS) {
-            int h = cand[2 * c], n = cand[2 * c + 1];
+            int h = cand_cur[2 * c], n = cand_cur[2 * c + 1];
             if (flip_apply(m, h, n, uint32_t(round))) {
                 int f = agg_inc(&n_flip);
                 if (f < FLIP_PER_CTA) { flips[6 * f] = h / 3; flips[6 * f + 1] = n; }
             }
         }
+        for (int c = tid; c < nc_prev; c += CL_THREADS) {
+            const int t = cand_old[2 * c] / 3, n = cand_old[2 * c + 1];
+            *(m.at(lock_nxt, t) + (t & m.mask)) = LOCK_FREE;
+            *(m.at(lock_nxt, n) + (n & m.mask)) = LOCK_FREE;
+        }
+        for (int i = tid; i < CL_MARK; i += CL_THREADS) mark_nxt[i] = 0u;
         sync();
         const int nf = min(n_flip, FLIP_PER_CTA);
-        // C1: resolve the outer neighbours (read only)
-        for (int f = tid; f < nf; f += CL_THREADS) {
-            int t = flips[6 * f], n = flips[6 * f + 1];
-            for (int k = 0; k < 4; ++k) {
-                int r = flip_resolve_slot(m, outer_slot(t, n, k), uint32_t(round), T);
-                if (r == -2) { set_err(err, ERRF_BOUNDS); r = -1; }
-                flips[6 * f + 2 + k] = r;
+        // a proposal for the next round, queued at the CTA owning its lower half-edge h
+        auto add_next = [&](int h, int n, uint32_t p) {
+            atomicMin(m.at(lock_nxt, h / 3) + ((h / 3) & m.mask), p);
+            atomicMin(m.at(lock_nxt, n) + (n & m.mask), p);
+            const int owner = (h / 3) >> shift;
+            int idx = agg_inc_keyed(sync.remote(&n_cand[nxt], owner));
+            if (idx < CAND_PER_CTA) {
+                int32_t* e = cand_list(nxt, owner) + 2 * idx;
+                e[0] = h;
+                e[1] = n;
             }
+        };
+        // C1: resolve the outer neighbours (read only); propose the outer edges
+        for (int f = tid; f < nf; f += CL_THREADS) {
+            int32_t* q = flips + 6 * f;
+            const int t = q[0], n = q[1];
+            int r[4], c[4], tw[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                r[k] = flip_resolve_slot(m, outer_slot(t, n, k), uint32_t(round), T);
+                if (r[k] == -2) { set_err(err, ERRF_BOUNDS); r[k] = -1; }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) q[2 + k] = r[k];
+            unsigned claimed = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int x = outer_slot(t, n, k);
+                // a hull edge (r < 0) tests against its own triangle, is never claimed, and is masked out
+                c[k] = r[k] >= 0 ? min(x, r[k]) : x;
+                tw[k] = r[k] >= 0 ? (c[k] == x ? r[k] : x) : x;
+                // the edge's bit lives at the CTA that owns its lower half-edge
+                const int owner = (c[k] / 3) >> shift;
+                const int lb = c[k] - 3 * (owner << shift);
+                const uint32_t bit = 1u << (lb & 31);
+                if (r[k] >= 0 && !(atomicOr(sync.remote(mark_nxt, owner) + (lb >> 5), bit) & bit)) claimed |= 1u << k;
+            }
+            unsigned flippable = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) flippable |= edge_flippable(m, c[k], tw[k]) ? 1u << k : 0u;
+            const unsigned want = claimed & flippable;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (want & (1u << k)) add_next(c[k], tw[k] / 3, prio(uint32_t(c[k]), uint32_t(round + 1)));
         }
         sync();
-        // C2: relink, queue the outer edges at their owners, release locks, requeue lost proposals
-        // the edge's bit and list entry live at the CTA that owns its lower half-edge
-        auto push = [&](int x, int r) {
-            if (r < 0) return;
-            const int c = min(x, r), owner = (c / 3) >> shift;
-            const int lb = c - 3 * (owner << shift);
-            const uint32_t bit = 1u << (lb & 31);
-            if (atomicOr(sync.remote(mark_nxt, owner) + (lb >> 5), bit) & bit) return;
-            int* cnt = sync.remote(&n_wl[nxt], owner);
-            int idx = agg_inc_keyed(cnt);
-            if (idx < WL_PER_CTA) D.cwl[size_t(owner) * 2 * WL_PER_CTA + size_t(nxt) * WL_PER_CTA + idx] = c;
-        };
-        for (int f = tid; f < nf; f += CL_THREADS) {
-            int t = flips[6 * f], n = flips[6 * f + 1];
-            flip_relink(m, t, n, flips + 6 * f + 2);
-            for (int k = 0; k < 4; ++k) push(outer_slot(t, n, k), flips[6 * f + 2 + k]);
-        }
+        // C2: relink; re-propose the own proposals that lost (no outer edge of a flipped pair)
+        if (tid == 0) { n_flip = 0; n_cand[cur] = 0; }   // both were read before the last barrier
+        for (int f = tid; f < nf; f += CL_THREADS) flip_relink(m, flips[6 * f], flips[6 * f + 1], flips + 6 * f + 2);
         for (int c = tid; c < nc; c += CL_THREADS) {
-            int h = cand[2 * c], n = cand[2 * c + 1], t = h / 3;
-            *(m.at(m.llock, t) + (t & m.mask)) = LOCK_FREE;
-            *(m.at(m.llock, n) + (n & m.mask)) = LOCK_FREE;
-            if (m.fround(t) != round && m.fround(n) != round) push(h, m.opp(h));
+            const int h = cand_cur[2 * c], n = cand_cur[2 * c + 1], t = h / 3;
+            if (m.fround(t) != round && m.fround(n) != round) add_next(h, n, prio(uint32_t(h), uint32_t(round + 1)));
         }
         flips_total += nf;
-        if (tid == 0) { n_cand[nxt] = 0; n_flip = 0; }
+        nc_prev = nc;
         sync();
-        if (tid == 0 && n_wl[nxt] > WL_PER_CTA) { set_err(err, ERRF_BOUNDS); stop = 1; }
-        // every CTA's stop flag is final after this barrier and unchanged until
-        // the next round's proposals, so all CTAs take the same decision
-        sync();
-        int any_stop = 0;
-        for (int r = 0; r < csize; ++r) any_stop |= *sync.remote(&stop, r);
-        if (any_stop) break;
     }
     // write back this CTA's slice
     for (int t = t0 + tid; t < t1; t += CL_THREADS) {
