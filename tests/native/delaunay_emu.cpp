@@ -17,8 +17,14 @@ using namespace elas::del;
 // row (points of a row share y).  tris_out: room for cap triangles.  Returns
 // the triangle count, or -1 on an internal error.  stats (nullable):
 // [0] flip rounds, [1] flips.
-extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const int32_t* row_off, int nrows,
-                            int32_t* tris_out, int cap, long long* stats) {
+// phased = 0: rounds in the propose / flip / resolve / relink formulation
+// with worklists (k_flip_global).  phased = 1: rounds in the three-phase
+// formulation of k_flip_local and k_flip_smem (flip; resolve and propose
+// the outer edges; relink and re-propose the lost proposals; two lock
+// arrays by round parity).  Both must give the same triangles, in the same
+// slots, after the same rounds and flips.
+static int emu_core(const int32_t* px, const int32_t* py, int n, const int32_t* row_off, int nrows,
+                    int32_t* tris_out, int cap, long long* stats, int phased) {
     Pts P{px, py};
     // 1. per-row sort + dedup (k_rowsort)
     std::vector<int32_t> srt(std::max(n, 1)), rcnt(nrows, 0);
@@ -98,7 +104,72 @@ extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const i
     std::vector<char> mark(3 * size_t(T), 0);
     int n_cur = 3 * T;
     long long rounds = 0, nflips = 0;
-    for (int round = 0; round < 100000; ++round) {
+    if (phased) {
+        std::vector<uint32_t> lock1(Tmax, LOCK_FREE);
+        std::vector<int32_t> cl[2];
+        // round 0's proposals: every interior edge once (owner rule), with lock array 0
+        m.tlock = lock.data();
+        for (int h = 0; h < 3 * T; ++h)
+            if (!flip_propose(m, h, T, 0u, true, [&](int hh, int nn) { cl[0].push_back(hh); cl[0].push_back(nn); }))
+                return -1;
+        for (int round = 0; round < 100000; ++round) {
+            const int cur = round & 1, nxt = cur ^ 1;
+            std::vector<int32_t>& cc = cl[cur];
+            std::vector<int32_t>& cn = cl[nxt];
+            uint32_t* lock_cur = cur ? lock1.data() : lock.data();
+            uint32_t* lock_nxt = cur ? lock.data() : lock1.data();
+            rounds = round + 1;
+            if (cc.empty()) break;
+            // B: flip the winners; release the previous round's locks (list cn); clear the bitset
+            m.tlock = lock_cur;
+            int nf = 0;
+            for (size_t c = 0; c < cc.size(); c += 2)
+                if (flip_apply(m, cc[c], cc[c + 1], uint32_t(round))) {
+                    flips[6 * nf] = cc[c] / 3;
+                    flips[6 * nf + 1] = cc[c + 1];
+                    ++nf;
+                }
+            for (size_t c = 0; c < cn.size(); c += 2) {
+                lock_nxt[cn[c] / 3] = LOCK_FREE;
+                lock_nxt[cn[c + 1]] = LOCK_FREE;
+            }
+            cn.clear();
+            std::fill(mark.begin(), mark.end(), 0);
+            auto propose_next = [&](int h, int nn) {
+                const uint32_t p = prio(uint32_t(h), uint32_t(round + 1));
+                if (p < lock_nxt[h / 3]) lock_nxt[h / 3] = p;
+                if (p < lock_nxt[nn]) lock_nxt[nn] = p;
+                cn.push_back(h);
+                cn.push_back(nn);
+            };
+            // C1: resolve every flipped pair's outer neighbours, then test and
+            // propose the outer edges (vertices are final after B)
+            for (int f = 0; f < nf; ++f)
+                for (int k = 0; k < 4; ++k) {
+                    int r = flip_resolve_slot(m, outer_slot(flips[6 * f], flips[6 * f + 1], k), uint32_t(round), T);
+                    if (r == -2) return -1;
+                    flips[6 * f + 2 + k] = r;
+                }
+            for (int f = 0; f < nf; ++f)
+                for (int k = 0; k < 4; ++k) {
+                    const int x = outer_slot(flips[6 * f], flips[6 * f + 1], k), r = flips[6 * f + 2 + k];
+                    if (r < 0) continue;
+                    const int c = std::min(x, r), tw = c == x ? r : x;
+                    if (mark[c]) continue;
+                    mark[c] = 1;
+                    if (edge_flippable(m, c, tw)) propose_next(c, tw / 3);
+                }
+            // C2: relink; re-propose the lost proposals without a new test
+            for (int f = 0; f < nf; ++f) flip_relink(m, flips[6 * f], flips[6 * f + 1], &flips[6 * f + 2]);
+            for (size_t c = 0; c < cc.size(); c += 2) {
+                const int h = cc[c], n2 = cc[c + 1], t = h / 3;
+                if (fround[t] != round && fround[n2] != round) propose_next(h, n2);
+            }
+            nflips += nf;
+        }
+        n_cur = 0;
+    }
+    for (int round = 0; !phased && round < 100000; ++round) {
         const std::vector<int32_t>& cur = wl[round & 1];
         std::vector<int32_t>& nxt = wl[(round + 1) & 1];
         int nc = 0;
@@ -152,6 +223,16 @@ extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const i
     if (T <= cap) std::memcpy(tris_out, tri.data(), sizeof(int32_t) * 3 * size_t(T));
     if (stats) { stats[0] = rounds; stats[1] = nflips; }
     return T;
+}
+
+extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const int32_t* row_off, int nrows,
+                            int32_t* tris_out, int cap, long long* stats) {
+    return emu_core(px, py, n, row_off, nrows, tris_out, cap, stats, 0);
+}
+
+extern "C" int emu_delaunay_phased(const int32_t* px, const int32_t* py, int n, const int32_t* row_off, int nrows,
+                                   int32_t* tris_out, int cap, long long* stats) {
+    return emu_core(px, py, n, row_off, nrows, tris_out, cap, stats, 1);
 }
 
 // The flip predicates on packed coordinates, for checks against exact

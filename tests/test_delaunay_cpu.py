@@ -9,8 +9,10 @@ import oracle
 import elas_b200 as eb
 
 
-def emu_triangulate(lib, xy, row_of):
-    """xy: (n,2) int32 in lattice-row order; row_of: lattice row per point."""
+def emu_triangulate(lib, xy, row_of, phased=False):
+    """xy: (n,2) int32 in lattice-row order; row_of: lattice row per point.
+    phased: run the flips in the three-phase round formulation of the
+    one-SM and cluster kernels instead of the worklist formulation."""
     n = xy.shape[0]
     nrows = int(row_of.max()) + 1 if n else 1
     row_off = np.zeros(nrows + 1, np.int32)
@@ -21,9 +23,10 @@ def emu_triangulate(lib, xy, row_of):
     cap = 2 * n + 16
     out = np.zeros((cap, 3), np.int32)
     st = np.zeros(2, np.int64)
-    T = lib.emu_delaunay(x.ctypes.data_as(ctypes.c_void_p), y.ctypes.data_as(ctypes.c_void_p), n,
-                         row_off.ctypes.data_as(ctypes.c_void_p), nrows, out.ctypes.data_as(ctypes.c_void_p), cap,
-                         st.ctypes.data_as(ctypes.c_void_p))
+    fn = lib.emu_delaunay_phased if phased else lib.emu_delaunay
+    T = fn(x.ctypes.data_as(ctypes.c_void_p), y.ctypes.data_as(ctypes.c_void_p), n,
+           row_off.ctypes.data_as(ctypes.c_void_p), nrows, out.ctypes.data_as(ctypes.c_void_p), cap,
+           st.ctypes.data_as(ctypes.c_void_p))
     assert T >= 0
     return out[:T], st
 
@@ -142,3 +145,29 @@ def test_packed_predicates_exact_at_the_size_limits(emu_lib):
         buf = np.ascontiguousarray(pts.reshape(-1))
         assert emu_lib.emu_orient_p(buf.ctypes.data_as(ctypes.c_void_p)) == o
         assert emu_lib.emu_incircle_p(buf.ctypes.data_as(ctypes.c_void_p)) == det
+
+
+def test_three_phase_rounds_equal_worklist_rounds(emu_lib):
+    """The flip kernels run each round as flip / resolve-and-propose /
+    relink-and-repropose, testing the next round's edges while resolving.
+    That formulation must make the same flips in every round as the
+    propose / flip / resolve / relink worklist one: same triangles in the
+    same slots, same rounds, same flips."""
+    sets = []
+    for preset in (0, 1):
+        L, R, _, _ = eb.synth_pair(preset, 3)
+        p = eb.params_config(eb.synth_dims(preset)[2])
+        _, _, st = oracle.process(L, R, p, dumps=True)
+        uvd = st["support"]
+        for right in (0, 1):
+            sets.append((oracle.support_points(uvd, right), uvd[:, 1] // 5))
+    rng = np.random.default_rng(11)
+    for keep in (1.0, 0.5, 0.1):
+        sets.append(lattice_points(rng, 30, 40, 5, keep, jitter_d=8))
+    for xy, row_of in sets:
+        if xy.shape[0] < 3:
+            continue
+        t0, s0 = emu_triangulate(emu_lib, xy, row_of)
+        t1, s1 = emu_triangulate(emu_lib, xy, row_of, phased=True)
+        assert np.array_equal(t0, t1)
+        assert tuple(s0) == tuple(s1)
