@@ -61,20 +61,44 @@ def profile_traffic(name):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """SM clock and throttle reasons sampled during a timed region.  NVML is
+    polled from a thread about every millisecond (a 20-step region of a
+    1242x375 pair lasts about 10 ms); nvidia-smi, whose period is 100 ms, is
+    the fallback.  Read-only: no clock or other setting is changed."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
     def __init__(self, index):
         self.index = index
+        self.samples = []          # (sm_mhz, reasons mask)
+        self.max_mhz = None
+        self.nvml = None
         self.proc = None
         self.lines = []
+        self._stop = threading.Event()
+        self.thread = None
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.nvml = (pynvml, h)
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
+        try:
+            fields = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                      "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                      "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + fields,
                                           "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
@@ -82,20 +106,43 @@ class ClockSampler:
         except OSError:
             self.proc = None
 
+    def _poll(self):
+        pynvml, h = self.nvml
+        while not self._stop.is_set():
+            try:
+                mhz = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                mask = int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))
+                self.samples.append((mhz, mask))
+            except Exception:
+                break
+            time.sleep(0.001)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        self._stop.set()
+        if self.nvml:
+            self.thread.join(timeout=5)
+            pynvml = self.nvml[0]
+            reasons = set()
+            for _, mask in self.samples:
+                for name, attr in self.REASONS:
+                    if mask & getattr(pynvml, attr, 0):
+                        reasons.add(name)
+            sm = [m for m, _ in self.samples]
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                    "reasons": sorted(reasons), "samples": len(sm), "source": "nvml, ~1 ms polling"}
         if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock source"], "samples": 0}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        names = [n for n, _ in self.REASONS]
         for line in self.lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
@@ -109,7 +156,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 100 ms period"}
 
 
 def replica_seed(rank):
@@ -311,7 +358,8 @@ def run_ours(args):
     out = {
         "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded slanted-plane scenes, see DESIGN.md)",
+        "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic: seeded slanted textured planes, z-buffered right view, noise sigma 2",
         "config": {"workload": "elas_pair_1242x375_disp0-255", "width": W, "height": H, "disp_max": D,
                    "pairs_per_step_per_gpu": 1, "l2": "flushed before every step (256 MiB write)",
                    "parallelism": f"replicas x{world}", "params": "reference kernel constants + post-filters"},
@@ -459,11 +507,11 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import oracle
+    import oracle   # the generator and presets come from the oracle library: no product library is loaded
 
-    W, H, D = eb.synth_dims(PRESET)
-    L, R, _, _ = eb.synth_pair(PRESET, 1000)
-    p = eb.params_config(D)
+    W, H, D = oracle.synth_dims(PRESET)
+    L, R, _, _ = oracle.synth_pair(PRESET, 1000)
+    p = oracle.params_config(D)
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
         oracle.process(L, R, p, threads=threads)

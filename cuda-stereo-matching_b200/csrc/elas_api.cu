@@ -33,6 +33,10 @@ struct elas_handle {
     std::string last_error;
     int64_t launches = 0;
 
+    // fallback switches for tests (elas_b200_set_test_mode)
+    int test_flags = 0;
+    int flip_round_limit = 0;     // 0 = the library's own bound
+
     // workspace arena
     void* arena = nullptr;
     size_t arena_bytes = 0;
@@ -292,7 +296,12 @@ int ensure_workspace(elas_handle* h, const Geom& g) {
                                              " bytes failed: " + cudaGetErrorString(e));
         }
         h->arena_bytes = need;
+        // cudaMemset runs on the legacy default stream, which the caller's
+        // stream and the batch workers' non-blocking streams are not ordered
+        // after: without the wait, the zero fill can land after the first
+        // kernels of this call have written the workspace.
         CK(cudaMemset(h->arena, 0, need));
+        CK(cudaDeviceSynchronize());
     }
     layout(h, g, (char*)h->arena);
     for (int k = 0; k < 2; ++k) {
@@ -469,7 +478,8 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     n += 2;
     CK(mark(ELAS_TIME_DELAUNAY));
     CK(launch_delaunay(h->del[0], h->del[1], h->row_off, g.ch + corners, g.cw * g.ch + 6 * corners, h->num_sms,
-                       h->cluster_size, h->err, st, &n));
+                       h->cluster_size, h->err, st, &n, (h->test_flags & ELAS_TEST_FLIP_GLOBAL) != 0,
+                       h->flip_round_limit));
     CK(mark(ELAS_TIME_PRIOR));
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
                     h->rast, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1, h->num_sms, st));
@@ -484,7 +494,7 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     go.W = W >> sub;
     go.H = H >> sub;
     CK(launch_dense(h->desc0, h->desc1, h->prior0, h->prior1, h->grid0, h->grid1, h->raw0, h->raw1, g, dp,
-                    prior_shift(g, dp), h->err, st, shape, sub));
+                    prior_shift(g, dp), h->err, st, shape, sub, (h->test_flags & ELAS_TEST_DENSE_BITSET) != 0));
     n += 1;
     CK(mark(ELAS_TIME_LR));
     // The checked maps also land where the post-filter chain starts: in the
@@ -537,7 +547,8 @@ int run_pipeline_graphed(elas_handle* h, const uint8_t* img0, const uint8_t* img
     }
     std::vector<int64_t> sig = {int64_t(img0), int64_t(img1), int64_t(out0), int64_t(out1), W, H,
                                 int64_t(h->arena), int64_t(h->arena_bytes), int64_t(h->pn_in), int64_t(h->pn_bins),
-                                int64_t(h->pn_stats), h->timing ? 1 : 0, h->prop ? 1 : 0, h->prop_version};
+                                int64_t(h->pn_stats), h->timing ? 1 : 0, h->prop ? 1 : 0, h->prop_version,
+                                h->test_flags, h->flip_round_limit};
     int64_t pw[sizeof(elas_params) / 8 + 1] = {};
     std::memcpy(pw, &h->params, sizeof(elas_params));
     for (int64_t x : pw) sig.push_back(x);
@@ -618,6 +629,8 @@ int issue_batch(elas_handle* h, int n, const uint8_t* const* l, const uint8_t* c
         elas_handle* w = h->slots[i];
         cudaStream_t ws = h->slot_streams[i];
         w->params = h->params;
+        w->test_flags = h->test_flags;
+        w->flip_round_limit = h->flip_round_limit;
         if (dmax) w->params.disp_max = dmax[i];
         if (w->prop_version != h->prop_version) {
             int rc = set_proposal_weights(w, h->prop ? h->prop_params.data() : nullptr,
@@ -934,6 +947,8 @@ int elas_b200_process_batch_device(elas_handle* h, int n, const uint8_t* const* 
     std::memcpy(pw, &h->params, sizeof(elas_params));
     for (int64_t x : pw) sig.push_back(x);
     sig.push_back(int64_t(st));
+    sig.push_back(h->test_flags);
+    sig.push_back(h->flip_round_limit);
     if (h->use_graphs && h->graph_exec && sig == h->graph_sig) {
         CK(cudaGraphLaunch(h->graph_exec, st));
     } else {
@@ -957,6 +972,15 @@ int elas_b200_process_batch_device(elas_handle* h, int n, const uint8_t* const* 
         }
     }
     if (!stream) CK(cudaStreamSynchronize(st));
+    return ELAS_OK;
+}
+
+int elas_b200_set_test_mode(elas_handle* h, int32_t flags, int32_t flip_round_limit) {
+    if (!h) return ELAS_ERR_INVALID_ARG;
+    if ((flags & ~(ELAS_TEST_FLIP_GLOBAL | ELAS_TEST_DENSE_BITSET)) != 0 || flip_round_limit < 0)
+        return fail(h, ELAS_ERR_INVALID_ARG, "unknown test flag or negative round limit");
+    h->test_flags = flags;
+    h->flip_round_limit = flip_round_limit;
     return ELAS_OK;
 }
 

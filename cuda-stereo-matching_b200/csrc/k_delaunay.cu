@@ -984,7 +984,8 @@ int cluster_size_for_flip() {
 }
 
 cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int nmax, int num_sms,
-                            int csize, unsigned* err, cudaStream_t st, int* nlaunch) {
+                            int csize, unsigned* err, cudaStream_t st, int* nlaunch, bool force_global,
+                            int round_limit) {
     launch_k(k_rowsort, dim3(nrows, 2), 512, 0, st, d0, d1, row_off, nrows, err);
     launch_k(k_plan, 2, 1024, 0, st, d0, d1, row_off, nrows, err);
     // the pocket walk's chain and stack (2 sides x (index, x, y, 4-int stack
@@ -999,11 +1000,13 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
     launch_k(k_hash_insert, dim3(blocks, 2), 256, 0, st, d0, d1, err);
     launch_k(k_link, dim3(blocks, 2), 256, 0, st, d0, d1, err);
     int launched = 6;
-    const int max_rounds = 100000;
-    cudaFuncSetAttribute(k_flip_local, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LOC_SMEM));
-    launch_k(k_flip_local, 2, 1024, LOC_SMEM, st, d0, d1, max_rounds, err);
-    ++launched;
-    if (csize > 0) {
+    const int max_rounds = round_limit > 0 ? round_limit : 100000;
+    if (!force_global) {
+        cudaFuncSetAttribute(k_flip_local, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LOC_SMEM));
+        launch_k(k_flip_local, 2, 1024, LOC_SMEM, st, d0, d1, max_rounds, err);
+        ++launched;
+    }
+    if (csize > 0 && !force_global) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(2 * csize);
         cfg.blockDim = dim3(CL_THREADS);
@@ -1024,7 +1027,7 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
     // launched when none can be (at most 2 * nmax + 16 triangles).  It packs
     // the corner coordinates itself; every flip kernel writes its triangles
     // rotated to start at their smallest vertex index.
-    if (csize == 0 || 2LL * nmax + 16 > (long long)csize * SLICE_MAX) {
+    if (force_global || csize == 0 || 2LL * nmax + 16 > (long long)csize * SLICE_MAX) {
         launch_k(k_flip_global, 2, FLIP_THREADS, 0, st, d0, d1, max_rounds, err);
         ++launched;
     }

@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
                                                const uint32_t* __restrict__ prior0, const uint32_t* __restrict__ prior1,
                                                const uint32_t* __restrict__ grid0, const uint32_t* __restrict__ grid1,
                                                float* __restrict__ disp0, float* __restrict__ disp1, Geom g,
-                                               DevParams p, int pshift, int sub, unsigned* err) {
+                                               DevParams p, int pshift, int sub, int lcap, unsigned* err) {
     grid_dep_wait();
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ uint64_t bar;
@@ -247,11 +247,11 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
             while (bits) {
                 int d = 32 * w + __ffs(bits) - 1;
                 bits &= bits - 1;
-                if (n < LMAX) lst[c * LMAX + n] = int16_t(d);
+                if (n < lcap) lst[c * LMAX + n] = int16_t(d);
                 ++n;
             }
         }
-        lcnt[c] = uint8_t(n > LMAX ? 255 : n);
+        lcnt[c] = uint8_t(n > lcap ? 255 : n);
     }
     // first pixel of this thread and its prefetch
     int o = tid, u = o << sub;
@@ -407,7 +407,10 @@ size_t dense_smem_bytes(const Geom& g) { return size_t(g.W) * 16 + size_t(g.gw) 
 
 cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t* prior0, const uint32_t* prior1,
                          const uint32_t* grid0, const uint32_t* grid1, float* disp0, float* disp1, const Geom& g,
-                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads, int sub) {
+                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads, int sub,
+                         bool force_bitset) {
+    // list capacity per cell (0 sends every non-empty cell to the bitset walk)
+    const int lcap = force_bitset ? 0 : LMAX;
     size_t smem = dense_smem_bytes(g);
     if (threads <= 0) threads = 512;
     threads = imin(threads, (((g.W >> sub) + 31) / 32) * 32);
@@ -415,11 +418,11 @@ cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t*
     if (p.plane_radius == 2) {
         cudaFuncSetAttribute(k_dense<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         launch_k(k_dense<2>, grid, threads, smem, st, desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
-                                                pshift, sub, err);
+                                                pshift, sub, lcap, err);
     } else {
         cudaFuncSetAttribute(k_dense<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         launch_k(k_dense<0>, grid, threads, smem, st, desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
-                                                pshift, sub, err);
+                                                pshift, sub, lcap, err);
     }
     return cudaGetLastError();
 }

@@ -41,13 +41,14 @@ __device__ __forceinline__ int uf_find(int32_t* lab, int x, unsigned* err) {
 }
 
 // Labels start at the left neighbour when it is connected (the most common
-// union), else at the pixel itself.
+// union), else at the pixel itself.  One thread per pixel on a 1-D grid (a
+// map of any height fits).
 __global__ void k_uf_init(const float* __restrict__ D, int32_t* __restrict__ lab, int32_t* __restrict__ sz, int W,
                           int H, float thr) {
     grid_dep_wait();
-    int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
-    if (u >= W || v >= H) return;
-    int i = v * W + u;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W * H) return;
+    const int u = i % W;
     float d = D[i];
     int l = -1;
     if (d >= 0) {
@@ -78,9 +79,9 @@ __device__ void uf_union(int32_t* lab, int a, int b, unsigned* err) {
 
 __global__ void k_uf_union(const float* __restrict__ D, int32_t* lab, int W, int H, float thr, unsigned* err) {
     grid_dep_wait();
-    int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
-    if (u >= W || v >= H) return;
-    int i = v * W + u;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W * H) return;
+    const int u = i % W, v = i / W;
     float d = D[i];
     if (d < 0) return;
     if (u + 1 < W) {
@@ -544,16 +545,44 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
 // segment sizes and an error word) is this one file-scope array, resident on
 // every GPU that loads the library until the process exits.  In host code
 // the array's name is only a host-side stand-in, so its device address is
-// looked up once per device with cudaGetSymbolAddress (the first call on a
-// device, which should therefore happen outside any stream capture) and
-// cached.  Every call reuses the array; the kernels initialise all of it
-// that must start at zero, and calls that overlap on the GPU race.
+// looked up with cudaGetSymbolAddress once per device and CUDA context (the
+// first call on a device, and the first after a cudaDeviceReset, which
+// should therefore happen outside any stream capture) and cached.  Every
+// call reuses the array; the kernels initialise all of it that must start
+// at zero, and calls that overlap on the GPU race.
+//
+// The error word receives the bounds flag of the union-find walks, which
+// valid inputs cannot raise: labels only ever decrease, so a find walks at
+// most width*height <= 2^19 nodes, and a union retries only after another
+// thread's hook succeeded, at most 2^19 times -- both below UF_LIMIT.  The
+// call does not read it back (that would synchronise the caller's stream).
 static __device__ __align__(256) int32_t g_noalloc_scratch[3 * ELAS_NOALLOC_MAX_PIXELS + 64];
 
 namespace {
 constexpr int kNoallocMaxDevices = 64;
-int32_t* g_noalloc_base[kNoallocMaxDevices] = {};
+struct NoallocSlot {
+    void* ctx = nullptr;        // CUcontext the address was looked up in
+    int32_t* base = nullptr;
+};
+NoallocSlot g_noalloc_slot[kNoallocMaxDevices];
 std::mutex g_noalloc_mutex;
+
+// The current CUDA context through the runtime's driver entry point (no
+// link against libcuda); null if the entry point is unavailable.
+void* current_context() {
+    using GetCtx = int (*)(void**);
+    static GetCtx fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<GetCtx>(p);
+    }();
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
 }  // namespace
 
 }  // namespace elas
@@ -568,12 +597,15 @@ extern "C" int elas_b200_speckle_noalloc(const float* d_in, float* d_out, int32_
     int32_t* base = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_base[dev]) {
+        NoallocSlot& slot = g_noalloc_slot[dev];
+        void* ctx = current_context();
+        if (!slot.base || ctx != slot.ctx) {
             void* p = nullptr;
             if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return ELAS_ERR_CUDA;
-            g_noalloc_base[dev] = static_cast<int32_t*>(p);
+            slot.base = static_cast<int32_t*>(p);
+            slot.ctx = ctx;
         }
-        base = g_noalloc_base[dev];
+        base = slot.base;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int W = width, H = height, n = W * H, tb = 256;
@@ -581,17 +613,18 @@ extern "C" int elas_b200_speckle_noalloc(const float* d_in, float* d_out, int32_
     int32_t* root = base + ELAS_NOALLOC_MAX_PIXELS;
     int32_t* sz = base + 2 * ELAS_NOALLOC_MAX_PIXELS;
     unsigned* err = reinterpret_cast<unsigned*>(base + 3 * ELAS_NOALLOC_MAX_PIXELS);
+    // each call's own status: an earlier, unrelated launch error is not this call's
     if (d_out != d_in &&
         cudaMemcpyAsync(d_out, d_in, size_t(n) * sizeof(float), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
         return ELAS_ERR_CUDA;
     if (cudaMemsetAsync(err, 0, sizeof(unsigned), st) != cudaSuccess) return ELAS_ERR_CUDA;
     if (min_size > 0) {
-        const dim3 grid2((W + tb - 1) / tb, H);
-        launch_k(k_uf_init, grid2, tb, 0, st, d_out, lab, sz, W, H, sim_threshold);
-        launch_k(k_uf_union, grid2, tb, 0, st, d_out, lab, W, H, sim_threshold, err);
-        launch_k(k_uf_count, (n + tb - 1) / tb, tb, 0, st, lab, root, sz, n, err);
-        launch_k(k_uf_apply, (n + tb - 1) / tb, tb, 0, st, d_out, root, sz, n, min_size);
+        const int blocks = (n + tb - 1) / tb;
+        if (launch_k(k_uf_init, blocks, tb, 0, st, d_out, lab, sz, W, H, sim_threshold) != cudaSuccess ||
+            launch_k(k_uf_union, blocks, tb, 0, st, d_out, lab, W, H, sim_threshold, err) != cudaSuccess ||
+            launch_k(k_uf_count, blocks, tb, 0, st, lab, root, sz, n, err) != cudaSuccess ||
+            launch_k(k_uf_apply, blocks, tb, 0, st, d_out, root, sz, n, min_size) != cudaSuccess)
+            return ELAS_ERR_CUDA;
     }
-    return cudaGetLastError() == cudaSuccess ? ELAS_OK : ELAS_ERR_CUDA;
+    return ELAS_OK;
 }
-

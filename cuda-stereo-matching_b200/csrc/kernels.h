@@ -54,8 +54,11 @@ cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_of
 cudaError_t launch_grid(const int32_t* can, uint32_t* tmp0, uint32_t* tmp1, uint32_t* grid0, uint32_t* grid1,
                         const Geom& g, cudaStream_t st);
 
+// force_global: flip every problem with the global-memory kernel (tests);
+// round_limit > 0 caps the flip rounds (ERRF_FLIP_LIMIT when hit).
 cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int nmax, int num_sms,
-                            int cluster_size, unsigned* err, cudaStream_t st, int* nlaunch);
+                            int cluster_size, unsigned* err, cudaStream_t st, int* nlaunch, bool force_global = false,
+                            int round_limit = 0);
 // Largest cluster (16 or 8 CTAs) with two co-resident copies for the flip
 // kernel, or 0 if none fits.
 int cluster_size_for_flip();
@@ -72,7 +75,8 @@ size_t raster_bytes();
 size_t dense_smem_bytes(const Geom& g);
 cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t* prior0, const uint32_t* prior1,
                          const uint32_t* grid0, const uint32_t* grid1, float* disp0, float* disp1, const Geom& g,
-                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads, int sub = 0);
+                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads, int sub = 0,
+                         bool force_bitset = false);
 
 // L/R check into o0/o1 and, where c0 is not null, also into c0/c1
 cudaError_t launch_lr(const float* d0, const float* d1, float* o0, float* o1, float* c0, float* c1, const Geom& g,

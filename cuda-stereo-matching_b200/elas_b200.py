@@ -101,6 +101,7 @@ def library():
         lib.elas_b200_process_batch_device.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                                        c_void_p, c_void_p, c_void_p]
         lib.elas_b200_set_graphs.argtypes = [c_void_p, c_int]
+        lib.elas_b200_set_test_mode.argtypes = [c_void_p, c_int32, c_int32]
         lib.elas_b200_batch_latency.argtypes = [c_void_p, c_void_p, c_int]
         lib.elas_b200_dense_shape.argtypes = [c_void_p, c_int32, c_int32]
         lib.elas_b200_set_proposal.argtypes = [c_void_p, c_void_p, c_int32]
@@ -276,6 +277,14 @@ class Elas:
 
     def set_graphs(self, enable=True):
         self._check(self._lib.elas_b200_set_graphs(self._h, int(bool(enable))))
+
+    TEST_FLIP_GLOBAL = 1      # every triangulation on the global-memory flip kernel
+    TEST_DENSE_BITSET = 2     # every dense candidate list walked as a bitset
+
+    def set_test_mode(self, flags=0, flip_round_limit=0):
+        """Force fallback paths (results unchanged) and/or cap the flip rounds
+        (a triangulation that needs more raises ElasError with status 7)."""
+        self._check(self._lib.elas_b200_set_test_mode(self._h, int(flags), int(flip_round_limit)))
 
     def batch_latency(self, n):
         """Milliseconds from the last batch's start to each pair's completion."""

@@ -56,7 +56,9 @@ typedef struct elas_params {
     int32_t incon_window_size;      /* half window of the inconsistency filter */
     int32_t incon_threshold;        /* disparity similarity of the inconsistency filter */
     int32_t incon_min_support;      /* min number of consistent support points */
-    bool    add_corners;            /* unimplemented in the reference; ignored here as there */
+    bool    add_corners;            /* frame the support points with the four image corners (declared
+                                       but unimplemented in the reference; implemented here, and on
+                                       in the Elas::parameters() defaults, src/Elas.h:51) */
     int32_t grid_size;              /* cell size of the disparity candidate grid */
     float   beta;                   /* image likelihood parameter */
     float   gamma;                  /* prior constant */
@@ -162,6 +164,24 @@ int elas_b200_process_batch_device(elas_handle* h, int n,
  * the handle's own stream) and whose later calls replay the graph.  A caller
  * that is itself capturing a stream gets plain launches. */
 int elas_b200_set_graphs(elas_handle* h, int enable);
+
+/* Fallback switches, for tests of paths that the usual inputs never reach.
+ * No counterpart in the reference (its Delaunay runs on the CPU and its
+ * dense kernel has one path, src/Kernels/KerComputeDisparity.cu:155-316).
+ *   ELAS_TEST_FLIP_GLOBAL   every triangulation is flipped by the global-
+ *                           memory kernel, which otherwise runs only for
+ *                           triangulations larger than a cluster holds;
+ *   ELAS_TEST_DENSE_BITSET  every grid cell's candidates are walked as a
+ *                           bitset, the path otherwise taken only by cells
+ *                           with more candidates than the per-row list holds.
+ * The results are the same as without the flags.  flip_round_limit > 0
+ * caps the edge-flipping rounds (0 = the library's own bound); a
+ * triangulation that needs more rounds makes the call return
+ * ELAS_ERR_TIMEOUT with the device still usable.  Batches pass the settings
+ * on to their workers. */
+#define ELAS_TEST_FLIP_GLOBAL   1
+#define ELAS_TEST_DENSE_BITSET  2
+int elas_b200_set_test_mode(elas_handle* h, int32_t flags, int32_t flip_round_limit);
 
 /* Per-pair latency (ms from the batch's start to the pair's completion) of
  * the last batch.  Returns the number of pairs (>= 0), or minus a status
@@ -296,11 +316,17 @@ int elas_b200_get_timing(elas_handle* h, float* ms_out, int n);
  * Scratch lives in one fixed array of 3 * ELAS_NOALLOC_MAX_PIXELS int32
  * (6 MiB) in the library's device image; every GPU that loads the library
  * holds it until the process exits.  width * height above
- * ELAS_NOALLOC_MAX_PIXELS returns ELAS_ERR_TOO_LARGE.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress), so
- * make that first call outside any stream capture.  All calls share the
- * array: calls that overlap on the GPU (other streams, other threads) race
- * and give wrong results; serialise them.
+ * ELAS_NOALLOC_MAX_PIXELS returns ELAS_ERR_TOO_LARGE; any aspect ratio
+ * within it is accepted.  The first call on a device, and the first after a
+ * cudaDeviceReset, looks up the array's device address
+ * (cudaGetSymbolAddress), so make that call outside any stream capture.
+ * All calls share the array: calls that overlap on the GPU (other streams,
+ * other threads) race and give wrong results; serialise them.
+ *
+ * The call is asynchronous and returns only host-side and launch errors.
+ * The kernels' own bounds check is not reported: valid inputs cannot
+ * trigger it (every union-find walk and retry loop is bounded well above
+ * the 2^19 steps a map of this size can need).
  */
 int elas_b200_speckle_noalloc(const float* d_in, float* d_out, int32_t width, int32_t height,
                               float sim_threshold, int32_t min_size, void* stream);

@@ -1,6 +1,9 @@
 """Build recipe for the oracle (test infrastructure only).
 
-* oracle/liboracle.so      -- the CPU restatement in elas_oracle.cpp
+* oracle/liboracle.so      -- the CPU restatement in elas_oracle.cpp, plus
+  the seeded scene generator (cuda-stereo-matching_b200/csrc/synth.cpp,
+  compiled from the same source as the product's copy) so that the CPU
+  baseline and the reference arm of the benchmark load no product library
 * oracle/_ref/libreftriangle.so -- the reference's own Triangle
   (src/triangle.cpp) compiled from the reference tree, with the C shim
   tri_ref_shim.cpp.
@@ -9,14 +12,22 @@
   CPU Triangle path its default build takes) compiled for sm_100a with the C
   shim ref_elas_shim.cu.
 The _ref libraries are built only where the reference tree is present; the
-prebuilt files travel with the repository snapshot.
+prebuilt files travel with the repository snapshot.  The reference's src/
+directory is taken from the ref_src argument, else the ELAS_REFERENCE_SRC
+environment variable, else the reference checkout this recipe was written
+against (command line: python build_oracle.py [--force] [--ref-src DIR]).
 """
 import os
 import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = "/root/reference/src"
+SYNTH = os.path.join(os.path.dirname(HERE), "cuda-stereo-matching_b200", "csrc", "synth.cpp")
+DEFAULT_REF_SRC = "/root/reference/src"
+
+
+def ref_src_dir(ref_src=None):
+    return ref_src or os.environ.get("ELAS_REFERENCE_SRC") or DEFAULT_REF_SRC
 
 
 def _run(cmd):
@@ -26,13 +37,15 @@ def _run(cmd):
 def build_oracle(force=False):
     out = os.path.join(HERE, "liboracle.so")
     src = os.path.join(HERE, "elas_oracle.cpp")
-    if force or not os.path.exists(out) or os.path.getmtime(out) < os.path.getmtime(src):
+    if force or not os.path.exists(out) or os.path.getmtime(out) < max(os.path.getmtime(src),
+                                                                        os.path.getmtime(SYNTH)):
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
-              src, "-o", out, "-ldl"])
+              src, SYNTH, "-o", out, "-ldl"])
     return out
 
 
-def build_ref(force=False):
+def build_ref(force=False, ref_src=None):
+    REF_SRC = ref_src_dir(ref_src)
     out_dir = os.path.join(HERE, "_ref")
     out = os.path.join(out_dir, "libreftriangle.so")
     tri = os.path.join(REF_SRC, "triangle.cpp")
@@ -46,7 +59,8 @@ def build_ref(force=False):
     return out
 
 
-def build_ref_elas(force=False):
+def build_ref_elas(force=False, ref_src=None):
+    REF_SRC = ref_src_dir(ref_src)
     out_dir = os.path.join(HERE, "_ref")
     out = os.path.join(out_dir, "libelasref.so")
     elas = os.path.join(REF_SRC, "Elas.cu")
@@ -66,6 +80,7 @@ def build_ref_elas(force=False):
 
 if __name__ == "__main__":
     force = "--force" in sys.argv
+    src = sys.argv[sys.argv.index("--ref-src") + 1] if "--ref-src" in sys.argv else None
     print(build_oracle(force))
-    print(build_ref(force))
-    print(build_ref_elas(force))
+    print(build_ref(force, src))
+    print(build_ref_elas(force, src))

@@ -83,6 +83,64 @@ def P(a):
     return a.ctypes.data_as(c_void_p)
 
 
+# ---- parameter presets and benchmark inputs without the product library ----
+# (the benchmark's CPU baseline and reference arm use these, so they load
+# only oracle libraries)
+
+def params_reference():
+    """The constants the reference kernels are compiled with
+    (src/Kernels/KernelsCommon.h:8-27) on the Elas::parameters layout, every
+    post-filter off (the reference's process() stops after the left/right
+    check, src/Elas.cu:107-119).  Equal to the library's
+    elas_params_reference(); the tests compare the two."""
+    p = ElasParams()
+    p.disp_min, p.disp_max = 0, 255
+    p.support_threshold, p.support_texture, p.candidate_stepsize = 0.85, 10, 5
+    p.incon_window_size, p.incon_threshold, p.incon_min_support = 5, 5, 5
+    p.add_corners, p.grid_size = False, 20
+    p.beta, p.gamma, p.sigma, p.sradius = 0.02, 3.0, 1.0, 2.0
+    p.match_texture, p.lr_threshold, p.speckle_sim_threshold = 0, 2, 1.0
+    p.speckle_size, p.ipol_gap_width = 0, 0
+    p.filter_median = p.filter_adaptive_mean = p.postprocess_only_left = p.subsampling = False
+    return p
+
+
+def params_config(disp_max, post=True):
+    """The benchmark configurations' parameters: the reference constants with
+    the configured disparity range, post-filters (speckle 200, gap width 3,
+    median and adaptive mean) on unless post is False."""
+    p = params_reference()
+    p.disp_max = int(disp_max)
+    if post:
+        p.speckle_size, p.ipol_gap_width = 200, 3
+        p.filter_median = p.filter_adaptive_mean = True
+    return p
+
+
+def synth_dims(preset):
+    w, h, d = c_int32(), c_int32(), c_int32()
+    if lib().elas_b200_synth_dims(preset, ctypes.byref(w), ctypes.byref(h), ctypes.byref(d)) != 0:
+        raise RuntimeError(f"unknown scene preset {preset}")
+    return w.value, h.value, d.value
+
+
+def synth_pair(preset, seed, width=0, height=0, disp_max=0, gt=True):
+    """The seeded synthetic pair of the benchmark (the same generator source
+    as the product's, compiled into the oracle library):
+    (left, right, gt_left, gt_right), the ground truths None unless gt."""
+    W, H, _ = synth_dims(preset)
+    W, H = width or W, height or H
+    left = np.empty((H, W), np.uint8)
+    right = np.empty((H, W), np.uint8)
+    gl = np.empty((H, W), np.float32) if gt else None
+    gr = np.empty((H, W), np.float32) if gt else None
+    rc = lib().elas_b200_synth_pair(preset, ctypes.c_uint64(seed), W, H, disp_max, P(left), P(right),
+                                    P(gl) if gt else None, P(gr) if gt else None)
+    if rc != 0:
+        raise RuntimeError(f"synthetic pair failed with status {rc}")
+    return left, right, gl, gr
+
+
 def geom(W, H, p):
     cw, ch = W // p.candidate_stepsize, H // p.candidate_stepsize
     gw = int(np.ceil(np.float32(W) / np.float32(p.grid_size)))

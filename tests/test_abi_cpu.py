@@ -83,3 +83,10 @@ def test_cpp_class_header_compiles_and_links(tmp_path):
                     "-L", os.path.dirname(eb.LIB_PATH), "-lelas_b200",
                     "-Wl,-rpath," + os.path.dirname(eb.LIB_PATH)], check=True)
     assert exe.exists()
+
+
+def test_test_mode_switch_validates_without_a_device():
+    """elas_b200_set_test_mode rejects unknown flags and negative limits
+    (checked on the host; a null handle is an invalid argument)."""
+    lib = eb.library()
+    assert lib.elas_b200_set_test_mode(None, 0, 0) == 1

@@ -33,3 +33,22 @@ def test_synth_right_view_is_the_warped_left_view():
 def test_synth_custom_size():
     L, R, gl, gr = eb.synth_pair(3, 1, width=320, height=240, disp_max=64)
     assert L.shape == (240, 320) and gl.max() < 64
+
+
+@pytest.mark.parametrize("preset,seed", [(0, 5), (1, 1000), (3, 12)])
+def test_oracle_carries_the_same_generator_and_presets(preset, seed):
+    """The benchmark's CPU baseline and reference arm take their inputs and
+    parameters from the oracle library, so they load no product library:
+    the oracle's copies must equal the library's."""
+    import oracle
+
+    kw = dict(width=320, height=240, disp_max=64) if preset == 3 else {}
+    a = eb.synth_pair(preset, seed, **kw)
+    b = oracle.synth_pair(preset, seed, **kw)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    assert oracle.synth_dims(preset) == eb.synth_dims(preset)
+    assert oracle.params_reference().as_dict() == eb.params_reference().as_dict()
+    for D in (63, 255, 511):
+        for post in (True, False):
+            assert oracle.params_config(D, post).as_dict() == eb.params_config(D, post).as_dict()

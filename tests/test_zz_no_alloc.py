@@ -56,3 +56,48 @@ def test_speckle_noalloc_rejects_oversized_input():
     fn = _entry()
     buf = torch.zeros(16, device="cuda")
     assert fn(buf.data_ptr(), buf.data_ptr(), 2048, 1024, 1.0, 200, None) == 8   # ELAS_ERR_TOO_LARGE
+
+
+
+def _oracle_speckle(D, sim, size):
+    """The oracle's post-filter with speckle removal as its only pass (the
+    regular entry point's speckle stage equals it; see the parity tests)."""
+    import oracle
+
+    p = eb.params_reference()
+    p.speckle_sim_threshold = sim
+    p.speckle_size = size
+    return oracle.postprocess(D, p)
+
+
+def _blocky(rng, h, w):
+    """Piecewise-constant segments of varied size, +0.5 jitter, 10 % holes."""
+    base = rng.integers(0, 40, (h // 4 + 1, w // 4 + 1)).astype(np.float32)
+    D = np.kron(base, np.ones((4, 4), np.float32))[:h, :w].copy()
+    D += rng.integers(0, 2, (h, w)).astype(np.float32) * 0.5
+    D[rng.random((h, w)) < 0.1] = -1.0
+    return np.ascontiguousarray(D)
+
+
+def test_speckle_noalloc_in_place_small_after_large_and_no_op():
+    """In place (d_in == d_out); a small map right after a large one (the
+    shared scratch still holds the large map's labels); a one-column map
+    taller than the 65535-row limit of a grid's y dimension; min_size = 0
+    (output equals input).  Each against the oracle's speckle pass."""
+    import torch
+
+    fn = _entry()
+    stream = torch.cuda.current_stream().cuda_stream
+    rng = np.random.default_rng(5)
+    for h, w, size in [(700, 740, 12), (33, 47, 5), (70000, 1, 3), (600, 800, 0)]:
+        D = _blocky(rng, h, w)
+        d = torch.from_numpy(D.copy()).cuda()
+        torch.cuda.synchronize()
+        rc = fn(d.data_ptr(), d.data_ptr(), w, h, 1.0, size, stream)
+        assert rc == eb.ELAS_OK, (h, w, rc)
+        torch.cuda.synchronize()
+        got = d.cpu().numpy()
+        if size == 0:
+            assert np.array_equal(got, D)
+        else:
+            np.testing.assert_allclose(got, _oracle_speckle(D, 1.0, size), atol=1e-4, rtol=0)
