@@ -17,7 +17,7 @@ OBJ_DIR = os.path.join(HERE, "_build")
 
 CU_SOURCES = ["k_descriptor.cu", "k_support.cu", "k_delaunay.cu", "k_dense.cu", "k_post.cu", "k_proposal.cu",
               "k_proposal_tc.cu", "elas_api.cu"]
-CPP_SOURCES = ["synth.cpp"]
+CPP_SOURCES = ["synth.cpp", "elas_group.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp"]
@@ -42,14 +42,15 @@ def build(force=False, verbose=False, ptxas_info=False):
         if force or _stale(obj, [path] + headers):
             cmd = [NVCC] + ARCH + COMMON + ["-c", path, "-o", obj]
             if src.endswith(".cpp"):
-                cmd = [NVCC, "-Wno-deprecated-gpu-targets"] + COMMON + ["-x", "c++", "-c", path, "-o", obj]
+                cmd = [NVCC, "-Wno-deprecated-gpu-targets"] + COMMON + ["-Xcompiler", "-pthread", "-x", "c++", "-c",
+                                                                        path, "-o", obj]
             if ptxas_info and src.endswith(".cu"):
                 cmd.insert(1, "-Xptxas=-v")
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)
     if force or _stale(OUT, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lgomp"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lgomp", "-lpthread"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -51,12 +51,14 @@ struct elas_handle {
     DelDev del[2]{};
     uint32_t *prior0 = nullptr, *prior1 = nullptr;
     void* rast = nullptr;   // per-triangle plane/edge set-up of both views
+    PriorBins pbins{};      // triangles binned by image row, both views
     float *raw0 = nullptr, *raw1 = nullptr, *lr0 = nullptr, *lr1 = nullptr;
     float *out0 = nullptr, *out1 = nullptr;
     float* tmp[2] = {nullptr, nullptr};          // post-filter ping-pong buffer per view
     int32_t* lab[2] = {nullptr, nullptr};        // union-find labels per view
     int32_t* root[2] = {nullptr, nullptr};       // union-find roots per view
     int32_t* usize[2] = {nullptr, nullptr};      // segment sizes per view
+    int32_t* roots[2] = {nullptr, nullptr};      // tile-local roots of the speckle labelling per view
     unsigned* err = nullptr;
 
     // per-stage timing
@@ -262,6 +264,11 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         D.Hmax = uint32_t(hmax);
     }
     h->rast = take(2 * tmax * raster_bytes());
+    const size_t bin_cap = prior_bin_capacity(g, int(tmax));
+    h->pbins.cnt = (int32_t*)take(2 * (size_t(g.H) + 1) * 4);
+    h->pbins.off = (int32_t*)take(2 * (size_t(g.H) + 1) * 4);
+    h->pbins.list = (int32_t*)take(2 * bin_cap * 4);
+    h->pbins.cap = int(bin_cap);
     h->prior0 = (uint32_t*)take(px * 4);
     h->prior1 = (uint32_t*)take(px * 4);
     h->raw0 = (float*)take(px * 4);
@@ -275,6 +282,7 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         h->lab[k] = (int32_t*)take(px * 4);
         h->root[k] = (int32_t*)take(px * 4);
         h->usize[k] = (int32_t*)take(px * 4);
+        h->roots[k] = (int32_t*)take(px * 4 + 4);
     }
     h->err = (unsigned*)take(64);
     return off;
@@ -325,17 +333,18 @@ int check_dims(elas_handle* h, const int32_t* dims, int& W, int& H) {
         int64_t tmax = 2LL * g.cw * g.ch + 16;
         if ((tmax + 1) >> (32 - prior_shift(g, dp)) != 0)
             return fail(h, ELAS_ERR_UNSUPPORTED, "too many candidate points for the packed plane prior");
-        if (dense_smem_bytes(g) > 220 * 1024)
-            return fail(h, ELAS_ERR_UNSUPPORTED, "image too wide for the dense row in shared memory");
+        if (dense_smem_bytes(g, 1024, 0) > 220 * 1024)
+            return fail(h, ELAS_ERR_UNSUPPORTED, "disparity range too wide for the dense window in shared memory");
     }
     return ELAS_OK;
 }
 
-// Dense-matching autotuner.  The CTA shape (threads per row CTA) changes
-// only how the row's pixels are spread over threads, never the result; the
-// first call with a new (width class, disp_max) times each shape on its own
-// data (CUDA events on the stream) and keeps the fastest.  Inside a stream
-// capture an untuned class uses 512 threads.
+// Dense-matching autotuner.  The CTA shape (output columns per segment
+// CTA, 256 threads at most) changes only how a row's pixels are spread over
+// CTAs and threads, never the result; the first call with a new (width
+// class, disp_max) times each shape on its own data (CUDA events on the
+// stream) and keeps the fastest.  Inside a stream capture an untuned class
+// uses 256 columns.
 constexpr int DENSE_SHAPES[4] = {128, 256, 512, 1024};
 
 int dense_threads_for(elas_handle* h, const Geom& g, const DevParams& dp, cudaStream_t st, int* nlaunch, int* out) {
@@ -346,11 +355,11 @@ int dense_threads_for(elas_handle* h, const Geom& g, const DevParams& dp, cudaSt
     if (it != t->dense_threads.end()) { *out = it->second; return ELAS_OK; }
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(st, &cs));
-    if (cs != cudaStreamCaptureStatusNone) { *out = 512; return ELAS_OK; }
+    if (cs != cudaStreamCaptureStatusNone) { *out = 256; return ELAS_OK; }
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    int best = 512;
+    int best = 256;
     float best_ms = 1e30f;
     for (int shape : DENSE_SHAPES) {
         float shape_ms = 1e30f;
@@ -482,9 +491,9 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
                        h->flip_round_limit));
     CK(mark(ELAS_TIME_PRIOR));
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
-                    h->rast, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1, h->num_sms, st));
-    n += 2;
-    int shape = 512;
+                    h->rast, h->pbins, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1,
+                    h->num_sms, h->err, st, &n));
+    int shape = 256;
     rc = dense_threads_for(h, g, dp, st, &n, &shape);
     if (rc != ELAS_OK) return rc;
     CK(mark(ELAS_TIME_DENSE));
@@ -517,6 +526,7 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
         pv.lab[k] = h->lab[k];
         pv.root[k] = h->root[k];
         pv.sz[k] = h->usize[k];
+        pv.roots[k] = h->roots[k];
     }
     CK(launch_post(pv, nviews, go, dp, p.filter_median, p.filter_adaptive_mean, h->err, st,
                    &n));

@@ -568,6 +568,7 @@ constexpr int LOC_PTS = 4096;      // support points (vertex ids) of a one-SM pr
 constexpr int LOC_CAND = 1536;     // proposals of a round in shared memory (two round lists)
 constexpr int LOC_FLIP = 1280;     // flipped pairs in shared memory
 constexpr int LOC_MARK = (3 * LOC_T + 31) / 32;   // words of a per-round half-edge bitset
+constexpr int FLIP_TAIL = 64;      // rounds with at most this many proposals run on one warp
 constexpr size_t LOC_SMEM = size_t(36) * LOC_T + size_t(4) * LOC_PTS + size_t(16) * LOC_CAND +
                             size_t(24) * LOC_FLIP + size_t(8) * LOC_MARK;
 // round 0 stages each warp's owned half-edges (64 entries) in the flip list's
@@ -639,7 +640,10 @@ __global__ void __launch_bounds__(1024) k_flip_local(DelDev d0, DelDev d1, int m
     __syncthreads();
     int round = 0, flips_total = 0, nc_prev = 0;
     bool converged = false;
-    for (; round < max_rounds; ++round) {
+    // One round with threads [0, nt) of the CTA (index `me`), `sync` the
+    // barrier among them.  Returns 0 to continue, 1 when converged, 2 on
+    // an overflow.
+    auto flip_round = [&](const int me, const int nt, auto&& sync) -> int {
         const int cur = round & 1, nxt = cur ^ 1;
         // selected by value: a dynamically indexed pair would live in local memory
         const List2 cand_cur = cur ? cand1 : cand0, cand_nxt = cur ? cand0 : cand1;
@@ -647,14 +651,14 @@ __global__ void __launch_bounds__(1024) k_flip_local(DelDev d0, DelDev d1, int m
         uint32_t* const lock_nxt = cur ? lock0 : lock1;
         uint32_t* const mark_nxt = cur ? mark0 : mark1;
         const int nc = n_cand[cur];             // final since the last barrier; equal in every thread
-        if (nc == 0) { converged = true; break; }
+        if (nc == 0) { converged = true; return 1; }
         if (nc > cand_cur.cap()) {
-            if (tid == 0) set_err(err, ERRF_BOUNDS);
-            break;
+            if (me == 0) set_err(err, ERRF_BOUNDS);
+            return 2;
         }
         // B: flip the winners; release the previous round's locks; clear the next round's bitset
         m.llock = lock_cur;
-        for (int c = tid; c < nc; c += NT) {
+        for (int c = me; c < nc; c += nt) {
             const int32_t* cc = cand_cur.slot(c);
             int h = cc[0], n = cc[1];
             if (flip_apply(m, h, n, uint32_t(round))) {
@@ -663,13 +667,13 @@ __global__ void __launch_bounds__(1024) k_flip_local(DelDev d0, DelDev d1, int m
                 q[0] = h / 3; q[1] = n;
             }
         }
-        for (int c = tid; c < nc_prev; c += NT) {
+        for (int c = me; c < nc_prev; c += nt) {
             const int32_t* cc = cand_nxt.slot(c);
             lock_nxt[cc[0] / 3] = LOCK_FREE;
             lock_nxt[cc[1]] = LOCK_FREE;
         }
-        for (int i = tid; i < LOC_MARK; i += NT) mark_nxt[i] = 0u;
-        __syncthreads();
+        for (int i = me; i < LOC_MARK; i += nt) mark_nxt[i] = 0u;
+        sync();
         const int nf = n_flip;
         auto add_next = [&](int hh, int nn, uint32_t p) {
             atomicMin(lock_nxt + hh / 3, p);
@@ -680,7 +684,7 @@ __global__ void __launch_bounds__(1024) k_flip_local(DelDev d0, DelDev d1, int m
         // C1: resolve the outer neighbours (read only); propose the outer edges.
         // The four edges of a pair go through each step together (claims,
         // tests, one list reservation per warp), so their latencies overlap.
-        for (int f = tid; f < nf; f += NT) {
+        for (int f = me; f < nf; f += nt) {
             int32_t* q = flips.slot(f);
             const int t = q[0], n = q[1];
             int r[4], c[4], tw[4];
@@ -730,22 +734,40 @@ __global__ void __launch_bounds__(1024) k_flip_local(DelDev d0, DelDev d1, int m
                 ++base;
             }
         }
-        __syncthreads();
+        sync();
         // C2: relink; re-propose the lost proposals (their edges are no outer
         // edge of a flipped pair, so the bitset need not see them)
-        if (tid == 0) { n_flip = 0; n_cand[cur] = 0; }   // both were read before the last barrier
-        for (int f = tid; f < nf; f += NT) {
+        if (me == 0) { n_flip = 0; n_cand[cur] = 0; }   // both were read before the last barrier
+        for (int f = me; f < nf; f += nt) {
             int32_t* q = flips.slot(f);
             flip_relink(m, q[0], q[1], q + 2);
         }
-        for (int c = tid; c < nc; c += NT) {
+        for (int c = me; c < nc; c += nt) {
             const int32_t* cc = cand_cur.slot(c);
             const int h = cc[0], n = cc[1], t = h / 3;
             if (m.fround(t) != round && m.fround(n) != round) add_next(h, n, prio(uint32_t(h), uint32_t(round + 1)));
         }
         flips_total += nf;
         nc_prev = nc;
-        __syncthreads();
+        sync();
+        return 0;
+    };
+    // The whole CTA runs the rounds while they are large; once a round
+    // starts with at most FLIP_TAIL proposals, warp 0 runs every remaining
+    // round alone with warp barriers (the same rounds: the phases only lose
+    // the cost of block-wide barriers), and the other warps wait at the end.
+    int state = 0;
+    for (; round < max_rounds; ++round) {
+        const int nc_top = n_cand[round & 1];   // uniform: read after a block barrier
+        if (nc_top > 0 && nc_top <= FLIP_TAIL) break;
+        state = flip_round(tid, NT, [] { __syncthreads(); });
+        if (state) break;
+    }
+    if (state == 0 && round < max_rounds && tid < 32) {
+        for (; round < max_rounds; ++round) {
+            state = flip_round(tid, 32, [] { __syncwarp(); });
+            if (state) break;
+        }
     }
     __syncthreads();
     for (int t = tid; t < T; t += NT) {

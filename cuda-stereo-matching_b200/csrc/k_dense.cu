@@ -3,12 +3,14 @@
 // Prior: replaces kerComputeDepthApproximation
 // (src/Kernels/KerComputeDisparity.cu:9-152), one thread per triangle with
 // long serial scanline loops.  Here one thread per triangle solves the plane
-// (same double Gauss-Jordan as kerSolve, :321-375) and sets up the edges,
-// then a warp per triangle splits its columns.  A pixel covered by more than one
-// triangle (rounding at shared vertices) must keep the last triangle in
-// list order, as a sequential rasteriser would; the prior is therefore
-// written with a 32-bit atomicMax of (triangle+1) << pshift | d_plane, which
-// makes the result independent of scheduling.  d_plane is stored clamped to
+// (same double Gauss-Jordan as kerSolve, :321-375), sets up the edges and
+// finds the rows it writes; the triangles are then binned by row and one
+// CTA per row paints its row in shared memory and writes it once.  A pixel
+// covered by more than one triangle (rounding at shared vertices) must keep
+// the last triangle in list order, as a sequential rasteriser would; the
+// row is therefore painted with a 32-bit atomicMax of
+// (triangle+1) << pshift | d_plane, which makes the result independent of
+// scheduling.  d_plane is stored clamped to
 // [0, disp_max + plane_radius + 1] (0 standing for every d_plane <= 0): the
 // dense step treats all values beyond either end alike.
 //
@@ -69,7 +71,29 @@ struct Raster {
     float pa, pb, pc;
     float A_u, B_u, C_u;
     float AB_a, AC_a, BC_a, AB_b, AC_b, BC_b;
+    int r0, r1;        // rows the triangle writes lie in [r0, r1] (r0 > r1: none)
 };
+
+// Rows of one part of the scan-line raster: columns u in [ua, ub) write the
+// rows [va, vb) with va = max(min(v1, v2), 0), vb = min(max(v1, v2), H),
+// v1 from the long edge AC and v2 from the part's edge.  Each of v1, v2 is
+// a truncated fma of u, monotone in u, so the extremes over the part are at
+// its first and last column.
+__device__ __forceinline__ int raster_row(float a, float b, int u) {
+    return int(__float2uint_rz(__fmaf_rn(a, float(u), b)));
+}
+__device__ void part_rows(const Raster& R, int part, int W, int H, int& r0, int& r1) {
+    const int ua = part ? int(R.B_u) : int(R.A_u), ub = part ? int(R.C_u) : int(R.B_u);
+    const int u0 = imax(ua, 0), u1 = imin(ub, W) - 1;
+    if (ua == ub || u0 > u1) return;
+    const float ea = part ? R.BC_a : R.AB_a, eb = part ? R.BC_b : R.AB_b;
+    const int a0 = raster_row(R.AC_a, R.AC_b, u0), a1 = raster_row(R.AC_a, R.AC_b, u1);
+    const int b0 = raster_row(ea, eb, u0), b1 = raster_row(ea, eb, u1);
+    const int lo = imax(imin(imin(a0, a1), imin(b0, b1)), 0);
+    const int hi = imin(imax(imax(a0, a1), imax(b0, b1)), H) - 1;
+    r0 = imin(r0, lo);
+    r1 = imax(r1, hi);
+}
 
 __device__ void setup_triangle(const int32_t* tri, const int32_t* can, const int32_t* uvd, int cw, int step,
                                bool right, Raster& R) {
@@ -117,13 +141,15 @@ __device__ void setup_triangle(const int32_t* tri, const int32_t* can, const int
     R.BC_b = __fmaf_rn(-R.BC_a, B_u, B_v);
 }
 
-// One thread per (view, triangle): plane and edge set-up, once.
+// One thread per (view, triangle): plane and edge set-up, the triangle's
+// row range, and its contribution to the per-row counts as a difference
+// array (+1 at its first row, -1 after its last).
 __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__ tri0,
                                                      const int32_t* __restrict__ tri1,
                                                      const int32_t* __restrict__ ctr0,
                                                      const int32_t* __restrict__ ctr1,
                                                      const int32_t* __restrict__ can, const int32_t* __restrict__ uvd,
-                                                     Raster* __restrict__ rast, int Tmax, Geom g) {
+                                                     Raster* __restrict__ rast, int Tmax, Geom g, int32_t* diff) {
     grid_dep_wait();
     const int T0 = ctr0[0], T1 = ctr1[0];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T0 + T1; i += gridDim.x * blockDim.x) {
@@ -131,46 +157,138 @@ __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__
         const int t = right ? i - T0 : i;
         Raster R;
         setup_triangle((right ? tri1 : tri0) + 3 * size_t(t), can, uvd, g.cw, g.step, right, R);
+        int r0 = g.H, r1 = -1;
+        part_rows(R, 0, g.W, g.H, r0, r1);
+        part_rows(R, 1, g.W, g.H, r0, r1);
+        R.r0 = r0;
+        R.r1 = r1;
         rast[(right ? Tmax : 0) + t] = R;
+        if (r0 <= r1) {
+            int32_t* d = diff + (right ? g.H + 1 : 0);
+            atomicAdd(d + r0, 1);
+            atomicAdd(d + r1 + 1, -1);
+        }
     }
 }
 
-// One warp per (view, triangle), lanes over columns; every pixel keeps the
-// last covering triangle through atomicMax on the packed value.
-__global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict__ ctr0,
-                                                      const int32_t* __restrict__ ctr1,
-                                                      const Raster* __restrict__ rast, int Tmax,
-                                                      uint32_t* prior0, uint32_t* prior1, Geom g, int pshift,
-                                                      int dcap) {
+// One 1024-thread block per view: counts from the difference array, their
+// exclusive prefix sums (the row offsets), and the fill cursors (written
+// over the difference array).
+__global__ void __launch_bounds__(1024) k_prior_scan(int32_t* diff, int32_t* off, int H) {
     grid_dep_wait();
-    const int lane = threadIdx.x & 31;
+    __shared__ int ws[33];
+    int32_t* d = diff + blockIdx.x * (H + 1);
+    int32_t* o = off + blockIdx.x * (H + 1);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int per = (H + 1023) / 1024, i0 = imin(tid * per, H), i1 = imin(i0 + per, H);
+    auto scan = [&](int x, int& total) {    // exclusive block scan
+        int y = x;
+#pragma unroll
+        for (int k = 1; k < 32; k <<= 1) {
+            const int z = __shfl_up_sync(0xffffffffu, y, k);
+            if (lane >= k) y += z;
+        }
+        if (lane == 31) ws[warp] = y;
+        __syncthreads();
+        if (warp == 0) {
+            const int w = ws[lane];
+            int c = w;
+#pragma unroll
+            for (int k = 1; k < 32; k <<= 1) {
+                const int z = __shfl_up_sync(0xffffffffu, c, k);
+                if (lane >= k) c += z;
+            }
+            ws[lane] = c - w;
+            if (lane == 31) ws[32] = c;
+        }
+        __syncthreads();
+        const int r = y - x + ws[warp];
+        total = ws[32];
+        __syncthreads();
+        return r;
+    };
+    int sd = 0, total = 0;
+    for (int i = i0; i < i1; ++i) sd += d[i];
+    int c = scan(sd, total);               // count at row i0 - 1 (before the chunk's differences)
+    int sc = 0;
+    for (int i = i0; i < i1; ++i) { c += d[i]; sc += c; }
+    int base = scan(sc, total);
+    c -= sd;                                // back to the count before the chunk
+    for (int i = i0; i < i1; ++i) {
+        c += d[i];
+        o[i] = base;
+        d[i] = base;                        // fill cursor
+        base += c;
+    }
+    if (tid == 0) o[H] = total;
+}
+
+// One thread per (view, triangle): append the triangle to the list of each
+// row of its range (the order within a row carries no meaning: the raster
+// keeps the largest triangle index per pixel).
+__global__ void __launch_bounds__(256) k_prior_fill(const int32_t* __restrict__ ctr0, const int32_t* __restrict__ ctr1,
+                                                    const Raster* __restrict__ rast, int Tmax, int H, int32_t* cursor,
+                                                    int32_t* list, int cap, unsigned* err) {
+    grid_dep_wait();
     const int T0 = ctr0[0], T1 = ctr1[0];
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < T0 + T1; i += nw) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T0 + T1; i += gridDim.x * blockDim.x) {
         const bool right = i >= T0;
         const int t = right ? i - T0 : i;
-        const Raster R = rast[(right ? Tmax : 0) + t];
+        const Raster& R = rast[(right ? Tmax : 0) + t];
+        int32_t* cur = cursor + (right ? H + 1 : 0);
+        int32_t* l = list + (right ? size_t(cap) : 0);
+        for (int r = R.r0; r <= R.r1; ++r) {
+            const int pos = atomicAdd(cur + r, 1);
+            if (pos < cap) l[pos] = t;
+            else atomicOr(err, ERRF_BOUNDS);
+        }
+    }
+}
+
+// One CTA per (row, view): every triangle of the row's list paints the
+// columns it covers in this row into a shared-memory row with atomicMax of
+// (triangle+1) << pshift | d_plane -- the last triangle in list order wins,
+// as a sequential rasteriser writing the triangles in order would leave it --
+// and the row is then written out whole (0 where nothing covers a pixel).
+// Coverage and values are the reference's scan-line expressions
+// (KerComputeDisparity.cu:57-150) with its contraction made explicit.
+__global__ void __launch_bounds__(256) k_prior_rows(const Raster* __restrict__ rast, int Tmax,
+                                                    const int32_t* __restrict__ off,
+                                                    const int32_t* __restrict__ list, int cap, uint32_t* prior0,
+                                                    uint32_t* prior1, Geom g, int pshift, int dcap) {
+    grid_dep_wait();
+    extern __shared__ uint32_t prow[];
+    const int v = blockIdx.x, view = blockIdx.y, W = g.W;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    for (int u = tid; u < W; u += blockDim.x) prow[u] = 0u;
+    __syncthreads();
+    const int32_t* o = off + view * (g.H + 1);
+    const int b = imin(o[v], cap), e = imin(o[v + 1], cap);
+    const int32_t* l = list + (view ? size_t(cap) : 0);
+    const Raster* rs = rast + (view ? Tmax : 0);
+    const float fv = float(v);
+    for (int k = b + warp; k < e; k += nw) {
+        const int t = l[k];
+        const Raster R = rs[t];
         const uint32_t tag = uint32_t(t + 1) << pshift;
-        uint32_t* prior = right ? prior1 : prior0;
         for (int part = 0; part < 2; ++part) {
             const int ua = part ? int(R.B_u) : int(R.A_u), ub = part ? int(R.C_u) : int(R.B_u);
             if (ua == ub) continue;
             const float ea = part ? R.BC_a : R.AB_a, eb = part ? R.BC_b : R.AB_b;
-            for (int u = imax(ua, 0) + lane; u < imin(ub, g.W); u += 32) {
-                const float fu = float(u);
-                const int v1 = int(__float2uint_rz(__fmaf_rn(R.AC_a, fu, R.AC_b)));
-                const int v2 = int(__float2uint_rz(__fmaf_rn(ea, fu, eb)));
+            for (int u = imax(ua, 0) + lane; u < imin(ub, W); u += 32) {
+                const int v1 = raster_row(R.AC_a, R.AC_b, u), v2 = raster_row(ea, eb, u);
                 const int va = imax(imin(v1, v2), 0), vb = imin(imax(v1, v2), g.H);
-                auto value = [&](int v) {
-                    const float dp = __fadd_rn(__fmaf_rn(R.pa, fu, __fmul_rn(R.pb, float(v))), R.pc);
-                    int d = __float2int_rz(dp);
-                    d = d <= 0 ? 0 : (d > dcap ? dcap : d);
-                    return tag | uint32_t(d);
-                };
-                for (int v = va; v < vb; ++v) atomicMax(&prior[size_t(v) * g.W + u], value(v));
+                if (v < va || v >= vb) continue;
+                const float dp = __fadd_rn(__fmaf_rn(R.pa, float(u), __fmul_rn(R.pb, fv)), R.pc);
+                int d = __float2int_rz(dp);
+                d = d <= 0 ? 0 : (d > dcap ? dcap : d);
+                atomicMax(&prow[u], tag | uint32_t(d));
             }
         }
     }
+    __syncthreads();
+    uint32_t* out = (view ? prior1 : prior0) + size_t(v) * W;
+    for (int u = tid; u < W; u += blockDim.x) out[u] = prow[u];
 }
 
 // Candidate-list entries per grid cell kept in shared memory; cells with
@@ -188,9 +306,16 @@ constexpr int PK_NONE = 10000 * 4096;   // the reference's start value: energy 1
 __device__ __forceinline__ int pk_ed(int e, int d) { return e * 4096 + d; }
 __device__ __forceinline__ void take_min(int e, int d, int& best) { best = min(best, pk_ed(e, d)); }
 
-// blockIdx.x = row, blockIdx.y = view (0 left, 1 right).  The other view's
-// descriptor row arrives by bulk copy (TMA) while the CTA expands the
-// candidate lists of the row's grid cells into shared memory.
+// One CTA per (column segment, view) of one row: blockIdx.x = 2 * segment +
+// view (the two views of a segment are neighbours in launch order, so the
+// descriptor row one of them reads as its own the other reads as the other
+// view while it is still in L2), blockIdx.y = output row.  A segment is
+// `seg` output columns.  The part of the other view's descriptor row that
+// the segment's pixels can reach -- its columns widened by disp_max towards
+// the matching direction -- arrives by bulk copy (TMA) while the CTA expands
+// the candidate lists of the segment's grid cells into shared memory, so a
+// CTA holds (seg + disp_max) x 16 bytes instead of a whole row and many CTAs
+// share an SM.
 //
 // Per pixel u the reference evaluates the cell's sorted list, skipping the
 // plane window [d_plane - r, d_plane + r] and every d whose warped column
@@ -207,56 +332,64 @@ __device__ __forceinline__ void take_min(int e, int d, int& best) { best = min(b
 //   * the own descriptor and the prior of the thread's next pixel are
 //     loaded before the current pixel is matched.
 template <int RFIX>
-__global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0, const uint4* __restrict__ desc1,
-                                               const uint32_t* __restrict__ prior0, const uint32_t* __restrict__ prior1,
-                                               const uint32_t* __restrict__ grid0, const uint32_t* __restrict__ grid1,
-                                               float* __restrict__ disp0, float* __restrict__ disp1, Geom g,
-                                               DevParams p, int pshift, int sub, int lcap, unsigned* err) {
+__global__ void __launch_bounds__(256) k_dense(const uint4* __restrict__ desc0, const uint4* __restrict__ desc1,
+                                              const uint32_t* __restrict__ prior0, const uint32_t* __restrict__ prior1,
+                                              const uint32_t* __restrict__ grid0, const uint32_t* __restrict__ grid1,
+                                              float* __restrict__ disp0, float* __restrict__ disp1, Geom g,
+                                              DevParams p, int pshift, int sub, int seg, int lcap, unsigned* err) {
     grid_dep_wait();
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ uint64_t bar;
     // sub = 1: every second row and column (output (W/2) x (H/2))
-    const int v = int(blockIdx.x) << sub;
-    const bool right = blockIdx.y != 0;
+    const int v = int(blockIdx.y) << sub;
+    const bool right = (blockIdx.x & 1) != 0;
     const int W = g.W, H = g.H;
     const int tid = threadIdx.x, NT = blockDim.x;
     const int Wo = W >> sub;
-    float* disp = (right ? disp1 : disp0) + size_t(blockIdx.x) * Wo;
+    const int o0 = int(blockIdx.x >> 1) * seg, o1 = imin(o0 + seg, Wo);
+    float* disp = (right ? disp1 : disp0) + size_t(blockIdx.y) * Wo;
     if (!(v > 3 && v < H - 3)) {           // CTA-uniform: no copy is issued for these rows
-        for (int o = tid; o < Wo; o += NT) disp[o] = -1.0f;
+        for (int o = o0 + tid; o < o1; o += NT) disp[o] = -1.0f;
         return;
     }
-    uint4* row = reinterpret_cast<uint4*>(sm);
-    int16_t* lst = reinterpret_cast<int16_t*>(sm + size_t(W) * 16);
-    uint8_t* lcnt = reinterpret_cast<uint8_t*>(lst + size_t(g.gw) * LMAX);
+    // columns of the segment, and the other row's window they can reach
+    const int ua = o0 << sub, ub = (o1 - 1) << sub;
+    const int c0 = right ? ua : imax(ua - g.D, 0);
+    const int c1 = right ? imin(ub + g.D + 1, W) : ub + 1;
+    const int cell0 = ua / g.gs, ncell = ub / g.gs - cell0 + 1;
+    uint4* win = reinterpret_cast<uint4*>(sm);
+    const size_t win_bytes = size_t(((seg - 1) << sub) + 1 + g.D) * 16;
+    int16_t* lst = reinterpret_cast<int16_t*>(sm + win_bytes);
+    uint8_t* lcnt = reinterpret_cast<uint8_t*>(lst + size_t(ncell) * LMAX);
+    const uint4* row = win - c0;          // row[u] for u in [c0, c1)
     const uint4* self = (right ? desc1 : desc0) + size_t(v) * W;
     const uint4* other = (right ? desc0 : desc1) + size_t(v) * W;
     const uint32_t* prior = (right ? prior1 : prior0) + size_t(v) * W;
     const uint32_t* grid = right ? grid1 : grid0;
     if (tid == 0) {
         mbar_init(&bar, 1);
-        mbar_expect_tx(&bar, unsigned(W) * 16u);
-        bulk_g2s_chunked(row, other, unsigned(W) * 16u, &bar);
+        mbar_expect_tx(&bar, unsigned(c1 - c0) * 16u);
+        bulk_g2s_chunked(win, other + c0, unsigned(c1 - c0) * 16u, &bar);
     }
     const int gy = floordiv(v, g.gs);
-    for (int c = tid; c < g.gw; c += NT) {
-        const uint32_t* cell = grid + (size_t(gy) * g.gw + c) * g.words;
+    for (int k = tid; k < ncell; k += NT) {
+        const uint32_t* cell = grid + (size_t(gy) * g.gw + cell0 + k) * g.words;
         int n = 0;
         for (int w = 0; w < g.words; ++w) {
             uint32_t bits = cell[w];
             while (bits) {
                 int d = 32 * w + __ffs(bits) - 1;
                 bits &= bits - 1;
-                if (n < lcap) lst[c * LMAX + n] = int16_t(d);
+                if (n < lcap) lst[k * LMAX + n] = int16_t(d);
                 ++n;
             }
         }
-        lcnt[c] = uint8_t(n > lcap ? 255 : n);
+        lcnt[k] = uint8_t(n > lcap ? 255 : n);
     }
     // first pixel of this thread and its prefetch
-    int o = tid, u = o << sub;
-    uint32_t pk_next = o < Wo ? prior[u] : 0u;
-    uint4 I_next = o < Wo ? self[u] : make_uint4(0, 0, 0, 0);
+    int o = o0 + tid, u = o << sub;
+    uint32_t pk_next = o < o1 ? prior[u] : 0u;
+    uint4 I_next = o < o1 ? self[u] : make_uint4(0, 0, 0, 0);
     __syncthreads();
     if (!mbar_wait_bounded(&bar, 0, MBAR_WAIT_LIMIT)) {
         if (tid == 0) atomicOr(err, ERRF_TMA_TIMEOUT);
@@ -267,16 +400,17 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
     const int r = RFIX > 0 ? RFIX : p.plane_radius;
     const uint32_t dmask = (1u << pshift) - 1u;
     const int gs = g.gs;
-    // cell of u, advanced incrementally (u grows by NT per iteration)
+    // cell of u relative to the segment's first cell, advanced incrementally
     int cell = u / gs, rem = u - cell * gs;
+    cell -= cell0;
     const int ustep = NT << sub;
     const int cstep = ustep / gs, rstep = ustep - cstep * gs;
-    for (; o < Wo; o += NT, u += ustep) {
+    for (; o < o1; o += NT, u += ustep) {
         const uint32_t pk = pk_next;
         const uint4 I1 = I_next;
         const int c = cell;
         {
-            if (o + NT < Wo) { pk_next = prior[u + ustep]; I_next = self[u + ustep]; }
+            if (o + NT < o1) { pk_next = prior[u + ustep]; I_next = self[u + ustep]; }
             cell += cstep;
             rem += rstep;
             if (rem >= gs) { rem -= gs; ++cell; }
@@ -318,7 +452,7 @@ __global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0,
                     }
                 }
             } else {
-                const uint32_t* cw = grid + (size_t(gy) * g.gw + c) * g.words;
+                const uint32_t* cw = grid + (size_t(gy) * g.gw + cell0 + c) * g.words;
                 bool done = false;
                 for (int w = 0; w < g.words && !done; ++w) {
                     uint32_t bits = cw[w];
@@ -387,42 +521,60 @@ __global__ void k_lr(const float* __restrict__ D1, const float* __restrict__ D2,
 
 }  // namespace
 
+size_t prior_bin_capacity(const Geom& g, int Tmax) {
+    // a row crosses about two triangles per support point of its lattice
+    // rows; twice that, plus four row entries per triangle
+    return size_t(4) * Tmax + size_t(4) * g.H * (size_t(g.cw) + 2);
+}
+
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
-                         int Tmax, const int32_t* can, const int32_t* uvd, void* rast, uint32_t* prior0,
-                         uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms, cudaStream_t st) {
-    size_t n = size_t(g.W) * g.H * sizeof(uint32_t);
-    cudaMemsetAsync(prior0, 0, n, st);
-    cudaMemsetAsync(prior1, 0, n, st);
+                         int Tmax, const int32_t* can, const int32_t* uvd, void* rast, const PriorBins& bins,
+                         uint32_t* prior0, uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms,
+                         unsigned* err, cudaStream_t st, int* nlaunch) {
+    cudaMemsetAsync(bins.cnt, 0, size_t(2) * (g.H + 1) * sizeof(int32_t), st);
     Raster* R = static_cast<Raster*>(rast);
-    launch_k(k_prior_setup, imax(1, imin(8 * num_sms, (2 * Tmax + 255) / 256)), 256, 0, st, tri0, tri1, ctr0, ctr1, can,
-                                                                                      uvd, R, Tmax, g);
-    int blocks = imax(1, imin(16 * num_sms, (2 * Tmax + 7) / 8));
-    launch_k(k_prior_raster, blocks, 256, 0, st, ctr0, ctr1, R, Tmax, prior0, prior1, g, pshift, dcap);
+    const int tblocks = imax(1, imin(8 * num_sms, (2 * Tmax + 255) / 256));
+    launch_k(k_prior_setup, tblocks, 256, 0, st, tri0, tri1, ctr0, ctr1, can, uvd, R, Tmax, g, bins.cnt);
+    launch_k(k_prior_scan, 2, 1024, 0, st, bins.cnt, bins.off, g.H);
+    launch_k(k_prior_fill, tblocks, 256, 0, st, ctr0, ctr1, R, Tmax, g.H, bins.cnt, bins.list, bins.cap, err);
+    const size_t smem = size_t(g.W) * sizeof(uint32_t);
+    cudaFuncSetAttribute(k_prior_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    launch_k(k_prior_rows, dim3(g.H, 2), 256, smem, st, R, Tmax, bins.off, bins.list, bins.cap, prior0, prior1, g,
+             pshift, dcap);
+    if (nlaunch) *nlaunch += 4;
     return cudaGetLastError();
 }
 
 size_t raster_bytes() { return sizeof(Raster); }
 
-size_t dense_smem_bytes(const Geom& g) { return size_t(g.W) * 16 + size_t(g.gw) * (LMAX * 2 + 1); }
+// Shared memory of a dense CTA of `seg` output columns: the other row's
+// window and the candidate lists of the segment's cells.
+size_t dense_smem_bytes(const Geom& g, int seg, int sub) {
+    const size_t span = size_t((seg - 1) << sub) + 1;
+    const size_t cells = span / size_t(g.gs) + 2;
+    return (span + size_t(g.D)) * 16 + cells * (LMAX * 2 + 1);
+}
 
 cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t* prior0, const uint32_t* prior1,
                          const uint32_t* grid0, const uint32_t* grid1, float* disp0, float* disp1, const Geom& g,
-                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads, int sub,
+                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int seg, int sub,
                          bool force_bitset) {
     // list capacity per cell (0 sends every non-empty cell to the bitset walk)
     const int lcap = force_bitset ? 0 : LMAX;
-    size_t smem = dense_smem_bytes(g);
-    if (threads <= 0) threads = 512;
-    threads = imin(threads, (((g.W >> sub) + 31) / 32) * 32);
-    const dim3 grid(g.H >> sub, 2);
+    if (seg <= 0) seg = 256;
+    const int Wo = g.W >> sub;
+    seg = imin(seg, ((Wo + 31) / 32) * 32);
+    const int threads = imin(seg, 256);
+    const size_t smem = dense_smem_bytes(g, seg, sub);
+    const dim3 grid(2 * ((Wo + seg - 1) / seg), g.H >> sub);
     if (p.plane_radius == 2) {
         cudaFuncSetAttribute(k_dense<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         launch_k(k_dense<2>, grid, threads, smem, st, desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
-                                                pshift, sub, lcap, err);
+                 pshift, sub, seg, lcap, err);
     } else {
         cudaFuncSetAttribute(k_dense<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         launch_k(k_dense<0>, grid, threads, smem, st, desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
-                                                pshift, sub, lcap, err);
+                 pshift, sub, seg, lcap, err);
     }
     return cudaGetLastError();
 }

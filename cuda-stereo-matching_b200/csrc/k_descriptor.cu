@@ -3,10 +3,13 @@
 // Replaces kerComputeSobel (src/Kernels/KerDescriptor.cu:8-50) and
 // kerComputeDescriptor (src/Kernels/KerDescriptor.cu:52-101), which write
 // the du/dv images to global memory and read them back with 16 scalar byte
-// loads per pixel.  Here one CTA loads a 70x14 image tile into shared memory,
-// computes du/dv for the 68x12 halo region there and writes the 64x8
-// descriptors as coalesced 16-byte stores: global traffic is 1 byte read +
-// 16 bytes written per pixel and both images run in one launch.
+// loads per pixel.  Here one CTA stages a 70x22 image tile in shared memory
+// with 16-byte vector loads (each tile row is covered by the aligned 16-byte
+// words around it; an aligned 16-byte word never crosses a page, so the
+// bytes it carries beyond the row are harmless and ignored), computes du/dv
+// for the 68x20 halo region there and writes the 64x16 descriptors as
+// coalesced 16-byte stores: global traffic is 1 byte read + 16 bytes
+// written per pixel and both images run in one launch.
 //
 // Arithmetic: du = clamp((s >> 2) + 128, 0, 255) with s the integer Sobel
 // sum; this equals the reference's float form
@@ -23,40 +26,65 @@ namespace elas {
 
 namespace {
 
-constexpr int TX = 64, TY = 8;                 // output tile
+constexpr int TX = 64, TY = 16;                // output tile
 constexpr int IW = TX + 6, IH = TY + 6;        // image tile (halo 3)
 constexpr int GW = TX + 4, GH = TY + 4;        // du/dv tile (halo 2)
+constexpr int RW = 7;                          // 16-byte words staged per image tile row (70 + 15 bytes at most)
 
 __device__ __forceinline__ int sobel_u8(int s) {
     int q = (s >> 2) + 128;
     return q < 0 ? 0 : (q > 255 ? 255 : q);
 }
 
+// vec = 1: both image bases are 16-byte aligned, rows are staged by 16-byte
+// loads; vec = 0: byte loads (caller buffers of any alignment).
+template <bool VEC>
 __global__ void __launch_bounds__(256) k_descriptor(const uint8_t* __restrict__ img0,
                                                     const uint8_t* __restrict__ img1,
                                                     uint4* __restrict__ desc0,
                                                     uint4* __restrict__ desc1, int W, int H) {
     grid_dep_wait();
-    __shared__ uint8_t im[IH][IW + 2];
+    __shared__ __align__(16) uint8_t raw[IH][RW * 16];   // staged words of each tile row
+    __shared__ int roff[IH];                              // byte of image column u0 - 3 within raw[r]
     __shared__ uint8_t du[GH][GW];
     __shared__ uint8_t dv[GH][GW];
     const uint8_t* img = blockIdx.z ? img1 : img0;
     uint4* desc = blockIdx.z ? desc1 : desc0;
     const int u0 = blockIdx.x * TX, v0 = blockIdx.y * TY;
     const int tid = threadIdx.x;
-
-    for (int i = tid; i < IH * IW; i += 256) {
-        int r = i / IW, c = i % IW;
-        int u = u0 - 3 + c, v = v0 - 3 + r;
-        im[r][c] = (u >= 0 && u < W && v >= 0 && v < H) ? img[size_t(v) * W + u] : 0;
+    const int ulo = imax(u0 - 3, 0), uhi = imin(u0 + TX + 3, W);   // image columns of the tile, [ulo, uhi)
+    if (VEC) {
+        for (int i = tid; i < IH * RW; i += 256) {
+            const int r = i / RW, k = i % RW;
+            const int v = v0 - 3 + r;
+            if (v < 0 || v >= H) continue;
+            const size_t s = size_t(v) * W + ulo;
+            const size_t a = s & ~size_t(15);                      // first aligned word of the row's bytes
+            const size_t e = size_t(v) * W + uhi;
+            if (k == 0) roff[r] = int(s - a) - (ulo - (u0 - 3));
+            if (a + size_t(k) * 16 < e)
+                reinterpret_cast<uint4*>(raw[r])[k] = *reinterpret_cast<const uint4*>(img + a + size_t(k) * 16);
+        }
+    } else {
+        for (int i = tid; i < IH * IW; i += 256) {
+            const int r = i / IW, c = i % IW;
+            const int u = u0 - 3 + c, v = v0 - 3 + r;
+            if (c == 0) roff[r] = 0;
+            if (u >= 0 && u < W && v >= 0 && v < H) raw[r][c] = img[size_t(v) * W + u];
+        }
     }
     __syncthreads();
+    // image byte at tile (r, c), i.e. (u, v) = (u0 - 3 + c, v0 - 3 + r); 0 outside the image
+    auto im = [&](int r, int c) -> int {
+        const int u = u0 - 3 + c, v = v0 - 3 + r;
+        return (u >= 0 && u < W && v >= 0 && v < H) ? int(raw[r][c + roff[r]]) : 0;
+    };
     for (int i = tid; i < GH * GW; i += 256) {
         int r = i / GW, c = i % GW;
         // image tile coordinates of (u, v) = (c + 1, r + 1)
-        int a00 = im[r][c], a01 = im[r][c + 1], a02 = im[r][c + 2];
-        int a10 = im[r + 1][c], a12 = im[r + 1][c + 2];
-        int a20 = im[r + 2][c], a21 = im[r + 2][c + 1], a22 = im[r + 2][c + 2];
+        int a00 = im(r, c), a01 = im(r, c + 1), a02 = im(r, c + 2);
+        int a10 = im(r + 1, c), a12 = im(r + 1, c + 2);
+        int a20 = im(r + 2, c), a21 = im(r + 2, c + 1), a22 = im(r + 2, c + 2);
         int sdu = a00 + 2 * a10 + a20 - a02 - 2 * a12 - a22;
         int sdv = a00 + 2 * a01 + a02 - a20 - 2 * a21 - a22;
         du[r][c] = uint8_t(sobel_u8(sdu));
@@ -86,7 +114,9 @@ __global__ void __launch_bounds__(256) k_descriptor(const uint8_t* __restrict__ 
 cudaError_t launch_descriptor(const uint8_t* img0, const uint8_t* img1, uint4* desc0, uint4* desc1,
                               int W, int H, cudaStream_t st) {
     dim3 grid((W + TX - 1) / TX, (H + TY - 1) / TY, 2);
-    launch_k(k_descriptor, grid, 256, 0, st, img0, img1, desc0, desc1, W, H);
+    const bool vec = ((reinterpret_cast<uintptr_t>(img0) | reinterpret_cast<uintptr_t>(img1)) & 15) == 0;
+    if (vec) launch_k(k_descriptor<true>, grid, 256, 0, st, img0, img1, desc0, desc1, W, H);
+    else launch_k(k_descriptor<false>, grid, 256, 0, st, img0, img1, desc0, desc1, W, H);
     return cudaGetLastError();
 }
 

@@ -117,11 +117,28 @@ __global__ void k_uf_count(int32_t* lab, int32_t* __restrict__ root, int32_t* sz
 // component.  The segments, hence the result, are those of a whole-image
 // union-find.
 //   lab[i]  the global index of i's tile-local root (-1 invalid); the local
-//           roots are the nodes of the global forest
-//   sz[i]   the pixel count of i's tile component if i is its local root, else 0;
-//           after the count, -(global root + 1) at every local root
-//   acc[g]  the segment size at global root g (zeroed by the tile kernel)
+//           roots are the nodes of the global forest (a local root's entry is
+//           its parent there, itself until the border pass hooks it)
+//   sz[r]   at a local root r only: the pixel count of its tile component;
+//           after the count, -(global root + 1)
+//   acc[g]  the segment size at global root g (zeroed at every local root by
+//           the tile kernel; global roots are local roots)
+//   roots   [0] the number of local roots, then their global indices
+// Only lab is written per pixel.  A pixel j's segment size is then
+// acc[-sz[lab[j]] - 1]: lab[j] is j's local root or, for a local root that
+// was hooked, another local root of the same segment.
 constexpr int SPK_T = 32;
+
+// One slot per calling lane in the list whose length is *ctr: one atomic per
+// converged group of lanes.
+__device__ __forceinline__ int agg_add(int32_t* ctr) {
+    const unsigned mask = __activemask();
+    const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(ctr, __popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
 
 __device__ __forceinline__ int lfind(int* L, int x) {
     for (int it = 0; it < SPK_T * SPK_T; ++it) {
@@ -195,8 +212,12 @@ __global__ void __launch_bounds__(1024) k_spk_tile(PostViews pv, int W, int H, f
         const size_t i = size_t(y) * W + x;
         const int rx = blockIdx.x * SPK_T + (r & (SPK_T - 1)), ry = blockIdx.y * SPK_T + (r / SPK_T);
         pv.lab[view][i] = r >= 0 ? int(size_t(ry) * W + rx) : -1;
-        pv.sz[view][i] = (r == t) ? C[t] : 0;
-        pv.root[view][i] = 0;
+        if (r == t) {                   // a local root: its count, its segment-size slot, its list entry
+            pv.sz[view][i] = C[t];
+            pv.root[view][i] = 0;
+            int32_t* roots = pv.roots[view];
+            roots[1 + agg_add(roots)] = int(i);
+        }
     }
 }
 
@@ -228,21 +249,23 @@ __global__ void k_spk_border(PostViews pv, int W, int H, float thr, unsigned* er
     }
 }
 
-// Sizes: every tile-local root adds its count at its global root g and
-// keeps -(g + 1) in its size slot (only this thread reads that slot).
+// Sizes: every tile-local root (from the roots list) adds its count at its
+// global root g and keeps -(g + 1) in its size slot (only this thread reads
+// that slot).
 __global__ void k_spk_count(PostViews pv, int n, unsigned* err) {
     grid_dep_wait();
     const int view = blockIdx.z;
     int32_t* lab = pv.lab[view];
     int32_t* sz = pv.sz[view];
     int32_t* acc = pv.root[view];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int32_t* roots = pv.roots[view];
+    const int nr = min(roots[0], n);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nr; k += gridDim.x * blockDim.x) {
+        const int i = roots[1 + k];
         const int c = sz[i];
-        if (c > 0) {
-            const int g = uf_find(lab, i, err);
-            atomicAdd(&acc[g], c);
-            sz[i] = -(g + 1);
-        }
+        const int g = uf_find(lab, i, err);
+        atomicAdd(&acc[g], c);
+        sz[i] = -(g + 1);
     }
 }
 
@@ -259,11 +282,7 @@ __global__ void k_spk_apply(PostViews pv, int n, int min_size) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float d = D[i];
         float o = d;
-        if (d >= 0) {
-            int m = sz[i];
-            if (m >= 0) m = sz[lab[i]];
-            if (acc[-m - 1] < min_size) o = -1.0f;
-        }
+        if (d >= 0 && acc[-sz[lab[i]] - 1] < min_size) o = -1.0f;
         O[i] = o;
     }
 }
@@ -362,11 +381,11 @@ __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, 
     const int32_t* __restrict__ lab = pv.lab[blockIdx.z];
     const int32_t* __restrict__ sz = pv.sz[blockIdx.z];
     const int32_t* __restrict__ acc = pv.root[blockIdx.z];
-    // The speckle decision of k_spk_apply: a pixel's tile-local root (the
-    // pixel itself when sz[j] < 0, else lab[j]) holds -(global root + 1),
-    // whose segment size is acc[global root].  The value, sz[j] and lab[j]
-    // are loaded together, so each pixel waits on three dependent loads, and
-    // the loop is unrolled so that two pixels' chains overlap.
+    // The speckle decision of k_spk_apply: the local root lab[j] holds
+    // -(global root + 1) in its size slot, whose segment size is
+    // acc[global root].  The value and lab[j] are loaded together, so each
+    // pixel waits on three dependent loads, and the loop is unrolled so that
+    // two pixels' chains overlap.
 #pragma unroll 2
     for (int i = tid; i < PS * PS; i += 1024) {
         int r = i / PS, c = i % PS;
@@ -376,11 +395,8 @@ __global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, 
             const size_t j = size_t(y) * W + x;
             d = src[j];
             if (spk_min > 0) {
-                const int m0 = sz[j], l = lab[j];
-                if (d >= 0) {
-                    const int m = m0 < 0 ? m0 : sz[l];     // a valid pixel has l >= 0
-                    if (acc[-m - 1] < spk_min) d = -1.0f;
-                }
+                const int l = lab[j];
+                if (d >= 0 && acc[-sz[l] - 1] < spk_min) d = -1.0f;   // a valid pixel has l >= 0
             }
         }
         S[r][c] = d;
@@ -483,6 +499,7 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
     // with the tile filter following, speckle removal is applied as it loads
     const bool fuse = post_fuses_speckle(p, median, adaptive_mean);
     if (p.speckle_size > 0) {
+        for (int k = 0; k < nviews; ++k) cudaMemsetAsync(pv.roots[k], 0, sizeof(int32_t), st);
         const dim3 tiles((W + SPK_T - 1) / SPK_T, (H + SPK_T - 1) / SPK_T, nviews);
         launch_k(k_spk_tile, tiles, dim3(SPK_T, SPK_T), 0, st, pv, W, H, p.speckle_sim_threshold);
         const long long border = (long long)H * (tiles.x - 1) + (long long)W * (tiles.y - 1);

@@ -63,19 +63,34 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
 // kernel, or 0 if none fits.
 int cluster_size_for_flip();
 
+// Triangles binned by image row, per view: the prior is rasterised one row
+// at a time from these lists.
+struct PriorBins {
+    int32_t* cnt;      // [2][H + 1] triangles whose row range holds row v (then the fill cursors)
+    int32_t* off;      // [2][H + 1] exclusive prefix sums of cnt
+    int32_t* list;     // [2][cap] triangle indices, row by row
+    int cap;           // entries per view
+};
+// Entries per view that the row lists can hold for a W x H pair with at
+// most Tmax triangles (overflow raises ERRF_BOUNDS).
+size_t prior_bin_capacity(const Geom& g, int Tmax);
+
 // Plane prior of both views: prior[v*W+u] = (triangle+1) << pshift | d,
 // d = d_plane clamped to [0, dcap] (dcap = disp_max + plane_radius + 1),
-// 0 where no triangle covers the pixel.  The buffers are zeroed here.
+// 0 where no triangle covers the pixel.  Every pixel is written.
 // rast: scratch of 2 * Tmax * raster_bytes() for the per-triangle set-up.
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
-                         int Tmax, const int32_t* can, const int32_t* uvd, void* rast, uint32_t* prior0,
-                         uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms, cudaStream_t st);
+                         int Tmax, const int32_t* can, const int32_t* uvd, void* rast, const PriorBins& bins,
+                         uint32_t* prior0, uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms,
+                         unsigned* err, cudaStream_t st, int* nlaunch);
 size_t raster_bytes();
 
-size_t dense_smem_bytes(const Geom& g);
+// Dense matching of both views; `seg` output columns per CTA (the
+// autotuned shape; it never changes the result).
+size_t dense_smem_bytes(const Geom& g, int seg, int sub);
 cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t* prior0, const uint32_t* prior1,
                          const uint32_t* grid0, const uint32_t* grid1, float* disp0, float* disp1, const Geom& g,
-                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads, int sub = 0,
+                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int seg, int sub = 0,
                          bool force_bitset = false);
 
 // L/R check into o0/o1 and, where c0 is not null, also into c0/c1
@@ -84,7 +99,8 @@ cudaError_t launch_lr(const float* d0, const float* d1, float* o0, float* o1, fl
 
 // Buffers of the post-filter chain, per view: the filters ping-pong between
 // cur and nxt (the chain starts in cur; the result is copied to out if it
-// does not end there); lab/root/sz are union-find scratch (W*H int32 each).
+// does not end there); lab/root/sz are union-find scratch (W*H int32 each),
+// roots the list of tile-local roots (W*H + 1 int32).
 struct PostViews {
     float* cur[2];
     float* nxt[2];
@@ -92,6 +108,7 @@ struct PostViews {
     int32_t* lab[2];
     int32_t* root[2];
     int32_t* sz[2];
+    int32_t* roots[2];
 };
 
 // True when launch_post applies the speckle result while loading the fused

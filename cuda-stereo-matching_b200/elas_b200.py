@@ -102,6 +102,13 @@ def library():
                                                        c_void_p, c_void_p, c_void_p]
         lib.elas_b200_set_graphs.argtypes = [c_void_p, c_int]
         lib.elas_b200_set_test_mode.argtypes = [c_void_p, c_int32, c_int32]
+        lib.elas_b200_group_create.argtypes = [pp, c_void_p, c_int, POINTER(c_void_p)]
+        lib.elas_b200_group_destroy.argtypes = [c_void_p]
+        lib.elas_b200_group_set_params.argtypes = [c_void_p, pp]
+        lib.elas_b200_group_last_error.restype = ctypes.c_char_p
+        lib.elas_b200_group_last_error.argtypes = [c_void_p]
+        lib.elas_b200_group_plan.argtypes = [c_int, c_void_p, c_void_p, c_int32, c_int, c_void_p]
+        lib.elas_b200_group_process_batch.argtypes = [c_void_p, c_int] + [c_void_p] * 7
         lib.elas_b200_batch_latency.argtypes = [c_void_p, c_void_p, c_int]
         lib.elas_b200_dense_shape.argtypes = [c_void_p, c_int32, c_int32]
         lib.elas_b200_set_proposal.argtypes = [c_void_p, c_void_p, c_int32]
@@ -376,3 +383,75 @@ def pn_corr_loss(f, labels, nlab, hd, wd, disp_max, df, loss_sum, correct, strea
 def pn_adam(p, g, m, v, n, lr, beta1, beta2, eps, step, stream=None):
     _pn_check(library().elas_b200_pn_adam(c_void_p(p), c_void_p(g), c_void_p(m), c_void_p(v), n, lr, beta1, beta2,
                                           eps, step, c_void_p(stream) if stream else None))
+
+
+# ---- pair-parallel batches over several GPUs ----
+
+def group_plan(dims, ndev, disp_max=None, default_disp_max=255):
+    """Device entry of each pair under the group's plan (host only)."""
+    d = np.ascontiguousarray(np.asarray(dims, np.int32).reshape(-1))
+    n = d.size // 2
+    dm = np.ascontiguousarray(np.asarray(disp_max, np.int32)) if disp_max is not None else None
+    out = np.zeros(max(n, 1), np.int32)
+    rc = library().elas_b200_group_plan(n, _ptr(d), _ptr(dm) if dm is not None else None, int(default_disp_max),
+                                        int(ndev), _ptr(out))
+    if rc != ELAS_OK:
+        raise ElasError(rc)
+    return out[:n]
+
+
+class ElasGroup:
+    """One matcher per device entry; batches are dealt to the devices with no
+    exchange between them (elas_b200_group_*)."""
+
+    def __init__(self, params, devices):
+        self._lib = library()
+        self._g = c_void_p()
+        self.params = params.copy()
+        devs = np.ascontiguousarray(np.asarray(devices, np.int32))
+        rc = self._lib.elas_b200_group_create(ctypes.byref(self.params), _ptr(devs), devs.size, ctypes.byref(self._g))
+        if rc != ELAS_OK:
+            raise ElasError(rc)
+
+    def close(self):
+        if self._g:
+            self._lib.elas_b200_group_destroy(self._g)
+            self._g = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != ELAS_OK:
+            msg = self._lib.elas_b200_group_last_error(self._g)
+            raise ElasError(rc, msg.decode() if msg else "")
+
+    def set_params(self, params):
+        self._check(self._lib.elas_b200_group_set_params(self._g, ctypes.byref(params)))
+        self.params = params.copy()
+
+    def process_batch(self, lefts, rights, disp_max=None):
+        """Returns (D1 list, D2 list, plan)."""
+        n = len(lefts)
+        keep, outs1, outs2 = [], [], []
+        dims = np.zeros(2 * n, np.int32)
+        sub = self.params.subsampling
+        for i, (l, r) in enumerate(zip(lefts, rights)):
+            l = np.ascontiguousarray(l, np.uint8)
+            r = np.ascontiguousarray(r, np.uint8)
+            keep += [l, r]
+            H, W = l.shape
+            dims[2 * i], dims[2 * i + 1] = W, H
+            shape = (H // 2, W // 2) if sub else (H, W)
+            outs1.append(np.empty(shape, np.float32))
+            outs2.append(np.empty(shape, np.float32))
+        arr = lambda xs: (c_void_p * n)(*[x.ctypes.data for x in xs])
+        dm = np.asarray(disp_max, np.int32) if disp_max is not None else None
+        plan = np.zeros(n, np.int32)
+        self._check(self._lib.elas_b200_group_process_batch(self._g, n, arr(keep[0::2]), arr(keep[1::2]),
+                                                            arr(outs1), arr(outs2), _ptr(dims),
+                                                            _ptr(dm) if dm is not None else None, _ptr(plan)))
+        return outs1, outs2, plan

@@ -292,6 +292,39 @@ int elas_b200_set_timing(elas_handle* h, int enable);
  * (ELAS_TIME_COUNT values) to ms_out. */
 int elas_b200_get_timing(elas_handle* h, float* ms_out, int n);
 
+/* ---- pair-parallel batches over several GPUs ---- */
+
+/*
+ * A group of matchers, one handle per entry of `devices` (a device may
+ * appear more than once).  No counterpart in the reference, which runs one
+ * pair on device 0 (src/Elas.h:70-83).  Stereo pairs are independent, so a
+ * batch is dealt to the devices with no exchange between them: no peer
+ * memory access and no collective.
+ */
+typedef struct elas_group elas_group;
+int elas_b200_group_create(const elas_params* params, const int32_t* devices, int ndev, elas_group** out);
+int elas_b200_group_destroy(elas_group* g);
+int elas_b200_group_set_params(elas_group* g, const elas_params* params);
+const char* elas_b200_group_last_error(const elas_group* g);
+
+/* The plan a group batch uses: pair i goes to device entry assign[i].
+ * Pairs are taken largest estimated cost first (width * height *
+ * (1 + disp_max / 128)), each to the least-loaded entry; equal costs keep
+ * pair order, so the plan is a pure function of its inputs (host only, no
+ * device needed).  disp_max_per_pair (nullable) overrides disp_max. */
+int elas_b200_group_plan(int n, const int32_t* dims, const int32_t* disp_max_per_pair, int32_t disp_max, int ndev,
+                         int32_t* assign);
+
+/* elas_b200_process_batch over the group: every device entry runs its share
+ * of the plan as one batch on its own host thread; blocks until all outputs
+ * are in host memory.  assign_out (nullable) receives the plan.  Outputs
+ * equal single-pair elas_b200_process calls with each pair's disp_max. */
+int elas_b200_group_process_batch(elas_group* g, int n,
+                                  const uint8_t* const* lefts, const uint8_t* const* rights,
+                                  float* const* disp_lefts, float* const* disp_rights,
+                                  const int32_t* dims, const int32_t* disp_max_per_pair,
+                                  int32_t* assign_out);
+
 /* ---- allocation-free speckle removal ---- */
 
 /* Largest image (width * height) elas_b200_speckle_noalloc accepts. */

@@ -191,3 +191,22 @@ def test_flip_round_limit_returns_timeout(elas):
             elas.set_test_mode(0)
     again1, again2 = elas.process(L, R)
     assert np.array_equal(good1, again1) and np.array_equal(good2, again2)
+
+
+def test_group_batch_equals_singles(elas):
+    """The pair-parallel runner with two entries on device 0 (two handles,
+    each on its own host thread, no wait between them): every pair equals
+    its single-pair run, and the plan it reports is the host plan."""
+    shapes = [(320, 240, 64), (640, 480, 128), (480, 272, 256), (336, 256, 64), (1024, 512, 128)]
+    dmax = [d for (_, _, d) in shapes]
+    pairs = _batch_pairs(shapes, 4200)
+    ref = _singles(elas, pairs, dmax)
+    g = eb.ElasGroup(eb.params_config(64), [0, 0])
+    try:
+        d1, d2, plan = g.process_batch([x[0] for x in pairs], [x[1] for x in pairs], disp_max=dmax)
+    finally:
+        g.close()
+    assert plan.tolist() == eb.group_plan([(w, h) for (w, h, _) in shapes], 2, dmax).tolist()
+    assert set(plan.tolist()) == {0, 1}
+    for i, ((s1, s2), x1, x2) in enumerate(zip(ref, d1, d2)):
+        assert np.array_equal(s1, x1) and np.array_equal(s2, x2), i
