@@ -528,8 +528,7 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
         pv.sz[k] = h->usize[k];
         pv.roots[k] = h->roots[k];
     }
-    CK(launch_post(pv, nviews, go, dp, p.filter_median, p.filter_adaptive_mean, h->err, st,
-                   &n));
+    CK(launch_post(pv, nviews, go, dp, p.filter_median, p.filter_adaptive_mean, h->err, st, &n, h->num_sms));
     CK(mark(ELAS_TIME_COUNT));
     h->launches += n;
     h->have_last = true;

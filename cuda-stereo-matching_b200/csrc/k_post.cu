@@ -344,140 +344,151 @@ __device__ __forceinline__ float gap_fill(const float* line, int stride, int k, 
 // 9-input sorting network (25 compare-exchanges, depth 7; checked by the
 // 0-1 principle on all 512 binary inputs).
 template <int I, int J>
-__device__ __forceinline__ void cex(float* a) {
+__device__ __forceinline__ void cex(float (&a)[9]) {
     const float x = a[I], y = a[J];
     a[I] = fminf(x, y);
     a[J] = fmaxf(x, y);
 }
-__device__ __forceinline__ void sort9(float* a) {
+__device__ __forceinline__ void sort9(float (&a)[9]) {
     cex<0, 3>(a); cex<1, 7>(a); cex<2, 5>(a); cex<4, 8>(a); cex<0, 7>(a); cex<2, 4>(a); cex<3, 8>(a);
     cex<5, 6>(a); cex<0, 2>(a); cex<1, 3>(a); cex<4, 5>(a); cex<7, 8>(a); cex<1, 4>(a); cex<3, 6>(a);
     cex<5, 7>(a); cex<0, 1>(a); cex<2, 4>(a); cex<3, 5>(a); cex<6, 8>(a); cex<2, 3>(a); cex<4, 5>(a);
     cex<6, 7>(a); cex<1, 2>(a); cex<3, 4>(a); cex<5, 6>(a);
 }
 
-constexpr int WT_SMEM = 1024;                   // adaptive-mean weights for |diff| = k/4, k < 1024
+// Adaptive-mean weights.  Every value the mean reads is a multiple of 1/4
+// (integer disparities, halves from the row gap pass, quarters from the
+// column pass) below 4096, so with the key K = 4 * d the weight of a valid
+// pair is WT[|K_q - K_p|], WT[j] = 1 / (1 + (j/4)^2) made by the same
+// correctly rounded operations as the direct formula.  Invalid pixels get a
+// key far away from every valid one, and indices past the valid range hold
+// weight 0, so an invalid neighbour adds 0 to both sums (bit for bit the
+// same as skipping it).
+constexpr int WT_N = 16384;                     // > 4 * 4095, the largest valid |K_q - K_p|
+constexpr int K_INVALID = 1 << 20;
 
 // spk_min > 0: the input is the L/R result before speckle removal, and
 // every loaded pixel goes through the speckle decision of k_spk_apply
 // (segments smaller than spk_min become invalid) on the way in.
+//
+// Persistent: each CTA builds the weight table once and walks its tiles
+// (both views) with a stride of the grid size.
 template <int G, bool GAP, bool MEAN, bool MEDIAN>
-__global__ void __launch_bounds__(1024) k_post_tile(PostViews pv, int W, int H, int gap, int spk_min) {
+__global__ void __launch_bounds__(1024, 2) k_post_tile(PostViews pv, int W, int H, int gap, int spk_min,
+                                                       int nviews) {
     grid_dep_wait();
     constexpr int PHALO = G + 3, PS = PT + 2 * PHALO;   // S tile side
-    __shared__ float WT[MEAN ? WT_SMEM : 1];
+    extern __shared__ float WT[];               // WT_N weights when MEAN
     __shared__ float S[PS][PS];                 // input, halo PHALO
     __shared__ float G2[PS][PT + 6];            // after the row pass: columns [-3, 35)
     __shared__ float V[PT + 6][PT + 6];         // after the column pass: [-3, 35)^2
+    __shared__ int K[MEAN ? PT + 6 : 1][PT + 6];   // mean keys of V
     __shared__ float M[PT + 2][PT + 2];         // after the mean: [-1, 33)^2
-    const float* __restrict__ src = pv.cur[blockIdx.z];
-    float* __restrict__ dst = pv.nxt[blockIdx.z];
-    const int u0 = blockIdx.x * PT, v0 = blockIdx.y * PT, tid = threadIdx.x;
+    const int tid = threadIdx.x;
     const float OUT = -2.0f;                    // outside the image (never valid, never filled)
-    if (MEAN) {
-        float q = float(tid) * 0.25f;
-        WT[tid] = __frcp_rn(__fmaf_rn(q, q, 1.0f));
-    }
-    const int32_t* __restrict__ lab = pv.lab[blockIdx.z];
-    const int32_t* __restrict__ sz = pv.sz[blockIdx.z];
-    const int32_t* __restrict__ acc = pv.root[blockIdx.z];
-    // The speckle decision of k_spk_apply: the local root lab[j] holds
-    // -(global root + 1) in its size slot, whose segment size is
-    // acc[global root].  The value and lab[j] are loaded together, so each
-    // pixel waits on three dependent loads, and the loop is unrolled so that
-    // two pixels' chains overlap.
+    if (MEAN)
+        for (int j = tid; j < WT_N; j += 1024) {
+            const float q = float(j) * 0.25f;
+            WT[j] = j <= 4 * 4095 ? __frcp_rn(__fmaf_rn(q, q, 1.0f)) : 0.0f;
+        }
+    const int tiles_x = (W + PT - 1) / PT, tiles_y = (H + PT - 1) / PT, per_view = tiles_x * tiles_y;
+    for (int tile = blockIdx.x; tile < nviews * per_view; tile += gridDim.x) {
+        const int view = tile / per_view, tv = tile - view * per_view;
+        const float* __restrict__ src = pv.cur[view];
+        float* __restrict__ dst = pv.nxt[view];
+        const int u0 = (tv % tiles_x) * PT, v0 = (tv / tiles_x) * PT;
+        const int32_t* __restrict__ lab = pv.lab[view];
+        const int32_t* __restrict__ sz = pv.sz[view];
+        const int32_t* __restrict__ acc = pv.root[view];
+        __syncthreads();                        // the previous tile (and the table) is done with
+        // The speckle decision of k_spk_apply: the local root lab[j] holds
+        // -(global root + 1) in its size slot, whose segment size is
+        // acc[global root].  The value and lab[j] are loaded together, so each
+        // pixel waits on three dependent loads, and the loop is unrolled so that
+        // two pixels' chains overlap.
 #pragma unroll 2
-    for (int i = tid; i < PS * PS; i += 1024) {
-        int r = i / PS, c = i % PS;
-        int x = u0 - PHALO + c, y = v0 - PHALO + r;
-        float d = OUT;
-        if (x >= 0 && x < W && y >= 0 && y < H) {
-            const size_t j = size_t(y) * W + x;
-            d = src[j];
-            if (spk_min > 0) {
-                const int l = lab[j];
-                if (d >= 0 && acc[-sz[l] - 1] < spk_min) d = -1.0f;   // a valid pixel has l >= 0
-            }
-        }
-        S[r][c] = d;
-    }
-    __syncthreads();
-    // row pass on rows [-PHALO, 32+PHALO), columns [-3, 35)
-    for (int i = tid; i < PS * (PT + 6); i += 1024) {
-        int r = i / (PT + 6), c = i % (PT + 6);
-        int x = u0 - 3 + c;
-        float val = S[r][c + PHALO - 3];
-        if (GAP && val != OUT && val < 0) val = gap_fill(&S[r][c + PHALO - 3], 1, x, W, gap, val);
-        G2[r][c] = val;
-    }
-    __syncthreads();
-    // column pass on [-3, 35)^2
-    for (int i = tid; i < (PT + 6) * (PT + 6); i += 1024) {
-        int r = i / (PT + 6), c = i % (PT + 6);
-        int y = v0 - 3 + r;
-        float val = G2[r + PHALO - 3][c];
-        if (GAP && val != OUT && val < 0) val = gap_fill(&G2[r + PHALO - 3][c], PT + 6, y, H, gap, val);
-        V[r][c] = val;
-    }
-    __syncthreads();
-    // mean on [-1, 33)^2.  An invalid neighbour adds weight 0 (num and den
-    // unchanged, bit for bit), so the loop has no branch.  The weight table
-    // holds 1/(1 + (k/4)^2) for k < WT_SMEM, made by the same correctly
-    // rounded operations as the direct formula; k = 4|diff| is recovered
-    // without a float-to-int conversion: t = 4|diff| + 2^23 puts the
-    // integer part in the low mantissa bits, and t - 2^23 == 4|diff| holds
-    // exactly when 4|diff| is an integer below 2^23.
-    for (int i = tid; i < (PT + 2) * (PT + 2); i += 1024) {
-        int r = i / (PT + 2), c = i % (PT + 2);
-        float dp = V[r + 2][c + 2];
-        float out = dp;
-        if (MEAN && dp >= 0) {
-            float num = 0.0f, den = 0.0f;
-#pragma unroll
-            for (int dy = -2; dy <= 2; ++dy)
-#pragma unroll
-                for (int dx = -2; dx <= 2; ++dx) {
-                    const float dq = V[r + 2 + dy][c + 2 + dx];
-                    const float diff = __fsub_rn(dq, dp);
-                    const float k4 = dq >= 0 ? fabsf(diff) * 4.0f : 0.0f;   // invalid: any table entry
-                    const float t = __fadd_rn(k4, 8388608.0f);
-                    const int ki = __float_as_int(t) - 0x4B000000;
-                    float w;
-                    if (__fsub_rn(t, 8388608.0f) == k4 && ki < WT_SMEM) w = WT[ki];
-                    else w = __frcp_rn(__fmaf_rn(diff, diff, 1.0f));
-                    w = dq >= 0 ? w : 0.0f;
-                    num = __fmaf_rn(w, dq, num);
-                    den = __fadd_rn(den, w);
+        for (int i = tid; i < PS * PS; i += 1024) {
+            int r = i / PS, c = i % PS;
+            int x = u0 - PHALO + c, y = v0 - PHALO + r;
+            float d = OUT;
+            if (x >= 0 && x < W && y >= 0 && y < H) {
+                const size_t j = size_t(y) * W + x;
+                d = src[j];
+                if (spk_min > 0) {
+                    const int l = lab[j];
+                    if (d >= 0 && acc[-sz[l] - 1] < spk_min) d = -1.0f;   // a valid pixel has l >= 0
                 }
-            out = __fdiv_rn(num, den);
-        }
-        M[r][c] = out;
-    }
-    __syncthreads();
-    {
-        int ty = tid / PT, tx = tid % PT;
-        int u = u0 + tx, v = v0 + ty;
-        if (u < W && v < H) {
-            float c = M[ty + 1][tx + 1];
-            float out = c;
-            if (MEDIAN && c >= 0) {
-                // invalid neighbours sort last as +inf; the lower median of the
-                // n valid values is then element (n-1)/2 (all in registers)
-                float a[9];
-                int n = 0;
-#pragma unroll
-                for (int k = 0; k < 9; ++k) {
-                    float q = M[ty + k / 3][tx + k % 3];
-                    n += q >= 0 ? 1 : 0;
-                    a[k] = q >= 0 ? q : INFINITY;
-                }
-                sort9(a);
-                const int m = (n - 1) >> 1;     // n >= 1 (the centre), so m in [0, 4]
-                out = a[0];
-#pragma unroll
-                for (int k = 1; k < 5; ++k) out = m == k ? a[k] : out;
             }
-            dst[size_t(v) * W + u] = out;
+            S[r][c] = d;
+        }
+        __syncthreads();
+        // row pass on rows [-PHALO, 32+PHALO), columns [-3, 35)
+        for (int i = tid; i < PS * (PT + 6); i += 1024) {
+            int r = i / (PT + 6), c = i % (PT + 6);
+            int x = u0 - 3 + c;
+            float val = S[r][c + PHALO - 3];
+            if (GAP && val != OUT && val < 0) val = gap_fill(&S[r][c + PHALO - 3], 1, x, W, gap, val);
+            G2[r][c] = val;
+        }
+        __syncthreads();
+        // column pass on [-3, 35)^2
+        for (int i = tid; i < (PT + 6) * (PT + 6); i += 1024) {
+            int r = i / (PT + 6), c = i % (PT + 6);
+            int y = v0 - 3 + r;
+            float val = G2[r + PHALO - 3][c];
+            if (GAP && val != OUT && val < 0) val = gap_fill(&G2[r + PHALO - 3][c], PT + 6, y, H, gap, val);
+            V[r][c] = val;
+            if (MEAN) K[r][c] = val >= 0 ? __float2int_rn(val * 4.0f) : K_INVALID;
+        }
+        __syncthreads();
+        // mean on [-1, 33)^2, in the oracle's (dy, dx) order: num by fma, den by add
+        for (int i = tid; i < (PT + 2) * (PT + 2); i += 1024) {
+            int r = i / (PT + 2), c = i % (PT + 2);
+            float dp = V[r + 2][c + 2];
+            float out = dp;
+            if (MEAN && dp >= 0) {
+                const int kp = K[r + 2][c + 2];
+                float num = 0.0f, den = 0.0f;
+#pragma unroll
+                for (int dy = -2; dy <= 2; ++dy)
+#pragma unroll
+                    for (int dx = -2; dx <= 2; ++dx) {
+                        const float dq = V[r + 2 + dy][c + 2 + dx];
+                        const int j = min(abs(K[r + 2 + dy][c + 2 + dx] - kp), WT_N - 1);
+                        const float w = WT[j];
+                        num = __fmaf_rn(w, dq, num);
+                        den = __fadd_rn(den, w);
+                    }
+                out = __fdiv_rn(num, den);
+            }
+            M[r][c] = out;
+        }
+        __syncthreads();
+        {
+            int ty = tid / PT, tx = tid % PT;
+            int u = u0 + tx, v = v0 + ty;
+            if (u < W && v < H) {
+                float c = M[ty + 1][tx + 1];
+                float out = c;
+                if (MEDIAN && c >= 0) {
+                    // invalid neighbours sort last as +inf; the lower median of the
+                    // n valid values is then element (n-1)/2 (all in registers)
+                    float a[9];
+                    int n = 0;
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) {
+                        float q = M[ty + k / 3][tx + k % 3];
+                        n += q >= 0 ? 1 : 0;
+                        a[k] = q >= 0 ? q : INFINITY;
+                    }
+                    sort9(a);
+                    const int m = (n - 1) >> 1;     // n >= 1 (the centre), so m in [0, 4]
+                    out = a[0];
+#pragma unroll
+                    for (int k = 1; k < 5; ++k) out = m == k ? a[k] : out;
+                }
+                dst[size_t(v) * W + u] = out;
+            }
         }
     }
 }
@@ -490,7 +501,7 @@ bool post_fuses_speckle(const DevParams& p, bool median, bool adaptive_mean) {
 }
 
 cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams& p, bool median,
-                        bool adaptive_mean, unsigned* err, cudaStream_t st, int* nlaunch) {
+                        bool adaptive_mean, unsigned* err, cudaStream_t st, int* nlaunch, int num_sms) {
     const int W = g.W, H = g.H, n = W * H;
     int launched = 0;
     auto flip = [&]() {
@@ -523,24 +534,30 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         launched += 2;
     }
     if (tile_gap || adaptive_mean || median) {
-        dim3 grid((W + PT - 1) / PT, (H + PT - 1) / PT, nviews);
+        const int tiles = ((W + PT - 1) / PT) * ((H + PT - 1) / PT) * nviews;
+        const int grid = imax(1, imin(tiles, 2 * num_sms));
+        const size_t smem = adaptive_mean ? WT_N * sizeof(float) : 0;
         const int key = (tile_gap ? 4 : 0) | (adaptive_mean ? 2 : 0) | (median ? 1 : 0);
+        auto go = [&](auto kern) {
+            if (smem) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            launch_k(kern, grid, 1024, smem, st, pv, W, H, gap, spk, nviews);
+        };
         if (!tile_gap || gap <= 3) {   // halo 6
             switch (key) {
-            case 1: launch_k(k_post_tile<3, false, false, true>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
-            case 2: launch_k(k_post_tile<3, false, true, false>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
-            case 3: launch_k(k_post_tile<3, false, true, true>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
-            case 4: launch_k(k_post_tile<3, true, false, false>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
-            case 5: launch_k(k_post_tile<3, true, false, true>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
-            case 6: launch_k(k_post_tile<3, true, true, false>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
-            default: launch_k(k_post_tile<3, true, true, true>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
+            case 1: go(k_post_tile<3, false, false, true>); break;
+            case 2: go(k_post_tile<3, false, true, false>); break;
+            case 3: go(k_post_tile<3, false, true, true>); break;
+            case 4: go(k_post_tile<3, true, false, false>); break;
+            case 5: go(k_post_tile<3, true, false, true>); break;
+            case 6: go(k_post_tile<3, true, true, false>); break;
+            default: go(k_post_tile<3, true, true, true>); break;
             }
         } else {                       // gaps 4..8: halo 11
             switch (key) {
-            case 4: launch_k(k_post_tile<PGMAX, true, false, false>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
-            case 5: launch_k(k_post_tile<PGMAX, true, false, true>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
-            case 6: launch_k(k_post_tile<PGMAX, true, true, false>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
-            default: launch_k(k_post_tile<PGMAX, true, true, true>, grid, 1024, 0, st, pv, W, H, gap, spk); break;
+            case 4: go(k_post_tile<PGMAX, true, false, false>); break;
+            case 5: go(k_post_tile<PGMAX, true, false, true>); break;
+            case 6: go(k_post_tile<PGMAX, true, true, false>); break;
+            default: go(k_post_tile<PGMAX, true, true, true>); break;
             }
         }
         flip();

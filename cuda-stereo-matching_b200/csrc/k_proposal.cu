@@ -14,6 +14,7 @@
 #include <cstdint>
 
 #include "common.cuh"
+#include "launch.cuh"
 #include "proposal.h"
 
 namespace elas {
@@ -274,7 +275,7 @@ cudaError_t launch_features(const uint4* desc0, const uint4* desc1, __nv_bfloat1
                             cudaStream_t st) {
     const int Hd = H / 4, Wd = W / 4;
     if (Hd <= 0 || Wd <= 0) return cudaSuccess;
-    k_features<<<dim3((Wd + 63) / 64, Hd, 2), 64, 0, st>>>(desc0, desc1, out, W, Hd, Wd);
+    launch_k(k_features, dim3((Wd + 63) / 64, Hd, 2), 64, 0, st, desc0, desc1, out, W, Hd, Wd);
     return cudaGetLastError();
 }
 

@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "launch.cuh"
 #include "proposal.h"
 
 namespace elas {
@@ -109,7 +110,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     k_conv_tc(const __grid_constant__ CUtensorMap in_map, const __nv_bfloat16* __restrict__ wts,
               const float* __restrict__ bias, __nv_bfloat16* __restrict__ out, int Hd, int Wd, int relu,
               unsigned* err) {
-    grid_dep_wait();
+    // Launched with programmatic dependent launch: everything up to
+    // grid_dep_wait() below (barriers, tensor memory, the weights and
+    // biases, which no earlier kernel writes) overlaps the previous layer's
+    // tail; the activations are read only after the wait.
     extern __shared__ uint8_t tc_raw[];
     __shared__ __align__(8) uint64_t full[STAGES];
     __shared__ __align__(8) uint64_t wbar, mbar;
@@ -149,6 +153,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (tid == 0 && ntile > 0) {
         mbar_expect_tx(&wbar, uint32_t(W_BYTES));
         bulk_g2s_chunked(wsm, wts, uint32_t(W_BYTES), &wbar);
+    }
+    grid_dep_wait();
+    if (tid == 0 && ntile > 0) {
         for (int i = 0; i < STAGES - 1 && i < ntile; ++i) {
             int img, y, x0;
             tile_coords(i, img, y, x0);
@@ -438,9 +445,10 @@ cudaError_t launch_infer(const InferWeights& iw, const __nv_bfloat16* in, __nv_b
     for (int l = 0; l < LAYERS; ++l) {
         CUtensorMap map;
         if (!make_act_map(&map, src[l], Hd, Wd)) return cudaErrorInvalidValue;
-        k_conv_tc<<<grid, TC_THREADS, TC_SMEM, st>>>(map, iw.w + size_t(l) * TAPS * CH * CH, iw.b + size_t(l) * CH,
-                                                    dst[l], Hd, Wd, l < LAYERS - 1, err);
-        e = cudaGetLastError();
+        e = launch_k(k_conv_tc, grid, TC_THREADS, TC_SMEM, st, map,
+                     static_cast<const __nv_bfloat16*>(iw.w + size_t(l) * TAPS * CH * CH),
+                     static_cast<const float*>(iw.b + size_t(l) * CH), dst[l], Hd, Wd, int(l < LAYERS - 1), err);
+        if (e == cudaSuccess) e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -454,9 +462,9 @@ cudaError_t launch_topk(const __nv_bfloat16* F, uint32_t* bins, int Hd, int Wd, 
     if (smem <= 200 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_topk_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
-        k_topk_rows<<<ch, 256, smem, st>>>(F, bins, Hd, Wd, cw, step, D);
+        launch_k(k_topk_rows, ch, 256, smem, st, F, bins, Hd, Wd, cw, step, D);
     } else {
-        k_topk<<<(n * 32 + 255) / 256, 256, 0, st>>>(F, bins, Hd, Wd, cw, ch, step, D);
+        launch_k(k_topk, (n * 32 + 255) / 256, 256, 0, st, F, bins, Hd, Wd, cw, ch, step, D);
     }
     return cudaGetLastError();
 }

@@ -399,18 +399,90 @@ __device__ __forceinline__ void slice_of(int lo, int hi, int j, int Q, int& da, 
     db = imin(hi, da + per - 1);
 }
 
+// Restricted sweep (learned proposal) by the Q threads of a group: thread j
+// matches elements j, j + Q, ... of the packed bin set (up to four bins of
+// width w, each widened by pn::MARGIN on both sides; overlaps counted once,
+// clipped to [dmin, dmax]) into a packed state of energy << 17 | d.
+template <int DIR>
+__device__ __forceinline__ Best2 restricted_slice(const uint4* self_m2, const uint4* self_p2, const uint4* oth_m2,
+                                                  const uint4* oth_p2, int u, int dmin, int dmax, uint32_t bins,
+                                                  int w, int j, int Q) {
+    Best2 s{PK_INF, PK_INF};
+    const int L = w + 2 * pn::MARGIN;
+    int lo[pn::TOPK];
+#pragma unroll
+    for (int r = 0; r < pn::TOPK; ++r) {
+        const uint32_t b = (bins >> (8 * r)) & 0xffu;
+        lo[r] = b == pn::NO_BIN ? INT32_MIN / 2 : int(b) * w - pn::MARGIN;
+    }
+    const uint4 c0 = self_m2[u - 2], c1 = self_m2[u + 2], c2 = self_p2[u - 2], c3 = self_p2[u + 2];
+    for (int e = j; e < pn::TOPK * L; e += Q) {
+        static_assert(pn::TOPK == 4, "e / L below assumes four bins");
+        const int r = int(e >= L) + int(e >= 2 * L) + int(e >= 3 * L);   // e / L, as e < 4 L
+        const int lor = r == 0 ? lo[0] : r == 1 ? lo[1] : r == 2 ? lo[2] : lo[3];
+        if (lor == INT32_MIN / 2) continue;
+        const int d = lor + (e - r * L);
+        if (d < dmin || d > dmax) continue;
+        bool dup = false;
+#pragma unroll
+        for (int q = 0; q < pn::TOPK - 1; ++q)
+            if (q < r && d >= lo[q] && d < lo[q] + L) dup = true;
+        if (dup) continue;
+        const int uw = u + DIR * d;
+        int en = sad16(c0, oth_m2[uw - 2]);
+        en = sad16(c1, oth_m2[uw + 2], en);
+        en = sad16(c2, oth_p2[uw - 2], en);
+        en = sad16(c3, oth_p2[uw + 2], en);
+        best2_add(s, (uint32_t(en) << 17) | uint32_t(d));
+    }
+    return s;
+}
+
+// The restricted sweep's decision: accepted iff the minimum energy of the
+// set is attained once and (float)E1 < thr * (float)E2, E2 the smallest
+// energy of the other disparities of the set.
+template <int Q>
+__device__ __forceinline__ int group_decide_unique(Best2 s, float thr) {
+#pragma unroll
+    for (int o = Q / 2; o > 0; o >>= 1) {
+        Best2 t;
+        t.v1 = __shfl_xor_sync(0xffffffffu, s.v1, o);
+        t.v2 = __shfl_xor_sync(0xffffffffu, s.v2, o);
+        best2_merge(s, t);
+    }
+    if (s.v1 == PK_INF) return -1;
+    const int e1 = int(s.v1 >> 17);
+    const int e2 = s.v2 == PK_INF ? INF_E : int(s.v2 >> 17);
+    if (e2 == e1) return -1;
+    return float(e1) < thr * float(e2) ? int(s.v1 & 0xfffu) : -1;
+}
+
 // grid.x = segments of a candidate row, grid.y = candidate rows; blockDim =
 // Q x candidates per pass.  SMEM: the four descriptor rows arrive by bulk
 // copy (TMA); otherwise they are read through L1 from global memory.
+//
+// The candidates that need a sweep are compacted into shared-memory lists
+// before each sweep pass, so the groups of a warp all have work:
+//   PROP  every candidate first tries its learned search set (left view,
+//         then the right view from u - d, both with the restricted rule,
+//         then the left/right test); the ones it settles are final, the
+//         rest join the list of full sweeps;
+//   left  full L->R sweeps of the listed candidates;
+//   right full R->L sweeps from u - d of the candidates the left pass
+//         accepted, and the left/right test.
 constexpr int SWEEP_Q_THREADS = 512;   // at most 64 candidates x 8 threads per pass (128 registers)
-template <int Q, bool SMEM>
+constexpr int SETTLED = 1 << 20;       // res[] flag: accepted by the learned proposal, no full right pass
+template <int Q, bool SMEM, bool PROP>
 __global__ void __launch_bounds__(SWEEP_Q_THREADS) k_support_sweep_q(const uint4* __restrict__ desc0,
                                                           const uint4* __restrict__ desc1,
                                                           int32_t* __restrict__ can_out, Geom g, DevParams p,
-                                                          int seg, unsigned* err) {
+                                                          int seg, unsigned* err, const uint32_t* __restrict__ bins,
+                                                          int32_t* __restrict__ stats) {
     grid_dep_wait();
     extern __shared__ __align__(128) uint4 rows[];
     __shared__ int res[256];
+    __shared__ int16_t lst[256];
+    __shared__ int nlst;
     __shared__ uint64_t bar;
     const int W = g.W, H = g.H;
     const int vc = blockIdx.y;
@@ -436,61 +508,114 @@ __global__ void __launch_bounds__(SWEEP_Q_THREADS) k_support_sweep_q(const uint4
         L_m2 = desc0 + size_t(v - 2) * W; L_p2 = desc0 + size_t(v + 2) * W;
         R_m2 = desc1 + size_t(v - 2) * W; R_p2 = desc1 + size_t(v + 2) * W;
     }
+    const int n_seg = c_end - c_begin;
+    for (int i = threadIdx.x; i < n_seg; i += blockDim.x) res[i] = -1;
+    if (threadIdx.x == 0) nlst = 0;
     __syncthreads();
     if (SMEM && !mbar_wait_bounded(&bar, 0, MBAR_WAIT_LIMIT)) {
         if (threadIdx.x == 0) atomicOr(err, ERRF_TMA_TIMEOUT);
         mbar_wait_bounded(&bar, 0, MBAR_WAIT_LIMIT);   // let the copies in flight land before exiting
         return;
     }
-    const int j = threadIdx.x % Q, per_pass = blockDim.x / Q;
-    const int n_seg = c_end - c_begin;
+    const int j = threadIdx.x % Q, grp = threadIdx.x / Q, per_pass = blockDim.x / Q;
+    // candidates that pass the texture and range tests (the learned search set first, with PROP)
     const int passes = (n_seg + per_pass - 1) / per_pass;   // uniform: every lane joins the shuffles
-    // left view: candidates of the segment, swept L->R
     for (int pass = 0; pass < passes; ++pass) {
-        const int ci = c_begin + pass * per_pass + int(threadIdx.x) / Q;
+        const int k = pass * per_pass + grp, ci = c_begin + k;
         const int u = ci * g.step;
         bool active = false;
         int dmax = 0;
-        if (ci < c_end && u >= 5 && u <= W - 6 && texture16(desc0[size_t(v) * W + u]) >= p.support_texture) {
+        if (k < n_seg && u >= 5 && u <= W - 6 && texture16(desc0[size_t(v) * W + u]) >= p.support_texture) {
             dmax = min(g.D, u - 5);
             active = dmax - g.dmin >= 10;
         }
-        Best2 st{PK_INF, PK_INF};
-        if (active) {
-            int da, db;
-            slice_of(g.dmin, dmax, j, Q, da, db);
-            st = sweep_slice<-1>(L_m2, L_p2, R_m2, R_p2, u, g.dmin, da, db);
-        }
-        const int r = group_decide<Q>(st, p.support_threshold);
-        if (ci < c_end && j == 0) res[ci - c_begin] = active ? r : -1;
-    }
-    __syncthreads();
-    // right view: re-match accepted candidates from u - d
-    for (int pass = 0; pass < passes; ++pass) {
-        const int ci = c_begin + pass * per_pass + int(threadIdx.x) / Q;
-        const int dl = ci < c_end ? res[ci - c_begin] : -1;
-        bool active = false;
-        int ur = 0, dmax = 0;
-        if (dl >= 0) {
-            ur = ci * g.step - dl;
-            if (texture16(desc1[size_t(v) * W + ur]) >= p.support_texture) {
-                dmax = min(g.D, W - ur - 5);
-                active = dmax - g.dmin >= 10;
+        bool settled = false;
+        if (PROP) {
+            const uint32_t bset = active ? bins[size_t(vc) * g.cw + ci] : 0xffffffffu;
+            const int w = pn::bin_width(g.D);
+            Best2 sl{PK_INF, PK_INF};
+            if (bset != 0xffffffffu)
+                sl = restricted_slice<-1>(L_m2, L_p2, R_m2, R_p2, u, g.dmin, dmax, bset, w, j, Q);
+            const int rl = group_decide_unique<Q>(sl, p.support_threshold);
+            bool tryr = false;
+            int ur = 0, dmaxr = 0;
+            if (rl >= 0) {
+                ur = u - rl;
+                dmaxr = min(g.D, W - ur - 5);
+                tryr = texture16(desc1[size_t(v) * W + ur]) >= p.support_texture && dmaxr - g.dmin >= 10;
+            }
+            Best2 sr{PK_INF, PK_INF};
+            if (tryr) sr = restricted_slice<1>(R_m2, R_p2, L_m2, L_p2, ur, g.dmin, dmaxr, bset, w, j, Q);
+            const int rr = group_decide_unique<Q>(sr, p.support_threshold);
+            settled = tryr && rr >= 0 && abs(rl - rr) <= p.lr_threshold;
+            if (j == 0 && active) {
+                atomicAdd(&stats[settled ? 0 : 1], 1);
+                if (settled) res[k] = rl | SETTLED;
             }
         }
-        Best2 st{PK_INF, PK_INF};
-        if (active) {
-            int da, db;
-            slice_of(g.dmin, dmax, j, Q, da, db);
-            st = sweep_slice<1>(R_m2, R_p2, L_m2, L_p2, ur, g.dmin, da, db);
-        }
-        const int dr = group_decide<Q>(st, p.support_threshold);
-        __syncwarp();
-        if (ci < c_end && j == 0) res[ci - c_begin] = (active && dr >= 0 && abs(dl - dr) <= p.lr_threshold) ? dl : -1;
+        if (j == 0 && active && !settled) lst[atomicAdd(&nlst, 1)] = int16_t(k);
     }
     __syncthreads();
-    for (int ci = c_begin + threadIdx.x; ci < c_end; ci += blockDim.x)
-        can_out[size_t(vc) * g.cw + ci] = res[ci - c_begin];
+    // left view: full L->R sweeps of the listed candidates
+    {
+        const int nl = nlst;
+        const int lp = (nl + per_pass - 1) / per_pass;
+        for (int pass = 0; pass < lp; ++pass) {
+            const int q = pass * per_pass + grp;
+            const bool active = q < nl;
+            const int k = active ? lst[q] : 0;
+            const int u = (c_begin + k) * g.step;
+            Best2 st{PK_INF, PK_INF};
+            if (active) {
+                int da, db;
+                slice_of(g.dmin, min(g.D, u - 5), j, Q, da, db);
+                st = sweep_slice<-1>(L_m2, L_p2, R_m2, R_p2, u, g.dmin, da, db);
+            }
+            const int r = group_decide<Q>(st, p.support_threshold);
+            if (active && j == 0) res[k] = r;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) nlst = 0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < n_seg; k += blockDim.x) {
+        const int r = res[k];
+        if (r >= 0 && !(r & SETTLED)) lst[atomicAdd(&nlst, 1)] = int16_t(k);
+    }
+    __syncthreads();
+    // right view: re-match the candidates the full left sweep accepted, from u - d
+    {
+        const int nl = nlst;
+        const int rp = (nl + per_pass - 1) / per_pass;
+        for (int pass = 0; pass < rp; ++pass) {
+            const int q = pass * per_pass + grp;
+            const int k = q < nl ? lst[q] : 0;
+            const int dl = q < nl ? res[k] : -1;
+            bool active = false;
+            int ur = 0, dmax = 0;
+            if (dl >= 0) {
+                ur = (c_begin + k) * g.step - dl;
+                if (texture16(desc1[size_t(v) * W + ur]) >= p.support_texture) {
+                    dmax = min(g.D, W - ur - 5);
+                    active = dmax - g.dmin >= 10;
+                }
+            }
+            Best2 st{PK_INF, PK_INF};
+            if (active) {
+                int da, db;
+                slice_of(g.dmin, dmax, j, Q, da, db);
+                st = sweep_slice<1>(R_m2, R_p2, L_m2, L_p2, ur, g.dmin, da, db);
+            }
+            const int dr = group_decide<Q>(st, p.support_threshold);
+            __syncwarp();
+            if (q < nl && j == 0) res[k] = (active && dr >= 0 && abs(dl - dr) <= p.lr_threshold) ? dl : -1;
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < n_seg; k += blockDim.x) {
+        const int r = res[k];
+        can_out[size_t(vc) * g.cw + c_begin + k] = r >= 0 ? (r & ~SETTLED) : -1;
+    }
 }
 
 // removeInconsistentSupportPoints with snapshot semantics: reads can_in,
@@ -794,8 +919,22 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
         int qseg = imax(1, (g.cw + qsegs - 1) / qsegs);
         qseg = (qseg + 3) & ~3;
         const int threads = imin(qseg, SWEEP_Q_THREADS / Q) * Q;
-        cudaFuncSetAttribute(k_support_sweep_q<Q, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        launch_k(k_support_sweep_q<Q, true>, dim3(qsegs, rows), threads, smem, st, desc0, desc1, can_lr, g, p, qseg, err);
+        cudaFuncSetAttribute(k_support_sweep_q<Q, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(smem));
+        launch_k(k_support_sweep_q<Q, true, false>, dim3(qsegs, rows), threads, smem, st, desc0, desc1, can_lr, g, p,
+                 qseg, err, nullptr, nullptr);
+    } else if (bins && smem <= 200 * 1024) {
+        // learned proposal: the same kernel, search sets first, fallbacks compacted
+        constexpr int Q = 8;
+        const long long cands = (long long)g.cw * imax(rows, 1);
+        const int want = int(imin(256, imax(32, int((cands + 2 * num_sms - 1) / (2 * num_sms)))));
+        const int qsegs = imax(1, (g.cw + want - 1) / want);
+        int qseg = imax(1, (g.cw + qsegs - 1) / qsegs);
+        qseg = (qseg + 3) & ~3;
+        const int threads = imin(qseg, SWEEP_Q_THREADS / Q) * Q;
+        cudaFuncSetAttribute(k_support_sweep_q<Q, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        launch_k(k_support_sweep_q<Q, true, true>, dim3(qsegs, rows), threads, smem, st, desc0, desc1, can_lr, g, p,
+                 qseg, err, bins, stats);
     } else if (smem <= 200 * 1024) {
         if (bins) {
             cudaFuncSetAttribute(k_support_sweep<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));

@@ -119,6 +119,6 @@ bool post_fuses_speckle(const DevParams& p, bool median, bool adaptive_mean);
 
 // Post-filters on nviews (1 or 2) disparity images.
 cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams& p, bool median, bool adaptive_mean,
-                        unsigned* err, cudaStream_t st, int* nlaunch);
+                        unsigned* err, cudaStream_t st, int* nlaunch, int num_sms);
 
 }  // namespace elas
