@@ -60,6 +60,7 @@ struct elas_handle {
     int32_t* usize[2] = {nullptr, nullptr};      // segment sizes per view
     int32_t* roots[2] = {nullptr, nullptr};      // tile-local roots of the speckle labelling per view
     unsigned* err = nullptr;
+    unsigned* err_host = nullptr;   // pinned copy of the error word (read back after each host-buffer call)
 
     // per-stage timing
     bool timing = false;
@@ -480,11 +481,9 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     n += 4;
     CK(mark(ELAS_TIME_COMPACT));
     const int corners = p.add_corners ? 1 : 0;
-    CK(launch_compact(h->can, h->row_cnt, h->row_off, h->uvd, h->x0, h->x1, h->y, g, st, corners));
-    n += 3 + corners;
+    CK(launch_compact(h->can, h->row_cnt, h->row_off, h->uvd, h->x0, h->x1, h->y, g, st, corners, &n));
     CK(mark(ELAS_TIME_GRID));
-    CK(launch_grid(h->can, h->gtmp0, h->gtmp1, h->grid0, h->grid1, g, st));
-    n += 2;
+    CK(launch_grid(h->can, h->gtmp0, h->gtmp1, h->grid0, h->grid1, g, st, &n));
     CK(mark(ELAS_TIME_DELAUNAY));
     CK(launch_delaunay(h->del[0], h->del[1], h->row_off, g.ch + corners, g.cw * g.ch + 6 * corners, h->num_sms,
                        h->cluster_size, h->err, st, &n, (h->test_flags & ELAS_TEST_FLIP_GLOBAL) != 0,
@@ -697,9 +696,10 @@ int check_batch(elas_handle* h, int n, const int32_t* dims, const int32_t* dmax)
 }
 
 int check_device_errors(elas_handle* h, cudaStream_t st) {
-    unsigned e = 0;
-    CK(cudaMemcpyAsync(&e, h->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    if (!h->err_host) CK(cudaHostAlloc(reinterpret_cast<void**>(&h->err_host), sizeof(unsigned), cudaHostAllocDefault));
+    CK(cudaMemcpyAsync(h->err_host, h->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    const unsigned e = *h->err_host;
     if (e & ERRF_FLIP_LIMIT) return fail(h, ELAS_ERR_TIMEOUT, "edge flipping hit its round limit");
     if (e) return fail(h, ELAS_ERR_INTERNAL, "device consistency check failed, flags " + std::to_string(e));
     return ELAS_OK;
@@ -849,6 +849,7 @@ int elas_b200_destroy(elas_handle* h) {
         cudaDeviceSynchronize();
         cudaFree(h->arena);
     }
+    if (h->err_host) cudaFreeHost(h->err_host);
     delete h;
     return ELAS_OK;
 }

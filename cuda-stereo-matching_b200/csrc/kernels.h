@@ -49,10 +49,10 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
                            cudaStream_t st, const uint32_t* bins = nullptr, int32_t* stats = nullptr);
 
 cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_off, int32_t* uvd, int32_t* x0,
-                           int32_t* x1, int32_t* y, const Geom& g, cudaStream_t st, int corners = 0);
+                           int32_t* x1, int32_t* y, const Geom& g, cudaStream_t st, int corners, int* nlaunch);
 
 cudaError_t launch_grid(const int32_t* can, uint32_t* tmp0, uint32_t* tmp1, uint32_t* grid0, uint32_t* grid1,
-                        const Geom& g, cudaStream_t st);
+                        const Geom& g, cudaStream_t st, int* nlaunch);
 
 // force_global: flip every problem with the global-memory kernel (tests);
 // round_limit > 0 caps the flip rounds (ERRF_FLIP_LIMIT when hit).
