@@ -50,10 +50,14 @@ def build(force=False, verbose=False, ptxas_info=False):
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)
     if force or _stale(OUT, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lgomp", "-lpthread"]
+        # link beside the library and rename it into place, so that a reader
+        # never sees a partly written file
+        tmp = OUT + ".tmp"
+        cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lgomp", "-lpthread"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
+        os.replace(tmp, OUT)
     # the command-line front end (host code linked against the library)
     if force or _stale(CLI, CLI_SOURCES + [OUT, os.path.join(HERE, "..", "include", "elas_b200.h")]):
         cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(HERE, "..", "include"), CLI_SOURCES[0], "-o", CLI,

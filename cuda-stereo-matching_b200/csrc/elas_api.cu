@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -443,8 +444,11 @@ void free_pn(elas_handle* h) {
     if (h->pw.b) cudaFree(h->pw.b);
 }
 
+// host_out: out0/out1 are device-mapped pinned host memory.  Every
+// intermediate then stays in device memory and only the last pass of each
+// view writes there, so the results cross PCIe while that pass computes.
 int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float* out0, float* out1, int W, int H,
-                 cudaStream_t st) {
+                 cudaStream_t st, bool host_out = false) {
     const elas_params& p = h->params;
     Geom g = geom_of(W, H, p);
     DevParams dp = dev_params(p);
@@ -510,8 +514,9 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     // removal applied inside the tile filter), in the scratch maps, so that
     // the last pass writes the outputs.
     const int nviews = p.postprocess_only_left ? 1 : 2;
-    const bool from_tmp = post_fuses_speckle(dp, p.filter_median, p.filter_adaptive_mean);
+    const bool from_tmp = host_out || post_fuses_speckle(dp, p.filter_median, p.filter_adaptive_mean);
     float* outs[2] = {out0, out1};
+    float* dev_outs[2] = {host_out ? h->out0 : out0, host_out ? h->out1 : out1};   // device partners of tmp
     float* start[2];
     for (int k = 0; k < 2; ++k) start[k] = from_tmp && k < nviews ? h->tmp[k] : outs[k];
     CK(launch_lr(h->raw0, h->raw1, h->lr0, h->lr1, start[0], start[1], g, p.lr_threshold, st, sub));
@@ -520,7 +525,7 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     PostViews pv;
     for (int k = 0; k < 2; ++k) {
         pv.cur[k] = start[k];
-        pv.nxt[k] = start[k] == outs[k] ? h->tmp[k] : outs[k];
+        pv.nxt[k] = start[k] == dev_outs[k] ? h->tmp[k] : dev_outs[k];
         pv.out[k] = outs[k];
         pv.lab[k] = h->lab[k];
         pv.root[k] = h->root[k];
@@ -542,10 +547,11 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
 // only launch the graph.  A caller that is itself capturing gets the plain
 // launches, which join its capture.
 int run_pipeline_graphed(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float* out0, float* out1, int W,
-                         int H, cudaStream_t st) {
+                         int H, cudaStream_t st, bool host_out = false) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(st, &cs));
-    if (!h->use_graphs || cs != cudaStreamCaptureStatusNone) return run_pipeline(h, img0, img1, out0, out1, W, H, st);
+    if (!h->use_graphs || cs != cudaStreamCaptureStatusNone)
+        return run_pipeline(h, img0, img1, out0, out1, W, H, st, host_out);
     const Geom g = geom_of(W, H, h->params);
     int rc = ensure_workspace(h, g);
     if (rc != ELAS_OK) return rc;
@@ -556,7 +562,7 @@ int run_pipeline_graphed(elas_handle* h, const uint8_t* img0, const uint8_t* img
     std::vector<int64_t> sig = {int64_t(img0), int64_t(img1), int64_t(out0), int64_t(out1), W, H,
                                 int64_t(h->arena), int64_t(h->arena_bytes), int64_t(h->pn_in), int64_t(h->pn_bins),
                                 int64_t(h->pn_stats), h->timing ? 1 : 0, h->prop ? 1 : 0, h->prop_version,
-                                h->test_flags, h->flip_round_limit};
+                                h->test_flags, h->flip_round_limit, host_out ? 1 : 0};
     int64_t pw[sizeof(elas_params) / 8 + 1] = {};
     std::memcpy(pw, &h->params, sizeof(elas_params));
     for (int64_t x : pw) sig.push_back(x);
@@ -570,13 +576,13 @@ int run_pipeline_graphed(elas_handle* h, const uint8_t* img0, const uint8_t* img
     }
     if (sig != h->single_seen) {
         h->single_seen = sig;
-        return run_pipeline(h, img0, img1, out0, out1, W, H, st);
+        return run_pipeline(h, img0, img1, out0, out1, W, H, st, host_out);
     }
     if (!h->own_stream) CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     if (h->single_exec) { cudaGraphExecDestroy(h->single_exec); h->single_exec = nullptr; }
     const long long before = h->launches;
     CK(cudaStreamBeginCapture(h->own_stream, cudaStreamCaptureModeThreadLocal));
-    rc = run_pipeline(h, img0, img1, out0, out1, W, H, h->own_stream);
+    rc = run_pipeline(h, img0, img1, out0, out1, W, H, h->own_stream, host_out);
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(h->own_stream, &graph);
     if (rc != ELAS_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
@@ -693,6 +699,23 @@ int check_batch(elas_handle* h, int n, const int32_t* dims, const int32_t* dmax)
         if (rc != ELAS_OK) return rc;
     }
     return ELAS_OK;
+}
+
+// The device address of a pinned, device-mapped host buffer; null for any
+// other pointer (pageable memory, device memory) or when
+// ELAS_B200_ZERO_COPY=0 is set in the environment.
+float* mapped_host(float* p) {
+    static const bool on = [] {
+        const char* e = std::getenv("ELAS_B200_ZERO_COPY");
+        return !(e && e[0] == '0');
+    }();
+    if (!on) return nullptr;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost && a.devicePointer ? static_cast<float*>(a.devicePointer) : nullptr;
 }
 
 int check_device_errors(elas_handle* h, cudaStream_t st) {
@@ -898,6 +921,15 @@ int elas_b200_process(elas_handle* h, const uint8_t* left, const uint8_t* right,
     const size_t px = size_t(W) * H;
     CK(cudaMemcpyAsync(h->img0, left, px, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(h->img1, right, px, cudaMemcpyHostToDevice, st));
+    // Pinned, device-mapped output buffers receive the results from the
+    // last post-filter pass itself (no separate device-to-host copy).
+    float* m1 = mapped_host(disp_left);
+    float* m2 = mapped_host(disp_right);
+    if (m1 && m2) {
+        rc = run_pipeline_graphed(h, h->img0, h->img1, m1, m2, W, H, st, true);
+        if (rc != ELAS_OK) return rc;
+        return check_device_errors(h, st);
+    }
     rc = run_pipeline_graphed(h, h->img0, h->img1, h->out0, h->out1, W, H, st);
     if (rc != ELAS_OK) return rc;
     const size_t po = out_pixels(W, H, h->params);

@@ -534,6 +534,12 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         launched += 2;
     }
     if (tile_gap || adaptive_mean || median) {
+        // the tile pass is the chain's last: it writes the final buffers
+        // directly unless one of them is its own input
+        bool direct = true;
+        for (int k = 0; k < nviews; ++k) direct = direct && pv.out[k] != pv.cur[k];
+        if (direct)
+            for (int k = 0; k < nviews; ++k) pv.nxt[k] = pv.out[k];
         const int tiles = ((W + PT - 1) / PT) * ((H + PT - 1) / PT) * nviews;
         const int grid = imax(1, imin(tiles, 2 * num_sms));
         const size_t smem = adaptive_mean ? WT_N * sizeof(float) : 0;
@@ -563,9 +569,9 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         flip();
         launched += 1;
     }
-    for (int k = 0; k < nviews; ++k)
+    for (int k = 0; k < nviews; ++k)   // cudaMemcpyDefault: the final buffer may be mapped host memory
         if (pv.cur[k] != pv.out[k])
-            cudaMemcpyAsync(pv.out[k], pv.cur[k], size_t(n) * sizeof(float), cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(pv.out[k], pv.cur[k], size_t(n) * sizeof(float), cudaMemcpyDefault, st);
     if (nlaunch) *nlaunch += launched;
     return cudaGetLastError();
 }

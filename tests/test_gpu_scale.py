@@ -210,3 +210,38 @@ def test_group_batch_equals_singles(elas):
     assert set(plan.tolist()) == {0, 1}
     for i, ((s1, s2), x1, x2) in enumerate(zip(ref, d1, d2)):
         assert np.array_equal(s1, x1) and np.array_equal(s2, x2), i
+
+
+@pytest.mark.parametrize("mode", ["config", "reference", "only_left", "subsampling"])
+def test_pinned_outputs_equal_pageable(elas, mode):
+    """Host-buffer calls whose output buffers are pinned (device-mapped)
+    receive the maps from the last post-filter pass directly; the maps equal
+    those of the same call with pageable buffers, bit for bit, on the first
+    (eager) and the later (graph) calls."""
+    import ctypes
+
+    import torch
+
+    L, R, _, _ = eb.synth_pair(1, 51)
+    H, W = L.shape
+    p = eb.params_reference() if mode == "reference" else eb.params_config(255)
+    if mode == "only_left":
+        p.postprocess_only_left = True
+    if mode == "subsampling":
+        p.subsampling = True
+    elas.set_params(p)
+    ref1, ref2 = elas.process(L, R)
+    shape = ref1.shape
+    d1 = torch.full(shape, 7.0, dtype=torch.float32).pin_memory()
+    d2 = torch.full(shape, 7.0, dtype=torch.float32).pin_memory()
+    dims = np.array([W, H, W], np.int32)
+    lib = eb.library()
+    for call in range(3):
+        d1.fill_(7.0)
+        d2.fill_(7.0)
+        rc = lib.elas_b200_process(elas._h, L.ctypes.data_as(ctypes.c_void_p), R.ctypes.data_as(ctypes.c_void_p),
+                                   ctypes.c_void_p(d1.data_ptr()), ctypes.c_void_p(d2.data_ptr()),
+                                   dims.ctypes.data_as(ctypes.c_void_p), None)
+        elas._check(rc)
+        assert np.array_equal(d1.numpy(), ref1), (mode, call)
+        assert np.array_equal(d2.numpy(), ref2), (mode, call)
