@@ -52,7 +52,6 @@ struct elas_handle {
     DelDev del[2]{};
     uint32_t *prior0 = nullptr, *prior1 = nullptr;
     void* rast = nullptr;   // per-triangle plane/edge set-up of both views
-    PriorBins pbins{};      // triangles binned by image row, both views
     float *raw0 = nullptr, *raw1 = nullptr, *lr0 = nullptr, *lr1 = nullptr;
     float *out0 = nullptr, *out1 = nullptr;
     float* tmp[2] = {nullptr, nullptr};          // post-filter ping-pong buffer per view
@@ -266,11 +265,6 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         D.Hmax = uint32_t(hmax);
     }
     h->rast = take(2 * tmax * raster_bytes());
-    const size_t bin_cap = prior_bin_capacity(g, int(tmax));
-    h->pbins.cnt = (int32_t*)take(2 * (size_t(g.H) + 1) * 4);
-    h->pbins.off = (int32_t*)take(2 * (size_t(g.H) + 1) * 4);
-    h->pbins.list = (int32_t*)take(2 * bin_cap * 4);
-    h->pbins.cap = int(bin_cap);
     h->prior0 = (uint32_t*)take(px * 4);
     h->prior1 = (uint32_t*)take(px * 4);
     h->raw0 = (float*)take(px * 4);
@@ -494,8 +488,8 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
                        h->flip_round_limit));
     CK(mark(ELAS_TIME_PRIOR));
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
-                    h->rast, h->pbins, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1,
-                    h->num_sms, h->err, st, &n));
+                    h->rast, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1, h->num_sms, st,
+                    &n));
     int shape = 256;
     rc = dense_threads_for(h, g, dp, st, &n, &shape);
     if (rc != ELAS_OK) return rc;

@@ -3,14 +3,12 @@
 // Prior: replaces kerComputeDepthApproximation
 // (src/Kernels/KerComputeDisparity.cu:9-152), one thread per triangle with
 // long serial scanline loops.  Here one thread per triangle solves the plane
-// (same double Gauss-Jordan as kerSolve, :321-375), sets up the edges and
-// finds the rows it writes; the triangles are then binned by row and one
-// CTA per row paints its row in shared memory and writes it once.  A pixel
-// covered by more than one triangle (rounding at shared vertices) must keep
-// the last triangle in list order, as a sequential rasteriser would; the
-// row is therefore painted with a 32-bit atomicMax of
-// (triangle+1) << pshift | d_plane, which makes the result independent of
-// scheduling.  d_plane is stored clamped to
+// (same double Gauss-Jordan as kerSolve, :321-375) and sets up the edges,
+// then a warp per triangle splits its columns.  A pixel covered by more than one
+// triangle (rounding at shared vertices) must keep the last triangle in
+// list order, as a sequential rasteriser would; the prior is therefore
+// written with a 32-bit atomicMax of (triangle+1) << pshift | d_plane, which
+// makes the result independent of scheduling.  d_plane is stored clamped to
 // [0, disp_max + plane_radius + 1] (0 standing for every d_plane <= 0): the
 // dense step treats all values beyond either end alike.
 //
@@ -71,29 +69,7 @@ struct Raster {
     float pa, pb, pc;
     float A_u, B_u, C_u;
     float AB_a, AC_a, BC_a, AB_b, AC_b, BC_b;
-    int r0, r1;        // rows the triangle writes lie in [r0, r1] (r0 > r1: none)
 };
-
-// Rows of one part of the scan-line raster: columns u in [ua, ub) write the
-// rows [va, vb) with va = max(min(v1, v2), 0), vb = min(max(v1, v2), H),
-// v1 from the long edge AC and v2 from the part's edge.  Each of v1, v2 is
-// a truncated fma of u, monotone in u, so the extremes over the part are at
-// its first and last column.
-__device__ __forceinline__ int raster_row(float a, float b, int u) {
-    return int(__float2uint_rz(__fmaf_rn(a, float(u), b)));
-}
-__device__ void part_rows(const Raster& R, int part, int W, int H, int& r0, int& r1) {
-    const int ua = part ? int(R.B_u) : int(R.A_u), ub = part ? int(R.C_u) : int(R.B_u);
-    const int u0 = imax(ua, 0), u1 = imin(ub, W) - 1;
-    if (ua == ub || u0 > u1) return;
-    const float ea = part ? R.BC_a : R.AB_a, eb = part ? R.BC_b : R.AB_b;
-    const int a0 = raster_row(R.AC_a, R.AC_b, u0), a1 = raster_row(R.AC_a, R.AC_b, u1);
-    const int b0 = raster_row(ea, eb, u0), b1 = raster_row(ea, eb, u1);
-    const int lo = imax(imin(imin(a0, a1), imin(b0, b1)), 0);
-    const int hi = imin(imax(imax(a0, a1), imax(b0, b1)), H) - 1;
-    r0 = imin(r0, lo);
-    r1 = imax(r1, hi);
-}
 
 __device__ void setup_triangle(const int32_t* tri, const int32_t* can, const int32_t* uvd, int cw, int step,
                                bool right, Raster& R) {
@@ -141,15 +117,13 @@ __device__ void setup_triangle(const int32_t* tri, const int32_t* can, const int
     R.BC_b = __fmaf_rn(-R.BC_a, B_u, B_v);
 }
 
-// One thread per (view, triangle): plane and edge set-up, the triangle's
-// row range, and its contribution to the per-row counts as a difference
-// array (+1 at its first row, -1 after its last).
+// One thread per (view, triangle): plane and edge set-up, once.
 __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__ tri0,
                                                      const int32_t* __restrict__ tri1,
                                                      const int32_t* __restrict__ ctr0,
                                                      const int32_t* __restrict__ ctr1,
                                                      const int32_t* __restrict__ can, const int32_t* __restrict__ uvd,
-                                                     Raster* __restrict__ rast, int Tmax, Geom g, int32_t* diff) {
+                                                     Raster* __restrict__ rast, int Tmax, Geom g) {
     grid_dep_wait();
     const int T0 = ctr0[0], T1 = ctr1[0];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T0 + T1; i += gridDim.x * blockDim.x) {
@@ -157,138 +131,46 @@ __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__
         const int t = right ? i - T0 : i;
         Raster R;
         setup_triangle((right ? tri1 : tri0) + 3 * size_t(t), can, uvd, g.cw, g.step, right, R);
-        int r0 = g.H, r1 = -1;
-        part_rows(R, 0, g.W, g.H, r0, r1);
-        part_rows(R, 1, g.W, g.H, r0, r1);
-        R.r0 = r0;
-        R.r1 = r1;
         rast[(right ? Tmax : 0) + t] = R;
-        if (r0 <= r1) {
-            int32_t* d = diff + (right ? g.H + 1 : 0);
-            atomicAdd(d + r0, 1);
-            atomicAdd(d + r1 + 1, -1);
-        }
     }
 }
 
-// One 1024-thread block per view: counts from the difference array, their
-// exclusive prefix sums (the row offsets), and the fill cursors (written
-// over the difference array).
-__global__ void __launch_bounds__(1024) k_prior_scan(int32_t* diff, int32_t* off, int H) {
+// One warp per (view, triangle), lanes over columns; every pixel keeps the
+// last covering triangle through atomicMax on the packed value.
+__global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict__ ctr0,
+                                                      const int32_t* __restrict__ ctr1,
+                                                      const Raster* __restrict__ rast, int Tmax,
+                                                      uint32_t* prior0, uint32_t* prior1, Geom g, int pshift,
+                                                      int dcap) {
     grid_dep_wait();
-    __shared__ int ws[33];
-    int32_t* d = diff + blockIdx.x * (H + 1);
-    int32_t* o = off + blockIdx.x * (H + 1);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int per = (H + 1023) / 1024, i0 = imin(tid * per, H), i1 = imin(i0 + per, H);
-    auto scan = [&](int x, int& total) {    // exclusive block scan
-        int y = x;
-#pragma unroll
-        for (int k = 1; k < 32; k <<= 1) {
-            const int z = __shfl_up_sync(0xffffffffu, y, k);
-            if (lane >= k) y += z;
-        }
-        if (lane == 31) ws[warp] = y;
-        __syncthreads();
-        if (warp == 0) {
-            const int w = ws[lane];
-            int c = w;
-#pragma unroll
-            for (int k = 1; k < 32; k <<= 1) {
-                const int z = __shfl_up_sync(0xffffffffu, c, k);
-                if (lane >= k) c += z;
-            }
-            ws[lane] = c - w;
-            if (lane == 31) ws[32] = c;
-        }
-        __syncthreads();
-        const int r = y - x + ws[warp];
-        total = ws[32];
-        __syncthreads();
-        return r;
-    };
-    int sd = 0, total = 0;
-    for (int i = i0; i < i1; ++i) sd += d[i];
-    int c = scan(sd, total);               // count at row i0 - 1 (before the chunk's differences)
-    int sc = 0;
-    for (int i = i0; i < i1; ++i) { c += d[i]; sc += c; }
-    int base = scan(sc, total);
-    c -= sd;                                // back to the count before the chunk
-    for (int i = i0; i < i1; ++i) {
-        c += d[i];
-        o[i] = base;
-        d[i] = base;                        // fill cursor
-        base += c;
-    }
-    if (tid == 0) o[H] = total;
-}
-
-// One thread per (view, triangle): append the triangle to the list of each
-// row of its range (the order within a row carries no meaning: the raster
-// keeps the largest triangle index per pixel).
-__global__ void __launch_bounds__(256) k_prior_fill(const int32_t* __restrict__ ctr0, const int32_t* __restrict__ ctr1,
-                                                    const Raster* __restrict__ rast, int Tmax, int H, int32_t* cursor,
-                                                    int32_t* list, int cap, unsigned* err) {
-    grid_dep_wait();
+    const int lane = threadIdx.x & 31;
     const int T0 = ctr0[0], T1 = ctr1[0];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T0 + T1; i += gridDim.x * blockDim.x) {
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < T0 + T1; i += nw) {
         const bool right = i >= T0;
         const int t = right ? i - T0 : i;
-        const Raster& R = rast[(right ? Tmax : 0) + t];
-        int32_t* cur = cursor + (right ? H + 1 : 0);
-        int32_t* l = list + (right ? size_t(cap) : 0);
-        for (int r = R.r0; r <= R.r1; ++r) {
-            const int pos = atomicAdd(cur + r, 1);
-            if (pos < cap) l[pos] = t;
-            else atomicOr(err, ERRF_BOUNDS);
-        }
-    }
-}
-
-// One CTA per (row, view): every triangle of the row's list paints the
-// columns it covers in this row into a shared-memory row with atomicMax of
-// (triangle+1) << pshift | d_plane -- the last triangle in list order wins,
-// as a sequential rasteriser writing the triangles in order would leave it --
-// and the row is then written out whole (0 where nothing covers a pixel).
-// Coverage and values are the reference's scan-line expressions
-// (KerComputeDisparity.cu:57-150) with its contraction made explicit.
-__global__ void __launch_bounds__(256) k_prior_rows(const Raster* __restrict__ rast, int Tmax,
-                                                    const int32_t* __restrict__ off,
-                                                    const int32_t* __restrict__ list, int cap, uint32_t* prior0,
-                                                    uint32_t* prior1, Geom g, int pshift, int dcap) {
-    grid_dep_wait();
-    extern __shared__ uint32_t prow[];
-    const int v = blockIdx.x, view = blockIdx.y, W = g.W;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    for (int u = tid; u < W; u += blockDim.x) prow[u] = 0u;
-    __syncthreads();
-    const int32_t* o = off + view * (g.H + 1);
-    const int b = imin(o[v], cap), e = imin(o[v + 1], cap);
-    const int32_t* l = list + (view ? size_t(cap) : 0);
-    const Raster* rs = rast + (view ? Tmax : 0);
-    const float fv = float(v);
-    for (int k = b + warp; k < e; k += nw) {
-        const int t = l[k];
-        const Raster R = rs[t];
+        const Raster R = rast[(right ? Tmax : 0) + t];
         const uint32_t tag = uint32_t(t + 1) << pshift;
+        uint32_t* prior = right ? prior1 : prior0;
         for (int part = 0; part < 2; ++part) {
             const int ua = part ? int(R.B_u) : int(R.A_u), ub = part ? int(R.C_u) : int(R.B_u);
             if (ua == ub) continue;
             const float ea = part ? R.BC_a : R.AB_a, eb = part ? R.BC_b : R.AB_b;
-            for (int u = imax(ua, 0) + lane; u < imin(ub, W); u += 32) {
-                const int v1 = raster_row(R.AC_a, R.AC_b, u), v2 = raster_row(ea, eb, u);
+            for (int u = imax(ua, 0) + lane; u < imin(ub, g.W); u += 32) {
+                const float fu = float(u);
+                const int v1 = int(__float2uint_rz(__fmaf_rn(R.AC_a, fu, R.AC_b)));
+                const int v2 = int(__float2uint_rz(__fmaf_rn(ea, fu, eb)));
                 const int va = imax(imin(v1, v2), 0), vb = imin(imax(v1, v2), g.H);
-                if (v < va || v >= vb) continue;
-                const float dp = __fadd_rn(__fmaf_rn(R.pa, float(u), __fmul_rn(R.pb, fv)), R.pc);
-                int d = __float2int_rz(dp);
-                d = d <= 0 ? 0 : (d > dcap ? dcap : d);
-                atomicMax(&prow[u], tag | uint32_t(d));
+                auto value = [&](int v) {
+                    const float dp = __fadd_rn(__fmaf_rn(R.pa, fu, __fmul_rn(R.pb, float(v))), R.pc);
+                    int d = __float2int_rz(dp);
+                    d = d <= 0 ? 0 : (d > dcap ? dcap : d);
+                    return tag | uint32_t(d);
+                };
+                for (int v = va; v < vb; ++v) atomicMax(&prior[size_t(v) * g.W + u], value(v));
             }
         }
     }
-    __syncthreads();
-    uint32_t* out = (view ? prior1 : prior0) + size_t(v) * W;
-    for (int u = tid; u < W; u += blockDim.x) out[u] = prow[u];
 }
 
 // Candidate-list entries per grid cell kept in shared memory; cells with
@@ -521,27 +403,19 @@ __global__ void k_lr(const float* __restrict__ D1, const float* __restrict__ D2,
 
 }  // namespace
 
-size_t prior_bin_capacity(const Geom& g, int Tmax) {
-    // a row crosses about two triangles per support point of its lattice
-    // rows; twice that, plus four row entries per triangle
-    return size_t(4) * Tmax + size_t(4) * g.H * (size_t(g.cw) + 2);
-}
-
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
-                         int Tmax, const int32_t* can, const int32_t* uvd, void* rast, const PriorBins& bins,
-                         uint32_t* prior0, uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms,
-                         unsigned* err, cudaStream_t st, int* nlaunch) {
-    cudaMemsetAsync(bins.cnt, 0, size_t(2) * (g.H + 1) * sizeof(int32_t), st);
+                         int Tmax, const int32_t* can, const int32_t* uvd, void* rast, uint32_t* prior0,
+                         uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms, cudaStream_t st,
+                         int* nlaunch) {
+    size_t n = size_t(g.W) * g.H * sizeof(uint32_t);
+    cudaMemsetAsync(prior0, 0, n, st);
+    cudaMemsetAsync(prior1, 0, n, st);
     Raster* R = static_cast<Raster*>(rast);
-    const int tblocks = imax(1, imin(8 * num_sms, (2 * Tmax + 255) / 256));
-    launch_k(k_prior_setup, tblocks, 256, 0, st, tri0, tri1, ctr0, ctr1, can, uvd, R, Tmax, g, bins.cnt);
-    launch_k(k_prior_scan, 2, 1024, 0, st, bins.cnt, bins.off, g.H);
-    launch_k(k_prior_fill, tblocks, 256, 0, st, ctr0, ctr1, R, Tmax, g.H, bins.cnt, bins.list, bins.cap, err);
-    const size_t smem = size_t(g.W) * sizeof(uint32_t);
-    cudaFuncSetAttribute(k_prior_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    launch_k(k_prior_rows, dim3(g.H, 2), 256, smem, st, R, Tmax, bins.off, bins.list, bins.cap, prior0, prior1, g,
-             pshift, dcap);
-    if (nlaunch) *nlaunch += 4;
+    launch_k(k_prior_setup, imax(1, imin(8 * num_sms, (2 * Tmax + 255) / 256)), 256, 0, st, tri0, tri1, ctr0, ctr1, can,
+                                                                                      uvd, R, Tmax, g);
+    int blocks = imax(1, imin(16 * num_sms, (2 * Tmax + 7) / 8));
+    launch_k(k_prior_raster, blocks, 256, 0, st, ctr0, ctr1, R, Tmax, prior0, prior1, g, pshift, dcap);
+    if (nlaunch) *nlaunch += 2;
     return cudaGetLastError();
 }
 

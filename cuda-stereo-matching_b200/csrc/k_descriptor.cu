@@ -18,6 +18,7 @@
 // (u or v outside [3, size-4]) are written as zero; the reference leaves
 // them uninitialised.
 #include <cuda_runtime.h>
+#include <cstdlib>
 #include "common.cuh"
 #include "launch.cuh"
 #include "kernels.h"
@@ -36,24 +37,27 @@ __device__ __forceinline__ int sobel_u8(int s) {
     return q < 0 ? 0 : (q > 255 ? 255 : q);
 }
 
-// vec = 1: both image bases are 16-byte aligned, rows are staged by 16-byte
-// loads; vec = 0: byte loads (caller buffers of any alignment).
+// VEC: both image bases are 16-byte aligned and rows are staged by 16-byte
+// loads; otherwise by byte loads (caller buffers of any alignment).  Either
+// way the staged bytes are then laid out as a zero-padded tile, so the
+// Sobel pass reads shared memory with no bounds tests.
 template <bool VEC>
 __global__ void __launch_bounds__(256) k_descriptor(const uint8_t* __restrict__ img0,
                                                     const uint8_t* __restrict__ img1,
                                                     uint4* __restrict__ desc0,
                                                     uint4* __restrict__ desc1, int W, int H) {
     grid_dep_wait();
-    __shared__ __align__(16) uint8_t raw[IH][RW * 16];   // staged words of each tile row
+    __shared__ __align__(16) uint8_t raw[VEC ? IH : 1][RW * 16];   // staged words of each tile row
     __shared__ int roff[IH];                              // byte of image column u0 - 3 within raw[r]
+    __shared__ uint8_t im[IH][IW + 2];                    // the tile, 0 outside the image
     __shared__ uint8_t du[GH][GW];
     __shared__ uint8_t dv[GH][GW];
     const uint8_t* img = blockIdx.z ? img1 : img0;
     uint4* desc = blockIdx.z ? desc1 : desc0;
     const int u0 = blockIdx.x * TX, v0 = blockIdx.y * TY;
     const int tid = threadIdx.x;
-    const int ulo = imax(u0 - 3, 0), uhi = imin(u0 + TX + 3, W);   // image columns of the tile, [ulo, uhi)
     if (VEC) {
+        const int ulo = imax(u0 - 3, 0), uhi = imin(u0 + TX + 3, W);   // image columns of the tile, [ulo, uhi)
         for (int i = tid; i < IH * RW; i += 256) {
             const int r = i / RW, k = i % RW;
             const int v = v0 - 3 + r;
@@ -65,26 +69,22 @@ __global__ void __launch_bounds__(256) k_descriptor(const uint8_t* __restrict__ 
             if (a + size_t(k) * 16 < e)
                 reinterpret_cast<uint4*>(raw[r])[k] = *reinterpret_cast<const uint4*>(img + a + size_t(k) * 16);
         }
-    } else {
-        for (int i = tid; i < IH * IW; i += 256) {
-            const int r = i / IW, c = i % IW;
-            const int u = u0 - 3 + c, v = v0 - 3 + r;
-            if (c == 0) roff[r] = 0;
-            if (u >= 0 && u < W && v >= 0 && v < H) raw[r][c] = img[size_t(v) * W + u];
-        }
+        __syncthreads();
+    }
+    for (int i = tid; i < IH * IW; i += 256) {
+        const int r = i / IW, c = i % IW;
+        const int u = u0 - 3 + c, v = v0 - 3 + r;
+        uint8_t b = 0;
+        if (u >= 0 && u < W && v >= 0 && v < H) b = VEC ? raw[r][c + roff[r]] : img[size_t(v) * W + u];
+        im[r][c] = b;
     }
     __syncthreads();
-    // image byte at tile (r, c), i.e. (u, v) = (u0 - 3 + c, v0 - 3 + r); 0 outside the image
-    auto im = [&](int r, int c) -> int {
-        const int u = u0 - 3 + c, v = v0 - 3 + r;
-        return (u >= 0 && u < W && v >= 0 && v < H) ? int(raw[r][c + roff[r]]) : 0;
-    };
     for (int i = tid; i < GH * GW; i += 256) {
         int r = i / GW, c = i % GW;
         // image tile coordinates of (u, v) = (c + 1, r + 1)
-        int a00 = im(r, c), a01 = im(r, c + 1), a02 = im(r, c + 2);
-        int a10 = im(r + 1, c), a12 = im(r + 1, c + 2);
-        int a20 = im(r + 2, c), a21 = im(r + 2, c + 1), a22 = im(r + 2, c + 2);
+        int a00 = im[r][c], a01 = im[r][c + 1], a02 = im[r][c + 2];
+        int a10 = im[r + 1][c], a12 = im[r + 1][c + 2];
+        int a20 = im[r + 2][c], a21 = im[r + 2][c + 1], a22 = im[r + 2][c + 2];
         int sdu = a00 + 2 * a10 + a20 - a02 - 2 * a12 - a22;
         int sdv = a00 + 2 * a01 + a02 - a20 - 2 * a21 - a22;
         du[r][c] = uint8_t(sobel_u8(sdu));
@@ -114,7 +114,11 @@ __global__ void __launch_bounds__(256) k_descriptor(const uint8_t* __restrict__ 
 cudaError_t launch_descriptor(const uint8_t* img0, const uint8_t* img1, uint4* desc0, uint4* desc1,
                               int W, int H, cudaStream_t st) {
     dim3 grid((W + TX - 1) / TX, (H + TY - 1) / TY, 2);
-    const bool vec = ((reinterpret_cast<uintptr_t>(img0) | reinterpret_cast<uintptr_t>(img1)) & 15) == 0;
+    static const bool vec_on = [] {
+        const char* e = std::getenv("ELAS_B200_DESC_VEC");
+        return !(e && e[0] == '0');
+    }();
+    const bool vec = vec_on && ((reinterpret_cast<uintptr_t>(img0) | reinterpret_cast<uintptr_t>(img1)) & 15) == 0;
     if (vec) launch_k(k_descriptor<true>, grid, 256, 0, st, img0, img1, desc0, desc1, W, H);
     else launch_k(k_descriptor<false>, grid, 256, 0, st, img0, img1, desc0, desc1, W, H);
     return cudaGetLastError();

@@ -129,17 +129,6 @@ __global__ void k_uf_count(int32_t* lab, int32_t* __restrict__ root, int32_t* sz
 // was hooked, another local root of the same segment.
 constexpr int SPK_T = 32;
 
-// One slot per calling lane in the list whose length is *ctr: one atomic per
-// converged group of lanes.
-__device__ __forceinline__ int agg_add(int32_t* ctr) {
-    const unsigned mask = __activemask();
-    const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(ctr, __popc(mask));
-    base = __shfl_sync(mask, base, leader);
-    return base + __popc(mask & ((1u << lane) - 1u));
-}
-
 __device__ __forceinline__ int lfind(int* L, int x) {
     for (int it = 0; it < SPK_T * SPK_T; ++it) {
         const int p = L[x];
@@ -207,16 +196,23 @@ __global__ void __launch_bounds__(1024) k_spk_tile(PostViews pv, int W, int H, f
         const unsigned peers = __match_any_sync(0xffffffffu, r);
         if (r >= 0 && tx == __ffs(peers) - 1) atomicAdd(&C[r], __popc(peers));
     }
+    // the tile's local roots take consecutive list slots: one reservation per tile
+    __shared__ int n_roots, base;
+    if (t == 0) n_roots = 0;
+    __syncthreads();
+    const bool is_root = in && r == t;
+    const int slot = is_root ? atomicAdd(&n_roots, 1) : 0;
+    __syncthreads();
+    if (t == 0) base = n_roots > 0 ? atomicAdd(pv.roots[view], n_roots) : 0;
     __syncthreads();
     if (in) {
         const size_t i = size_t(y) * W + x;
         const int rx = blockIdx.x * SPK_T + (r & (SPK_T - 1)), ry = blockIdx.y * SPK_T + (r / SPK_T);
         pv.lab[view][i] = r >= 0 ? int(size_t(ry) * W + rx) : -1;
-        if (r == t) {                   // a local root: its count, its segment-size slot, its list entry
+        if (is_root) {                  // a local root: its count, its segment-size slot, its list entry
             pv.sz[view][i] = C[t];
             pv.root[view][i] = 0;
-            int32_t* roots = pv.roots[view];
-            roots[1 + agg_add(roots)] = int(i);
+            pv.roots[view][1 + base + slot] = int(i);
         }
     }
 }
@@ -358,27 +354,25 @@ __device__ __forceinline__ void sort9(float (&a)[9]) {
 
 // Adaptive-mean weights.  Every value the mean reads is a multiple of 1/4
 // (integer disparities, halves from the row gap pass, quarters from the
-// column pass) below 4096, so with the key K = 4 * d the weight of a valid
-// pair is WT[|K_q - K_p|], WT[j] = 1 / (1 + (j/4)^2) made by the same
-// correctly rounded operations as the direct formula.  Invalid pixels get a
-// key far away from every valid one, and indices past the valid range hold
-// weight 0, so an invalid neighbour adds 0 to both sums (bit for bit the
-// same as skipping it).
-constexpr int WT_N = 16384;                     // > 4 * 4095, the largest valid |K_q - K_p|
+// column pass) in [0, disp_max], so with the key K = 4 * d the weight of a
+// valid pair is WT[|K_q - K_p|], WT[j] = 1 / (1 + (j/4)^2) made by the same
+// correctly rounded operations as the direct formula, for j <= 4 disp_max.
+// Invalid pixels get a key far away from every valid one, which lands on
+// the table's last entry, weight 0: an invalid neighbour adds 0 to both
+// sums (bit for bit the same as skipping it).  The table has
+// 4 disp_max + 2 entries.
 constexpr int K_INVALID = 1 << 20;
 
 // spk_min > 0: the input is the L/R result before speckle removal, and
 // every loaded pixel goes through the speckle decision of k_spk_apply
 // (segments smaller than spk_min become invalid) on the way in.
-//
-// Persistent: each CTA builds the weight table once and walks its tiles
-// (both views) with a stride of the grid size.
+// One CTA per 32x32 tile; blockIdx.z = view.
 template <int G, bool GAP, bool MEAN, bool MEDIAN>
 __global__ void __launch_bounds__(1024, 2) k_post_tile(PostViews pv, int W, int H, int gap, int spk_min,
-                                                       int nviews) {
+                                                       int wt_n) {
     grid_dep_wait();
     constexpr int PHALO = G + 3, PS = PT + 2 * PHALO;   // S tile side
-    extern __shared__ float WT[];               // WT_N weights when MEAN
+    extern __shared__ float WT[];               // wt_n weights when MEAN
     __shared__ float S[PS][PS];                 // input, halo PHALO
     __shared__ float G2[PS][PT + 6];            // after the row pass: columns [-3, 35)
     __shared__ float V[PT + 6][PT + 6];         // after the column pass: [-3, 35)^2
@@ -387,20 +381,18 @@ __global__ void __launch_bounds__(1024, 2) k_post_tile(PostViews pv, int W, int 
     const int tid = threadIdx.x;
     const float OUT = -2.0f;                    // outside the image (never valid, never filled)
     if (MEAN)
-        for (int j = tid; j < WT_N; j += 1024) {
+        for (int j = tid; j < wt_n; j += 1024) {
             const float q = float(j) * 0.25f;
-            WT[j] = j <= 4 * 4095 ? __frcp_rn(__fmaf_rn(q, q, 1.0f)) : 0.0f;
+            WT[j] = j < wt_n - 1 ? __frcp_rn(__fmaf_rn(q, q, 1.0f)) : 0.0f;
         }
-    const int tiles_x = (W + PT - 1) / PT, tiles_y = (H + PT - 1) / PT, per_view = tiles_x * tiles_y;
-    for (int tile = blockIdx.x; tile < nviews * per_view; tile += gridDim.x) {
-        const int view = tile / per_view, tv = tile - view * per_view;
+    {
+        const int view = blockIdx.z;
         const float* __restrict__ src = pv.cur[view];
         float* __restrict__ dst = pv.nxt[view];
-        const int u0 = (tv % tiles_x) * PT, v0 = (tv / tiles_x) * PT;
+        const int u0 = blockIdx.x * PT, v0 = blockIdx.y * PT;
         const int32_t* __restrict__ lab = pv.lab[view];
         const int32_t* __restrict__ sz = pv.sz[view];
         const int32_t* __restrict__ acc = pv.root[view];
-        __syncthreads();                        // the previous tile (and the table) is done with
         // The speckle decision of k_spk_apply: the local root lab[j] holds
         // -(global root + 1) in its size slot, whose segment size is
         // acc[global root].  The value and lab[j] are loaded together, so each
@@ -454,7 +446,7 @@ __global__ void __launch_bounds__(1024, 2) k_post_tile(PostViews pv, int W, int 
 #pragma unroll
                     for (int dx = -2; dx <= 2; ++dx) {
                         const float dq = V[r + 2 + dy][c + 2 + dx];
-                        const int j = min(abs(K[r + 2 + dy][c + 2 + dx] - kp), WT_N - 1);
+                        const int j = min(abs(K[r + 2 + dy][c + 2 + dx] - kp), wt_n - 1);
                         const float w = WT[j];
                         num = __fmaf_rn(w, dq, num);
                         den = __fadd_rn(den, w);
@@ -540,13 +532,13 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         for (int k = 0; k < nviews; ++k) direct = direct && pv.out[k] != pv.cur[k];
         if (direct)
             for (int k = 0; k < nviews; ++k) pv.nxt[k] = pv.out[k];
-        const int tiles = ((W + PT - 1) / PT) * ((H + PT - 1) / PT) * nviews;
-        const int grid = imax(1, imin(tiles, 2 * num_sms));
-        const size_t smem = adaptive_mean ? WT_N * sizeof(float) : 0;
+        const dim3 grid((W + PT - 1) / PT, (H + PT - 1) / PT, nviews);
+        const int wt_n = 4 * g.D + 2;
+        const size_t smem = adaptive_mean ? size_t(wt_n) * sizeof(float) : 0;
         const int key = (tile_gap ? 4 : 0) | (adaptive_mean ? 2 : 0) | (median ? 1 : 0);
         auto go = [&](auto kern) {
             if (smem) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-            launch_k(kern, grid, 1024, smem, st, pv, W, H, gap, spk, nviews);
+            launch_k(kern, grid, 1024, smem, st, pv, W, H, gap, spk, wt_n);
         };
         if (!tile_gap || gap <= 3) {   // halo 6
             switch (key) {

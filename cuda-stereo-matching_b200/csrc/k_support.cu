@@ -768,44 +768,6 @@ __global__ void k_row_scan(const int32_t* __restrict__ row_cnt, int32_t* __restr
     }
 }
 
-// k_row_count and k_row_scan in one block: warps count the lattice rows
-// (warp-wide sums of coalesced reads) into shared memory, then the block
-// scans them as k_row_scan does.  For lattices up to 16384 rows.
-__global__ void __launch_bounds__(1024) k_row_offsets(const int32_t* __restrict__ can, int32_t* __restrict__ row_off,
-                                                      Geom g, int corners) {
-    grid_dep_wait();
-    extern __shared__ int rc[];                 // [ch] row counts
-    __shared__ int part[1024];
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int n = g.ch;
-    for (int r = warp; r < n; r += 32) {
-        int cnt = 0;
-        for (int x = lane; x < g.cw; x += 32) cnt += can[size_t(r) * g.cw + x] >= 0;
-        cnt = __reduce_add_sync(0xffffffffu, cnt);
-        if (lane == 0) rc[r] = cnt;
-    }
-    __syncthreads();
-    const int per = (n + blockDim.x - 1) / blockDim.x;
-    const int b = t * per, e = min(n, b + per);
-    int s = 0;
-    for (int i = b; i < e; ++i) s += rc[i];
-    part[t] = s;
-    __syncthreads();
-    for (int o = 1; o < blockDim.x; o <<= 1) {
-        int x = t >= o ? part[t - o] : 0;
-        __syncthreads();
-        part[t] += x;
-        __syncthreads();
-    }
-    const int front = corners ? 3 : 0;
-    int run = part[t] - s;
-    for (int i = b; i < e; ++i) { row_off[i] = run + (i > 0 ? front : 0); run += rc[i]; }
-    if (t == blockDim.x - 1) {
-        row_off[n] = part[t] + front;
-        if (corners) row_off[n + 1] = part[t] + 6;
-    }
-}
-
 // Write the support list in raster order: uvd (u, v, d), and the point
 // coordinates of both views (x0 = u, x1 = u - d, y = v).
 __global__ void k_compact(const int32_t* __restrict__ can, const int32_t* __restrict__ row_off,
@@ -932,51 +894,6 @@ __global__ void k_grid_diffuse(const uint32_t* __restrict__ t0, const uint32_t* 
     out[i] = o;
 }
 
-// k_grid_load and k_grid_diffuse in one pass: one CTA per cell row vg
-// builds the loaded bitsets of cell rows vg-1 .. vg+1 (both views) in
-// shared memory from the candidate rows that fall in them, then writes the
-// 3x3 OR-diffusion of row vg (border cells empty).  OR is order-independent,
-// so the result is the two-kernel one bit for bit.
-__global__ void __launch_bounds__(256) k_grid_fused(const int32_t* __restrict__ can, uint32_t* __restrict__ g0,
-                                                    uint32_t* __restrict__ g1, Geom g) {
-    grid_dep_wait();
-    extern __shared__ uint32_t gb[];            // [3 rows][2 views][gw * words]
-    const int vg = blockIdx.x, tid = threadIdx.x;
-    const int rw = g.gw * g.words;
-    for (int i = tid; i < 6 * rw; i += blockDim.x) gb[i] = 0u;
-    __syncthreads();
-    // candidate rows y with floordiv(y * step, gs) in [vg - 1, vg + 1]
-    const int y0 = imax(0, ((vg - 1) * g.gs + g.step - 1) / g.step);
-    const int y1 = imin(g.ch - 1, ((vg + 2) * g.gs - 1) / g.step);
-    for (int y = y0; y <= y1; ++y) {
-        const int v = y * g.step, rvg = floordiv(v, g.gs);
-        if (rvg < vg - 1 || rvg > vg + 1 || rvg < 0 || rvg >= g.gh) continue;
-        uint32_t* row = gb + (rvg - (vg - 1)) * 2 * rw;
-        for (int x = tid; x < g.cw; x += blockDim.x) {
-            const int dc = can[size_t(y) * g.cw + x];
-            if (dc < 0) continue;
-            const int u = x * g.step;
-            const int ug0 = floordiv(u, g.gs), ug1 = floordiv(u - dc, g.gs);
-            for (int d = max(dc - 1, 0); d <= min(dc + 1, g.D); ++d) {
-                const uint32_t bit = 1u << (d & 31);
-                if (ug0 >= 0 && ug0 < g.gw) atomicOr(&row[ug0 * g.words + (d >> 5)], bit);
-                if (ug1 >= 0 && ug1 < g.gw) atomicOr(&row[rw + ug1 * g.words + (d >> 5)], bit);
-            }
-        }
-    }
-    __syncthreads();
-    const bool interior_row = vg > 0 && vg < g.gh - 1;
-    for (int i = tid; i < 2 * rw; i += blockDim.x) {
-        const int view = i / rw, k = i - view * rw;
-        const int ug = k / g.words, w = k - ug * g.words;
-        uint32_t o = 0;
-        if (interior_row && ug > 0 && ug < g.gw - 1)
-            for (int dy = 0; dy < 3; ++dy)
-                for (int dx = -1; dx <= 1; ++dx) o |= gb[(dy * 2 + view) * rw + (ug + dx) * g.words + w];
-        (view ? g1 : g0)[size_t(vg) * rw + k] = o;
-    }
-}
-
 }  // namespace
 
 cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_lr, int32_t* can_tmp,
@@ -1052,16 +969,9 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
 cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_off, int32_t* uvd, int32_t* x0,
                            int32_t* x1, int32_t* y, const Geom& g, cudaStream_t st, int corners, int* nlaunch) {
     int launched = 1 + (corners ? 1 : 0);
-    if (g.ch <= 16384) {
-        const size_t smem = size_t(imax(g.ch, 1)) * sizeof(int);
-        cudaFuncSetAttribute(k_row_offsets, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        launch_k(k_row_offsets, 1, 1024, smem, st, can, row_off, g, corners);
-        launched += 1;
-    } else {
-        launch_k(k_row_count, g.ch, 128, 0, st, can, row_cnt, g);
-        launch_k(k_row_scan, 1, 1024, 0, st, row_cnt, row_off, g.ch, corners);
-        launched += 2;
-    }
+    launch_k(k_row_count, g.ch, 128, 0, st, can, row_cnt, g);
+    launch_k(k_row_scan, 1, 1024, 0, st, row_cnt, row_off, g.ch, corners);
+    launched += 2;
     launch_k(k_compact, g.ch, 256, 0, st, can, row_off, uvd, x0, x1, y, g, corners ? 3 : 0);
     if (corners) launch_k(k_corners, 1, 1024, 0, st, row_off, uvd, x0, x1, y, g);
     if (nlaunch) *nlaunch += launched;
@@ -1070,13 +980,6 @@ cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_of
 
 cudaError_t launch_grid(const int32_t* can, uint32_t* tmp0, uint32_t* tmp1, uint32_t* grid0, uint32_t* grid1,
                         const Geom& g, cudaStream_t st, int* nlaunch) {
-    const size_t fused_smem = size_t(6) * g.gw * g.words * sizeof(uint32_t);
-    if (fused_smem <= 96 * 1024) {
-        cudaFuncSetAttribute(k_grid_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, int(fused_smem));
-        launch_k(k_grid_fused, g.gh, 256, fused_smem, st, can, grid0, grid1, g);
-        if (nlaunch) *nlaunch += 1;
-        return cudaGetLastError();
-    }
     if (nlaunch) *nlaunch += 2;
     size_t n = size_t(g.gw) * g.gh * g.words;
     cudaMemsetAsync(tmp0, 0, n * sizeof(uint32_t), st);

@@ -63,26 +63,14 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
 // kernel, or 0 if none fits.
 int cluster_size_for_flip();
 
-// Triangles binned by image row, per view: the prior is rasterised one row
-// at a time from these lists.
-struct PriorBins {
-    int32_t* cnt;      // [2][H + 1] triangles whose row range holds row v (then the fill cursors)
-    int32_t* off;      // [2][H + 1] exclusive prefix sums of cnt
-    int32_t* list;     // [2][cap] triangle indices, row by row
-    int cap;           // entries per view
-};
-// Entries per view that the row lists can hold for a W x H pair with at
-// most Tmax triangles (overflow raises ERRF_BOUNDS).
-size_t prior_bin_capacity(const Geom& g, int Tmax);
-
 // Plane prior of both views: prior[v*W+u] = (triangle+1) << pshift | d,
 // d = d_plane clamped to [0, dcap] (dcap = disp_max + plane_radius + 1),
-// 0 where no triangle covers the pixel.  Every pixel is written.
+// 0 where no triangle covers the pixel.  The buffers are zeroed here.
 // rast: scratch of 2 * Tmax * raster_bytes() for the per-triangle set-up.
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
-                         int Tmax, const int32_t* can, const int32_t* uvd, void* rast, const PriorBins& bins,
-                         uint32_t* prior0, uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms,
-                         unsigned* err, cudaStream_t st, int* nlaunch);
+                         int Tmax, const int32_t* can, const int32_t* uvd, void* rast, uint32_t* prior0,
+                         uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms, cudaStream_t st,
+                         int* nlaunch);
 size_t raster_bytes();
 
 // Dense matching of both views; `seg` output columns per CTA (the
