@@ -17,11 +17,12 @@
 // oracle evaluates the identical operation sequence.
 //
 // Dense: replaces kerComputeDisparity (KerComputeDisparity.cu:155-316).
-// One CTA per image row and view; the other view's descriptor row is
-// staged in shared memory; the candidate list of the pixel's grid cell is a
-// bitset walked in ascending order (the reference's sorted int list),
-// skipping the plane window, then the plane window with the penalty added.
-// Strict '<' keeps the first minimum in that order, as the reference does.
+// One CTA per (row, column segment, view); the part of the other view's
+// descriptor row the segment can reach is staged in shared memory; the
+// candidate list of the pixel's grid cell is a bitset walked in ascending
+// order (the reference's sorted int list), skipping the plane window, then
+// the plane window with the penalty added.  Strict '<' keeps the first
+// minimum in that order, as the reference does.
 #include <cuda_runtime.h>
 #include "common.cuh"
 #include "launch.cuh"
@@ -254,19 +255,35 @@ __global__ void __launch_bounds__(256) k_dense(const uint4* __restrict__ desc0, 
         bulk_g2s_chunked(win, other + c0, unsigned(c1 - c0) * 16u, &bar);
     }
     const int gy = floordiv(v, g.gs);
-    for (int k = tid; k < ncell; k += NT) {
-        const uint32_t* cell = grid + (size_t(gy) * g.gw + cell0 + k) * g.words;
-        int n = 0;
-        for (int w = 0; w < g.words; ++w) {
-            uint32_t bits = cell[w];
-            while (bits) {
-                int d = 32 * w + __ffs(bits) - 1;
-                bits &= bits - 1;
-                if (n < lcap) lst[k * LMAX + n] = int16_t(d);
-                ++n;
+    // one warp per cell: lanes take consecutive words of its bitset and a
+    // warp prefix sum of their bit counts gives each lane its place, so the
+    // list comes out in ascending order (NT is a multiple of 32)
+    {
+        const int lane = tid & 31;
+        for (int k = tid >> 5; k < ncell; k += NT >> 5) {
+            const uint32_t* cell = grid + (size_t(gy) * g.gw + cell0 + k) * g.words;
+            int n = 0;
+            for (int w0 = 0; w0 < g.words; w0 += 32) {
+                const int w = w0 + lane;
+                uint32_t bits = w < g.words ? cell[w] : 0u;
+                const int c = __popc(bits);
+                int pre = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, pre, o);
+                    if (lane >= o) pre += y;
+                }
+                int pos = n + pre - c;
+                while (bits) {
+                    const int d = 32 * w + __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    if (pos < lcap) lst[k * LMAX + pos] = int16_t(d);
+                    ++pos;
+                }
+                n += __shfl_sync(0xffffffffu, pre, 31);
             }
+            if (lane == 0) lcnt[k] = uint8_t(n > lcap ? 255 : n);
         }
-        lcnt[k] = uint8_t(n > lcap ? 255 : n);
     }
     // first pixel of this thread and its prefetch
     int o = o0 + tid, u = o << sub;

@@ -366,10 +366,11 @@ constexpr int K_INVALID = 1 << 20;
 // spk_min > 0: the input is the L/R result before speckle removal, and
 // every loaded pixel goes through the speckle decision of k_spk_apply
 // (segments smaller than spk_min become invalid) on the way in.
-// One CTA per 32x32 tile; blockIdx.z = view.
+// Persistent: each CTA builds the weight table once and walks 32x32 tiles
+// of both views with a stride of the grid size.
 template <int G, bool GAP, bool MEAN, bool MEDIAN>
 __global__ void __launch_bounds__(1024, 2) k_post_tile(PostViews pv, int W, int H, int gap, int spk_min,
-                                                       int wt_n) {
+                                                       int wt_n, int nviews) {
     grid_dep_wait();
     constexpr int PHALO = G + 3, PS = PT + 2 * PHALO;   // S tile side
     extern __shared__ float WT[];               // wt_n weights when MEAN
@@ -385,14 +386,16 @@ __global__ void __launch_bounds__(1024, 2) k_post_tile(PostViews pv, int W, int 
             const float q = float(j) * 0.25f;
             WT[j] = j < wt_n - 1 ? __frcp_rn(__fmaf_rn(q, q, 1.0f)) : 0.0f;
         }
-    {
-        const int view = blockIdx.z;
+    const int tiles_x = (W + PT - 1) / PT, tiles_y = (H + PT - 1) / PT, per_view = tiles_x * tiles_y;
+    for (int tile = blockIdx.x; tile < nviews * per_view; tile += gridDim.x) {
+        const int view = tile / per_view, tv = tile - view * per_view;
         const float* __restrict__ src = pv.cur[view];
         float* __restrict__ dst = pv.nxt[view];
-        const int u0 = blockIdx.x * PT, v0 = blockIdx.y * PT;
+        const int u0 = (tv % tiles_x) * PT, v0 = (tv / tiles_x) * PT;
         const int32_t* __restrict__ lab = pv.lab[view];
         const int32_t* __restrict__ sz = pv.sz[view];
         const int32_t* __restrict__ acc = pv.root[view];
+        __syncthreads();                        // the previous tile (and the table) is done with
         // The speckle decision of k_spk_apply: the local root lab[j] holds
         // -(global root + 1) in its size slot, whose segment size is
         // acc[global root].  The value and lab[j] are loaded together, so each
@@ -532,13 +535,14 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         for (int k = 0; k < nviews; ++k) direct = direct && pv.out[k] != pv.cur[k];
         if (direct)
             for (int k = 0; k < nviews; ++k) pv.nxt[k] = pv.out[k];
-        const dim3 grid((W + PT - 1) / PT, (H + PT - 1) / PT, nviews);
+        const int tiles = ((W + PT - 1) / PT) * ((H + PT - 1) / PT) * nviews;
+        const int grid = imax(1, imin(tiles, 2 * num_sms));
         const int wt_n = 4 * g.D + 2;
         const size_t smem = adaptive_mean ? size_t(wt_n) * sizeof(float) : 0;
         const int key = (tile_gap ? 4 : 0) | (adaptive_mean ? 2 : 0) | (median ? 1 : 0);
         auto go = [&](auto kern) {
             if (smem) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-            launch_k(kern, grid, 1024, smem, st, pv, W, H, gap, spk, wt_n);
+            launch_k(kern, grid, 1024, smem, st, pv, W, H, gap, spk, wt_n, nviews);
         };
         if (!tile_gap || gap <= 3) {   // halo 6
             switch (key) {
