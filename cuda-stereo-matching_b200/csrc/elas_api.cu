@@ -329,18 +329,17 @@ int check_dims(elas_handle* h, const int32_t* dims, int& W, int& H) {
         int64_t tmax = 2LL * g.cw * g.ch + 16;
         if ((tmax + 1) >> (32 - prior_shift(g, dp)) != 0)
             return fail(h, ELAS_ERR_UNSUPPORTED, "too many candidate points for the packed plane prior");
-        if (dense_smem_bytes(g, 1024, 0) > 220 * 1024)
-            return fail(h, ELAS_ERR_UNSUPPORTED, "disparity range too wide for the dense window in shared memory");
+        if (dense_smem_bytes(g) > 220 * 1024)
+            return fail(h, ELAS_ERR_UNSUPPORTED, "image too wide for the dense row in shared memory");
     }
     return ELAS_OK;
 }
 
-// Dense-matching autotuner.  The CTA shape (output columns per segment
-// CTA, 256 threads at most) changes only how a row's pixels are spread over
-// CTAs and threads, never the result; the first call with a new (width
-// class, disp_max) times each shape on its own data (CUDA events on the
-// stream) and keeps the fastest.  Inside a stream capture an untuned class
-// uses 256 columns.
+// Dense-matching autotuner.  The CTA shape (threads per row CTA) changes
+// only how the row's pixels are spread over threads, never the result; the
+// first call with a new (width class, disp_max) times each shape on its own
+// data (CUDA events on the stream) and keeps the fastest.  Inside a stream
+// capture an untuned class uses 512 threads.
 constexpr int DENSE_SHAPES[4] = {128, 256, 512, 1024};
 
 int dense_threads_for(elas_handle* h, const Geom& g, const DevParams& dp, cudaStream_t st, int* nlaunch, int* out) {
@@ -351,11 +350,11 @@ int dense_threads_for(elas_handle* h, const Geom& g, const DevParams& dp, cudaSt
     if (it != t->dense_threads.end()) { *out = it->second; return ELAS_OK; }
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(st, &cs));
-    if (cs != cudaStreamCaptureStatusNone) { *out = 256; return ELAS_OK; }
+    if (cs != cudaStreamCaptureStatusNone) { *out = 512; return ELAS_OK; }
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    int best = 256;
+    int best = 512;
     float best_ms = 1e30f;
     for (int shape : DENSE_SHAPES) {
         float shape_ms = 1e30f;
@@ -490,7 +489,7 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
                     h->rast, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1, h->num_sms, st,
                     &n));
-    int shape = 256;
+    int shape = 512;
     rc = dense_threads_for(h, g, dp, st, &n, &shape);
     if (rc != ELAS_OK) return rc;
     CK(mark(ELAS_TIME_DENSE));

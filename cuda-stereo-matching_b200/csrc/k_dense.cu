@@ -17,12 +17,11 @@
 // oracle evaluates the identical operation sequence.
 //
 // Dense: replaces kerComputeDisparity (KerComputeDisparity.cu:155-316).
-// One CTA per (row, column segment, view); the part of the other view's
-// descriptor row the segment can reach is staged in shared memory; the
-// candidate list of the pixel's grid cell is a bitset walked in ascending
-// order (the reference's sorted int list), skipping the plane window, then
-// the plane window with the penalty added.  Strict '<' keeps the first
-// minimum in that order, as the reference does.
+// One CTA per image row and view; the other view's descriptor row is
+// staged in shared memory; the candidate list of the pixel's grid cell is a
+// bitset walked in ascending order (the reference's sorted int list),
+// skipping the plane window, then the plane window with the penalty added.
+// Strict '<' keeps the first minimum in that order, as the reference does.
 #include <cuda_runtime.h>
 #include "common.cuh"
 #include "launch.cuh"
@@ -189,16 +188,9 @@ constexpr int PK_NONE = 10000 * 4096;   // the reference's start value: energy 1
 __device__ __forceinline__ int pk_ed(int e, int d) { return e * 4096 + d; }
 __device__ __forceinline__ void take_min(int e, int d, int& best) { best = min(best, pk_ed(e, d)); }
 
-// One CTA per (column segment, view) of one row: blockIdx.x = 2 * segment +
-// view (the two views of a segment are neighbours in launch order, so the
-// descriptor row one of them reads as its own the other reads as the other
-// view while it is still in L2), blockIdx.y = output row.  A segment is
-// `seg` output columns.  The part of the other view's descriptor row that
-// the segment's pixels can reach -- its columns widened by disp_max towards
-// the matching direction -- arrives by bulk copy (TMA) while the CTA expands
-// the candidate lists of the segment's grid cells into shared memory, so a
-// CTA holds (seg + disp_max) x 16 bytes instead of a whole row and many CTAs
-// share an SM.
+// blockIdx.x = row, blockIdx.y = view (0 left, 1 right).  The other view's
+// descriptor row arrives by bulk copy (TMA) while the CTA expands the
+// candidate lists of the row's grid cells into shared memory.
 //
 // Per pixel u the reference evaluates the cell's sorted list, skipping the
 // plane window [d_plane - r, d_plane + r] and every d whose warped column
@@ -215,80 +207,56 @@ __device__ __forceinline__ void take_min(int e, int d, int& best) { best = min(b
 //   * the own descriptor and the prior of the thread's next pixel are
 //     loaded before the current pixel is matched.
 template <int RFIX>
-__global__ void __launch_bounds__(256) k_dense(const uint4* __restrict__ desc0, const uint4* __restrict__ desc1,
-                                              const uint32_t* __restrict__ prior0, const uint32_t* __restrict__ prior1,
-                                              const uint32_t* __restrict__ grid0, const uint32_t* __restrict__ grid1,
-                                              float* __restrict__ disp0, float* __restrict__ disp1, Geom g,
-                                              DevParams p, int pshift, int sub, int seg, int lcap, unsigned* err) {
+__global__ void __launch_bounds__(1024) k_dense(const uint4* __restrict__ desc0, const uint4* __restrict__ desc1,
+                                               const uint32_t* __restrict__ prior0, const uint32_t* __restrict__ prior1,
+                                               const uint32_t* __restrict__ grid0, const uint32_t* __restrict__ grid1,
+                                               float* __restrict__ disp0, float* __restrict__ disp1, Geom g,
+                                               DevParams p, int pshift, int sub, int lcap, unsigned* err) {
     grid_dep_wait();
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ uint64_t bar;
     // sub = 1: every second row and column (output (W/2) x (H/2))
-    const int v = int(blockIdx.y) << sub;
-    const bool right = (blockIdx.x & 1) != 0;
+    const int v = int(blockIdx.x) << sub;
+    const bool right = blockIdx.y != 0;
     const int W = g.W, H = g.H;
     const int tid = threadIdx.x, NT = blockDim.x;
     const int Wo = W >> sub;
-    const int o0 = int(blockIdx.x >> 1) * seg, o1 = imin(o0 + seg, Wo);
-    float* disp = (right ? disp1 : disp0) + size_t(blockIdx.y) * Wo;
+    float* disp = (right ? disp1 : disp0) + size_t(blockIdx.x) * Wo;
     if (!(v > 3 && v < H - 3)) {           // CTA-uniform: no copy is issued for these rows
-        for (int o = o0 + tid; o < o1; o += NT) disp[o] = -1.0f;
+        for (int o = tid; o < Wo; o += NT) disp[o] = -1.0f;
         return;
     }
-    // columns of the segment, and the other row's window they can reach
-    const int ua = o0 << sub, ub = (o1 - 1) << sub;
-    const int c0 = right ? ua : imax(ua - g.D, 0);
-    const int c1 = right ? imin(ub + g.D + 1, W) : ub + 1;
-    const int cell0 = ua / g.gs, ncell = ub / g.gs - cell0 + 1;
-    uint4* win = reinterpret_cast<uint4*>(sm);
-    const size_t win_bytes = size_t(((seg - 1) << sub) + 1 + g.D) * 16;
-    int16_t* lst = reinterpret_cast<int16_t*>(sm + win_bytes);
-    uint8_t* lcnt = reinterpret_cast<uint8_t*>(lst + size_t(ncell) * LMAX);
-    const uint4* row = win - c0;          // row[u] for u in [c0, c1)
+    uint4* row = reinterpret_cast<uint4*>(sm);
+    int16_t* lst = reinterpret_cast<int16_t*>(sm + size_t(W) * 16);
+    uint8_t* lcnt = reinterpret_cast<uint8_t*>(lst + size_t(g.gw) * LMAX);
     const uint4* self = (right ? desc1 : desc0) + size_t(v) * W;
     const uint4* other = (right ? desc0 : desc1) + size_t(v) * W;
     const uint32_t* prior = (right ? prior1 : prior0) + size_t(v) * W;
     const uint32_t* grid = right ? grid1 : grid0;
     if (tid == 0) {
         mbar_init(&bar, 1);
-        mbar_expect_tx(&bar, unsigned(c1 - c0) * 16u);
-        bulk_g2s_chunked(win, other + c0, unsigned(c1 - c0) * 16u, &bar);
+        mbar_expect_tx(&bar, unsigned(W) * 16u);
+        bulk_g2s_chunked(row, other, unsigned(W) * 16u, &bar);
     }
     const int gy = floordiv(v, g.gs);
-    // one warp per cell: lanes take consecutive words of its bitset and a
-    // warp prefix sum of their bit counts gives each lane its place, so the
-    // list comes out in ascending order (NT is a multiple of 32)
-    {
-        const int lane = tid & 31;
-        for (int k = tid >> 5; k < ncell; k += NT >> 5) {
-            const uint32_t* cell = grid + (size_t(gy) * g.gw + cell0 + k) * g.words;
-            int n = 0;
-            for (int w0 = 0; w0 < g.words; w0 += 32) {
-                const int w = w0 + lane;
-                uint32_t bits = w < g.words ? cell[w] : 0u;
-                const int c = __popc(bits);
-                int pre = c;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, pre, o);
-                    if (lane >= o) pre += y;
-                }
-                int pos = n + pre - c;
-                while (bits) {
-                    const int d = 32 * w + __ffs(bits) - 1;
-                    bits &= bits - 1;
-                    if (pos < lcap) lst[k * LMAX + pos] = int16_t(d);
-                    ++pos;
-                }
-                n += __shfl_sync(0xffffffffu, pre, 31);
+    for (int c = tid; c < g.gw; c += NT) {
+        const uint32_t* cell = grid + (size_t(gy) * g.gw + c) * g.words;
+        int n = 0;
+        for (int w = 0; w < g.words; ++w) {
+            uint32_t bits = cell[w];
+            while (bits) {
+                int d = 32 * w + __ffs(bits) - 1;
+                bits &= bits - 1;
+                if (n < lcap) lst[c * LMAX + n] = int16_t(d);
+                ++n;
             }
-            if (lane == 0) lcnt[k] = uint8_t(n > lcap ? 255 : n);
         }
+        lcnt[c] = uint8_t(n > lcap ? 255 : n);
     }
     // first pixel of this thread and its prefetch
-    int o = o0 + tid, u = o << sub;
-    uint32_t pk_next = o < o1 ? prior[u] : 0u;
-    uint4 I_next = o < o1 ? self[u] : make_uint4(0, 0, 0, 0);
+    int o = tid, u = o << sub;
+    uint32_t pk_next = o < Wo ? prior[u] : 0u;
+    uint4 I_next = o < Wo ? self[u] : make_uint4(0, 0, 0, 0);
     __syncthreads();
     if (!mbar_wait_bounded(&bar, 0, MBAR_WAIT_LIMIT)) {
         if (tid == 0) atomicOr(err, ERRF_TMA_TIMEOUT);
@@ -299,17 +267,16 @@ __global__ void __launch_bounds__(256) k_dense(const uint4* __restrict__ desc0, 
     const int r = RFIX > 0 ? RFIX : p.plane_radius;
     const uint32_t dmask = (1u << pshift) - 1u;
     const int gs = g.gs;
-    // cell of u relative to the segment's first cell, advanced incrementally
+    // cell of u, advanced incrementally (u grows by NT per iteration)
     int cell = u / gs, rem = u - cell * gs;
-    cell -= cell0;
     const int ustep = NT << sub;
     const int cstep = ustep / gs, rstep = ustep - cstep * gs;
-    for (; o < o1; o += NT, u += ustep) {
+    for (; o < Wo; o += NT, u += ustep) {
         const uint32_t pk = pk_next;
         const uint4 I1 = I_next;
         const int c = cell;
         {
-            if (o + NT < o1) { pk_next = prior[u + ustep]; I_next = self[u + ustep]; }
+            if (o + NT < Wo) { pk_next = prior[u + ustep]; I_next = self[u + ustep]; }
             cell += cstep;
             rem += rstep;
             if (rem >= gs) { rem -= gs; ++cell; }
@@ -351,7 +318,7 @@ __global__ void __launch_bounds__(256) k_dense(const uint4* __restrict__ desc0, 
                     }
                 }
             } else {
-                const uint32_t* cw = grid + (size_t(gy) * g.gw + cell0 + c) * g.words;
+                const uint32_t* cw = grid + (size_t(gy) * g.gw + c) * g.words;
                 bool done = false;
                 for (int w = 0; w < g.words && !done; ++w) {
                     uint32_t bits = cw[w];
@@ -438,34 +405,26 @@ cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t
 
 size_t raster_bytes() { return sizeof(Raster); }
 
-// Shared memory of a dense CTA of `seg` output columns: the other row's
-// window and the candidate lists of the segment's cells.
-size_t dense_smem_bytes(const Geom& g, int seg, int sub) {
-    const size_t span = size_t((seg - 1) << sub) + 1;
-    const size_t cells = span / size_t(g.gs) + 2;
-    return (span + size_t(g.D)) * 16 + cells * (LMAX * 2 + 1);
-}
+size_t dense_smem_bytes(const Geom& g) { return size_t(g.W) * 16 + size_t(g.gw) * (LMAX * 2 + 1); }
 
 cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t* prior0, const uint32_t* prior1,
                          const uint32_t* grid0, const uint32_t* grid1, float* disp0, float* disp1, const Geom& g,
-                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int seg, int sub,
+                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads, int sub,
                          bool force_bitset) {
     // list capacity per cell (0 sends every non-empty cell to the bitset walk)
     const int lcap = force_bitset ? 0 : LMAX;
-    if (seg <= 0) seg = 256;
-    const int Wo = g.W >> sub;
-    seg = imin(seg, ((Wo + 31) / 32) * 32);
-    const int threads = imin(seg, 256);
-    const size_t smem = dense_smem_bytes(g, seg, sub);
-    const dim3 grid(2 * ((Wo + seg - 1) / seg), g.H >> sub);
+    size_t smem = dense_smem_bytes(g);
+    if (threads <= 0) threads = 512;
+    threads = imin(threads, (((g.W >> sub) + 31) / 32) * 32);
+    const dim3 grid(g.H >> sub, 2);
     if (p.plane_radius == 2) {
         cudaFuncSetAttribute(k_dense<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         launch_k(k_dense<2>, grid, threads, smem, st, desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
-                 pshift, sub, seg, lcap, err);
+                                                pshift, sub, lcap, err);
     } else {
         cudaFuncSetAttribute(k_dense<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         launch_k(k_dense<0>, grid, threads, smem, st, desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
-                 pshift, sub, seg, lcap, err);
+                                                pshift, sub, lcap, err);
     }
     return cudaGetLastError();
 }

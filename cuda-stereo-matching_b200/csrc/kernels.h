@@ -73,12 +73,10 @@ cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t
                          int* nlaunch);
 size_t raster_bytes();
 
-// Dense matching of both views; `seg` output columns per CTA (the
-// autotuned shape; it never changes the result).
-size_t dense_smem_bytes(const Geom& g, int seg, int sub);
+size_t dense_smem_bytes(const Geom& g);
 cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t* prior0, const uint32_t* prior1,
                          const uint32_t* grid0, const uint32_t* grid1, float* disp0, float* disp1, const Geom& g,
-                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int seg, int sub = 0,
+                         const DevParams& p, int pshift, unsigned* err, cudaStream_t st, int threads, int sub = 0,
                          bool force_bitset = false);
 
 // L/R check into o0/o1 and, where c0 is not null, also into c0/c1

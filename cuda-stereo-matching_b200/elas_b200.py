@@ -13,7 +13,8 @@ from ctypes import POINTER, c_bool, c_float, c_int, c_int32, c_int64, c_size_t, 
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libelas_b200.so")
+# ELAS_B200_LIB may name another build of the library (for side-by-side measurements)
+LIB_PATH = os.environ.get("ELAS_B200_LIB") or os.path.join(HERE, "libelas_b200.so")
 
 ELAS_OK = 0
 STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported", 3: "CUDA error", 4: "out of memory",
