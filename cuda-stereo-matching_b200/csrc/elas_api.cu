@@ -52,6 +52,7 @@ struct elas_handle {
     DelDev del[2]{};
     uint32_t *prior0 = nullptr, *prior1 = nullptr;
     void* rast = nullptr;   // per-triangle plane/edge set-up of both views
+    PriorTiles ptiles{};    // triangles binned by prior tile, both views
     float *raw0 = nullptr, *raw1 = nullptr, *lr0 = nullptr, *lr1 = nullptr;
     float *out0 = nullptr, *out1 = nullptr;
     float* tmp[2] = {nullptr, nullptr};          // post-filter ping-pong buffer per view
@@ -265,6 +266,13 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         D.Hmax = uint32_t(hmax);
     }
     h->rast = take(2 * tmax * raster_bytes());
+    {
+        const size_t nt = prior_tile_count(g), cap = prior_list_capacity(g, int(tmax));
+        h->ptiles.cnt = (int32_t*)take(2 * (nt + 1) * 4);
+        h->ptiles.off = (int32_t*)take(2 * (nt + 1) * 4);
+        h->ptiles.list = (int32_t*)take(2 * cap * 4);
+        h->ptiles.cap = int(cap);
+    }
     h->prior0 = (uint32_t*)take(px * 4);
     h->prior1 = (uint32_t*)take(px * 4);
     h->raw0 = (float*)take(px * 4);
@@ -475,7 +483,7 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     }
     CK(launch_support(h->desc0, h->desc1, h->can_lr, nullptr, h->can, g, dp, h->num_sms, h->err, st, bins,
                       h->pn_used ? h->pn_stats : nullptr));
-    n += 4;
+    n += 3;
     CK(mark(ELAS_TIME_COMPACT));
     const int corners = p.add_corners ? 1 : 0;
     CK(launch_compact(h->can, h->row_cnt, h->row_off, h->uvd, h->x0, h->x1, h->y, g, st, corners, &n));
@@ -487,8 +495,8 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
                        h->flip_round_limit));
     CK(mark(ELAS_TIME_PRIOR));
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
-                    h->rast, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1, h->num_sms, st,
-                    &n));
+                    h->rast, h->ptiles, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1,
+                    h->num_sms, h->err, st, &n));
     int shape = 512;
     rc = dense_threads_for(h, g, dp, st, &n, &shape);
     if (rc != ELAS_OK) return rc;

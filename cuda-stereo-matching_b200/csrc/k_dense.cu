@@ -3,12 +3,14 @@
 // Prior: replaces kerComputeDepthApproximation
 // (src/Kernels/KerComputeDisparity.cu:9-152), one thread per triangle with
 // long serial scanline loops.  Here one thread per triangle solves the plane
-// (same double Gauss-Jordan as kerSolve, :321-375) and sets up the edges,
-// then a warp per triangle splits its columns.  A pixel covered by more than one
-// triangle (rounding at shared vertices) must keep the last triangle in
-// list order, as a sequential rasteriser would; the prior is therefore
-// written with a 32-bit atomicMax of (triangle+1) << pshift | d_plane, which
-// makes the result independent of scheduling.  d_plane is stored clamped to
+// (same double Gauss-Jordan as kerSolve, :321-375), sets up the edges and
+// finds the 64x32 prior tiles its pixels can fall in; the triangles are
+// binned by tile, and one CTA per tile paints it in shared memory and writes
+// it once.  A pixel covered by more than one triangle (rounding at shared
+// vertices) must keep the last triangle in list order, as a sequential
+// rasteriser would; the tile is therefore painted with a 32-bit atomicMax of
+// (triangle+1) << pshift | d_plane, which makes the result independent of
+// scheduling.  d_plane is stored clamped to
 // [0, disp_max + plane_radius + 1] (0 standing for every d_plane <= 0): the
 // dense step treats all values beyond either end alike.
 //
@@ -69,7 +71,33 @@ struct Raster {
     float pa, pb, pc;
     float A_u, B_u, C_u;
     float AB_a, AC_a, BC_a, AB_b, AC_b, BC_b;
+    int tx0, tx1, ty0, ty1;     // prior tiles its pixels can fall in (tx0 > tx1: none)
 };
+
+// Prior tiles: each is painted by one CTA in shared memory and written once.
+constexpr int PT_W = 64, PT_H = 32;
+
+// Rows of one part of the scan-line raster: columns u in [ua, ub) write the
+// rows [va, vb) with va = max(min(v1, v2), 0), vb = min(max(v1, v2), H),
+// v1 from the long edge AC and v2 from the part's edge.  Each of v1, v2 is
+// a truncated fma of u, monotone in u, so the extremes over the part are at
+// its first and last column.
+__device__ __forceinline__ int raster_row(float a, float b, int u) {
+    return int(__float2uint_rz(__fmaf_rn(a, float(u), b)));
+}
+__device__ void part_rows(const Raster& R, int part, int W, int H, int& r0, int& r1) {
+    const int ua = part ? int(R.B_u) : int(R.A_u), ub = part ? int(R.C_u) : int(R.B_u);
+    const int u0 = imax(ua, 0), u1 = imin(ub, W) - 1;
+    if (ua == ub || u0 > u1) return;
+    const float ea = part ? R.BC_a : R.AB_a, eb = part ? R.BC_b : R.AB_b;
+    const int a0 = raster_row(R.AC_a, R.AC_b, u0), a1 = raster_row(R.AC_a, R.AC_b, u1);
+    const int b0 = raster_row(ea, eb, u0), b1 = raster_row(ea, eb, u1);
+    const int lo = imax(imin(imin(a0, a1), imin(b0, b1)), 0);
+    const int hi = imin(imax(imax(a0, a1), imax(b0, b1)), H) - 1;
+    if (lo > hi) return;
+    r0 = imin(r0, lo);
+    r1 = imax(r1, hi);
+}
 
 __device__ void setup_triangle(const int32_t* tri, const int32_t* can, const int32_t* uvd, int cw, int step,
                                bool right, Raster& R) {
@@ -117,13 +145,16 @@ __device__ void setup_triangle(const int32_t* tri, const int32_t* can, const int
     R.BC_b = __fmaf_rn(-R.BC_a, B_u, B_v);
 }
 
-// One thread per (view, triangle): plane and edge set-up, once.
+// One thread per (view, triangle): plane and edge set-up, the prior tiles
+// its pixels can fall in (from the exact row range of the raster and its
+// column range), and one count per such tile.
 __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__ tri0,
                                                      const int32_t* __restrict__ tri1,
                                                      const int32_t* __restrict__ ctr0,
                                                      const int32_t* __restrict__ ctr1,
                                                      const int32_t* __restrict__ can, const int32_t* __restrict__ uvd,
-                                                     Raster* __restrict__ rast, int Tmax, Geom g) {
+                                                     Raster* __restrict__ rast, int Tmax, Geom g, int32_t* tcnt,
+                                                     int ntx, int ntiles) {
     grid_dep_wait();
     const int T0 = ctr0[0], T1 = ctr1[0];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T0 + T1; i += gridDim.x * blockDim.x) {
@@ -131,45 +162,137 @@ __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__
         const int t = right ? i - T0 : i;
         Raster R;
         setup_triangle((right ? tri1 : tri0) + 3 * size_t(t), can, uvd, g.cw, g.step, right, R);
+        int r0 = g.H, r1 = -1;
+        part_rows(R, 0, g.W, g.H, r0, r1);
+        part_rows(R, 1, g.W, g.H, r0, r1);
+        const int u0 = imax(int(R.A_u), 0), u1 = imin(int(R.C_u), g.W) - 1;
+        R.tx0 = 1; R.tx1 = 0; R.ty0 = 1; R.ty1 = 0;
+        if (r0 <= r1 && u0 <= u1) {
+            R.tx0 = u0 / PT_W; R.tx1 = u1 / PT_W;
+            R.ty0 = r0 / PT_H; R.ty1 = r1 / PT_H;
+        }
         rast[(right ? Tmax : 0) + t] = R;
+        int32_t* c = tcnt + (right ? ntiles + 1 : 0);
+        for (int ty = R.ty0; ty <= R.ty1; ++ty)
+            for (int tx = R.tx0; tx <= R.tx1; ++tx) atomicAdd(c + ty * ntx + tx, 1);
     }
 }
 
-// One warp per (view, triangle), lanes over columns; every pixel keeps the
-// last covering triangle through atomicMax on the packed value.
-__global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict__ ctr0,
-                                                      const int32_t* __restrict__ ctr1,
-                                                      const Raster* __restrict__ rast, int Tmax,
-                                                      uint32_t* prior0, uint32_t* prior1, Geom g, int pshift,
-                                                      int dcap) {
+// One 1024-thread block per view: exclusive prefix sums of the tile counts
+// (the list offsets), which also become the fill cursors.
+__global__ void __launch_bounds__(1024) k_prior_scan(int32_t* cnt, int32_t* off, int n) {
     grid_dep_wait();
-    const int lane = threadIdx.x & 31;
+    __shared__ int ws[33];
+    int32_t* c = cnt + blockIdx.x * (n + 1);
+    int32_t* o = off + blockIdx.x * (n + 1);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int per = (n + 1023) / 1024, i0 = imin(tid * per, n), i1 = imin(i0 + per, n);
+    int sum = 0;
+    for (int i = i0; i < i1; ++i) sum += c[i];
+    int y = sum;
+#pragma unroll
+    for (int k = 1; k < 32; k <<= 1) {
+        const int z = __shfl_up_sync(0xffffffffu, y, k);
+        if (lane >= k) y += z;
+    }
+    if (lane == 31) ws[warp] = y;
+    __syncthreads();
+    if (warp == 0) {
+        const int w = ws[lane];
+        int x = w;
+#pragma unroll
+        for (int k = 1; k < 32; k <<= 1) {
+            const int z = __shfl_up_sync(0xffffffffu, x, k);
+            if (lane >= k) x += z;
+        }
+        ws[lane] = x - w;
+        if (lane == 31) ws[32] = x;
+    }
+    __syncthreads();
+    int run = y - sum + ws[warp];
+    for (int i = i0; i < i1; ++i) {
+        const int k = c[i];
+        o[i] = run;
+        c[i] = run;
+        run += k;
+    }
+    if (tid == 0) o[n] = ws[32];
+}
+
+// One thread per (view, triangle): its index into the list of each of its
+// tiles (the order within a tile carries no meaning: the paint keeps the
+// largest triangle index per pixel).
+__global__ void __launch_bounds__(256) k_prior_fill(const int32_t* __restrict__ ctr0, const int32_t* __restrict__ ctr1,
+                                                    const Raster* __restrict__ rast, int Tmax, int32_t* cursor,
+                                                    int32_t* list, int cap, int ntx, int ntiles, unsigned* err) {
+    grid_dep_wait();
     const int T0 = ctr0[0], T1 = ctr1[0];
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < T0 + T1; i += nw) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T0 + T1; i += gridDim.x * blockDim.x) {
         const bool right = i >= T0;
         const int t = right ? i - T0 : i;
-        const Raster R = rast[(right ? Tmax : 0) + t];
+        const Raster& R = rast[(right ? Tmax : 0) + t];
+        int32_t* cur = cursor + (right ? ntiles + 1 : 0);
+        int32_t* l = list + (right ? size_t(cap) : 0);
+        for (int ty = R.ty0; ty <= R.ty1; ++ty)
+            for (int tx = R.tx0; tx <= R.tx1; ++tx) {
+                const int pos = atomicAdd(cur + ty * ntx + tx, 1);
+                if (pos < cap) l[pos] = t;
+                else atomicOr(err, ERRF_BOUNDS);
+            }
+    }
+}
+
+// One CTA per (prior tile, view): every triangle of the tile's list paints
+// the pixels it covers in the tile into shared memory with atomicMax of
+// (triangle+1) << pshift | d_plane -- the last triangle in list order wins,
+// as a sequential rasteriser writing the triangles in order would leave it
+// -- and the tile is then written out whole (0 where nothing covers a
+// pixel), so no memset is needed.  A warp per triangle, lanes over columns;
+// coverage and values are the reference's scan-line expressions
+// (KerComputeDisparity.cu:57-150) with its contraction made explicit.
+__global__ void __launch_bounds__(256) k_prior_tiles(const Raster* __restrict__ rast, int Tmax,
+                                                     const int32_t* __restrict__ off,
+                                                     const int32_t* __restrict__ list, int cap, uint32_t* prior0,
+                                                     uint32_t* prior1, Geom g, int pshift, int dcap, int ntx,
+                                                     int ntiles) {
+    grid_dep_wait();
+    __shared__ uint32_t pt[PT_H][PT_W];
+    const int view = blockIdx.z, tu0 = blockIdx.x * PT_W, tv0 = blockIdx.y * PT_H;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    for (int i = tid; i < PT_W * PT_H; i += blockDim.x) (&pt[0][0])[i] = 0u;
+    __syncthreads();
+    const int32_t* o = off + view * (ntiles + 1);
+    const int tile = blockIdx.y * ntx + blockIdx.x;
+    const int b = imin(o[tile], cap), e = imin(o[tile + 1], cap);
+    const int32_t* l = list + (view ? size_t(cap) : 0);
+    const Raster* rs = rast + (view ? Tmax : 0);
+    for (int k = b + warp; k < e; k += nw) {
+        const int t = l[k];
+        const Raster R = rs[t];
         const uint32_t tag = uint32_t(t + 1) << pshift;
-        uint32_t* prior = right ? prior1 : prior0;
         for (int part = 0; part < 2; ++part) {
             const int ua = part ? int(R.B_u) : int(R.A_u), ub = part ? int(R.C_u) : int(R.B_u);
             if (ua == ub) continue;
             const float ea = part ? R.BC_a : R.AB_a, eb = part ? R.BC_b : R.AB_b;
-            for (int u = imax(ua, 0) + lane; u < imin(ub, g.W); u += 32) {
+            const int cu0 = imax(imax(ua, 0), tu0), cu1 = imin(imin(ub, g.W), tu0 + PT_W);
+            for (int u = cu0 + lane; u < cu1; u += 32) {
                 const float fu = float(u);
-                const int v1 = int(__float2uint_rz(__fmaf_rn(R.AC_a, fu, R.AC_b)));
-                const int v2 = int(__float2uint_rz(__fmaf_rn(ea, fu, eb)));
-                const int va = imax(imin(v1, v2), 0), vb = imin(imax(v1, v2), g.H);
-                auto value = [&](int v) {
+                const int v1 = raster_row(R.AC_a, R.AC_b, u), v2 = raster_row(ea, eb, u);
+                const int va = imax(imax(imin(v1, v2), 0), tv0), vb = imin(imin(imax(v1, v2), g.H), tv0 + PT_H);
+                for (int v = va; v < vb; ++v) {
                     const float dp = __fadd_rn(__fmaf_rn(R.pa, fu, __fmul_rn(R.pb, float(v))), R.pc);
                     int d = __float2int_rz(dp);
                     d = d <= 0 ? 0 : (d > dcap ? dcap : d);
-                    return tag | uint32_t(d);
-                };
-                for (int v = va; v < vb; ++v) atomicMax(&prior[size_t(v) * g.W + u], value(v));
+                    atomicMax(&pt[v - tv0][u - tu0], tag | uint32_t(d));
+                }
             }
         }
+    }
+    __syncthreads();
+    uint32_t* prior = view ? prior1 : prior0;
+    for (int i = tid; i < PT_W * PT_H; i += blockDim.x) {
+        const int r = i / PT_W, c = i - r * PT_W, u = tu0 + c, v = tv0 + r;
+        if (u < g.W && v < g.H) prior[size_t(v) * g.W + u] = pt[r][c];
     }
 }
 
@@ -387,19 +510,27 @@ __global__ void k_lr(const float* __restrict__ D1, const float* __restrict__ D2,
 
 }  // namespace
 
+size_t prior_tile_count(const Geom& g) { return size_t((g.W + PT_W - 1) / PT_W) * ((g.H + PT_H - 1) / PT_H); }
+
+size_t prior_list_capacity(const Geom& g, int Tmax) {
+    // about two tiles per triangle are typical; this leaves a factor of eight
+    return size_t(16) * Tmax + size_t(16) * prior_tile_count(g);
+}
+
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
-                         int Tmax, const int32_t* can, const int32_t* uvd, void* rast, uint32_t* prior0,
-                         uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms, cudaStream_t st,
-                         int* nlaunch) {
-    size_t n = size_t(g.W) * g.H * sizeof(uint32_t);
-    cudaMemsetAsync(prior0, 0, n, st);
-    cudaMemsetAsync(prior1, 0, n, st);
+                         int Tmax, const int32_t* can, const int32_t* uvd, void* rast, const PriorTiles& tl,
+                         uint32_t* prior0, uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms,
+                         unsigned* err, cudaStream_t st, int* nlaunch) {
+    const int ntx = (g.W + PT_W - 1) / PT_W, nty = (g.H + PT_H - 1) / PT_H, ntiles = ntx * nty;
+    cudaMemsetAsync(tl.cnt, 0, size_t(2) * (ntiles + 1) * sizeof(int32_t), st);
     Raster* R = static_cast<Raster*>(rast);
-    launch_k(k_prior_setup, imax(1, imin(8 * num_sms, (2 * Tmax + 255) / 256)), 256, 0, st, tri0, tri1, ctr0, ctr1, can,
-                                                                                      uvd, R, Tmax, g);
-    int blocks = imax(1, imin(16 * num_sms, (2 * Tmax + 7) / 8));
-    launch_k(k_prior_raster, blocks, 256, 0, st, ctr0, ctr1, R, Tmax, prior0, prior1, g, pshift, dcap);
-    if (nlaunch) *nlaunch += 2;
+    const int tblocks = imax(1, imin(8 * num_sms, (2 * Tmax + 255) / 256));
+    launch_k(k_prior_setup, tblocks, 256, 0, st, tri0, tri1, ctr0, ctr1, can, uvd, R, Tmax, g, tl.cnt, ntx, ntiles);
+    launch_k(k_prior_scan, 2, 1024, 0, st, tl.cnt, tl.off, ntiles);
+    launch_k(k_prior_fill, tblocks, 256, 0, st, ctr0, ctr1, R, Tmax, tl.cnt, tl.list, tl.cap, ntx, ntiles, err);
+    launch_k(k_prior_tiles, dim3(ntx, nty, 2), 256, 0, st, R, Tmax, tl.off, tl.list, tl.cap, prior0, prior1, g,
+             pshift, dcap, ntx, ntiles);
+    if (nlaunch) *nlaunch += 4;
     return cudaGetLastError();
 }
 

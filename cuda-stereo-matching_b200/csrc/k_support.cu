@@ -618,27 +618,10 @@ __global__ void __launch_bounds__(SWEEP_Q_THREADS) k_support_sweep_q(const uint4
     }
 }
 
-// removeInconsistentSupportPoints with snapshot semantics: reads can_in,
-// writes can_out.  The reference's bound `y < can_width`
-// (KerSupportMatches.cu:208) is kept: rows y >= cw pass through.
-__global__ void k_incon(const int32_t* __restrict__ cin, int32_t* __restrict__ cout, Geom g, DevParams p) {
-    grid_dep_wait();
-    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= g.cw || y >= g.ch) return;
-    int d = cin[size_t(y) * g.cw + x];
-    int out = d;
-    if (d >= 0 && y < g.cw) {
-        const int ws = p.incon_window;
-        int support = 0;
-        for (int y2 = max(0, y - ws); y2 <= min(g.ch - 1, y + ws); ++y2)
-            for (int x2 = max(0, x - ws); x2 <= min(g.cw - 1, x + ws); ++x2) {
-                int d2 = cin[size_t(y2) * g.cw + x2];
-                if (d2 >= 0 && abs(d - d2) <= p.incon_threshold) ++support;
-            }
-        if (support < p.incon_min_support) out = -1;
-    }
-    cout[size_t(y) * g.cw + x] = out;
-}
+// removeInconsistentSupportPoints with snapshot semantics (k_incon_rows
+// below reads the unfiltered lattice and writes a separate one).  The
+// reference's bound `y < can_width` (KerSupportMatches.cu:208) is kept: rows
+// y >= cw pass through.
 
 // Redundancy filter along one line (removeRedundantSupportPoints*,
 // KerSupportMatches.cu:241-357): point k is removed when it has a similar
@@ -724,6 +707,36 @@ __global__ void k_redundant(int32_t* __restrict__ can, Geom g, int horizontal) {
         if (horizontal) can[size_t(l) * g.cw + k] = a[k];
         else can[size_t(k) * g.cw + l] = a[k];
     }
+}
+
+// k_incon and the horizontal k_redundant pass in one kernel: one CTA per
+// candidate row computes the row's inconsistency filter (as k_incon, reading
+// the unfiltered lattice) into shared memory, warp 0 runs the row's
+// redundancy recurrence there, and the row is written once.
+__global__ void k_incon_rows(const int32_t* __restrict__ cin, int32_t* __restrict__ cout, Geom g, DevParams p) {
+    grid_dep_wait();
+    extern __shared__ int row[];                 // cw ints, then cw code bytes
+    uint8_t* code = reinterpret_cast<uint8_t*>(row + g.cw);
+    const int y = blockIdx.x;
+    for (int x = threadIdx.x; x < g.cw; x += blockDim.x) {
+        const int d = cin[size_t(y) * g.cw + x];
+        int out = d;
+        if (d >= 0 && y < g.cw) {
+            const int ws = p.incon_window;
+            int support = 0;
+            for (int y2 = max(0, y - ws); y2 <= min(g.ch - 1, y + ws); ++y2)
+                for (int x2 = max(0, x - ws); x2 <= min(g.cw - 1, x + ws); ++x2) {
+                    const int d2 = cin[size_t(y2) * g.cw + x2];
+                    if (d2 >= 0 && abs(d - d2) <= p.incon_threshold) ++support;
+                }
+            if (support < p.incon_min_support) out = -1;
+        }
+        row[x] = out;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) redundant_line(row, code, g.cw, threadIdx.x);
+    __syncthreads();
+    for (int x = threadIdx.x; x < g.cw; x += blockDim.x) cout[size_t(y) * g.cw + x] = row[x];
 }
 
 // Count valid candidates per row.
@@ -954,13 +967,14 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
             launch_k(k_support_sweep<false, false>, grid, SWEEP_THREADS, 0, st, desc0, desc1, can_lr, g, p, seg, err,
                                                                           nullptr, nullptr);
     }
-    launch_k(k_incon, dim3((g.cw + 127) / 128, g.ch), 128, 0, st, can_lr, can, g, p);
     {
-        int wpb = 4;
-        size_t sm = size_t(wpb) * g.cw * (sizeof(int) + 1);
-        launch_k(k_redundant, (g.ch + wpb - 1) / wpb, 32 * wpb, sm, st, can, g, 1);
-        sm = size_t(wpb) * g.ch * (sizeof(int) + 1);
-        launch_k(k_redundant, (g.cw + wpb - 1) / wpb, 32 * wpb, sm, st, can, g, 0);
+        const size_t sm = size_t(g.cw) * (sizeof(int) + 1);
+        const int threads = imin(1024, imax(32, ((g.cw + 31) / 32) * 32));
+        cudaFuncSetAttribute(k_incon_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+        launch_k(k_incon_rows, g.ch, threads, sm, st, can_lr, can, g, p);
+        const int wpb = 4;
+        const size_t smv = size_t(wpb) * g.ch * (sizeof(int) + 1);
+        launch_k(k_redundant, (g.cw + wpb - 1) / wpb, 32 * wpb, smv, st, can, g, 0);
     }
     (void)can_tmp;
     return cudaGetLastError();

@@ -63,14 +63,24 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
 // kernel, or 0 if none fits.
 int cluster_size_for_flip();
 
+// Triangles binned by 64x32 prior tile, both views.
+struct PriorTiles {
+    int32_t* cnt;      // [2][tiles + 1] counts, then the fill cursors
+    int32_t* off;      // [2][tiles + 1] list offsets
+    int32_t* list;     // [2][cap] triangle indices, tile by tile
+    int cap;           // entries per view (overflow raises ERRF_BOUNDS)
+};
+size_t prior_tile_count(const Geom& g);
+size_t prior_list_capacity(const Geom& g, int Tmax);
+
 // Plane prior of both views: prior[v*W+u] = (triangle+1) << pshift | d,
 // d = d_plane clamped to [0, dcap] (dcap = disp_max + plane_radius + 1),
-// 0 where no triangle covers the pixel.  The buffers are zeroed here.
+// 0 where no triangle covers the pixel.  Every pixel is written.
 // rast: scratch of 2 * Tmax * raster_bytes() for the per-triangle set-up.
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
-                         int Tmax, const int32_t* can, const int32_t* uvd, void* rast, uint32_t* prior0,
-                         uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms, cudaStream_t st,
-                         int* nlaunch);
+                         int Tmax, const int32_t* can, const int32_t* uvd, void* rast, const PriorTiles& tl,
+                         uint32_t* prior0, uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms,
+                         unsigned* err, cudaStream_t st, int* nlaunch);
 size_t raster_bytes();
 
 size_t dense_smem_bytes(const Geom& g);
