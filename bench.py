@@ -511,6 +511,8 @@ def run_only(args):
     hbm, peak_kind = peaks()
     if args.only == "large":
         out = run_large(torch, args, flush, stream, hbm, peak_kind)
+    elif args.only == "learned":
+        out = run_learned(torch, n1=3, n2=2)
     else:
         out = run_batch(torch, args, flush, stream)
     print(json.dumps(out))
@@ -560,7 +562,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
-    ap.add_argument("--only", choices=["large", "batch"], default=None,
+    ap.add_argument("--only", choices=["large", "batch", "learned"], default=None,
                     help="run one secondary workload alone (for profiling) and print its block")
     args = ap.parse_args()
     if args.warmup < 3:

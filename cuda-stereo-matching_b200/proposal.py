@@ -237,12 +237,32 @@ def evaluate(torch, theta, preset, seeds, log=None, flush_bytes=256 << 20):
             disagree.append(float(((np.abs(dp - dq) > 2) | ((dp < 0) != (dq < 0))).mean()))
             if log and (i + 1) % 50 == 0:
                 log(f"evaluated {i + 1}/{len(seeds)} pairs")
+    # support-stage device time of both paths on the last pair (per-stage
+    # event marks on, after the timed pairs): the stage the proposal narrows,
+    # network included on the learned side
+    support_ms = {}
+    for name, e in engines.items():
+        o1, o2 = outs[name]
+        e.set_timing(True)
+        acc = []
+        for k in range(6):
+            flush.zero_()
+            e.process_device(dl.data_ptr(), dr.data_ptr(), o1.data_ptr(), o2.data_ptr(), W, H,
+                             stream=stream.cuda_stream)
+            t = e.timing()
+            if k >= 2:
+                acc.append(t["support"])
+        e.set_timing(False)
+        support_ms[name] = float(np.median(acc))
     plain.close()
     learned.close()
     out = {"workload": f"{W}x{H}_disp0-{D}", "pairs": len(seeds), "seeds": f"{seeds[0]}..{seeds[-1]}",
            "fallback_rate": fell / max(settled + fell, 1), "candidates_settled": settled, "candidates_fell_back": fell,
            "bad2px_plain": float(np.mean(bad["plain"])), "bad2px_learned": float(np.mean(bad["learned"])),
            "disagree_2px": float(np.mean(disagree))}
+    out["support_stage_ms_plain"] = support_ms["plain"]
+    out["support_stage_ms_learned"] = support_ms["learned"]
+    out["support_stage_speedup"] = support_ms["plain"] / support_ms["learned"]
     for name in ("plain", "learned"):
         out[f"pairs_per_s_{name}"] = len(seeds) / (sum(ms[name]) / 1e3)
         out[f"ms_per_pair_{name}"] = float(np.mean(ms[name]))
