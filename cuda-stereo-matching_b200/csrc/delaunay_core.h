@@ -35,6 +35,7 @@
 // sequential host emulation used by the CPU tests.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include "common.cuh"
 
@@ -328,6 +329,338 @@ struct FlatTri {
     HD void set_opp(int h, int o) { topp[h] = o; }
     HD void set_fround(int t, int32_t r) { tround[t] = r; }
 };
+
+// ---------------------------------------------------------------------------
+// Stars: the Delaunay neighbours of one point, found directly.
+//
+// Under the perturbation the triangulation is unique, so each point's star
+// (its neighbours in counter-clockwise order) can be computed on its own and
+// the stars of all points agree.  The walk around p starts at p's nearest
+// neighbour q0 (the disc with diameter p q0 holds no other point, so p q0 is
+// an edge of every Delaunay triangulation).  From an edge p->q the next
+// neighbour on a side is, among the points strictly on that side, the one
+// whose circle through p and q holds no other of them: the circles through
+// p and q form a pencil, and "b lies inside the circle through p, q, a" is a
+// strict total order on the points of one side (the perturbed incircle
+// determinant is antisymmetric in a and b).  The minimum of that order is the
+// next neighbour; a side with no point marks a hull edge.  The walk goes
+// counter-clockwise until it returns to q0 (an interior point) or meets the
+// hull, and then clockwise from q0 to the hull on the other side.
+
+constexpr uint32_t PXY_NONE = 0xFFFFFFFFu;   // a dropped duplicate point
+
+// For the edge p->q and two points a, b on the walk's side, is b the better
+// next neighbour (inside the circle through p, q and a)?  side > 0: left of
+// p->q, triangle (p, q, a) counter-clockwise; side < 0: right, triangle
+// (p, a, q).
+HD bool star_better(int ip, uint32_t pp, int iq, uint32_t pq, int ia, uint32_t pa, int ib, uint32_t pb, int side) {
+    return side > 0 ? inside_sos_p(ip, pp, iq, pq, ia, pa, ib, pb) : inside_sos_p(ip, pp, ia, pa, iq, pq, ib, pb);
+}
+
+// Is b strictly on the walk's side of p->q?
+HD bool star_side(uint32_t pp, uint32_t pq, uint32_t pb, int side) {
+    const int64_t o = orient_p(pp, pq, pb);
+    return side > 0 ? o > 0 : o < 0;
+}
+
+// Does every point inside the circle through p, q and r lie in the square
+// |x - px|, |y - py| <= R?  Points exist only in the box [bx0, bx1] x
+// [by0, by1] (all points of the problem), so only the part of the circle
+// inside the box counts: its extent is bounded through the circle's chords
+// at the box edges nearest the centre.  Every point outside the square is
+// at least R + 1 away from p in x or in y, which leaves a pixel of margin
+// for the rounding of the centre and the chords (the centre's numerators
+// and denominator are exact integers in double).  *need: the square that
+// would pass.
+HD bool circle_within(uint32_t pp, uint32_t pq, uint32_t pr, int R, const int32_t* box, int* need) {
+    const double qx = dx_p(pq, pp), qy = dy_p(pq, pp), rx = dx_p(pr, pp), ry = dy_p(pr, pp);
+    const double d = 2.0 * (qx * ry - qy * rx);
+    const double q2 = qx * qx + qy * qy, r2 = rx * rx + ry * ry;
+    const double cx = (ry * q2 - qy * r2) / d, cy = (qx * r2 - rx * q2) / d;
+    const double rho2 = cx * cx + cy * cy;
+    // the box relative to p
+    const double bx0 = box[0] - px_of(pp), by0 = box[1] - py_of(pp), bx1 = box[2] - px_of(pp), by1 = box[3] - py_of(pp);
+    const double ey = fmin(fmax(cy, by0), by1) - cy, ex = fmin(fmax(cx, bx0), bx1) - cx;
+    double ext = 0.0;
+    if (ey * ey < rho2 && ex * ex < rho2) {
+        const double h = sqrt(rho2 - ey * ey), v = sqrt(rho2 - ex * ex);
+        const double x0 = fmax(cx - h, bx0), x1 = fmin(cx + h, bx1);
+        const double y0 = fmax(cy - v, by0), y1 = fmin(cy + v, by1);
+        ext = fmax(fmax(-x0, x1), fmax(-y0, y1));
+    }
+    if (need) *need = ext < 1e9 ? int(ext) + 2 : (1 << 30);
+    return ext <= double(R);
+}
+
+// Search policy of the star walk.  A search first takes a point's window,
+// the points with |x - px|, |y - py| <= R0, staged once per point (up to
+// STAR_CAP of them), and then squares of doubling half-size Rs
+// (star_square) around p until its answer is proven:
+//  * nearest neighbour at distance d: proven once d <= Rs; if the first
+//    square with a candidate does not prove it, the square of half-size d
+//    holds the answer and is searched last;
+//  * next neighbour r: proven once its circle passes circle_within(Rs).
+//    When the circle reaches no further than 2 Rs, the part of the circle
+//    through p, q, r inside the box is searched instead of the next square
+//    (the answer's circle on that side of p->q nests inside it, so the
+//    answer lies there).  A near-collinear r has a huge circle although the
+//    answer is often just outside the window: growing the square finds it
+//    at a small cost where the circle would cover much of the box.
+// A square covering the box holds every point, so its answer is final (and
+// "none" proves a hull edge).
+constexpr int STAR_CAP = 512;
+
+// The window's half-size R0 of a problem: 3.5 mean point spacings (the
+// square root of the box area per point), within [16, 128] pixels.  Most
+// stars then need no second search (a smaller window makes most steps
+// search again, a larger one makes every step scan more points).  Exact
+// double operations: the same value on the host and the device.
+HD int star_r0(const int32_t* box, int n) {
+    const double area = double(box[2] - box[0] + 1) * double(box[3] - box[1] + 1);
+    const double r = 3.5 * sqrt(area / double(n > 0 ? n : 1));
+    return r < 16.0 ? 16 : (r > 128.0 ? 128 : int(r));
+}
+constexpr int STAR_NB = 256;      // neighbours of one point on each side of its start
+
+// Half-size of the next square after one of half-size R held no candidate.
+HD int star_square(int R) { return R < (1 << 20) ? 2 * R : R; }
+
+// The rows [y0, y1] and, per row y, the columns [x0, x1] of a region:
+// a square of half-size R around (px, py), or the circle (centre (cx, cy),
+// squared radius rho2, absolute coordinates) with a pixel of margin; both
+// clipped to the box.  An empty range has y0 > y1 or x0 > x1.
+struct StarRegion {
+    bool circle;
+    double cx, cy, rho2;
+    int32_t sx0, sx1;     // square columns
+    int32_t y0, y1;
+    // optional half-plane (a square searched for a next neighbour): only
+    // the points strictly on side `side` of the line through (hx, hy) with
+    // direction (ux, uy) count, kept with a pixel of margin
+    int32_t hx, hy, ux, uy, side;
+    HD void cols(int32_t y, const int32_t* box, int32_t* x0, int32_t* x1) const {
+        if (!circle) {
+            *x0 = sx0;
+            *x1 = sx1;
+            if (side != 0) {
+                if (uy == 0) {
+                    if (int64_t(ux) * (y - hy) * side <= 0) *x0 = *x1 + 1;
+                } else {
+                    const double xl = double(hx) + double(ux) * double(y - hy) / double(uy);
+                    if ((uy > 0) == (side > 0))
+                        *x1 = int32_t(fmax(fmin(double(*x1), ceil(xl) + 1.0), double(*x0) - 1.0));
+                    else
+                        *x0 = int32_t(fmin(fmax(double(*x0), floor(xl) - 1.0), double(*x1) + 1.0));
+                }
+            }
+            return;
+        }
+        // half-chord at row y, plus a pixel for the rounding of the centre
+        // and radius (both far below a pixel at these coordinates)
+        const double dy = double(y) - cy;
+        const double h = sqrt(fmax(rho2 - dy * dy, 0.0)) + 1.0;
+        // clamped into the box (an empty range stays empty) before the
+        // conversion: a near-degenerate circle's centre can lie far outside
+        *x0 = int32_t(fmin(fmax(floor(cx - h) - 1.0, double(box[0])), double(box[2]) + 1.0));
+        *x1 = int32_t(fmax(fmin(ceil(cx + h) + 1.0, double(box[2])), double(box[0]) - 1.0));
+    }
+};
+
+HD StarRegion star_square_region(uint32_t pp, int R, const int32_t* box) {
+    StarRegion g;
+    g.circle = false;
+    g.cx = g.cy = g.rho2 = 0.0;
+    g.hx = g.hy = g.ux = g.uy = g.side = 0;
+    const int32_t px = px_of(pp), py = py_of(pp);
+    g.sx0 = imax(px - R, box[0]);
+    g.sx1 = imin(px + R, box[2]);
+    g.y0 = imax(py - R, box[1]);
+    g.y1 = imin(py + R, box[3]);
+    return g;
+}
+
+// The square of half-size R around p restricted to side `side` of p->q.
+HD StarRegion star_half_region(uint32_t pp, uint32_t pq, int side, int R, const int32_t* box) {
+    StarRegion g = star_square_region(pp, R, box);
+    g.hx = px_of(pp);
+    g.hy = py_of(pp);
+    g.ux = dx_p(pq, pp);
+    g.uy = dy_p(pq, pp);
+    g.side = side;
+    return g;
+}
+
+// The circle through p, q and r (any order), clipped to the box.
+HD StarRegion star_circle_region(uint32_t pp, uint32_t pq, uint32_t pr, const int32_t* box) {
+    const double qx = dx_p(pq, pp), qy = dy_p(pq, pp), rx = dx_p(pr, pp), ry = dy_p(pr, pp);
+    const double d = 2.0 * (qx * ry - qy * rx);
+    const double q2 = qx * qx + qy * qy, r2 = rx * rx + ry * ry;
+    const double cx = (ry * q2 - qy * r2) / d, cy = (qx * r2 - rx * q2) / d;
+    StarRegion g;
+    g.circle = true;
+    g.hx = g.hy = g.ux = g.uy = g.side = 0;
+    g.cx = cx + px_of(pp);
+    g.cy = cy + py_of(pp);
+    g.rho2 = cx * cx + cy * cy;
+    g.sx0 = g.sx1 = 0;
+    const double rho = sqrt(g.rho2);
+    g.y0 = int32_t(fmax(floor(g.cy - rho) - 1.0, double(box[1])));
+    g.y1 = int32_t(fmin(ceil(g.cy + rho) + 1.0, double(box[3])));
+    return g;
+}
+
+// Walk the star.  An interior point (hn < 0) starts at nearest(), p's
+// nearest neighbour, and walks counter-clockwise until it is back there.  A
+// point of the hull boundary starts at hn, its successor on the boundary
+// (counter-clockwise, the interior on the left), and walks until it reaches
+// hp, its predecessor.  next(q, side) returns the next neighbour after q on
+// that side (-1: none, so p->q is a hull edge; -2: the search failed).
+// The neighbours are appended to ccw (counter-clockwise) and, should an
+// interior point meet the hull (all points collinear), to cw (clockwise from
+// the start); star_at gives them in counter-clockwise order.  Returns false
+// if a search failed or a list would pass cap.
+template <class Nearest, class Next>
+HD bool star_walk(int hn, int hp, Nearest nearest, Next next, int32_t* ccw, int32_t* cw, int cap, int* m, int* k,
+                  bool* closed) {
+    *m = 0;
+    *k = 0;
+    *closed = false;
+    const int q0 = hn >= 0 ? hn : nearest();
+    if (q0 < 0) return q0 == -1;
+    ccw[(*m)++] = q0;
+    int q = q0;
+    for (;;) {
+        const int r = next(q, +1);
+        if (r == -2) return false;
+        if (r < 0) break;
+        if (r == q0) {
+            *closed = hn < 0;
+            return hn < 0;
+        }
+        if (*m >= cap) return false;
+        ccw[(*m)++] = r;
+        if (r == hp) return true;
+        q = r;
+    }
+    if (hn >= 0) return true;
+    q = q0;
+    for (;;) {
+        const int r = next(q, -1);
+        if (r == -2) return false;
+        if (r < 0) break;
+        if (*k >= cap) return false;
+        cw[(*k)++] = r;
+        q = r;
+    }
+    return true;
+}
+
+// The hull boundary, counter-clockwise (the interior on the left of each
+// step), from the rows' extreme points: the top row left to right, the
+// right chain down, the bottom row right to left, the left chain up.  The
+// chains are the rows' last (first) points with the concave ones removed by
+// the monotone stack walk; collinear points stay, as every point on the
+// boundary is a vertex of the triangulation.  xy[s] holds the packed
+// coordinates of the leftmost (side 0) or rightmost (side 1) point of
+// non-empty row s (of R, top to bottom).  Writes the chain as row positions
+// (top to bottom; room for R) and its length.
+HD void hull_chain(int side, int R, const uint32_t* xy, int32_t* st, int* len) {
+    int sp = 0;
+    uint32_t a = 0, b = 0;     // the stack's top two points
+    for (int s = 0; s < R; ++s) {
+        const uint32_t x = xy[s];
+        while (sp >= 2) {
+            const int64_t o = orient_p(a, b, x);
+            if (side ? o < 0 : o > 0) {
+                --sp;
+                b = a;
+                if (sp >= 2) a = xy[st[sp - 2]];
+            } else {
+                break;
+            }
+        }
+        st[sp++] = s;
+        a = b;
+        b = x;
+    }
+    *len = sp;
+}
+
+// The same chain, decided point by point (for a parallel build): row i's
+// point is dropped by the stack walk exactly when it lies strictly inside
+// the segment of two other chain points j < i < k (strictly right of L_j ->
+// L_k for the left chain, left of it for the right chain).  With
+// coordinates relative to point i and x mirrored for the right chain, that
+// holds iff min_{j<i} x_j / -y_j + min_{k>i} x_k / y_k < 0 (the rows above
+// have y < 0, those below y > 0); both minima and their sum are compared
+// as exact fractions.  |x| <= 18094 and 0 < y <= 16383 (the coordinate
+// limits of orient_p), so every cross product is below 2^29 and the final
+// sum below 2^30: exact in int32.
+HD bool hull_on_chain(int side, int R, const uint32_t* xy, int i) {
+    if (i == 0 || i == R - 1) return true;
+    const uint32_t c = xy[i];
+    const int sg = side ? -1 : 1;
+    // each minimum over four interleaved partial minima (independent chains)
+    int32_t n[2][4], d[2][4];
+    for (int h = 0; h < 2; ++h)
+        for (int u = 0; u < 4; ++u) {
+            n[h][u] = 1;
+            d[h][u] = 0;     // +infinity: 1/0 compares above every fraction below
+        }
+    auto fold = [&](int h, int u, uint32_t v, int dsign) {
+        const int32_t x = sg * dx_p(v, c), dd = dsign * dy_p(v, c);
+        if (d[h][u] == 0 || x * d[h][u] < n[h][u] * dd) {
+            n[h][u] = x;
+            d[h][u] = dd;
+        }
+    };
+    int j = 0;
+    for (; j + 4 <= i; j += 4)
+        for (int u = 0; u < 4; ++u) fold(0, u, xy[j + u], -1);
+    for (; j < i; ++j) fold(0, 0, xy[j], -1);
+    int k = i + 1;
+    for (; k + 4 <= R; k += 4)
+        for (int u = 0; u < 4; ++u) fold(1, u, xy[k + u], 1);
+    for (; k < R; ++k) fold(1, 0, xy[k], 1);
+    int32_t sn = n[0][0], sd = d[0][0], tn = n[1][0], td = d[1][0];
+    for (int u = 1; u < 4; ++u) {
+        if (d[0][u] != 0 && n[0][u] * sd < sn * d[0][u]) { sn = n[0][u]; sd = d[0][u]; }
+        if (d[1][u] != 0 && n[1][u] * td < tn * d[1][u]) { tn = n[1][u]; td = d[1][u]; }
+    }
+    return sn * td + tn * sd >= 0;
+}
+
+// Position j of the boundary cycle (hull_chain's layout): top row (tl
+// points) left to right, right chain rows 1..nr-1, bottom row (bl points)
+// right to left from its second last, left chain rows nl-2..1.  Returns
+// (row position, index within that row); the cycle has
+// tl + (nr - 1) + (bl - 1) + (nl - 2) points when the top and bottom rows
+// differ.
+HD int hull_cycle_len(int tl, int bl, int nl, int nr) { return tl + (nr - 1) + (bl - 1) + (nl - 2); }
+HD void hull_cycle_at(int j, int R, int tl, int bl, const int32_t* lstk, int nl, const int32_t* rstk, int nr,
+                      int* row, int* pos, bool* last) {
+    *last = false;
+    if (j < tl) { *row = 0; *pos = j; return; }
+    j -= tl;
+    if (j < nr - 1) { *row = rstk[j + 1]; *pos = 0; *last = true; return; }
+    j -= nr - 1;
+    if (j < bl - 1) { *row = R - 1; *pos = bl - 2 - j; return; }
+    j -= bl - 1;
+    *row = lstk[nl - 2 - j];
+    *pos = 0;
+}
+
+// Neighbour i in counter-clockwise order: the clockwise part reversed, then
+// the counter-clockwise part.
+HD int32_t star_at(const int32_t* ccw, int m, const int32_t* cw, int k, int i) {
+    (void)m;
+    return i < k ? cw[k - 1 - i] : ccw[i - k];
+}
+
+// Triangles of a star of deg neighbours: (p, nb(i), nb(i+1)), wrapping when
+// closed.  Triangle i is emitted by p when p is its smallest vertex, which
+// makes it come out normalised (see normalise below).
+HD int star_tris(int deg, bool closed) { return closed ? deg : (deg > 0 ? deg - 1 : 0); }
 
 // Rotate a triangle so its smallest vertex index comes first.
 HD void normalise(int32_t* v) {

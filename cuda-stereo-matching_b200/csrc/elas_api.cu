@@ -258,6 +258,17 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         D.ccand = (int32_t*)take(16 * 2 * per_cta * 4);
         D.cflips = (int32_t*)take(16 * per_cta * 4);
         D.ctr = (int32_t*)take(16 * 4);
+        D.pxy = (uint32_t*)take(nmax * 4);
+        D.sxy = (uint32_t*)take(nmax * 4);
+        D.ne_y = (int32_t*)take(rows * 4);
+        D.tcnt = (int32_t*)take(nmax * 4);
+        D.toff = (int32_t*)take(nmax * 4);
+        D.sown = (int32_t*)take(24 * nmax * 4);
+        D.spool = (int32_t*)take(2 * tmax * 4);
+        D.hnext = (int32_t*)take(nmax * 4);
+        D.hprev = (int32_t*)take(nmax * 4);
+        D.box = (int32_t*)take(32);
+        D.ylut = (int32_t*)take((size_t(g.H) + 2) * 4);
         D.hkey = (unsigned long long*)take(hmax * 8);
         D.hcnt = (int32_t*)take(hmax * 4);
         D.hval = (int32_t*)take(2 * hmax * 4);
@@ -490,13 +501,20 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     CK(mark(ELAS_TIME_GRID));
     CK(launch_grid(h->can, h->gtmp0, h->gtmp1, h->grid0, h->grid1, g, st, &n));
     CK(mark(ELAS_TIME_DELAUNAY));
-    CK(launch_delaunay(h->del[0], h->del[1], h->row_off, g.ch + corners, g.cw * g.ch + 6 * corners, h->num_sms,
-                       h->cluster_size, h->err, st, &n, (h->test_flags & ELAS_TEST_FLIP_GLOBAL) != 0,
+    const bool flips = (h->test_flags & (ELAS_TEST_DELAUNAY_FLIPS | ELAS_TEST_FLIP_GLOBAL)) != 0 ||
+                       h->flip_round_limit > 0 ||
+                       ((h->test_flags & ELAS_TEST_DELAUNAY_STARS) == 0 &&
+                        (long long)W * H > DELAUNAY_STARS_MAX_PIXELS);
+    CK(launch_delaunay(h->del[0], h->del[1], h->row_off, g.ch + corners, g.cw * g.ch + 6 * corners, H, h->num_sms,
+                       h->cluster_size, h->err, st, &n, flips, (h->test_flags & ELAS_TEST_FLIP_GLOBAL) != 0,
                        h->flip_round_limit));
     CK(mark(ELAS_TIME_PRIOR));
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
                     h->rast, h->ptiles, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1,
-                    h->num_sms, h->err, st, &n));
+                    h->num_sms, h->err, st, &n,
+                    (h->test_flags & ELAS_TEST_PRIOR_TILED) != 0 ||
+                        ((h->test_flags & ELAS_TEST_PRIOR_DIRECT) == 0 &&
+                         (long long)W * H >= PRIOR_TILED_MIN_PIXELS)));
     int shape = 512;
     rc = dense_threads_for(h, g, dp, st, &n, &shape);
     if (rc != ELAS_OK) return rc;
@@ -1020,8 +1038,15 @@ int elas_b200_process_batch_device(elas_handle* h, int n, const uint8_t* const* 
 
 int elas_b200_set_test_mode(elas_handle* h, int32_t flags, int32_t flip_round_limit) {
     if (!h) return ELAS_ERR_INVALID_ARG;
-    if ((flags & ~(ELAS_TEST_FLIP_GLOBAL | ELAS_TEST_DENSE_BITSET)) != 0 || flip_round_limit < 0)
+    const int32_t known = ELAS_TEST_FLIP_GLOBAL | ELAS_TEST_DENSE_BITSET | ELAS_TEST_PRIOR_TILED |
+                          ELAS_TEST_PRIOR_DIRECT | ELAS_TEST_DELAUNAY_FLIPS | ELAS_TEST_DELAUNAY_STARS;
+    if ((flags & ~known) != 0 || flip_round_limit < 0)
         return fail(h, ELAS_ERR_INVALID_ARG, "unknown test flag or negative round limit");
+    if ((flags & ELAS_TEST_DELAUNAY_STARS) &&
+        ((flags & (ELAS_TEST_DELAUNAY_FLIPS | ELAS_TEST_FLIP_GLOBAL)) || flip_round_limit > 0))
+        return fail(h, ELAS_ERR_INVALID_ARG, "both Delaunay constructions forced");
+    if ((flags & ELAS_TEST_PRIOR_TILED) && (flags & ELAS_TEST_PRIOR_DIRECT))
+        return fail(h, ELAS_ERR_INVALID_ARG, "both prior paint paths forced");
     h->test_flags = flags;
     h->flip_round_limit = flip_round_limit;
     return ELAS_OK;

@@ -5,6 +5,7 @@
 //
 // Both views run as two independent problems inside the same launches:
 // problem 0 triangulates (u, v), problem 1 triangulates (u - d, v).
+#include <climits>
 #include <cooperative_groups.h>
 #include <type_traits>
 #include <cuda_runtime.h>
@@ -127,8 +128,9 @@ __device__ __forceinline__ void propose_owned(int h0, int h1, int32_t* ring, Opp
 }
 
 // Per lattice row: sort the row's points by (x, index), drop repeated x
-// (keeps the lowest index), write the unique list to srt[row_off[r] ..] and
-// its length to rcnt[r].
+// (keeps the lowest index), write the unique list to srt[row_off[r] ..]
+// (with the packed coordinates beside it in sxy) and its length to rcnt[r];
+// pxy[i] gets point i's packed coordinates, or PXY_NONE if it was dropped.
 __global__ void __launch_bounds__(512) k_rowsort(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off,
                                                  int nrows, unsigned* err) {
     grid_dep_wait();
@@ -181,23 +183,107 @@ __global__ void __launch_bounds__(512) k_rowsort(DelDev d0, DelDev d1, const int
     }
     __syncthreads();
     int base = wcnt[warp];
+    const int32_t yr = n > 0 ? D.y[b] : 0;      // the row's y
     for (int i0 = warp * span; i0 < min(n, (warp + 1) * span); i0 += 32) {
         int i = i0 + lane;
-        bool k = i < min(n, (warp + 1) * span) && keep[i];
+        const bool in = i < min(n, (warp + 1) * span);
+        bool k = in && keep[i];
         unsigned m = __ballot_sync(0xffffffffu, k);
-        if (k) D.srt[b + base + __popc(m & ((1u << lane) - 1))] = int32_t(key[i] & 0xffffffffu);
+        if (in) {
+            const int32_t idx = int32_t(key[i] & 0xffffffffu);
+            const uint32_t xy = pack_xy(int32_t(uint32_t(key[i] >> 32) ^ 0x80000000u), yr);
+            // packed coordinates by point (the star searches), PXY_NONE for a dropped duplicate
+            D.pxy[idx] = k ? xy : PXY_NONE;
+            D.hnext[idx] = -1;
+            D.hprev[idx] = -1;
+            if (k) {
+                const int pos = b + base + __popc(m & ((1u << lane) - 1));
+                D.srt[pos] = idx;
+                D.sxy[pos] = xy;
+            }
+        }
         base += __popc(m);
     }
 }
 
-// Non-empty rows (list + rank) and strip offsets.  One 1024-thread block
-// per problem.  ctr[7] = 1 when the plan holds (two non-empty rows at least,
+// For the star construction, in the block of k_plan once the non-empty
+// rows and their y are known: the table ylut (y -> first non-empty row at or
+// below y, for y in [0, H]), the box of all points (box[0..3]) and the
+// window half-size (box[4], star_r0), and the hull boundary
+// (hnext / hprev of every boundary point; the rows' extreme points are
+// staged in shared memory and each decided by hull_on_chain).
+__device__ void star_setup(const DelDev& D, const int32_t* __restrict__ row_off, int R, int H, int npts,
+                           uint32_t* xyf, uint32_t* xyl, int32_t* lstk, int32_t* rstk, int* ws) {
+    __shared__ int box_s[4];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    __syncthreads();     // ne_y was written by other threads of the block
+    for (int s = tid; s <= R; s += nt) {
+        const int lo = s ? D.ne_y[s - 1] + 1 : 0, hi = s < R ? D.ne_y[s] : H;
+        for (int v = lo; v <= hi && v <= H; ++v) D.ylut[v] = s;
+    }
+    if (tid == 0) {
+        box_s[0] = INT_MAX;
+        box_s[2] = INT_MIN;
+    }
+    __syncthreads();
+    for (int s = tid; s < R; s += nt) {
+        const int r = D.ne[s], b = row_off[r];
+        xyf[s] = D.sxy[b];
+        xyl[s] = D.sxy[b + D.rcnt[r] - 1];
+        atomicMin(&box_s[0], px_of(xyf[s]));
+        atomicMax(&box_s[2], px_of(xyl[s]));
+    }
+    __syncthreads();
+    if (tid == 0) {
+        D.box[0] = R ? box_s[0] : 0;
+        D.box[1] = R ? D.ne_y[0] : 0;
+        D.box[2] = R ? box_s[2] : 0;
+        D.box[3] = R ? D.ne_y[R - 1] : 0;
+        const int32_t b[4] = {D.box[0], D.box[1], D.box[2], D.box[3]};
+        D.box[4] = star_r0(b, npts);
+    }
+    if (R < 2) return;
+    // the chains, decided point by point and compacted in row order
+    int nl = 0, nr = 0;
+    for (int b = 0; b < R; b += nt) {
+        const int i = b + tid;
+        const int fl = i < R && hull_on_chain(0, R, xyf, i) ? 1 : 0;
+        const int fr = i < R && hull_on_chain(1, R, xyl, i) ? 1 : 0;
+        int tl_ = 0, tr_ = 0;
+        const int pl = block_scan(fl, ws, &tl_);
+        const int pr = block_scan(fr, ws, &tr_);
+        if (fl) lstk[nl + pl] = i;
+        if (fr) rstk[nr + pr] = i;
+        nl += tl_;
+        nr += tr_;
+    }
+    __syncthreads();
+    const int top = D.ne[0], bot = D.ne[R - 1];
+    const int tl = D.rcnt[top], bl = D.rcnt[bot];
+    const int C = hull_cycle_len(tl, bl, nl, nr);
+    auto at = [&](int j) {
+        int row, pos;
+        bool last;
+        hull_cycle_at(j, R, tl, bl, lstk, nl, rstk, nr, &row, &pos, &last);
+        const int r = D.ne[row];
+        return D.srt[row_off[r] + (last ? D.rcnt[r] - 1 : pos)];
+    };
+    for (int j = tid; j < C; j += nt) {
+        const int v = at(j);
+        D.hnext[v] = at(j + 1 == C ? 0 : j + 1);
+        D.hprev[v] = at(j == 0 ? C - 1 : j - 1);
+    }
+}
+
+// Non-empty rows (list, and their y for the star searches) and strip
+// offsets.  One 1024-thread block per problem.  ctr[7] = 1 when the plan holds (two non-empty rows at least,
 // strips and pockets within Tmax); the strips and pockets are then built by
 // k_strips, which also sets the triangle count ctr[0].
 __global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off,
-                                               int nrows, unsigned* err) {
+                                               int nrows, int H, unsigned* err) {
     grid_dep_wait();
     __shared__ int ws[33];
+    extern __shared__ uint32_t hsm[];    // hull: 4 arrays of nrows entries
     DelDev D = blockIdx.x ? d1 : d0;
     int R = 0, total = 0;
     // non-empty rows in order, and each row's rank
@@ -209,6 +295,9 @@ __global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32
         R += total;
     }
     __syncthreads();
+    for (int s = threadIdx.x; s < R; s += blockDim.x) D.ne_y[s] = D.y[row_off[D.ne[s]]];
+    star_setup(D, row_off, R, H, row_off[nrows], hsm, hsm + nrows, reinterpret_cast<int32_t*>(hsm + 2 * nrows),
+               reinterpret_cast<int32_t*>(hsm + 3 * nrows), ws);
     // strip s between ne[s] and ne[s+1] holds rcnt[ne[s]] + rcnt[ne[s+1]] - 2 triangles
     int off = 0;
     for (int s0 = 0; s0 < R - 1; s0 += blockDim.x) {
@@ -227,6 +316,403 @@ __global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32
         D.ctr[7] = (R >= 2 && fits) ? 1 : 0;
         D.ctr[8] = 0;    // set to 1 by the flip kernel that handles the problem
         D.ctr[9] = row_off[nrows];   // support points (vertex ids) of the problem
+        D.ctr[4] = 0;    // flip rounds and flips (the flip kernels set them)
+        D.ctr[5] = 0;
+        D.ctr[11] = 0;   // star construction: overflow pool cursor, windows grown, searches over all points
+        D.ctr[12] = 0;
+        D.ctr[13] = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Star construction (delaunay_core.h, star_walk): one warp per point finds
+// the point's Delaunay neighbours directly, with no initial triangulation
+// and no flips.  Candidates come from the rows (ne_y gives each non-empty
+// row's y; a row's points are sorted by x with their packed coordinates in
+// sxy), gathered into shared memory per window; every search is a warp-wide
+// minimum under the star order, so its answer does not depend on how the
+// lanes split the candidates.
+
+constexpr int STAR_WARPS = 8;      // points in flight per CTA
+constexpr int STAR_SLOT = 12;      // owned triangles kept in a point's own slot; more go to the pool
+
+// The star order as a float key: for the edge p->q (u = q - p) and a
+// candidate s (relative to p) strictly on the walk's side, the centre of
+// the circle through p, q, s lies at q/2 + t (-uy, ux) with
+// t = (|s|^2 - u.s) / (2 cross(u, s)); the next neighbour has the smallest
+// t on the left and the largest on the right, i.e. the smallest
+// (|s|^2 - u.s) / |cross(u, s)| on either side.  Numerator and denominator
+// are exact in int32 (below 2^31 at the coordinate limits of orient_p);
+// the key carries at most three roundings (two conversions, one division of
+// at most 2 ulp), a relative error below 4e-7, so keys further apart than
+// 4e-6 of the larger order their points correctly and closer ones are
+// compared exactly.
+__device__ __forceinline__ bool star_key(int32_t ux, int32_t uy, int32_t sx, int32_t sy, int side, float* key) {
+    const int32_t cr = ux * sy - uy * sx;           // orient(p, q, s)
+    if (side > 0 ? cr <= 0 : cr >= 0) return false;
+    const int32_t num = sx * sx + sy * sy - (ux * sx + uy * sy);
+    *key = __fdividef(__int2float_rn(num), __int2float_rn(cr > 0 ? cr : -cr));
+    return true;
+}
+
+struct StarSmem {
+    int32_t cid[STAR_CAP];         // the point's window: point index
+    uint32_t cxy[STAR_CAP];        // and packed coordinates
+    int32_t ccw[STAR_NB];          // the walk's two neighbour lists
+    int32_t cw[STAR_NB];
+};
+
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
+}
+
+// Every point of a region, spread evenly over the warp's lanes: each lane
+// takes a row (ylut gives the rows of the region's y range), finds the
+// row's column range by binary search in the row's sorted coordinates, and
+// the ranges of 32 rows are then dealt out one point per lane (a lane finds
+// the row of its point by a binary search over the lanes' offsets).
+// take(index, packed xy, k) receives each point with its running number k.
+template <class Take>
+__device__ void star_stream(const DelDev& D, const int32_t* __restrict__ row_off, const StarRegion& g,
+                            const int32_t* box, int lane, Take&& take) {
+    if (g.y0 > g.y1) return;
+    const int s0 = D.ylut[g.y0], s1 = D.ylut[g.y1 + 1];
+    int done = 0;
+    for (int sb = s0; sb < s1; sb += 32) {
+        const int srow = sb + lane;
+        int b = 0, n = 0;
+        if (srow < s1) {
+            int32_t x0, x1;
+            g.cols(D.ne_y[srow], box, &x0, &x1);
+            if (x0 <= x1) {
+                const int r = D.ne[srow];
+                const int base = row_off[r], cnt = D.rcnt[r];
+                const uint32_t* xs = D.sxy + base;
+                int l = 0, h = cnt;
+                while (l < h) {
+                    const int mid = (l + h) >> 1;
+                    if (px_of(xs[mid]) < x0) l = mid + 1;
+                    else h = mid;
+                }
+                const int lb = l;
+                h = cnt;
+                while (l < h) {
+                    const int mid = (l + h) >> 1;
+                    if (px_of(xs[mid]) <= x1) l = mid + 1;
+                    else h = mid;
+                }
+                b = base + lb;
+                n = l - lb;
+            }
+        }
+        int incl = n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int tot = __shfl_sync(0xffffffffu, incl, 31), excl = incl - n;
+        for (int kb = 0; kb < tot; kb += 32) {
+            const int k = kb + lane;
+            int j = 0;
+#pragma unroll
+            for (int st = 16; st > 0; st >>= 1) {
+                const int c = j + st;
+                const int e = __shfl_sync(0xffffffffu, excl, c & 31);
+                if (c < 32 && e <= k) j = c;
+            }
+            const int jb = __shfl_sync(0xffffffffu, b, j), je = __shfl_sync(0xffffffffu, excl, j);
+            if (k < tot) {
+                const int pos = jb + k - je;
+                take(D.srt[pos], D.sxy[pos], done + k);
+            }
+        }
+        done += tot;
+    }
+}
+
+// Grid-stride over (point, view) with one warp per point: the star
+// (star_walk with the two-phase searches of the search policy), its owned
+// triangles (p the smallest vertex) counted into tcnt[p] and stored as
+// vertex pairs in p's slot (or in the pool when more than STAR_SLOT).
+__global__ void __launch_bounds__(STAR_WARPS * 32, 4) k_star(DelDev d0, DelDev d1,
+                                                           const int32_t* __restrict__ row_off, unsigned* err) {
+    grid_dep_wait();
+    __shared__ StarSmem smem[STAR_WARPS];
+    const DelDev& D = blockIdx.y ? d1 : d0;
+    const int N = D.ctr[9];
+    const int32_t box[4] = {D.box[0], D.box[1], D.box[2], D.box[3]};
+    const int R0 = D.box[4];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    StarSmem& sm = smem[warp];
+    for (int p = blockIdx.x * STAR_WARPS + warp; p < N; p += gridDim.x * STAR_WARPS) {
+        const uint32_t pp = D.pxy[p];
+        if (pp == PXY_NONE) {
+            if (lane == 0) D.tcnt[p] = 0;
+            continue;
+        }
+        const int px = px_of(pp), py = py_of(pp);
+        const int hn = D.hnext[p], hp = D.hprev[p];
+        int circles = 0, squares = 0;
+        // phase 1: the window, staged once (streamed again by each search if it holds more than STAR_CAP)
+        const StarRegion win = star_square_region(pp, R0, box);
+        int K = 0;
+        star_stream(D, row_off, win, box, lane, [&](int32_t s, uint32_t sxy, int k) {
+            if (k < STAR_CAP) {
+                sm.cid[k] = s;
+                sm.cxy[k] = sxy;
+            }
+            K = k + 1;
+        });
+        K = __reduce_max_sync(0xffffffffu, K);
+        __syncwarp();
+        const bool staged = K <= STAR_CAP;
+        auto window = [&](auto&& take) {
+            if (staged) {
+                for (int k = lane; k < K; k += 32) take(sm.cid[k], sm.cxy[k]);
+            } else {
+                star_stream(D, row_off, win, box, lane, [&](int32_t s, uint32_t sxy, int) { take(s, sxy); });
+            }
+        };
+        auto covers = [&](int Rs) {
+            return px - Rs <= box[0] && px + Rs >= box[2] && py - Rs <= box[1] && py + Rs >= box[3];
+        };
+        // coordinates of the walk's start (q0) and of the last neighbour
+        // found, so a step need not load its edge's far end again
+        int c0 = hn, c1 = -1;
+        uint32_t x0c = hn >= 0 ? D.pxy[hn] : 0u, x1c = 0u;
+        auto nearest = [&]() -> int {
+            unsigned long long best = ~0ull;
+            uint32_t nxy = 0;
+            auto take = [&](int32_t s, uint32_t sxy) {
+                if (s == p) return;
+                const int32_t dx = dx_p(sxy, pp), dy = dy_p(sxy, pp);
+                const unsigned long long key = uint64_t(uint32_t(dx * dx + dy * dy)) << 32 | uint32_t(s);
+                if (key < best) {
+                    best = key;
+                    nxy = sxy;
+                }
+            };
+            auto take3 = [&](int32_t s, uint32_t sxy, int) { take(s, sxy); };
+            auto finish = [&]() {
+                const unsigned long long g = warp_min_u64(best);
+                const int wl = __ffs(__ballot_sync(0xffffffffu, best == g)) - 1;
+                nxy = __shfl_sync(0xffffffffu, nxy, wl < 0 ? 0 : wl);
+                best = g;
+            };
+            window(take);
+            finish();
+            int Rs = R0;
+            while (best == ~0ull) {
+                if (covers(Rs)) return -1;
+                Rs = star_square(Rs);
+                ++squares;
+                star_stream(D, row_off, star_square_region(pp, Rs, box), box, lane, take3);
+                finish();
+            }
+            // the nearest lies within distance sqrt(d2): proven if the square
+            // searched holds that disc, else the square of that half-size
+            const uint64_t d2 = best >> 32;
+            if (d2 > uint64_t(Rs) * uint64_t(Rs)) {
+                int d = int(sqrt(double(d2)));
+                while (uint64_t(d) * uint64_t(d) < d2) ++d;
+                ++circles;
+                best = ~0ull;
+                star_stream(D, row_off, star_square_region(pp, d, box), box, lane, take3);
+                finish();
+            }
+            c0 = int(uint32_t(best));
+            x0c = nxy;
+            return c0;
+        };
+        auto next = [&](int q, int side) -> int {
+            const uint32_t pq = q == c1 ? x1c : (q == c0 ? x0c : D.pxy[q]);
+            const int32_t ux = dx_p(pq, pp), uy = dy_p(pq, pp);
+            int bi = -1;
+            uint32_t bxy = 0;
+            float bk = 0.0f;
+            // b replaces a (keys ka, kb) under the star order: decided by the
+            // keys when they differ by more than their rounding can explain,
+            // else exactly (star_better)
+            auto wins = [&](float ka, int a, uint32_t axy, float kb, int b, uint32_t bxy2) {
+                const float m = 4e-6f * fmaxf(fabsf(ka), fabsf(kb));
+                if (kb < ka - m) return true;
+                if (kb > ka + m) return false;
+                return star_better(p, pp, q, pq, a, axy, b, bxy2, side);
+            };
+            auto take = [&](int32_t s, uint32_t sxy) {
+                float k;
+                if (!star_key(ux, uy, dx_p(sxy, pp), dy_p(sxy, pp), side, &k)) return;
+                if (bi < 0 || wins(bk, bi, bxy, k, s, sxy)) {
+                    bi = s;
+                    bxy = sxy;
+                    bk = k;
+                }
+            };
+            auto take3 = [&](int32_t s, uint32_t sxy, int) { take(s, sxy); };
+            // Minimum under the star order over the lanes' bests.  Fast path:
+            // the smallest key (one reduction over order-preserving key
+            // bits), final unless another lane's best lies within the keys'
+            // rounding of it; then a butterfly decides exactly (the order is
+            // strict and total, so every lane ends with the same point).  A
+            // lane's other candidates need no look: each is worse than its
+            // lane's best, which the winner beats.
+            auto reduce = [&]() {
+                const uint32_t kb = __float_as_uint(bk);
+                const uint32_t u = bi < 0 ? 0xffffffffu : ((kb & 0x80000000u) ? ~kb : (kb | 0x80000000u));
+                const uint32_t umin = __reduce_min_sync(0xffffffffu, u);
+                if (umin == 0xffffffffu) return;            // no lane holds a candidate
+                const int wl = __ffs(__ballot_sync(0xffffffffu, u == umin)) - 1;
+                const int wi = __shfl_sync(0xffffffffu, bi, wl);
+                const uint32_t wxy = __shfl_sync(0xffffffffu, bxy, wl);
+                const float wk = __shfl_sync(0xffffffffu, bk, wl);
+                const bool tie = bi >= 0 && bi != wi && fabsf(bk - wk) <= 4e-6f * fmaxf(fabsf(bk), fabsf(wk));
+                if (__ballot_sync(0xffffffffu, tie) == 0u) {
+                    bi = wi;
+                    bxy = wxy;
+                    bk = wk;
+                    return;
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                    const uint32_t oxy = __shfl_xor_sync(0xffffffffu, bxy, o);
+                    const float ok = __shfl_xor_sync(0xffffffffu, bk, o);
+                    if (oi >= 0 && oi != bi && (bi < 0 || wins(bk, bi, bxy, ok, oi, oxy))) {
+                        bi = oi;
+                        bxy = oxy;
+                        bk = ok;
+                    }
+                }
+            };
+            window(take);
+            reduce();
+            for (int Rs = R0;;) {
+                if (bi >= 0) {
+                    int need = 0;
+                    if (circle_within(pp, pq, bxy, Rs, box, &need)) break;
+                    if (need <= 2 * Rs) {
+                        ++circles;
+                        star_stream(D, row_off, star_circle_region(pp, pq, bxy, box), box, lane, take3);
+                        reduce();
+                        break;
+                    }
+                }
+                if (covers(Rs)) break;
+                Rs = star_square(Rs);
+                ++squares;
+                star_stream(D, row_off, star_half_region(pp, pq, side, Rs, box), box, lane, take3);
+                reduce();
+            }
+            if (bi >= 0) {
+                c1 = bi;
+                x1c = bxy;
+            }
+            return bi;
+        };
+        int m = 0, k = 0;
+        bool closed = false;
+        const bool ok = star_walk(hn, hp, nearest, next, sm.ccw, sm.cw, STAR_NB, &m, &k, &closed);
+        __syncwarp();
+        int own = 0;
+        const int deg = m + k, nt = ok ? star_tris(deg, closed) : 0;
+        for (int b = 0; b < nt; b += 32) {
+            const int i = b + lane;
+            bool o = false;
+            if (i < nt) {
+                const int a = star_at(sm.ccw, m, sm.cw, k, i), c = star_at(sm.ccw, m, sm.cw, k, i + 1 == deg ? 0 : i + 1);
+                o = p < a && p < c;
+            }
+            own += __popc(__ballot_sync(0xffffffffu, o));
+        }
+        int32_t* dst = D.sown + size_t(p) * 2 * STAR_SLOT;
+        if (own > STAR_SLOT) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&D.ctr[11], own);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base + own > D.Tmax) {
+                if (lane == 0) set_err(err, ERRF_BOUNDS);
+                own = 0;
+            } else {
+                if (lane == 0) dst[0] = base;
+                dst = D.spool + 2 * size_t(base);
+            }
+        }
+        if (!ok && lane == 0) set_err(err, ERRF_BOUNDS);
+        int pos = 0;
+        for (int b = 0; b < nt && own > 0; b += 32) {
+            const int i = b + lane;
+            bool o = false;
+            int a = 0, c = 0;
+            if (i < nt) {
+                a = star_at(sm.ccw, m, sm.cw, k, i);
+                c = star_at(sm.ccw, m, sm.cw, k, i + 1 == deg ? 0 : i + 1);
+                o = p < a && p < c;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, o);
+            if (o) {
+                const int j = pos + __popc(bal & ((1u << lane) - 1u));
+                dst[2 * j] = a;
+                dst[2 * j + 1] = c;
+            }
+            pos += __popc(bal);
+        }
+        if (lane == 0) {
+            D.tcnt[p] = own;
+            if (circles) atomicAdd(&D.ctr[12], circles);
+            if (squares) atomicAdd(&D.ctr[13], squares);
+        }
+        __syncwarp();
+    }
+}
+
+// One 1024-thread block per problem: triangle offsets (exclusive prefix
+// sums of the owned counts, in point order) and the triangle count ctr[0].
+__global__ void __launch_bounds__(1024) k_star_scan(DelDev d0, DelDev d1, unsigned* err) {
+    grid_dep_wait();
+    __shared__ int ws[33];
+    const DelDev& D = blockIdx.x ? d1 : d0;
+    const int N = D.ctr[9];
+    const int per = (N + 1023) / 1024, i0 = imin(int(threadIdx.x) * per, N), i1 = imin(i0 + per, N);
+    int sum = 0;
+    for (int i = i0; i < i1; ++i) sum += D.tcnt[i];
+    int total = 0;
+    int run = block_scan(sum, ws, &total);
+    for (int i = i0; i < i1; ++i) {
+        D.toff[i] = run;
+        run += D.tcnt[i];
+    }
+    if (threadIdx.x == 0) {
+        const bool fits = total <= D.Tmax;
+        if (!fits) set_err(err, ERRF_TRI_COUNT);
+        D.ctr[0] = fits ? total : 0;
+    }
+}
+
+// One thread per (point, view): the point's owned triangles (p, a, b) at
+// its offset, so the list is in point order and the same on every run.
+__global__ void k_star_emit(DelDev d0, DelDev d1) {
+    grid_dep_wait();
+    const DelDev& D = blockIdx.y ? d1 : d0;
+    const int N = D.ctr[9];
+    if (D.ctr[0] == 0) return;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
+        const int c = D.tcnt[p];
+        if (c == 0) continue;
+        const int o = D.toff[p];
+        const int32_t* slot = D.sown + size_t(p) * 2 * STAR_SLOT;
+        const int32_t* src = c <= STAR_SLOT ? slot : D.spool + 2 * size_t(slot[0]);
+        int32_t* t = D.tri + 3 * size_t(o);
+        for (int j = 0; j < c; ++j) {
+            t[3 * j] = p;
+            t[3 * j + 1] = src[2 * j];
+            t[3 * j + 2] = src[2 * j + 1];
+        }
     }
 }
 
@@ -984,7 +1470,7 @@ __global__ void __launch_bounds__(CL_THREADS) k_flip_smem(DelDev d0, DelDev d1, 
 int cluster_size_for_flip() {
     int sizes[2] = {16, 8};
     size_t smem = CL_SMEM;
-    cudaFuncSetAttribute(k_flip_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    allow_smem(k_flip_smem);
     cudaFuncSetAttribute(k_flip_smem, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     for (int cs : sizes) {
         cudaLaunchConfig_t cfg = {};
@@ -1005,11 +1491,21 @@ int cluster_size_for_flip() {
     return 0;
 }
 
-cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int nmax, int num_sms,
-                            int csize, unsigned* err, cudaStream_t st, int* nlaunch, bool force_global,
-                            int round_limit) {
+cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int nmax, int H, int num_sms,
+                            int csize, unsigned* err, cudaStream_t st, int* nlaunch, bool flips,
+                            bool force_global, int round_limit) {
     launch_k(k_rowsort, dim3(nrows, 2), 512, 0, st, d0, d1, row_off, nrows, err);
-    launch_k(k_plan, 2, 1024, 0, st, d0, d1, row_off, nrows, err);
+    const size_t plan_smem = size_t(16) * nrows;
+    allow_smem(k_plan);
+    launch_k(k_plan, 2, 1024, plan_smem, st, d0, d1, row_off, nrows, H, err);
+    if (!flips) {
+        launch_k(k_star, dim3(imax(1, imin((nmax + STAR_WARPS - 1) / STAR_WARPS, 6 * num_sms)), 2), STAR_WARPS * 32,
+                 0, st, d0, d1, row_off, err);
+        launch_k(k_star_scan, 2, 1024, 0, st, d0, d1, err);
+        launch_k(k_star_emit, dim3(imax(1, imin((nmax + 255) / 256, 4 * num_sms)), 2), 256, 0, st, d0, d1);
+        if (nlaunch) *nlaunch += 5;
+        return cudaGetLastError();
+    }
     // the pocket walk's chain and stack (2 sides x (index, x, y, 4-int stack
     // records) = 56 bytes a row) in shared memory up to 32 KiB; every block
     // of k_strips carries it
@@ -1024,7 +1520,7 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
     int launched = 6;
     const int max_rounds = round_limit > 0 ? round_limit : 100000;
     if (!force_global) {
-        cudaFuncSetAttribute(k_flip_local, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LOC_SMEM));
+        allow_smem(k_flip_local);
         launch_k(k_flip_local, 2, 1024, LOC_SMEM, st, d0, d1, max_rounds, err);
         ++launched;
     }

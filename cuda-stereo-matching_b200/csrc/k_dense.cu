@@ -3,14 +3,19 @@
 // Prior: replaces kerComputeDepthApproximation
 // (src/Kernels/KerComputeDisparity.cu:9-152), one thread per triangle with
 // long serial scanline loops.  Here one thread per triangle solves the plane
-// (same double Gauss-Jordan as kerSolve, :321-375), sets up the edges and
-// finds the 64x32 prior tiles its pixels can fall in; the triangles are
-// binned by tile, and one CTA per tile paints it in shared memory and writes
-// it once.  A pixel covered by more than one triangle (rounding at shared
-// vertices) must keep the last triangle in list order, as a sequential
-// rasteriser would; the tile is therefore painted with a 32-bit atomicMax of
-// (triangle+1) << pshift | d_plane, which makes the result independent of
-// scheduling.  d_plane is stored clamped to
+// (same double Gauss-Jordan as kerSolve, :321-375) and sets up the edges.
+// Two ways to paint, chosen by image size (both give the same bytes):
+//   * direct: a warp per triangle, lanes over its columns, atomics straight
+//     into the zeroed prior (two launches after the memset; the faster one
+//     for small images);
+//   * tiled: the set-up also finds the 64x32 prior tiles a triangle's pixels
+//     can fall in, the triangles are binned by tile, and one CTA per tile
+//     paints it in shared memory and writes it once (no memset, no global
+//     atomics; the faster one from about a megapixel up).
+// A pixel covered by more than one triangle (rounding at shared vertices)
+// must keep the last triangle in list order, as a sequential rasteriser
+// would; both paint with a 32-bit atomicMax of (triangle+1) << pshift |
+// d_plane, which makes the result independent of scheduling.  d_plane is stored clamped to
 // [0, disp_max + plane_radius + 1] (0 standing for every d_plane <= 0): the
 // dense step treats all values beyond either end alike.
 //
@@ -145,9 +150,10 @@ __device__ void setup_triangle(const int32_t* tri, const int32_t* can, const int
     R.BC_b = __fmaf_rn(-R.BC_a, B_u, B_v);
 }
 
-// One thread per (view, triangle): plane and edge set-up, the prior tiles
-// its pixels can fall in (from the exact row range of the raster and its
-// column range), and one count per such tile.
+// One thread per (view, triangle): plane and edge set-up and, for the tiled
+// paint (tcnt non-null), the prior tiles its pixels can fall in (from the
+// exact row range of the raster and its column range) with one count per
+// such tile.
 __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__ tri0,
                                                      const int32_t* __restrict__ tri1,
                                                      const int32_t* __restrict__ ctr0,
@@ -162,6 +168,10 @@ __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__
         const int t = right ? i - T0 : i;
         Raster R;
         setup_triangle((right ? tri1 : tri0) + 3 * size_t(t), can, uvd, g.cw, g.step, right, R);
+        if (!tcnt) {
+            rast[(right ? Tmax : 0) + t] = R;
+            continue;
+        }
         int r0 = g.H, r1 = -1;
         part_rows(R, 0, g.W, g.H, r0, r1);
         part_rows(R, 1, g.W, g.H, r0, r1);
@@ -175,6 +185,43 @@ __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__
         int32_t* c = tcnt + (right ? ntiles + 1 : 0);
         for (int ty = R.ty0; ty <= R.ty1; ++ty)
             for (int tx = R.tx0; tx <= R.tx1; ++tx) atomicAdd(c + ty * ntx + tx, 1);
+    }
+}
+
+// Direct paint: one warp per (view, triangle), lanes over columns; every
+// pixel keeps the last covering triangle through atomicMax on the packed
+// value in the zeroed prior.
+__global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict__ ctr0,
+                                                      const int32_t* __restrict__ ctr1,
+                                                      const Raster* __restrict__ rast, int Tmax,
+                                                      uint32_t* prior0, uint32_t* prior1, Geom g, int pshift,
+                                                      int dcap) {
+    grid_dep_wait();
+    const int lane = threadIdx.x & 31;
+    const int T0 = ctr0[0], T1 = ctr1[0];
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < T0 + T1; i += nw) {
+        const bool right = i >= T0;
+        const int t = right ? i - T0 : i;
+        const Raster R = rast[(right ? Tmax : 0) + t];
+        const uint32_t tag = uint32_t(t + 1) << pshift;
+        uint32_t* prior = right ? prior1 : prior0;
+        for (int part = 0; part < 2; ++part) {
+            const int ua = part ? int(R.B_u) : int(R.A_u), ub = part ? int(R.C_u) : int(R.B_u);
+            if (ua == ub) continue;
+            const float ea = part ? R.BC_a : R.AB_a, eb = part ? R.BC_b : R.AB_b;
+            for (int u = imax(ua, 0) + lane; u < imin(ub, g.W); u += 32) {
+                const float fu = float(u);
+                const int v1 = raster_row(R.AC_a, R.AC_b, u), v2 = raster_row(ea, eb, u);
+                const int va = imax(imin(v1, v2), 0), vb = imin(imax(v1, v2), g.H);
+                for (int v = va; v < vb; ++v) {
+                    const float dp = __fadd_rn(__fmaf_rn(R.pa, fu, __fmul_rn(R.pb, float(v))), R.pc);
+                    int d = __float2int_rz(dp);
+                    d = d <= 0 ? 0 : (d > dcap ? dcap : d);
+                    atomicMax(&prior[size_t(v) * g.W + u], tag | uint32_t(d));
+                }
+            }
+        }
     }
 }
 
@@ -520,11 +567,22 @@ size_t prior_list_capacity(const Geom& g, int Tmax) {
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
                          int Tmax, const int32_t* can, const int32_t* uvd, void* rast, const PriorTiles& tl,
                          uint32_t* prior0, uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms,
-                         unsigned* err, cudaStream_t st, int* nlaunch) {
-    const int ntx = (g.W + PT_W - 1) / PT_W, nty = (g.H + PT_H - 1) / PT_H, ntiles = ntx * nty;
-    cudaMemsetAsync(tl.cnt, 0, size_t(2) * (ntiles + 1) * sizeof(int32_t), st);
+                         unsigned* err, cudaStream_t st, int* nlaunch, bool tiled) {
     Raster* R = static_cast<Raster*>(rast);
     const int tblocks = imax(1, imin(8 * num_sms, (2 * Tmax + 255) / 256));
+    if (!tiled) {
+        const size_t n = size_t(g.W) * g.H * sizeof(uint32_t);
+        cudaMemsetAsync(prior0, 0, n, st);
+        cudaMemsetAsync(prior1, 0, n, st);
+        launch_k(k_prior_setup, tblocks, 256, 0, st, tri0, tri1, ctr0, ctr1, can, uvd, R, Tmax, g,
+                 static_cast<int32_t*>(nullptr), 0, 0);
+        launch_k(k_prior_raster, imax(1, imin(16 * num_sms, (2 * Tmax + 7) / 8)), 256, 0, st, ctr0, ctr1, R, Tmax,
+                 prior0, prior1, g, pshift, dcap);
+        if (nlaunch) *nlaunch += 2;
+        return cudaGetLastError();
+    }
+    const int ntx = (g.W + PT_W - 1) / PT_W, nty = (g.H + PT_H - 1) / PT_H, ntiles = ntx * nty;
+    cudaMemsetAsync(tl.cnt, 0, size_t(2) * (ntiles + 1) * sizeof(int32_t), st);
     launch_k(k_prior_setup, tblocks, 256, 0, st, tri0, tri1, ctr0, ctr1, can, uvd, R, Tmax, g, tl.cnt, ntx, ntiles);
     launch_k(k_prior_scan, 2, 1024, 0, st, tl.cnt, tl.off, ntiles);
     launch_k(k_prior_fill, tblocks, 256, 0, st, ctr0, ctr1, R, Tmax, tl.cnt, tl.list, tl.cap, ntx, ntiles, err);
@@ -549,11 +607,11 @@ cudaError_t launch_dense(const uint4* desc0, const uint4* desc1, const uint32_t*
     threads = imin(threads, (((g.W >> sub) + 31) / 32) * 32);
     const dim3 grid(g.H >> sub, 2);
     if (p.plane_radius == 2) {
-        cudaFuncSetAttribute(k_dense<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        allow_smem(k_dense<2>);
         launch_k(k_dense<2>, grid, threads, smem, st, desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
                                                 pshift, sub, lcap, err);
     } else {
-        cudaFuncSetAttribute(k_dense<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        allow_smem(k_dense<0>);
         launch_k(k_dense<0>, grid, threads, smem, st, desc0, desc1, prior0, prior1, grid0, grid1, disp0, disp1, g, p,
                                                 pshift, sub, lcap, err);
     }

@@ -360,7 +360,8 @@ __device__ __forceinline__ void sort9(float (&a)[9]) {
 // Invalid pixels get a key far away from every valid one, which lands on
 // the table's last entry, weight 0: an invalid neighbour adds 0 to both
 // sums (bit for bit the same as skipping it).  The table has
-// 4 disp_max + 2 entries.
+// 4 disp_max + 2 entries.  The neighbour's value is read back from its key
+// (K / 4 is exact for these quarters), so the 5x5 window loads one array.
 constexpr int K_INVALID = 1 << 20;
 
 // spk_min > 0: the input is the L/R result before speckle removal, and
@@ -448,8 +449,9 @@ __global__ void __launch_bounds__(1024, 2) k_post_tile(PostViews pv, int W, int 
                 for (int dy = -2; dy <= 2; ++dy)
 #pragma unroll
                     for (int dx = -2; dx <= 2; ++dx) {
-                        const float dq = V[r + 2 + dy][c + 2 + dx];
-                        const int j = min(abs(K[r + 2 + dy][c + 2 + dx] - kp), wt_n - 1);
+                        const int kq = K[r + 2 + dy][c + 2 + dx];
+                        const float dq = __int2float_rn(kq) * 0.25f;
+                        const int j = min(abs(kq - kp), wt_n - 1);
                         const float w = WT[j];
                         num = __fmaf_rn(w, dq, num);
                         den = __fadd_rn(den, w);
@@ -541,7 +543,7 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         const size_t smem = adaptive_mean ? size_t(wt_n) * sizeof(float) : 0;
         const int key = (tile_gap ? 4 : 0) | (adaptive_mean ? 2 : 0) | (median ? 1 : 0);
         auto go = [&](auto kern) {
-            if (smem) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            if (smem) allow_smem(kern);
             launch_k(kern, grid, 1024, smem, st, pv, W, H, gap, spk, wt_n, nviews);
         };
         if (!tile_gap || gap <= 3) {   // halo 6

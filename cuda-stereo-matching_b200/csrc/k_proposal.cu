@@ -286,7 +286,7 @@ cudaError_t launch_bf16_to_f32(const __nv_bfloat16* in, float* out, size_t n, cu
 
 cudaError_t launch_conv_f32(const float* x, const float* mask, const float* w, const float* b, float* y, int nimg,
                             int Hd, int Wd, int relu, cudaStream_t st) {
-    cudaFuncSetAttribute(k_conv_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, int(CONV_F32_SMEM));
+    allow_smem(k_conv_f32);
     k_conv_f32<<<dim3((Wd + SEG - 1) / SEG, Hd, nimg), SEG * CH, CONV_F32_SMEM, st>>>(x, mask, w, b, y, Hd, Wd,
                                                                                        relu);
     return cudaGetLastError();

@@ -433,7 +433,7 @@ cudaError_t launch_infer(const InferWeights& iw, const __nv_bfloat16* in, __nv_b
     const __nv_bfloat16* src[LAYERS] = {in, act0, act1, act0};
     __nv_bfloat16* dst[LAYERS] = {act0, act1, act0, out};
     const int tiles = 2 * Hd * ((Wd + TILE_M - 1) / TILE_M);
-    cudaError_t e = cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TC_SMEM));
+    cudaError_t e = allow_smem(k_conv_tc);
     if (e != cudaSuccess) return e;
     // persistent CTAs: as many per SM as shared memory allows (each holds its
     // own 32-column accumulator), so one CTA's epilogue overlaps another's MMAs
@@ -460,7 +460,7 @@ cudaError_t launch_topk(const __nv_bfloat16* F, uint32_t* bins, int Hd, int Wd, 
     if (n <= 0) return cudaSuccess;
     const size_t smem = size_t(Wd) * CH * sizeof(__nv_bfloat16);
     if (smem <= 200 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_topk_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaError_t e = allow_smem(k_topk_rows);
         if (e != cudaSuccess) return e;
         launch_k(k_topk_rows, ch, 256, smem, st, F, bins, Hd, Wd, cw, step, D);
     } else {

@@ -932,8 +932,7 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
         int qseg = imax(1, (g.cw + qsegs - 1) / qsegs);
         qseg = (qseg + 3) & ~3;
         const int threads = imin(qseg, SWEEP_Q_THREADS / Q) * Q;
-        cudaFuncSetAttribute(k_support_sweep_q<Q, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(smem));
+        allow_smem(k_support_sweep_q<Q, true, false>);
         launch_k(k_support_sweep_q<Q, true, false>, dim3(qsegs, rows), threads, smem, st, desc0, desc1, can_lr, g, p,
                  qseg, err, nullptr, nullptr);
     } else if (bins && smem <= 200 * 1024) {
@@ -945,17 +944,16 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
         int qseg = imax(1, (g.cw + qsegs - 1) / qsegs);
         qseg = (qseg + 3) & ~3;
         const int threads = imin(qseg, SWEEP_Q_THREADS / Q) * Q;
-        cudaFuncSetAttribute(k_support_sweep_q<Q, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        allow_smem(k_support_sweep_q<Q, true, true>);
         launch_k(k_support_sweep_q<Q, true, true>, dim3(qsegs, rows), threads, smem, st, desc0, desc1, can_lr, g, p,
                  qseg, err, bins, stats);
     } else if (smem <= 200 * 1024) {
         if (bins) {
-            cudaFuncSetAttribute(k_support_sweep<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            allow_smem(k_support_sweep<true, true>);
             launch_k(k_support_sweep<true, true>, grid, SWEEP_THREADS, smem, st, desc0, desc1, can_lr, g, p, seg, err, bins,
                                                                            stats);
         } else {
-            cudaFuncSetAttribute(k_support_sweep<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(smem));
+            allow_smem(k_support_sweep<true, false>);
             launch_k(k_support_sweep<true, false>, grid, SWEEP_THREADS, smem, st, desc0, desc1, can_lr, g, p, seg, err,
                                                                             nullptr, nullptr);
         }
@@ -970,7 +968,7 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
     {
         const size_t sm = size_t(g.cw) * (sizeof(int) + 1);
         const int threads = imin(1024, imax(32, ((g.cw + 31) / 32) * 32));
-        cudaFuncSetAttribute(k_incon_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+        allow_smem(k_incon_rows);
         launch_k(k_incon_rows, g.ch, threads, sm, st, can_lr, can, g, p);
         const int wpb = 4;
         const size_t smv = size_t(wpb) * g.ch * (sizeof(int) + 1);

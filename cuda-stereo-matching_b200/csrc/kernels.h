@@ -29,7 +29,20 @@ struct DelDev {
     int32_t* ccand;        // cluster kernel: per-CTA proposals  [16 * 2 * 6 * 4096]
     int32_t* cflips;       // cluster kernel: per-CTA flips      [16 * 6 * 4096]
     int32_t* ctr;          // [16]: 0 triangles, 1 strip triangles, 4 flip rounds, 5 flips,
-                           //       6 non-empty rows, 8 handled by the cluster kernel
+                           //       6 non-empty rows, 8 handled by the cluster kernel, 9 points,
+                           //       11 star pool cursor, 12 star windows grown,
+                           //       13 star searches over every point
+    uint32_t* pxy;         // [Nmax] packed coordinates by point (PXY_NONE: dropped duplicate)
+    uint32_t* sxy;         // [Nmax] packed coordinates beside srt
+    int32_t* ne_y;         // [rows] y of each non-empty row
+    int32_t* tcnt;         // [Nmax] triangles owned by each point (star construction)
+    int32_t* toff;         // [Nmax] their offsets in tri
+    int32_t* sown;         // [24*Nmax] owned triangles' vertex pairs, per point
+    int32_t* spool;        // [2*Tmax] pairs of points owning more than the slot holds
+    int32_t* hnext;        // [Nmax] successor on the hull boundary (-1: interior point)
+    int32_t* hprev;        // [Nmax] predecessor on the hull boundary
+    int32_t* box;          // [8] x0, y0, x1, y1 of all points, [4] star window half-size
+    int32_t* ylut;         // [H+2] y -> first non-empty row at or below y
     unsigned long long* hkey;  // [Hmax]
     int32_t* hcnt;         // [Hmax]
     int32_t* hval;         // [2*Hmax]
@@ -54,11 +67,14 @@ cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_of
 cudaError_t launch_grid(const int32_t* can, uint32_t* tmp0, uint32_t* tmp1, uint32_t* grid0, uint32_t* grid1,
                         const Geom& g, cudaStream_t st, int* nlaunch);
 
-// force_global: flip every problem with the global-memory kernel (tests);
-// round_limit > 0 caps the flip rounds (ERRF_FLIP_LIMIT when hit).
-cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int nmax, int num_sms,
-                            int cluster_size, unsigned* err, cudaStream_t st, int* nlaunch, bool force_global = false,
-                            int round_limit = 0);
+// Default: every point's star found directly (k_star).  flips: row strips
+// and Lawson edge flips instead; then force_global flips every problem with
+// the global-memory kernel (tests) and round_limit > 0 caps the flip rounds
+// (ERRF_FLIP_LIMIT when hit).  Both give the same triangles (the unique
+// triangulation under the perturbation), in different list orders.
+cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int nrows, int nmax, int H, int num_sms,
+                            int cluster_size, unsigned* err, cudaStream_t st, int* nlaunch, bool flips = false,
+                            bool force_global = false, int round_limit = 0);
 // Largest cluster (16 or 8 CTAs) with two co-resident copies for the flip
 // kernel, or 0 if none fits.
 int cluster_size_for_flip();
@@ -77,10 +93,19 @@ size_t prior_list_capacity(const Geom& g, int Tmax);
 // d = d_plane clamped to [0, dcap] (dcap = disp_max + plane_radius + 1),
 // 0 where no triangle covers the pixel.  Every pixel is written.
 // rast: scratch of 2 * Tmax * raster_bytes() for the per-triangle set-up.
+// tiled: paint tile by tile in shared memory (tl used) instead of with
+// global atomics into the zeroed prior; the same bytes either way.
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
                          int Tmax, const int32_t* can, const int32_t* uvd, void* rast, const PriorTiles& tl,
                          uint32_t* prior0, uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms,
-                         unsigned* err, cudaStream_t st, int* nlaunch);
+                         unsigned* err, cudaStream_t st, int* nlaunch, bool tiled);
+// Images from this many pixels up take the tiled prior paint (measured:
+// the direct paint is faster at 1242x375, the tiled one at 2880x1988).
+constexpr long long PRIOR_TILED_MIN_PIXELS = 1LL << 20;
+// Images up to this many pixels take the star construction of the
+// Delaunay triangulations, larger ones the strips and flips (measured: the
+// stars are faster at 1242x375, the flips at 2880x1988).
+constexpr long long DELAUNAY_STARS_MAX_PIXELS = 1LL << 21;
 size_t raster_bytes();
 
 size_t dense_smem_bytes(const Geom& g);

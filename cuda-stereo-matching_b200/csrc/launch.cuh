@@ -39,4 +39,23 @@ inline cudaError_t launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_
     return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
+// Allow a kernel every dynamic shared memory size the device offers beside
+// its static shared memory.  The attribute belongs to the function, not to
+// a launch: host threads that launch one kernel with different sizes
+// (handles on one device) would undo each other's per-size setting, so it
+// is always set to the same maximum.
+template <class K>
+inline cudaError_t allow_smem(K kernel) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    int optin = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kernel);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - int(fa.sharedSizeBytes));
+    if (e != cudaSuccess) cudaGetLastError();     // reported by the return value, not left behind
+    return e;
+}
+
 }  // namespace elas

@@ -288,6 +288,10 @@ class Elas:
 
     TEST_FLIP_GLOBAL = 1      # every triangulation on the global-memory flip kernel
     TEST_DENSE_BITSET = 2     # every dense candidate list walked as a bitset
+    TEST_PRIOR_TILED = 4      # plane prior painted tile by tile at every size
+    TEST_PRIOR_DIRECT = 8     # plane prior painted with global atomics at every size
+    TEST_DELAUNAY_FLIPS = 16  # triangulations from row strips and edge flips at every size
+    TEST_DELAUNAY_STARS = 32  # triangulations found star by star at every size
 
     def set_test_mode(self, flags=0, flip_round_limit=0):
         """Force fallback paths (results unchanged) and/or cap the flip rounds

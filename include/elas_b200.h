@@ -168,19 +168,38 @@ int elas_b200_set_graphs(elas_handle* h, int enable);
 /* Fallback switches, for tests of paths that the usual inputs never reach.
  * No counterpart in the reference (its Delaunay runs on the CPU and its
  * dense kernel has one path, src/Kernels/KerComputeDisparity.cu:155-316).
- *   ELAS_TEST_FLIP_GLOBAL   every triangulation is flipped by the global-
+ *   ELAS_TEST_DELAUNAY_FLIPS the triangulations are built from row strips
+ *                           and repaired by edge flips (otherwise above
+ *                           2^21 pixels) instead of being found star by
+ *                           star (the same triangles, listed in another
+ *                           order);
+ *   ELAS_TEST_DELAUNAY_STARS the triangulations are found star by star
+ *                           (otherwise up to 2^21 pixels); not together
+ *                           with the flip switches or a round limit;
+ *   ELAS_TEST_FLIP_GLOBAL   (implies the flip construction) every
+ *                           triangulation is flipped by the global-
  *                           memory kernel, which otherwise runs only for
  *                           triangulations larger than a cluster holds;
  *   ELAS_TEST_DENSE_BITSET  every grid cell's candidates are walked as a
  *                           bitset, the path otherwise taken only by cells
- *                           with more candidates than the per-row list holds.
+ *                           with more candidates than the per-row list holds;
+ *   ELAS_TEST_PRIOR_TILED   the plane prior is painted tile by tile in shared
+ *                           memory (otherwise from 2^20 pixels up);
+ *   ELAS_TEST_PRIOR_DIRECT  the plane prior is painted with global atomics
+ *                           (otherwise below 2^20 pixels); not together with
+ *                           ELAS_TEST_PRIOR_TILED.
  * The results are the same as without the flags.  flip_round_limit > 0
- * caps the edge-flipping rounds (0 = the library's own bound); a
+ * (which implies the flip construction) caps the edge-flipping rounds
+ * (0 = the library's own bound); a
  * triangulation that needs more rounds makes the call return
  * ELAS_ERR_TIMEOUT with the device still usable.  Batches pass the settings
  * on to their workers. */
 #define ELAS_TEST_FLIP_GLOBAL   1
 #define ELAS_TEST_DENSE_BITSET  2
+#define ELAS_TEST_PRIOR_TILED   4
+#define ELAS_TEST_PRIOR_DIRECT  8
+#define ELAS_TEST_DELAUNAY_FLIPS 16
+#define ELAS_TEST_DELAUNAY_STARS 32
 int elas_b200_set_test_mode(elas_handle* h, int32_t flags, int32_t flip_round_limit);
 
 /* Per-pair latency (ms from the batch's start to the pair's completion) of

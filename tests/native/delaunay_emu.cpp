@@ -4,6 +4,7 @@
 // same __host__ __device__ functions (delaunay_core.h), so the algorithm can
 // be checked on the CPU against the exact checker and Triangle.
 #include <algorithm>
+#include <cstdlib>
 #include <cstdint>
 #include <cstring>
 #include <unordered_map>
@@ -233,6 +234,191 @@ extern "C" int emu_delaunay(const int32_t* px, const int32_t* py, int n, const i
 extern "C" int emu_delaunay_phased(const int32_t* px, const int32_t* py, int n, const int32_t* row_off, int nrows,
                                    int32_t* tris_out, int cap, long long* stats) {
     return emu_core(px, py, n, row_off, nrows, tris_out, cap, stats, 1);
+}
+
+// Star construction (k_hull, k_star, k_star_scan, k_star_emit),
+// sequentially: the same rows, hull boundary, windows, walk and owner rule,
+// one point after another, each search a plain loop under the star order.  Triangles come out in point
+// order, as on the device.  stats (nullable): [0] phase-2 searches, [1]
+// squares grown, [2] candidates examined outside the staged windows.
+// Returns the triangle count, or -1.
+extern "C" int emu_delaunay_star(const int32_t* px, const int32_t* py, int n, const int32_t* row_off, int nrows,
+                                 int32_t* tris_out, int cap, long long* stats) {
+    // rows sorted by (x, index), repeated x dropped (k_rowsort)
+    std::vector<int32_t> srt(std::max(n, 1)), rcnt(nrows, 0);
+    std::vector<uint32_t> pxy(std::max(n, 1), PXY_NONE), sxy(std::max(n, 1), 0);
+    for (int r = 0; r < nrows; ++r) {
+        std::vector<int32_t> v;
+        for (int i = row_off[r]; i < row_off[r + 1]; ++i) v.push_back(i);
+        std::sort(v.begin(), v.end(), [&](int a, int b) { return px[a] != px[b] ? px[a] < px[b] : a < b; });
+        int m = 0;
+        for (size_t k = 0; k < v.size(); ++k)
+            if (k == 0 || px[v[k]] != px[v[k - 1]]) {
+                srt[row_off[r] + m] = v[k];
+                sxy[row_off[r] + m] = pxy[v[k]] = pack_xy(px[v[k]], py[v[k]]);
+                ++m;
+            }
+        rcnt[r] = m;
+    }
+    std::vector<int> ne;
+    for (int r = 0; r < nrows; ++r)
+        if (rcnt[r] > 0) ne.push_back(r);
+    // hull boundary and the box of all points (k_hull)
+    std::vector<int32_t> hnext(std::max(n, 1), -1), hprev(std::max(n, 1), -1);
+    int32_t box[4] = {0, 0, 0, 0};
+    const int R = int(ne.size());
+    if (R >= 1) {
+        box[0] = px[srt[row_off[ne[0]]]];
+        box[2] = px[srt[row_off[ne[0]] + rcnt[ne[0]] - 1]];
+        for (int s2 = 0; s2 < R; ++s2) {
+            box[0] = std::min(box[0], px[srt[row_off[ne[s2]]]]);
+            box[2] = std::max(box[2], px[srt[row_off[ne[s2]] + rcnt[ne[s2]] - 1]]);
+        }
+        box[1] = py[row_off[ne[0]]];
+        box[3] = py[row_off[ne[R - 1]]];
+    }
+    if (R >= 2) {
+        std::vector<int32_t> lst(R), rst(R);
+        int nl = 0, nr = 0;
+        auto first = [&](int s2) { return srt[row_off[ne[s2]]]; };
+        auto last = [&](int s2) { return srt[row_off[ne[s2]] + rcnt[ne[s2]] - 1]; };
+        std::vector<uint32_t> xyf(R), xyl(R);
+        for (int s2 = 0; s2 < R; ++s2) {
+            xyf[s2] = pxy[first(s2)];
+            xyl[s2] = pxy[last(s2)];
+        }
+        hull_chain(0, R, xyf.data(), lst.data(), &nl);
+        hull_chain(1, R, xyl.data(), rst.data(), &nr);
+        const int tl = rcnt[ne[0]], bl = rcnt[ne[R - 1]];
+        const int C = hull_cycle_len(tl, bl, nl, nr);
+        auto at = [&](int j) {
+            int row, pos;
+            bool lastp;
+            hull_cycle_at(j, R, tl, bl, lst.data(), nl, rst.data(), nr, &row, &pos, &lastp);
+            return lastp ? last(row) : srt[row_off[ne[row]] + pos];
+        };
+        for (int j = 0; j < C; ++j) {
+            hnext[at(j)] = at(j + 1 == C ? 0 : j + 1);
+            hprev[at(j)] = at(j == 0 ? C - 1 : j - 1);
+        }
+    }
+    long long circles = 0, squares = 0, evals = 0;
+    const int R0 = star_r0(box, n);
+    std::vector<int32_t> tri, ccw(STAR_NB), cw(STAR_NB);
+    std::vector<std::pair<int32_t, uint32_t>> win;
+    // every point of a region, row by row (the device splits them over lanes)
+    auto each_in = [&](const StarRegion& g, auto&& take) {
+        for (int r : ne) {
+            const int32_t y = py[row_off[r]];
+            if (y < g.y0 || y > g.y1) continue;
+            int32_t x0, x1;
+            g.cols(y, box, &x0, &x1);
+            for (int j = row_off[r]; j < row_off[r] + rcnt[r]; ++j) {
+                const int32_t x = px_of(sxy[j]);
+                if (x >= x0 && x <= x1) {
+                    ++evals;
+                    take(srt[j], sxy[j]);
+                }
+            }
+        }
+    };
+    for (int p = 0; p < n; ++p) {
+        const uint32_t pp = pxy[p];
+        if (pp == PXY_NONE) continue;
+        const int32_t x0 = px_of(pp), y0 = py_of(pp);
+        auto covers = [&](int Rs) {
+            return x0 - Rs <= box[0] && x0 + Rs >= box[2] && y0 - Rs <= box[1] && y0 + Rs >= box[3];
+        };
+        win.clear();
+        each_in(star_square_region(pp, R0, box), [&](int32_t s2, uint32_t sx) { win.push_back({s2, sx}); });
+        auto nearest = [&]() -> int {
+            unsigned long long best = ~0ull;
+            auto take = [&](int s2, uint32_t sx) {
+                if (s2 == p) return;
+                const int32_t dx = dx_p(sx, pp), dy = dy_p(sx, pp);
+                best = std::min<unsigned long long>(best, uint64_t(uint32_t(dx * dx + dy * dy)) << 32 | uint32_t(s2));
+            };
+            for (auto& c : win) take(c.first, c.second);
+            int Rs = R0;
+            while (best == ~0ull) {
+                if (covers(Rs)) return -1;
+                Rs = star_square(Rs);
+                ++squares;
+                each_in(star_square_region(pp, Rs, box), take);
+            }
+            // the nearest lies within distance sqrt(d2): proven if the square
+            // searched holds that disc, else the square of that half-size
+            const uint64_t d2 = best >> 32;
+            if (d2 <= uint64_t(Rs) * uint64_t(Rs)) return int(uint32_t(best));
+            int d = int(std::sqrt(double(d2)));
+            while (uint64_t(d) * uint64_t(d) < d2) ++d;
+            ++circles;
+            best = ~0ull;
+            each_in(star_square_region(pp, d, box), take);
+            return int(uint32_t(best));
+        };
+        auto next = [&](int q, int side) -> int {
+            const uint32_t pq = pxy[q];
+            int bi = -1;
+            uint32_t bxy = 0;
+            auto take = [&](int s2, uint32_t sx) {
+                if (!star_side(pp, pq, sx, side)) return;
+                if (bi < 0 || star_better(p, pp, q, pq, bi, bxy, s2, sx, side)) {
+                    bi = s2;
+                    bxy = sx;
+                }
+            };
+            for (auto& c : win) take(c.first, c.second);
+            for (int Rs = R0;;) {
+                if (bi >= 0) {
+                    int need = 0;
+                    if (circle_within(pp, pq, bxy, Rs, box, &need)) return bi;
+                    if (need <= 2 * Rs) {
+                        ++circles;
+                        each_in(star_circle_region(pp, pq, bxy, box), take);
+                        return bi;
+                    }
+                }
+                if (covers(Rs)) return bi;
+                Rs = star_square(Rs);
+                ++squares;
+                each_in(star_half_region(pp, pq, side, Rs, box), take);
+            }
+        };
+        int m = 0, k = 0;
+        bool closed = false;
+        if (!star_walk(hnext[p], hprev[p], nearest, next, ccw.data(), cw.data(), STAR_NB, &m, &k, &closed))
+            return -1;
+        const int deg = m + k, nt = star_tris(deg, closed);
+        for (int i = 0; i < nt; ++i) {
+            const int a = star_at(ccw.data(), m, cw.data(), k, i);
+            const int b = star_at(ccw.data(), m, cw.data(), k, i + 1 == deg ? 0 : i + 1);
+            if (p < a && p < b) {
+                tri.push_back(p);
+                tri.push_back(a);
+                tri.push_back(b);
+            }
+        }
+    }
+    const int T = int(tri.size() / 3);
+    if (T <= cap) std::memcpy(tris_out, tri.data(), sizeof(int32_t) * tri.size());
+    if (stats) { stats[0] = circles; stats[1] = squares; stats[2] = evals; }
+    return T;
+}
+
+// hull_chain (the stack walk) and hull_on_chain (the per-point test of the
+// device) on one chain: returns 1 if they keep the same points.
+extern "C" int emu_hull_agree(const int32_t* xs, const int32_t* ys, int R, int side) {
+    std::vector<uint32_t> xy(std::max(R, 1));
+    for (int i = 0; i < R; ++i) xy[i] = pack_xy(xs[i], ys[i]);
+    std::vector<int32_t> st(std::max(R, 1));
+    int n = 0;
+    hull_chain(side, R, xy.data(), st.data(), &n);
+    std::vector<char> keep(std::max(R, 1), 0);
+    for (int j = 0; j < n; ++j) keep[st[j]] = 1;
+    for (int i = 0; i < R; ++i)
+        if (bool(keep[i]) != hull_on_chain(side, R, xy.data(), i)) return 0;
+    return 1;
 }
 
 // The flip predicates on packed coordinates, for checks against exact

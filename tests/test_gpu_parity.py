@@ -343,17 +343,49 @@ def test_add_corners_parity(elas, preset, seed, D):
 
 
 @pytest.mark.parametrize("preset", [1, 2])
+def test_stars_match_host_emulation(elas, emu_lib, preset):
+    """The star kernels (forced at 2880x1988, which takes the flips by
+    default) give, list order included, the triangles of the sequential
+    host emulation of the star construction: each search is a
+    minimum under a strict total order, so how the lanes split the
+    candidates cannot change it, and the list is in point order."""
+    from test_delaunay_cpu import emu_star
+
+    W, H, D = eb.synth_dims(preset)
+    L, R, _, _ = eb.synth_pair(preset, 1)
+    elas.set_params(eb.params_config(D))
+    elas.set_test_mode(eb.Elas.TEST_DELAUNAY_STARS)
+    try:
+        elas.process(L, R)
+    finally:
+        elas.set_test_mode(0)
+    uvd = elas.stage("support").view(np.int32).reshape(-1, 3)
+    ctr = elas.stage("del_counters").view(np.int32).reshape(2, 16)
+    for right, key in ((0, "tri_left"), (1, "tri_right")):
+        xy = oracle.support_points(uvd, right)
+        tris, st = emu_star(emu_lib, xy, uvd[:, 1] // 5)
+        got = elas.stage(key).view(np.int32).reshape(-1, 3)
+        assert ctr[right, 0] == tris.shape[0]
+        assert np.array_equal(got, tris), key
+        assert (ctr[right, 12], ctr[right, 13]) == (st[0], st[1]), (right, ctr[right], st)
+
+
+@pytest.mark.parametrize("preset", [1, 2])
 def test_flip_rounds_match_host_emulation(elas, emu_lib, preset):
-    """The flip kernels (one SM at 1242x375, a cluster at 2880x1988) take the
-    same rounds and flips as the sequential host emulation of the algorithm:
-    each round's outcome is fixed by the edge priorities, whatever the order
-    in which threads reach the lists."""
+    """The flip construction (forced): the flip kernels (one SM at 1242x375,
+    a cluster at 2880x1988) take the same rounds and flips as the sequential
+    host emulation of the algorithm: each round's outcome is fixed by the
+    edge priorities, whatever the order in which threads reach the lists."""
     from test_delaunay_cpu import emu_triangulate
 
     W, H, D = eb.synth_dims(preset)
     L, R, _, _ = eb.synth_pair(preset, 1)
     elas.set_params(eb.params_config(D))
-    elas.process(L, R)
+    elas.set_test_mode(eb.Elas.TEST_DELAUNAY_FLIPS)
+    try:
+        elas.process(L, R)
+    finally:
+        elas.set_test_mode(0)
     uvd = elas.stage("support").view(np.int32).reshape(-1, 3)
     ctr = elas.stage("del_counters").view(np.int32).reshape(2, 16)
     for right, key in ((0, "tri_left"), (1, "tri_right")):

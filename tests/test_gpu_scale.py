@@ -9,7 +9,8 @@
   (whose workers allocate and zero their workspaces) bit-equal as well.
 * Fallbacks the usual inputs never reach, forced through
   elas_b200_set_test_mode: the global-memory flip kernel, the dense bitset
-  walk, and the flip round limit returning ELAS_ERR_TIMEOUT.
+  walk, each size's other prior paint path, and the flip round limit
+  returning ELAS_ERR_TIMEOUT.
 """
 import numpy as np
 import pytest
@@ -40,6 +41,24 @@ def test_stagewise_parity_config2(elas, seed):
     assert (ctr[:, 0] > 4096).all(), "the large case must exceed the one-SM flip kernel"
     valid = D1 >= 0
     assert valid.mean() > 0.5
+
+
+def test_stagewise_parity_config2_star_construction(elas):
+    """2880x1988, D 0-511, with the triangulations found star by star (the
+    size takes the strips and flips by default): every stage against the
+    oracle, the same triangle sets as the flip construction."""
+    L, R, gt, _ = eb.synth_pair(2, 3)
+    p = eb.params_config(511)
+    elas.set_params(p)
+    elas.process(L, R)
+    flips = [elas.stage(k).view(np.int32).reshape(-1, 3).copy() for k in ("tri_left", "tri_right")]
+    elas.set_test_mode(eb.Elas.TEST_DELAUNAY_STARS)
+    try:
+        D1, D2, g = run_and_compare(elas, L, R, p, check_triangle=False)
+    finally:
+        elas.set_test_mode(0)
+    for key, ref in zip(("tri_left", "tri_right"), flips):
+        assert {tuple(t) for t in ref.tolist()} == {tuple(t) for t in g[key].tolist()}, key
 
 
 def _batch_pairs(shapes, seed0):
@@ -171,6 +190,26 @@ def test_forced_dense_bitset_walk(elas, preset, seed):
         elas.set_test_mode(0)
     assert np.array_equal(g["disp_left"].reshape(-1), ref[0])
     assert np.array_equal(g["disp_right"].reshape(-1), ref[1])
+
+
+@pytest.mark.parametrize("preset,seed,flag", [(1, 61, "TEST_PRIOR_TILED"), (2, 62, "TEST_PRIOR_DIRECT")])
+def test_forced_prior_paint(elas, preset, seed, flag):
+    """The plane prior through the paint path the image size does not pick
+    (tile by tile at 1242x375, global atomics at 2880x1988): every stage
+    bit-exact against the oracle, and the prior equal to the default path's."""
+    W, H, D = eb.synth_dims(preset)
+    L, R, _, _ = eb.synth_pair(preset, seed)
+    p = eb.params_config(D)
+    elas.set_params(p)
+    elas.process(L, R)
+    ref = [elas.stage(k).copy() for k in ("prior_left", "prior_right")]
+    elas.set_test_mode(getattr(eb.Elas, flag))
+    try:
+        run_and_compare(elas, L, R, p, check_triangle=False)
+        got = [elas.stage(k) for k in ("prior_left", "prior_right")]
+    finally:
+        elas.set_test_mode(0)
+    assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
 
 
 def test_flip_round_limit_returns_timeout(elas):
