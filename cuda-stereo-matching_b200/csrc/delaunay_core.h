@@ -438,6 +438,22 @@ struct StarRegion {
     // the points strictly on side `side` of the line through (hx, hy) with
     // direction (ux, uy) count, kept with a pixel of margin
     int32_t hx, hy, ux, uy, side;
+    // optional hole (a ring, the square minus a smaller one): rows
+    // [ky0, ky1] lose the columns [kx0, kx1]
+    int32_t kx0, kx1, ky0, ky1;
+    bool hole;
+    // The columns of row y as up to two ranges [x0, x1], [x2, x3] (empty
+    // when the first bound exceeds the second).
+    HD void cols2(int32_t y, const int32_t* box, int32_t* x0, int32_t* x1, int32_t* x2, int32_t* x3) const {
+        cols(y, box, x0, x1);
+        *x2 = 1;
+        *x3 = 0;
+        if (hole && y >= ky0 && y <= ky1) {
+            *x2 = imax(*x0, kx1 + 1);
+            *x3 = *x1;
+            *x1 = imin(*x1, kx0 - 1);
+        }
+    }
     HD void cols(int32_t y, const int32_t* box, int32_t* x0, int32_t* x1) const {
         if (!circle) {
             *x0 = sx0;
@@ -471,11 +487,25 @@ HD StarRegion star_square_region(uint32_t pp, int R, const int32_t* box) {
     g.circle = false;
     g.cx = g.cy = g.rho2 = 0.0;
     g.hx = g.hy = g.ux = g.uy = g.side = 0;
+    g.kx0 = g.kx1 = g.ky0 = g.ky1 = 0;
+    g.hole = false;
     const int32_t px = px_of(pp), py = py_of(pp);
     g.sx0 = imax(px - R, box[0]);
     g.sx1 = imin(px + R, box[2]);
     g.y0 = imax(py - R, box[1]);
     g.y1 = imin(py + R, box[3]);
+    return g;
+}
+
+// The ring between the squares of half-sizes R and 2R around p.
+HD StarRegion star_ring_region(uint32_t pp, int R, const int32_t* box) {
+    StarRegion g = star_square_region(pp, 2 * R, box);
+    const int32_t px = px_of(pp), py = py_of(pp);
+    g.hole = true;
+    g.kx0 = px - R;
+    g.kx1 = px + R;
+    g.ky0 = py - R;
+    g.ky1 = py + R;
     return g;
 }
 
@@ -499,6 +529,8 @@ HD StarRegion star_circle_region(uint32_t pp, uint32_t pq, uint32_t pr, const in
     StarRegion g;
     g.circle = true;
     g.hx = g.hy = g.ux = g.uy = g.side = 0;
+    g.kx0 = g.kx1 = g.ky0 = g.ky1 = 0;
+    g.hole = false;
     g.cx = cx + px_of(pp);
     g.cy = cy + py_of(pp);
     g.rho2 = cx * cx + cy * cy;

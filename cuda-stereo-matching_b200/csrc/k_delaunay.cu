@@ -373,9 +373,10 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
 
 // Every point of a region, spread evenly over the warp's lanes: each lane
 // takes a row (ylut gives the rows of the region's y range), finds the
-// row's column range by binary search in the row's sorted coordinates, and
-// the ranges of 32 rows are then dealt out one point per lane (a lane finds
-// the row of its point by a binary search over the lanes' offsets).
+// row's column ranges (one, or two beside a ring's hole) by binary search
+// in the row's sorted coordinates, and the ranges of 32 rows are then dealt
+// out one point per lane (a lane finds the row of its point by a binary
+// search over the lanes' offsets).
 // take(index, packed xy, k) receives each point with its running number k.
 template <class Take>
 __device__ void star_stream(const DelDev& D, const int32_t* __restrict__ row_off, const StarRegion& g,
@@ -383,33 +384,45 @@ __device__ void star_stream(const DelDev& D, const int32_t* __restrict__ row_off
     if (g.y0 > g.y1) return;
     const int s0 = D.ylut[g.y0], s1 = D.ylut[g.y1 + 1];
     int done = 0;
+    // positions [lo, hi) of the row's sorted points with x in [x0, x1]
+    auto range = [&](const uint32_t* xs, int cnt, int32_t x0, int32_t x1, int* b, int* n) {
+        int l = 0, h = cnt;
+        while (l < h) {
+            const int mid = (l + h) >> 1;
+            if (px_of(xs[mid]) < x0) l = mid + 1;
+            else h = mid;
+        }
+        const int lb = l;
+        h = cnt;
+        while (l < h) {
+            const int mid = (l + h) >> 1;
+            if (px_of(xs[mid]) <= x1) l = mid + 1;
+            else h = mid;
+        }
+        *b = lb;
+        *n = l - lb;
+    };
     for (int sb = s0; sb < s1; sb += 32) {
         const int srow = sb + lane;
-        int b = 0, n = 0;
+        int b = 0, n0 = 0, b1 = 0, n1 = 0;
         if (srow < s1) {
-            int32_t x0, x1;
-            g.cols(D.ne_y[srow], box, &x0, &x1);
-            if (x0 <= x1) {
+            int32_t x0, x1, x2, x3;
+            g.cols2(D.ne_y[srow], box, &x0, &x1, &x2, &x3);
+            if (x0 <= x1 || x2 <= x3) {
                 const int r = D.ne[srow];
                 const int base = row_off[r], cnt = D.rcnt[r];
                 const uint32_t* xs = D.sxy + base;
-                int l = 0, h = cnt;
-                while (l < h) {
-                    const int mid = (l + h) >> 1;
-                    if (px_of(xs[mid]) < x0) l = mid + 1;
-                    else h = mid;
+                if (x0 <= x1) {
+                    range(xs, cnt, x0, x1, &b, &n0);
+                    b += base;
                 }
-                const int lb = l;
-                h = cnt;
-                while (l < h) {
-                    const int mid = (l + h) >> 1;
-                    if (px_of(xs[mid]) <= x1) l = mid + 1;
-                    else h = mid;
+                if (x2 <= x3) {
+                    range(xs, cnt, x2, x3, &b1, &n1);
+                    b1 += base;
                 }
-                b = base + lb;
-                n = l - lb;
             }
         }
+        const int n = n0 + n1;
         int incl = n;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -427,8 +440,10 @@ __device__ void star_stream(const DelDev& D, const int32_t* __restrict__ row_off
                 if (c < 32 && e <= k) j = c;
             }
             const int jb = __shfl_sync(0xffffffffu, b, j), je = __shfl_sync(0xffffffffu, excl, j);
+            const int jn0 = __shfl_sync(0xffffffffu, n0, j), jb1 = __shfl_sync(0xffffffffu, b1, j);
             if (k < tot) {
-                const int pos = jb + k - je;
+                const int o = k - je;
+                const int pos = o < jn0 ? jb + o : jb1 + (o - jn0);
                 take(D.srt[pos], D.sxy[pos], done + k);
             }
         }
@@ -472,6 +487,31 @@ __global__ void __launch_bounds__(STAR_WARPS * 32, 4) k_star(DelDev d0, DelDev d
         K = __reduce_max_sync(0xffffffffu, K);
         __syncwarp();
         const bool staged = K <= STAR_CAP;
+        // the window grows (and stays grown for the point's later searches)
+        // while its rings fit behind the staged points
+        int Rw = R0;
+        bool ring_full = !staged;
+        auto grow = [&](auto&& take) {
+            ++squares;
+            int T = 0;
+            star_stream(D, row_off, star_ring_region(pp, Rw, box), box, lane, [&](int32_t s, uint32_t sxy, int k) {
+                take(s, sxy);
+                if (K + k < STAR_CAP) {
+                    sm.cid[K + k] = s;
+                    sm.cxy[K + k] = sxy;
+                }
+                T = k + 1;
+            });
+            T = __reduce_max_sync(0xffffffffu, T);
+            __syncwarp();
+            if (K + T > STAR_CAP) {
+                ring_full = true;
+                return false;
+            }
+            K += T;
+            Rw *= 2;
+            return true;
+        };
         auto window = [&](auto&& take) {
             if (staged) {
                 for (int k = lane; k < K; k += 32) take(sm.cid[k], sm.cxy[k]);
@@ -507,25 +547,31 @@ __global__ void __launch_bounds__(STAR_WARPS * 32, 4) k_star(DelDev d0, DelDev d
             };
             window(take);
             finish();
-            int Rs = R0;
-            while (best == ~0ull) {
-                if (covers(Rs)) return -1;
+            for (int Rs = Rw;;) {
+                const uint64_t d2 = best >> 32;
+                if (best != ~0ull && d2 <= uint64_t(Rs) * uint64_t(Rs)) break;
+                if (covers(Rs)) break;
+                if (Rs == Rw && !ring_full) {
+                    Rs = grow(take) ? Rw : 2 * Rs;
+                    finish();
+                    continue;
+                }
+                if (best != ~0ull) {
+                    // the nearest lies within distance sqrt(d2): the square of that half-size
+                    int d = int(sqrt(double(d2)));
+                    while (uint64_t(d) * uint64_t(d) < d2) ++d;
+                    ++circles;
+                    best = ~0ull;
+                    star_stream(D, row_off, star_square_region(pp, d, box), box, lane, take3);
+                    finish();
+                    break;
+                }
                 Rs = star_square(Rs);
                 ++squares;
                 star_stream(D, row_off, star_square_region(pp, Rs, box), box, lane, take3);
                 finish();
             }
-            // the nearest lies within distance sqrt(d2): proven if the square
-            // searched holds that disc, else the square of that half-size
-            const uint64_t d2 = best >> 32;
-            if (d2 > uint64_t(Rs) * uint64_t(Rs)) {
-                int d = int(sqrt(double(d2)));
-                while (uint64_t(d) * uint64_t(d) < d2) ++d;
-                ++circles;
-                best = ~0ull;
-                star_stream(D, row_off, star_square_region(pp, d, box), box, lane, take3);
-                finish();
-            }
+            if (best == ~0ull) return -1;
             c0 = int(uint32_t(best));
             x0c = nxy;
             return c0;
@@ -592,18 +638,21 @@ __global__ void __launch_bounds__(STAR_WARPS * 32, 4) k_star(DelDev d0, DelDev d
             };
             window(take);
             reduce();
-            for (int Rs = R0;;) {
-                if (bi >= 0) {
-                    int need = 0;
-                    if (circle_within(pp, pq, bxy, Rs, box, &need)) break;
-                    if (need <= 2 * Rs) {
-                        ++circles;
-                        star_stream(D, row_off, star_circle_region(pp, pq, bxy, box), box, lane, take3);
-                        reduce();
-                        break;
-                    }
-                }
+            for (int Rs = Rw;;) {
+                int need = 0;
+                if (bi >= 0 && circle_within(pp, pq, bxy, Rs, box, &need)) break;
                 if (covers(Rs)) break;
+                if (Rs == Rw && !ring_full) {
+                    Rs = grow(take) ? Rw : 2 * Rs;
+                    reduce();
+                    continue;
+                }
+                if (bi >= 0 && need <= 2 * Rs) {
+                    ++circles;
+                    star_stream(D, row_off, star_circle_region(pp, pq, bxy, box), box, lane, take3);
+                    reduce();
+                    break;
+                }
                 Rs = star_square(Rs);
                 ++squares;
                 star_stream(D, row_off, star_half_region(pp, pq, side, Rs, box), box, lane, take3);

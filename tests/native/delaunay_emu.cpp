@@ -311,11 +311,11 @@ extern "C" int emu_delaunay_star(const int32_t* px, const int32_t* py, int n, co
         for (int r : ne) {
             const int32_t y = py[row_off[r]];
             if (y < g.y0 || y > g.y1) continue;
-            int32_t x0, x1;
-            g.cols(y, box, &x0, &x1);
+            int32_t x0, x1, x2, x3;
+            g.cols2(y, box, &x0, &x1, &x2, &x3);
             for (int j = row_off[r]; j < row_off[r] + rcnt[r]; ++j) {
                 const int32_t x = px_of(sxy[j]);
-                if (x >= x0 && x <= x1) {
+                if ((x >= x0 && x <= x1) || (x >= x2 && x <= x3)) {
                     ++evals;
                     take(srt[j], sxy[j]);
                 }
@@ -329,8 +329,30 @@ extern "C" int emu_delaunay_star(const int32_t* px, const int32_t* py, int n, co
         auto covers = [&](int Rs) {
             return x0 - Rs <= box[0] && x0 + Rs >= box[2] && y0 - Rs <= box[1] && y0 + Rs >= box[3];
         };
+        // the window: staged once, grown (persisting for the point's later
+        // searches) while its rings fit STAR_CAP
         win.clear();
         each_in(star_square_region(pp, R0, box), [&](int32_t s2, uint32_t sx) { win.push_back({s2, sx}); });
+        const bool staged = win.size() <= size_t(STAR_CAP);
+        int Rw = R0;
+        bool ring_full = !staged;
+        // one window growth, its ring's points given to take; false once
+        // the rings no longer fit (the ring was still searched)
+        auto grow = [&](auto&& take) {
+            ++squares;
+            const size_t K0 = win.size();
+            each_in(star_ring_region(pp, Rw, box), [&](int32_t s2, uint32_t sx) {
+                take(s2, sx);
+                win.push_back({s2, sx});
+            });
+            if (win.size() > size_t(STAR_CAP)) {
+                win.resize(K0);
+                ring_full = true;
+                return false;
+            }
+            Rw *= 2;
+            return true;
+        };
         auto nearest = [&]() -> int {
             unsigned long long best = ~0ull;
             auto take = [&](int s2, uint32_t sx) {
@@ -339,23 +361,28 @@ extern "C" int emu_delaunay_star(const int32_t* px, const int32_t* py, int n, co
                 best = std::min<unsigned long long>(best, uint64_t(uint32_t(dx * dx + dy * dy)) << 32 | uint32_t(s2));
             };
             for (auto& c : win) take(c.first, c.second);
-            int Rs = R0;
-            while (best == ~0ull) {
-                if (covers(Rs)) return -1;
+            for (int Rs = Rw;;) {
+                const uint64_t d2 = best >> 32;
+                if (best != ~0ull && d2 <= uint64_t(Rs) * uint64_t(Rs)) return int(uint32_t(best));
+                if (covers(Rs)) return best == ~0ull ? -1 : int(uint32_t(best));
+                if (Rs == Rw && !ring_full) {
+                    if (!grow(take)) Rs *= 2;
+                    else Rs = Rw;
+                    continue;
+                }
+                if (best != ~0ull) {
+                    // the nearest lies within distance sqrt(d2): the square of that half-size
+                    int d = int(std::sqrt(double(d2)));
+                    while (uint64_t(d) * uint64_t(d) < d2) ++d;
+                    ++circles;
+                    best = ~0ull;
+                    each_in(star_square_region(pp, d, box), take);
+                    return int(uint32_t(best));
+                }
                 Rs = star_square(Rs);
                 ++squares;
                 each_in(star_square_region(pp, Rs, box), take);
             }
-            // the nearest lies within distance sqrt(d2): proven if the square
-            // searched holds that disc, else the square of that half-size
-            const uint64_t d2 = best >> 32;
-            if (d2 <= uint64_t(Rs) * uint64_t(Rs)) return int(uint32_t(best));
-            int d = int(std::sqrt(double(d2)));
-            while (uint64_t(d) * uint64_t(d) < d2) ++d;
-            ++circles;
-            best = ~0ull;
-            each_in(star_square_region(pp, d, box), take);
-            return int(uint32_t(best));
         };
         auto next = [&](int q, int side) -> int {
             const uint32_t pq = pxy[q];
@@ -369,17 +396,20 @@ extern "C" int emu_delaunay_star(const int32_t* px, const int32_t* py, int n, co
                 }
             };
             for (auto& c : win) take(c.first, c.second);
-            for (int Rs = R0;;) {
-                if (bi >= 0) {
-                    int need = 0;
-                    if (circle_within(pp, pq, bxy, Rs, box, &need)) return bi;
-                    if (need <= 2 * Rs) {
-                        ++circles;
-                        each_in(star_circle_region(pp, pq, bxy, box), take);
-                        return bi;
-                    }
-                }
+            for (int Rs = Rw;;) {
+                int need = 0;
+                if (bi >= 0 && circle_within(pp, pq, bxy, Rs, box, &need)) return bi;
                 if (covers(Rs)) return bi;
+                if (Rs == Rw && !ring_full) {
+                    if (!grow(take)) Rs *= 2;
+                    else Rs = Rw;
+                    continue;
+                }
+                if (bi >= 0 && need <= 2 * Rs) {
+                    ++circles;
+                    each_in(star_circle_region(pp, pq, bxy, box), take);
+                    return bi;
+                }
                 Rs = star_square(Rs);
                 ++squares;
                 each_in(star_half_region(pp, pq, side, Rs, box), take);

@@ -155,7 +155,7 @@ def test_stars_across_empty_regions_and_rings(emu_lib):
     xy = np.array(sorted(set(pts), key=lambda q: (q[1], q[0])), np.int32)
     row_of = xy[:, 1] // 5
     _, st = emu_star(emu_lib, xy, row_of)
-    assert st[0] > 0 and st[1] > 0
+    assert st[1] > 0 and st[2] > 0      # windows grew and searched beyond the first square
     check_case(emu_lib, xy, row_of)
 
 
