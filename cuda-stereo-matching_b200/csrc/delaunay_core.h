@@ -392,6 +392,33 @@ HD bool circle_within(uint32_t pp, uint32_t pq, uint32_t pr, int R, const int32_
     return ext <= double(R);
 }
 
+// circle_within's answer without its extent, by comparisons only: every
+// quantity scaled by D = |2 cross(q - p, r - p)| (the centre's numerators,
+// the box, R), so no division and no square root.  The centre numerators
+// and the scaled box are exact integers in double; the squared terms
+// (below 2^93) carry a relative rounding of 2^-53, which moves a decision
+// by far less than the pixel of margin circle_within relies on.
+HD bool circle_inside(uint32_t pp, uint32_t pq, uint32_t pr, int R, const int32_t* box) {
+    const double qx = dx_p(pq, pp), qy = dy_p(pq, pp), rx = dx_p(pr, pp), ry = dy_p(pr, pp);
+    const double d2x = 2.0 * (qx * ry - qy * rx);
+    const double q2 = qx * qx + qy * qy, r2 = rx * rx + ry * ry;
+    const double sg = d2x < 0.0 ? -1.0 : 1.0, D = fabs(d2x);
+    const double CX = sg * (ry * q2 - qy * r2), CY = sg * (qx * r2 - rx * q2);   // centre * D
+    const double RHO2 = CX * CX + CY * CY;                                       // radius^2 * D^2
+    const double BX0 = (box[0] - px_of(pp)) * D, BY0 = (box[1] - py_of(pp)) * D;
+    const double BX1 = (box[2] - px_of(pp)) * D, BY1 = (box[3] - py_of(pp)) * D;
+    const double EY = fmin(fmax(CY, BY0), BY1) - CY, EX = fmin(fmax(CX, BX0), BX1) - CX;
+    if (EY * EY >= RHO2 || EX * EX >= RHO2) return true;     // the circle misses the box
+    const double RD = double(R) * D, H2 = RHO2 - EY * EY, V2 = RHO2 - EX * EX;
+    // each side of the clipped extent: the box edge itself, or the chord end
+    auto side_ok = [](double edge, double c, double rd, double h2) {
+        // max(c - h, edge) >= -rd  (edge, c scaled), i.e. edge >= -rd or h <= c + rd
+        return edge >= -rd || (c + rd >= 0.0 && h2 <= (c + rd) * (c + rd));
+    };
+    return side_ok(BX0, CX, RD, H2) && side_ok(-BX1, -CX, RD, H2) && side_ok(BY0, CY, RD, V2) &&
+           side_ok(-BY1, -CY, RD, V2);
+}
+
 // Search policy of the star walk.  A search first takes a point's window,
 // the points with |x - px|, |y - py| <= R0, staged once per point (up to
 // STAR_CAP of them), and then squares of doubling half-size Rs

@@ -207,39 +207,39 @@ __global__ void __launch_bounds__(512) k_rowsort(DelDev d0, DelDev d1, const int
 }
 
 // For the star construction, in the block of k_plan once the non-empty
-// rows and their y are known: the table ylut (y -> first non-empty row at or
-// below y, for y in [0, H]), the box of all points (box[0..3]) and the
-// window half-size (box[4], star_r0), and the hull boundary
-// (hnext / hprev of every boundary point; the rows' extreme points are
-// staged in shared memory and each decided by hull_on_chain).
-__device__ void star_setup(const DelDev& D, const int32_t* __restrict__ row_off, int R, int H, int npts,
-                           uint32_t* xyf, uint32_t* xyl, int32_t* lstk, int32_t* rstk, int* ws) {
+// rows (ne, with their y in ney, both in shared memory) are known: the
+// table ylut (y -> first non-empty row at or below y, for y in [0, H]),
+// the box of all points (box[0..3]) and the window half-size (box[4],
+// star_r0), and the hull boundary (hnext / hprev of every boundary point;
+// the rows' extreme points are staged in shared memory and each decided by
+// hull_on_chain).  roff and cnt: the rows' offsets and unique counts, also
+// in shared memory.
+__device__ void star_setup(const DelDev& D, const int32_t* roff, const int32_t* cnt, const int32_t* ne,
+                           const int32_t* ney, int R, int H, int npts, uint32_t* xyf, uint32_t* xyl, int32_t* lstk,
+                           int32_t* rstk, int* ws) {
     __shared__ int box_s[4];
     const int tid = threadIdx.x, nt = blockDim.x;
-    __syncthreads();     // ne_y was written by other threads of the block
-    for (int s = tid; s <= R; s += nt) {
-        const int lo = s ? D.ne_y[s - 1] + 1 : 0, hi = s < R ? D.ne_y[s] : H;
-        for (int v = lo; v <= hi && v <= H; ++v) D.ylut[v] = s;
-    }
     if (tid == 0) {
         box_s[0] = INT_MAX;
         box_s[2] = INT_MIN;
     }
     __syncthreads();
+    for (int s = tid; s <= R; s += nt) {
+        const int lo = s ? ney[s - 1] + 1 : 0, hi = s < R ? ney[s] : H;
+        for (int v = lo; v <= hi && v <= H; ++v) D.ylut[v] = s;
+    }
     for (int s = tid; s < R; s += nt) {
-        const int r = D.ne[s], b = row_off[r];
-        xyf[s] = D.sxy[b];
-        xyl[s] = D.sxy[b + D.rcnt[r] - 1];
-        atomicMin(&box_s[0], px_of(xyf[s]));
-        atomicMax(&box_s[2], px_of(xyl[s]));
+        const int r = ne[s], b = roff[r];
+        const uint32_t f = D.sxy[b], l = D.sxy[b + cnt[r] - 1];
+        xyf[s] = f;
+        xyl[s] = l;
+        atomicMin(&box_s[0], px_of(f));
+        atomicMax(&box_s[2], px_of(l));
     }
     __syncthreads();
     if (tid == 0) {
-        D.box[0] = R ? box_s[0] : 0;
-        D.box[1] = R ? D.ne_y[0] : 0;
-        D.box[2] = R ? box_s[2] : 0;
-        D.box[3] = R ? D.ne_y[R - 1] : 0;
-        const int32_t b[4] = {D.box[0], D.box[1], D.box[2], D.box[3]};
+        const int32_t b[4] = {R ? box_s[0] : 0, R ? ney[0] : 0, R ? box_s[2] : 0, R ? ney[R - 1] : 0};
+        for (int k = 0; k < 4; ++k) D.box[k] = b[k];
         D.box[4] = star_r0(b, npts);
     }
     if (R < 2) return;
@@ -258,15 +258,14 @@ __device__ void star_setup(const DelDev& D, const int32_t* __restrict__ row_off,
         nr += tr_;
     }
     __syncthreads();
-    const int top = D.ne[0], bot = D.ne[R - 1];
-    const int tl = D.rcnt[top], bl = D.rcnt[bot];
+    const int tl = cnt[ne[0]], bl = cnt[ne[R - 1]];
     const int C = hull_cycle_len(tl, bl, nl, nr);
     auto at = [&](int j) {
         int row, pos;
         bool last;
         hull_cycle_at(j, R, tl, bl, lstk, nl, rstk, nr, &row, &pos, &last);
-        const int r = D.ne[row];
-        return D.srt[row_off[r] + (last ? D.rcnt[r] - 1 : pos)];
+        const int r = ne[row];
+        return D.srt[roff[r] + (last ? cnt[r] - 1 : pos)];
     };
     for (int j = tid; j < C; j += nt) {
         const int v = at(j);
@@ -275,50 +274,72 @@ __device__ void star_setup(const DelDev& D, const int32_t* __restrict__ row_off,
     }
 }
 
-// Non-empty rows (list, and their y for the star searches) and strip
-// offsets.  One 1024-thread block per problem.  ctr[7] = 1 when the plan holds (two non-empty rows at least,
-// strips and pockets within Tmax); the strips and pockets are then built by
-// k_strips, which also sets the triangle count ctr[0].
+// Non-empty rows (list, and their y for the star searches), then either the
+// star set-up (stars) or the strip offsets (flips).  One 1024-thread block
+// per problem; the per-row arrays are staged in shared memory (8 arrays of
+// nrows entries).  ctr[7] = 1 when the strip plan holds (two non-empty rows
+// at least, strips and pockets within Tmax); the strips and pockets are then
+// built by k_strips, which also sets the triangle count ctr[0].
 __global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32_t* __restrict__ row_off,
-                                               int nrows, int H, unsigned* err) {
+                                               int nrows, int H, int flips, unsigned* err) {
     grid_dep_wait();
     __shared__ int ws[33];
-    extern __shared__ uint32_t hsm[];    // hull: 4 arrays of nrows entries
+    extern __shared__ int32_t psm[];
+    int32_t* roff = psm;
+    int32_t* cnt = psm + nrows;
+    int32_t* ne = psm + 2 * nrows;
+    int32_t* ney = psm + 3 * nrows;
     DelDev D = blockIdx.x ? d1 : d0;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int r = tid; r < nrows; r += nt) {
+        roff[r] = row_off[r];
+        cnt[r] = D.rcnt[r];
+    }
+    __syncthreads();
     int R = 0, total = 0;
-    // non-empty rows in order, and each row's rank
-    for (int r0 = 0; r0 < nrows; r0 += blockDim.x) {
-        int r = r0 + threadIdx.x;
-        int f = (r < nrows && D.rcnt[r] > 0) ? 1 : 0;
-        int pos = block_scan(f, ws, &total);
-        if (f) D.ne[R + pos] = r;
+    // non-empty rows in order
+    for (int r0 = 0; r0 < nrows; r0 += nt) {
+        const int r = r0 + tid;
+        const int f = (r < nrows && cnt[r] > 0) ? 1 : 0;
+        const int pos = block_scan(f, ws, &total);
+        if (f) ne[R + pos] = r;
         R += total;
     }
     __syncthreads();
-    for (int s = threadIdx.x; s < R; s += blockDim.x) D.ne_y[s] = D.y[row_off[D.ne[s]]];
-    star_setup(D, row_off, R, H, row_off[nrows], hsm, hsm + nrows, reinterpret_cast<int32_t*>(hsm + 2 * nrows),
-               reinterpret_cast<int32_t*>(hsm + 3 * nrows), ws);
-    // strip s between ne[s] and ne[s+1] holds rcnt[ne[s]] + rcnt[ne[s+1]] - 2 triangles
-    int off = 0;
-    for (int s0 = 0; s0 < R - 1; s0 += blockDim.x) {
-        int s = s0 + threadIdx.x;
-        int c = s < R - 1 ? D.rcnt[D.ne[s]] + D.rcnt[D.ne[s + 1]] - 2 : 0;
-        int pos = block_scan(c, ws, &total);
-        if (s < R - 1) D.soff[s] = off + pos;
-        off += total;
+    for (int s = tid; s < R; s += nt) {
+        const int y = D.y[roff[ne[s]]];
+        ney[s] = y;
+        D.ne[s] = ne[s];
+        D.ne_y[s] = y;
     }
-    if (threadIdx.x == 0) {
+    __syncthreads();
+    const int npts = row_off[nrows];
+    int off = 0;
+    if (!flips) {
+        star_setup(D, roff, cnt, ne, ney, R, H, npts, reinterpret_cast<uint32_t*>(psm + 4 * nrows),
+                   reinterpret_cast<uint32_t*>(psm + 5 * nrows), psm + 6 * nrows, psm + 7 * nrows, ws);
+    } else {
+        // strip s between ne[s] and ne[s+1] holds cnt[ne[s]] + cnt[ne[s+1]] - 2 triangles
+        for (int s0 = 0; s0 < R - 1; s0 += nt) {
+            const int s2 = s0 + tid;
+            const int c = s2 < R - 1 ? cnt[ne[s2]] + cnt[ne[s2 + 1]] - 2 : 0;
+            const int pos = block_scan(c, ws, &total);
+            if (s2 < R - 1) D.soff[s2] = off + pos;
+            off += total;
+        }
+    }
+    if (tid == 0) {
         const bool fits = off + 2 * R <= D.Tmax;
-        if (R >= 2 && !fits) set_err(err, ERRF_TRI_COUNT);
+        if (flips && R >= 2 && !fits) set_err(err, ERRF_TRI_COUNT);
         D.ctr[0] = 0;
         D.ctr[1] = off;
         D.ctr[6] = R;
-        D.ctr[7] = (R >= 2 && fits) ? 1 : 0;
+        D.ctr[7] = (flips && R >= 2 && fits) ? 1 : 0;
         D.ctr[8] = 0;    // set to 1 by the flip kernel that handles the problem
-        D.ctr[9] = row_off[nrows];   // support points (vertex ids) of the problem
+        D.ctr[9] = npts;  // support points (vertex ids) of the problem
         D.ctr[4] = 0;    // flip rounds and flips (the flip kernels set them)
         D.ctr[5] = 0;
-        D.ctr[11] = 0;   // star construction: overflow pool cursor, windows grown, searches over all points
+        D.ctr[11] = 0;   // star construction: overflow pool cursor, searches beyond the window, windows grown
         D.ctr[12] = 0;
         D.ctr[13] = 0;
     }
@@ -639,14 +660,15 @@ __global__ void __launch_bounds__(STAR_WARPS * 32, 4) k_star(DelDev d0, DelDev d
             window(take);
             reduce();
             for (int Rs = Rw;;) {
-                int need = 0;
-                if (bi >= 0 && circle_within(pp, pq, bxy, Rs, box, &need)) break;
+                if (bi >= 0 && circle_inside(pp, pq, bxy, Rs, box)) break;
                 if (covers(Rs)) break;
                 if (Rs == Rw && !ring_full) {
                     Rs = grow(take) ? Rw : 2 * Rs;
                     reduce();
                     continue;
                 }
+                int need = 0;
+                if (bi >= 0) circle_within(pp, pq, bxy, Rs, box, &need);
                 if (bi >= 0 && need <= 2 * Rs) {
                     ++circles;
                     star_stream(D, row_off, star_circle_region(pp, pq, bxy, box), box, lane, take3);
@@ -1544,9 +1566,9 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
                             int csize, unsigned* err, cudaStream_t st, int* nlaunch, bool flips,
                             bool force_global, int round_limit) {
     launch_k(k_rowsort, dim3(nrows, 2), 512, 0, st, d0, d1, row_off, nrows, err);
-    const size_t plan_smem = size_t(16) * nrows;
+    const size_t plan_smem = size_t(32) * nrows;
     allow_smem(k_plan);
-    launch_k(k_plan, 2, 1024, plan_smem, st, d0, d1, row_off, nrows, H, err);
+    launch_k(k_plan, 2, 1024, plan_smem, st, d0, d1, row_off, nrows, H, flips ? 1 : 0, err);
     if (!flips) {
         launch_k(k_star, dim3(imax(1, imin((nmax + STAR_WARPS - 1) / STAR_WARPS, 6 * num_sms)), 2), STAR_WARPS * 32,
                  0, st, d0, d1, row_off, err);

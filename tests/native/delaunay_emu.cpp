@@ -397,14 +397,15 @@ extern "C" int emu_delaunay_star(const int32_t* px, const int32_t* py, int n, co
             };
             for (auto& c : win) take(c.first, c.second);
             for (int Rs = Rw;;) {
-                int need = 0;
-                if (bi >= 0 && circle_within(pp, pq, bxy, Rs, box, &need)) return bi;
+                if (bi >= 0 && circle_inside(pp, pq, bxy, Rs, box)) return bi;
                 if (covers(Rs)) return bi;
                 if (Rs == Rw && !ring_full) {
                     if (!grow(take)) Rs *= 2;
                     else Rs = Rw;
                     continue;
                 }
+                int need = 0;
+                if (bi >= 0) circle_within(pp, pq, bxy, Rs, box, &need);
                 if (bi >= 0 && need <= 2 * Rs) {
                     ++circles;
                     each_in(star_circle_region(pp, pq, bxy, box), take);
