@@ -261,6 +261,7 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
         D.pxy = (uint32_t*)take(nmax * 4);
         D.sxy = (uint32_t*)take(nmax * 4);
         D.ne_y = (int32_t*)take(rows * 4);
+        D.rinfo = (int4*)take(rows * 16);
         D.tcnt = (int32_t*)take(nmax * 4);
         D.toff = (int32_t*)take(nmax * 4);
         D.sown = (int32_t*)take(24 * nmax * 4);

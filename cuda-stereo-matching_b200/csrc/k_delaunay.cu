@@ -307,10 +307,12 @@ __global__ void __launch_bounds__(1024) k_plan(DelDev d0, DelDev d1, const int32
     }
     __syncthreads();
     for (int s = tid; s < R; s += nt) {
-        const int y = D.y[roff[ne[s]]];
+        const int r = ne[s];
+        const int y = D.y[roff[r]];
         ney[s] = y;
-        D.ne[s] = ne[s];
+        D.ne[s] = r;
         D.ne_y[s] = y;
+        D.rinfo[s] = make_int4(y, roff[r], cnt[r], 0);
     }
     __syncthreads();
     const int npts = row_off[nrows];
@@ -393,7 +395,8 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
 }
 
 // Every point of a region, spread evenly over the warp's lanes: each lane
-// takes a row (ylut gives the rows of the region's y range), finds the
+// takes a row (ylut gives the rows of the region's y range, rinfo each
+// row's y, first position and count in one 16-byte load), finds the
 // row's column ranges (one, or two beside a ring's hole) by binary search
 // in the row's sorted coordinates, and the ranges of 32 rows are then dealt
 // out one point per lane (a lane finds the row of its point by a binary
@@ -427,11 +430,11 @@ __device__ void star_stream(const DelDev& D, const int32_t* __restrict__ row_off
         const int srow = sb + lane;
         int b = 0, n0 = 0, b1 = 0, n1 = 0;
         if (srow < s1) {
+            const int4 ri = D.rinfo[srow];      // y, first position, unique points
             int32_t x0, x1, x2, x3;
-            g.cols2(D.ne_y[srow], box, &x0, &x1, &x2, &x3);
+            g.cols2(ri.x, box, &x0, &x1, &x2, &x3);
             if (x0 <= x1 || x2 <= x3) {
-                const int r = D.ne[srow];
-                const int base = row_off[r], cnt = D.rcnt[r];
+                const int base = ri.y, cnt = ri.z;
                 const uint32_t* xs = D.sxy + base;
                 if (x0 <= x1) {
                     range(xs, cnt, x0, x1, &b, &n0);

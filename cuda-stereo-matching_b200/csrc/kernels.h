@@ -35,6 +35,7 @@ struct DelDev {
     uint32_t* pxy;         // [Nmax] packed coordinates by point (PXY_NONE: dropped duplicate)
     uint32_t* sxy;         // [Nmax] packed coordinates beside srt
     int32_t* ne_y;         // [rows] y of each non-empty row
+    int4* rinfo;           // [rows] non-empty row: y, first position in srt, unique points
     int32_t* tcnt;         // [Nmax] triangles owned by each point (star construction)
     int32_t* toff;         // [Nmax] their offsets in tri
     int32_t* sown;         // [24*Nmax] owned triangles' vertex pairs, per point
