@@ -63,6 +63,11 @@ struct elas_handle {
     unsigned* err = nullptr;
     unsigned* err_host = nullptr;   // pinned copy of the error word (read back after each host-buffer call)
 
+    // side stream for the disparity grid, which runs beside the Delaunay
+    // and prior stages (it needs only the support list)
+    cudaStream_t side = nullptr;
+    cudaEvent_t side_fork = nullptr, side_join = nullptr;
+
     // per-stage timing
     bool timing = false;
     cudaEvent_t ev[ELAS_TIME_COUNT + 1] = {};
@@ -500,7 +505,22 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     const int corners = p.add_corners ? 1 : 0;
     CK(launch_compact(h->can, h->row_cnt, h->row_off, h->uvd, h->x0, h->x1, h->y, g, st, corners, &n));
     CK(mark(ELAS_TIME_GRID));
-    CK(launch_grid(h->can, h->gtmp0, h->gtmp1, h->grid0, h->grid1, g, st, &n));
+    // The grid needs only the support list: it runs on the side stream
+    // beside the Delaunay and prior stages and joins before dense matching
+    // (recorded as graph edges inside a capture).  With stage timing on it
+    // runs in line, so that the stage marks keep their meaning.
+    const bool fork = !h->timing;
+    if (fork) {
+        if (!h->side) CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+        if (!h->side_fork) CK(cudaEventCreateWithFlags(&h->side_fork, cudaEventDisableTiming));
+        if (!h->side_join) CK(cudaEventCreateWithFlags(&h->side_join, cudaEventDisableTiming));
+        CK(cudaEventRecordWithFlags(h->side_fork, st, ev_flags & ~cudaEventRecordExternal));
+        CK(cudaStreamWaitEvent(h->side, h->side_fork, 0));
+        CK(launch_grid(h->can, h->gtmp0, h->gtmp1, h->grid0, h->grid1, g, h->side, &n));
+        CK(cudaEventRecordWithFlags(h->side_join, h->side, 0));
+    } else {
+        CK(launch_grid(h->can, h->gtmp0, h->gtmp1, h->grid0, h->grid1, g, st, &n));
+    }
     CK(mark(ELAS_TIME_DELAUNAY));
     const bool flips = (h->test_flags & (ELAS_TEST_DELAUNAY_FLIPS | ELAS_TEST_FLIP_GLOBAL)) != 0 ||
                        h->flip_round_limit > 0 ||
@@ -516,6 +536,7 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
                     (h->test_flags & ELAS_TEST_PRIOR_TILED) != 0 ||
                         ((h->test_flags & ELAS_TEST_PRIOR_DIRECT) == 0 &&
                          (long long)W * H >= PRIOR_TILED_MIN_PIXELS)));
+    if (fork) CK(cudaStreamWaitEvent(st, h->side_join, 0));
     int shape = 512;
     rc = dense_threads_for(h, g, dp, st, &n, &shape);
     if (rc != ELAS_OK) return rc;
@@ -885,6 +906,9 @@ int elas_b200_destroy(elas_handle* h) {
     free_pn(h);
     if (h->single_exec) cudaGraphExecDestroy(h->single_exec);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->side_fork) cudaEventDestroy(h->side_fork);
+    if (h->side_join) cudaEventDestroy(h->side_join);
     for (int i = 0; i <= ELAS_TIME_COUNT; ++i)
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);
     if (h->arena) {
