@@ -509,14 +509,22 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     // beside the Delaunay and prior stages and joins before dense matching
     // (recorded as graph edges inside a capture).  With stage timing on it
     // runs in line, so that the stage marks keep their meaning.
+    // The direct prior paint also needs zeroed prior maps, which the side
+    // stream clears meanwhile; the join then comes before the prior stage.
     const bool fork = !h->timing;
+    const bool tiled = (h->test_flags & ELAS_TEST_PRIOR_TILED) != 0 ||
+                       ((h->test_flags & ELAS_TEST_PRIOR_DIRECT) == 0 && (long long)W * H >= PRIOR_TILED_MIN_PIXELS);
     if (fork) {
         if (!h->side) CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
         if (!h->side_fork) CK(cudaEventCreateWithFlags(&h->side_fork, cudaEventDisableTiming));
         if (!h->side_join) CK(cudaEventCreateWithFlags(&h->side_join, cudaEventDisableTiming));
-        CK(cudaEventRecordWithFlags(h->side_fork, st, ev_flags & ~cudaEventRecordExternal));
+        CK(cudaEventRecordWithFlags(h->side_fork, st, 0));
         CK(cudaStreamWaitEvent(h->side, h->side_fork, 0));
         CK(launch_grid(h->can, h->gtmp0, h->gtmp1, h->grid0, h->grid1, g, h->side, &n));
+        if (!tiled) {
+            CK(cudaMemsetAsync(h->prior0, 0, size_t(W) * H * sizeof(uint32_t), h->side));
+            CK(cudaMemsetAsync(h->prior1, 0, size_t(W) * H * sizeof(uint32_t), h->side));
+        }
         CK(cudaEventRecordWithFlags(h->side_join, h->side, 0));
     } else {
         CK(launch_grid(h->can, h->gtmp0, h->gtmp1, h->grid0, h->grid1, g, st, &n));
@@ -530,13 +538,10 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
                        h->cluster_size, h->err, st, &n, flips, (h->test_flags & ELAS_TEST_FLIP_GLOBAL) != 0,
                        h->flip_round_limit));
     CK(mark(ELAS_TIME_PRIOR));
+    if (fork) CK(cudaStreamWaitEvent(st, h->side_join, 0));
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
                     h->rast, h->ptiles, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1,
-                    h->num_sms, h->err, st, &n,
-                    (h->test_flags & ELAS_TEST_PRIOR_TILED) != 0 ||
-                        ((h->test_flags & ELAS_TEST_PRIOR_DIRECT) == 0 &&
-                         (long long)W * H >= PRIOR_TILED_MIN_PIXELS)));
-    if (fork) CK(cudaStreamWaitEvent(st, h->side_join, 0));
+                    h->num_sms, h->err, st, &n, tiled, fork && !tiled));
     int shape = 512;
     rc = dense_threads_for(h, g, dp, st, &n, &shape);
     if (rc != ELAS_OK) return rc;

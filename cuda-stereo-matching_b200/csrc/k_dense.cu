@@ -567,13 +567,15 @@ size_t prior_list_capacity(const Geom& g, int Tmax) {
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
                          int Tmax, const int32_t* can, const int32_t* uvd, void* rast, const PriorTiles& tl,
                          uint32_t* prior0, uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms,
-                         unsigned* err, cudaStream_t st, int* nlaunch, bool tiled) {
+                         unsigned* err, cudaStream_t st, int* nlaunch, bool tiled, bool zeroed) {
     Raster* R = static_cast<Raster*>(rast);
     const int tblocks = imax(1, imin(8 * num_sms, (2 * Tmax + 255) / 256));
     if (!tiled) {
         const size_t n = size_t(g.W) * g.H * sizeof(uint32_t);
-        cudaMemsetAsync(prior0, 0, n, st);
-        cudaMemsetAsync(prior1, 0, n, st);
+        if (!zeroed) {
+            cudaMemsetAsync(prior0, 0, n, st);
+            cudaMemsetAsync(prior1, 0, n, st);
+        }
         launch_k(k_prior_setup, tblocks, 256, 0, st, tri0, tri1, ctr0, ctr1, can, uvd, R, Tmax, g,
                  static_cast<int32_t*>(nullptr), 0, 0);
         launch_k(k_prior_raster, imax(1, imin(16 * num_sms, (2 * Tmax + 7) / 8)), 256, 0, st, ctr0, ctr1, R, Tmax,

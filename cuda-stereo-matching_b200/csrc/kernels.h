@@ -96,10 +96,11 @@ size_t prior_list_capacity(const Geom& g, int Tmax);
 // rast: scratch of 2 * Tmax * raster_bytes() for the per-triangle set-up.
 // tiled: paint tile by tile in shared memory (tl used) instead of with
 // global atomics into the zeroed prior; the same bytes either way.
+// zeroed: (direct paint) the caller has zeroed both priors already.
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
                          int Tmax, const int32_t* can, const int32_t* uvd, void* rast, const PriorTiles& tl,
                          uint32_t* prior0, uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms,
-                         unsigned* err, cudaStream_t st, int* nlaunch, bool tiled);
+                         unsigned* err, cudaStream_t st, int* nlaunch, bool tiled, bool zeroed = false);
 // Images from this many pixels up take the tiled prior paint (measured:
 // the direct paint is faster at 1242x375, the tiled one at 2880x1988).
 constexpr long long PRIOR_TILED_MIN_PIXELS = 1LL << 20;
