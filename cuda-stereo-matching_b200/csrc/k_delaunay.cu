@@ -745,48 +745,52 @@ __global__ void __launch_bounds__(STAR_WARPS * 32, 4) k_star(DelDev d0, DelDev d
     }
 }
 
-// One 1024-thread block per problem: triangle offsets (exclusive prefix
-// sums of the owned counts, in point order) and the triangle count ctr[0].
-__global__ void __launch_bounds__(1024) k_star_scan(DelDev d0, DelDev d1, unsigned* err) {
+// 256 points per CTA, both problems: each point's owned triangles (p, a,
+// b) at its offset, the exclusive prefix sum of the owned counts in point
+// order, so the list is in point order and the same on every run.  A CTA
+// finds the sum of all points before its range itself (the star
+// construction runs up to 2^21 pixels, some 10^4 points a view, so the
+// repeated sums are cheap and save a separate scan launch); CTA 0 also
+// sums every point and writes the triangle count ctr[0].
+constexpr int EMIT_THREADS = 256;
+__global__ void __launch_bounds__(EMIT_THREADS) k_star_emit(DelDev d0, DelDev d1, unsigned* err) {
     grid_dep_wait();
     __shared__ int ws[33];
-    const DelDev& D = blockIdx.x ? d1 : d0;
+    const DelDev& D = blockIdx.y ? d1 : d0;
     const int N = D.ctr[9];
-    const int per = (N + 1023) / 1024, i0 = imin(int(threadIdx.x) * per, N), i1 = imin(i0 + per, N);
-    int sum = 0;
-    for (int i = i0; i < i1; ++i) sum += D.tcnt[i];
-    int total = 0;
-    int run = block_scan(sum, ws, &total);
-    for (int i = i0; i < i1; ++i) {
-        D.toff[i] = run;
-        run += D.tcnt[i];
+    const int start = blockIdx.x * EMIT_THREADS, tid = threadIdx.x;
+    if (start >= N && blockIdx.x != 0) return;
+    const int lim = blockIdx.x == 0 ? N : start;     // CTA 0 sums everything (the total), the others their prefix
+    int pre = 0, total = 0, tmp = 0;
+    for (int i = tid; i < lim; i += EMIT_THREADS) {
+        if (i < start) pre += D.tcnt[i];
+        total += D.tcnt[i];
     }
-    if (threadIdx.x == 0) {
+    block_scan(pre, ws, &tmp);
+    pre = tmp;
+    block_scan(total, ws, &tmp);
+    total = tmp;
+    const int p = start + tid;
+    const int c = p < N ? D.tcnt[p] : 0;
+    int mine = 0;
+    const int off = pre + block_scan(c, ws, &mine);
+    if (blockIdx.x == 0 && tid == 0) {
         const bool fits = total <= D.Tmax;
         if (!fits) set_err(err, ERRF_TRI_COUNT);
         D.ctr[0] = fits ? total : 0;
     }
-}
-
-// One thread per (point, view): the point's owned triangles (p, a, b) at
-// its offset, so the list is in point order and the same on every run.
-__global__ void k_star_emit(DelDev d0, DelDev d1) {
-    grid_dep_wait();
-    const DelDev& D = blockIdx.y ? d1 : d0;
-    const int N = D.ctr[9];
-    if (D.ctr[0] == 0) return;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
-        const int c = D.tcnt[p];
-        if (c == 0) continue;
-        const int o = D.toff[p];
-        const int32_t* slot = D.sown + size_t(p) * 2 * STAR_SLOT;
-        const int32_t* src = c <= STAR_SLOT ? slot : D.spool + 2 * size_t(slot[0]);
-        int32_t* t = D.tri + 3 * size_t(o);
-        for (int j = 0; j < c; ++j) {
-            t[3 * j] = p;
-            t[3 * j + 1] = src[2 * j];
-            t[3 * j + 2] = src[2 * j + 1];
-        }
+    if (c == 0) return;
+    if (off + c > D.Tmax) {
+        set_err(err, ERRF_TRI_COUNT);
+        return;
+    }
+    const int32_t* slot = D.sown + size_t(p) * 2 * STAR_SLOT;
+    const int32_t* src = c <= STAR_SLOT ? slot : D.spool + 2 * size_t(slot[0]);
+    int32_t* t = D.tri + 3 * size_t(off);
+    for (int j = 0; j < c; ++j) {
+        t[3 * j] = p;
+        t[3 * j + 1] = src[2 * j];
+        t[3 * j + 2] = src[2 * j + 1];
     }
 }
 
@@ -1575,9 +1579,9 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
     if (!flips) {
         launch_k(k_star, dim3(imax(1, imin((nmax + STAR_WARPS - 1) / STAR_WARPS, 6 * num_sms)), 2), STAR_WARPS * 32,
                  0, st, d0, d1, row_off, err);
-        launch_k(k_star_scan, 2, 1024, 0, st, d0, d1, err);
-        launch_k(k_star_emit, dim3(imax(1, imin((nmax + 255) / 256, 4 * num_sms)), 2), 256, 0, st, d0, d1);
-        if (nlaunch) *nlaunch += 5;
+        launch_k(k_star_emit, dim3(imax(1, (nmax + EMIT_THREADS - 1) / EMIT_THREADS), 2), EMIT_THREADS, 0, st, d0, d1,
+                 err);
+        if (nlaunch) *nlaunch += 4;
         return cudaGetLastError();
     }
     // the pocket walk's chain and stack (2 sides x (index, x, y, 4-int stack
