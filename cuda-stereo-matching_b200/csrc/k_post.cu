@@ -150,69 +150,103 @@ __device__ __forceinline__ void lunion(int* L, int a, int b) {
     }
 }
 
-__global__ void __launch_bounds__(1024) k_spk_tile(PostViews pv, int W, int H, float thr) {
+// A CTA of 32 x 8 threads per 32x32 tile, each thread taking the tile rows
+// ty, ty + 8, ty + 16, ty + 24 (a warp holds one tile row at a time, for
+// the run ballots): eight such CTAs fit on an SM where a tile per
+// 1024-thread CTA fitted two, so the waits at the tile's barriers overlap
+// with other tiles' work.
+constexpr int SPK_ROWS = 8;
+constexpr int SPK_RPT = SPK_T / SPK_ROWS;
+__global__ void __launch_bounds__(SPK_T * SPK_ROWS) k_spk_tile(PostViews pv, int W, int H, float thr) {
     grid_dep_wait();
     __shared__ float S[SPK_T][SPK_T];
     __shared__ int L[SPK_T * SPK_T];
     __shared__ int C[SPK_T * SPK_T];
+    __shared__ int n_roots, base;
     const int view = blockIdx.z;
     const float* __restrict__ D = pv.cur[view];
-    const int tx = threadIdx.x, ty = threadIdx.y, t = ty * SPK_T + tx;   // a warp per tile row
-    const int x = blockIdx.x * SPK_T + tx, y = blockIdx.y * SPK_T + ty;
-    const bool in = x < W && y < H;
-    const float d = in ? D[size_t(y) * W + x] : -1.0f;
-    const bool valid = d >= 0;
-    S[ty][tx] = d;
-    C[t] = 0;
-    // runs of the row: every pixel points at the first pixel of its run
-    const float dl = __shfl_up_sync(0xffffffffu, d, 1);
-    const bool conn_l = valid && tx > 0 && dl >= 0 && fabsf(d - dl) <= thr;
-    const unsigned starts = __ballot_sync(0xffffffffu, valid && !conn_l);
-    const unsigned mine = starts & (0xffffffffu >> (31 - tx));
-    L[t] = valid ? ty * SPK_T + (31 - __clz(mine)) : t;
+    const int tx = threadIdx.x, tid = threadIdx.y * SPK_T + tx;
+    const int x = blockIdx.x * SPK_T + tx;
+    float d[SPK_RPT], dl[SPK_RPT];
+    bool conn_l[SPK_RPT];
+#pragma unroll
+    for (int j = 0; j < SPK_RPT; ++j) {
+        const int ty = threadIdx.y + SPK_ROWS * j, t = ty * SPK_T + tx, y = blockIdx.y * SPK_T + ty;
+        const bool in = x < W && y < H;
+        d[j] = in ? D[size_t(y) * W + x] : -1.0f;
+        const bool valid = d[j] >= 0;
+        S[ty][tx] = d[j];
+        C[t] = 0;
+        // runs of the row: every pixel points at the first pixel of its run
+        dl[j] = __shfl_up_sync(0xffffffffu, d[j], 1);
+        conn_l[j] = valid && tx > 0 && dl[j] >= 0 && fabsf(d[j] - dl[j]) <= thr;
+        const unsigned starts = __ballot_sync(0xffffffffu, valid && !conn_l[j]);
+        const unsigned mine = starts & (0xffffffffu >> (31 - tx));
+        L[t] = valid ? ty * SPK_T + (31 - __clz(mine)) : t;
+    }
+    if (tid == 0) n_roots = 0;
     __syncthreads();
     // vertical links; a link is implied when the left neighbours make the same one
-    if (valid && ty + 1 < SPK_T) {
-        const float q = S[ty + 1][tx];
-        if (q >= 0 && fabsf(q - d) <= thr) {
-            bool implied = false;
-            if (tx > 0) {
-                const float ql = S[ty + 1][tx - 1];
-                implied = conn_l && ql >= 0 && fabsf(ql - q) <= thr && fabsf(ql - dl) <= thr;
+#pragma unroll
+    for (int j = 0; j < SPK_RPT; ++j) {
+        const int ty = threadIdx.y + SPK_ROWS * j, t = ty * SPK_T + tx;
+        if (d[j] >= 0 && ty + 1 < SPK_T) {
+            const float q = S[ty + 1][tx];
+            if (q >= 0 && fabsf(q - d[j]) <= thr) {
+                bool implied = false;
+                if (tx > 0) {
+                    const float ql = S[ty + 1][tx - 1];
+                    implied = conn_l[j] && ql >= 0 && fabsf(ql - q) <= thr && fabsf(ql - dl[j]) <= thr;
+                }
+                if (!implied) lunion(L, t, t + SPK_T);
             }
-            if (!implied) lunion(L, t, t + SPK_T);
         }
     }
     __syncthreads();
     // roots: the run heads (the only nodes of the forest) walk to their
     // root and keep it; every pixel then reads its head's entry
-    const bool head = valid && !conn_l;
-    int r = head ? lfind(L, t) : -1;
+    int r[SPK_RPT];
+#pragma unroll
+    for (int j = 0; j < SPK_RPT; ++j) {
+        const int t = (threadIdx.y + SPK_ROWS * j) * SPK_T + tx;
+        r[j] = d[j] >= 0 && !conn_l[j] ? lfind(L, t) : -1;
+    }
     __syncthreads();
-    if (head) L[t] = r;
+#pragma unroll
+    for (int j = 0; j < SPK_RPT; ++j)
+        if (d[j] >= 0 && !conn_l[j]) L[(threadIdx.y + SPK_ROWS * j) * SPK_T + tx] = r[j];
     __syncthreads();
-    if (valid && !head) r = L[L[t]];
-    {   // component sizes, one shared atomic per group of lanes with the same root
-        const unsigned peers = __match_any_sync(0xffffffffu, r);
-        if (r >= 0 && tx == __ffs(peers) - 1) atomicAdd(&C[r], __popc(peers));
+#pragma unroll
+    for (int j = 0; j < SPK_RPT; ++j) {
+        const int t = (threadIdx.y + SPK_ROWS * j) * SPK_T + tx;
+        if (d[j] >= 0 && conn_l[j]) r[j] = L[L[t]];
+        // component sizes, one shared atomic per group of lanes with the same root
+        const unsigned peers = __match_any_sync(0xffffffffu, r[j]);
+        if (r[j] >= 0 && tx == __ffs(peers) - 1) atomicAdd(&C[r[j]], __popc(peers));
     }
     // the tile's local roots take consecutive list slots: one reservation per tile
-    __shared__ int n_roots, base;
-    if (t == 0) n_roots = 0;
+    int slot[SPK_RPT];
+#pragma unroll
+    for (int j = 0; j < SPK_RPT; ++j) {
+        const int ty = threadIdx.y + SPK_ROWS * j, t = ty * SPK_T + tx;
+        const bool is_root = x < W && blockIdx.y * SPK_T + ty < H && r[j] == t;
+        slot[j] = is_root ? atomicAdd(&n_roots, 1) : -1;
+    }
     __syncthreads();
-    const bool is_root = in && r == t;
-    const int slot = is_root ? atomicAdd(&n_roots, 1) : 0;
+    if (tid == 0) base = n_roots > 0 ? atomicAdd(pv.roots[view], n_roots) : 0;
     __syncthreads();
-    if (t == 0) base = n_roots > 0 ? atomicAdd(pv.roots[view], n_roots) : 0;
-    __syncthreads();
-    if (in) {
-        const size_t i = size_t(y) * W + x;
-        const int rx = blockIdx.x * SPK_T + (r & (SPK_T - 1)), ry = blockIdx.y * SPK_T + (r / SPK_T);
-        pv.lab[view][i] = r >= 0 ? int(size_t(ry) * W + rx) : -1;
-        if (is_root) {                  // a local root: its count, its segment-size slot, its list entry
-            pv.sz[view][i] = C[t];
-            pv.root[view][i] = 0;
-            pv.roots[view][1 + base + slot] = int(i);
+#pragma unroll
+    for (int j = 0; j < SPK_RPT; ++j) {
+        const int ty = threadIdx.y + SPK_ROWS * j, t = ty * SPK_T + tx, y = blockIdx.y * SPK_T + ty;
+        if (x < W && y < H) {
+            const size_t i = size_t(y) * W + x;
+            const int rx = blockIdx.x * SPK_T + (r[j] & (SPK_T - 1)), ry = blockIdx.y * SPK_T + (r[j] / SPK_T);
+            pv.lab[view][i] = r[j] >= 0 ? int(size_t(ry) * W + rx) : -1;
+            if (slot[j] >= 0) {         // a local root: its count, its segment-size slot, its list entry
+                pv.sz[view][i] = C[t];
+                pv.root[view][i] = 0;
+                pv.roots[view][1 + base + slot[j]] = int(i);
+            }
         }
     }
 }
@@ -509,7 +543,7 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
     if (p.speckle_size > 0) {
         for (int k = 0; k < nviews; ++k) cudaMemsetAsync(pv.roots[k], 0, sizeof(int32_t), st);
         const dim3 tiles((W + SPK_T - 1) / SPK_T, (H + SPK_T - 1) / SPK_T, nviews);
-        launch_k(k_spk_tile, tiles, dim3(SPK_T, SPK_T), 0, st, pv, W, H, p.speckle_sim_threshold);
+        launch_k(k_spk_tile, tiles, dim3(SPK_T, SPK_ROWS), 0, st, pv, W, H, p.speckle_sim_threshold);
         const long long border = (long long)H * (tiles.x - 1) + (long long)W * (tiles.y - 1);
         const int gb = int(border / 256 + 1 < 4096 ? border / 256 + 1 : 4096);
         launch_k(k_spk_border, dim3(gb, 1, nviews), 256, 0, st, pv, W, H, p.speckle_sim_threshold, err);
