@@ -403,9 +403,10 @@ constexpr int K_INVALID = 1 << 20;
 // (segments smaller than spk_min become invalid) on the way in.
 // Persistent: each CTA builds the weight table once and walks 32x32 tiles
 // of both views with a stride of the grid size.
-template <int G, bool GAP, bool MEAN, bool MEDIAN>
-__global__ void __launch_bounds__(1024, 2) k_post_tile(PostViews pv, int W, int H, int gap, int spk_min,
-                                                       int wt_n, int nviews) {
+constexpr int POST_THREADS = 512;    // threads of a tile-filter CTA (measured against 256 and 1024)
+template <int G, bool GAP, bool MEAN, bool MEDIAN, int NT>
+__global__ void __launch_bounds__(NT, 2048 / NT) k_post_tile(PostViews pv, int W, int H, int gap, int spk_min,
+                                                             int wt_n, int nviews) {
     grid_dep_wait();
     constexpr int PHALO = G + 3, PS = PT + 2 * PHALO;   // S tile side
     extern __shared__ float WT[];               // wt_n weights when MEAN
@@ -417,7 +418,7 @@ __global__ void __launch_bounds__(1024, 2) k_post_tile(PostViews pv, int W, int 
     const int tid = threadIdx.x;
     const float OUT = -2.0f;                    // outside the image (never valid, never filled)
     if (MEAN)
-        for (int j = tid; j < wt_n; j += 1024) {
+        for (int j = tid; j < wt_n; j += NT) {
             const float q = float(j) * 0.25f;
             WT[j] = j < wt_n - 1 ? __frcp_rn(__fmaf_rn(q, q, 1.0f)) : 0.0f;
         }
@@ -437,7 +438,7 @@ __global__ void __launch_bounds__(1024, 2) k_post_tile(PostViews pv, int W, int 
         // pixel waits on three dependent loads, and the loop is unrolled so that
         // two pixels' chains overlap.
 #pragma unroll 2
-        for (int i = tid; i < PS * PS; i += 1024) {
+        for (int i = tid; i < PS * PS; i += NT) {
             int r = i / PS, c = i % PS;
             int x = u0 - PHALO + c, y = v0 - PHALO + r;
             float d = OUT;
@@ -453,7 +454,7 @@ __global__ void __launch_bounds__(1024, 2) k_post_tile(PostViews pv, int W, int 
         }
         __syncthreads();
         // row pass on rows [-PHALO, 32+PHALO), columns [-3, 35)
-        for (int i = tid; i < PS * (PT + 6); i += 1024) {
+        for (int i = tid; i < PS * (PT + 6); i += NT) {
             int r = i / (PT + 6), c = i % (PT + 6);
             int x = u0 - 3 + c;
             float val = S[r][c + PHALO - 3];
@@ -462,7 +463,7 @@ __global__ void __launch_bounds__(1024, 2) k_post_tile(PostViews pv, int W, int 
         }
         __syncthreads();
         // column pass on [-3, 35)^2
-        for (int i = tid; i < (PT + 6) * (PT + 6); i += 1024) {
+        for (int i = tid; i < (PT + 6) * (PT + 6); i += NT) {
             int r = i / (PT + 6), c = i % (PT + 6);
             int y = v0 - 3 + r;
             float val = G2[r + PHALO - 3][c];
@@ -472,7 +473,7 @@ __global__ void __launch_bounds__(1024, 2) k_post_tile(PostViews pv, int W, int 
         }
         __syncthreads();
         // mean on [-1, 33)^2, in the oracle's (dy, dx) order: num by fma, den by add
-        for (int i = tid; i < (PT + 2) * (PT + 2); i += 1024) {
+        for (int i = tid; i < (PT + 2) * (PT + 2); i += NT) {
             int r = i / (PT + 2), c = i % (PT + 2);
             float dp = V[r + 2][c + 2];
             float out = dp;
@@ -495,8 +496,8 @@ __global__ void __launch_bounds__(1024, 2) k_post_tile(PostViews pv, int W, int 
             M[r][c] = out;
         }
         __syncthreads();
-        {
-            int ty = tid / PT, tx = tid % PT;
+        for (int o = tid; o < PT * PT; o += NT) {
+            int ty = o / PT, tx = o % PT;
             int u = u0 + tx, v = v0 + ty;
             if (u < W && v < H) {
                 float c = M[ty + 1][tx + 1];
@@ -572,30 +573,30 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         if (direct)
             for (int k = 0; k < nviews; ++k) pv.nxt[k] = pv.out[k];
         const int tiles = ((W + PT - 1) / PT) * ((H + PT - 1) / PT) * nviews;
-        const int grid = imax(1, imin(tiles, 2 * num_sms));
+        const int grid = imax(1, imin(tiles, (2048 / POST_THREADS) * num_sms));
         const int wt_n = 4 * g.D + 2;
         const size_t smem = adaptive_mean ? size_t(wt_n) * sizeof(float) : 0;
         const int key = (tile_gap ? 4 : 0) | (adaptive_mean ? 2 : 0) | (median ? 1 : 0);
         auto go = [&](auto kern) {
             if (smem) allow_smem(kern);
-            launch_k(kern, grid, 1024, smem, st, pv, W, H, gap, spk, wt_n, nviews);
+            launch_k(kern, grid, POST_THREADS, smem, st, pv, W, H, gap, spk, wt_n, nviews);
         };
         if (!tile_gap || gap <= 3) {   // halo 6
             switch (key) {
-            case 1: go(k_post_tile<3, false, false, true>); break;
-            case 2: go(k_post_tile<3, false, true, false>); break;
-            case 3: go(k_post_tile<3, false, true, true>); break;
-            case 4: go(k_post_tile<3, true, false, false>); break;
-            case 5: go(k_post_tile<3, true, false, true>); break;
-            case 6: go(k_post_tile<3, true, true, false>); break;
-            default: go(k_post_tile<3, true, true, true>); break;
+            case 1: go(k_post_tile<3, false, false, true, POST_THREADS>); break;
+            case 2: go(k_post_tile<3, false, true, false, POST_THREADS>); break;
+            case 3: go(k_post_tile<3, false, true, true, POST_THREADS>); break;
+            case 4: go(k_post_tile<3, true, false, false, POST_THREADS>); break;
+            case 5: go(k_post_tile<3, true, false, true, POST_THREADS>); break;
+            case 6: go(k_post_tile<3, true, true, false, POST_THREADS>); break;
+            default: go(k_post_tile<3, true, true, true, POST_THREADS>); break;
             }
         } else {                       // gaps 4..8: halo 11
             switch (key) {
-            case 4: go(k_post_tile<PGMAX, true, false, false>); break;
-            case 5: go(k_post_tile<PGMAX, true, false, true>); break;
-            case 6: go(k_post_tile<PGMAX, true, true, false>); break;
-            default: go(k_post_tile<PGMAX, true, true, true>); break;
+            case 4: go(k_post_tile<PGMAX, true, false, false, POST_THREADS>); break;
+            case 5: go(k_post_tile<PGMAX, true, false, true, POST_THREADS>); break;
+            case 6: go(k_post_tile<PGMAX, true, true, false, POST_THREADS>); break;
+            default: go(k_post_tile<PGMAX, true, true, true, POST_THREADS>); break;
             }
         }
         flip();
