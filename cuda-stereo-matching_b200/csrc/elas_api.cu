@@ -284,11 +284,11 @@ size_t layout(elas_handle* h, const Geom& g, char* base) {
     }
     h->rast = take(2 * tmax * raster_bytes());
     {
-        const size_t nt = prior_tile_count(g), cap = prior_list_capacity(g, int(tmax));
+        const size_t nt = prior_tile_count(g), cap = prior_overflow_capacity(g, int(tmax));
         h->ptiles.cnt = (int32_t*)take(2 * (nt + 1) * 4);
-        h->ptiles.off = (int32_t*)take(2 * (nt + 1) * 4);
-        h->ptiles.list = (int32_t*)take(2 * cap * 4);
-        h->ptiles.cap = int(cap);
+        h->ptiles.bins = (int32_t*)take(2 * nt * PT_BIN * 4);
+        h->ptiles.ovf = (int32_t*)take(2 * cap * 2 * 4);
+        h->ptiles.ovf_cap = int(cap);
     }
     h->prior0 = (uint32_t*)take(px * 4);
     h->prior1 = (uint32_t*)take(px * 4);
@@ -541,7 +541,8 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
     if (fork) CK(cudaStreamWaitEvent(st, h->side_join, 0));
     CK(launch_prior(h->del[0].tri, h->del[1].tri, h->del[0].ctr, h->del[1].ctr, h->del[0].Tmax, h->can, h->uvd,
                     h->rast, h->ptiles, h->prior0, h->prior1, g, prior_shift(g, dp), g.D + dp.plane_radius + 1,
-                    h->num_sms, h->err, st, &n, tiled, fork && !tiled));
+                    h->num_sms, h->err, st, &n, tiled, fork && !tiled,
+                    (h->test_flags & ELAS_TEST_PRIOR_SMALL_BINS) ? 2 : PT_BIN));
     int shape = 512;
     rc = dense_threads_for(h, g, dp, st, &n, &shape);
     if (rc != ELAS_OK) return rc;
@@ -1069,7 +1070,8 @@ int elas_b200_process_batch_device(elas_handle* h, int n, const uint8_t* const* 
 int elas_b200_set_test_mode(elas_handle* h, int32_t flags, int32_t flip_round_limit) {
     if (!h) return ELAS_ERR_INVALID_ARG;
     const int32_t known = ELAS_TEST_FLIP_GLOBAL | ELAS_TEST_DENSE_BITSET | ELAS_TEST_PRIOR_TILED |
-                          ELAS_TEST_PRIOR_DIRECT | ELAS_TEST_DELAUNAY_FLIPS | ELAS_TEST_DELAUNAY_STARS;
+                          ELAS_TEST_PRIOR_DIRECT | ELAS_TEST_DELAUNAY_FLIPS | ELAS_TEST_DELAUNAY_STARS |
+                          ELAS_TEST_PRIOR_SMALL_BINS;
     if ((flags & ~known) != 0 || flip_round_limit < 0)
         return fail(h, ELAS_ERR_INVALID_ARG, "unknown test flag or negative round limit");
     if ((flags & ELAS_TEST_DELAUNAY_STARS) &&

@@ -9,9 +9,10 @@
 //     into the zeroed prior (two launches after the memset; the faster one
 //     for small images);
 //   * tiled: the set-up also finds the 64x32 prior tiles a triangle's pixels
-//     can fall in, the triangles are binned by tile, and one CTA per tile
-//     paints it in shared memory and writes it once (no memset, no global
-//     atomics; the faster one from about a megapixel up).
+//     can fall in and drops the triangle into each tile's fixed bin (the
+//     slot its count's atomic returns; no scan), and one CTA per tile paints
+//     it in shared memory and writes it once (no memset, no global atomics
+//     on the prior; the faster one from about a megapixel up).
 // A pixel covered by more than one triangle (rounding at shared vertices)
 // must keep the last triangle in list order, as a sequential rasteriser
 // would; both paint with a 32-bit atomicMax of (triangle+1) << pshift |
@@ -152,15 +153,18 @@ __device__ void setup_triangle(const int32_t* tri, const int32_t* can, const int
 
 // One thread per (view, triangle): plane and edge set-up and, for the tiled
 // paint (tcnt non-null), the prior tiles its pixels can fall in (from the
-// exact row range of the raster and its column range) with one count per
-// such tile.
+// exact row range of the raster and its column range).  The triangle goes
+// into each such tile's bin of PT_BIN entries at the slot its count's
+// atomic returns, or, once a bin is full, into the view's overflow list of
+// (tile, triangle) pairs (tcnt[ntiles] counts those).
 __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__ tri0,
                                                      const int32_t* __restrict__ tri1,
                                                      const int32_t* __restrict__ ctr0,
                                                      const int32_t* __restrict__ ctr1,
                                                      const int32_t* __restrict__ can, const int32_t* __restrict__ uvd,
                                                      Raster* __restrict__ rast, int Tmax, Geom g, int32_t* tcnt,
-                                                     int ntx, int ntiles) {
+                                                     int ntx, int ntiles, int32_t* bins, int32_t* ovf, int ovf_cap,
+                                                     int bin_cap, unsigned* err) {
     grid_dep_wait();
     const int T0 = ctr0[0], T1 = ctr1[0];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T0 + T1; i += gridDim.x * blockDim.x) {
@@ -183,8 +187,24 @@ __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__
         }
         rast[(right ? Tmax : 0) + t] = R;
         int32_t* c = tcnt + (right ? ntiles + 1 : 0);
+        int32_t* b = bins + (right ? size_t(ntiles) * PT_BIN : 0);
+        int32_t* o = ovf + (right ? 2 * size_t(ovf_cap) : 0);
         for (int ty = R.ty0; ty <= R.ty1; ++ty)
-            for (int tx = R.tx0; tx <= R.tx1; ++tx) atomicAdd(c + ty * ntx + tx, 1);
+            for (int tx = R.tx0; tx <= R.tx1; ++tx) {
+                const int tile = ty * ntx + tx;
+                const int pos = atomicAdd(c + tile, 1);
+                if (pos < bin_cap) {
+                    b[size_t(tile) * PT_BIN + pos] = t;
+                } else {
+                    const int k = atomicAdd(c + ntiles, 1);
+                    if (k < ovf_cap) {
+                        o[2 * k] = tile;
+                        o[2 * k + 1] = t;
+                    } else {
+                        atomicOr(err, ERRF_BOUNDS);
+                    }
+                }
+            }
     }
 }
 
@@ -225,70 +245,6 @@ __global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict_
     }
 }
 
-// One 1024-thread block per view: exclusive prefix sums of the tile counts
-// (the list offsets), which also become the fill cursors.
-__global__ void __launch_bounds__(1024) k_prior_scan(int32_t* cnt, int32_t* off, int n) {
-    grid_dep_wait();
-    __shared__ int ws[33];
-    int32_t* c = cnt + blockIdx.x * (n + 1);
-    int32_t* o = off + blockIdx.x * (n + 1);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int per = (n + 1023) / 1024, i0 = imin(tid * per, n), i1 = imin(i0 + per, n);
-    int sum = 0;
-    for (int i = i0; i < i1; ++i) sum += c[i];
-    int y = sum;
-#pragma unroll
-    for (int k = 1; k < 32; k <<= 1) {
-        const int z = __shfl_up_sync(0xffffffffu, y, k);
-        if (lane >= k) y += z;
-    }
-    if (lane == 31) ws[warp] = y;
-    __syncthreads();
-    if (warp == 0) {
-        const int w = ws[lane];
-        int x = w;
-#pragma unroll
-        for (int k = 1; k < 32; k <<= 1) {
-            const int z = __shfl_up_sync(0xffffffffu, x, k);
-            if (lane >= k) x += z;
-        }
-        ws[lane] = x - w;
-        if (lane == 31) ws[32] = x;
-    }
-    __syncthreads();
-    int run = y - sum + ws[warp];
-    for (int i = i0; i < i1; ++i) {
-        const int k = c[i];
-        o[i] = run;
-        c[i] = run;
-        run += k;
-    }
-    if (tid == 0) o[n] = ws[32];
-}
-
-// One thread per (view, triangle): its index into the list of each of its
-// tiles (the order within a tile carries no meaning: the paint keeps the
-// largest triangle index per pixel).
-__global__ void __launch_bounds__(256) k_prior_fill(const int32_t* __restrict__ ctr0, const int32_t* __restrict__ ctr1,
-                                                    const Raster* __restrict__ rast, int Tmax, int32_t* cursor,
-                                                    int32_t* list, int cap, int ntx, int ntiles, unsigned* err) {
-    grid_dep_wait();
-    const int T0 = ctr0[0], T1 = ctr1[0];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T0 + T1; i += gridDim.x * blockDim.x) {
-        const bool right = i >= T0;
-        const int t = right ? i - T0 : i;
-        const Raster& R = rast[(right ? Tmax : 0) + t];
-        int32_t* cur = cursor + (right ? ntiles + 1 : 0);
-        int32_t* l = list + (right ? size_t(cap) : 0);
-        for (int ty = R.ty0; ty <= R.ty1; ++ty)
-            for (int tx = R.tx0; tx <= R.tx1; ++tx) {
-                const int pos = atomicAdd(cur + ty * ntx + tx, 1);
-                if (pos < cap) l[pos] = t;
-                else atomicOr(err, ERRF_BOUNDS);
-            }
-    }
-}
-
 // One CTA per (prior tile, view): every triangle of the tile's list paints
 // the pixels it covers in the tile into shared memory with atomicMax of
 // (triangle+1) << pshift | d_plane -- the last triangle in list order wins,
@@ -298,23 +254,23 @@ __global__ void __launch_bounds__(256) k_prior_fill(const int32_t* __restrict__ 
 // coverage and values are the reference's scan-line expressions
 // (KerComputeDisparity.cu:57-150) with its contraction made explicit.
 __global__ void __launch_bounds__(256) k_prior_tiles(const Raster* __restrict__ rast, int Tmax,
-                                                     const int32_t* __restrict__ off,
-                                                     const int32_t* __restrict__ list, int cap, uint32_t* prior0,
-                                                     uint32_t* prior1, Geom g, int pshift, int dcap, int ntx,
-                                                     int ntiles) {
+                                                     const int32_t* __restrict__ tcnt,
+                                                     const int32_t* __restrict__ bins,
+                                                     const int32_t* __restrict__ ovf, int ovf_cap, int bin_cap,
+                                                     uint32_t* prior0, uint32_t* prior1, Geom g, int pshift, int dcap,
+                                                     int ntx, int ntiles) {
     grid_dep_wait();
     __shared__ uint32_t pt[PT_H][PT_W];
     const int view = blockIdx.z, tu0 = blockIdx.x * PT_W, tv0 = blockIdx.y * PT_H;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
     for (int i = tid; i < PT_W * PT_H; i += blockDim.x) (&pt[0][0])[i] = 0u;
     __syncthreads();
-    const int32_t* o = off + view * (ntiles + 1);
+    const int32_t* c = tcnt + view * (ntiles + 1);
     const int tile = blockIdx.y * ntx + blockIdx.x;
-    const int b = imin(o[tile], cap), e = imin(o[tile + 1], cap);
-    const int32_t* l = list + (view ? size_t(cap) : 0);
+    const int n = c[tile];
+    const int32_t* b = bins + (view ? size_t(ntiles) * PT_BIN : 0) + size_t(tile) * PT_BIN;
     const Raster* rs = rast + (view ? Tmax : 0);
-    for (int k = b + warp; k < e; k += nw) {
-        const int t = l[k];
+    auto paint = [&](int t) {
         const Raster R = rs[t];
         const uint32_t tag = uint32_t(t + 1) << pshift;
         for (int part = 0; part < 2; ++part) {
@@ -334,6 +290,13 @@ __global__ void __launch_bounds__(256) k_prior_tiles(const Raster* __restrict__ 
                 }
             }
         }
+    };
+    for (int k = warp; k < imin(n, bin_cap); k += nw) paint(b[k]);
+    if (n > bin_cap) {      // a full bin: the rest of its triangles are in the overflow list
+        const int no = imin(c[ntiles], ovf_cap);
+        const int32_t* o = ovf + (view ? 2 * size_t(ovf_cap) : 0);
+        for (int k = warp; k < no; k += nw)
+            if (o[2 * k] == tile) paint(o[2 * k + 1]);
     }
     __syncthreads();
     uint32_t* prior = view ? prior1 : prior0;
@@ -559,15 +522,15 @@ __global__ void k_lr(const float* __restrict__ D1, const float* __restrict__ D2,
 
 size_t prior_tile_count(const Geom& g) { return size_t((g.W + PT_W - 1) / PT_W) * ((g.H + PT_H - 1) / PT_H); }
 
-size_t prior_list_capacity(const Geom& g, int Tmax) {
-    // about two tiles per triangle are typical; this leaves a factor of eight
-    return size_t(16) * Tmax + size_t(16) * prior_tile_count(g);
+size_t prior_overflow_capacity(const Geom& g, int Tmax) {
+    // bins overflow only where a 64x32 tile meets more than PT_BIN triangles
+    return size_t(2) * Tmax + size_t(16) * prior_tile_count(g);
 }
 
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
                          int Tmax, const int32_t* can, const int32_t* uvd, void* rast, const PriorTiles& tl,
                          uint32_t* prior0, uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms,
-                         unsigned* err, cudaStream_t st, int* nlaunch, bool tiled, bool zeroed) {
+                         unsigned* err, cudaStream_t st, int* nlaunch, bool tiled, bool zeroed, int bin_cap) {
     Raster* R = static_cast<Raster*>(rast);
     const int tblocks = imax(1, imin(8 * num_sms, (2 * Tmax + 255) / 256));
     if (!tiled) {
@@ -577,7 +540,8 @@ cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t
             cudaMemsetAsync(prior1, 0, n, st);
         }
         launch_k(k_prior_setup, tblocks, 256, 0, st, tri0, tri1, ctr0, ctr1, can, uvd, R, Tmax, g,
-                 static_cast<int32_t*>(nullptr), 0, 0);
+                 static_cast<int32_t*>(nullptr), 0, 0, static_cast<int32_t*>(nullptr), static_cast<int32_t*>(nullptr),
+                 0, 0, err);
         launch_k(k_prior_raster, imax(1, imin(16 * num_sms, (2 * Tmax + 7) / 8)), 256, 0, st, ctr0, ctr1, R, Tmax,
                  prior0, prior1, g, pshift, dcap);
         if (nlaunch) *nlaunch += 2;
@@ -585,12 +549,11 @@ cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t
     }
     const int ntx = (g.W + PT_W - 1) / PT_W, nty = (g.H + PT_H - 1) / PT_H, ntiles = ntx * nty;
     cudaMemsetAsync(tl.cnt, 0, size_t(2) * (ntiles + 1) * sizeof(int32_t), st);
-    launch_k(k_prior_setup, tblocks, 256, 0, st, tri0, tri1, ctr0, ctr1, can, uvd, R, Tmax, g, tl.cnt, ntx, ntiles);
-    launch_k(k_prior_scan, 2, 1024, 0, st, tl.cnt, tl.off, ntiles);
-    launch_k(k_prior_fill, tblocks, 256, 0, st, ctr0, ctr1, R, Tmax, tl.cnt, tl.list, tl.cap, ntx, ntiles, err);
-    launch_k(k_prior_tiles, dim3(ntx, nty, 2), 256, 0, st, R, Tmax, tl.off, tl.list, tl.cap, prior0, prior1, g,
-             pshift, dcap, ntx, ntiles);
-    if (nlaunch) *nlaunch += 4;
+    launch_k(k_prior_setup, tblocks, 256, 0, st, tri0, tri1, ctr0, ctr1, can, uvd, R, Tmax, g, tl.cnt, ntx, ntiles,
+             tl.bins, tl.ovf, tl.ovf_cap, bin_cap, err);
+    launch_k(k_prior_tiles, dim3(ntx, nty, 2), 256, 0, st, R, Tmax, tl.cnt, tl.bins, tl.ovf, tl.ovf_cap, bin_cap,
+             prior0, prior1, g, pshift, dcap, ntx, ntiles);
+    if (nlaunch) *nlaunch += 2;
     return cudaGetLastError();
 }
 

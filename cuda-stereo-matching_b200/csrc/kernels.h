@@ -80,15 +80,17 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
 // kernel, or 0 if none fits.
 int cluster_size_for_flip();
 
-// Triangles binned by 64x32 prior tile, both views.
+// Triangles binned by 64x32 prior tile, both views: a bin of PT_BIN
+// entries per tile, the rest of a full bin's triangles in an overflow list.
+constexpr int PT_BIN = 128;
 struct PriorTiles {
-    int32_t* cnt;      // [2][tiles + 1] counts, then the fill cursors
-    int32_t* off;      // [2][tiles + 1] list offsets
-    int32_t* list;     // [2][cap] triangle indices, tile by tile
-    int cap;           // entries per view (overflow raises ERRF_BOUNDS)
+    int32_t* cnt;      // [2][tiles + 1] triangles per tile; [tiles]: overflow pairs
+    int32_t* bins;     // [2][tiles][PT_BIN] triangle indices
+    int32_t* ovf;      // [2][ovf_cap][2] (tile, triangle) beyond full bins
+    int ovf_cap;       // pairs per view (more raise ERRF_BOUNDS)
 };
 size_t prior_tile_count(const Geom& g);
-size_t prior_list_capacity(const Geom& g, int Tmax);
+size_t prior_overflow_capacity(const Geom& g, int Tmax);
 
 // Plane prior of both views: prior[v*W+u] = (triangle+1) << pshift | d,
 // d = d_plane clamped to [0, dcap] (dcap = disp_max + plane_radius + 1),
@@ -97,10 +99,13 @@ size_t prior_list_capacity(const Geom& g, int Tmax);
 // tiled: paint tile by tile in shared memory (tl used) instead of with
 // global atomics into the zeroed prior; the same bytes either way.
 // zeroed: (direct paint) the caller has zeroed both priors already.
+// bin_cap: (tiled paint) entries used of each tile's bin (tests lower it so
+// that the overflow list is used).
 cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t* ctr0, const int32_t* ctr1,
                          int Tmax, const int32_t* can, const int32_t* uvd, void* rast, const PriorTiles& tl,
                          uint32_t* prior0, uint32_t* prior1, const Geom& g, int pshift, int dcap, int num_sms,
-                         unsigned* err, cudaStream_t st, int* nlaunch, bool tiled, bool zeroed = false);
+                         unsigned* err, cudaStream_t st, int* nlaunch, bool tiled, bool zeroed = false,
+                         int bin_cap = PT_BIN);
 // Images from this many pixels up take the tiled prior paint (measured:
 // the direct paint is faster at 1242x375, the tiled one at 2880x1988).
 constexpr long long PRIOR_TILED_MIN_PIXELS = 1LL << 20;

@@ -292,6 +292,7 @@ class Elas:
     TEST_PRIOR_DIRECT = 8     # plane prior painted with global atomics at every size
     TEST_DELAUNAY_FLIPS = 16  # triangulations from row strips and edge flips at every size
     TEST_DELAUNAY_STARS = 32  # triangulations found star by star at every size
+    TEST_PRIOR_SMALL_BINS = 256  # tiled prior paint with 2-entry tile bins (the overflow list used)
 
     def set_test_mode(self, flags=0, flip_round_limit=0):
         """Force fallback paths (results unchanged) and/or cap the flip rounds

@@ -187,7 +187,10 @@ int elas_b200_set_graphs(elas_handle* h, int enable);
  *                           memory (otherwise from 2^20 pixels up);
  *   ELAS_TEST_PRIOR_DIRECT  the plane prior is painted with global atomics
  *                           (otherwise below 2^20 pixels); not together with
- *                           ELAS_TEST_PRIOR_TILED.
+ *                           ELAS_TEST_PRIOR_TILED;
+ *   ELAS_TEST_PRIOR_SMALL_BINS the tiled paint keeps 2 triangles per tile in
+ *                           each tile's bin (otherwise 128), so that most go
+ *                           through the overflow list.
  * The results are the same as without the flags.  flip_round_limit > 0
  * (which implies the flip construction) caps the edge-flipping rounds
  * (0 = the library's own bound); a
@@ -200,6 +203,7 @@ int elas_b200_set_graphs(elas_handle* h, int enable);
 #define ELAS_TEST_PRIOR_DIRECT  8
 #define ELAS_TEST_DELAUNAY_FLIPS 16
 #define ELAS_TEST_DELAUNAY_STARS 32
+#define ELAS_TEST_PRIOR_SMALL_BINS 256
 int elas_b200_set_test_mode(elas_handle* h, int32_t flags, int32_t flip_round_limit);
 
 /* Per-pair latency (ms from the batch's start to the pair's completion) of

@@ -192,18 +192,22 @@ def test_forced_dense_bitset_walk(elas, preset, seed):
     assert np.array_equal(g["disp_right"].reshape(-1), ref[1])
 
 
-@pytest.mark.parametrize("preset,seed,flag", [(1, 61, "TEST_PRIOR_TILED"), (2, 62, "TEST_PRIOR_DIRECT")])
+@pytest.mark.parametrize("preset,seed,flag", [(1, 61, "TEST_PRIOR_TILED"), (2, 62, "TEST_PRIOR_DIRECT"),
+                                               (1, 63, "TEST_PRIOR_TILED TEST_PRIOR_SMALL_BINS"),
+                                               (2, 64, "TEST_PRIOR_SMALL_BINS")])
 def test_forced_prior_paint(elas, preset, seed, flag):
     """The plane prior through the paint path the image size does not pick
-    (tile by tile at 1242x375, global atomics at 2880x1988): every stage
-    bit-exact against the oracle, and the prior equal to the default path's."""
+    (tile by tile at 1242x375, global atomics at 2880x1988), and the tiled
+    paint with 2-entry tile bins (most triangles through the overflow
+    list): every stage bit-exact against the oracle, and the prior equal to
+    the default path's."""
     W, H, D = eb.synth_dims(preset)
     L, R, _, _ = eb.synth_pair(preset, seed)
     p = eb.params_config(D)
     elas.set_params(p)
     elas.process(L, R)
     ref = [elas.stage(k).copy() for k in ("prior_left", "prior_right")]
-    elas.set_test_mode(getattr(eb.Elas, flag))
+    elas.set_test_mode(sum(getattr(eb.Elas, f) for f in flag.split()))
     try:
         run_and_compare(elas, L, R, p, check_triangle=False)
         got = [elas.stage(k) for k in ("prior_left", "prior_right")]
