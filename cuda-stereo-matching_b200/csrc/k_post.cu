@@ -251,8 +251,13 @@ __global__ void __launch_bounds__(SPK_T * SPK_ROWS) k_spk_tile(PostViews pv, int
     }
 }
 
-// Links across tile borders: item k < H * tx_n is the right border of tile
-// column k % tx_n in row k / tx_n; the rest are bottom borders.
+// Links across tile borders: item k < H * (tx_n - 1) is row k % H of the
+// right border of tile column k / H; the rest are bottom borders, x
+// fastest.  Neighbouring lanes thus hold neighbouring pixel pairs of one
+// border, and a segment crossing it over many pixels makes the same union
+// (the same two tile-local roots) many times: a lane skips its union when
+// the lane before it holds the same connected pair (unions are idempotent,
+// so the segments are the same).
 __global__ void k_spk_border(PostViews pv, int W, int H, float thr, unsigned* err) {
     grid_dep_wait();
     const int view = blockIdx.z;
@@ -260,22 +265,34 @@ __global__ void k_spk_border(PostViews pv, int W, int H, float thr, unsigned* er
     int32_t* lab = pv.lab[view];
     const int txn = (W + SPK_T - 1) / SPK_T, tyn = (H + SPK_T - 1) / SPK_T;
     const long long nr = (long long)H * (txn - 1), nb = (long long)W * (tyn - 1);
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nr + nb;
-         k += (long long)gridDim.x * blockDim.x) {
-        int x, y, x2, y2;
-        if (k < nr) {
-            y = int(k / (txn - 1));
-            x = int(k % (txn - 1)) * SPK_T + SPK_T - 1;
-            x2 = x + 1; y2 = y;
-        } else {
-            const long long kb = k - nr;
-            x = int(kb % W);
-            y = int(kb / W) * SPK_T + SPK_T - 1;
-            x2 = x; y2 = y + 1;
+    const int lane = threadIdx.x & 31;
+    // every lane of a warp runs the same trip count (the shuffle below)
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long k0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); k0 < nr + nb; k0 += stride) {
+        const long long k = k0 + lane;
+        int a = -1, b = -1;
+        if (k < nr + nb) {
+            int x, y, x2, y2;
+            if (k < nr) {
+                y = int(k % H);
+                x = int(k / H) * SPK_T + SPK_T - 1;
+                x2 = x + 1; y2 = y;
+            } else {
+                const long long kb = k - nr;
+                x = int(kb % W);
+                y = int(kb / W) * SPK_T + SPK_T - 1;
+                x2 = x; y2 = y + 1;
+            }
+            const size_t i = size_t(y) * W + x, j = size_t(y2) * W + x2;
+            const float d = D[i], q = D[j];
+            if (d >= 0 && q >= 0 && fabsf(q - d) <= thr) {
+                a = lab[i];
+                b = lab[j];
+            }
         }
-        const size_t i = size_t(y) * W + x, j = size_t(y2) * W + x2;
-        const float d = D[i], q = D[j];
-        if (d >= 0 && q >= 0 && fabsf(q - d) <= thr) uf_union(lab, lab[i], lab[j], err);
+        const int pa = __shfl_up_sync(0xffffffffu, a, 1), pb = __shfl_up_sync(0xffffffffu, b, 1);
+        const bool same = lane > 0 && pa == a && pb == b;
+        if (a >= 0 && !same) uf_union(lab, a, b, err);
     }
 }
 
@@ -290,12 +307,21 @@ __global__ void k_spk_count(PostViews pv, int n, unsigned* err) {
     int32_t* acc = pv.root[view];
     const int32_t* roots = pv.roots[view];
     const int nr = min(roots[0], n);
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nr; k += gridDim.x * blockDim.x) {
-        const int i = roots[1 + k];
-        const int c = sz[i];
-        const int g = uf_find(lab, i, err);
-        atomicAdd(&acc[g], c);
-        sz[i] = -(g + 1);
+    const int lane = threadIdx.x & 31;
+    // warp-uniform trips; lanes with the same global root add their counts
+    // with one atomic (neighbouring list entries often share a segment)
+    for (int k0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); k0 < nr; k0 += gridDim.x * blockDim.x) {
+        const int k = k0 + lane;
+        int i = -1, c = 0, g = -1;
+        if (k < nr) {
+            i = roots[1 + k];
+            c = sz[i];
+            g = uf_find(lab, i, err);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, g);
+        const int total = __reduce_add_sync(peers, c);
+        if (g >= 0 && lane == __ffs(peers) - 1) atomicAdd(&acc[g], total);
+        if (i >= 0) sz[i] = -(g + 1);
     }
 }
 
