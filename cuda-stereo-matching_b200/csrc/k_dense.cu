@@ -39,36 +39,74 @@ namespace elas {
 
 namespace {
 
-// kerSolve with the row update written as fma(-y, dum, x).
-__device__ bool solve3(double A[3][3], double B[3]) {
+// kerSolve with the row update written as fma(-y, dum, x).  The pivot row
+// and column are data-dependent; every access to A and B goes through
+// compile-time indices and selects, so the system stays in registers (an
+// indexed 3x3 array would live in local memory).  The arithmetic and its
+// order are kerSolve's: the pivot row is scaled after its pivot is set to
+// 1, and the other rows are updated column by column with the pivot
+// column's entry zeroed first.
+template <int N, typename T>
+__device__ __forceinline__ T pick(const T (&v)[N], int i) {
+    T r = v[0];
+#pragma unroll
+    for (int k = 1; k < N; ++k) r = i == k ? v[k] : r;
+    return r;
+}
+__device__ __forceinline__ bool solve3(double (&A)[3][3], double (&B)[3]) {
     const double eps = 1e-20;
     int ipiv[3] = {0, 0, 0};
     int irow = 0, icol = 0;
-#pragma unroll 1
+#pragma unroll
     for (int i = 0; i < 3; ++i) {
         double big = 0.0;
+#pragma unroll
         for (int j = 0; j < 3; ++j)
             if (ipiv[j] != 1)
+#pragma unroll
                 for (int k = 0; k < 3; ++k)
                     if (ipiv[k] == 0)
                         if (fabs(A[j][k]) >= big) { big = fabs(A[j][k]); irow = j; icol = k; }
-        ++ipiv[icol];
-        if (irow != icol) {
-            for (int l = 0; l < 3; ++l) { double t = A[irow][l]; A[irow][l] = A[icol][l]; A[icol][l] = t; }
-            double t = B[irow]; B[irow] = B[icol]; B[icol] = t;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) ipiv[k] += k == icol;
+        // swap rows irow and icol (a no-op when they are equal)
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+            const double col[3] = {A[0][l], A[1][l], A[2][l]};
+            const double ar = pick(col, irow), ac = pick(col, icol);
+#pragma unroll
+            for (int r = 0; r < 3; ++r) A[r][l] = r == irow ? ac : (r == icol ? ar : A[r][l]);
         }
-        if (fabs(A[icol][icol]) < eps) return false;
-        double pivinv = __ddiv_rn(1.0, A[icol][icol]);
-        A[icol][icol] = 1.0;
-        for (int l = 0; l < 3; ++l) A[icol][l] = __dmul_rn(A[icol][l], pivinv);
-        B[icol] = __dmul_rn(B[icol], pivinv);
-        for (int ll = 0; ll < 3; ++ll)
-            if (ll != icol) {
-                double dum = A[ll][icol];
-                A[ll][icol] = 0.0;
-                for (int l = 0; l < 3; ++l) A[ll][l] = __fma_rn(-A[icol][l], dum, A[ll][l]);
-                B[ll] = __fma_rn(-B[icol], dum, B[ll]);
+        {
+            const double br = pick(B, irow), bc = pick(B, icol);
+#pragma unroll
+            for (int r = 0; r < 3; ++r) B[r] = r == irow ? bc : (r == icol ? br : B[r]);
+        }
+        double prow[3];
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+            const double col[3] = {A[0][l], A[1][l], A[2][l]};
+            prow[l] = pick(col, icol);
+        }
+        const double piv = pick(prow, icol);
+        if (fabs(piv) < eps) return false;
+        const double pivinv = __ddiv_rn(1.0, piv);
+#pragma unroll
+        for (int l = 0; l < 3; ++l) prow[l] = __dmul_rn(l == icol ? 1.0 : prow[l], pivinv);
+        const double bp = __dmul_rn(pick(B, icol), pivinv);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            if (r == icol) {
+#pragma unroll
+                for (int l = 0; l < 3; ++l) A[r][l] = prow[l];
+                B[r] = bp;
+            } else {
+                const double dum = pick(A[r], icol);
+#pragma unroll
+                for (int l = 0; l < 3; ++l) A[r][l] = __fma_rn(-prow[l], dum, l == icol ? 0.0 : A[r][l]);
+                B[r] = __fma_rn(-bp, dum, B[r]);
             }
+        }
     }
     return true;
 }
