@@ -194,7 +194,10 @@ __device__ void setup_triangle(const int32_t* tri, const int32_t* can, const int
 // exact row range of the raster and its column range).  The triangle goes
 // into each such tile's bin of PT_BIN entries at the slot its count's
 // atomic returns, or, once a bin is full, into the view's overflow list of
-// (tile, triangle) pairs (tcnt[ntiles] counts those).
+// (tile, triangle) pairs (tcnt[ntiles] counts those).  A triangle whose box
+// spans more than four tiles (the long hull triangles) has its tiles shared
+// out over the warp's lanes: one lane would wait for each returning atomic
+// in turn.
 __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__ tri0,
                                                      const int32_t* __restrict__ tri1,
                                                      const int32_t* __restrict__ ctr0,
@@ -204,45 +207,64 @@ __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__
                                                      int ntx, int ntiles, int32_t* bins, int32_t* ovf, int ovf_cap,
                                                      int bin_cap, unsigned* err) {
     grid_dep_wait();
-    const int T0 = ctr0[0], T1 = ctr1[0];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T0 + T1; i += gridDim.x * blockDim.x) {
-        const bool right = i >= T0;
+    const int T0 = ctr0[0], T1 = ctr1[0], lane = threadIdx.x & 31;
+    // whole warps step through the list, so that a warp can share the
+    // tile loop of a triangle whose bounding box spans many tiles
+    for (int base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; base < T0 + T1; base += gridDim.x * blockDim.x) {
+        const int i = base + lane;
+        const bool valid = i < T0 + T1, right = i >= T0;
         const int t = right ? i - T0 : i;
         Raster R;
-        setup_triangle((right ? tri1 : tri0) + 3 * size_t(t), can, uvd, g.cw, g.step, right, R);
-        if (!tcnt) {
-            rast[(right ? Tmax : 0) + t] = R;
-            continue;
-        }
-        int r0 = g.H, r1 = -1;
-        part_rows(R, 0, g.W, g.H, r0, r1);
-        part_rows(R, 1, g.W, g.H, r0, r1);
-        const int u0 = imax(int(R.A_u), 0), u1 = imin(int(R.C_u), g.W) - 1;
-        R.tx0 = 1; R.tx1 = 0; R.ty0 = 1; R.ty1 = 0;
-        if (r0 <= r1 && u0 <= u1) {
-            R.tx0 = u0 / PT_W; R.tx1 = u1 / PT_W;
-            R.ty0 = r0 / PT_H; R.ty1 = r1 / PT_H;
-        }
-        rast[(right ? Tmax : 0) + t] = R;
-        int32_t* c = tcnt + (right ? ntiles + 1 : 0);
-        int32_t* b = bins + (right ? size_t(ntiles) * PT_BIN : 0);
-        int32_t* o = ovf + (right ? 2 * size_t(ovf_cap) : 0);
-        for (int ty = R.ty0; ty <= R.ty1; ++ty)
-            for (int tx = R.tx0; tx <= R.tx1; ++tx) {
-                const int tile = ty * ntx + tx;
-                const int pos = atomicAdd(c + tile, 1);
-                if (pos < bin_cap) {
-                    b[size_t(tile) * PT_BIN + pos] = t;
-                } else {
-                    const int k = atomicAdd(c + ntiles, 1);
-                    if (k < ovf_cap) {
-                        o[2 * k] = tile;
-                        o[2 * k + 1] = t;
-                    } else {
-                        atomicOr(err, ERRF_BOUNDS);
-                    }
+        int tx0 = 0, tx1 = -1, ty0 = 0, ty1 = -1;
+        if (valid) {
+            setup_triangle((right ? tri1 : tri0) + 3 * size_t(t), can, uvd, g.cw, g.step, right, R);
+            if (tcnt) {
+                int r0 = g.H, r1 = -1;
+                part_rows(R, 0, g.W, g.H, r0, r1);
+                part_rows(R, 1, g.W, g.H, r0, r1);
+                const int u0 = imax(int(R.A_u), 0), u1 = imin(int(R.C_u), g.W) - 1;
+                R.tx0 = 1; R.tx1 = 0; R.ty0 = 1; R.ty1 = 0;
+                if (r0 <= r1 && u0 <= u1) {
+                    R.tx0 = tx0 = u0 / PT_W; R.tx1 = tx1 = u1 / PT_W;
+                    R.ty0 = ty0 = r0 / PT_H; R.ty1 = ty1 = r1 / PT_H;
                 }
             }
+            rast[(right ? Tmax : 0) + t] = R;
+        }
+        if (!tcnt) continue;
+        // one (tile, triangle) entry: the triangle goes into the tile's bin
+        // at the slot its count's atomic returns, or into the overflow list
+        auto drop = [&](int tile, int tt, bool rt) {
+            int32_t* c = tcnt + (rt ? ntiles + 1 : 0);
+            const int pos = atomicAdd(c + tile, 1);
+            if (pos < bin_cap) {
+                bins[(rt ? size_t(ntiles) * PT_BIN : 0) + size_t(tile) * PT_BIN + pos] = tt;
+            } else {
+                const int k = atomicAdd(c + ntiles, 1);
+                int32_t* o = ovf + (rt ? 2 * size_t(ovf_cap) : 0);
+                if (k < ovf_cap) {
+                    o[2 * k] = tile;
+                    o[2 * k + 1] = tt;
+                } else {
+                    atomicOr(err, ERRF_BOUNDS);
+                }
+            }
+        };
+        const int nx = tx1 - tx0 + 1, ntl = nx * (ty1 - ty0 + 1);   // 0 when empty
+        const bool wide = ntl > 4;
+        if (!wide)
+            for (int ty = ty0; ty <= ty1; ++ty)
+                for (int tx = tx0; tx <= tx1; ++tx) drop(ty * ntx + tx, t, right);
+        for (unsigned m = __ballot_sync(0xffffffffu, wide); m; m &= m - 1) {
+            const int src = __ffs(m) - 1;
+            const int wt = __shfl_sync(0xffffffffu, t, src), wr = __shfl_sync(0xffffffffu, int(right), src);
+            const int wx0 = __shfl_sync(0xffffffffu, tx0, src), wy0 = __shfl_sync(0xffffffffu, ty0, src);
+            const int wnx = __shfl_sync(0xffffffffu, nx, src), wn = __shfl_sync(0xffffffffu, ntl, src);
+            for (int k = lane; k < wn; k += 32) {
+                const int ty = wy0 + k / wnx, tx = wx0 + k % wnx;
+                drop(ty * ntx + tx, wt, wr != 0);
+            }
+        }
     }
 }
 
