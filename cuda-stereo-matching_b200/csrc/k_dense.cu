@@ -5,7 +5,7 @@
 // long serial scanline loops.  Here one thread per triangle solves the plane
 // (same double Gauss-Jordan as kerSolve, :321-375) and sets up the edges.
 // Two ways to paint, chosen by image size (both give the same bytes):
-//   * direct: a warp per triangle, lanes over its columns, atomics straight
+//   * direct: a warp per triangle, lanes over its pixels, atomics straight
 //     into the zeroed prior (two launches after the memset; the faster one
 //     for small images);
 //   * tiled: the set-up also finds the 64x32 prior tiles a triangle's pixels
@@ -268,9 +268,42 @@ __global__ void __launch_bounds__(256) k_prior_setup(const int32_t* __restrict__
     }
 }
 
-// Direct paint: one warp per (view, triangle), lanes over columns; every
-// pixel keeps the last covering triangle through atomicMax on the packed
-// value in the zeroed prior.
+// A warp paints one triangle's pixels inside the window [wu0, wu1) x
+// [wv0, wv1): column u of [A_u, C_u) writes the rows between the long edge
+// AC and the edge AB (u < B_u) or BC (u >= B_u), the reference's two
+// scan-line parts (KerComputeDisparity.cu:57-150) run as one column range,
+// with its contraction made explicit; the window clips exactly as the
+// image bounds do.  The lanes are laid out as cw columns x 32/cw rows, cw
+// the smallest of 4, 8, 16, 32 that covers the range, so that a narrow
+// triangle keeps most lanes busy.
+template <typename Put>
+__device__ __forceinline__ void paint_warp(const Raster& R, int wu0, int wu1, int wv0, int wv1, int lane, int dcap,
+                                           Put put) {
+    const int ub = int(R.B_u);
+    const int cu0 = imax(int(R.A_u), wu0), cu1 = imin(int(R.C_u), wu1), nc = cu1 - cu0;
+    if (nc <= 0) return;
+    const int lg = nc <= 4 ? 2 : (nc <= 8 ? 3 : (nc <= 16 ? 4 : 5));
+    const int cw = 1 << lg, cl = lane & (cw - 1), rl = lane >> lg, rh = 32 >> lg;
+    for (int c0 = cu0; c0 < cu1; c0 += cw) {
+        const int u = c0 + cl;
+        if (u >= cu1) continue;
+        const bool second = u >= ub;
+        const float ea = second ? R.BC_a : R.AB_a, eb = second ? R.BC_b : R.AB_b;
+        const float fu = float(u);
+        const int v1 = raster_row(R.AC_a, R.AC_b, u), v2 = raster_row(ea, eb, u);
+        const int va = imax(imin(v1, v2), wv0), vb = imin(imax(v1, v2), wv1);
+        for (int v = va + rl; v < vb; v += rh) {
+            const float dp = __fadd_rn(__fmaf_rn(R.pa, fu, __fmul_rn(R.pb, float(v))), R.pc);
+            int d = __float2int_rz(dp);
+            d = d <= 0 ? 0 : (d > dcap ? dcap : d);
+            put(u, v, uint32_t(d));
+        }
+    }
+}
+
+// Direct paint: one warp per (view, triangle); every pixel keeps the last
+// covering triangle through atomicMax on the packed value in the zeroed
+// prior.
 __global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict__ ctr0,
                                                       const int32_t* __restrict__ ctr1,
                                                       const Raster* __restrict__ rast, int Tmax,
@@ -286,22 +319,8 @@ __global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict_
         const Raster R = rast[(right ? Tmax : 0) + t];
         const uint32_t tag = uint32_t(t + 1) << pshift;
         uint32_t* prior = right ? prior1 : prior0;
-        for (int part = 0; part < 2; ++part) {
-            const int ua = part ? int(R.B_u) : int(R.A_u), ub = part ? int(R.C_u) : int(R.B_u);
-            if (ua == ub) continue;
-            const float ea = part ? R.BC_a : R.AB_a, eb = part ? R.BC_b : R.AB_b;
-            for (int u = imax(ua, 0) + lane; u < imin(ub, g.W); u += 32) {
-                const float fu = float(u);
-                const int v1 = raster_row(R.AC_a, R.AC_b, u), v2 = raster_row(ea, eb, u);
-                const int va = imax(imin(v1, v2), 0), vb = imin(imax(v1, v2), g.H);
-                for (int v = va; v < vb; ++v) {
-                    const float dp = __fadd_rn(__fmaf_rn(R.pa, fu, __fmul_rn(R.pb, float(v))), R.pc);
-                    int d = __float2int_rz(dp);
-                    d = d <= 0 ? 0 : (d > dcap ? dcap : d);
-                    atomicMax(&prior[size_t(v) * g.W + u], tag | uint32_t(d));
-                }
-            }
-        }
+        paint_warp(R, 0, g.W, 0, g.H, lane, dcap,
+                   [&](int u, int v, uint32_t d) { atomicMax(&prior[size_t(v) * g.W + u], tag | d); });
     }
 }
 
@@ -310,9 +329,7 @@ __global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict_
 // (triangle+1) << pshift | d_plane -- the last triangle in list order wins,
 // as a sequential rasteriser writing the triangles in order would leave it
 // -- and the tile is then written out whole (0 where nothing covers a
-// pixel), so no memset is needed.  A warp per triangle, lanes over columns;
-// coverage and values are the reference's scan-line expressions
-// (KerComputeDisparity.cu:57-150) with its contraction made explicit.
+// pixel), so no memset is needed.  A warp per triangle.
 __global__ void __launch_bounds__(256) k_prior_tiles(const Raster* __restrict__ rast, int Tmax,
                                                      const int32_t* __restrict__ tcnt,
                                                      const int32_t* __restrict__ bins,
@@ -330,26 +347,12 @@ __global__ void __launch_bounds__(256) k_prior_tiles(const Raster* __restrict__ 
     const int n = c[tile];
     const int32_t* b = bins + (view ? size_t(ntiles) * PT_BIN : 0) + size_t(tile) * PT_BIN;
     const Raster* rs = rast + (view ? Tmax : 0);
+    const int wu1 = imin(tu0 + PT_W, g.W), wv1 = imin(tv0 + PT_H, g.H);
     auto paint = [&](int t) {
         const Raster R = rs[t];
         const uint32_t tag = uint32_t(t + 1) << pshift;
-        for (int part = 0; part < 2; ++part) {
-            const int ua = part ? int(R.B_u) : int(R.A_u), ub = part ? int(R.C_u) : int(R.B_u);
-            if (ua == ub) continue;
-            const float ea = part ? R.BC_a : R.AB_a, eb = part ? R.BC_b : R.AB_b;
-            const int cu0 = imax(imax(ua, 0), tu0), cu1 = imin(imin(ub, g.W), tu0 + PT_W);
-            for (int u = cu0 + lane; u < cu1; u += 32) {
-                const float fu = float(u);
-                const int v1 = raster_row(R.AC_a, R.AC_b, u), v2 = raster_row(ea, eb, u);
-                const int va = imax(imax(imin(v1, v2), 0), tv0), vb = imin(imin(imax(v1, v2), g.H), tv0 + PT_H);
-                for (int v = va; v < vb; ++v) {
-                    const float dp = __fadd_rn(__fmaf_rn(R.pa, fu, __fmul_rn(R.pb, float(v))), R.pc);
-                    int d = __float2int_rz(dp);
-                    d = d <= 0 ? 0 : (d > dcap ? dcap : d);
-                    atomicMax(&pt[v - tv0][u - tu0], tag | uint32_t(d));
-                }
-            }
-        }
+        paint_warp(R, tu0, wu1, tv0, wv1, lane, dcap,
+                   [&](int u, int v, uint32_t d) { atomicMax(&pt[v - tv0][u - tu0], tag | d); });
     };
     for (int k = warp; k < imin(n, bin_cap); k += nw) paint(b[k]);
     if (n > bin_cap) {      // a full bin: the rest of its triangles are in the overflow list
@@ -361,8 +364,8 @@ __global__ void __launch_bounds__(256) k_prior_tiles(const Raster* __restrict__ 
     __syncthreads();
     uint32_t* prior = view ? prior1 : prior0;
     for (int i = tid; i < PT_W * PT_H; i += blockDim.x) {
-        const int r = i / PT_W, c = i - r * PT_W, u = tu0 + c, v = tv0 + r;
-        if (u < g.W && v < g.H) prior[size_t(v) * g.W + u] = pt[r][c];
+        const int r = i / PT_W, cc = i - r * PT_W, u = tu0 + cc, v = tv0 + r;
+        if (u < g.W && v < g.H) prior[size_t(v) * g.W + u] = pt[r][cc];
     }
 }
 
