@@ -637,16 +637,22 @@ __global__ void __launch_bounds__(SWEEP_Q_THREADS) k_support_sweep_q(const uint4
 // and each lane replays its chunk from its actual entry state.
 __device__ void redundant_line(int* a, uint8_t* code, int len, int lane) {
     for (int k = lane; k < len; k += 32) {
-        int d = a[k];
+        // the ten neighbours are loaded independently (no early exit), so
+        // their loads overlap
+        const int d = a[k];
         int c = 0;
         if (d >= 0) {
             c = 1;
-            for (int j = 1; j <= 5 && k + j < len; ++j) {
-                int d2 = a[k + j];
-                if (d2 >= 0 && abs(d - d2) <= 1) { c |= 2; break; }
+            bool right = false;
+#pragma unroll
+            for (int j = 1; j <= 5; ++j) {
+                const int d2 = k + j < len ? a[k + j] : -1;
+                right = right || (d2 >= 0 && abs(d - d2) <= 1);
             }
-            for (int b = 0; b < 5 && k - 1 - b >= 0; ++b) {
-                int d2 = a[k - 1 - b];
+            c |= right ? 2 : 0;
+#pragma unroll
+            for (int b = 0; b < 5; ++b) {
+                const int d2 = k - 1 - b >= 0 ? a[k - 1 - b] : -1;
                 if (d2 >= 0 && abs(d - d2) <= 1) c |= 4 << b;
             }
         }
@@ -656,6 +662,7 @@ __device__ void redundant_line(int* a, uint8_t* code, int len, int lane) {
     const int chunk = (len + 31) / 32;
     const int k0 = imin(len, lane * chunk), k1 = imin(len, k0 + chunk);
     uint32_t H0 = 0xAAAAAAAAu, H1 = 0xCCCCCCCCu, H2 = 0xF0F0F0F0u, H3 = 0xFF00FF00u, H4 = 0xFFFF0000u;
+#pragma unroll 4
     for (int k = k0; k < k1; ++k) {
         const unsigned c = code[k];
         uint32_t R = 0;
@@ -679,6 +686,7 @@ __device__ void redundant_line(int* a, uint8_t* code, int len, int lane) {
             (((h4 >> s) & 1u) << 4);
     }
     unsigned hist = mine;   // bit b: point k-1-b was removed
+#pragma unroll 4
     for (int k = k0; k < k1; ++k) {
         const unsigned c = code[k];
         const unsigned rem = (c & 1u) && (c & 2u) && ((c >> 2) & ~hist & 31u) ? 1u : 0u;
@@ -712,26 +720,43 @@ __global__ void k_redundant(int32_t* __restrict__ can, Geom g, int horizontal) {
 // k_incon and the horizontal k_redundant pass in one kernel: one CTA per
 // candidate row computes the row's inconsistency filter (as k_incon, reading
 // the unfiltered lattice) into shared memory, warp 0 runs the row's
-// redundancy recurrence there, and the row is written once.
+// redundancy recurrence there, and the row is written once.  The window's
+// lattice rows are staged in shared memory first (STAGED; windows too tall
+// for it read the lattice in place), and PARTS neighbouring lanes share a
+// candidate, each counting every PARTS-th window row; the counts are summed
+// across the lanes.  Narrow lattices (few candidates per row, too few CTAs
+// to fill the GPU) take 4 lanes per candidate, wide ones 1.
+constexpr size_t INCON_STAGE_MAX = 96 * 1024;   // shared-memory bytes up to which the window is staged
+template <bool STAGED, int PARTS>
 __global__ void k_incon_rows(const int32_t* __restrict__ cin, int32_t* __restrict__ cout, Geom g, DevParams p) {
     grid_dep_wait();
-    extern __shared__ int row[];                 // cw ints, then cw code bytes
+    extern __shared__ int sm[];                  // [window rows x cw ints when STAGED], cw ints, cw code bytes
+    const int ws = p.incon_window, y = blockIdx.x;
+    const int ylo = max(0, y - ws), yhi = min(g.ch - 1, y + ws), nr = yhi - ylo + 1;
+    int* row = sm + (STAGED ? nr * g.cw : 0);
     uint8_t* code = reinterpret_cast<uint8_t*>(row + g.cw);
-    const int y = blockIdx.x;
-    for (int x = threadIdx.x; x < g.cw; x += blockDim.x) {
-        const int d = cin[size_t(y) * g.cw + x];
-        int out = d;
-        if (d >= 0 && y < g.cw) {
-            const int ws = p.incon_window;
-            int support = 0;
-            for (int y2 = max(0, y - ws); y2 <= min(g.ch - 1, y + ws); ++y2)
-                for (int x2 = max(0, x - ws); x2 <= min(g.cw - 1, x + ws); ++x2) {
-                    const int d2 = cin[size_t(y2) * g.cw + x2];
-                    if (d2 >= 0 && abs(d - d2) <= p.incon_threshold) ++support;
+    const int* win = STAGED ? sm : cin + size_t(ylo) * g.cw;    // the window's rows, from ylo
+    if (STAGED) {
+        for (int i = threadIdx.x; i < nr * g.cw; i += blockDim.x) sm[i] = cin[size_t(ylo) * g.cw + i];
+        __syncthreads();
+    }
+    const int part = threadIdx.x % PARTS, per = blockDim.x / PARTS;
+    for (int x0 = 0; x0 < g.cw; x0 += per) {   // every lane of a warp takes the same trips (the shuffles)
+        const int x = x0 + int(threadIdx.x) / PARTS;
+        const int d = x < g.cw ? win[(y - ylo) * g.cw + x] : -1;
+        const bool check = d >= 0 && y < g.cw;
+        int support = 0;
+        if (check) {
+            const int xa = max(0, x - ws), xb = min(g.cw - 1, x + ws);
+            for (int r = part; r < nr; r += PARTS)
+                for (int x2 = xa; x2 <= xb; ++x2) {
+                    const int d2 = win[r * g.cw + x2];
+                    support += d2 >= 0 && abs(d - d2) <= p.incon_threshold;
                 }
-            if (support < p.incon_min_support) out = -1;
         }
-        row[x] = out;
+#pragma unroll
+        for (int o = 1; o < PARTS; o <<= 1) support += __shfl_xor_sync(0xffffffffu, support, o);
+        if (x < g.cw && part == 0) row[x] = check && support < p.incon_min_support ? -1 : d;
     }
     __syncthreads();
     if (threadIdx.x < 32) redundant_line(row, code, g.cw, threadIdx.x);
@@ -967,9 +992,23 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
     }
     {
         const size_t sm = size_t(g.cw) * (sizeof(int) + 1);
-        const int threads = imin(1024, imax(32, ((g.cw + 31) / 32) * 32));
-        allow_smem(k_incon_rows);
-        launch_k(k_incon_rows, g.ch, threads, sm, st, can_lr, can, g, p);
+        const size_t wsm = size_t(imin(2 * p.incon_window + 1, g.ch)) * g.cw * sizeof(int);
+        const int parts = g.cw <= 256 ? 4 : (g.cw <= 512 ? 2 : 1);
+        const int threads = imin(1024, imax(32, ((parts * g.cw + 31) / 32) * 32));
+        const bool staged = sm + wsm <= INCON_STAGE_MAX;
+        auto go = [&](auto kern, size_t bytes) {
+            allow_smem(kern);
+            launch_k(kern, g.ch, threads, bytes, st, can_lr, can, g, p);
+        };
+        if (staged) {
+            if (parts == 4) go(k_incon_rows<true, 4>, sm + wsm);
+            else if (parts == 2) go(k_incon_rows<true, 2>, sm + wsm);
+            else go(k_incon_rows<true, 1>, sm + wsm);
+        } else {
+            if (parts == 4) go(k_incon_rows<false, 4>, sm);
+            else if (parts == 2) go(k_incon_rows<false, 2>, sm);
+            else go(k_incon_rows<false, 1>, sm);
+        }
         const int wpb = 4;
         const size_t smv = size_t(wpb) * g.ch * (sizeof(int) + 1);
         launch_k(k_redundant, (g.cw + wpb - 1) / wpb, 32 * wpb, smv, st, can, g, 0);

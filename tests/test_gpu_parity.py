@@ -118,6 +118,20 @@ def test_non_default_parameters(elas):
     run_and_compare(elas, L, R, p)
 
 
+@pytest.mark.parametrize("width,height,ws", [(2000, 300, 0), (2000, 300, 10), (2000, 300, 40), (1200, 600, 60),
+                                             (2800, 300, 40)])
+def test_inconsistency_window_sizes(elas, width, height, ws):
+    """The inconsistency filter shares a candidate among 4, 2 or 1 lanes by
+    the lattice width (240, 400 and 560 candidates per row here) and stages
+    its window rows in shared memory when they fit; the half windows of 60
+    at 1200x600 and of 40 at 2000x300 and 2800x300 do not fit and read the
+    lattice in place."""
+    L, R, _, _ = eb.synth_pair(3, 21, width=width, height=height, disp_max=96)
+    p = eb.params_config(96)
+    p.incon_window_size = ws
+    run_and_compare(elas, L, R, p, check_triangle=False)
+
+
 @pytest.mark.parametrize("filt", ["speckle", "gap", "gap_wide", "mean", "median"])
 def test_post_filters_individually(elas, filt):
     L, R, _, _ = eb.synth_pair(1, 3)
