@@ -479,7 +479,10 @@ __device__ void star_stream(const DelDev& D, const int32_t* __restrict__ row_off
 // (star_walk with the two-phase searches of the search policy), its owned
 // triangles (p the smallest vertex) counted into tcnt[p] and stored as
 // vertex pairs in p's slot (or in the pool when more than STAR_SLOT).
-__global__ void __launch_bounds__(STAR_WARPS * 32, 4) k_star(DelDev d0, DelDev d1,
+// Three CTAs per SM (80 registers a thread): measured faster at 1242x375
+// than four (64 registers, more spills) and than two (no spills, but the
+// points no longer fit one wave).
+__global__ void __launch_bounds__(STAR_WARPS * 32, 3) k_star(DelDev d0, DelDev d1,
                                                            const int32_t* __restrict__ row_off, unsigned* err) {
     grid_dep_wait();
     __shared__ StarSmem smem[STAR_WARPS];
