@@ -226,6 +226,31 @@ def test_device_api_matches_host_api(elas):
     assert np.array_equal(o1.cpu().numpy(), h1) and np.array_equal(o2.cpu().numpy(), h2)
 
 
+@pytest.mark.parametrize("shift", [1, 3])
+def test_device_api_unaligned_images(elas, shift):
+    """Device images that do not start on a 16-byte boundary take the
+    descriptor's byte-wise staging; the result equals the host-buffer call
+    (whose workspace copies are aligned)."""
+    import torch
+
+    L, R, _, _ = eb.synth_pair(3, 11, width=333, height=211, disp_max=95)
+    p = eb.params_config(95)
+    elas.set_params(p)
+    h1, h2 = elas.process(L, R)
+    H, W = L.shape
+    bl = torch.zeros(H * W + 16, dtype=torch.uint8, device="cuda")
+    br = torch.zeros_like(bl)
+    bl[shift:shift + H * W] = torch.from_numpy(L.reshape(-1)).cuda()
+    br[shift:shift + H * W] = torch.from_numpy(R.reshape(-1)).cuda()
+    o1 = torch.empty((H, W), dtype=torch.float32, device="cuda")
+    o2 = torch.empty_like(o1)
+    torch.cuda.synchronize()
+    elas.process_device(bl.data_ptr() + shift, br.data_ptr() + shift, o1.data_ptr(), o2.data_ptr(), W, H,
+                        stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(o1.cpu().numpy(), h1) and np.array_equal(o2.cpu().numpy(), h2)
+
+
 def test_cpp_drop_in_class_runs(tmp_path):
     import os
     import subprocess
