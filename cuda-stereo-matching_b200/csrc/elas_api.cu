@@ -498,8 +498,8 @@ int run_pipeline(elas_handle* h, const uint8_t* img0, const uint8_t* img1, float
         bins = h->pn_bins;
         n += 6;
     }
-    CK(launch_support(h->desc0, h->desc1, h->can_lr, nullptr, h->can, g, dp, h->num_sms, h->err, st, bins,
-                      h->pn_used ? h->pn_stats : nullptr));
+    CK(launch_support(h->desc0, h->desc1, h->can_lr, nullptr, h->can, h->row_cnt, g, dp, h->num_sms, h->err, st,
+                      bins, h->pn_used ? h->pn_stats : nullptr));
     n += 3;
     CK(mark(ELAS_TIME_COMPACT));
     const int corners = p.add_corners ? 1 : 0;

@@ -696,8 +696,10 @@ __device__ void redundant_line(int* a, uint8_t* code, int len, int lane) {
     __syncwarp();
 }
 
-// One warp per line; horizontal = 1: rows, 0: columns.
-__global__ void k_redundant(int32_t* __restrict__ can, Geom g, int horizontal) {
+// One warp per line; horizontal = 1: rows, 0: columns.  row_cnt (vertical
+// pass, zeroed by k_incon_rows): every point kept adds 1 to its row's count,
+// which k_compact turns into the row's first list position.
+__global__ void k_redundant(int32_t* __restrict__ can, Geom g, int horizontal, int32_t* __restrict__ row_cnt) {
     grid_dep_wait();
     extern __shared__ int lines[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -714,6 +716,7 @@ __global__ void k_redundant(int32_t* __restrict__ can, Geom g, int horizontal) {
     for (int k = lane; k < len; k += 32) {
         if (horizontal) can[size_t(l) * g.cw + k] = a[k];
         else can[size_t(k) * g.cw + l] = a[k];
+        if (row_cnt && !horizontal && a[k] >= 0) atomicAdd(&row_cnt[k], 1);
     }
 }
 
@@ -728,8 +731,10 @@ __global__ void k_redundant(int32_t* __restrict__ can, Geom g, int horizontal) {
 // to fill the GPU) take 4 lanes per candidate, wide ones 1.
 constexpr size_t INCON_STAGE_MAX = 96 * 1024;   // shared-memory bytes up to which the window is staged
 template <bool STAGED, int PARTS>
-__global__ void k_incon_rows(const int32_t* __restrict__ cin, int32_t* __restrict__ cout, Geom g, DevParams p) {
+__global__ void k_incon_rows(const int32_t* __restrict__ cin, int32_t* __restrict__ cout, Geom g, DevParams p,
+                             int32_t* __restrict__ row_cnt) {
     grid_dep_wait();
+    if (threadIdx.x == 0) row_cnt[blockIdx.x] = 0;     // counted by the vertical redundancy pass
     extern __shared__ int sm[];                  // [window rows x cw ints when STAGED], cw ints, cw code bytes
     const int ws = p.incon_window, y = blockIdx.x;
     const int ylo = max(0, y - ws), yhi = min(g.ch - 1, y + ws), nr = yhi - ylo + 1;
@@ -764,59 +769,38 @@ __global__ void k_incon_rows(const int32_t* __restrict__ cin, int32_t* __restric
     for (int x = threadIdx.x; x < g.cw; x += blockDim.x) cout[size_t(y) * g.cw + x] = row[x];
 }
 
-// Count valid candidates per row.
-__global__ void k_row_count(const int32_t* __restrict__ can, int32_t* __restrict__ row_cnt, Geom g) {
-    grid_dep_wait();
-    __shared__ int s;
-    if (threadIdx.x == 0) s = 0;
-    __syncthreads();
-    int cnt = 0;
-    for (int x = threadIdx.x; x < g.cw; x += blockDim.x) cnt += can[size_t(blockIdx.x) * g.cw + x] >= 0;
-    cnt = __reduce_add_sync(0xffffffffu, cnt);
-    if ((threadIdx.x & 31) == 0) atomicAdd(&s, cnt);
-    __syncthreads();
-    if (threadIdx.x == 0) row_cnt[blockIdx.x] = s;
-}
-
-// Exclusive scan of the row counts (single block); row_off[ch] = total.
-// corners: three corner points lead row 0 and three more form the extra
-// row ch (row_off[ch + 1] = total + 6).
-__global__ void k_row_scan(const int32_t* __restrict__ row_cnt, int32_t* __restrict__ row_off, int n, int corners) {
-    grid_dep_wait();
-    __shared__ int part[1024];
-    const int t = threadIdx.x;
-    const int per = (n + blockDim.x - 1) / blockDim.x;
-    const int b = t * per, e = min(n, b + per);
-    int s = 0;
-    for (int i = b; i < e; ++i) s += row_cnt[i];
-    part[t] = s;
-    __syncthreads();
-    for (int o = 1; o < blockDim.x; o <<= 1) {
-        int x = t >= o ? part[t - o] : 0;
-        __syncthreads();
-        part[t] += x;
-        __syncthreads();
-    }
-    const int front = corners ? 3 : 0;
-    int run = part[t] - s;
-    for (int i = b; i < e; ++i) { row_off[i] = run + (i > 0 ? front : 0); run += row_cnt[i]; }
-    if (t == blockDim.x - 1) {
-        row_off[n] = part[t] + front;
-        if (corners) row_off[n + 1] = part[t] + 6;
-    }
-}
-
 // Write the support list in raster order: uvd (u, v, d), and the point
-// coordinates of both views (x0 = u, x1 = u - d, y = v).
-__global__ void k_compact(const int32_t* __restrict__ can, const int32_t* __restrict__ row_off,
-                          int32_t* __restrict__ uvd, int32_t* __restrict__ x0, int32_t* __restrict__ x1,
-                          int32_t* __restrict__ y, Geom g, int lead) {
+// coordinates of both views (x0 = u, x1 = u - d, y = v).  One CTA per
+// lattice row; the row's first list position is the sum of the counts of
+// the rows before it (row_cnt, counted by the vertical redundancy pass),
+// summed here, so no scan pass runs.  row_off gets every row's first
+// position, row_off[ch] the total.  front = 3 with add_corners: three
+// corner points lead row 0 (row_off[0] stays 0, row 0 spans them) and three
+// more form the extra row ch (row_off[ch + 1] = total + 6).
+__global__ void k_compact(const int32_t* __restrict__ can, const int32_t* __restrict__ row_cnt,
+                          int32_t* __restrict__ row_off, int32_t* __restrict__ uvd, int32_t* __restrict__ x0,
+                          int32_t* __restrict__ x1, int32_t* __restrict__ y, Geom g, int front) {
     grid_dep_wait();
     __shared__ int warp_tot[32];
     __shared__ int base;
     const int r = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (threadIdx.x == 0) base = row_off[r] + (r == 0 ? lead : 0);
+    int pre = 0;
+    for (int i = threadIdx.x; i < r; i += blockDim.x) pre += row_cnt[i];
+    pre = __reduce_add_sync(0xffffffffu, pre);
+    if (lane == 0) warp_tot[warp] = pre;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int sum = 0;
+        for (int w = 0; w < nw; ++w) sum += warp_tot[w];
+        base = sum + front;
+        row_off[r] = sum + (r > 0 ? front : 0);
+        if (r == g.ch - 1) {
+            const int total = sum + row_cnt[r];
+            row_off[g.ch] = total + front;
+            if (front) row_off[g.ch + 1] = total + 6;
+        }
+    }
     __syncthreads();
     for (int x0c = 0; x0c < g.cw; x0c += blockDim.x) {
         int x = x0c + threadIdx.x;
@@ -935,8 +919,8 @@ __global__ void k_grid_diffuse(const uint32_t* __restrict__ t0, const uint32_t* 
 }  // namespace
 
 cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_lr, int32_t* can_tmp,
-                           int32_t* can, const Geom& g, const DevParams& p, int num_sms, unsigned* err,
-                           cudaStream_t st, const uint32_t* bins, int32_t* stats) {
+                           int32_t* can, int32_t* row_cnt, const Geom& g, const DevParams& p, int num_sms,
+                           unsigned* err, cudaStream_t st, const uint32_t* bins, int32_t* stats) {
     // segments: about 4 CTAs per SM in flight
     int rows = g.ch;
     int segs = imax(1, (4 * num_sms + rows - 1) / imax(rows, 1));
@@ -998,7 +982,7 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
         const bool staged = sm + wsm <= INCON_STAGE_MAX;
         auto go = [&](auto kern, size_t bytes) {
             allow_smem(kern);
-            launch_k(kern, g.ch, threads, bytes, st, can_lr, can, g, p);
+            launch_k(kern, g.ch, threads, bytes, st, can_lr, can, g, p, row_cnt);
         };
         if (staged) {
             if (parts == 4) go(k_incon_rows<true, 4>, sm + wsm);
@@ -1011,19 +995,16 @@ cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_
         }
         const int wpb = 4;
         const size_t smv = size_t(wpb) * g.ch * (sizeof(int) + 1);
-        launch_k(k_redundant, (g.cw + wpb - 1) / wpb, 32 * wpb, smv, st, can, g, 0);
+        launch_k(k_redundant, (g.cw + wpb - 1) / wpb, 32 * wpb, smv, st, can, g, 0, row_cnt);
     }
     (void)can_tmp;
     return cudaGetLastError();
 }
 
-cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_off, int32_t* uvd, int32_t* x0,
+cudaError_t launch_compact(const int32_t* can, const int32_t* row_cnt, int32_t* row_off, int32_t* uvd, int32_t* x0,
                            int32_t* x1, int32_t* y, const Geom& g, cudaStream_t st, int corners, int* nlaunch) {
-    int launched = 1 + (corners ? 1 : 0);
-    launch_k(k_row_count, g.ch, 128, 0, st, can, row_cnt, g);
-    launch_k(k_row_scan, 1, 1024, 0, st, row_cnt, row_off, g.ch, corners);
-    launched += 2;
-    launch_k(k_compact, g.ch, 256, 0, st, can, row_off, uvd, x0, x1, y, g, corners ? 3 : 0);
+    const int launched = 1 + (corners ? 1 : 0);
+    launch_k(k_compact, g.ch, 256, 0, st, can, row_cnt, row_off, uvd, x0, x1, y, g, corners ? 3 : 0);
     if (corners) launch_k(k_corners, 1, 1024, 0, st, row_off, uvd, x0, x1, y, g);
     if (nlaunch) *nlaunch += launched;
     return cudaGetLastError();

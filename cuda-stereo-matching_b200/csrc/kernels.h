@@ -58,11 +58,13 @@ cudaError_t launch_descriptor(const uint8_t* img0, const uint8_t* img1, uint4* d
 // bins (nullable): packed learned search sets per candidate; then stats[0]
 // counts candidates the proposal settled and stats[1] those that fell back
 // to the full sweep.
+// row_cnt (ch entries) receives the number of support points per lattice
+// row, which launch_compact consumes.
 cudaError_t launch_support(const uint4* desc0, const uint4* desc1, int32_t* can_lr, int32_t* can_tmp,
-                           int32_t* can, const Geom& g, const DevParams& p, int num_sms, unsigned* err,
-                           cudaStream_t st, const uint32_t* bins = nullptr, int32_t* stats = nullptr);
+                           int32_t* can, int32_t* row_cnt, const Geom& g, const DevParams& p, int num_sms,
+                           unsigned* err, cudaStream_t st, const uint32_t* bins = nullptr, int32_t* stats = nullptr);
 
-cudaError_t launch_compact(const int32_t* can, int32_t* row_cnt, int32_t* row_off, int32_t* uvd, int32_t* x0,
+cudaError_t launch_compact(const int32_t* can, const int32_t* row_cnt, int32_t* row_off, int32_t* uvd, int32_t* x0,
                            int32_t* x1, int32_t* y, const Geom& g, cudaStream_t st, int corners, int* nlaunch);
 
 cudaError_t launch_grid(const int32_t* can, uint32_t* tmp0, uint32_t* tmp1, uint32_t* grid0, uint32_t* grid1,
