@@ -6,8 +6,8 @@
 // (same double Gauss-Jordan as kerSolve, :321-375) and sets up the edges.
 // Two ways to paint, chosen by image size (both give the same bytes):
 //   * direct: a warp per triangle, lanes over its pixels, atomics straight
-//     into the zeroed prior (two launches after the memset; the faster one
-//     for small images);
+//     into the zeroed prior (one launch after the memset, each warp setting
+//     its triangle up itself; the faster one for small images);
 //   * tiled: the set-up also finds the 64x32 prior tiles a triangle's pixels
 //     can fall in and drops the triangle into each tile's fixed bin (the
 //     slot its count's atomic returns; no scan), and one CTA per tile paints
@@ -301,12 +301,16 @@ __device__ __forceinline__ void paint_warp(const Raster& R, int wu0, int wu1, in
     }
 }
 
-// Direct paint: one warp per (view, triangle); every pixel keeps the last
-// covering triangle through atomicMax on the packed value in the zeroed
-// prior.
-__global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict__ ctr0,
+// Direct paint: one warp per (view, triangle), which first sets the
+// triangle up itself (every lane the same operations on the same loads, so
+// no per-triangle record goes through memory and no set-up launch runs);
+// every pixel keeps the last covering triangle through atomicMax on the
+// packed value in the zeroed prior.
+__global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict__ tri0,
+                                                      const int32_t* __restrict__ tri1,
+                                                      const int32_t* __restrict__ ctr0,
                                                       const int32_t* __restrict__ ctr1,
-                                                      const Raster* __restrict__ rast, int Tmax,
+                                                      const int32_t* __restrict__ can, const int32_t* __restrict__ uvd,
                                                       uint32_t* prior0, uint32_t* prior1, Geom g, int pshift,
                                                       int dcap) {
     grid_dep_wait();
@@ -316,7 +320,8 @@ __global__ void __launch_bounds__(256) k_prior_raster(const int32_t* __restrict_
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < T0 + T1; i += nw) {
         const bool right = i >= T0;
         const int t = right ? i - T0 : i;
-        const Raster R = rast[(right ? Tmax : 0) + t];
+        Raster R;
+        setup_triangle((right ? tri1 : tri0) + 3 * size_t(t), can, uvd, g.cw, g.step, right, R);
         const uint32_t tag = uint32_t(t + 1) << pshift;
         uint32_t* prior = right ? prior1 : prior0;
         paint_warp(R, 0, g.W, 0, g.H, lane, dcap,
@@ -602,12 +607,9 @@ cudaError_t launch_prior(const int32_t* tri0, const int32_t* tri1, const int32_t
             cudaMemsetAsync(prior0, 0, n, st);
             cudaMemsetAsync(prior1, 0, n, st);
         }
-        launch_k(k_prior_setup, tblocks, 256, 0, st, tri0, tri1, ctr0, ctr1, can, uvd, R, Tmax, g,
-                 static_cast<int32_t*>(nullptr), 0, 0, static_cast<int32_t*>(nullptr), static_cast<int32_t*>(nullptr),
-                 0, 0, err);
-        launch_k(k_prior_raster, imax(1, imin(16 * num_sms, (2 * Tmax + 7) / 8)), 256, 0, st, ctr0, ctr1, R, Tmax,
-                 prior0, prior1, g, pshift, dcap);
-        if (nlaunch) *nlaunch += 2;
+        launch_k(k_prior_raster, imax(1, imin(16 * num_sms, (2 * Tmax + 7) / 8)), 256, 0, st, tri0, tri1, ctr0, ctr1,
+                 can, uvd, prior0, prior1, g, pshift, dcap);
+        if (nlaunch) *nlaunch += 1;
         return cudaGetLastError();
     }
     const int ntx = (g.W + PT_W - 1) / PT_W, nty = (g.H + PT_H - 1) / PT_H, ntiles = ntx * nty;
