@@ -486,13 +486,15 @@ __global__ void __launch_bounds__(STAR_WARPS * 32, 3) k_star(DelDev d0, DelDev d
                                                            const int32_t* __restrict__ row_off, unsigned* err) {
     grid_dep_wait();
     __shared__ StarSmem smem[STAR_WARPS];
-    const DelDev& D = blockIdx.y ? d1 : d0;
+    // blockIdx.x is the view, so that the two views' first blocks (the ones
+    // with points) are dispatched side by side
+    const DelDev& D = blockIdx.x ? d1 : d0;
     const int N = D.ctr[9];
     const int32_t box[4] = {D.box[0], D.box[1], D.box[2], D.box[3]};
     const int R0 = D.box[4];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     StarSmem& sm = smem[warp];
-    for (int p = blockIdx.x * STAR_WARPS + warp; p < N; p += gridDim.x * STAR_WARPS) {
+    for (int p = blockIdx.y * STAR_WARPS + warp; p < N; p += gridDim.y * STAR_WARPS) {
         const uint32_t pp = D.pxy[p];
         if (pp == PXY_NONE) {
             if (lane == 0) D.tcnt[p] = 0;
@@ -1580,7 +1582,7 @@ cudaError_t launch_delaunay(DelDev& d0, DelDev& d1, const int32_t* row_off, int 
     allow_smem(k_plan);
     launch_k(k_plan, 2, 1024, plan_smem, st, d0, d1, row_off, nrows, H, flips ? 1 : 0, err);
     if (!flips) {
-        launch_k(k_star, dim3(imax(1, imin((nmax + STAR_WARPS - 1) / STAR_WARPS, 6 * num_sms)), 2), STAR_WARPS * 32,
+        launch_k(k_star, dim3(2, imax(1, imin((nmax + STAR_WARPS - 1) / STAR_WARPS, 6 * num_sms))), STAR_WARPS * 32,
                  0, st, d0, d1, row_off, err);
         launch_k(k_star_emit, dim3(imax(1, (nmax + EMIT_THREADS - 1) / EMIT_THREADS), 2), EMIT_THREADS, 0, st, d0, d1,
                  err);
