@@ -575,9 +575,9 @@ cudaError_t launch_post(PostViews pv, int nviews, const Geom& g, const DevParams
         const int gb = int(border / 256 + 1 < 4096 ? border / 256 + 1 : 4096);
         launch_k(k_spk_border, dim3(gb, 1, nviews), 256, 0, st, pv, W, H, p.speckle_sim_threshold, err);
         const int gn = imax(1, imin(8 * 1024, (n + 255) / 256));
-        // the roots list is far shorter than the image: a grid of a few CTAs
-        // per SM walks it (idle CTAs cost their launch)
-        launch_k(k_spk_count, dim3(imin(gn, 4 * num_sms), 1, nviews), 256, 0, st, pv, n, err);
+        // the roots list is far shorter than the image: a grid of one CTA per
+        // SM walks it (idle CTAs cost their launch; measured against four)
+        launch_k(k_spk_count, dim3(imin(gn, num_sms), 1, nviews), 256, 0, st, pv, n, err);
         launched += 3;
         if (!fuse) {
             launch_k(k_spk_apply, dim3(gn, 1, nviews), 256, 0, st, pv, n, p.speckle_size);
